@@ -1,0 +1,142 @@
+/*
+ * prandtl_b200.h -- C ABI of the B200 (sm_100a) DGSEM right-hand side and
+ * Runge-Kutta step of Prandtl.
+ *
+ * The reference exposes this hot path as
+ *     class DGSEMOperator : public mfem::TimeDependentOperator
+ *         void Mult(const Vector &u, Vector &dudt) const;      (src/Operators/DGSEMOperator.hpp:105)
+ *         real_t GetMaxCharSpeed();                            (DGSEMOperator.hpp:106-109)
+ *         real_t &GetTimeRef();                                (DGSEMOperator.hpp:111-114)
+ * driven by mfem::ODESolver::Step (src/Simulation/Simulation.cpp:1010).  The
+ * entry points below are what that surface binds to: plain pointers and
+ * sizes, no C++ or CUDA types.  A header-only MFEM adapter
+ * (prandtl_b200/shim/dgsem_operator_gpu.hpp) restores the class interface.
+ *
+ * Data layout (identical to the reference's mfem::Vector, Ordering::byNODES):
+ *   u[f*Ndof + e*Np^dim + node], f = 0..dim+1 (rho, rho*v, E), node
+ *   lexicographic with x fastest, Np = order + 1, Ndof = E*Np^dim.
+ * State and RHS are FP64.
+ *
+ * Every call returns a prandtl_status; nothing aborts, traps or exits.
+ * A handle owns one CUDA stream and its scratch buffers; calls on one handle
+ * are serialised, different handles are independent.
+ */
+#ifndef PRANDTL_B200_H
+#define PRANDTL_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum prandtl_status {
+    PRANDTL_OK = 0,
+    PRANDTL_EINVAL = 1,        /* bad argument or descriptor */
+    PRANDTL_ENOMEM = 2,        /* device allocation failed */
+    PRANDTL_ENONFINITE = 3,    /* non-finite state detected (NaN check) */
+    PRANDTL_ETIMEDOUT = 4,     /* a bounded wait ran out */
+    PRANDTL_ECUDA = 5,         /* CUDA runtime error (text in prandtl_last_error) */
+    PRANDTL_EUNSUPPORTED = 6   /* valid input outside what this build implements */
+} prandtl_status;
+
+/* Pointer-location flags for the u / dudt arguments. */
+#define PRANDTL_PTR_HOST 0     /* host memory: staged through the handle's device buffers */
+#define PRANDTL_PTR_DEVICE 1   /* device memory on the handle's GPU: zero-copy */
+
+/* Time-integration schemes of prandtl_step. */
+#define PRANDTL_RK3SSP 0       /* Shu-Osher SSP-RK3, mfem::RK3SSPSolver operation order */
+#define PRANDTL_LSRK45 1       /* Carpenter-Kennedy five-stage fourth-order 2N-storage RK */
+
+/* Mesh in the form the DGSEM kernels consume.  Built by the caller from its
+ * mfem::ParMesh (per element: ElementTransformation::AdjugateJacobian and
+ * Weight of the affine map from [0,1]^dim; per interior face:
+ * FaceElementTransformations Elem1No/Elem2No, local faces and CalcOrtho). */
+typedef struct prandtl_mesh_desc {
+    int dim;                   /* 2 or 3 */
+    int order;                 /* polynomial degree N (1..5); Np = N + 1 Gauss-Lobatto nodes */
+    int num_elements;          /* E */
+    int num_faces;             /* F interior faces (periodic meshes: all faces) */
+    const double *elem_adj;    /* [E][dim][dim] adjugate of the element Jacobian, row-major */
+    const double *elem_detj;   /* [E] Jacobian determinant */
+    const int *face_elems;     /* [F][4] elem1, lface1, elem2, lface2; lface = 2*dir + side,
+                                  side 0 is the xi_dir = 0 face; traces aligned */
+    const double *face_nor;    /* [F][dim] scaled normal outward from elem1 (|n| = face measure) */
+} prandtl_mesh_desc;
+
+/* Physics and switches.  Defaults (prandtl_config_default) match the
+ * reference's Simulation::LoadConfig defaults (Simulation.cpp:153-157) and
+ * PhysicsConstants (src/Physics/Physics.hpp:27-37). */
+typedef struct prandtl_config {
+    double gamma;              /* 1.4 */
+    double Pr;                 /* 0.72 */
+    double mu;                 /* 0.02, dynamic viscosity (constant unless sutherland) */
+    double R_gas;              /* 287.05 */
+    double alpha_max;          /* 0.5, blending cap (DGSEMOperator.hpp:99) */
+    double alpha_min;          /* 0.001 */
+    int parabolic;             /* 0: Euler; 1: Navier-Stokes with BR1 lifting (PARABOLIC) */
+    int blending;              /* 1: modal indicator + subcell FV blending (SUBCELL_FV_BLENDING) */
+    int sutherland;            /* 1: Sutherland viscosity (SUTHERLAND) */
+    int quirks;                /* 0: reproduce the reference bit-for-bit in intent, including its
+                                  known defects; 1: defects fixed (entropy-conservative 3D NS) */
+    int surface_dissipation;   /* 1: reference surface flux; 0: entropy-conservative surface
+                                  flux (verification switch, no reference counterpart) */
+    int precision;             /* 0: FP64 throughout (the only value accepted by this build) */
+    double timeout_s;          /* bound on every host-side wait; 0 selects 120 s */
+} prandtl_config;
+
+typedef struct prandtl_handle prandtl_handle;
+
+/* Fill *cfg with the reference defaults. */
+void prandtl_config_default(prandtl_config *cfg);
+
+/* Build an operator for one mesh (DGSEMOperator ctor, DGSEMOperator.cpp:5-50,
+ * plus DGSEMIntegrator ctor tables, DGSEMIntegrator.cpp:8-149).  Selects the
+ * current CUDA device.  Allocates all device memory it will ever use. */
+prandtl_status prandtl_create(const prandtl_mesh_desc *mesh, const prandtl_config *cfg,
+                              prandtl_handle **out);
+
+prandtl_status prandtl_destroy(prandtl_handle *h);
+
+/* dudt = L(u): one RHS evaluation (DGSEMOperator::Mult, DGSEMOperator.cpp:537-591).
+ * t is the operator time (TimeDependentOperator::SetTime); the periodic
+ * problems here are autonomous.  lambda_max (may be NULL) receives the
+ * largest |V|+c over all nodes of u (GetMaxCharSpeed with a per-call, not
+ * running, maximum).  ptr_flags: PRANDTL_PTR_HOST or PRANDTL_PTR_DEVICE. */
+prandtl_status prandtl_rhs(prandtl_handle *h, const double *u, double *dudt, double t,
+                           double *lambda_max, int ptr_flags);
+
+/* nsteps steps of size dt applied to u in place (ODESolver::Step,
+ * Simulation.cpp:1010); each stage fuses the RK update into the RHS kernel. */
+prandtl_status prandtl_step(prandtl_handle *h, double *u, double t, double dt, int scheme,
+                            int nsteps, int ptr_flags);
+
+/* Per-element blending coefficient of the last RHS evaluation ([E] values;
+ * the reference's `alpha` ParGridFunction on fes0). */
+prandtl_status prandtl_get_alpha(prandtl_handle *h, double *alpha, int ptr_flags);
+
+/* CFL step dt = cfl*hmin/(lambda_max*(N+1)^2) (Simulation.cpp:906,1017). */
+double prandtl_cfl_dt(double cfl, double hmin, double lambda_max, int order);
+
+/* Use a caller-owned cudaStream_t (passed as void*) instead of the handle's. */
+prandtl_status prandtl_set_stream(prandtl_handle *h, void *cuda_stream);
+
+/* Wait for all work on the handle's stream, at most cfg->timeout_s. */
+prandtl_status prandtl_synchronize(prandtl_handle *h);
+
+/* Number of kernels this handle has launched (instrumentation). */
+long long prandtl_kernel_launches(const prandtl_handle *h);
+
+/* Bytes of device memory owned by the handle. */
+size_t prandtl_device_bytes(const prandtl_handle *h);
+
+/* Text of the last error on this handle ("" if none); h may be NULL for the
+ * last error of a failed prandtl_create on this thread. */
+const char *prandtl_last_error(const prandtl_handle *h);
+
+const char *prandtl_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,83 @@
+/*
+ * prandtl_oracle.h -- CPU restatement of the Prandtl DGSEM right-hand side and
+ * Runge-Kutta step, used ONLY as the test oracle and as the timed CPU baseline.
+ *
+ * This is test infrastructure.  Nothing in the product (prandtl_b200/, the
+ * C-ABI library) links, loads or calls it; only tests/, __graft_entry__.smoke()
+ * and bench.py's cpu_baseline / --impl reference leg use it, as the checker.
+ *
+ * Parity status: pinned at the integrator level against the reference's own
+ * sources compiled under oracle/_ref (see oracle/ref_harness/).  The MFEM
+ * geometry pieces (Gauss-Lobatto rule, affine transformations, face normals)
+ * are restated from their mathematics on both sides.
+ *
+ * Layout conventions (identical to the product's C-ABI):
+ *   state u: MFEM Ordering::byNODES, u[f*Ndof + e*Np^dim + node], node
+ *            lexicographic with x fastest, Ndof = E*Np^dim, nf = dim+2 fields.
+ *   local face lf = 2*dir + side, side 0 is the xi_dir = 0 face, side 1 the
+ *            xi_dir = 1 face; face nodes enumerated lexicographically over the
+ *            remaining directions (lower direction fastest).
+ *   faces:   face_elems[f] = {elem1, lface1, elem2, lface2}; face_nor[f] is the
+ *            scaled normal (outward from elem1, |n| = face measure on the
+ *            [0,1] reference face), i.e. MFEM's CalcOrtho result.
+ */
+#ifndef PRANDTL_ORACLE_H
+#define PRANDTL_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oracle_mesh {
+    int dim;              /* 2 or 3 */
+    int order;            /* polynomial degree N; Np = N + 1 nodes per direction */
+    int num_elements;
+    int num_faces;
+    const double *elem_adj;   /* [E][dim][dim] adjugate of the (affine) element Jacobian */
+    const double *elem_detj;  /* [E] Jacobian determinant */
+    const int *face_elems;    /* [F][4] elem1, lface1, elem2, lface2 */
+    const double *face_nor;   /* [F][dim] */
+} oracle_mesh;
+
+typedef struct oracle_config {
+    double gamma;
+    double Pr;
+    double mu;
+    double R_gas;
+    double alpha_max;
+    double alpha_min;
+    int parabolic;            /* Navier-Stokes: BR1 lifting + viscous fluxes */
+    int blending;             /* Persson-Peraire indicator + subcell FV blending */
+    int sutherland;           /* Sutherland viscosity law */
+    int quirks;               /* 0: reproduce the reference exactly; 1: fixed */
+    int surface_dissipation;  /* 1: as the reference; 0: EC surface flux (test switch) */
+} oracle_config;
+
+/* One RHS evaluation dudt = L(u).  alpha (may be NULL) receives the per-element
+ * blending coefficient, lambda_max (may be NULL) the largest |V|+c of any state
+ * the fluxes saw.  grad (may be NULL; NS only) receives the lifted primitive
+ * gradients [dim][nf*Ndof].  Returns 0 on success. */
+int oracle_rhs(const oracle_mesh *m, const oracle_config *c, const double *u,
+               double *dudt, double *alpha, double *lambda_max, double *grad,
+               int nthreads);
+
+/* nsteps explicit steps of size dt, in place.  scheme: 0 = SSP-RK3 (Shu-Osher,
+ * MFEM RK3SSPSolver operation order), 1 = Carpenter-Kennedy LSRK4(5) 2N. */
+int oracle_step(const oracle_mesh *m, const oracle_config *c, double *u,
+                double t, double dt, int scheme, int nsteps, int nthreads);
+
+/* Gauss-Lobatto nodes/weights on [0,1] and the derivative matrix D[i][l]
+ * (Np*Np, row i = node) exactly as the oracle uses them. */
+int oracle_gl(int order, double *nodes, double *weights, double *D);
+
+/* Pointwise functions, exported for golden-vector tests. */
+double oracle_log_mean(double x, double y);
+double oracle_volume_flux(int dim, double gamma, const double *s1, const double *s2,
+                          const double *m1, const double *m2, double *F);
+double oracle_face_flux(int dim, double gamma, int quirks, int dissipation,
+                        const double *s1, const double *s2, const double *nor, double *F);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,117 @@
+"""ctypes binding of the CPU oracle (liboracle.so).
+
+Test infrastructure: imported only by tests/, __graft_entry__.smoke() and the
+cpu_baseline / --impl reference legs of bench.py, as the checker.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+class OracleMesh(C.Structure):
+    _fields_ = [("dim", C.c_int), ("order", C.c_int), ("num_elements", C.c_int),
+                ("num_faces", C.c_int), ("elem_adj", C.POINTER(C.c_double)),
+                ("elem_detj", C.POINTER(C.c_double)), ("face_elems", C.POINTER(C.c_int)),
+                ("face_nor", C.POINTER(C.c_double))]
+
+
+class OracleConfig(C.Structure):
+    _fields_ = [("gamma", C.c_double), ("Pr", C.c_double), ("mu", C.c_double),
+                ("R_gas", C.c_double), ("alpha_max", C.c_double), ("alpha_min", C.c_double),
+                ("parabolic", C.c_int), ("blending", C.c_int), ("sutherland", C.c_int),
+                ("quirks", C.c_int), ("surface_dissipation", C.c_int)]
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        dp = C.POINTER(C.c_double)
+        L.oracle_rhs.argtypes = [C.POINTER(OracleMesh), C.POINTER(OracleConfig), dp, dp, dp, dp, dp, C.c_int]
+        L.oracle_rhs.restype = C.c_int
+        L.oracle_step.argtypes = [C.POINTER(OracleMesh), C.POINTER(OracleConfig), dp, C.c_double,
+                                  C.c_double, C.c_int, C.c_int, C.c_int]
+        L.oracle_step.restype = C.c_int
+        L.oracle_gl.argtypes = [C.c_int, dp, dp, dp]
+        L.oracle_log_mean.argtypes = [C.c_double, C.c_double]
+        L.oracle_log_mean.restype = C.c_double
+        L.oracle_volume_flux.argtypes = [C.c_int, C.c_double, dp, dp, dp, dp, dp]
+        L.oracle_volume_flux.restype = C.c_double
+        L.oracle_face_flux.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, dp, dp, dp, dp]
+        L.oracle_face_flux.restype = C.c_double
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Oracle:
+    """Holds one mesh + physics configuration for repeated oracle calls."""
+
+    def __init__(self, mesh, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05, alpha_max=0.5,
+                 alpha_min=0.001, parabolic=0, blending=0, sutherland=0, quirks=0,
+                 surface_dissipation=1, nthreads=None):
+        self.mesh = mesh
+        self._adj = np.ascontiguousarray(mesh.elem_adj, dtype=np.float64)
+        self._detj = np.ascontiguousarray(mesh.elem_detj, dtype=np.float64)
+        self._faces = np.ascontiguousarray(mesh.face_elems, dtype=np.int32)
+        self._nor = np.ascontiguousarray(mesh.face_nor, dtype=np.float64)
+        self.m = OracleMesh(mesh.dim, mesh.order, mesh.num_elements, mesh.num_faces,
+                            _p(self._adj), _p(self._detj),
+                            self._faces.ctypes.data_as(C.POINTER(C.c_int)), _p(self._nor))
+        self.c = OracleConfig(gamma, Pr, mu, R_gas, alpha_max, alpha_min, parabolic, blending,
+                              sutherland, quirks, surface_dissipation)
+        self.nthreads = nthreads or os.cpu_count() or 1
+
+    @property
+    def size(self):
+        return self.mesh.num_fields * self.mesh.ndof
+
+    def rhs(self, u, want_alpha=False, want_grad=False):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        dudt = np.empty_like(u)
+        alpha = np.empty(self.mesh.num_elements) if want_alpha else None
+        lam = np.zeros(1)
+        grad = np.empty(self.mesh.dim * u.size) if want_grad else None
+        rc = lib().oracle_rhs(C.byref(self.m), C.byref(self.c), _p(u), _p(dudt),
+                              _p(alpha) if alpha is not None else None, _p(lam),
+                              _p(grad) if grad is not None else None, self.nthreads)
+        if rc != 0:
+            raise RuntimeError(f"oracle_rhs failed ({rc})")
+        out = {"dudt": dudt, "lambda_max": float(lam[0])}
+        if alpha is not None:
+            out["alpha"] = alpha
+        if grad is not None:
+            out["grad"] = grad
+        return out
+
+    def step(self, u, dt, scheme=1, nsteps=1, t=0.0):
+        u = np.array(u, dtype=np.float64, copy=True)
+        rc = lib().oracle_step(C.byref(self.m), C.byref(self.c), _p(u), t, dt, scheme, nsteps,
+                               self.nthreads)
+        if rc != 0:
+            raise RuntimeError(f"oracle_step failed ({rc})")
+        return u
+
+
+def gl(order):
+    n = order + 1
+    x, w, D = np.empty(n), np.empty(n), np.empty(n * n)
+    lib().oracle_gl(order, _p(x), _p(w), _p(D))
+    return x, w, D.reshape(n, n)

@@ -1,0 +1,526 @@
+// prandtl_api.cu -- host side of the C ABI (include/prandtl_b200.h).
+//
+// Owns the per-mesh device state: geometry and neighbour tables, the 1D
+// operator tables, scratch (NS gradients, RK registers, staging) and one CUDA
+// stream.  All waits are bounded by the configured timeout.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/prandtl_b200.h"
+#include "dgsem_kernels.cuh"
+
+using namespace prandtl;
+
+struct prandtl_handle {
+    int dim = 0, order = 0, Np = 0, nd = 0, nf = 0, E = 0, F = 0;
+    long long Ndof = 0;
+    prandtl_config cfg{};
+    PhysParams P{};
+    OpTables T{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaEvent_t done = nullptr;
+    // device memory
+    double *d_geo = nullptr;
+    int4 *d_nbr = nullptr;
+    double *d_fnor = nullptr;
+    double *d_in = nullptr, *d_out = nullptr;     // staging / ping-pong states
+    double *d_rk1 = nullptr, *d_rk2 = nullptr;    // RK registers
+    double *d_grad = nullptr;                     // NS primitive gradients
+    double *d_alpha = nullptr;
+    unsigned long long *d_lambda = nullptr;
+    size_t bytes = 0;
+    long long launches = 0;
+    std::string err;
+    std::mutex mu;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+prandtl_status fail(prandtl_handle *h, prandtl_status st, const std::string &msg) {
+    if (h) h->err = msg;
+    else g_create_error = msg;
+    return st;
+}
+
+prandtl_status cuda_fail(prandtl_handle *h, cudaError_t e, const char *what) {
+    std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+    return fail(h, e == cudaErrorMemoryAllocation ? PRANDTL_ENOMEM : PRANDTL_ECUDA, msg);
+}
+
+#define CK(h, call, what)                                   \
+    do {                                                    \
+        cudaError_t _e = (call);                            \
+        if (_e != cudaSuccess) return cuda_fail(h, _e, what); \
+    } while (0)
+
+// ---- 1D tables (mirrors DGSEMIntegrator.cpp:41-82 and ModalBasis.cpp:110-135)
+long double legendre_ld(int n, long double x, long double *dp) {
+    long double p0 = 1.0L, p1 = x, dp0 = 0.0L, dp1 = 1.0L;
+    if (n == 0) { *dp = 0.0L; return 1.0L; }
+    for (int k = 1; k < n; ++k) {
+        long double p2 = ((2 * k + 1) * x * p1 - k * p0) / (k + 1);
+        long double dp2 = dp0 + (2 * k + 1) * p1;
+        p0 = p1; p1 = p2; dp0 = dp1; dp1 = dp2;
+    }
+    *dp = dp1;
+    return p1;
+}
+
+void build_tables(int N, OpTables &T) {
+    const int Np = N + 1;
+    std::memset(&T, 0, sizeof(T));
+    // Gauss-Lobatto nodes/weights on [0,1]
+    const long double pi = 3.14159265358979323846264338327950288L;
+    std::vector<long double> xs(Np);
+    for (int i = 0; i < Np; ++i) {
+        long double xi = -cosl(pi * i / N);
+        if (i > 0 && i < N)
+            for (int it = 0; it < 100; ++it) {
+                long double dP, P = legendre_ld(N, xi, &dP);
+                long double dx = ((1.0L - xi * xi) * dP) / (-(long double)N * (N + 1) * P);
+                xi -= dx;
+                if (fabsl(dx) < 1e-30L) break;
+            }
+        xs[i] = xi;
+    }
+    for (int i = 0; i < Np; ++i) {
+        long double dP, P = legendre_ld(N, xs[i], &dP);
+        T.x[i] = (double)((xs[i] + 1.0L) * 0.5L);
+        T.w[i] = (double)(2.0L / ((long double)N * (N + 1) * P * P) * 0.5L);
+    }
+    T.x[0] = 0.0;
+    T.x[N] = 1.0;
+    // barycentric differentiation matrix
+    std::vector<double> wb(Np, 1.0);
+    for (int i = 1; i < Np; ++i)
+        for (int j = 0; j < i; ++j) {
+            wb[j] *= (T.x[j] - T.x[i]);
+            wb[i] *= (T.x[i] - T.x[j]);
+        }
+    for (int i = 0; i < Np; ++i) wb[i] = 1.0 / wb[i];
+    for (int iL = 0; iL < Np; ++iL)
+        for (int i = 0; i < Np; ++i)
+            if (iL != i) {
+                T.D[i * Np + iL] = wb[iL] / wb[i] / (T.x[i] - T.x[iL]);
+                T.D[i * Np + i] -= T.D[i * Np + iL];
+            }
+    for (int q = 0; q < Np * Np; ++q) {
+        T.Dhat[q] = T.D[q];
+        T.Dhat2[q] = 2.0 * T.D[q];
+    }
+    T.Dhat[0] += 1.0 / T.w[0];
+    T.Dhat[(Np - 1) * Np + Np - 1] -= 1.0 / T.w[Np - 1];
+    T.Dhat2[0] += 1.0 / T.w[0];
+    T.Dhat2[(Np - 1) * Np + Np - 1] -= 1.0 / T.w[Np - 1];
+    // 1D Vandermonde of shifted Legendre P_a(2x-1): V[l][a], inverted (Gauss-Jordan)
+    std::vector<double> V(Np * Np), I(Np * Np, 0.0);
+    for (int l = 0; l < Np; ++l) {
+        double u[8], z = 2.0 * T.x[l] - 1.0;
+        u[0] = 1.0;
+        if (N >= 1) u[1] = z;
+        for (int n = 1; n < N; ++n) u[n + 1] = ((2 * n + 1) * z * u[n] - n * u[n - 1]) / (n + 1);
+        for (int a = 0; a < Np; ++a) V[l * Np + a] = u[a];
+    }
+    for (int i = 0; i < Np; ++i) I[i * Np + i] = 1.0;
+    for (int c = 0; c < Np; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < Np; ++r)
+            if (std::fabs(V[r * Np + c]) > std::fabs(V[piv * Np + c])) piv = r;
+        for (int k = 0; k < Np; ++k) {
+            std::swap(V[c * Np + k], V[piv * Np + k]);
+            std::swap(I[c * Np + k], I[piv * Np + k]);
+        }
+        const double d = 1.0 / V[c * Np + c];
+        for (int k = 0; k < Np; ++k) { V[c * Np + k] *= d; I[c * Np + k] *= d; }
+        for (int r = 0; r < Np; ++r) {
+            if (r == c) continue;
+            const double f = V[r * Np + c];
+            for (int k = 0; k < Np; ++k) { V[r * Np + k] -= f * V[c * Np + k]; I[r * Np + k] -= f * I[c * Np + k]; }
+        }
+    }
+    // I = V^{-1}: I[a][l] maps nodal values (l) to mode a
+    for (int q = 0; q < Np * Np; ++q) T.Vinv[q] = I[q];
+}
+
+void build_phys(const prandtl_config &c, int N, PhysParams &P) {
+    P.gamma = c.gamma;
+    P.gammaM1 = c.gamma - 1.0;
+    P.gammaM1Inverse = 1.0 / P.gammaM1;
+    P.PrInverse = 1.0 / c.Pr;
+    P.mu = c.mu;
+    P.mu_bulk = 2.0 / 3.0;     // Physics.hpp:34
+    P.R_gas = c.R_gas;
+    P.mu0 = 1.716e-5;          // Physics.hpp:35-37
+    P.T0 = 273.15;
+    P.Ts = 110.4;
+    P.T0pTs = P.T0 + P.Ts;
+    P.alpha_max = c.alpha_max;
+    P.alpha_min = c.alpha_min;
+    P.modal_threshold = 0.5 * std::pow(10.0, -1.8 * std::pow((double)N, 0.25));   // DGSEMOperator.cpp:25
+    P.sutherland = c.sutherland;
+    P.quirks = c.quirks;
+    P.dissipation = c.surface_dissipation;
+    P.blending = c.blending;
+}
+
+prandtl_status wait_stream(prandtl_handle *h) {
+    cudaError_t e = cudaEventRecord(h->done, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaEventRecord");
+    const double limit = h->cfg.timeout_s > 0 ? h->cfg.timeout_s : 120.0;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        e = cudaEventQuery(h->done);
+        if (e == cudaSuccess) return PRANDTL_OK;
+        if (e != cudaErrorNotReady) return cuda_fail(h, e, "device work failed");
+        const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > limit) return fail(h, PRANDTL_ETIMEDOUT, "wait for the handle's stream timed out");
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+MeshDev mesh_dev(const prandtl_handle *h) {
+    MeshDev m;
+    m.geo = h->d_geo;
+    m.nbr = h->d_nbr;
+    m.fnor = h->d_fnor;
+    m.E = h->E;
+    m.Ndof = h->Ndof;
+    return m;
+}
+
+// One RHS evaluation of `u` with the given epilogue.
+prandtl_status run_rhs(prandtl_handle *h, const double *u, RhsArgs a) {
+    const MeshDev m = mesh_dev(h);
+    a.u = u;
+    const bool ns = h->cfg.parabolic != 0;
+    if (ns) {
+        LiftArgs la{u, h->d_grad};
+        cudaError_t e = launch_lift(h->dim, h->order, m, la, h->P, h->T, h->stream);
+        if (e != cudaSuccess) return cuda_fail(h, e, "lift kernel launch");
+        h->launches++;
+        a.grad = h->d_grad;
+    }
+    a.alpha = h->cfg.blending ? h->d_alpha : nullptr;
+    cudaError_t e = launch_rhs(h->dim, h->order, ns, m, a, h->P, h->T, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "rhs kernel launch");
+    h->launches++;
+    return PRANDTL_OK;
+}
+
+void free_all(prandtl_handle *h) {
+    cudaFree(h->d_geo);
+    cudaFree(h->d_nbr);
+    cudaFree(h->d_fnor);
+    cudaFree(h->d_in);
+    cudaFree(h->d_out);
+    cudaFree(h->d_rk1);
+    cudaFree(h->d_rk2);
+    cudaFree(h->d_grad);
+    cudaFree(h->d_alpha);
+    cudaFree(h->d_lambda);
+    if (h->done) cudaEventDestroy(h->done);
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+}
+
+template <typename T>
+prandtl_status dalloc(prandtl_handle *h, T **p, size_t count, const char *what) {
+    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+    if (e != cudaSuccess) { *p = nullptr; return cuda_fail(h, e, what); }
+    h->bytes += count * sizeof(T);
+    return PRANDTL_OK;
+}
+
+}   // namespace
+
+extern "C" {
+
+void prandtl_config_default(prandtl_config *c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->gamma = 1.4;
+    c->Pr = 0.72;
+    c->mu = 0.02;
+    c->R_gas = 287.05;
+    c->alpha_max = 0.5;
+    c->alpha_min = 0.001;
+    c->surface_dissipation = 1;
+    c->timeout_s = 120.0;
+}
+
+prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config *cfg,
+                              prandtl_handle **out) {
+    g_create_error.clear();
+    if (!out) return fail(nullptr, PRANDTL_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (!md || !cfg) return fail(nullptr, PRANDTL_EINVAL, "mesh or config is NULL");
+    if (md->dim != 2 && md->dim != 3) return fail(nullptr, PRANDTL_EUNSUPPORTED, "dim must be 2 or 3");
+    if (!order_supported(md->dim, md->order))
+        return fail(nullptr, PRANDTL_EUNSUPPORTED, "order must be in 1..5");
+    if (md->num_elements <= 0 || md->num_faces < 0) return fail(nullptr, PRANDTL_EINVAL, "bad sizes");
+    if (!md->elem_adj || !md->elem_detj || (md->num_faces > 0 && (!md->face_elems || !md->face_nor)))
+        return fail(nullptr, PRANDTL_EINVAL, "mesh arrays missing");
+    if (cfg->precision != 0) return fail(nullptr, PRANDTL_EUNSUPPORTED, "only precision 0 (FP64) is built");
+    if (!(cfg->gamma > 1.0) || !(cfg->Pr > 0.0)) return fail(nullptr, PRANDTL_EINVAL, "bad gamma/Pr");
+
+    const int dim = md->dim, NFACE = 2 * dim, E = md->num_elements, F = md->num_faces;
+    // neighbour table: every element face must be an interior face exactly once
+    std::vector<int4> nbr((size_t)E * NFACE, make_int4(-1, -1, -1, -1));
+    for (int f = 0; f < F; ++f) {
+        const int *fe = md->face_elems + 4 * f;
+        const int e1 = fe[0], l1 = fe[1], e2 = fe[2], l2 = fe[3];
+        if (e1 < 0 || e1 >= E || e2 < 0 || e2 >= E || l1 < 0 || l1 >= NFACE || l2 < 0 || l2 >= NFACE)
+            return fail(nullptr, PRANDTL_EINVAL, "face " + std::to_string(f) + " out of range");
+        if ((l1 >> 1) != (l2 >> 1) || (l1 ^ l2) != 1)
+            return fail(nullptr, PRANDTL_EUNSUPPORTED,
+                        "face " + std::to_string(f) + ": only aligned opposite faces are supported");
+        int4 &a = nbr[(size_t)e1 * NFACE + l1];
+        int4 &b = nbr[(size_t)e2 * NFACE + l2];
+        if (a.x >= 0 || b.x >= 0)
+            return fail(nullptr, PRANDTL_EINVAL, "element face listed twice (face " + std::to_string(f) + ")");
+        a = make_int4(e2, l2, f, 0);
+        b = make_int4(e1, l1, f, 1);
+    }
+    for (size_t q = 0; q < nbr.size(); ++q)
+        if (nbr[q].x < 0)
+            return fail(nullptr, PRANDTL_EUNSUPPORTED,
+                        "element " + std::to_string(q / NFACE) + " has a boundary face; only periodic meshes are built");
+    for (int e = 0; e < E; ++e)
+        if (!(md->elem_detj[e] > 0.0)) return fail(nullptr, PRANDTL_EINVAL, "non-positive det J");
+
+    int ndev = 0;
+    cudaError_t ce = cudaGetDeviceCount(&ndev);
+    if (ce != cudaSuccess || ndev == 0)
+        return fail(nullptr, PRANDTL_ECUDA, std::string("no CUDA device: ") + cudaGetErrorString(ce));
+
+    prandtl_handle *h = new prandtl_handle();
+    h->dim = dim;
+    h->order = md->order;
+    h->Np = md->order + 1;
+    h->nd = 1;
+    for (int d = 0; d < dim; ++d) h->nd *= h->Np;
+    h->nf = dim + 2;
+    h->E = E;
+    h->F = F;
+    h->Ndof = (long long)E * h->nd;
+    h->cfg = *cfg;
+    if (h->cfg.timeout_s <= 0) h->cfg.timeout_s = 120.0;
+    build_tables(md->order, h->T);
+    build_phys(h->cfg, md->order, h->P);
+    cudaGetDevice(&h->device);
+
+    auto bail = [&](prandtl_status st) {
+        g_create_error = h->err;
+        free_all(h);
+        delete h;
+        return st;
+    };
+    prandtl_status st;
+    if ((ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(cuda_fail(h, ce, "cudaStreamCreate"));
+    h->own_stream = true;
+    if ((ce = cudaEventCreateWithFlags(&h->done, cudaEventDisableTiming)) != cudaSuccess)
+        return bail(cuda_fail(h, ce, "cudaEventCreate"));
+    const size_t S = (size_t)h->nf * h->Ndof;
+    const int GEO = dim * dim + 1;
+    if ((st = dalloc(h, &h->d_geo, (size_t)E * GEO, "geometry")) != PRANDTL_OK) return bail(st);
+    if ((st = dalloc(h, &h->d_nbr, nbr.size(), "neighbours")) != PRANDTL_OK) return bail(st);
+    if ((st = dalloc(h, &h->d_fnor, (size_t)(F > 0 ? F : 1) * dim, "normals")) != PRANDTL_OK) return bail(st);
+    if ((st = dalloc(h, &h->d_in, S, "state in")) != PRANDTL_OK) return bail(st);
+    if ((st = dalloc(h, &h->d_out, S, "state out")) != PRANDTL_OK) return bail(st);
+    if ((st = dalloc(h, &h->d_rk1, S, "rk register 1")) != PRANDTL_OK) return bail(st);
+    if ((st = dalloc(h, &h->d_rk2, S, "rk register 2")) != PRANDTL_OK) return bail(st);
+    if (cfg->parabolic && (st = dalloc(h, &h->d_grad, (size_t)dim * S, "gradients")) != PRANDTL_OK) return bail(st);
+    if ((st = dalloc(h, &h->d_alpha, (size_t)E, "alpha")) != PRANDTL_OK) return bail(st);
+    if ((st = dalloc(h, &h->d_lambda, 1, "lambda")) != PRANDTL_OK) return bail(st);
+
+    std::vector<double> geo((size_t)E * GEO);
+    for (int e = 0; e < E; ++e) {
+        for (int q = 0; q < dim * dim; ++q) geo[(size_t)e * GEO + q] = md->elem_adj[(size_t)e * dim * dim + q];
+        geo[(size_t)e * GEO + dim * dim] = md->elem_detj[e];
+    }
+    if ((ce = cudaMemcpy(h->d_geo, geo.data(), geo.size() * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return bail(cuda_fail(h, ce, "upload geometry"));
+    if ((ce = cudaMemcpy(h->d_nbr, nbr.data(), nbr.size() * sizeof(int4), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return bail(cuda_fail(h, ce, "upload neighbours"));
+    if (F > 0 && (ce = cudaMemcpy(h->d_fnor, md->face_nor, (size_t)F * dim * sizeof(double),
+                                  cudaMemcpyHostToDevice)) != cudaSuccess)
+        return bail(cuda_fail(h, ce, "upload normals"));
+    if ((ce = cudaMemset(h->d_alpha, 0, (size_t)E * sizeof(double))) != cudaSuccess)
+        return bail(cuda_fail(h, ce, "memset alpha"));
+    *out = h;
+    return PRANDTL_OK;
+}
+
+prandtl_status prandtl_destroy(prandtl_handle *h) {
+    if (!h) return PRANDTL_EINVAL;
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        cudaSetDevice(h->device);
+        if (h->stream) wait_stream(h);
+        free_all(h);
+    }
+    delete h;
+    return PRANDTL_OK;
+}
+
+prandtl_status prandtl_rhs(prandtl_handle *h, const double *u, double *dudt, double t,
+                           double *lambda_max, int ptr_flags) {
+    (void)t;
+    if (!h || !u || !dudt) return h ? fail(h, PRANDTL_EINVAL, "null pointer") : PRANDTL_EINVAL;
+    std::lock_guard<std::mutex> lk(h->mu);
+    h->err.clear();
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    const size_t bytes = (size_t)h->nf * h->Ndof * sizeof(double);
+    const bool dev = (ptr_flags & PRANDTL_PTR_DEVICE) != 0;
+    const double *u_d = u;
+    double *dudt_d = dudt;
+    if (!dev) {
+        CK(h, cudaMemcpyAsync(h->d_in, u, bytes, cudaMemcpyHostToDevice, h->stream), "H2D u");
+        u_d = h->d_in;
+        dudt_d = h->d_out;
+    }
+    if (lambda_max) CK(h, cudaMemsetAsync(h->d_lambda, 0, sizeof(unsigned long long), h->stream), "memset");
+    RhsArgs a{};
+    a.dudt = dudt_d;
+    a.lambda = lambda_max ? h->d_lambda : nullptr;
+    a.mode = EPI_STORE;
+    prandtl_status st = run_rhs(h, u_d, a);
+    if (st != PRANDTL_OK) return st;
+    unsigned long long lam_bits = 0;
+    if (!dev) CK(h, cudaMemcpyAsync(dudt, h->d_out, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H dudt");
+    if (lambda_max)
+        CK(h, cudaMemcpyAsync(&lam_bits, h->d_lambda, sizeof(lam_bits), cudaMemcpyDeviceToHost, h->stream), "D2H lambda");
+    if (!dev || lambda_max) {
+        st = wait_stream(h);
+        if (st != PRANDTL_OK) return st;
+    }
+    if (lambda_max) {
+        double v;
+        std::memcpy(&v, &lam_bits, sizeof(v));
+        *lambda_max = v;
+    }
+    return PRANDTL_OK;
+}
+
+prandtl_status prandtl_step(prandtl_handle *h, double *u, double t, double dt, int scheme,
+                            int nsteps, int ptr_flags) {
+    (void)t;
+    if (!h || !u) return h ? fail(h, PRANDTL_EINVAL, "null pointer") : PRANDTL_EINVAL;
+    if (nsteps < 0 || !(std::isfinite(dt))) return fail(h, PRANDTL_EINVAL, "bad nsteps/dt");
+    if (scheme != PRANDTL_RK3SSP && scheme != PRANDTL_LSRK45) return fail(h, PRANDTL_EINVAL, "unknown scheme");
+    std::lock_guard<std::mutex> lk(h->mu);
+    h->err.clear();
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    const size_t bytes = (size_t)h->nf * h->Ndof * sizeof(double);
+    const bool dev = (ptr_flags & PRANDTL_PTR_DEVICE) != 0;
+    double *x = u;
+    if (!dev) {
+        CK(h, cudaMemcpyAsync(h->d_in, u, bytes, cudaMemcpyHostToDevice, h->stream), "H2D u");
+        x = h->d_in;
+    }
+    prandtl_status st = PRANDTL_OK;
+    if (scheme == PRANDTL_RK3SSP) {
+        double *y1 = h->d_rk1, *y2 = h->d_rk2;
+        for (int s = 0; s < nsteps && st == PRANDTL_OK; ++s) {
+            RhsArgs a{};
+            a.dt = dt;
+            a.x0 = x;
+            a.mode = EPI_SSP1; a.u_out = y1;
+            if ((st = run_rhs(h, x, a)) != PRANDTL_OK) break;
+            a.mode = EPI_SSP2; a.u_out = y2;
+            if ((st = run_rhs(h, y1, a)) != PRANDTL_OK) break;
+            a.mode = EPI_SSP3; a.u_out = x;
+            st = run_rhs(h, y2, a);
+        }
+    } else {
+        static const double A[5] = {0.0, -567301805773.0 / 1357537059087.0,
+                                    -2404267990393.0 / 2016746695238.0,
+                                    -3550918686646.0 / 2091501179385.0,
+                                    -1275806237668.0 / 842570457699.0};
+        static const double B[5] = {1432997174477.0 / 9575080441755.0,
+                                    5161836677717.0 / 13612068292357.0,
+                                    1720146321549.0 / 2090206949498.0,
+                                    3134564353537.0 / 4481467310338.0,
+                                    2277821191437.0 / 14882151754819.0};
+        double *cur = x, *other = (x == h->d_in) ? h->d_out : h->d_rk2;
+        double *du = h->d_rk1;
+        for (int s = 0; s < nsteps && st == PRANDTL_OK; ++s)
+            for (int k = 0; k < 5; ++k) {
+                RhsArgs a{};
+                a.mode = EPI_LSRK;
+                a.dt = dt;
+                a.rkA = A[k];
+                a.rkB = B[k];
+                a.du = du;
+                a.u_out = other;
+                if ((st = run_rhs(h, cur, a)) != PRANDTL_OK) break;
+                std::swap(cur, other);
+            }
+        if (st == PRANDTL_OK && cur != x)
+            CK(h, cudaMemcpyAsync(x, cur, bytes, cudaMemcpyDeviceToDevice, h->stream), "copy result");
+    }
+    if (st != PRANDTL_OK) return st;
+    if (!dev) {
+        CK(h, cudaMemcpyAsync(u, x, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H u");
+        st = wait_stream(h);
+    }
+    return st;
+}
+
+prandtl_status prandtl_get_alpha(prandtl_handle *h, double *alpha, int ptr_flags) {
+    if (!h || !alpha) return h ? fail(h, PRANDTL_EINVAL, "null pointer") : PRANDTL_EINVAL;
+    std::lock_guard<std::mutex> lk(h->mu);
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    const bool dev = (ptr_flags & PRANDTL_PTR_DEVICE) != 0;
+    CK(h, cudaMemcpyAsync(alpha, h->d_alpha, (size_t)h->E * sizeof(double),
+                          dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream),
+       "copy alpha");
+    return wait_stream(h);
+}
+
+double prandtl_cfl_dt(double cfl, double hmin, double lambda_max, int order) {
+    return cfl * hmin / (lambda_max * std::pow(order + 1, 2));
+}
+
+prandtl_status prandtl_set_stream(prandtl_handle *h, void *cuda_stream) {
+    if (!h) return PRANDTL_EINVAL;
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (h->own_stream && h->stream) {
+        prandtl_status st = wait_stream(h);
+        if (st != PRANDTL_OK) return st;
+        cudaStreamDestroy(h->stream);
+    }
+    h->stream = (cudaStream_t)cuda_stream;
+    h->own_stream = false;
+    return PRANDTL_OK;
+}
+
+prandtl_status prandtl_synchronize(prandtl_handle *h) {
+    if (!h) return PRANDTL_EINVAL;
+    std::lock_guard<std::mutex> lk(h->mu);
+    return wait_stream(h);
+}
+
+long long prandtl_kernel_launches(const prandtl_handle *h) { return h ? h->launches : 0; }
+
+size_t prandtl_device_bytes(const prandtl_handle *h) { return h ? h->bytes : 0; }
+
+const char *prandtl_last_error(const prandtl_handle *h) {
+    return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+const char *prandtl_version(void) { return "prandtl_b200 0.1 (sm_100a, FP64)"; }
+
+}   // extern "C"

@@ -1,0 +1,204 @@
+"""Periodic hexahedral / quadrilateral meshes in the descriptor form the C-ABI takes.
+
+The reference reads its meshes through MFEM (``Simulation.cpp:271-336``) and the
+DGSEM kernels only ever see, per element, the affine Jacobian's adjugate and
+determinant (``ElementTransformation::AdjugateJacobian`` / ``Weight``), and per
+interior face the two neighbouring elements plus MFEM's ``CalcOrtho`` scaled
+normal (outward from ``Elem1``).  This module builds exactly that for a
+periodic box of ``n[0] x ... x n[dim-1]`` elements, optionally sheared by a
+global affine map (every element stays a parallelogram / parallelepiped).
+
+Element order is lexicographic (x fastest).  Which element of a face is
+``Elem1`` follows MFEM's face generation: elements are visited in order and
+each element's local faces in MFEM's local order; the first visitor owns the
+face.  For n >= 2 that is the lower element index; for n == 1 the face joins an
+element to itself and the first local face in MFEM's order is Elem1's.
+
+Local faces are numbered ``lf = 2*dir + side`` (side 0: xi_dir = 0).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# MFEM's local face order as (dir, side): Geometry::SQUARE faces 0..3 are
+# y=0, x=1, y=1, x=0; Geometry::CUBE faces 0..5 are z=0, y=0, x=1, y=1, x=0, z=1.
+_MFEM_FACE_ORDER = {
+    2: [(1, 0), (0, 1), (1, 1), (0, 0)],
+    3: [(2, 0), (1, 0), (0, 1), (1, 1), (0, 0), (2, 1)],
+}
+
+
+def gauss_lobatto(order: int):
+    """Gauss-Lobatto nodes and weights on [0, 1] (long-double Newton on P'_N)."""
+    N = order
+    Np = N + 1
+    if N < 1:
+        raise ValueError("order must be >= 1")
+    xs = np.empty(Np, dtype=np.longdouble)
+    for i in range(Np):
+        xi = -np.cos(np.longdouble(np.pi) * i / N)
+        if 0 < i < N:
+            for _ in range(100):
+                p0, p1, dp0, dp1 = np.longdouble(1), xi, np.longdouble(0), np.longdouble(1)
+                for k in range(1, N):
+                    p2 = ((2 * k + 1) * xi * p1 - k * p0) / (k + 1)
+                    dp2 = dp0 + (2 * k + 1) * p1
+                    p0, p1, dp0, dp1 = p1, p2, dp1, dp2
+                f = (1 - xi * xi) * dp1
+                fp = -np.longdouble(N * (N + 1)) * p1
+                dx = f / fp
+                xi = xi - dx
+                if abs(dx) < 1e-30:
+                    break
+        xs[i] = xi
+    w = np.empty(Np, dtype=np.longdouble)
+    for i in range(Np):
+        p0, p1 = np.longdouble(1), xs[i]
+        for k in range(1, N):
+            p0, p1 = p1, ((2 * k + 1) * xs[i] * p1 - k * p0) / (k + 1)
+        w[i] = 2 / (np.longdouble(N * (N + 1)) * p1 * p1)
+    x = np.array((xs + 1) * 0.5, dtype=np.float64)
+    x[0], x[-1] = 0.0, 1.0
+    return x, np.array(w * 0.5, dtype=np.float64)
+
+
+def _adjugate(J: np.ndarray) -> np.ndarray:
+    """Explicit 2x2 / 3x3 adjugate (as MFEM's CalcAdjugate)."""
+    d = J.shape[0]
+    if d == 2:
+        return np.array([[J[1, 1], -J[0, 1]], [-J[1, 0], J[0, 0]]])
+    a = np.empty((3, 3))
+    a[0, 0] = J[1, 1] * J[2, 2] - J[1, 2] * J[2, 1]
+    a[0, 1] = J[0, 2] * J[2, 1] - J[0, 1] * J[2, 2]
+    a[0, 2] = J[0, 1] * J[1, 2] - J[0, 2] * J[1, 1]
+    a[1, 0] = J[1, 2] * J[2, 0] - J[1, 0] * J[2, 2]
+    a[1, 1] = J[0, 0] * J[2, 2] - J[0, 2] * J[2, 0]
+    a[1, 2] = J[0, 2] * J[1, 0] - J[0, 0] * J[1, 2]
+    a[2, 0] = J[1, 0] * J[2, 1] - J[1, 1] * J[2, 0]
+    a[2, 1] = J[0, 1] * J[2, 0] - J[0, 0] * J[2, 1]
+    a[2, 2] = J[0, 0] * J[1, 1] - J[0, 1] * J[1, 0]
+    return a
+
+
+def _det(J: np.ndarray) -> float:
+    if J.shape[0] == 2:
+        return float(J[0, 0] * J[1, 1] - J[0, 1] * J[1, 0])
+    return float(J[0, 0] * (J[1, 1] * J[2, 2] - J[1, 2] * J[2, 1])
+                 - J[0, 1] * (J[1, 0] * J[2, 2] - J[1, 2] * J[2, 0])
+                 + J[0, 2] * (J[1, 0] * J[2, 1] - J[1, 1] * J[2, 0]))
+
+
+@dataclass
+class Mesh:
+    """Descriptor arrays for ``prandtl_mesh_desc`` plus node coordinates."""
+
+    dim: int
+    order: int
+    n: tuple
+    elem_adj: np.ndarray      # (E, dim, dim) float64
+    elem_detj: np.ndarray     # (E,) float64
+    face_elems: np.ndarray    # (F, 4) int32: elem1, lface1, elem2, lface2
+    face_nor: np.ndarray      # (F, dim) float64
+    coords: np.ndarray        # (dim, E*Np^dim) physical node coordinates
+    hmin: float               # min element size (MFEM GetElementSize(e, 1))
+    nodes_1d: np.ndarray = field(default=None)
+    weights_1d: np.ndarray = field(default=None)
+
+    @property
+    def Np(self) -> int:
+        return self.order + 1
+
+    @property
+    def nodes_per_elem(self) -> int:
+        return self.Np ** self.dim
+
+    @property
+    def num_elements(self) -> int:
+        return int(self.elem_detj.shape[0])
+
+    @property
+    def num_faces(self) -> int:
+        return int(self.face_elems.shape[0])
+
+    @property
+    def ndof(self) -> int:
+        """Nodes per field (MFEM's scalar dof count)."""
+        return self.num_elements * self.nodes_per_elem
+
+    @property
+    def num_fields(self) -> int:
+        return self.dim + 2
+
+    def node_weights(self) -> np.ndarray:
+        """Quadrature weight w_i w_j (w_k) * |J| per node, shape (E*Np^dim,)."""
+        w = self.weights_1d
+        if self.dim == 2:
+            wn = np.outer(w, w).reshape(-1)          # [j][i] -> node j*Np+i
+        else:
+            wn = np.einsum("k,j,i->kji", w, w, w).reshape(-1)
+        return (self.elem_detj[:, None] * wn[None, :]).reshape(-1)
+
+
+def periodic_box(dim: int, n, order: int, lo=0.0, hi=1.0, affine=None) -> Mesh:
+    """Periodic box mesh [lo, hi]^dim with n elements per direction.
+
+    ``n`` may be an int or a per-direction tuple; ``lo``/``hi`` scalars or
+    per-direction tuples.  ``affine`` (dim x dim) maps the box afterwards,
+    x = affine @ X, keeping every element affine.
+    """
+    if dim not in (2, 3):
+        raise ValueError("dim must be 2 or 3")
+    n = tuple([n] * dim) if np.isscalar(n) else tuple(int(v) for v in n)
+    lo = np.broadcast_to(np.asarray(lo, dtype=np.float64), (dim,)).copy()
+    hi = np.broadcast_to(np.asarray(hi, dtype=np.float64), (dim,)).copy()
+    M = np.eye(dim) if affine is None else np.asarray(affine, dtype=np.float64)
+    h = (hi - lo) / np.asarray(n, dtype=np.float64)
+    E = int(np.prod(n))
+    J = M @ np.diag(h)
+    adj = _adjugate(J)
+    detj = _det(J)
+    elem_adj = np.broadcast_to(adj, (E, dim, dim)).copy()
+    elem_detj = np.full(E, detj)
+
+    # element index <-> cell coordinates (x fastest)
+    idx = np.arange(E)
+    cell = np.stack([(idx // int(np.prod(n[:d]))) % n[d] for d in range(dim)])   # (dim, E)
+    strides = [int(np.prod(n[:d])) for d in range(dim)]
+    order_pos = {fs: p for p, fs in enumerate(_MFEM_FACE_ORDER[dim])}
+
+    faces = []
+    normals = []
+    for d in range(dim):
+        up = cell.copy()
+        up[d] = (up[d] + 1) % n[d]
+        e_up = sum(up[k] * strides[k] for k in range(dim))
+        for e in range(E):
+            eu = int(e_up[e])
+            if n[d] >= 2:
+                if e < eu:
+                    faces.append((e, 2 * d + 1, eu, 2 * d + 0))
+                    normals.append(+adj[d])
+                else:
+                    faces.append((eu, 2 * d + 0, e, 2 * d + 1))
+                    normals.append(-adj[d])
+            else:
+                first_side = 0 if order_pos[(d, 0)] < order_pos[(d, 1)] else 1
+                faces.append((e, 2 * d + first_side, e, 2 * d + 1 - first_side))
+                normals.append(adj[d] if first_side == 1 else -adj[d])
+    face_elems = np.asarray(faces, dtype=np.int32).reshape(-1, 4)
+    face_nor = np.asarray(normals, dtype=np.float64).reshape(-1, dim)
+
+    x1, w1 = gauss_lobatto(order)
+    Np = order + 1
+    # reference-cell node coordinates, lexicographic x fastest
+    grids = np.meshgrid(*([x1] * dim), indexing="ij")   # grids[d][i0,i1,(i2)]
+    ref = np.stack([g.transpose().reshape(-1) for g in grids])   # (dim, Np^dim)
+    X = lo[:, None, None] + (cell[:, :, None] + ref[:, None, :]) * h[:, None, None]   # (dim,E,nd)
+    coords = np.einsum("ab,bek->aek", M, X).reshape(dim, -1)
+    # GetElementSize(e, 1): smallest singular value of J
+    hmin = float(np.linalg.svd(J, compute_uv=False).min())
+    return Mesh(dim=dim, order=order, n=n, elem_adj=elem_adj, elem_detj=elem_detj,
+                face_elems=face_elems, face_nor=face_nor, coords=coords, hmin=hmin,
+                nodes_1d=x1, weights_1d=w1)

@@ -1,0 +1,134 @@
+"""Python mirror of the reference operator interface, backed by the C ABI.
+
+``DGSEMOperator`` mirrors ``Prandtl::DGSEMOperator`` (src/Operators/DGSEMOperator.hpp:15-141):
+``Mult(u, dudt)`` evaluates the DGSEM right-hand side, ``GetMaxCharSpeed()``
+returns the largest characteristic speed seen by the last evaluation, and the
+time lives in ``t`` (TimeDependentOperator::SetTime / GetTimeRef).  ``Step``
+plays the role of the mfem::ODESolver the reference drives it with
+(Simulation.cpp:177-206, :1010).
+
+Arrays may be numpy (host memory: staged through the handle's device buffers)
+or torch CUDA tensors (device memory: zero copy).  Every call goes to the
+CUDA kernels; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .mesh import Mesh
+
+_SCHEMES = {"RK3SSP": _lib.RK3SSP, "LSRK45": _lib.LSRK45, 0: _lib.RK3SSP, 1: _lib.LSRK45}
+
+
+def _ptr(a):
+    """(pointer, flag) for a numpy array or a torch tensor."""
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise TypeError("arrays must be C-contiguous float64")
+        return a.ctypes.data, _lib.PTR_HOST
+    if hasattr(a, "data_ptr"):   # torch.Tensor
+        import torch
+        if a.dtype != torch.float64 or not a.is_contiguous():
+            raise TypeError("tensors must be contiguous float64")
+        return a.data_ptr(), (_lib.PTR_DEVICE if a.is_cuda else _lib.PTR_HOST)
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+class DGSEMOperator:
+    def __init__(self, mesh: Mesh, *, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05,
+                 parabolic=False, blending=False, sutherland=False, alpha_max=0.5,
+                 alpha_min=0.001, quirks="reference", surface_dissipation=True,
+                 timeout_s=120.0):
+        L = _lib.load()
+        self.mesh = mesh
+        self._adj = np.ascontiguousarray(mesh.elem_adj, dtype=np.float64)
+        self._detj = np.ascontiguousarray(mesh.elem_detj, dtype=np.float64)
+        self._faces = np.ascontiguousarray(mesh.face_elems, dtype=np.int32)
+        self._nor = np.ascontiguousarray(mesh.face_nor, dtype=np.float64)
+        dp = C.POINTER(C.c_double)
+        desc = _lib.MeshDesc(mesh.dim, mesh.order, mesh.num_elements, mesh.num_faces,
+                             self._adj.ctypes.data_as(dp), self._detj.ctypes.data_as(dp),
+                             self._faces.ctypes.data_as(C.POINTER(C.c_int)),
+                             self._nor.ctypes.data_as(dp))
+        cfg = _lib.Config()
+        L.prandtl_config_default(C.byref(cfg))
+        cfg.gamma, cfg.Pr, cfg.mu, cfg.R_gas = gamma, Pr, mu, R_gas
+        cfg.alpha_max, cfg.alpha_min = alpha_max, alpha_min
+        cfg.parabolic, cfg.blending, cfg.sutherland = int(parabolic), int(blending), int(sutherland)
+        if quirks not in ("reference", "fixed", 0, 1):
+            raise ValueError("quirks must be 'reference' or 'fixed'")
+        cfg.quirks = 1 if quirks in ("fixed", 1) else 0
+        cfg.surface_dissipation = int(bool(surface_dissipation))
+        cfg.timeout_s = timeout_s
+        h = C.c_void_p()
+        _lib.check(L.prandtl_create(C.byref(desc), C.byref(cfg), C.byref(h)), None)
+        self._h = h
+        self._L = L
+        self.t = 0.0
+        self.max_char_speed = -1.0
+        self.height = self.width = mesh.num_fields * mesh.ndof
+
+    # -- mfem::TimeDependentOperator surface
+    def SetTime(self, t: float):
+        self.t = float(t)
+
+    def GetTime(self) -> float:
+        return self.t
+
+    def Mult(self, u, dudt):
+        pu, fu = _ptr(u)
+        pd, fd = _ptr(dudt)
+        if fu != fd:
+            raise ValueError("u and dudt must both be host or both be device arrays")
+        lam = C.c_double(0.0)
+        _lib.check(self._L.prandtl_rhs(self._h, pu, pd, self.t, C.byref(lam), fu), self._h)
+        self.max_char_speed = lam.value
+        return dudt
+
+    def GetMaxCharSpeed(self) -> float:
+        return self.max_char_speed
+
+    # -- mfem::ODESolver::Step equivalent
+    def Step(self, u, dt: float, scheme="RK3SSP", nsteps=1):
+        pu, fu = _ptr(u)
+        _lib.check(self._L.prandtl_step(self._h, pu, self.t, float(dt), _SCHEMES[scheme],
+                                        int(nsteps), fu), self._h)
+        self.t += nsteps * dt
+        return u
+
+    def alpha(self) -> np.ndarray:
+        out = np.empty(self.mesh.num_elements)
+        _lib.check(self._L.prandtl_get_alpha(self._h, out.ctypes.data, _lib.PTR_HOST), self._h)
+        return out
+
+    def cfl_dt(self, cfl: float, lambda_max: float | None = None) -> float:
+        lam = self.max_char_speed if lambda_max is None else lambda_max
+        return self._L.prandtl_cfl_dt(cfl, self.mesh.hmin, lam, self.mesh.order)
+
+    def set_stream(self, stream_ptr: int):
+        _lib.check(self._L.prandtl_set_stream(self._h, C.c_void_p(stream_ptr)), self._h)
+
+    def synchronize(self):
+        _lib.check(self._L.prandtl_synchronize(self._h), self._h)
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self._L.prandtl_kernel_launches(self._h))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self._L.prandtl_device_bytes(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.prandtl_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
