@@ -127,6 +127,17 @@ prandtl_status prandtl_synchronize(prandtl_handle *h);
 /* Number of kernels this handle has launched (instrumentation). */
 long long prandtl_kernel_launches(const prandtl_handle *h);
 
+/* Per-kernel CUDA-event timing (instrumentation, no reference counterpart).
+ * While enabled, every launch is bracketed by events on the handle's stream;
+ * prandtl_profile_read waits for the stream and returns the summed device
+ * time and launch count of one kernel since the last reset. */
+#define PRANDTL_KERNEL_RHS 0   /* fused volume + surface + RK-epilogue kernel */
+#define PRANDTL_KERNEL_LIFT 1  /* BR1 lifting kernel (Navier-Stokes) */
+#define PRANDTL_NUM_KERNELS 2
+prandtl_status prandtl_profile(prandtl_handle *h, int enable);
+prandtl_status prandtl_profile_read(prandtl_handle *h, int kernel, double *total_ms, long long *launches);
+prandtl_status prandtl_profile_reset(prandtl_handle *h);
+
 /* Bytes of device memory owned by the handle. */
 size_t prandtl_device_bytes(const prandtl_handle *h);
 

@@ -115,3 +115,56 @@ def gl(order):
     x, w, D = np.empty(n), np.empty(n), np.empty(n * n)
     lib().oracle_gl(order, _p(x), _p(w), _p(D))
     return x, w, D.reshape(n, n)
+
+
+# ---------------------------------------------------------------------------
+# The reference's own integrator sources, compiled by ref_harness/build_ref.sh
+# into _ref/ (only where the reference checkout is present).
+_REF_LIBS = {}
+_REF_VARIANTS = {(0, 0): "euler", (0, 1): "euler_blend", (1, 0): "ns", (1, 1): "ns_blend"}
+
+
+def ref_available():
+    return all(os.path.exists(os.path.join(_HERE, "_ref", f"libref_{v}.so")) for v in _REF_VARIANTS.values())
+
+
+def build_ref():
+    subprocess.run(["bash", os.path.join(_HERE, "ref_harness", "build_ref.sh")], check=True)
+
+
+def ref_lib(parabolic, blending):
+    key = (int(bool(parabolic)), int(bool(blending)))
+    if key not in _REF_LIBS:
+        L = C.CDLL(os.path.join(_HERE, "_ref", f"libref_{_REF_VARIANTS[key]}.so"))
+        dp = C.POINTER(C.c_double)
+        L.ref_rhs.argtypes = [C.POINTER(OracleMesh), C.POINTER(OracleConfig), dp, dp, dp, dp]
+        L.ref_rhs.restype = C.c_int
+        L.ref_log_mean.argtypes = [C.c_double, C.c_double]
+        L.ref_log_mean.restype = C.c_double
+        _REF_LIBS[key] = L
+    return _REF_LIBS[key]
+
+
+class RefOperator(Oracle):
+    """The reference's DGSEMIntegrator & co. run on the same mesh descriptor.
+
+    Only the reference's own behaviour exists here (no fixed mode); the
+    physics switches select the compile-time variant."""
+
+    def rhs(self, u, want_alpha=False, want_grad=False):
+        L = ref_lib(self.c.parabolic, self.c.blending)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        dudt = np.empty_like(u)
+        alpha = np.empty(self.mesh.num_elements) if want_alpha else None
+        grad = np.empty(self.mesh.dim * u.size) if want_grad else None
+        rc = L.ref_rhs(C.byref(self.m), C.byref(self.c), _p(u), _p(dudt),
+                       _p(alpha) if alpha is not None else None,
+                       _p(grad) if grad is not None else None)
+        if rc != 0:
+            raise RuntimeError("ref_rhs failed")
+        out = {"dudt": dudt}
+        if alpha is not None:
+            out["alpha"] = alpha
+        if grad is not None:
+            out["grad"] = grad
+        return out

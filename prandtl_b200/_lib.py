@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libprandtl_b200.so")
 PRANDTL_OK, PRANDTL_EINVAL, PRANDTL_ENOMEM, PRANDTL_ENONFINITE = 0, 1, 2, 3
 PRANDTL_ETIMEDOUT, PRANDTL_ECUDA, PRANDTL_EUNSUPPORTED = 4, 5, 6
 PTR_HOST, PTR_DEVICE = 0, 1
+KERNEL_RHS, KERNEL_LIFT = 0, 1
 RK3SSP, LSRK45 = 0, 1
 
 STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ENONFINITE", 4: "ETIMEDOUT",
@@ -22,7 +23,8 @@ STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ENONFINITE", 4: "ETIMEDOU
 # Every symbol include/prandtl_b200.h declares.
 EXPORTS = ["prandtl_config_default", "prandtl_create", "prandtl_destroy", "prandtl_rhs",
            "prandtl_step", "prandtl_get_alpha", "prandtl_cfl_dt", "prandtl_set_stream",
-           "prandtl_synchronize", "prandtl_kernel_launches", "prandtl_device_bytes",
+           "prandtl_synchronize", "prandtl_kernel_launches", "prandtl_profile",
+           "prandtl_profile_read", "prandtl_profile_reset", "prandtl_device_bytes",
            "prandtl_last_error", "prandtl_version"]
 
 
@@ -79,6 +81,12 @@ def load():
     L.prandtl_synchronize.restype = ip
     L.prandtl_kernel_launches.argtypes = [vp]
     L.prandtl_kernel_launches.restype = C.c_longlong
+    L.prandtl_profile.argtypes = [vp, ip]
+    L.prandtl_profile.restype = ip
+    L.prandtl_profile_read.argtypes = [vp, ip, dp, C.POINTER(C.c_longlong)]
+    L.prandtl_profile_read.restype = ip
+    L.prandtl_profile_reset.argtypes = [vp]
+    L.prandtl_profile_reset.restype = ip
     L.prandtl_device_bytes.argtypes = [vp]
     L.prandtl_device_bytes.restype = C.c_size_t
     L.prandtl_last_error.argtypes = [vp]

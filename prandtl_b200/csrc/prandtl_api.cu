@@ -40,6 +40,13 @@ struct prandtl_handle {
     unsigned long long *d_lambda = nullptr;
     size_t bytes = 0;
     long long launches = 0;
+    // optional per-kernel CUDA-event timing (prandtl_profile)
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_pool;
+    struct Rec { int kernel; cudaEvent_t a, b; };
+    std::vector<Rec> recs;
+    double prof_ms[PRANDTL_NUM_KERNELS] = {0};
+    long long prof_n[PRANDTL_NUM_KERNELS] = {0};
     std::string err;
     std::mutex mu;
 };
@@ -190,6 +197,19 @@ prandtl_status wait_stream(prandtl_handle *h) {
     }
 }
 
+// Event pair around one launch when profiling; returns the stop event or null.
+cudaEvent_t prof_begin(prandtl_handle *h, int kernel) {
+    if (!h->profiling || h->ev_pool.size() < 2 || h->recs.size() >= 8192) return nullptr;
+    cudaEvent_t a = h->ev_pool.back(); h->ev_pool.pop_back();
+    cudaEvent_t b = h->ev_pool.back(); h->ev_pool.pop_back();
+    cudaEventRecord(a, h->stream);
+    h->recs.push_back({kernel, a, b});
+    return b;
+}
+void prof_end(prandtl_handle *h, cudaEvent_t b) {
+    if (b) cudaEventRecord(b, h->stream);
+}
+
 MeshDev mesh_dev(const prandtl_handle *h) {
     MeshDev m;
     m.geo = h->d_geo;
@@ -207,13 +227,17 @@ prandtl_status run_rhs(prandtl_handle *h, const double *u, RhsArgs a) {
     const bool ns = h->cfg.parabolic != 0;
     if (ns) {
         LiftArgs la{u, h->d_grad};
+        cudaEvent_t pe = prof_begin(h, PRANDTL_KERNEL_LIFT);
         cudaError_t e = launch_lift(h->dim, h->order, m, la, h->P, h->T, h->stream);
+        prof_end(h, pe);
         if (e != cudaSuccess) return cuda_fail(h, e, "lift kernel launch");
         h->launches++;
         a.grad = h->d_grad;
     }
     a.alpha = h->cfg.blending ? h->d_alpha : nullptr;
+    cudaEvent_t pe = prof_begin(h, PRANDTL_KERNEL_RHS);
     cudaError_t e = launch_rhs(h->dim, h->order, ns, m, a, h->P, h->T, h->stream);
+    prof_end(h, pe);
     if (e != cudaSuccess) return cuda_fail(h, e, "rhs kernel launch");
     h->launches++;
     return PRANDTL_OK;
@@ -231,6 +255,10 @@ void free_all(prandtl_handle *h) {
     cudaFree(h->d_alpha);
     cudaFree(h->d_lambda);
     if (h->done) cudaEventDestroy(h->done);
+    for (auto &r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (auto ev : h->ev_pool) cudaEventDestroy(ev);
+    h->recs.clear();
+    h->ev_pool.clear();
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -514,6 +542,51 @@ prandtl_status prandtl_synchronize(prandtl_handle *h) {
 }
 
 long long prandtl_kernel_launches(const prandtl_handle *h) { return h ? h->launches : 0; }
+
+prandtl_status prandtl_profile(prandtl_handle *h, int enable) {
+    if (!h) return PRANDTL_EINVAL;
+    std::lock_guard<std::mutex> lk(h->mu);
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    if (enable && h->ev_pool.empty() && h->recs.empty()) {
+        for (int i = 0; i < 2 * 8192; ++i) {
+            cudaEvent_t ev;
+            CK(h, cudaEventCreate(&ev), "cudaEventCreate");
+            h->ev_pool.push_back(ev);
+        }
+    }
+    h->profiling = enable != 0;
+    return PRANDTL_OK;
+}
+
+prandtl_status prandtl_profile_read(prandtl_handle *h, int kernel, double *total_ms, long long *launches) {
+    if (!h || kernel < 0 || kernel >= PRANDTL_NUM_KERNELS) return PRANDTL_EINVAL;
+    std::lock_guard<std::mutex> lk(h->mu);
+    prandtl_status st = wait_stream(h);
+    if (st != PRANDTL_OK) return st;
+    for (auto &r : h->recs) {
+        float ms = 0.f;
+        CK(h, cudaEventElapsedTime(&ms, r.a, r.b), "cudaEventElapsedTime");
+        h->prof_ms[r.kernel] += ms;
+        h->prof_n[r.kernel] += 1;
+        h->ev_pool.push_back(r.a);
+        h->ev_pool.push_back(r.b);
+    }
+    h->recs.clear();
+    if (total_ms) *total_ms = h->prof_ms[kernel];
+    if (launches) *launches = h->prof_n[kernel];
+    return PRANDTL_OK;
+}
+
+prandtl_status prandtl_profile_reset(prandtl_handle *h) {
+    if (!h) return PRANDTL_EINVAL;
+    double ms;
+    long long n;
+    prandtl_status st = prandtl_profile_read(h, 0, &ms, &n);
+    if (st != PRANDTL_OK) return st;
+    std::lock_guard<std::mutex> lk(h->mu);
+    for (int k = 0; k < PRANDTL_NUM_KERNELS; ++k) { h->prof_ms[k] = 0.0; h->prof_n[k] = 0; }
+    return PRANDTL_OK;
+}
 
 size_t prandtl_device_bytes(const prandtl_handle *h) { return h ? h->bytes : 0; }
 

@@ -114,6 +114,22 @@ class DGSEMOperator:
     def synchronize(self):
         _lib.check(self._L.prandtl_synchronize(self._h), self._h)
 
+    def profile(self, enable: bool = True):
+        """Bracket every kernel launch with CUDA events (instrumentation)."""
+        _lib.check(self._L.prandtl_profile(self._h, int(enable)), self._h)
+
+    def profile_reset(self):
+        _lib.check(self._L.prandtl_profile_reset(self._h), self._h)
+
+    def profile_read(self):
+        """{kernel name: (total device ms, launches)} since the last reset."""
+        out = {}
+        for name, k in (("rhs", _lib.KERNEL_RHS), ("lift", _lib.KERNEL_LIFT)):
+            ms, n = C.c_double(0.0), C.c_longlong(0)
+            _lib.check(self._L.prandtl_profile_read(self._h, k, C.byref(ms), C.byref(n)), self._h)
+            out[name] = (ms.value, n.value)
+        return out
+
     @property
     def kernel_launches(self) -> int:
         return int(self._L.prandtl_kernel_launches(self._h))

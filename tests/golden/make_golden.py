@@ -1,0 +1,62 @@
+"""Generate golden RHS vectors from the reference's own DGSEM sources.
+
+Runs oracle/_ref/libref_*.so (the reference's DGSEMIntegrator, LiftingBR1,
+ChandrashekarFlux, NavierStokesFlux, BasicOperations, PerssonPeraireIndicator
+and ModalBasis compiled unmodified by oracle/ref_harness/build_ref.sh) on small
+seeded cases and stores inputs and outputs in reference_rhs.npz.
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from prandtl_b200 import cases  # noqa: E402
+from prandtl_b200.mesh import periodic_box  # noqa: E402
+
+# (name, dim, n, order, parabolic, blending, amplitude, seed)
+CASES = [
+    ("euler2d_n3_N3", 2, 3, 3, 0, 0, 0.10, 1),
+    ("euler2d_blend_n3_N3", 2, 3, 3, 0, 1, 0.30, 2),
+    ("ns2d_n3_N2", 2, 3, 2, 1, 0, 0.10, 3),
+    ("ns2d_blend_n2_N4", 2, 2, 4, 1, 1, 0.30, 4),
+    ("euler3d_n2_N2", 3, 2, 2, 0, 0, 0.10, 5),
+    ("euler3d_blend_n2_N3", 3, 2, 3, 0, 1, 0.30, 6),
+    ("ns3d_n2_N3", 3, 2, 3, 1, 0, 0.10, 7),
+    ("ns3d_blend_n2_N2", 3, 2, 2, 1, 1, 0.30, 8),
+]
+PHYS = dict(gamma=1.4, Pr=0.71, mu=0.01, R_gas=287.05, alpha_max=0.5, alpha_min=0.001)
+
+
+def case_inputs(dim, n, order, amp, seed):
+    rng = np.random.default_rng(100 + seed)
+    A = np.eye(dim) + 0.15 * rng.uniform(-1, 1, (dim, dim))
+    mesh = periodic_box(dim, n, order, 0.0, 1.0, affine=A)
+    base = cases.free_stream(mesh, rho=1.2, vel=[0.4, -0.3, 0.2][:dim], p=1.5)
+    return mesh, A, cases.perturbed(mesh, base, amp=amp, seed=seed)
+
+
+def main():
+    import pyoracle
+    if not pyoracle.ref_available():
+        pyoracle.build_ref()
+    out = {}
+    for name, dim, n, order, par, bl, amp, seed in CASES:
+        mesh, A, u = case_inputs(dim, n, order, amp, seed)
+        r = pyoracle.RefOperator(mesh, parabolic=par, blending=bl, **PHYS).rhs(u, want_alpha=True)
+        out[f"{name}/affine"] = A
+        out[f"{name}/u"] = u
+        out[f"{name}/dudt"] = r["dudt"]
+        out[f"{name}/alpha"] = r["alpha"]
+    np.savez_compressed(os.path.join(HERE, "reference_rhs.npz"), **out)
+    print(f"wrote {len(CASES)} cases")
+
+
+if __name__ == "__main__":
+    main()

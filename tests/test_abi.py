@@ -1,0 +1,103 @@
+"""C-ABI library: loads, exports every declared symbol, validates input without a GPU."""
+import ctypes as C
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from prandtl_b200 import _lib, build
+    if build.needs_build():
+        build.build()
+    return _lib.load()
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"\b(prandtl_\w+)\s*\(", src):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_every_declared_symbol_is_exported(lib):
+    from prandtl_b200 import _lib
+    names = declared_functions()
+    assert len(names) >= 10
+    for n in names:
+        assert hasattr(lib, n), f"{n} declared in include/ but not exported"
+    assert set(names) == set(_lib.EXPORTS)
+
+
+def test_config_defaults(lib):
+    from prandtl_b200 import _lib
+    c = _lib.Config()
+    lib.prandtl_config_default(C.byref(c))
+    assert (c.gamma, c.Pr, c.mu, c.R_gas) == (1.4, 0.72, 0.02, 287.05)
+    assert (c.alpha_max, c.alpha_min) == (0.5, 0.001)
+    assert c.surface_dissipation == 1 and c.quirks == 0 and c.precision == 0
+
+
+def test_cfl_dt(lib):
+    assert lib.prandtl_cfl_dt(0.5, 0.3125, 2.0, 3) == pytest.approx(0.5 * 0.3125 / (2.0 * 16))
+
+
+def _desc(mesh, keep):
+    from prandtl_b200 import _lib
+    dp = C.POINTER(C.c_double)
+    keep += [np.ascontiguousarray(mesh.elem_adj), np.ascontiguousarray(mesh.elem_detj),
+             np.ascontiguousarray(mesh.face_elems, dtype=np.int32), np.ascontiguousarray(mesh.face_nor)]
+    return _lib.MeshDesc(mesh.dim, mesh.order, mesh.num_elements, mesh.num_faces,
+                         keep[-4].ctypes.data_as(dp), keep[-3].ctypes.data_as(dp),
+                         keep[-2].ctypes.data_as(C.POINTER(C.c_int)), keep[-1].ctypes.data_as(dp))
+
+
+def test_create_validates_before_touching_the_device(lib):
+    from prandtl_b200 import _lib
+    from prandtl_b200.mesh import periodic_box
+    keep = []
+    cfg = _lib.Config()
+    lib.prandtl_config_default(C.byref(cfg))
+    h = C.c_void_p()
+    assert lib.prandtl_create(None, C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EINVAL
+    m = periodic_box(2, 2, 3)
+    d = _desc(m, keep)
+    d.order = 7
+    assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EUNSUPPORTED
+    assert b"order" in lib.prandtl_last_error(None)
+    d = _desc(m, keep)
+    d.num_faces -= 1   # an element face without a neighbour
+    assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EUNSUPPORTED
+    cfg.precision = 1
+    d = _desc(m, keep)
+    assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EUNSUPPORTED
+
+
+def test_create_without_gpu_reports_ecuda(lib):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from prandtl_b200 import _lib
+    from prandtl_b200.operator import DGSEMOperator
+    from prandtl_b200.mesh import periodic_box
+    with pytest.raises(_lib.PrandtlError) as ei:
+        DGSEMOperator(periodic_box(2, 2, 3))
+    assert ei.value.status == _lib.PRANDTL_ECUDA
+
+
+def test_null_handle_calls_fail_cleanly(lib):
+    from prandtl_b200 import _lib
+    assert lib.prandtl_destroy(None) == _lib.PRANDTL_EINVAL
+    assert lib.prandtl_rhs(None, None, None, 0.0, None, 0) == _lib.PRANDTL_EINVAL
+    assert lib.prandtl_step(None, None, 0.0, 0.1, 0, 1, 0) == _lib.PRANDTL_EINVAL
+    assert lib.prandtl_synchronize(None) == _lib.PRANDTL_EINVAL
+    assert lib.prandtl_kernel_launches(None) == 0
+    assert lib.prandtl_version().startswith(b"prandtl_b200")

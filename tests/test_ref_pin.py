@@ -1,0 +1,89 @@
+"""Pin of the CPU oracle against the reference's own DGSEM sources.
+
+oracle/_ref holds the reference's DGSEMIntegrator.cpp, LiftingBR1.cpp,
+ChandrashekarFlux.cpp, NavierStokesFlux.cpp, BasicOperations.cpp,
+PerssonPeraireIndicator.cpp and ModalBasis.cpp compiled unmodified against an
+MFEM stand-in (oracle/ref_harness).  tests/golden/reference_rhs.npz holds their
+outputs on seeded cases (tests/golden/make_golden.py).  Tolerance: normalised
+per-DOF error 1e-13 (different summation order only).
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import normalized_error
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+import make_golden  # noqa: E402
+
+PIN_TOL = 1e-13
+GOLDEN = np.load(os.path.join(HERE, "golden", "reference_rhs.npz"))
+
+
+@pytest.mark.parametrize("case", make_golden.CASES, ids=[c[0] for c in make_golden.CASES])
+def test_oracle_matches_reference_golden(oracle_mod, case):
+    name, dim, n, order, par, bl, amp, seed = case
+    mesh, A, u = make_golden.case_inputs(dim, n, order, amp, seed)
+    np.testing.assert_array_equal(A, GOLDEN[f"{name}/affine"])
+    np.testing.assert_array_equal(u, GOLDEN[f"{name}/u"])
+    r = oracle_mod.Oracle(mesh, parabolic=par, blending=bl, quirks=0, **make_golden.PHYS).rhs(u, want_alpha=True)
+    assert normalized_error(r["dudt"], GOLDEN[f"{name}/dudt"], mesh.num_fields) <= PIN_TOL
+    np.testing.assert_allclose(r["alpha"], GOLDEN[f"{name}/alpha"], rtol=0, atol=1e-14)
+    if bl:
+        assert (r["alpha"] > 0).any(), "blending case must exercise the subcell FV path"
+
+
+def _ref(oracle_mod):
+    if not oracle_mod.ref_available():
+        if not os.path.isdir("/root/reference/src"):
+            pytest.skip("reference sources not present on this host")
+        oracle_mod.build_ref()
+    return oracle_mod
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("par", [0, 1])
+@pytest.mark.parametrize("bl", [0, 1])
+@pytest.mark.parametrize("order", [1, 2, 3, 4, 5])
+def test_oracle_matches_reference_sources(oracle_mod, dim, par, bl, order):
+    o = _ref(oracle_mod)
+    from prandtl_b200 import cases
+    from prandtl_b200.mesh import periodic_box
+    rng = np.random.default_rng(order + 7 * dim)
+    A = np.eye(dim) + 0.15 * rng.uniform(-1, 1, (dim, dim))
+    n = 2 if (dim == 3 and order > 3) else 3
+    mesh = periodic_box(dim, n, order, 0.0, 1.0, affine=A)
+    base = cases.free_stream(mesh, rho=1.1, vel=[0.2, 0.5, -0.3][:dim], p=1.3)
+    u = cases.perturbed(mesh, base, amp=0.3 if bl else 0.1, seed=order)
+    kw = dict(parabolic=par, blending=bl, mu=0.01, Pr=0.71)
+    a = o.Oracle(mesh, quirks=0, **kw).rhs(u, want_alpha=True, want_grad=bool(par))
+    b = o.RefOperator(mesh, **kw).rhs(u, want_alpha=True, want_grad=bool(par))
+    assert normalized_error(a["dudt"], b["dudt"], mesh.num_fields) <= PIN_TOL
+    np.testing.assert_allclose(a["alpha"], b["alpha"], rtol=0, atol=1e-14)
+    if par:   # lifted primitive gradients (the reference's dudx/dudy/dudz)
+        assert normalized_error(a["grad"], b["grad"], dim * mesh.num_fields) <= PIN_TOL
+
+
+def test_periodic_self_neighbour_mesh(oracle_mod):
+    """n = 1: every face joins an element to itself (MFEM Elem1/Elem2 rule)."""
+    o = _ref(oracle_mod)
+    from prandtl_b200 import cases
+    from prandtl_b200.mesh import periodic_box
+    for dim in (2, 3):
+        mesh = periodic_box(dim, 1, 3, 0.0, 1.0)
+        u = cases.perturbed(mesh, cases.free_stream(mesh), amp=0.1, seed=2)
+        for par in (0, 1):
+            a = o.Oracle(mesh, quirks=0, parabolic=par, mu=0.01).rhs(u)["dudt"]
+            b = o.RefOperator(mesh, parabolic=par, mu=0.01).rhs(u)["dudt"]
+            assert normalized_error(a, b, mesh.num_fields) <= PIN_TOL
+
+
+def test_golden_fixtures_come_from_the_reference(oracle_mod):
+    o = _ref(oracle_mod)
+    for name, dim, n, order, par, bl, amp, seed in make_golden.CASES:
+        mesh, A, u = make_golden.case_inputs(dim, n, order, amp, seed)
+        r = o.RefOperator(mesh, parabolic=par, blending=bl, **make_golden.PHYS).rhs(u)
+        np.testing.assert_array_equal(r["dudt"], GOLDEN[f"{name}/dudt"])
