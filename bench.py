@@ -164,50 +164,79 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- CPU side
-def cpu_rate(n_cpu, order, steps=None, seconds=12.0, threads=None):
-    """DOF-updates/s of the CPU implementation on a TGV sample mesh."""
+def _cpu_worker(job):
+    """One CPU replica: LSRK4(5) steps of the TGV sample mesh.  kind 'reference'
+    runs the reference's own integrator sources (oracle/_ref), kind 'port' the
+    oracle restatement.  Returns (DOF updates, seconds)."""
+    kind, n_cpu, order, steps, seconds, threads = job
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
     import pyoracle
     from prandtl_b200 import cases
     from prandtl_b200.mesh import periodic_box
-    import numpy as np
     mesh = periodic_box(3, n_cpu, order, 0.0, 2 * np.pi)
     u = cases.taylor_green(mesh)
-    threads = threads or os.cpu_count() or 1
-    orc = pyoracle.Oracle(mesh, nthreads=threads, **{k: v for k, v in physics().items()
-                                                     if k in ("mu", "Pr", "gamma")},
-                          parabolic=1, blending=0)
-    lam = orc.rhs(u)["lambda_max"]
+    kw = dict(parabolic=1, blending=0, mu=1.0 / 1600.0, Pr=0.71, gamma=1.4)
+    cls = pyoracle.RefOperator if kind == "reference" else pyoracle.Oracle
+    op = cls(mesh, nthreads=threads, **kw)
+    lam = pyoracle.Oracle(mesh, nthreads=1, **kw).rhs(u)["lambda_max"]
     dt = 0.1 * mesh.hmin / (lam * (order + 1) ** 2)
-    u = orc.step(u, dt, scheme=1, nsteps=1)   # warm-up
+    u = op.step(u, dt, scheme=1, nsteps=1)   # warm-up
     done, t0 = 0, time.perf_counter()
     while True:
-        u = orc.step(u, dt, scheme=1, nsteps=1)
+        u = op.step(u, dt, scheme=1, nsteps=1)
         done += 1
         el = time.perf_counter() - t0
         if (steps is not None and done >= steps) or (steps is None and el >= seconds):
             break
-    dof = mesh.ndof * mesh.num_fields
-    return dof * done / el, dict(kind="port", cores=threads, steps=done, seconds=el,
-                                 sample=f"TGV {n_cpu}^3 elements N={order} ({dof} DOF), {done} LSRK4(5) "
-                                        f"steps, oracle C++ restatement -O2, {threads} threads")
+    return mesh.ndof * mesh.num_fields * done, el, done
+
+
+def cpu_rate(order, steps=None, seconds=12.0):
+    """DOF-updates/s of the CPU path on the host cores.
+
+    With the reference's own sources built (oracle/_ref) this is the
+    reference: one process per core, each advancing its own 4^3-element TGV
+    sample (the reference scales over cores by MPI domain decomposition,
+    run.sh `mpiexec -n`).  Otherwise the oracle port runs 8^3 elements with one
+    OpenMP thread per core."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import multiprocessing as mp
+    import pyoracle
+    cores = os.cpu_count() or 1
+    if pyoracle.ref_available():
+        n_cpu, kind = 4, "reference"
+        jobs = [(kind, n_cpu, order, steps, seconds, 1)] * cores
+        with mp.get_context("spawn").Pool(cores) as pool:
+            res = pool.map(_cpu_worker, jobs)
+        upd = sum(r[0] for r in res)
+        el = max(r[1] for r in res)
+        nstep = res[0][2]
+        sample = (f"reference DGSEM sources (oracle/_ref, -O2) x {cores} processes, each TGV "
+                  f"{n_cpu}^3 elements N={order}, {nstep} LSRK4(5) steps")
+    else:
+        n_cpu, kind = 8, "port"
+        with mp.get_context("spawn").Pool(1) as pool:
+            upd, el, nstep = pool.map(_cpu_worker, [(kind, n_cpu, order, steps, seconds, cores)])[0]
+        sample = (f"oracle C++ restatement -O2, {cores} OpenMP threads, TGV {n_cpu}^3 elements "
+                  f"N={order}, {nstep} LSRK4(5) steps")
+    return upd / el, dict(kind=kind, cores=cores, steps=nstep, seconds=el, sample=sample)
 
 
 def run_reference(args, rank):
     if rank != 0:
         return
-    n_cpu = max(2, min(args.n, 8))
-    # W warm-up steps, then K timed steps on the sample mesh
-    cpu_rate(n_cpu, args.order, steps=max(1, args.warmup))
-    rate, info = cpu_rate(n_cpu, args.order, steps=max(1, args.steps))
+    # W warm-up steps, then K timed steps of the sample workload
+    cpu_rate(args.order, steps=max(1, args.warmup))
+    rate, info = cpu_rate(args.order, steps=max(1, args.steps))
     line = {
         "metric": "DOF-updates/s/GPU", "value": rate, "unit": "DOF-updates/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * info["seconds"] / max(1, info["steps"]),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (standard TGV initial condition)",
-        "config": {"workload": workload_name(args.n, args.order), "sample_mesh": f"{n_cpu}^3",
-                   "order": args.order, "scheme": "LSRK45", "quirks": args.quirks},
+        "config": {"workload": workload_name(args.n, args.order), "order": args.order,
+                   "scheme": "LSRK45", "quirks": "reference (the reference's own code)"},
         "cpu_baseline": {"value": rate, "unit": "DOF-updates/s", "cores": info["cores"],
                          "kind": info["kind"], "sample": info["sample"]},
         "e2e": {"value": rate, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -354,7 +383,7 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
-            rate, info = cpu_rate(max(2, min(args.n, 8)), args.order, seconds=args.cpu_seconds)
+            rate, info = cpu_rate(args.order, seconds=args.cpu_seconds)
             cpu = {"value": rate, "unit": "DOF-updates/s", "cores": info["cores"],
                    "kind": info["kind"], "sample": info["sample"]}
         except Exception as exc:   # the oracle build is missing on this host

@@ -168,3 +168,33 @@ class RefOperator(Oracle):
         if grad is not None:
             out["grad"] = grad
         return out
+
+
+_LSRK_A = (0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+           -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0)
+_LSRK_B = (1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+           1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+           2277821191437.0 / 14882151754819.0)
+
+
+def _ref_step(self, u, dt, scheme=1, nsteps=1, t=0.0):
+    """RK steps around the reference RHS: SSP-RK3 in mfem::RK3SSPSolver order
+    or Carpenter-Kennedy LSRK4(5) (the reference has no low-storage scheme)."""
+    u = np.array(u, dtype=np.float64, copy=True)
+    for _ in range(nsteps):
+        if scheme == 0:
+            k = self.rhs(u)["dudt"]
+            y = u + dt * k
+            y += dt * self.rhs(y)["dudt"]
+            y = 3. / 4 * u + 1. / 4 * y
+            y += dt * self.rhs(y)["dudt"]
+            u = 1. / 3 * u + 2. / 3 * y
+        else:
+            du = np.zeros_like(u)
+            for a, b in zip(_LSRK_A, _LSRK_B):
+                du = a * du + dt * self.rhs(u)["dudt"]
+                u = u + b * du
+    return u
+
+
+RefOperator.step = _ref_step
