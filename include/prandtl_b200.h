@@ -37,7 +37,8 @@ typedef enum prandtl_status {
     PRANDTL_ENONFINITE = 3,    /* non-finite state detected (NaN check) */
     PRANDTL_ETIMEDOUT = 4,     /* a bounded wait ran out */
     PRANDTL_ECUDA = 5,         /* CUDA runtime error (text in prandtl_last_error) */
-    PRANDTL_EUNSUPPORTED = 6   /* valid input outside what this build implements */
+    PRANDTL_EUNSUPPORTED = 6,  /* valid input outside what this build implements */
+    PRANDTL_ETOOLARGE = 7      /* input larger than a fixed-size limit (prandtl_rhs_noalloc) */
 } prandtl_status;
 
 /* Pointer-location flags for the u / dudt arguments. */
@@ -146,6 +147,31 @@ size_t prandtl_device_bytes(const prandtl_handle *h);
 const char *prandtl_last_error(const prandtl_handle *h);
 
 const char *prandtl_version(void);
+
+/* ---- RHS without any memory allocation (no counterpart in the reference) ----
+ * For callers that cannot call cudaMalloc: code that runs inside another
+ * framework's memory pool, embeddings with a fixed device footprint, or code
+ * that must not change its footprint after start-up.  Computes the same
+ * dudt = L(u) as prandtl_rhs without a handle and without allocating: mesh
+ * arrays (the prandtl_mesh_desc pointers), u and dudt must already be in
+ * device memory of the current device; everything else lives in one
+ * file-scope device array of PRANDTL_NOALLOC_SCRATCH_BYTES that every GPU
+ * which loads this library holds until the process exits.
+ * Limit: dim*(dim+2)*Ndof doubles of gradients (Navier-Stokes only) plus
+ * E*(dim*dim+1) doubles and E*2*dim int4 of tables must fit, each rounded up
+ * to 256 bytes (3D N=3: about 4,200 elements); larger meshes return
+ * PRANDTL_ETOOLARGE before any device work.
+ * The first call on a device looks up the array's device address while that
+ * device is current; make that first call before any stream capture.  The
+ * call validates the mesh on the device, waits (bounded by cfg->timeout_s) for
+ * that check, then enqueues the kernels on `cuda_stream` (a cudaStream_t, NULL
+ * for the default stream) and returns without waiting for them.  All calls
+ * share the scratch array, which keeps the last call's contents; calls that
+ * overlap on the GPU (other streams or host threads on the same device) race.
+ * No lambda_max or blending-coefficient output. */
+#define PRANDTL_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+prandtl_status prandtl_rhs_noalloc(const prandtl_mesh_desc *mesh_dev, const prandtl_config *cfg,
+                                   const double *u_dev, double *dudt_dev, void *cuda_stream);
 
 #ifdef __cplusplus
 }

@@ -12,20 +12,20 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libprandtl_b200.so")
 
 PRANDTL_OK, PRANDTL_EINVAL, PRANDTL_ENOMEM, PRANDTL_ENONFINITE = 0, 1, 2, 3
-PRANDTL_ETIMEDOUT, PRANDTL_ECUDA, PRANDTL_EUNSUPPORTED = 4, 5, 6
+PRANDTL_ETIMEDOUT, PRANDTL_ECUDA, PRANDTL_EUNSUPPORTED, PRANDTL_ETOOLARGE = 4, 5, 6, 7
 PTR_HOST, PTR_DEVICE = 0, 1
 KERNEL_RHS, KERNEL_LIFT = 0, 1
 RK3SSP, LSRK45 = 0, 1
 
 STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ENONFINITE", 4: "ETIMEDOUT",
-                5: "ECUDA", 6: "EUNSUPPORTED"}
+                5: "ECUDA", 6: "EUNSUPPORTED", 7: "ETOOLARGE"}
 
 # Every symbol include/prandtl_b200.h declares.
 EXPORTS = ["prandtl_config_default", "prandtl_create", "prandtl_destroy", "prandtl_rhs",
            "prandtl_step", "prandtl_get_alpha", "prandtl_cfl_dt", "prandtl_set_stream",
            "prandtl_synchronize", "prandtl_kernel_launches", "prandtl_profile",
            "prandtl_profile_read", "prandtl_profile_reset", "prandtl_device_bytes",
-           "prandtl_last_error", "prandtl_version"]
+           "prandtl_last_error", "prandtl_version", "prandtl_rhs_noalloc"]
 
 
 class MeshDesc(C.Structure):
@@ -91,6 +91,8 @@ def load():
     L.prandtl_device_bytes.restype = C.c_size_t
     L.prandtl_last_error.argtypes = [vp]
     L.prandtl_last_error.restype = C.c_char_p
+    L.prandtl_rhs_noalloc.argtypes = [C.POINTER(MeshDesc), C.POINTER(Config), vp, vp, vp]
+    L.prandtl_rhs_noalloc.restype = ip
     L.prandtl_version.argtypes = []
     L.prandtl_version.restype = C.c_char_p
     _LIB = L

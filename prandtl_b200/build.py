@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libprandtl_b200.so")
-SOURCES = ["dgsem_kernels.cu", "prandtl_api.cu"]
+SOURCES = ["dgsem_kernels.cu", "prandtl_api.cu", "prandtl_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
