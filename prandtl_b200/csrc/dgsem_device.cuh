@@ -1,8 +1,13 @@
 // dgsem_device.cuh -- point-wise DGSEM physics on the device (sm_100a).
 //
-// Each function states the reference routine whose arithmetic it implements.
-// Arithmetic is templated on the working type `Real` (double for the FP64
-// path, float for the FP32-bulk form).
+// The two-point fluxes work on per-node primitives computed once per node
+// (hoisted out of the O(Np) partner loops): 1/rho, velocity, p, beta = rho/(2p),
+// 1/beta, |V|^2 and |V|+c.  Every division of the reference formulas becomes a
+// multiplication by one of those reciprocals, and the logarithmic mean needs a
+// single reciprocal on its series branch (it also returns 1/mean, which the
+// enthalpy term needs).  Each function cites the reference routine whose
+// arithmetic it restates; results agree with the reference formulas to a few
+// ulp per evaluation.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -33,163 +38,175 @@ struct OpTables {
 
 template <typename T> __device__ __forceinline__ T dmax(T a, T b) { return a > b ? a : b; }
 
-// BasicOperations.cpp:6-12: logarithmic mean with the series branch for
-// u = ((xi-1)/(xi+1))^2 < 1e-4.
+__device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+
+// Per-node primitives of a conserved state s = (rho, rho v, E).
+template <int DIM, typename Real>
+struct Prim {
+    Real rho, rrho, v[DIM], vsq, beta, rbeta, lam;
+};
+
+// ChandrashekarFlux.cpp:22-68 per node: v = m/rho, p = (g-1)(E - rho|v|^2/2),
+// beta = rho/(2p), lambda = |v| + sqrt(g p / rho) (BasicOperations.cpp:53-56).
+template <int DIM, typename Real>
+__device__ __forceinline__ Prim<DIM, Real> primitives(const Real *s, Real gamma, Real gammaM1) {
+    constexpr int NF = DIM + 2;
+    Prim<DIM, Real> q;
+    q.rho = s[0];
+    q.rrho = rcp(s[0]);
+    q.vsq = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        q.v[d] = s[1 + d] * q.rrho;
+        q.vsq += q.v[d] * q.v[d];
+    }
+    const Real p = gammaM1 * (s[NF - 1] - Real(0.5) * q.rho * q.vsq);
+    q.beta = Real(0.5) * q.rho * rcp(p);
+    q.rbeta = Real(2) * p * q.rrho;
+    q.lam = sqrt(q.vsq) + sqrt(gamma * p * q.rrho);
+    return q;
+}
+
+// BasicOperations.cpp:6-12.  Logarithmic mean of x, y > 0 and its inverse.
+// With f = (y-x)/(y+x) and u = f^2 the mean is ((x+y)/2) / P(u),
+// P(u) = 1 + u/3 + u^2/5 + u^3/7, on the reference's series branch u < 1e-4
+// (the reference writes it as (x+y)*52.5/(105+u(35+u(21+15u)))); there 1/P is
+// expanded to third order in a = P-1 (a < 3.5e-5, truncation < 2e-18).
+// Otherwise (y-x)/log(y/x), with y/x formed from the hoisted 1/x.
+// rs returns 1/(x+y).
 template <typename Real>
-__device__ __forceinline__ Real log_mean(Real x, Real y) {
-    const Real xi = y / x;
-    const Real u = (xi * (xi - Real(2)) + Real(1)) / (xi * (xi + Real(2)) + Real(1));
-    if (u < Real(1e-4))
-        return (x + y) * Real(52.5) / (Real(105) + u * (Real(35) + u * (Real(21) + Real(15) * u)));
-    return (y - x) / log(xi);
+__device__ __forceinline__ void log_mean(Real x, Real y, Real rx, Real &mean, Real &inv_mean, Real &rs) {
+    const Real s = x + y, d = y - x;
+    rs = rcp(s);
+    const Real f = d * rs;
+    const Real u = f * f;
+    if (u < Real(1e-4)) {
+        const Real a = u * (Real(1.0 / 3.0) + u * (Real(1.0 / 5.0) + u * Real(1.0 / 7.0)));
+        inv_mean = Real(2) * rs * (Real(1) + a);
+        mean = Real(0.5) * s * (Real(1) - a * (Real(1) - a * (Real(1) - a)));
+    } else {
+        const Real L = log(y * rx);
+        mean = d * rcp(L);
+        inv_mean = L * rcp(d);
+    }
 }
 
 // ChandrashekarFlux.cpp:11-83 with metric1 == metric2 == m (affine element,
-// so ComputeMean returns m exactly).  F has DIM+2 entries.
+// so ComputeMean returns m exactly).
 template <int DIM, typename Real>
-__device__ __forceinline__ void volume_flux(const Real *s1, const Real *s2, const Real *m,
-                                            Real gammaM1, Real gammaM1Inverse, Real *F) {
+__device__ __forceinline__ void volume_flux(const Prim<DIM, Real> &a, const Prim<DIM, Real> &b,
+                                            const Real *m, Real gammaM1Inverse, Real *F) {
     constexpr int NF = DIM + 2;
-    const Real rho1 = s1[0], rho2 = s2[0];
-    const Real rho_ln = log_mean(rho1, rho2);
-    Real vel1[DIM], vel2[DIM], vm[DIM];
-    Real V_sq1 = 0, V_sq2 = 0, Vn = 0, h_hat = 0;
+    Real rho_ln, irho_ln, rs_rho, beta_ln, ibeta_ln, rs_beta;
+    log_mean(a.rho, b.rho, a.rrho, rho_ln, irho_ln, rs_rho);
+    log_mean(a.beta, b.beta, a.rbeta, beta_ln, ibeta_ln, rs_beta);
+    Real vm[DIM], Vn = 0, h = Real(-0.25) * (a.vsq + b.vsq);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
-        vel1[d] = s1[1 + d] / rho1;
-        vel2[d] = s2[1 + d] / rho2;
-        vm[d] = Real(0.5) * (vel1[d] + vel2[d]);
-        V_sq1 += vel1[d] * vel1[d];
-        V_sq2 += vel2[d] * vel2[d];
+        vm[d] = Real(0.5) * (a.v[d] + b.v[d]);
         Vn += vm[d] * m[d];
-        h_hat += Real(-0.25) * (vel1[d] * vel1[d] + vel2[d] * vel2[d]) + vm[d] * vm[d];
+        h += vm[d] * vm[d];
     }
-    const Real p1 = gammaM1 * (s1[NF - 1] - Real(0.5) * rho1 * V_sq1);
-    const Real p2 = gammaM1 * (s2[NF - 1] - Real(0.5) * rho2 * V_sq2);
-    const Real beta1 = Real(0.5) * rho1 / p1, beta2 = Real(0.5) * rho2 / p2;
-    const Real beta_ln = log_mean(beta1, beta2);
-    const Real p_hat = Real(0.5) * (rho1 + rho2) / (beta1 + beta2);
-    h_hat += Real(0.5) / beta_ln * gammaM1Inverse + p_hat / rho_ln;
-    F[0] = rho_ln * Vn;
+    const Real p_hat = Real(0.5) * (a.rho + b.rho) * rs_beta;   // 0.5(rho1+rho2)/(beta1+beta2)
+    h += Real(0.5) * gammaM1Inverse * ibeta_ln + p_hat * irho_ln;
+    const Real F0 = rho_ln * Vn;
+    F[0] = F0;
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) F[1 + d] = Vn * (rho_ln * vm[d]) + p_hat * m[d];
-    F[NF - 1] = rho_ln * Vn * h_hat;
+    for (int d = 0; d < DIM; ++d) F[1 + d] = F0 * vm[d] + p_hat * m[d];
+    F[NF - 1] = F0 * h;
 }
 
-// ChandrashekarFlux.cpp:85-161: entropy-conservative flux minus the scalar
-// dissipation 0.5*lambda*jump*|n|.  quirk3 reproduces `rho_mean * dw + w_mean`
-// (:131) in 3D.
+// ChandrashekarFlux.cpp:85-161: entropy-conservative flux minus
+// 0.5*lambda*jump*|n| (conserved jumps for mass and momentum, the entropy
+// variable based `diss` for energy).  s1, s2 are the conserved inputs (for the
+// momentum jumps); quirk3 reproduces `rho_mean * dw + w_mean` (:131) in 3D.
 template <int DIM, typename Real>
-__device__ __forceinline__ void face_flux(const Real *s1, const Real *s2, const Real *nor,
-                                          Real gamma, Real gammaM1, Real gammaM1Inverse,
+__device__ __forceinline__ void face_flux(const Real *s1, const Prim<DIM, Real> &a, const Real *s2,
+                                          const Prim<DIM, Real> &b, const Real *nor, Real gammaM1Inverse,
                                           bool quirk3, bool dissipation, Real *flux) {
     constexpr int NF = DIM + 2;
     Real nn = 0;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) nn += nor[d] * nor[d];
-    const Real nor_mag = sqrt(nn);
-    const Real rho1 = s1[0], rho2 = s2[0];
-    const Real rho_mean = Real(0.5) * (rho1 + rho2);
-    const Real rho_ln = log_mean(rho1, rho2);
-    const Real drho = rho2 - rho1;
-    Real vm[DIM];
-    Real V_sq1 = 0, V_sq2 = 0, Vn = 0, h_hat = 0, diss = 0;
+    Real rho_ln, irho_ln, rs_rho, beta_ln, ibeta_ln, rs_beta;
+    log_mean(a.rho, b.rho, a.rrho, rho_ln, irho_ln, rs_rho);
+    log_mean(a.beta, b.beta, a.rbeta, beta_ln, ibeta_ln, rs_beta);
+    const Real rho_mean = Real(0.5) * (a.rho + b.rho);
+    const Real drho = b.rho - a.rho;
+    Real vm[DIM], Vn = 0, h = Real(-0.25) * (a.vsq + b.vsq), diss = 0;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
-        const Real a1 = s1[1 + d] / rho1, a2 = s2[1 + d] / rho2;
-        vm[d] = Real(0.5) * (a1 + a2);
-        const Real da = a2 - a1;
-        V_sq1 += a1 * a1;
-        V_sq2 += a2 * a2;
+        vm[d] = Real(0.5) * (a.v[d] + b.v[d]);
+        const Real dv = b.v[d] - a.v[d];
         Vn += vm[d] * nor[d];
-        h_hat += Real(-0.25) * (a1 * a1 + a2 * a2) + vm[d] * vm[d];
+        h += vm[d] * vm[d];
         if (DIM == 3 && d == 2 && quirk3)
-            diss += Real(0.5) * drho * a1 * a2 + rho_mean * da + vm[d];
+            diss += Real(0.5) * drho * a.v[d] * b.v[d] + rho_mean * dv + vm[d];
         else
-            diss += Real(0.5) * drho * a1 * a2 + rho_mean * da * vm[d];
+            diss += Real(0.5) * drho * a.v[d] * b.v[d] + rho_mean * dv * vm[d];
     }
-    const Real p1 = gammaM1 * (s1[NF - 1] - Real(0.5) * rho1 * V_sq1);
-    const Real p2 = gammaM1 * (s2[NF - 1] - Real(0.5) * rho2 * V_sq2);
-    Real lambda = sqrt(V_sq1) + sqrt(gamma * p1 / rho1);
-    lambda = dmax(lambda, sqrt(V_sq2) + sqrt(gamma * p2 / rho2));
-    const Real beta1 = Real(0.5) * rho1 / p1, beta2 = Real(0.5) * rho2 / p2;
-    const Real beta_ln = log_mean(beta1, beta2);
-    const Real p_hat = Real(0.5) * (rho1 + rho2) / (beta1 + beta2);
-    h_hat += Real(0.5) / beta_ln * gammaM1Inverse + p_hat / rho_ln;
-    diss += Real(0.5) * drho * gammaM1Inverse / beta_ln +
-            Real(0.5) * rho_mean * gammaM1Inverse * (Real(1) / beta2 - Real(1) / beta1);
-    const Real hl = dissipation ? Real(0.5) * lambda * nor_mag : Real(0);
-    flux[0] = rho_ln * Vn - hl * (rho2 - rho1);
+    const Real p_hat = rho_mean * rs_beta;
+    h += Real(0.5) * gammaM1Inverse * ibeta_ln + p_hat * irho_ln;
+    diss += Real(0.5) * drho * gammaM1Inverse * ibeta_ln + Real(0.5) * rho_mean * gammaM1Inverse * (b.rbeta - a.rbeta);
+    const Real hl = dissipation ? Real(0.5) * dmax(a.lam, b.lam) * sqrt(nn) : Real(0);
+    const Real F0 = rho_ln * Vn;
+    flux[0] = F0 - hl * drho;
 #pragma unroll
-    for (int d = 0; d < DIM; ++d)
-        flux[1 + d] = Vn * (rho_ln * vm[d]) + p_hat * nor[d] - hl * (s2[1 + d] - s1[1 + d]);
-    flux[NF - 1] = rho_ln * Vn * h_hat - hl * diss;
+    for (int d = 0; d < DIM; ++d) flux[1 + d] = F0 * vm[d] + p_hat * nor[d] - hl * (s2[1 + d] - s1[1 + d]);
+    flux[NF - 1] = F0 * h - hl * diss;
 }
 
-// NavierStokesFlux.cpp:12-90 (with Conserv2Prim, BasicOperations.cpp:172-186).
-// As in the reference, ComputePressure overwrites the momentum slots of
-// `state` with velocity (BasicOperations.cpp:33-34); callers that must not
-// see that pass a copy.  Fv is [NF][DIM]; row 0 is zero.
-template <int DIM, typename Real>
-__device__ __forceinline__ void viscous_flux(Real *state, const Real (*dq)[DIM + 2],
-                                             const PhysParams &P, Real (*Fv)[DIM]) {
+// NavierStokesFlux.cpp:12-90 from primitives (rho, v, p): the stress tensor with
+// the bulk coefficient mu_bulk = 2/3 and the heat flux lambda*cv grad T with
+// lambda = mu gamma / Pr; row 0 (mass) is zero.  dq[c] = d(rho, v, p)/dx_c.
+// Calls `emit(f, c, value)` for f = 1..NF-1, c = 0..DIM-1 so callers can
+// project or store without holding the whole matrix.
+template <int DIM, typename Real, typename Emit>
+__device__ __forceinline__ void viscous_flux(Real rho, Real rrho, const Real *v, Real p,
+                                             const Real (*dq)[DIM + 2], const PhysParams &P, Emit emit) {
     constexpr int NF = DIM + 2;
-    Real prim[NF];
-    prim[0] = state[0];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) prim[1 + d] = state[1 + d] / state[0];
-    {
-        const Real minv = Real(1) / state[0];
-        Real vv = 0;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) state[1 + d] *= minv;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) vv += state[1 + d] * state[1 + d];
-        prim[NF - 1] = Real(P.gammaM1) * (state[NF - 1] - Real(0.5) * state[0] * vv);
-    }
     Real mu = Real(P.mu);
     if (P.sutherland) {   // NavierStokesFlux.hpp:32-36
-        const Real T = prim[NF - 1] / (prim[0] * Real(P.R_gas));
-        mu = Real(P.mu0) * Real(P.T0pTs) / (T + Real(P.Ts)) * (T / Real(P.T0)) * sqrt(T / Real(P.T0));
+        const Real T = p * rrho * rcp(Real(P.R_gas));
+        mu = Real(P.mu0) * Real(P.T0pTs) * rcp(T + Real(P.Ts)) * (T * rcp(Real(P.T0))) * sqrt(T * rcp(Real(P.T0)));
     }
     const Real lambda = mu * Real(P.gamma) * Real(P.PrInverse);
     Real div = 0;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) div += dq[d][1 + d];
-    const Real gm1i = Real(P.gammaM1Inverse), mub = Real(P.mu_bulk);
+    const Real gm1i_r = Real(P.gammaM1Inverse) * rrho, pr = p * rrho, mub = Real(P.mu_bulk);
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
-        Fv[0][c] = 0;
-#pragma unroll
-        for (int r = 0; r < DIM; ++r) {
-            // tau(r, c): diagonal mu(2 du_r/dx_r - mu_bulk div), off-diagonal mu(du_r/dx_c + du_c/dx_r)
-            if (r == c)
-                Fv[1 + r][c] = mu * (Real(2) * dq[c][1 + r] - mub * div);
-            else
-                Fv[1 + r][c] = mu * (dq[c][1 + r] + dq[r][1 + c]);
-        }
-        const Real cv_dT = gm1i / prim[0] * (dq[c][NF - 1] - prim[NF - 1] / prim[0] * dq[c][0]);
         Real e = 0;
 #pragma unroll
-        for (int r = 0; r < DIM; ++r) e += prim[1 + r] * Fv[1 + r][c];
-        Fv[NF - 1][c] = e + lambda * cv_dT;
+        for (int r = 0; r < DIM; ++r) {
+            const Real tau = (r == c) ? mu * (Real(2) * dq[c][1 + r] - mub * div)
+                                      : mu * (dq[c][1 + r] + dq[r][1 + c]);
+            emit(1 + r, c, tau);
+            e += v[r] * tau;
+        }
+        const Real cv_dT = gm1i_r * (dq[c][NF - 1] - pr * dq[c][0]);
+        emit(NF - 1, c, e + lambda * cv_dT);
     }
 }
 
-// BasicOperations.cpp:81-104 on a private copy of the node state.
+// BasicOperations.cpp:81-104: entropy variables with beta = rho/p,
+// s = log(p rho^-gamma) = log p - gamma log rho.
 template <int DIM, typename Real>
 __device__ __forceinline__ void conserv2entropy(const Real *s, const PhysParams &P, Real *v) {
     constexpr int NF = DIM + 2;
-    const Real minv = Real(1) / s[0];
+    const Real minv = rcp(s[0]);
     Real vel[DIM], vv = 0;
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) vel[d] = s[1 + d] * minv;
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) vv += vel[d] * vel[d];
+    for (int d = 0; d < DIM; ++d) {
+        vel[d] = s[1 + d] * minv;
+        vv += vel[d] * vel[d];
+    }
     const Real v_sq = Real(0.5) * vv;
     const Real p = Real(P.gammaM1) * (s[NF - 1] - s[0] * v_sq);
-    const Real beta = s[0] / p;
-    const Real sent = log(p * pow(s[0], -Real(P.gamma)));
+    const Real beta = s[0] * rcp(p);
+    const Real sent = log(p) - Real(P.gamma) * log(s[0]);
     v[0] = (Real(P.gamma) - sent) * Real(P.gammaM1Inverse) - beta * v_sq;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) v[1 + d] = beta * vel[d];
@@ -197,36 +214,32 @@ __device__ __forceinline__ void conserv2entropy(const Real *s, const PhysParams 
 }
 
 // BasicOperations.cpp:126-170 for one node and one derivative direction.
-// quirks == 0 keeps the reference's aliasing (`vel /= state(0)` turns the
-// momentum slots of the state copy into velocity before the density-gradient
-// line reads them).
+// quirks == 0 keeps the reference's aliasing: `vel /= state(0)` turns the
+// momentum slots of its state copy into velocity before the density-gradient
+// line reads them.
 template <int DIM, typename Real>
-__device__ __forceinline__ void entropygrad2primgrad(const Real *s_in, const PhysParams &P, Real *g) {
+__device__ __forceinline__ void entropygrad2primgrad(const Real *s, const PhysParams &P, Real *g) {
     constexpr int NF = DIM + 2;
-    Real s[NF], gs[NF], vel[DIM];
+    const Real minv = rcp(s[0]);
+    Real vel[DIM], vv = 0, gs[NF];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) { s[f] = s_in[f]; gs[f] = g[f]; }
-    const Real minv = Real(1) / s[0];
-    Real vv = 0;
+    for (int f = 0; f < NF; ++f) gs[f] = g[f];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) vel[d] = s[1 + d] * minv;
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) vv += vel[d] * vel[d];
-    if (P.quirks == 0) {
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) s[1 + d] = vel[d];
+    for (int d = 0; d < DIM; ++d) {
+        vel[d] = s[1 + d] * minv;
+        vv += vel[d] * vel[d];
     }
     const Real v_sq = Real(0.5) * vv;
     const Real p = Real(P.gammaM1) * (s[NF - 1] - s[0] * v_sq);
     const Real KE = v_sq * s[0];
-    const Real pr = p / s[0];
+    const Real pr = p * minv, rp = s[0] * rcp(p);
     Real acc = 0;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
         g[1 + d] = pr * (gs[1 + d] + vel[d] * gs[NF - 1]);
-        acc += s[1 + d] * g[1 + d];
+        acc += ((P.quirks == 0) ? vel[d] : s[1 + d]) * g[1 + d];
     }
-    g[0] = s[0] * gs[0] - gs[NF - 1] * (KE - p * Real(P.gammaM1Inverse)) + s[0] / p * acc;
+    g[0] = s[0] * gs[0] - gs[NF - 1] * (KE - p * Real(P.gammaM1Inverse)) + rp * acc;
     g[NF - 1] = pr * (g[0] + p * gs[NF - 1]);
 }
 

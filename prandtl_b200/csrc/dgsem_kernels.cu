@@ -131,15 +131,57 @@ __device__ __forceinline__ void block_max_to(unsigned long long *dst, double v, 
     }
 }
 
+// Hoisted per-node primitive table in shared memory: H[k*ND + node].
+template <int DIM>
+struct HIdx {
+    static constexpr int RHO = 0, RRHO = 1, V = 2, VSQ = 2 + DIM, BETA = 3 + DIM, RBETA = 4 + DIM,
+                         LAM = 5 + DIM, K = 6 + DIM;
+};
+template <int DIM, int ND>
+__device__ __forceinline__ Prim<DIM, double> load_prim(const double *sH, int n) {
+    using I = HIdx<DIM>;
+    Prim<DIM, double> q;
+    q.rho = sH[I::RHO * ND + n];
+    q.rrho = sH[I::RRHO * ND + n];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) q.v[d] = sH[(I::V + d) * ND + n];
+    q.vsq = sH[I::VSQ * ND + n];
+    q.beta = sH[I::BETA * ND + n];
+    q.rbeta = sH[I::RBETA * ND + n];
+    q.lam = sH[I::LAM * ND + n];
+    return q;
+}
+template <int DIM, int ND>
+__device__ __forceinline__ void store_prim(double *sH, int n, const Prim<DIM, double> &q) {
+    using I = HIdx<DIM>;
+    sH[I::RHO * ND + n] = q.rho;
+    sH[I::RRHO * ND + n] = q.rrho;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) sH[(I::V + d) * ND + n] = q.v[d];
+    sH[I::VSQ * ND + n] = q.vsq;
+    sH[I::BETA * ND + n] = q.beta;
+    sH[I::RBETA * ND + n] = q.rbeta;
+    sH[I::LAM * ND + n] = q.lam;
+}
+
+template <int DIM, int NP, bool NS>
+struct RhsLayout {
+    using S = Shape<DIM, NP>;
+    static constexpr int ND = S::ND, NF = S::NF;
+    static constexpr int NSCR = cmax(cmax(S::NPAIR, S::NIF), cmax(S::NFI, 5 * ND / NF + 1)) * NF;
+    static constexpr int PER_ELEM = NF * ND + HIdx<DIM>::K * ND + NSCR + (NS ? DIM * NF * ND : 0);
+    static constexpr int MIN_BLOCKS = NS ? 3 : 4;
+};
+
 // ------------------------------------------------------------------- RHS
 template <int DIM, int NP, bool NS>
-__global__ void __launch_bounds__(Shape<DIM, NP>::THREADS)
+__global__ void __launch_bounds__(Shape<DIM, NP>::THREADS, (RhsLayout<DIM, NP, NS>::MIN_BLOCKS))
 rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_constant__ OpTables T) {
     using S = Shape<DIM, NP>;
+    using LY = RhsLayout<DIM, NP, NS>;
     constexpr int ND = S::ND, NF = S::NF, NLINE = S::NLINE, PPL = S::PPL, NPAIR = S::NPAIR;
     constexpr int NFN = S::NFN, NFI = S::NFI, NIF = S::NIF, EPB = S::EPB;
-    constexpr int NSCR = cmax(cmax(NPAIR, NIF), cmax(NFI, 5 * ND / NF + 1)) * NF;
-    constexpr int PER_ELEM = NF * ND + NSCR + (NS ? DIM * NF * ND : 0);
+    constexpr int NSCR = LY::NSCR, PER_ELEM = LY::PER_ELEM;
 
     extern __shared__ double smem[];
     __shared__ double sAlpha[EPB];
@@ -154,18 +196,22 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
     const int e_raw = blockIdx.x * EPB + el;
     const bool active = e_raw < m.E;
     const int e = active ? e_raw : m.E - 1;
-    double *sU = smem + S::TAB + el * PER_ELEM;
-    double *sS = sU + NF * ND;
-    double *sV = sS + NSCR;   // NS: contravariant viscous fluxes [DIM][NF][ND]
+    double *sU = smem + S::TAB + el * PER_ELEM;    // conserved state [NF][ND]
+    double *sH = sU + NF * ND;                     // hoisted primitives [K][ND]
+    double *sS = sH + HIdx<DIM>::K * ND;           // scratch: pairs / FV / face items
+    double *sV = sS + NSCR;                        // NS: contravariant viscous fluxes [DIM][NF][ND]
 
     const long long Ndof = m.Ndof;
     const long long gnode = (long long)e * ND + n;
+    const double gamma = P.gamma, gm1 = P.gammaM1, gm1i = P.gammaM1Inverse;
     double st[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
         st[f] = __ldg(a.u + f * Ndof + gnode);
         sU[f * ND + n] = st[f];
     }
+    const Prim<DIM, double> me = primitives<DIM, double>(st, gamma, gm1);
+    store_prim<DIM, ND>(sH, n, me);
     const double *geo = m.geo + (long long)e * (DIM * DIM + 1);
     double adj[DIM][DIM];
 #pragma unroll
@@ -176,63 +222,24 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
     int c[3];
     node_coords<NP>(n, c);
 
-    const double gamma = P.gamma, gm1 = P.gammaM1, gm1i = P.gammaM1Inverse;
-
     // ---- largest characteristic speed |V| + c of this state
-    if (a.lambda) {
-        double vv = 0;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) { const double vd = st[1 + d] / st[0]; vv += vd * vd; }
-        const double p = gm1 * (st[NF - 1] - 0.5 * st[0] * vv);
-        double lam = sqrt(vv) + sqrt(gamma * p / st[0]);
-        if (!active) lam = 0.0;
-        block_max_to<S::THREADS>(a.lambda, lam, sRed);
-    }
-
-    // ---- NS: primitive gradients (own node) and contravariant viscous flux
-    if constexpr (NS) {
-        double dq[DIM][NF];
-#pragma unroll
-        for (int d = 0; d < DIM; ++d)
-#pragma unroll
-            for (int f = 0; f < NF; ++f) dq[d][f] = __ldg(a.grad + (d * NF + f) * Ndof + gnode);
-        __syncthreads();   // sU complete (quirk Q1 reads another node's state)
-        double sv[NF], Fv[NF][DIM];
-        // Q1 (DGSEMIntegrator.cpp:620): the reference evaluates the volume
-        // viscous flux with the state of node Np^d-1 (stale member id1).
-        const int src = (P.quirks == 0) ? ND - 1 : n;
-#pragma unroll
-        for (int f = 0; f < NF; ++f) sv[f] = sU[f * ND + src];
-        viscous_flux<DIM, double>(sv, dq, P, Fv);
-        // flux_mat = adj * Fv^T (mfem::MultABt, :632)
-#pragma unroll
-        for (int r = 0; r < DIM; ++r)
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                double s = 0.0;
-#pragma unroll
-                for (int q = 0; q < DIM; ++q) s += adj[r][q] * Fv[f][q];
-                sV[(r * NF + f) * ND + n] = s;
-            }
-    }
+    if (a.lambda) block_max_to<S::THREADS>(a.lambda, active ? me.lam : 0.0, sRed);
 
     // ---- blending coefficient (PerssonPeraireIndicator.cpp:21-58, DGSEMOperator.cpp:60-80)
     if (P.blending) {
         double *b0 = sS, *b1 = sS + ND;
         {
-            double s[NF];
-#pragma unroll
-            for (int f = 0; f < NF; ++f) s[f] = st[f];
-            const double minv = 1.0 / s[0];
             double vv = 0;
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) { s[1 + d] *= minv; vv += s[1 + d] * s[1 + d]; }
-            b0[n] = s[0] * (gm1 * (s[NF - 1] - 0.5 * s[0] * vv));
+            for (int d = 0; d < DIM; ++d) {
+                const double vd = st[1 + d] * me.rrho;
+                vv += vd * vd;
+            }
+            b0[n] = st[0] * (gm1 * (st[NF - 1] - 0.5 * st[0] * vv));
         }
         __syncthreads();
-        // modes = V^-1 (rho p) as DIM passes of the 1D inverse Vandermonde
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) {
+        for (int d = 0; d < DIM; ++d) {   // modes = V^-1 (rho p), one direction per pass
             const double *in = (d & 1) ? b1 : b0;
             double *out = (d & 1) ? b0 : b1;
             int base, stride;
@@ -240,7 +247,6 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
             double s = 0.0;
 #pragma unroll
             for (int l = 0; l < NP; ++l) s += sVinv[c[d] * NP + l] * in[base + l * stride];
-            __syncthreads();
             out[n] = s;
             __syncthreads();
         }
@@ -269,6 +275,34 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
     } else {
         if (n == 0) sAlpha[el] = 0.0;
     }
+
+    // ---- NS: contravariant viscous flux of this node (flux_mat = adj * Fv^T, :632)
+    if constexpr (NS) {
+        double dq[DIM][NF];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+#pragma unroll
+            for (int f = 0; f < NF; ++f) dq[d][f] = __ldg(a.grad + (d * NF + f) * Ndof + gnode);
+        __syncthreads();   // sU/sH complete: quirk Q1 reads another node
+        // Q1 (DGSEMIntegrator.cpp:620): the reference evaluates the volume
+        // viscous flux with the state of node Np^d-1 (stale member id1).
+        const int src = (P.quirks == 0) ? ND - 1 : n;
+        const Prim<DIM, double> q = load_prim<DIM, ND>(sH, src);
+        double Vc[DIM][NF];
+#pragma unroll
+        for (int r = 0; r < DIM; ++r)
+#pragma unroll
+            for (int f = 0; f < NF; ++f) Vc[r][f] = 0.0;
+        const double pq = q.rbeta * q.rho * 0.5;   // p = rho/(2 beta)
+        viscous_flux<DIM, double>(q.rho, q.rrho, q.v, pq, dq, P, [&](int f, int cc, double val) {
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) Vc[r][f] += adj[r][cc] * val;
+        });
+#pragma unroll
+        for (int r = 0; r < DIM; ++r)
+#pragma unroll
+            for (int f = 0; f < NF; ++f) sV[(r * NF + f) * ND + n] = Vc[r][f];
+    }
     __syncthreads();
     const double alpha = sAlpha[el];
 
@@ -281,12 +315,10 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
         pair_decode<NP>(pp, pa, pb);
         line_base<DIM, NP>(dir, ln, base, stride);
         const int n1 = base + pa * stride, n2 = base + pb * stride;
-        double s1[NF], s2[NF], F[NF], mt[DIM];
-#pragma unroll
-        for (int f = 0; f < NF; ++f) { s1[f] = sU[f * ND + n1]; s2[f] = sU[f * ND + n2]; }
+        double F[NF], mt[DIM];
 #pragma unroll
         for (int q = 0; q < DIM; ++q) mt[q] = (dir == 0) ? adj[0][q] : (dir == 1 ? adj[1][q] : adj[DIM - 1][q]);
-        volume_flux<DIM, double>(s1, s2, mt, gm1, gm1i, F);
+        volume_flux<DIM, double>(load_prim<DIM, ND>(sH, n1), load_prim<DIM, ND>(sH, n2), mt, gm1i, F);
 #pragma unroll
         for (int f = 0; f < NF; ++f) sS[f * NPAIR + p] = F[f];
     }
@@ -305,8 +337,8 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
             const int pbase = dir * NLINE * PPL + ln * PPL;
 #pragma unroll
             for (int l = 0; l < NP; ++l) {
-                const double dh = sDh2[pos * NP + l];
                 if (l == pos) continue;
+                const double dh = sDh2[pos * NP + l];
                 int pidx;
                 bool zero = false;
                 if (NS && DIM == 3 && dir == 2 && l < pos && P.quirks == 0) {
@@ -348,22 +380,24 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
 
     // ---- subcell first-order FV (DGSEMIntegrator.cpp:972-1196), skipped when alpha == 0
     if (P.blending) {
-        for (int it = n; it < NIF; it += ND) {
-            if (alpha == 0.0) break;
-            const int dir = it / (NLINE * (NP - 1));
-            const int r = it - dir * NLINE * (NP - 1);
-            const int ln = r / (NP - 1), ii = r - ln * (NP - 1);
-            int base, stride;
-            line_base<DIM, NP>(dir, ln, base, stride);
-            const int n1 = base + ii * stride, n2 = n1 + stride;
-            double s1[NF], s2[NF], F[NF], nor[DIM];
+        if (alpha != 0.0) {
+            for (int it = n; it < NIF; it += ND) {
+                const int dir = it / (NLINE * (NP - 1));
+                const int r = it - dir * NLINE * (NP - 1);
+                const int ln = r / (NP - 1), ii = r - ln * (NP - 1);
+                int base, stride;
+                line_base<DIM, NP>(dir, ln, base, stride);
+                const int n1 = base + ii * stride, n2 = n1 + stride;
+                double s1[NF], s2[NF], F[NF], nor[DIM];
 #pragma unroll
-            for (int f = 0; f < NF; ++f) { s1[f] = sU[f * ND + n1]; s2[f] = sU[f * ND + n2]; }
+                for (int f = 0; f < NF; ++f) { s1[f] = sU[f * ND + n1]; s2[f] = sU[f * ND + n2]; }
 #pragma unroll
-            for (int q = 0; q < DIM; ++q) nor[q] = (dir == 0) ? adj[0][q] : (dir == 1 ? adj[1][q] : adj[DIM - 1][q]);
-            face_flux<DIM, double>(s1, s2, nor, gamma, gm1, gm1i, P.quirks == 0, true, F);
+                for (int q = 0; q < DIM; ++q) nor[q] = (dir == 0) ? adj[0][q] : (dir == 1 ? adj[1][q] : adj[DIM - 1][q]);
+                face_flux<DIM, double>(s1, load_prim<DIM, ND>(sH, n1), s2, load_prim<DIM, ND>(sH, n2), nor, gm1i,
+                                       P.quirks == 0, true, F);
 #pragma unroll
-            for (int f = 0; f < NF; ++f) sS[f * NIF + it] = F[f];
+                for (int f = 0; f < NF; ++f) sS[f * NIF + it] = F[f];
+            }
         }
         __syncthreads();
         if (alpha != 0.0) {
@@ -391,63 +425,55 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
     }
 
     // ---- surface fluxes of the element's own faces
-    const double w0 = sW[0];
+    const double aw = 1.0 / (sW[0] * J);
     for (int it = n; it < NFI; it += ND) {
         const int lf = it / NFN, fa = it - lf * NFN;
         const int no = face_node<DIM, NP>(lf, fa);
         const int4 t = __ldg(m.nbr + (long long)e * (2 * DIM) + lf);
         const int nn = face_node<DIM, NP>(t.y, fa);
         const long long gn = (long long)t.x * ND + nn;
+        const bool own_is_1 = (t.w == 0);
         double so[NF], sn[NF], nor[DIM], flux[NF], d1[NF];
 #pragma unroll
         for (int f = 0; f < NF; ++f) { so[f] = sU[f * ND + no]; sn[f] = __ldg(a.u + f * Ndof + gn); }
 #pragma unroll
         for (int q = 0; q < DIM; ++q) nor[q] = __ldg(m.fnor + (long long)t.z * DIM + q);
-        const bool own_is_1 = (t.w == 0);
-        double s1[NF], s2[NF];
+        Prim<DIM, double> po = load_prim<DIM, ND>(sH, no);
+        Prim<DIM, double> pn = primitives<DIM, double>(sn, gamma, gm1);
+        double fn[NF];
 #pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            s1[f] = own_is_1 ? so[f] : sn[f];
-            s2[f] = own_is_1 ? sn[f] : so[f];
-        }
-        if constexpr (!NS) {
-            face_flux<DIM, double>(s1, s2, nor, gamma, gm1, gm1i, P.quirks == 0, P.dissipation != 0, flux);
-#pragma unroll
-            for (int f = 0; f < NF; ++f) d1[f] = own_is_1 ? -flux[f] : flux[f];
-        } else {
-            // DGSEMIntegrator.cpp:435-494 (3D) / :496-549 (2D)
-            double q1[DIM][NF], q2[DIM][NF], Fv1[NF][DIM], Fv2[NF][DIM];
+        for (int f = 0; f < NF; ++f) fn[f] = 0.0;
+        if constexpr (NS) {
+            // DGSEMIntegrator.cpp:435-549: 0.5 (Fv1 + Fv2) . n from each trace's
+            // own state and lifted gradients
             const long long go = (long long)e * ND + no;
-            const long long g1 = own_is_1 ? go : gn, g2 = own_is_1 ? gn : go;
 #pragma unroll
-            for (int d = 0; d < DIM; ++d)
+            for (int side = 0; side < 2; ++side) {
+                const long long g = side == 0 ? go : gn;
+                const Prim<DIM, double> &q = side == 0 ? po : pn;
+                double dq[DIM][NF];
 #pragma unroll
-                for (int f = 0; f < NF; ++f) {
-                    q1[d][f] = __ldg(a.grad + (d * NF + f) * Ndof + g1);
-                    q2[d][f] = __ldg(a.grad + (d * NF + f) * Ndof + g2);
-                }
-            double c1[NF], c2[NF];
+                for (int d = 0; d < DIM; ++d)
 #pragma unroll
-            for (int f = 0; f < NF; ++f) { c1[f] = s1[f]; c2[f] = s2[f]; }
-            viscous_flux<DIM, double>(c1, q1, P, Fv1);
-            viscous_flux<DIM, double>(c2, q2, P, Fv2);
-            // Q8: ComputeViscousFlux overwrites the traces' momentum with velocity
-            // before ComputeFaceFlux reads them (DGSEMIntegrator.cpp:471-481);
-            // the fixed mode passes the untouched traces.
-            if (P.quirks == 0) {
-#pragma unroll
-                for (int f = 0; f < NF; ++f) { s1[f] = c1[f]; s2[f] = c2[f]; }
+                    for (int f = 0; f < NF; ++f) dq[d][f] = __ldg(a.grad + (d * NF + f) * Ndof + g);
+                viscous_flux<DIM, double>(q.rho, q.rrho, q.v, 0.5 * q.rbeta * q.rho, dq, P,
+                                          [&](int f, int cc, double val) { fn[f] += (0.5 * val) * nor[cc]; });
             }
-            face_flux<DIM, double>(s1, s2, nor, gamma, gm1, gm1i, P.quirks == 0, P.dissipation != 0, flux);
+            if (P.quirks == 0) {
+                // Q8 (BasicOperations.cpp:33-34 via NavierStokesFlux.cpp:14): the face
+                // Riemann flux reads states whose momentum slots now hold velocity.
 #pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                double fn = 0.0;
-#pragma unroll
-                for (int q = 0; q < DIM; ++q) fn += ((Fv1[f][q] + Fv2[f][q]) * 0.5) * nor[q];
-                d1[f] = own_is_1 ? (-flux[f] + fn) : (flux[f] - fn);
+                for (int d = 0; d < DIM; ++d) { so[1 + d] *= po.rrho; sn[1 + d] *= pn.rrho; }
+                po = primitives<DIM, double>(so, gamma, gm1);
+                pn = primitives<DIM, double>(sn, gamma, gm1);
             }
         }
-        const double aw = 1.0 / (w0 * J);
+        if (own_is_1)
+            face_flux<DIM, double>(so, po, sn, pn, nor, gm1i, P.quirks == 0, P.dissipation != 0, flux);
+        else
+            face_flux<DIM, double>(sn, pn, so, po, nor, gm1i, P.quirks == 0, P.dissipation != 0, flux);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) d1[f] = own_is_1 ? (-flux[f] + fn[f]) : (flux[f] - fn[f]);
 #pragma unroll
         for (int f = 0; f < NF; ++f) sS[f * NFI + it] = aw * d1[f];
     }
@@ -510,12 +536,11 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
 // (LiftingBR1.cpp:156-272), face lifting 1/2 (v2 - v1) n (LiftingBR1.cpp:10-115)
 // and the chain rule to primitive gradients (BasicOperations.cpp:126-170).
 template <int DIM, int NP>
-__global__ void __launch_bounds__(Shape<DIM, NP>::THREADS)
+__global__ void __launch_bounds__(Shape<DIM, NP>::THREADS, 4)
 lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_constant__ OpTables T) {
     using S = Shape<DIM, NP>;
-    constexpr int ND = S::ND, NF = S::NF, NFN = S::NFN, NFI = S::NFI, EPB = S::EPB;
+    constexpr int ND = S::ND, NF = S::NF, NFN = S::NFN, NFI = S::NFI;
     constexpr int PER_ELEM = 2 * NF * ND + DIM * NF * NFI;
-    (void)EPB;
     extern __shared__ double smem[];
     double *sT = smem;
     const double *sD = sT, *sW = sT + 4 * NP * NP;
@@ -549,40 +574,11 @@ lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_
     const double J = __ldg(geo + DIM * DIM);
     int c[3];
     node_coords<NP>(n, c);
+
+    // face part first (its neighbour loads overlap the element part):
+    // +1/(w0 J) * 1/2 (v_elem2 - v_elem1) * n_c on both sides
+    const double aw = 1.0 / (sW[0] * J);
     __syncthreads();
-
-    // element part: g1(f, r) = sum_l D(pos_r, l) v_l along direction r
-    double g1[NF][DIM];
-#pragma unroll
-    for (int f = 0; f < NF; ++f)
-#pragma unroll
-        for (int r = 0; r < DIM; ++r) g1[f][r] = 0.0;
-    int base[DIM], stride[DIM];
-#pragma unroll
-    for (int r = 0; r < DIM; ++r) line_base<DIM, NP>(r, line_index<DIM, NP>(r, c), base[r], stride[r]);
-#pragma unroll
-    for (int l = 0; l < NP; ++l)
-#pragma unroll
-        for (int r = 0; r < DIM; ++r) {
-            const double dl = sD[c[r] * NP + l];
-#pragma unroll
-            for (int f = 0; f < NF; ++f) g1[f][r] += sVe[f * ND + base[r] + l * stride[r]] * dl;
-        }
-    // grad_mat2 = grad_mat1 * adj, times 1/J (LiftingBR1.cpp:205-206)
-    const double mJ = 1.0 / J;
-    double g[DIM][NF];
-#pragma unroll
-    for (int q = 0; q < DIM; ++q)
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            double s = 0.0;
-#pragma unroll
-            for (int r = 0; r < DIM; ++r) s += g1[f][r] * adj[r][q];
-            g[q][f] = s * mJ;
-        }
-
-    // face part: +1/(w0 J) * 1/2 (v_elem2 - v_elem1) * n_c on both sides
-    const double w0 = sW[0];
     for (int it = n; it < NFI; it += ND) {
         const int lf = it / NFN, fa = it - lf * NFN;
         const int no = face_node<DIM, NP>(lf, fa);
@@ -596,7 +592,6 @@ lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_
 #pragma unroll
         for (int q = 0; q < DIM; ++q) nor[q] = __ldg(m.fnor + (long long)t.z * DIM + q);
         const bool own_is_1 = (t.w == 0);
-        const double aw = 1.0 / (w0 * J);
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
             const double vo = sVe[f * ND + no];
@@ -605,6 +600,36 @@ lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_
             for (int q = 0; q < DIM; ++q) sS[(q * NF + f) * NFI + it] = aw * (jf * nor[q]);
         }
     }
+
+    // element part: g1(f, r) = sum_l D(pos_r, l) v_l along direction r
+    double g1[NF][DIM];
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) g1[f][r] = 0.0;
+#pragma unroll
+    for (int r = 0; r < DIM; ++r) {
+        int base, stride;
+        line_base<DIM, NP>(r, line_index<DIM, NP>(r, c), base, stride);
+#pragma unroll
+        for (int l = 0; l < NP; ++l) {
+            const double dl = sD[c[r] * NP + l];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) g1[f][r] += sVe[f * ND + base + l * stride] * dl;
+        }
+    }
+    // grad_mat2 = grad_mat1 * adj, times 1/J (LiftingBR1.cpp:205-206)
+    const double mJ = 1.0 / J;
+    double g[DIM][NF];
+#pragma unroll
+    for (int q = 0; q < DIM; ++q)
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            double s = 0.0;
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) s += g1[f][r] * adj[r][q];
+            g[q][f] = s * mJ;
+        }
     __syncthreads();
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
@@ -631,10 +656,7 @@ lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_
 template <int DIM, int NP, bool NS>
 size_t rhs_smem() {
     using S = Shape<DIM, NP>;
-    constexpr int ND = S::ND, NF = S::NF;
-    constexpr int NSCR = cmax(cmax(S::NPAIR, S::NIF), cmax(S::NFI, 5 * ND / NF + 1)) * NF;
-    constexpr int PER_ELEM = NF * ND + NSCR + (NS ? DIM * NF * ND : 0);
-    return sizeof(double) * (S::TAB + (size_t)S::EPB * PER_ELEM);
+    return sizeof(double) * (S::TAB + (size_t)S::EPB * RhsLayout<DIM, NP, NS>::PER_ELEM);
 }
 template <int DIM, int NP>
 size_t lift_smem() {
