@@ -31,23 +31,27 @@ def needs_build() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(verbose_ptxas: bool = False, force: bool = False) -> str:
-    if not force and not needs_build():
+def build(verbose_ptxas: bool = False, force: bool = False, lib: str = LIB, defines=()) -> str:
+    """Compile the sources into `lib` (default: the in-tree library).  `defines`
+    are extra -D flags (launch-shape overrides used when tuning)."""
+    if not force and lib == LIB and not needs_build():
         return LIB
     objs = []
     for src in SOURCES:
         obj = os.path.join(CSRC, src.replace(".cu", ".o"))
+        obj = obj if lib == LIB else obj.replace(".o", f".{abs(hash(lib)) % 100000}.o")
         cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-               "--expt-relaxed-constexpr", "-c", os.path.join(CSRC, src), "-o", obj]
+               "--expt-relaxed-constexpr", *[f"-D{d}" for d in defines],
+               "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose_ptxas:
             cmd += ["-Xptxas", "-v"]
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", lib, *objs, "-lcudart"]
     subprocess.run(cmd, check=True)
     for o in objs:
         os.remove(o)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

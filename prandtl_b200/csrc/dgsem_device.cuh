@@ -38,7 +38,18 @@ struct OpTables {
 
 template <typename T> __device__ __forceinline__ T dmax(T a, T b) { return a > b ? a : b; }
 
-__device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
+// 1/x for positive normal x: hardware reciprocal estimate (PTX rcp.approx.ftz.f64)
+// refined by two Newton-Raphson steps r <- r + r (1 - x r), each doubling the
+// number of correct bits (Markstein, IBM J. Res. Dev. 34 (1990) 111-119).
+// Within an ulp of the correctly rounded reciprocal; no special-value paths.
+__device__ __forceinline__ double rcp(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
 __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
 
 // Per-node primitives of a conserved state s = (rho, rho v, E).

@@ -24,11 +24,9 @@ struct Shape {
     static constexpr int NF = DIM + 2;                  // conserved fields
     static constexpr int NLINE = ND / NP;               // lines per direction
     static constexpr int PPL = NP * (NP - 1) / 2;       // unique pairs per line
-    static constexpr int NPAIR = DIM * NLINE * PPL;     // unique volume pairs
     static constexpr int NFN = ND / NP;                 // nodes per face
     static constexpr int NFACE = 2 * DIM;
     static constexpr int NFI = NFACE * NFN;             // face-node items
-    static constexpr int NIF = DIM * NLINE * (NP - 1);  // subcell FV interfaces
     static constexpr int EPB = cmax(1, 128 / ND);       // elements per CTA
     static constexpr int THREADS = EPB * ND;
     static constexpr int TAB = 4 * NP * NP + 2 * NP;    // D, Dhat, Dhat2, Vinv, w, x
@@ -164,54 +162,77 @@ __device__ __forceinline__ void store_prim(double *sH, int n, const Prim<DIM, do
     sH[I::LAM * ND + n] = q.lam;
 }
 
+constexpr int next_pow2(int v) { return v <= 1 ? 1 : 2 * next_pow2((v + 1) / 2); }
+
+// Launch shape of the RHS kernel: warps per CTA and the minimum CTAs per SM the
+// register allocation must allow (launch bounds).
+#ifndef PRANDTL_NS_WARPS
+#define PRANDTL_NS_WARPS 4
+#endif
+#ifndef PRANDTL_NS_MINB
+#define PRANDTL_NS_MINB 3
+#endif
+#ifndef PRANDTL_EULER_WARPS
+#define PRANDTL_EULER_WARPS 4
+#endif
+#ifndef PRANDTL_EULER_MINB
+#define PRANDTL_EULER_MINB 5
+#endif
+
+// Warp-per-element layout of the RHS kernel: one group of GS lanes owns one
+// element (GS = 32, or the next power of two >= Np^d for small elements, so
+// a warp then holds several elements); lane `li` of a group owns the nodes
+// li, li+GS, ... and the pair / face / subcell items of the same stride.
+// Groups synchronise with __syncwarp only.
 template <int DIM, int NP, bool NS>
 struct RhsLayout {
     using S = Shape<DIM, NP>;
-    static constexpr int ND = S::ND, NF = S::NF;
-    static constexpr int NSCR = cmax(cmax(S::NPAIR, S::NIF), cmax(S::NFI, 5 * ND / NF + 1)) * NF;
-    static constexpr int PER_ELEM = NF * ND + HIdx<DIM>::K * ND + NSCR + (NS ? DIM * NF * ND : 0);
-    static constexpr int MIN_BLOCKS = NS ? 3 : 4;
+    static constexpr int ND = S::ND, NF = S::NF, NLINE = S::NLINE, PPL = S::PPL;
+    static constexpr int GS = ND >= 32 ? 32 : next_pow2(ND);
+    static constexpr int EPW = 32 / GS;                 // elements per warp
+    static constexpr int NPL = (ND + GS - 1) / GS;      // nodes per lane
+    static constexpr int WARPS = NS ? PRANDTL_NS_WARPS : PRANDTL_EULER_WARPS;
+    static constexpr int EPB = WARPS * EPW;             // elements per CTA
+    static constexpr int THREADS = WARPS * 32;
+    static constexpr int NPD = NLINE * PPL;             // pairs per direction
+    static constexpr int NID = NLINE * (NP - 1);        // subcell interfaces per direction
+    static constexpr int BUF = cmax(cmax(NPD, S::NFI), cmax(NID, (5 * ND + NF - 1) / NF)) * NF;
+    static constexpr int K = HIdx<DIM>::K;
+    static constexpr int PER_ELEM = K * ND + BUF + (NS ? DIM * NF * ND : 0);
+    static constexpr int MIN_BLOCKS = NS ? PRANDTL_NS_MINB : PRANDTL_EULER_MINB;
 };
 
 // ------------------------------------------------------------------- RHS
 template <int DIM, int NP, bool NS>
-__global__ void __launch_bounds__(Shape<DIM, NP>::THREADS, (RhsLayout<DIM, NP, NS>::MIN_BLOCKS))
+__global__ void __launch_bounds__(RhsLayout<DIM, NP, NS>::THREADS, (RhsLayout<DIM, NP, NS>::MIN_BLOCKS))
 rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_constant__ OpTables T) {
     using S = Shape<DIM, NP>;
     using LY = RhsLayout<DIM, NP, NS>;
-    constexpr int ND = S::ND, NF = S::NF, NLINE = S::NLINE, PPL = S::PPL, NPAIR = S::NPAIR;
-    constexpr int NFN = S::NFN, NFI = S::NFI, NIF = S::NIF, EPB = S::EPB;
-    constexpr int NSCR = LY::NSCR, PER_ELEM = LY::PER_ELEM;
+    constexpr int ND = S::ND, NF = S::NF, PPL = S::PPL;
+    constexpr int NFN = S::NFN, NFI = S::NFI, GS = LY::GS, NPL = LY::NPL;
+    constexpr int NPD = LY::NPD, NID = LY::NID;
 
     extern __shared__ double smem[];
-    __shared__ double sAlpha[EPB];
-    __shared__ double sRed[(S::THREADS + 31) / 32];
     double *sT = smem;
     const double *sDh = sT + NP * NP, *sDh2 = sT + 2 * NP * NP, *sVinv = sT + 3 * NP * NP;
     const double *sW = sT + 4 * NP * NP;
-    load_tables<NP>(T, sT, threadIdx.x, S::THREADS);
+    load_tables<NP>(T, sT, threadIdx.x, LY::THREADS);
+    __syncthreads();
 
-    const int el = threadIdx.x / ND;
-    const int n = threadIdx.x - el * ND;
-    const int e_raw = blockIdx.x * EPB + el;
+    const int lane = threadIdx.x & 31;
+    const int grp = threadIdx.x / GS;          // element slot within the CTA
+    const int li = threadIdx.x - grp * GS;     // lane within the group
+    const int e_raw = blockIdx.x * LY::EPB + grp;
     const bool active = e_raw < m.E;
     const int e = active ? e_raw : m.E - 1;
-    double *sU = smem + S::TAB + el * PER_ELEM;    // conserved state [NF][ND]
-    double *sH = sU + NF * ND;                     // hoisted primitives [K][ND]
-    double *sS = sH + HIdx<DIM>::K * ND;           // scratch: pairs / FV / face items
-    double *sV = sS + NSCR;                        // NS: contravariant viscous fluxes [DIM][NF][ND]
+    double *sH = smem + S::TAB + grp * LY::PER_ELEM;   // hoisted primitives [K][ND]
+    double *sF = sH + LY::K * ND;                       // pairs / subcell / face items / modes
+    double *sV = sF + LY::BUF;                          // NS: contravariant viscous fluxes [DIM][NF][ND]
+    const unsigned gmask = (GS == 32) ? 0xffffffffu : (((1u << GS) - 1u) << (lane & ~(GS - 1)));
+    (void)gmask;
 
     const long long Ndof = m.Ndof;
-    const long long gnode = (long long)e * ND + n;
     const double gamma = P.gamma, gm1 = P.gammaM1, gm1i = P.gammaM1Inverse;
-    double st[NF];
-#pragma unroll
-    for (int f = 0; f < NF; ++f) {
-        st[f] = __ldg(a.u + f * Ndof + gnode);
-        sU[f * ND + n] = st[f];
-    }
-    const Prim<DIM, double> me = primitives<DIM, double>(st, gamma, gm1);
-    store_prim<DIM, ND>(sH, n, me);
     const double *geo = m.geo + (long long)e * (DIM * DIM + 1);
     double adj[DIM][DIM];
 #pragma unroll
@@ -219,234 +240,282 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
 #pragma unroll
         for (int c2 = 0; c2 < DIM; ++c2) adj[r][c2] = __ldg(geo + r * DIM + c2);
     const double J = __ldg(geo + DIM * DIM);
-    int c[3];
-    node_coords<NP>(n, c);
+    const double mJ = 1.0 / J;
 
-    // ---- largest characteristic speed |V| + c of this state
-    if (a.lambda) block_max_to<S::THREADS>(a.lambda, active ? me.lam : 0.0, sRed);
+    // ---- own nodes: hoisted primitives; largest |V|+c
+    double lam = 0.0;
+#pragma unroll
+    for (int k = 0; k < NPL; ++k) {
+        const int n = li + k * GS;
+        if (n < ND) {
+            double st[NF];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) st[f] = __ldg(a.u + f * Ndof + (long long)e * ND + n);
+            const Prim<DIM, double> q = primitives<DIM, double>(st, gamma, gm1);
+            store_prim<DIM, ND>(sH, n, q);
+            lam = fmax(lam, q.lam);
+        }
+    }
+    if (a.lambda) {
+        double v = active ? lam : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0) atomic_max_pos(a.lambda, v);
+    }
+    __syncwarp();
 
     // ---- blending coefficient (PerssonPeraireIndicator.cpp:21-58, DGSEMOperator.cpp:60-80)
+    double alpha = 0.0;
     if (P.blending) {
-        double *b0 = sS, *b1 = sS + ND;
-        {
-            double vv = 0;
+        double *b0 = sF, *b1 = sF + ND;
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-                const double vd = st[1 + d] * me.rrho;
-                vv += vd * vd;
+        for (int k = 0; k < NPL; ++k) {
+            const int n = li + k * GS;
+            if (n < ND) {
+                // rho * ComputePressure(state) with v = m * (1/rho)
+                const Prim<DIM, double> q = load_prim<DIM, ND>(sH, n);
+                b0[n] = q.rho * (0.5 * q.rbeta * q.rho);
             }
-            b0[n] = st[0] * (gm1 * (st[NF - 1] - 0.5 * st[0] * vv));
         }
-        __syncthreads();
+        __syncwarp();
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {   // modes = V^-1 (rho p), one direction per pass
             const double *in = (d & 1) ? b1 : b0;
             double *out = (d & 1) ? b0 : b1;
-            int base, stride;
-            line_base<DIM, NP>(d, line_index<DIM, NP>(d, c), base, stride);
-            double s = 0.0;
 #pragma unroll
-            for (int l = 0; l < NP; ++l) s += sVinv[c[d] * NP + l] * in[base + l * stride];
-            out[n] = s;
-            __syncthreads();
-        }
-        const double md = ((DIM & 1) ? b1 : b0)[n];
-        int mx = c[0];
+            for (int k = 0; k < NPL; ++k) {
+                const int n = li + k * GS;
+                if (n < ND) {
+                    int c[3];
+                    node_coords<NP>(n, c);
+                    int base, stride;
+                    line_base<DIM, NP>(d, line_index<DIM, NP>(d, c), base, stride);
+                    double s = 0.0;
 #pragma unroll
-        for (int d = 1; d < DIM; ++d) mx = max(mx, c[d]);
-        double *r0 = sS + 2 * ND, *r1 = r0 + ND, *r2 = r1 + ND;
-        r0[n] = md * md;
-        r1[n] = (mx <= NP - 2) ? md * md : 0.0;
-        r2[n] = (mx <= NP - 3) ? md * md : 0.0;
-        __syncthreads();
-        if (n == 0) {
-            double e0 = 0, e1 = 0, e2 = 0;
-            for (int q = 0; q < ND; ++q) { e0 += r0[q]; e1 += r1[q]; e2 += r2[q]; }
-            double eta = 1.0 - e1 / e0;
-            eta = fmax(eta, 1.0 - e2 / e1);
-            const double thr = P.modal_threshold;
-            double al = 1.0 / (1.0 + exp(-9.21024 * (eta - thr) / thr));
-            if (al < P.alpha_min) al = 0.0;
-            else if (al > 1.0 - P.alpha_min) al = 1.0;
-            al = fmin(al, P.alpha_max);
-            sAlpha[el] = al;
-            if (a.alpha && active) a.alpha[e] = al;
-        }
-    } else {
-        if (n == 0) sAlpha[el] = 0.0;
-    }
-
-    // ---- NS: contravariant viscous flux of this node (flux_mat = adj * Fv^T, :632)
-    if constexpr (NS) {
-        double dq[DIM][NF];
-#pragma unroll
-        for (int d = 0; d < DIM; ++d)
-#pragma unroll
-            for (int f = 0; f < NF; ++f) dq[d][f] = __ldg(a.grad + (d * NF + f) * Ndof + gnode);
-        __syncthreads();   // sU/sH complete: quirk Q1 reads another node
-        // Q1 (DGSEMIntegrator.cpp:620): the reference evaluates the volume
-        // viscous flux with the state of node Np^d-1 (stale member id1).
-        const int src = (P.quirks == 0) ? ND - 1 : n;
-        const Prim<DIM, double> q = load_prim<DIM, ND>(sH, src);
-        double Vc[DIM][NF];
-#pragma unroll
-        for (int r = 0; r < DIM; ++r)
-#pragma unroll
-            for (int f = 0; f < NF; ++f) Vc[r][f] = 0.0;
-        const double pq = q.rbeta * q.rho * 0.5;   // p = rho/(2 beta)
-        viscous_flux<DIM, double>(q.rho, q.rrho, q.v, pq, dq, P, [&](int f, int cc, double val) {
-#pragma unroll
-            for (int r = 0; r < DIM; ++r) Vc[r][f] += adj[r][cc] * val;
-        });
-#pragma unroll
-        for (int r = 0; r < DIM; ++r)
-#pragma unroll
-            for (int f = 0; f < NF; ++f) sV[(r * NF + f) * ND + n] = Vc[r][f];
-    }
-    __syncthreads();
-    const double alpha = sAlpha[el];
-
-    // ---- two-point volume fluxes of every unique node pair
-    for (int p = n; p < NPAIR; p += ND) {
-        const int dir = p / (NLINE * PPL);
-        const int r = p - dir * NLINE * PPL;
-        const int ln = r / PPL, pp = r - ln * PPL;
-        int pa, pb, base, stride;
-        pair_decode<NP>(pp, pa, pb);
-        line_base<DIM, NP>(dir, ln, base, stride);
-        const int n1 = base + pa * stride, n2 = base + pb * stride;
-        double F[NF], mt[DIM];
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) mt[q] = (dir == 0) ? adj[0][q] : (dir == 1 ? adj[1][q] : adj[DIM - 1][q]);
-        volume_flux<DIM, double>(load_prim<DIM, ND>(sH, n1), load_prim<DIM, ND>(sH, n2), mt, gm1i, F);
-#pragma unroll
-        for (int f = 0; f < NF; ++f) sS[f * NPAIR + p] = F[f];
-    }
-    __syncthreads();
-
-    // ---- flux differencing: sum_l Dhat2(i,l) F#(i,l) per direction (F#(i,i) = 0)
-    double acc[NF];
-    {
-        double dUi[NF], dUv[NF];
-#pragma unroll
-        for (int f = 0; f < NF; ++f) { dUi[f] = 0.0; dUv[f] = 0.0; }
-#pragma unroll
-        for (int dir = 0; dir < DIM; ++dir) {
-            const int pos = c[dir];
-            const int ln = line_index<DIM, NP>(dir, c);
-            const int pbase = dir * NLINE * PPL + ln * PPL;
-#pragma unroll
-            for (int l = 0; l < NP; ++l) {
-                if (l == pos) continue;
-                const double dh = sDh2[pos * NP + l];
-                int pidx;
-                bool zero = false;
-                if (NS && DIM == 3 && dir == 2 && l < pos && P.quirks == 0) {
-                    // Q2 (DGSEMIntegrator.cpp:702): H(id2)(:,k) = g, the last
-                    // eta-pair flux of node (i,j,l): pair (j, Np-1) on the eta
-                    // line through (i, ., l); zero when j == Np-1.
-                    if (c[1] == NP - 1) zero = true;
-                    pidx = 1 * NLINE * PPL + (l * NP + c[0]) * PPL + pair_index<NP>(c[1], NP - 1);
-                } else {
-                    pidx = pbase + (l < pos ? pair_index<NP>(l, pos) : pair_index<NP>(pos, l));
-                }
-                if (!zero) {
-#pragma unroll
-                    for (int f = 0; f < NF; ++f) dUi[f] += dh * sS[f * NPAIR + pidx];
+                    for (int l = 0; l < NP; ++l) s += sVinv[c[d] * NP + l] * in[base + l * stride];
+                    out[n] = s;
                 }
             }
-            if constexpr (NS) {
-                int base, stride;
-                line_base<DIM, NP>(dir, ln, base, stride);
+            __syncwarp();
+        }
+        double e0 = 0, e1 = 0, e2 = 0;
+#pragma unroll
+        for (int k = 0; k < NPL; ++k) {
+            const int n = li + k * GS;
+            if (n < ND) {
+                int c[3];
+                node_coords<NP>(n, c);
+                const double md = ((DIM & 1) ? b1 : b0)[n];
+                int mx = c[0];
+#pragma unroll
+                for (int d = 1; d < DIM; ++d) mx = max(mx, c[d]);
+                e0 += md * md;
+                if (mx <= NP - 2) e1 += md * md;
+                if (mx <= NP - 3) e2 += md * md;
+            }
+        }
+        for (int o = GS / 2; o > 0; o >>= 1) {
+            e0 += __shfl_xor_sync(0xffffffffu, e0, o);
+            e1 += __shfl_xor_sync(0xffffffffu, e1, o);
+            e2 += __shfl_xor_sync(0xffffffffu, e2, o);
+        }
+        double eta = 1.0 - e1 / e0;
+        eta = fmax(eta, 1.0 - e2 / e1);
+        const double thr = P.modal_threshold;
+        alpha = 1.0 / (1.0 + exp(-9.21024 * (eta - thr) / thr));
+        if (alpha < P.alpha_min) alpha = 0.0;
+        else if (alpha > 1.0 - P.alpha_min) alpha = 1.0;
+        alpha = fmin(alpha, P.alpha_max);
+        if (li == 0 && a.alpha && active) a.alpha[e] = alpha;
+        __syncwarp();
+    }
+
+    // ---- NS: contravariant viscous flux of every own node (flux_mat = adj * Fv^T, :632)
+    if constexpr (NS) {
+#pragma unroll
+        for (int k = 0; k < NPL; ++k) {
+            const int n = li + k * GS;
+            if (n < ND) {
+                double dq[DIM][NF];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d)
+#pragma unroll
+                    for (int f = 0; f < NF; ++f)
+                        dq[d][f] = __ldg(a.grad + (d * NF + f) * Ndof + (long long)e * ND + n);
+                // Q1 (DGSEMIntegrator.cpp:620): the reference evaluates the volume
+                // viscous flux with the state of node Np^d-1 (stale member id1).
+                const int src = (P.quirks == 0) ? ND - 1 : n;
+                const Prim<DIM, double> q = load_prim<DIM, ND>(sH, src);
+                double Vc[DIM][NF];
+#pragma unroll
+                for (int r = 0; r < DIM; ++r)
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) Vc[r][f] = 0.0;
+                viscous_flux<DIM, double>(q.rho, q.rrho, q.v, 0.5 * q.rbeta * q.rho, dq, P,
+                                          [&](int f, int cc, double val) {
+#pragma unroll
+                                              for (int r = 0; r < DIM; ++r) Vc[r][f] += adj[r][cc] * val;
+                                          });
+#pragma unroll
+                for (int r = 0; r < DIM; ++r)
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) sV[(r * NF + f) * ND + n] = Vc[r][f];
+            }
+        }
+        __syncwarp();
+    }
+
+    // ---- flux differencing, one direction at a time:
+    //      sum_l Dhat2(i,l) F#(i,l) (F#(i,i) = 0) and, for NS, sum_l Dhat(i,l) Fv_l
+    double dUi[NPL][NF], dUv[NPL][NF];
+#pragma unroll
+    for (int k = 0; k < NPL; ++k)
+#pragma unroll
+        for (int f = 0; f < NF; ++f) { dUi[k][f] = 0.0; dUv[k][f] = 0.0; }
+#pragma unroll
+    for (int dir = 0; dir < DIM; ++dir) {
+        double mt[DIM];
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) mt[q] = adj[dir][q];
+        for (int p = li; p < NPD; p += GS) {
+            const int ln = p / PPL, pp = p - ln * PPL;
+            int pa, pb, base, stride;
+            pair_decode<NP>(pp, pa, pb);
+            line_base<DIM, NP>(dir, ln, base, stride);
+            double F[NF];
+            volume_flux<DIM, double>(load_prim<DIM, ND>(sH, base + pa * stride),
+                                     load_prim<DIM, ND>(sH, base + pb * stride), mt, gm1i, F);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) sF[f * NPD + p] = F[f];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < NPL; ++k) {
+            const int n = li + k * GS;
+            if (n < ND) {
+                int c[3];
+                node_coords<NP>(n, c);
+                const int pos = c[dir];
+                const int ln = line_index<DIM, NP>(dir, c);
 #pragma unroll
                 for (int l = 0; l < NP; ++l) {
-                    const double dh = sDh[pos * NP + l];
+                    if (l == pos) continue;
+                    const double dh = sDh2[pos * NP + l];
+                    if (NS && DIM == 3 && dir == 2 && l < pos && P.quirks == 0) {
+                        // Q2 (DGSEMIntegrator.cpp:702): H(id2)(:,k) = g, the last
+                        // eta-pair flux of node (i,j,l): the pair (j, Np-1) on the
+                        // eta line through (i, ., l); zero when j == Np-1.
+                        if (c[1] != NP - 1) {
+                            double F[NF], mg[DIM];
 #pragma unroll
-                    for (int f = 0; f < NF; ++f) dUv[f] += sV[(dir * NF + f) * ND + base + l * stride] * dh;
+                            for (int q = 0; q < DIM; ++q) mg[q] = adj[1][q];
+                            volume_flux<DIM, double>(load_prim<DIM, ND>(sH, (l * NP + c[1]) * NP + c[0]),
+                                                     load_prim<DIM, ND>(sH, (l * NP + NP - 1) * NP + c[0]), mg,
+                                                     gm1i, F);
+#pragma unroll
+                            for (int f = 0; f < NF; ++f) dUi[k][f] += dh * F[f];
+                        }
+                    } else {
+                        const int pidx = ln * PPL + (l < pos ? pair_index<NP>(l, pos) : pair_index<NP>(pos, l));
+#pragma unroll
+                        for (int f = 0; f < NF; ++f) dUi[k][f] += dh * sF[f * NPD + pidx];
+                    }
+                }
+                if constexpr (NS) {
+                    int base, stride;
+                    line_base<DIM, NP>(dir, ln, base, stride);
+#pragma unroll
+                    for (int l = 0; l < NP; ++l) {
+                        const double dh = sDh[pos * NP + l];
+#pragma unroll
+                        for (int f = 0; f < NF; ++f) dUv[k][f] += sV[(dir * NF + f) * ND + base + l * stride] * dh;
+                    }
                 }
             }
         }
-        const double mJ = 1.0 / J;
-        const double oma = 1.0 - alpha;
+        __syncwarp();
+    }
+    double acc[NPL][NF];
+#pragma unroll
+    for (int k = 0; k < NPL; ++k)
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-            double v = -dUi[f];
-            if (P.blending) v *= oma;
-            if (NS) v += dUv[f];
-            acc[f] = v * mJ;
+            double v = -dUi[k][f];
+            if (P.blending) v *= (1.0 - alpha);
+            if (NS) v += dUv[k][f];
+            acc[k][f] = v * mJ;
         }
-    }
-    __syncthreads();
 
     // ---- subcell first-order FV (DGSEMIntegrator.cpp:972-1196), skipped when alpha == 0
-    if (P.blending) {
-        if (alpha != 0.0) {
-            for (int it = n; it < NIF; it += ND) {
-                const int dir = it / (NLINE * (NP - 1));
-                const int r = it - dir * NLINE * (NP - 1);
-                const int ln = r / (NP - 1), ii = r - ln * (NP - 1);
+    if (P.blending && alpha != 0.0) {
+        double fv[NPL][NF];
+#pragma unroll
+        for (int dir = 0; dir < DIM; ++dir) {
+            double nor[DIM];
+#pragma unroll
+            for (int q = 0; q < DIM; ++q) nor[q] = adj[dir][q];
+            for (int it = li; it < NID; it += GS) {
+                const int ln = it / (NP - 1), ii = it - ln * (NP - 1);
                 int base, stride;
                 line_base<DIM, NP>(dir, ln, base, stride);
                 const int n1 = base + ii * stride, n2 = n1 + stride;
-                double s1[NF], s2[NF], F[NF], nor[DIM];
+                const Prim<DIM, double> q1 = load_prim<DIM, ND>(sH, n1), q2 = load_prim<DIM, ND>(sH, n2);
+                double s1[NF], s2[NF], F[NF];
 #pragma unroll
-                for (int f = 0; f < NF; ++f) { s1[f] = sU[f * ND + n1]; s2[f] = sU[f * ND + n2]; }
+                for (int d = 0; d < DIM; ++d) { s1[1 + d] = q1.rho * q1.v[d]; s2[1 + d] = q2.rho * q2.v[d]; }
+                face_flux<DIM, double>(s1, q1, s2, q2, nor, gm1i, P.quirks == 0, true, F);
 #pragma unroll
-                for (int q = 0; q < DIM; ++q) nor[q] = (dir == 0) ? adj[0][q] : (dir == 1 ? adj[1][q] : adj[DIM - 1][q]);
-                face_flux<DIM, double>(s1, load_prim<DIM, ND>(sH, n1), s2, load_prim<DIM, ND>(sH, n2), nor, gm1i,
-                                       P.quirks == 0, true, F);
-#pragma unroll
-                for (int f = 0; f < NF; ++f) sS[f * NIF + it] = F[f];
+                for (int f = 0; f < NF; ++f) sF[f * NID + it] = F[f];
             }
-        }
-        __syncthreads();
-        if (alpha != 0.0) {
-            double fv[NF];
+            __syncwarp();
 #pragma unroll
-            for (int dir = 0; dir < DIM; ++dir) {
-                const int pos = c[dir];
-                const int ln = line_index<DIM, NP>(dir, c);
-                const int ib = dir * NLINE * (NP - 1) + ln * (NP - 1);
-                const double mw = 1.0 / (J * sW[pos]);
+            for (int k = 0; k < NPL; ++k) {
+                const int n = li + k * GS;
+                if (n < ND) {
+                    int c[3];
+                    node_coords<NP>(n, c);
+                    const int pos = c[dir];
+                    const int ib = line_index<DIM, NP>(dir, c) * (NP - 1);
+                    const double mw = 1.0 / (J * sW[pos]);
 #pragma unroll
-                for (int f = 0; f < NF; ++f) {
-                    double v;
-                    if (pos == 0) v = -sS[f * NIF + ib];
-                    else if (pos == NP - 1) v = sS[f * NIF + ib + pos - 1];
-                    else v = sS[f * NIF + ib + pos - 1] - sS[f * NIF + ib + pos];
-                    v *= mw;
-                    fv[f] = (dir == 0) ? v : fv[f] + v;
+                    for (int f = 0; f < NF; ++f) {
+                        double v;
+                        if (pos == 0) v = -sF[f * NID + ib];
+                        else if (pos == NP - 1) v = sF[f * NID + ib + pos - 1];
+                        else v = sF[f * NID + ib + pos - 1] - sF[f * NID + ib + pos];
+                        v *= mw;
+                        fv[k][f] = (dir == 0) ? v : fv[k][f] + v;
+                    }
                 }
             }
-#pragma unroll
-            for (int f = 0; f < NF; ++f) acc[f] = fv[f] * alpha + acc[f];
+            __syncwarp();
         }
-        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < NPL; ++k)
+#pragma unroll
+            for (int f = 0; f < NF; ++f) acc[k][f] = fv[k][f] * alpha + acc[k][f];
     }
 
-    // ---- surface fluxes of the element's own faces
+    // ---- surface fluxes of the element's own faces; neighbour traces from global/L2
     const double aw = 1.0 / (sW[0] * J);
-    for (int it = n; it < NFI; it += ND) {
+    for (int it = li; it < NFI; it += GS) {
         const int lf = it / NFN, fa = it - lf * NFN;
         const int no = face_node<DIM, NP>(lf, fa);
         const int4 t = __ldg(m.nbr + (long long)e * (2 * DIM) + lf);
-        const int nn = face_node<DIM, NP>(t.y, fa);
-        const long long gn = (long long)t.x * ND + nn;
+        const long long gn = (long long)t.x * ND + face_node<DIM, NP>(t.y, fa);
+        const long long go = (long long)e * ND + no;
         const bool own_is_1 = (t.w == 0);
-        double so[NF], sn[NF], nor[DIM], flux[NF], d1[NF];
+        double so[NF], sn[NF], nor[DIM], flux[NF], fn[NF];
 #pragma unroll
-        for (int f = 0; f < NF; ++f) { so[f] = sU[f * ND + no]; sn[f] = __ldg(a.u + f * Ndof + gn); }
+        for (int f = 0; f < NF; ++f) { so[f] = __ldg(a.u + f * Ndof + go); sn[f] = __ldg(a.u + f * Ndof + gn); }
 #pragma unroll
         for (int q = 0; q < DIM; ++q) nor[q] = __ldg(m.fnor + (long long)t.z * DIM + q);
         Prim<DIM, double> po = load_prim<DIM, ND>(sH, no);
         Prim<DIM, double> pn = primitives<DIM, double>(sn, gamma, gm1);
-        double fn[NF];
 #pragma unroll
         for (int f = 0; f < NF; ++f) fn[f] = 0.0;
         if constexpr (NS) {
             // DGSEMIntegrator.cpp:435-549: 0.5 (Fv1 + Fv2) . n from each trace's
             // own state and lifted gradients
-            const long long go = (long long)e * ND + no;
 #pragma unroll
             for (int side = 0; side < 2; ++side) {
                 const long long g = side == 0 ? go : gn;
@@ -473,61 +542,70 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
         else
             face_flux<DIM, double>(sn, pn, so, po, nor, gm1i, P.quirks == 0, P.dissipation != 0, flux);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) d1[f] = own_is_1 ? (-flux[f] + fn[f]) : (flux[f] - fn[f]);
-#pragma unroll
-        for (int f = 0; f < NF; ++f) sS[f * NFI + it] = aw * d1[f];
+        for (int f = 0; f < NF; ++f) sF[f * NFI + it] = aw * (own_is_1 ? (fn[f] - flux[f]) : (flux[f] - fn[f]));
     }
-    __syncthreads();
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-        int lf = -1;
-        if (c[d] == 0) lf = 2 * d;
-        else if (c[d] == NP - 1) lf = 2 * d + 1;
-        if (lf >= 0) {
-            const int it = lf * NFN + face_tangential<DIM, NP>(d, c);
-#pragma unroll
-            for (int f = 0; f < NF; ++f) acc[f] += sS[f * NFI + it];
-        }
-    }
+    __syncwarp();
 
-    // ---- epilogue
+    // ---- gather face terms, epilogue
     if (!active) return;
-    switch (a.mode) {
-    case EPI_STORE:
 #pragma unroll
-        for (int f = 0; f < NF; ++f) a.dudt[f * Ndof + gnode] = acc[f];
-        break;
-    case EPI_LSRK:
+    for (int k = 0; k < NPL; ++k) {
+        const int n = li + k * GS;
+        if (n >= ND) continue;
+        int c[3];
+        node_coords<NP>(n, c);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            const long long g = f * Ndof + gnode;
-            const double dv = (a.rkA == 0.0) ? a.dt * acc[f] : a.rkA * a.du[g] + a.dt * acc[f];
-            a.du[g] = dv;
-            a.u_out[g] = st[f] + a.rkB * dv;
+        for (int d = 0; d < DIM; ++d) {
+            int lf = -1;
+            if (c[d] == 0) lf = 2 * d;
+            else if (c[d] == NP - 1) lf = 2 * d + 1;
+            if (lf >= 0) {
+                const int it = lf * NFN + face_tangential<DIM, NP>(d, c);
+#pragma unroll
+                for (int f = 0; f < NF; ++f) acc[k][f] += sF[f * NFI + it];
+            }
         }
-        break;
-    case EPI_SSP1:
+        const long long gnode = (long long)e * ND + n;
+        switch (a.mode) {
+        case EPI_STORE:
 #pragma unroll
-        for (int f = 0; f < NF; ++f) a.u_out[f * Ndof + gnode] = st[f] + a.dt * acc[f];
-        break;
-    case EPI_SSP2:
+            for (int f = 0; f < NF; ++f) a.dudt[f * Ndof + gnode] = acc[k][f];
+            break;
+        case EPI_LSRK:
 #pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            const long long g = f * Ndof + gnode;
-            const double y = st[f] + a.dt * acc[f];
-            a.u_out[g] = 3. / 4 * a.x0[g] + 1. / 4 * y;
+            for (int f = 0; f < NF; ++f) {
+                const long long g = f * Ndof + gnode;
+                const double dv = (a.rkA == 0.0) ? a.dt * acc[k][f] : a.rkA * a.du[g] + a.dt * acc[k][f];
+                a.du[g] = dv;
+                a.u_out[g] = __ldg(a.u + g) + a.rkB * dv;
+            }
+            break;
+        case EPI_SSP1:
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                const long long g = f * Ndof + gnode;
+                a.u_out[g] = __ldg(a.u + g) + a.dt * acc[k][f];
+            }
+            break;
+        case EPI_SSP2:
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                const long long g = f * Ndof + gnode;
+                const double y = __ldg(a.u + g) + a.dt * acc[k][f];
+                a.u_out[g] = 3. / 4 * a.x0[g] + 1. / 4 * y;
+            }
+            break;
+        case EPI_SSP3:
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                const long long g = f * Ndof + gnode;
+                const double y = __ldg(a.u + g) + a.dt * acc[k][f];
+                a.u_out[g] = 1. / 3 * a.x0[g] + 2. / 3 * y;
+            }
+            break;
+        default:
+            break;
         }
-        break;
-    case EPI_SSP3:
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            const long long g = f * Ndof + gnode;
-            const double y = st[f] + a.dt * acc[f];
-            a.u_out[g] = 1. / 3 * a.x0[g] + 2. / 3 * y;
-        }
-        break;
-    default:
-        break;
     }
 }
 
@@ -577,8 +655,8 @@ lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_
 
     // face part first (its neighbour loads overlap the element part):
     // +1/(w0 J) * 1/2 (v_elem2 - v_elem1) * n_c on both sides
+    __syncthreads();   // tables and entropy variables complete
     const double aw = 1.0 / (sW[0] * J);
-    __syncthreads();
     for (int it = n; it < NFI; it += ND) {
         const int lf = it / NFN, fa = it - lf * NFN;
         const int no = face_node<DIM, NP>(lf, fa);
@@ -655,8 +733,8 @@ lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_
 
 template <int DIM, int NP, bool NS>
 size_t rhs_smem() {
-    using S = Shape<DIM, NP>;
-    return sizeof(double) * (S::TAB + (size_t)S::EPB * RhsLayout<DIM, NP, NS>::PER_ELEM);
+    using LY = RhsLayout<DIM, NP, NS>;
+    return sizeof(double) * (Shape<DIM, NP>::TAB + (size_t)LY::EPB * LY::PER_ELEM);
 }
 template <int DIM, int NP>
 size_t lift_smem() {
@@ -665,25 +743,22 @@ size_t lift_smem() {
     return sizeof(double) * (S::TAB + (size_t)S::EPB * PER_ELEM);
 }
 
+template <int DIM, int NP, bool NS>
+cudaError_t rhs_launch_ns(const MeshDev &m, const RhsArgs &a, const PhysParams &P, const OpTables &T,
+                          cudaStream_t s) {
+    using LY = RhsLayout<DIM, NP, NS>;
+    const int grid = (m.E + LY::EPB - 1) / LY::EPB;
+    const size_t sm = rhs_smem<DIM, NP, NS>();
+    cudaError_t err = cudaFuncSetAttribute(rhs_kernel<DIM, NP, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)sm);
+    if (err != cudaSuccess) return err;
+    rhs_kernel<DIM, NP, NS><<<grid, LY::THREADS, sm, s>>>(m, a, P, T);
+    return cudaGetLastError();
+}
 template <int DIM, int NP>
 cudaError_t rhs_launch_t(bool ns, const MeshDev &m, const RhsArgs &a, const PhysParams &P,
                          const OpTables &T, cudaStream_t s) {
-    using S = Shape<DIM, NP>;
-    const int grid = (m.E + S::EPB - 1) / S::EPB;
-    if (ns) {
-        const size_t sm = rhs_smem<DIM, NP, true>();
-        cudaError_t err = cudaFuncSetAttribute(rhs_kernel<DIM, NP, true>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (err != cudaSuccess) return err;
-        rhs_kernel<DIM, NP, true><<<grid, S::THREADS, sm, s>>>(m, a, P, T);
-    } else {
-        const size_t sm = rhs_smem<DIM, NP, false>();
-        cudaError_t err = cudaFuncSetAttribute(rhs_kernel<DIM, NP, false>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (err != cudaSuccess) return err;
-        rhs_kernel<DIM, NP, false><<<grid, S::THREADS, sm, s>>>(m, a, P, T);
-    }
-    return cudaGetLastError();
+    return ns ? rhs_launch_ns<DIM, NP, true>(m, a, P, T, s) : rhs_launch_ns<DIM, NP, false>(m, a, P, T, s);
 }
 template <int DIM, int NP>
 cudaError_t lift_launch_t(const MeshDev &m, const LiftArgs &a, const PhysParams &P,
