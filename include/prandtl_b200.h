@@ -82,7 +82,10 @@ typedef struct prandtl_config {
                                   known defects; 1: defects fixed (entropy-conservative 3D NS) */
     int surface_dissipation;   /* 1: reference surface flux; 0: entropy-conservative surface
                                   flux (verification switch, no reference counterpart) */
-    int precision;             /* 0: FP64 throughout (the only value accepted by this build) */
+    int precision;             /* 0: FP64 throughout.  1: FP32 bulk -- two-point fluxes, flux
+                                  differencing, surface fluxes and stored gradients in FP32;
+                                  per-node primitives, entropy variables, lambda_max and the RK
+                                  state and registers in FP64 (no reference counterpart) */
     double timeout_s;          /* bound on every host-side wait; 0 selects 120 s */
 } prandtl_config;
 

@@ -93,18 +93,18 @@ __device__ __forceinline__ int face_tangential(int d, const int c[3]) {
     return c[t0] + NP * c[t1];
 }
 
-template <int NP>
-__device__ __forceinline__ void load_tables(const OpTables &T, double *sT, int tid, int nthreads) {
+template <int NP, typename Real>
+__device__ __forceinline__ void load_tables(const OpTables &T, Real *sT, int tid, int nthreads) {
     for (int q = tid; q < NP * NP; q += nthreads) {
         const int i = q / NP, l = q % NP;
-        sT[q] = T.D[i * NP + l];
-        sT[NP * NP + q] = T.Dhat[i * NP + l];
-        sT[2 * NP * NP + q] = T.Dhat2[i * NP + l];
-        sT[3 * NP * NP + q] = T.Vinv[i * NP + l];
+        sT[q] = Real(T.D[i * NP + l]);
+        sT[NP * NP + q] = Real(T.Dhat[i * NP + l]);
+        sT[2 * NP * NP + q] = Real(T.Dhat2[i * NP + l]);
+        sT[3 * NP * NP + q] = Real(T.Vinv[i * NP + l]);
     }
     for (int q = tid; q < NP; q += nthreads) {
-        sT[4 * NP * NP + q] = T.w[q];
-        sT[4 * NP * NP + NP + q] = T.x[q];
+        sT[4 * NP * NP + q] = Real(T.w[q]);
+        sT[4 * NP * NP + NP + q] = Real(T.x[q]);
     }
 }
 
@@ -135,10 +135,10 @@ struct HIdx {
     static constexpr int RHO = 0, RRHO = 1, V = 2, VSQ = 2 + DIM, BETA = 3 + DIM, RBETA = 4 + DIM,
                          LAM = 5 + DIM, K = 6 + DIM;
 };
-template <int DIM, int ND>
-__device__ __forceinline__ Prim<DIM, double> load_prim(const double *sH, int n) {
+template <int DIM, int ND, typename Real>
+__device__ __forceinline__ Prim<DIM, Real> load_prim(const Real *sH, int n) {
     using I = HIdx<DIM>;
-    Prim<DIM, double> q;
+    Prim<DIM, Real> q;
     q.rho = sH[I::RHO * ND + n];
     q.rrho = sH[I::RRHO * ND + n];
 #pragma unroll
@@ -149,17 +149,31 @@ __device__ __forceinline__ Prim<DIM, double> load_prim(const double *sH, int n) 
     q.lam = sH[I::LAM * ND + n];
     return q;
 }
-template <int DIM, int ND>
-__device__ __forceinline__ void store_prim(double *sH, int n, const Prim<DIM, double> &q) {
+template <int DIM, int ND, typename Real>
+__device__ __forceinline__ void store_prim(Real *sH, int n, const Prim<DIM, double> &q) {
     using I = HIdx<DIM>;
-    sH[I::RHO * ND + n] = q.rho;
-    sH[I::RRHO * ND + n] = q.rrho;
+    sH[I::RHO * ND + n] = Real(q.rho);
+    sH[I::RRHO * ND + n] = Real(q.rrho);
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) sH[(I::V + d) * ND + n] = q.v[d];
-    sH[I::VSQ * ND + n] = q.vsq;
-    sH[I::BETA * ND + n] = q.beta;
-    sH[I::RBETA * ND + n] = q.rbeta;
-    sH[I::LAM * ND + n] = q.lam;
+    for (int d = 0; d < DIM; ++d) sH[(I::V + d) * ND + n] = Real(q.v[d]);
+    sH[I::VSQ * ND + n] = Real(q.vsq);
+    sH[I::BETA * ND + n] = Real(q.beta);
+    sH[I::RBETA * ND + n] = Real(q.rbeta);
+    sH[I::LAM * ND + n] = Real(q.lam);
+}
+// Working-precision copy of primitives computed in FP64.
+template <int DIM, typename Real>
+__device__ __forceinline__ Prim<DIM, Real> cast_prim(const Prim<DIM, double> &q) {
+    Prim<DIM, Real> r;
+    r.rho = Real(q.rho);
+    r.rrho = Real(q.rrho);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) r.v[d] = Real(q.v[d]);
+    r.vsq = Real(q.vsq);
+    r.beta = Real(q.beta);
+    r.rbeta = Real(q.rbeta);
+    r.lam = Real(q.lam);
+    return r;
 }
 
 constexpr int next_pow2(int v) { return v <= 1 ? 1 : 2 * next_pow2((v + 1) / 2); }
@@ -178,45 +192,63 @@ constexpr int next_pow2(int v) { return v <= 1 ? 1 : 2 * next_pow2((v + 1) / 2);
 #ifndef PRANDTL_EULER_MINB
 #define PRANDTL_EULER_MINB 5
 #endif
+#ifndef PRANDTL_NS32_MINB
+#define PRANDTL_NS32_MINB 4
+#endif
+#ifndef PRANDTL_EULER32_MINB
+#define PRANDTL_EULER32_MINB 6
+#endif
 
 // Warp-per-element layout of the RHS kernel: one group of GS lanes owns one
 // element (GS = 32, or the next power of two >= Np^d for small elements, so
 // a warp then holds several elements); lane `li` of a group owns the nodes
 // li, li+GS, ... and the pair / face / subcell items of the same stride.
 // Groups synchronise with __syncwarp only.
-template <int DIM, int NP, bool NS>
+template <int DIM, int NP, bool NS, typename Real>
 struct RhsLayout {
     using S = Shape<DIM, NP>;
     static constexpr int ND = S::ND, NF = S::NF, NLINE = S::NLINE, PPL = S::PPL;
     static constexpr int GS = ND >= 32 ? 32 : next_pow2(ND);
     static constexpr int EPW = 32 / GS;                 // elements per warp
     static constexpr int NPL = (ND + GS - 1) / GS;      // nodes per lane
-    static constexpr int WARPS = NS ? PRANDTL_NS_WARPS : PRANDTL_EULER_WARPS;
-    static constexpr int EPB = WARPS * EPW;             // elements per CTA
-    static constexpr int THREADS = WARPS * 32;
     static constexpr int NPD = NLINE * PPL;             // pairs per direction
     static constexpr int NID = NLINE * (NP - 1);        // subcell interfaces per direction
     static constexpr int BUF = cmax(cmax(NPD, S::NFI), cmax(NID, (5 * ND + NF - 1) / NF)) * NF;
     static constexpr int K = HIdx<DIM>::K;
     static constexpr int PER_ELEM = K * ND + BUF + (NS ? DIM * NF * ND : 0);
-    static constexpr int MIN_BLOCKS = NS ? PRANDTL_NS_MINB : PRANDTL_EULER_MINB;
+    // warps per CTA: the configured count, reduced so the CTA's elements fit the
+    // 227 KB shared-memory limit
+    static constexpr int SMEM_MAX = 227 * 1024;
+    static constexpr int FIT = (SMEM_MAX / (int)sizeof(Real) - S::TAB) / (PER_ELEM * EPW);
+    static constexpr int WARPS_CFG = NS ? PRANDTL_NS_WARPS : PRANDTL_EULER_WARPS;
+    static constexpr int WARPS = cmax(1, FIT < WARPS_CFG ? FIT : WARPS_CFG);
+    static constexpr int EPB = WARPS * EPW;             // elements per CTA
+    static constexpr int THREADS = WARPS * 32;
+    static constexpr bool F64 = sizeof(Real) == 8;
+    static constexpr int MIN_BLOCKS = NS ? (F64 ? PRANDTL_NS_MINB : PRANDTL_NS32_MINB)
+                                         : (F64 ? PRANDTL_EULER_MINB : PRANDTL_EULER32_MINB);
 };
 
 // ------------------------------------------------------------------- RHS
-template <int DIM, int NP, bool NS>
-__global__ void __launch_bounds__(RhsLayout<DIM, NP, NS>::THREADS, (RhsLayout<DIM, NP, NS>::MIN_BLOCKS))
+// Real is the working precision of the O(Np^{d+1}) work (two-point fluxes,
+// flux differencing, surface fluxes, gradients): double for the plain FP64
+// path, float for the FP32-bulk form.  Per-node primitives are always formed
+// in FP64 from the FP64 state, and the RK stage update is FP64.
+template <int DIM, int NP, bool NS, typename Real>
+__global__ void __launch_bounds__(RhsLayout<DIM, NP, NS, Real>::THREADS, (RhsLayout<DIM, NP, NS, Real>::MIN_BLOCKS))
 rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_constant__ OpTables T) {
     using S = Shape<DIM, NP>;
-    using LY = RhsLayout<DIM, NP, NS>;
+    using LY = RhsLayout<DIM, NP, NS, Real>;
     constexpr int ND = S::ND, NF = S::NF, PPL = S::PPL;
     constexpr int NFN = S::NFN, NFI = S::NFI, GS = LY::GS, NPL = LY::NPL;
     constexpr int NPD = LY::NPD, NID = LY::NID;
 
-    extern __shared__ double smem[];
-    double *sT = smem;
-    const double *sDh = sT + NP * NP, *sDh2 = sT + 2 * NP * NP, *sVinv = sT + 3 * NP * NP;
-    const double *sW = sT + 4 * NP * NP;
-    load_tables<NP>(T, sT, threadIdx.x, LY::THREADS);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Real *smem = reinterpret_cast<Real *>(smem_raw);
+    Real *sT = smem;
+    const Real *sDh = sT + NP * NP, *sDh2 = sT + 2 * NP * NP, *sVinv = sT + 3 * NP * NP;
+    const Real *sW = sT + 4 * NP * NP;
+    load_tables<NP, Real>(T, sT, threadIdx.x, LY::THREADS);
     __syncthreads();
 
     const int lane = threadIdx.x & 31;
@@ -225,24 +257,25 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
     const int e_raw = blockIdx.x * LY::EPB + grp;
     const bool active = e_raw < m.E;
     const int e = active ? e_raw : m.E - 1;
-    double *sH = smem + S::TAB + grp * LY::PER_ELEM;   // hoisted primitives [K][ND]
-    double *sF = sH + LY::K * ND;                       // pairs / subcell / face items / modes
-    double *sV = sF + LY::BUF;                          // NS: contravariant viscous fluxes [DIM][NF][ND]
-    const unsigned gmask = (GS == 32) ? 0xffffffffu : (((1u << GS) - 1u) << (lane & ~(GS - 1)));
-    (void)gmask;
+    Real *sH = smem + S::TAB + grp * LY::PER_ELEM;   // hoisted primitives [K][ND]
+    Real *sF = sH + LY::K * ND;                       // pairs / subcell / face items / modes
+    Real *sV = sF + LY::BUF;                          // NS: contravariant viscous fluxes [DIM][NF][ND]
+    const Real *grad = nullptr;
+    if constexpr (NS) grad = LY::F64 ? reinterpret_cast<const Real *>(a.grad) : reinterpret_cast<const Real *>(a.grad32);
 
     const long long Ndof = m.Ndof;
-    const double gamma = P.gamma, gm1 = P.gammaM1, gm1i = P.gammaM1Inverse;
+    const double gamma = P.gamma, gm1 = P.gammaM1;
+    const Real gm1i = Real(P.gammaM1Inverse);
     const double *geo = m.geo + (long long)e * (DIM * DIM + 1);
-    double adj[DIM][DIM];
+    Real adj[DIM][DIM];
 #pragma unroll
     for (int r = 0; r < DIM; ++r)
 #pragma unroll
-        for (int c2 = 0; c2 < DIM; ++c2) adj[r][c2] = __ldg(geo + r * DIM + c2);
+        for (int c2 = 0; c2 < DIM; ++c2) adj[r][c2] = Real(__ldg(geo + r * DIM + c2));
     const double J = __ldg(geo + DIM * DIM);
-    const double mJ = 1.0 / J;
+    const Real mJ = Real(1.0 / J);
 
-    // ---- own nodes: hoisted primitives; largest |V|+c
+    // ---- own nodes: hoisted primitives (formed in FP64); largest |V|+c
     double lam = 0.0;
 #pragma unroll
     for (int k = 0; k < NPL; ++k) {
@@ -252,7 +285,7 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
 #pragma unroll
             for (int f = 0; f < NF; ++f) st[f] = __ldg(a.u + f * Ndof + (long long)e * ND + n);
             const Prim<DIM, double> q = primitives<DIM, double>(st, gamma, gm1);
-            store_prim<DIM, ND>(sH, n, q);
+            store_prim<DIM, ND, Real>(sH, n, q);
             lam = fmax(lam, q.lam);
         }
     }
@@ -264,23 +297,23 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
     __syncwarp();
 
     // ---- blending coefficient (PerssonPeraireIndicator.cpp:21-58, DGSEMOperator.cpp:60-80)
-    double alpha = 0.0;
+    Real alpha = 0;
     if (P.blending) {
-        double *b0 = sF, *b1 = sF + ND;
+        Real *b0 = sF, *b1 = sF + ND;
 #pragma unroll
         for (int k = 0; k < NPL; ++k) {
             const int n = li + k * GS;
             if (n < ND) {
                 // rho * ComputePressure(state) with v = m * (1/rho)
-                const Prim<DIM, double> q = load_prim<DIM, ND>(sH, n);
-                b0[n] = q.rho * (0.5 * q.rbeta * q.rho);
+                const Prim<DIM, Real> q = load_prim<DIM, ND, Real>(sH, n);
+                b0[n] = q.rho * (Real(0.5) * q.rbeta * q.rho);
             }
         }
         __syncwarp();
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {   // modes = V^-1 (rho p), one direction per pass
-            const double *in = (d & 1) ? b1 : b0;
-            double *out = (d & 1) ? b0 : b1;
+            const Real *in = (d & 1) ? b1 : b0;
+            Real *out = (d & 1) ? b0 : b1;
 #pragma unroll
             for (int k = 0; k < NPL; ++k) {
                 const int n = li + k * GS;
@@ -289,7 +322,7 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
                     node_coords<NP>(n, c);
                     int base, stride;
                     line_base<DIM, NP>(d, line_index<DIM, NP>(d, c), base, stride);
-                    double s = 0.0;
+                    Real s = 0;
 #pragma unroll
                     for (int l = 0; l < NP; ++l) s += sVinv[c[d] * NP + l] * in[base + l * stride];
                     out[n] = s;
@@ -304,7 +337,7 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
             if (n < ND) {
                 int c[3];
                 node_coords<NP>(n, c);
-                const double md = ((DIM & 1) ? b1 : b0)[n];
+                const double md = double(((DIM & 1) ? b1 : b0)[n]);
                 int mx = c[0];
 #pragma unroll
                 for (int d = 1; d < DIM; ++d) mx = max(mx, c[d]);
@@ -321,11 +354,12 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
         double eta = 1.0 - e1 / e0;
         eta = fmax(eta, 1.0 - e2 / e1);
         const double thr = P.modal_threshold;
-        alpha = 1.0 / (1.0 + exp(-9.21024 * (eta - thr) / thr));
-        if (alpha < P.alpha_min) alpha = 0.0;
-        else if (alpha > 1.0 - P.alpha_min) alpha = 1.0;
-        alpha = fmin(alpha, P.alpha_max);
-        if (li == 0 && a.alpha && active) a.alpha[e] = alpha;
+        double al = 1.0 / (1.0 + exp(-9.21024 * (eta - thr) / thr));
+        if (al < P.alpha_min) al = 0.0;
+        else if (al > 1.0 - P.alpha_min) al = 1.0;
+        al = fmin(al, P.alpha_max);
+        alpha = Real(al);
+        if (li == 0 && a.alpha && active) a.alpha[e] = al;
         __syncwarp();
     }
 
@@ -335,26 +369,26 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
         for (int k = 0; k < NPL; ++k) {
             const int n = li + k * GS;
             if (n < ND) {
-                double dq[DIM][NF];
+                Real dq[DIM][NF];
 #pragma unroll
                 for (int d = 0; d < DIM; ++d)
 #pragma unroll
                     for (int f = 0; f < NF; ++f)
-                        dq[d][f] = __ldg(a.grad + (d * NF + f) * Ndof + (long long)e * ND + n);
+                        dq[d][f] = __ldg(grad + (d * NF + f) * Ndof + (long long)e * ND + n);
                 // Q1 (DGSEMIntegrator.cpp:620): the reference evaluates the volume
                 // viscous flux with the state of node Np^d-1 (stale member id1).
                 const int src = (P.quirks == 0) ? ND - 1 : n;
-                const Prim<DIM, double> q = load_prim<DIM, ND>(sH, src);
-                double Vc[DIM][NF];
+                const Prim<DIM, Real> q = load_prim<DIM, ND, Real>(sH, src);
+                Real Vc[DIM][NF];
 #pragma unroll
                 for (int r = 0; r < DIM; ++r)
 #pragma unroll
-                    for (int f = 0; f < NF; ++f) Vc[r][f] = 0.0;
-                viscous_flux<DIM, double>(q.rho, q.rrho, q.v, 0.5 * q.rbeta * q.rho, dq, P,
-                                          [&](int f, int cc, double val) {
+                    for (int f = 0; f < NF; ++f) Vc[r][f] = 0;
+                viscous_flux<DIM, Real>(q.rho, q.rrho, q.v, Real(0.5) * q.rbeta * q.rho, dq, P,
+                                        [&](int f, int cc, Real val) {
 #pragma unroll
-                                              for (int r = 0; r < DIM; ++r) Vc[r][f] += adj[r][cc] * val;
-                                          });
+                                            for (int r = 0; r < DIM; ++r) Vc[r][f] += adj[r][cc] * val;
+                                        });
 #pragma unroll
                 for (int r = 0; r < DIM; ++r)
 #pragma unroll
@@ -366,14 +400,14 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
 
     // ---- flux differencing, one direction at a time:
     //      sum_l Dhat2(i,l) F#(i,l) (F#(i,i) = 0) and, for NS, sum_l Dhat(i,l) Fv_l
-    double dUi[NPL][NF], dUv[NPL][NF];
+    Real dUi[NPL][NF], dUv[NPL][NF];
 #pragma unroll
     for (int k = 0; k < NPL; ++k)
 #pragma unroll
-        for (int f = 0; f < NF; ++f) { dUi[k][f] = 0.0; dUv[k][f] = 0.0; }
+        for (int f = 0; f < NF; ++f) { dUi[k][f] = 0; dUv[k][f] = 0; }
 #pragma unroll
     for (int dir = 0; dir < DIM; ++dir) {
-        double mt[DIM];
+        Real mt[DIM];
 #pragma unroll
         for (int q = 0; q < DIM; ++q) mt[q] = adj[dir][q];
         for (int p = li; p < NPD; p += GS) {
@@ -381,9 +415,9 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
             int pa, pb, base, stride;
             pair_decode<NP>(pp, pa, pb);
             line_base<DIM, NP>(dir, ln, base, stride);
-            double F[NF];
-            volume_flux<DIM, double>(load_prim<DIM, ND>(sH, base + pa * stride),
-                                     load_prim<DIM, ND>(sH, base + pb * stride), mt, gm1i, F);
+            Real F[NF];
+            volume_flux<DIM, Real>(load_prim<DIM, ND, Real>(sH, base + pa * stride),
+                                   load_prim<DIM, ND, Real>(sH, base + pb * stride), mt, gm1i, F);
 #pragma unroll
             for (int f = 0; f < NF; ++f) sF[f * NPD + p] = F[f];
         }
@@ -399,18 +433,18 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
 #pragma unroll
                 for (int l = 0; l < NP; ++l) {
                     if (l == pos) continue;
-                    const double dh = sDh2[pos * NP + l];
+                    const Real dh = sDh2[pos * NP + l];
                     if (NS && DIM == 3 && dir == 2 && l < pos && P.quirks == 0) {
                         // Q2 (DGSEMIntegrator.cpp:702): H(id2)(:,k) = g, the last
                         // eta-pair flux of node (i,j,l): the pair (j, Np-1) on the
                         // eta line through (i, ., l); zero when j == Np-1.
                         if (c[1] != NP - 1) {
-                            double F[NF], mg[DIM];
+                            Real F[NF], mg[DIM];
 #pragma unroll
                             for (int q = 0; q < DIM; ++q) mg[q] = adj[1][q];
-                            volume_flux<DIM, double>(load_prim<DIM, ND>(sH, (l * NP + c[1]) * NP + c[0]),
-                                                     load_prim<DIM, ND>(sH, (l * NP + NP - 1) * NP + c[0]), mg,
-                                                     gm1i, F);
+                            volume_flux<DIM, Real>(load_prim<DIM, ND, Real>(sH, (l * NP + c[1]) * NP + c[0]),
+                                                   load_prim<DIM, ND, Real>(sH, (l * NP + NP - 1) * NP + c[0]), mg,
+                                                   gm1i, F);
 #pragma unroll
                             for (int f = 0; f < NF; ++f) dUi[k][f] += dh * F[f];
                         }
@@ -425,7 +459,7 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
                     line_base<DIM, NP>(dir, ln, base, stride);
 #pragma unroll
                     for (int l = 0; l < NP; ++l) {
-                        const double dh = sDh[pos * NP + l];
+                        const Real dh = sDh[pos * NP + l];
 #pragma unroll
                         for (int f = 0; f < NF; ++f) dUv[k][f] += sV[(dir * NF + f) * ND + base + l * stride] * dh;
                     }
@@ -434,23 +468,23 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
         }
         __syncwarp();
     }
-    double acc[NPL][NF];
+    Real acc[NPL][NF];
 #pragma unroll
     for (int k = 0; k < NPL; ++k)
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-            double v = -dUi[k][f];
-            if (P.blending) v *= (1.0 - alpha);
+            Real v = -dUi[k][f];
+            if (P.blending) v *= (Real(1) - alpha);
             if (NS) v += dUv[k][f];
             acc[k][f] = v * mJ;
         }
 
     // ---- subcell first-order FV (DGSEMIntegrator.cpp:972-1196), skipped when alpha == 0
-    if (P.blending && alpha != 0.0) {
-        double fv[NPL][NF];
+    if (P.blending && alpha != Real(0)) {
+        Real fv[NPL][NF];
 #pragma unroll
         for (int dir = 0; dir < DIM; ++dir) {
-            double nor[DIM];
+            Real nor[DIM];
 #pragma unroll
             for (int q = 0; q < DIM; ++q) nor[q] = adj[dir][q];
             for (int it = li; it < NID; it += GS) {
@@ -458,11 +492,11 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
                 int base, stride;
                 line_base<DIM, NP>(dir, ln, base, stride);
                 const int n1 = base + ii * stride, n2 = n1 + stride;
-                const Prim<DIM, double> q1 = load_prim<DIM, ND>(sH, n1), q2 = load_prim<DIM, ND>(sH, n2);
-                double s1[NF], s2[NF], F[NF];
+                const Prim<DIM, Real> q1 = load_prim<DIM, ND, Real>(sH, n1), q2 = load_prim<DIM, ND, Real>(sH, n2);
+                Real s1[NF], s2[NF], F[NF];
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) { s1[1 + d] = q1.rho * q1.v[d]; s2[1 + d] = q2.rho * q2.v[d]; }
-                face_flux<DIM, double>(s1, q1, s2, q2, nor, gm1i, P.quirks == 0, true, F);
+                face_flux<DIM, Real>(s1, q1, s2, q2, nor, gm1i, P.quirks == 0, true, F);
 #pragma unroll
                 for (int f = 0; f < NF; ++f) sF[f * NID + it] = F[f];
             }
@@ -475,10 +509,10 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
                     node_coords<NP>(n, c);
                     const int pos = c[dir];
                     const int ib = line_index<DIM, NP>(dir, c) * (NP - 1);
-                    const double mw = 1.0 / (J * sW[pos]);
+                    const Real mw = Real(1.0 / (J * double(sW[pos])));
 #pragma unroll
                     for (int f = 0; f < NF; ++f) {
-                        double v;
+                        Real v;
                         if (pos == 0) v = -sF[f * NID + ib];
                         else if (pos == NP - 1) v = sF[f * NID + ib + pos - 1];
                         else v = sF[f * NID + ib + pos - 1] - sF[f * NID + ib + pos];
@@ -496,7 +530,7 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
     }
 
     // ---- surface fluxes of the element's own faces; neighbour traces from global/L2
-    const double aw = 1.0 / (sW[0] * J);
+    const Real aw = Real(1.0 / (double(sW[0]) * J));
     for (int it = li; it < NFI; it += GS) {
         const int lf = it / NFN, fa = it - lf * NFN;
         const int no = face_node<DIM, NP>(lf, fa);
@@ -504,49 +538,54 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
         const long long gn = (long long)t.x * ND + face_node<DIM, NP>(t.y, fa);
         const long long go = (long long)e * ND + no;
         const bool own_is_1 = (t.w == 0);
-        double so[NF], sn[NF], nor[DIM], flux[NF], fn[NF];
+        double so[NF], sn[NF];
+        Real nor[DIM], flux[NF], fn[NF], mo[NF], mn[NF];
 #pragma unroll
         for (int f = 0; f < NF; ++f) { so[f] = __ldg(a.u + f * Ndof + go); sn[f] = __ldg(a.u + f * Ndof + gn); }
 #pragma unroll
-        for (int q = 0; q < DIM; ++q) nor[q] = __ldg(m.fnor + (long long)t.z * DIM + q);
-        Prim<DIM, double> po = load_prim<DIM, ND>(sH, no);
-        Prim<DIM, double> pn = primitives<DIM, double>(sn, gamma, gm1);
+        for (int q = 0; q < DIM; ++q) nor[q] = Real(__ldg(m.fnor + (long long)t.z * DIM + q));
+        Prim<DIM, Real> po = load_prim<DIM, ND, Real>(sH, no);
+        const Prim<DIM, double> pn64 = primitives<DIM, double>(sn, gamma, gm1);
+        Prim<DIM, Real> pn = cast_prim<DIM, Real>(pn64);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) fn[f] = 0.0;
+        for (int f = 0; f < NF; ++f) fn[f] = 0;
         if constexpr (NS) {
             // DGSEMIntegrator.cpp:435-549: 0.5 (Fv1 + Fv2) . n from each trace's
             // own state and lifted gradients
 #pragma unroll
             for (int side = 0; side < 2; ++side) {
                 const long long g = side == 0 ? go : gn;
-                const Prim<DIM, double> &q = side == 0 ? po : pn;
-                double dq[DIM][NF];
+                const Prim<DIM, Real> &q = side == 0 ? po : pn;
+                Real dq[DIM][NF];
 #pragma unroll
                 for (int d = 0; d < DIM; ++d)
 #pragma unroll
-                    for (int f = 0; f < NF; ++f) dq[d][f] = __ldg(a.grad + (d * NF + f) * Ndof + g);
-                viscous_flux<DIM, double>(q.rho, q.rrho, q.v, 0.5 * q.rbeta * q.rho, dq, P,
-                                          [&](int f, int cc, double val) { fn[f] += (0.5 * val) * nor[cc]; });
+                    for (int f = 0; f < NF; ++f) dq[d][f] = __ldg(grad + (d * NF + f) * Ndof + g);
+                viscous_flux<DIM, Real>(q.rho, q.rrho, q.v, Real(0.5) * q.rbeta * q.rho, dq, P,
+                                        [&](int f, int cc, Real val) { fn[f] += (Real(0.5) * val) * nor[cc]; });
             }
             if (P.quirks == 0) {
                 // Q8 (BasicOperations.cpp:33-34 via NavierStokesFlux.cpp:14): the face
                 // Riemann flux reads states whose momentum slots now hold velocity.
+                const Prim<DIM, double> po64 = primitives<DIM, double>(so, gamma, gm1);
 #pragma unroll
-                for (int d = 0; d < DIM; ++d) { so[1 + d] *= po.rrho; sn[1 + d] *= pn.rrho; }
-                po = primitives<DIM, double>(so, gamma, gm1);
-                pn = primitives<DIM, double>(sn, gamma, gm1);
+                for (int d = 0; d < DIM; ++d) { so[1 + d] *= po64.rrho; sn[1 + d] *= pn64.rrho; }
+                po = cast_prim<DIM, Real>(primitives<DIM, double>(so, gamma, gm1));
+                pn = cast_prim<DIM, Real>(primitives<DIM, double>(sn, gamma, gm1));
             }
         }
+#pragma unroll
+        for (int f = 0; f < NF; ++f) { mo[f] = Real(so[f]); mn[f] = Real(sn[f]); }
         if (own_is_1)
-            face_flux<DIM, double>(so, po, sn, pn, nor, gm1i, P.quirks == 0, P.dissipation != 0, flux);
+            face_flux<DIM, Real>(mo, po, mn, pn, nor, gm1i, P.quirks == 0, P.dissipation != 0, flux);
         else
-            face_flux<DIM, double>(sn, pn, so, po, nor, gm1i, P.quirks == 0, P.dissipation != 0, flux);
+            face_flux<DIM, Real>(mn, pn, mo, po, nor, gm1i, P.quirks == 0, P.dissipation != 0, flux);
 #pragma unroll
         for (int f = 0; f < NF; ++f) sF[f * NFI + it] = aw * (own_is_1 ? (fn[f] - flux[f]) : (flux[f] - fn[f]));
     }
     __syncwarp();
 
-    // ---- gather face terms, epilogue
+    // ---- gather face terms, epilogue (FP64 state update)
     if (!active) return;
 #pragma unroll
     for (int k = 0; k < NPL; ++k) {
@@ -569,13 +608,14 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
         switch (a.mode) {
         case EPI_STORE:
 #pragma unroll
-            for (int f = 0; f < NF; ++f) a.dudt[f * Ndof + gnode] = acc[k][f];
+            for (int f = 0; f < NF; ++f) a.dudt[f * Ndof + gnode] = double(acc[k][f]);
             break;
         case EPI_LSRK:
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 const long long g = f * Ndof + gnode;
-                const double dv = (a.rkA == 0.0) ? a.dt * acc[k][f] : a.rkA * a.du[g] + a.dt * acc[k][f];
+                const double L = double(acc[k][f]);
+                const double dv = (a.rkA == 0.0) ? a.dt * L : a.rkA * a.du[g] + a.dt * L;
                 a.du[g] = dv;
                 a.u_out[g] = __ldg(a.u + g) + a.rkB * dv;
             }
@@ -584,14 +624,14 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 const long long g = f * Ndof + gnode;
-                a.u_out[g] = __ldg(a.u + g) + a.dt * acc[k][f];
+                a.u_out[g] = __ldg(a.u + g) + a.dt * double(acc[k][f]);
             }
             break;
         case EPI_SSP2:
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 const long long g = f * Ndof + gnode;
-                const double y = __ldg(a.u + g) + a.dt * acc[k][f];
+                const double y = __ldg(a.u + g) + a.dt * double(acc[k][f]);
                 a.u_out[g] = 3. / 4 * a.x0[g] + 1. / 4 * y;
             }
             break;
@@ -599,7 +639,7 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 const long long g = f * Ndof + gnode;
-                const double y = __ldg(a.u + g) + a.dt * acc[k][f];
+                const double y = __ldg(a.u + g) + a.dt * double(acc[k][f]);
                 a.u_out[g] = 1. / 3 * a.x0[g] + 2. / 3 * y;
             }
             break;
@@ -613,16 +653,21 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
 // Entropy variables (BasicOperations.cpp:81-104), element gradient
 // (LiftingBR1.cpp:156-272), face lifting 1/2 (v2 - v1) n (LiftingBR1.cpp:10-115)
 // and the chain rule to primitive gradients (BasicOperations.cpp:126-170).
-template <int DIM, int NP>
+// The arithmetic is FP64 in both forms (it is per node and cheap); the lifted
+// gradients are stored in the working precision Out (double, or float for the
+// FP32-bulk form).
+template <int DIM, int NP, typename Out>
 __global__ void __launch_bounds__(Shape<DIM, NP>::THREADS, 4)
 lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_constant__ OpTables T) {
     using S = Shape<DIM, NP>;
     constexpr int ND = S::ND, NF = S::NF, NFN = S::NFN, NFI = S::NFI;
     constexpr int PER_ELEM = 2 * NF * ND + DIM * NF * NFI;
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *smem = reinterpret_cast<double *>(smem_raw);
     double *sT = smem;
     const double *sD = sT, *sW = sT + 4 * NP * NP;
-    load_tables<NP>(T, sT, threadIdx.x, S::THREADS);
+    load_tables<NP, double>(T, sT, threadIdx.x, S::THREADS);
+    Out *gout = sizeof(Out) == 8 ? reinterpret_cast<Out *>(a.grad) : reinterpret_cast<Out *>(a.grad32);
 
     const int el = threadIdx.x / ND;
     const int n = threadIdx.x - el * ND;
@@ -727,14 +772,14 @@ lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_
     for (int q = 0; q < DIM; ++q) {
         entropygrad2primgrad<DIM, double>(st, P, g[q]);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) a.grad[(q * NF + f) * Ndof + gnode] = g[q][f];
+        for (int f = 0; f < NF; ++f) gout[(q * NF + f) * Ndof + gnode] = Out(g[q][f]);
     }
 }
 
-template <int DIM, int NP, bool NS>
+template <int DIM, int NP, bool NS, typename Real>
 size_t rhs_smem() {
-    using LY = RhsLayout<DIM, NP, NS>;
-    return sizeof(double) * (Shape<DIM, NP>::TAB + (size_t)LY::EPB * LY::PER_ELEM);
+    using LY = RhsLayout<DIM, NP, NS, Real>;
+    return sizeof(Real) * (Shape<DIM, NP>::TAB + (size_t)LY::EPB * LY::PER_ELEM);
 }
 template <int DIM, int NP>
 size_t lift_smem() {
@@ -743,33 +788,33 @@ size_t lift_smem() {
     return sizeof(double) * (S::TAB + (size_t)S::EPB * PER_ELEM);
 }
 
-template <int DIM, int NP, bool NS>
+template <int DIM, int NP, bool NS, typename Real>
 cudaError_t rhs_launch_ns(const MeshDev &m, const RhsArgs &a, const PhysParams &P, const OpTables &T,
                           cudaStream_t s) {
-    using LY = RhsLayout<DIM, NP, NS>;
+    using LY = RhsLayout<DIM, NP, NS, Real>;
     const int grid = (m.E + LY::EPB - 1) / LY::EPB;
-    const size_t sm = rhs_smem<DIM, NP, NS>();
-    cudaError_t err = cudaFuncSetAttribute(rhs_kernel<DIM, NP, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)sm);
+    const size_t sm = rhs_smem<DIM, NP, NS, Real>();
+    cudaError_t err = cudaFuncSetAttribute(rhs_kernel<DIM, NP, NS, Real>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (err != cudaSuccess) return err;
-    rhs_kernel<DIM, NP, NS><<<grid, LY::THREADS, sm, s>>>(m, a, P, T);
+    rhs_kernel<DIM, NP, NS, Real><<<grid, LY::THREADS, sm, s>>>(m, a, P, T);
     return cudaGetLastError();
 }
-template <int DIM, int NP>
+template <int DIM, int NP, typename Real>
 cudaError_t rhs_launch_t(bool ns, const MeshDev &m, const RhsArgs &a, const PhysParams &P,
                          const OpTables &T, cudaStream_t s) {
-    return ns ? rhs_launch_ns<DIM, NP, true>(m, a, P, T, s) : rhs_launch_ns<DIM, NP, false>(m, a, P, T, s);
+    return ns ? rhs_launch_ns<DIM, NP, true, Real>(m, a, P, T, s) : rhs_launch_ns<DIM, NP, false, Real>(m, a, P, T, s);
 }
-template <int DIM, int NP>
+template <int DIM, int NP, typename Out>
 cudaError_t lift_launch_t(const MeshDev &m, const LiftArgs &a, const PhysParams &P,
                           const OpTables &T, cudaStream_t s) {
     using S = Shape<DIM, NP>;
     const int grid = (m.E + S::EPB - 1) / S::EPB;
     const size_t sm = lift_smem<DIM, NP>();
-    cudaError_t err = cudaFuncSetAttribute(lift_kernel<DIM, NP>,
+    cudaError_t err = cudaFuncSetAttribute(lift_kernel<DIM, NP, Out>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (err != cudaSuccess) return err;
-    lift_kernel<DIM, NP><<<grid, S::THREADS, sm, s>>>(m, a, P, T);
+    lift_kernel<DIM, NP, Out><<<grid, S::THREADS, sm, s>>>(m, a, P, T);
     return cudaGetLastError();
 }
 
@@ -779,29 +824,45 @@ bool order_supported(int dim, int order) {
     return (dim == 2 || dim == 3) && order >= 1 && order <= 5;
 }
 
-#define PRANDTL_DISPATCH(DIMV, FN, ...)                                  \
+#define PRANDTL_DISPATCH(DIMV, FN, REAL, ...)                            \
     switch (order) {                                                     \
-    case 1: return FN<DIMV, 2>(__VA_ARGS__);                             \
-    case 2: return FN<DIMV, 3>(__VA_ARGS__);                             \
-    case 3: return FN<DIMV, 4>(__VA_ARGS__);                             \
-    case 4: return FN<DIMV, 5>(__VA_ARGS__);                             \
-    case 5: return FN<DIMV, 6>(__VA_ARGS__);                             \
+    case 1: return FN<DIMV, 2, REAL>(__VA_ARGS__);                       \
+    case 2: return FN<DIMV, 3, REAL>(__VA_ARGS__);                       \
+    case 3: return FN<DIMV, 4, REAL>(__VA_ARGS__);                       \
+    case 4: return FN<DIMV, 5, REAL>(__VA_ARGS__);                       \
+    case 5: return FN<DIMV, 6, REAL>(__VA_ARGS__);                       \
     default: return cudaErrorInvalidValue;                               \
     }
 
 cudaError_t launch_rhs(int dim, int order, bool ns, const MeshDev &m, const RhsArgs &a,
                        const PhysParams &P, const OpTables &T, cudaStream_t s) {
     if (m.E <= 0) return cudaSuccess;
-    if (dim == 2) { PRANDTL_DISPATCH(2, rhs_launch_t, ns, m, a, P, T, s) }
-    if (dim == 3) { PRANDTL_DISPATCH(3, rhs_launch_t, ns, m, a, P, T, s) }
+    if (dim == 2) { PRANDTL_DISPATCH(2, rhs_launch_t, double, ns, m, a, P, T, s) }
+    if (dim == 3) { PRANDTL_DISPATCH(3, rhs_launch_t, double, ns, m, a, P, T, s) }
     return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_lift(int dim, int order, const MeshDev &m, const LiftArgs &a,
                         const PhysParams &P, const OpTables &T, cudaStream_t s) {
     if (m.E <= 0) return cudaSuccess;
-    if (dim == 2) { PRANDTL_DISPATCH(2, lift_launch_t, m, a, P, T, s) }
-    if (dim == 3) { PRANDTL_DISPATCH(3, lift_launch_t, m, a, P, T, s) }
+    if (dim == 2) { PRANDTL_DISPATCH(2, lift_launch_t, double, m, a, P, T, s) }
+    if (dim == 3) { PRANDTL_DISPATCH(3, lift_launch_t, double, m, a, P, T, s) }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_rhs_fp32(int dim, int order, bool ns, const MeshDev &m, const RhsArgs &a,
+                            const PhysParams &P, const OpTables &T, cudaStream_t s) {
+    if (m.E <= 0) return cudaSuccess;
+    if (dim == 2) { PRANDTL_DISPATCH(2, rhs_launch_t, float, ns, m, a, P, T, s) }
+    if (dim == 3) { PRANDTL_DISPATCH(3, rhs_launch_t, float, ns, m, a, P, T, s) }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_lift_fp32(int dim, int order, const MeshDev &m, const LiftArgs &a,
+                             const PhysParams &P, const OpTables &T, cudaStream_t s) {
+    if (m.E <= 0) return cudaSuccess;
+    if (dim == 2) { PRANDTL_DISPATCH(2, lift_launch_t, float, m, a, P, T, s) }
+    if (dim == 3) { PRANDTL_DISPATCH(3, lift_launch_t, float, m, a, P, T, s) }
     return cudaErrorInvalidValue;
 }
 

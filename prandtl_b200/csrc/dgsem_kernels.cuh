@@ -26,7 +26,7 @@ struct MeshDev {
 
 struct RhsArgs {
     const double *u;        // stage input state (byNODES)
-    const double *grad;     // NS: primitive gradients [DIM][NF][Ndof]
+    const double *grad;     // NS: primitive gradients [DIM][NF][Ndof] (FP64 path)
     double *dudt;           // EPI_STORE output
     double *u_out;          // RK output state
     double *du;             // LSRK register
@@ -35,11 +35,13 @@ struct RhsArgs {
     unsigned long long *lambda;   // max |V|+c as ordered bits (may be null)
     double dt, rkA, rkB;
     int mode;
+    const float *grad32;    // NS: primitive gradients, FP32-bulk form
 };
 
 struct LiftArgs {
     const double *u;
-    double *grad;
+    double *grad;           // FP64 path
+    float *grad32;          // FP32-bulk form
 };
 
 // Launchers (dispatch on dim and order).  Return cudaSuccess or the launch error.
@@ -47,6 +49,11 @@ cudaError_t launch_rhs(int dim, int order, bool ns, const MeshDev &m, const RhsA
                        const PhysParams &P, const OpTables &T, cudaStream_t s);
 cudaError_t launch_lift(int dim, int order, const MeshDev &m, const LiftArgs &a,
                         const PhysParams &P, const OpTables &T, cudaStream_t s);
+// FP32-bulk form: flux work in FP32, primitives and RK update in FP64.
+cudaError_t launch_rhs_fp32(int dim, int order, bool ns, const MeshDev &m, const RhsArgs &a,
+                            const PhysParams &P, const OpTables &T, cudaStream_t s);
+cudaError_t launch_lift_fp32(int dim, int order, const MeshDev &m, const LiftArgs &a,
+                             const PhysParams &P, const OpTables &T, cudaStream_t s);
 bool order_supported(int dim, int order);
 
 }   // namespace prandtl

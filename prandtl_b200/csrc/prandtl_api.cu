@@ -35,7 +35,8 @@ struct prandtl_handle {
     double *d_fnor = nullptr;
     double *d_in = nullptr, *d_out = nullptr;     // staging / ping-pong states
     double *d_rk1 = nullptr, *d_rk2 = nullptr;    // RK registers
-    double *d_grad = nullptr;                     // NS primitive gradients
+    double *d_grad = nullptr;                     // NS primitive gradients (FP64 path)
+    float *d_grad32 = nullptr;                    // NS primitive gradients (FP32-bulk form)
     double *d_alpha = nullptr;
     unsigned long long *d_lambda = nullptr;
     size_t bytes = 0;
@@ -225,18 +226,22 @@ prandtl_status run_rhs(prandtl_handle *h, const double *u, RhsArgs a) {
     const MeshDev m = mesh_dev(h);
     a.u = u;
     const bool ns = h->cfg.parabolic != 0;
+    const bool fp32 = h->cfg.precision == 1;
     if (ns) {
-        LiftArgs la{u, h->d_grad};
+        LiftArgs la{u, h->d_grad, h->d_grad32};
         cudaEvent_t pe = prof_begin(h, PRANDTL_KERNEL_LIFT);
-        cudaError_t e = launch_lift(h->dim, h->order, m, la, h->P, h->T, h->stream);
+        cudaError_t e = fp32 ? launch_lift_fp32(h->dim, h->order, m, la, h->P, h->T, h->stream)
+                             : launch_lift(h->dim, h->order, m, la, h->P, h->T, h->stream);
         prof_end(h, pe);
         if (e != cudaSuccess) return cuda_fail(h, e, "lift kernel launch");
         h->launches++;
         a.grad = h->d_grad;
+        a.grad32 = h->d_grad32;
     }
     a.alpha = h->cfg.blending ? h->d_alpha : nullptr;
     cudaEvent_t pe = prof_begin(h, PRANDTL_KERNEL_RHS);
-    cudaError_t e = launch_rhs(h->dim, h->order, ns, m, a, h->P, h->T, h->stream);
+    cudaError_t e = fp32 ? launch_rhs_fp32(h->dim, h->order, ns, m, a, h->P, h->T, h->stream)
+                         : launch_rhs(h->dim, h->order, ns, m, a, h->P, h->T, h->stream);
     prof_end(h, pe);
     if (e != cudaSuccess) return cuda_fail(h, e, "rhs kernel launch");
     h->launches++;
@@ -252,6 +257,7 @@ void free_all(prandtl_handle *h) {
     cudaFree(h->d_rk1);
     cudaFree(h->d_rk2);
     cudaFree(h->d_grad);
+    cudaFree(h->d_grad32);
     cudaFree(h->d_alpha);
     cudaFree(h->d_lambda);
     if (h->done) cudaEventDestroy(h->done);
@@ -299,7 +305,8 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
     if (md->num_elements <= 0 || md->num_faces < 0) return fail(nullptr, PRANDTL_EINVAL, "bad sizes");
     if (!md->elem_adj || !md->elem_detj || (md->num_faces > 0 && (!md->face_elems || !md->face_nor)))
         return fail(nullptr, PRANDTL_EINVAL, "mesh arrays missing");
-    if (cfg->precision != 0) return fail(nullptr, PRANDTL_EUNSUPPORTED, "only precision 0 (FP64) is built");
+    if (cfg->precision != 0 && cfg->precision != 1)
+        return fail(nullptr, PRANDTL_EUNSUPPORTED, "precision must be 0 (FP64) or 1 (FP32 bulk)");
     if (!(cfg->gamma > 1.0) || !(cfg->Pr > 0.0)) return fail(nullptr, PRANDTL_EINVAL, "bad gamma/Pr");
 
     const int dim = md->dim, NFACE = 2 * dim, E = md->num_elements, F = md->num_faces;
@@ -369,7 +376,10 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
     if ((st = dalloc(h, &h->d_out, S, "state out")) != PRANDTL_OK) return bail(st);
     if ((st = dalloc(h, &h->d_rk1, S, "rk register 1")) != PRANDTL_OK) return bail(st);
     if ((st = dalloc(h, &h->d_rk2, S, "rk register 2")) != PRANDTL_OK) return bail(st);
-    if (cfg->parabolic && (st = dalloc(h, &h->d_grad, (size_t)dim * S, "gradients")) != PRANDTL_OK) return bail(st);
+    if (cfg->parabolic && cfg->precision == 0 && (st = dalloc(h, &h->d_grad, (size_t)dim * S, "gradients")) != PRANDTL_OK)
+        return bail(st);
+    if (cfg->parabolic && cfg->precision == 1 && (st = dalloc(h, &h->d_grad32, (size_t)dim * S, "gradients")) != PRANDTL_OK)
+        return bail(st);
     if ((st = dalloc(h, &h->d_alpha, (size_t)E, "alpha")) != PRANDTL_OK) return bail(st);
     if ((st = dalloc(h, &h->d_lambda, 1, "lambda")) != PRANDTL_OK) return bail(st);
 
@@ -594,6 +604,6 @@ const char *prandtl_last_error(const prandtl_handle *h) {
     return h ? h->err.c_str() : g_create_error.c_str();
 }
 
-const char *prandtl_version(void) { return "prandtl_b200 0.1 (sm_100a, FP64)"; }
+const char *prandtl_version(void) { return "prandtl_b200 0.2 (sm_100a, FP64 + FP32-bulk)"; }
 
 }   // extern "C"

@@ -41,7 +41,7 @@ class DGSEMOperator:
     def __init__(self, mesh: Mesh, *, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05,
                  parabolic=False, blending=False, sutherland=False, alpha_max=0.5,
                  alpha_min=0.001, quirks="reference", surface_dissipation=True,
-                 timeout_s=120.0):
+                 precision="fp64", timeout_s=120.0):
         L = _lib.load()
         self.mesh = mesh
         self._adj = np.ascontiguousarray(mesh.elem_adj, dtype=np.float64)
@@ -62,6 +62,9 @@ class DGSEMOperator:
             raise ValueError("quirks must be 'reference' or 'fixed'")
         cfg.quirks = 1 if quirks in ("fixed", 1) else 0
         cfg.surface_dissipation = int(bool(surface_dissipation))
+        if precision not in ("fp64", "fp32"):
+            raise ValueError("precision must be 'fp64' or 'fp32' (FP32 bulk, FP64 RK state)")
+        cfg.precision = 1 if precision == "fp32" else 0
         cfg.timeout_s = timeout_s
         h = C.c_void_p()
         _lib.check(L.prandtl_create(C.byref(desc), C.byref(cfg), C.byref(h)), None)

@@ -76,7 +76,7 @@ def test_create_validates_before_touching_the_device(lib):
     d = _desc(m, keep)
     d.num_faces -= 1   # an element face without a neighbour
     assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EUNSUPPORTED
-    cfg.precision = 1
+    cfg.precision = 2
     d = _desc(m, keep)
     assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EUNSUPPORTED
 

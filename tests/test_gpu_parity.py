@@ -40,7 +40,7 @@ PHYS = [
 
 
 @pytest.mark.parametrize("dim,n,order", [(2, 3, 3), (2, 2, 1), (2, 4, 2), (2, 2, 4), (2, 2, 5),
-                                         (3, 2, 3), (3, 2, 1), (3, 3, 2), (3, 2, 4), (3, 1, 3)])
+                                         (3, 2, 3), (3, 2, 1), (3, 3, 2), (3, 2, 4), (3, 2, 5), (3, 1, 3)])
 @pytest.mark.parametrize("phys", range(len(PHYS)))
 @pytest.mark.parametrize("quirks", ["reference", "fixed"])
 def test_rhs_matches_oracle(oracle_mod, dim, n, order, phys, quirks):
