@@ -176,6 +176,107 @@ const char *prandtl_version(void);
 prandtl_status prandtl_rhs_noalloc(const prandtl_mesh_desc *mesh_dev, const prandtl_config *cfg,
                                    const double *u_dev, double *dudt_dev, void *cuda_stream);
 
+/* ---- Batches: many independent solves in one device arena ----------------
+ * Extends the reference's one-operator Mult/Step (DGSEMOperator.hpp:105,
+ * Simulation.cpp:1010) to many operators at once.  Each solve has its own
+ * periodic mesh, order, physics constants, time step and step count; all share
+ * the batch's working precision and RK scheme.  Solves stay resident in one
+ * device arena (admission by footprint; PRANDTL_ENOMEM when it has no room).
+ * Per RK stage, each (dim, order, physics) class runs one persistent launch of
+ * the lifting and one of the fused RHS + stage update over the work items of
+ * all its solves; the step's launch sequence is captured in a CUDA graph once
+ * and replayed.  Solve tables and work lists live in device memory, so solves
+ * admitted or retired between advances need no new capture.  Calls on one
+ * batch are serialised; batches are independent. */
+typedef struct prandtl_batch prandtl_batch;
+
+typedef struct {
+    int precision;          /* 0: FP64, 1: FP32 bulk (as prandtl_config.precision) */
+    int scheme;             /* PRANDTL_LSRK45 or PRANDTL_RK3SSP */
+    size_t arena_bytes;     /* device memory for resident solves; 0: half of the free memory */
+    int max_solves;         /* capacity of the solve table; 0: 4096 */
+    int steps_per_graph;    /* steps per captured graph; 0: 4 */
+    int use_graph;          /* 1: replay captured graphs; 0: launch stage by stage */
+    double timeout_s;       /* bound on every host wait; <= 0: 120 s */
+} prandtl_batch_config;
+
+typedef struct {
+    double dt;              /* time step (with cfl > 0: the first step's) */
+    double cfl;             /* > 0: after each step dt = cfl*hmin/(lambda_max (N+1)^2),
+                               lambda_max over that step's stages (Simulation.cpp:1013-1018) */
+    double hmin;            /* smallest element size, for cfl > 0 */
+    int nsteps;             /* steps to take */
+} prandtl_solve_desc;
+
+void prandtl_batch_config_default(prandtl_batch_config *c);
+prandtl_status prandtl_batch_create(const prandtl_batch_config *c, prandtl_batch **out);
+prandtl_status prandtl_batch_destroy(prandtl_batch *b);
+/* Arena bytes a solve of this mesh and physics takes. */
+prandtl_status prandtl_batch_footprint(prandtl_batch *b, const prandtl_mesh_desc *mesh,
+                                       const prandtl_config *cfg, size_t *bytes);
+/* Admit a solve with initial state u0 (byNODES; host or device per ptr_flags).
+ * cfg->precision is ignored (the batch's applies). */
+prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *mesh, const prandtl_config *cfg,
+                                 const double *u0, int ptr_flags, const prandtl_solve_desc *solve, int *id);
+/* Enqueue nsteps steps; each solve stops at its own step count.  Asynchronous. */
+prandtl_status prandtl_batch_advance(prandtl_batch *b, int nsteps);
+/* Wait (bounded) for the enqueued work. */
+prandtl_status prandtl_batch_sync(prandtl_batch *b);
+/* Waits, then lists up to `cap` resident solves with no steps left. */
+prandtl_status prandtl_batch_finished(prandtl_batch *b, int *ids, int cap, int *count);
+/* Waits, then reports one solve's progress, current dt and last-step lambda_max. */
+prandtl_status prandtl_batch_query(prandtl_batch *b, int id, int *steps_left, int *steps_done,
+                                   double *dt, double *lambda_max);
+/* Waits, then copies the solve's current state (byNODES) out. */
+prandtl_status prandtl_batch_read(prandtl_batch *b, int id, double *u, int ptr_flags);
+/* Retire a solve and free its arena range (after the enqueued work). */
+prandtl_status prandtl_batch_remove(prandtl_batch *b, int id);
+/* Autotuner: per class with resident solves, time `reps` launches of each RHS
+ * launch shape on the next step's first stage (which the step recomputes) and
+ * keep the fastest. */
+prandtl_status prandtl_batch_tune(prandtl_batch *b, int reps);
+/* Launch shape chosen for a class and the tuned times (ms per launch, -1 when
+ * not timed) of each of the *n_variants shapes; ms may be NULL. */
+prandtl_status prandtl_batch_class_info(prandtl_batch *b, int dim, int order, int parabolic,
+                                        int *variant, int *n_variants, double *ms);
+size_t prandtl_batch_device_bytes(const prandtl_batch *b);   /* arena + tables */
+size_t prandtl_batch_arena_bytes(const prandtl_batch *b);    /* arena only */
+long long prandtl_batch_kernel_launches(const prandtl_batch *b);
+const char *prandtl_batch_last_error(const prandtl_batch *b);
+
+/* ---- Serving: a request loop over one batch ------------------------------
+ * A worker thread admits submitted solves into a batch as arena room and
+ * table slots free up (first come, first served), advances all resident
+ * solves `steps_per_tick` steps at a time, and retires finished ones by
+ * copying their final state to the caller's buffer.  Requests that arrive
+ * while others run join the next tick: their stages share the launches of
+ * the resident solves. */
+typedef struct prandtl_server prandtl_server;
+
+typedef struct {
+    long long submitted, completed, rejected;
+    long long steps;                /* batch steps the worker enqueued */
+    double dof_updates;             /* sum over completed solves of nodes*fields*steps */
+    double busy_s;                  /* wall time with at least one resident solve */
+    int resident;                   /* solves resident now */
+} prandtl_serve_stats;
+
+prandtl_status prandtl_serve_create(const prandtl_batch_config *c, int steps_per_tick, prandtl_server **out);
+/* Copies mesh, config and u0 (host memory); u_out (host, nf*Ndof doubles) receives
+ * the final state and must stay valid until the request completes.  A request
+ * that can never fit the arena is rejected with PRANDTL_ENOMEM. */
+prandtl_status prandtl_serve_submit(prandtl_server *s, const prandtl_mesh_desc *mesh, const prandtl_config *cfg,
+                                    const double *u0, const prandtl_solve_desc *solve, double *u_out,
+                                    long long *ticket);
+/* done = 1 when the result is in u_out; seconds = submit-to-result time. */
+prandtl_status prandtl_serve_poll(prandtl_server *s, long long ticket, int *done, double *seconds);
+/* Waits up to timeout_s for the request; PRANDTL_ETIMEDOUT otherwise. */
+prandtl_status prandtl_serve_wait(prandtl_server *s, long long ticket, double timeout_s, double *seconds);
+prandtl_status prandtl_serve_stats_get(prandtl_server *s, prandtl_serve_stats *st);
+/* Stops the worker after the resident solves finish (bounded by the batch timeout) and frees everything. */
+prandtl_status prandtl_serve_destroy(prandtl_server *s);
+const char *prandtl_serve_last_error(prandtl_server *s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,7 +25,16 @@ EXPORTS = ["prandtl_config_default", "prandtl_create", "prandtl_destroy", "prand
            "prandtl_step", "prandtl_get_alpha", "prandtl_cfl_dt", "prandtl_set_stream",
            "prandtl_synchronize", "prandtl_kernel_launches", "prandtl_profile",
            "prandtl_profile_read", "prandtl_profile_reset", "prandtl_device_bytes",
-           "prandtl_last_error", "prandtl_version", "prandtl_rhs_noalloc"]
+           "prandtl_last_error", "prandtl_version", "prandtl_rhs_noalloc",
+           "prandtl_batch_config_default", "prandtl_batch_create", "prandtl_batch_destroy",
+           "prandtl_batch_footprint", "prandtl_batch_add", "prandtl_batch_advance",
+           "prandtl_batch_sync", "prandtl_batch_finished", "prandtl_batch_query",
+           "prandtl_batch_read", "prandtl_batch_remove", "prandtl_batch_tune",
+           "prandtl_batch_class_info", "prandtl_batch_device_bytes", "prandtl_batch_arena_bytes",
+           "prandtl_batch_kernel_launches", "prandtl_batch_last_error",
+           "prandtl_serve_create", "prandtl_serve_submit", "prandtl_serve_poll",
+           "prandtl_serve_wait", "prandtl_serve_stats_get", "prandtl_serve_destroy",
+           "prandtl_serve_last_error"]
 
 
 class MeshDesc(C.Structure):
@@ -41,6 +50,22 @@ class Config(C.Structure):
                 ("parabolic", C.c_int), ("blending", C.c_int), ("sutherland", C.c_int),
                 ("quirks", C.c_int), ("surface_dissipation", C.c_int), ("precision", C.c_int),
                 ("timeout_s", C.c_double)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("precision", C.c_int), ("scheme", C.c_int), ("arena_bytes", C.c_size_t),
+                ("max_solves", C.c_int), ("steps_per_graph", C.c_int), ("use_graph", C.c_int),
+                ("timeout_s", C.c_double)]
+
+
+class SolveDesc(C.Structure):
+    _fields_ = [("dt", C.c_double), ("cfl", C.c_double), ("hmin", C.c_double), ("nsteps", C.c_int)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("rejected", C.c_longlong),
+                ("steps", C.c_longlong), ("dof_updates", C.c_double), ("busy_s", C.c_double),
+                ("resident", C.c_int)]
 
 
 class PrandtlError(RuntimeError):
@@ -95,11 +120,47 @@ def load():
     L.prandtl_rhs_noalloc.restype = ip
     L.prandtl_version.argtypes = []
     L.prandtl_version.restype = C.c_char_p
+    # batches
+    bcp, sdp, mdp, cfp = C.POINTER(BatchConfig), C.POINTER(SolveDesc), C.POINTER(MeshDesc), C.POINTER(Config)
+    ipp = C.POINTER(C.c_int)
+    sig = {
+        "prandtl_batch_config_default": (None, [bcp]),
+        "prandtl_batch_create": (ip, [bcp, C.POINTER(vp)]),
+        "prandtl_batch_destroy": (ip, [vp]),
+        "prandtl_batch_footprint": (ip, [vp, mdp, cfp, C.POINTER(C.c_size_t)]),
+        "prandtl_batch_add": (ip, [vp, mdp, cfp, vp, ip, sdp, ipp]),
+        "prandtl_batch_advance": (ip, [vp, ip]),
+        "prandtl_batch_sync": (ip, [vp]),
+        "prandtl_batch_finished": (ip, [vp, ipp, ip, ipp]),
+        "prandtl_batch_query": (ip, [vp, ip, ipp, ipp, dp, dp]),
+        "prandtl_batch_read": (ip, [vp, ip, vp, ip]),
+        "prandtl_batch_remove": (ip, [vp, ip]),
+        "prandtl_batch_tune": (ip, [vp, ip]),
+        "prandtl_batch_class_info": (ip, [vp, ip, ip, ip, ipp, ipp, dp]),
+        "prandtl_batch_device_bytes": (C.c_size_t, [vp]),
+        "prandtl_batch_arena_bytes": (C.c_size_t, [vp]),
+        "prandtl_batch_kernel_launches": (C.c_longlong, [vp]),
+        "prandtl_batch_last_error": (C.c_char_p, [vp]),
+        "prandtl_serve_create": (ip, [bcp, ip, C.POINTER(vp)]),
+        "prandtl_serve_submit": (ip, [vp, mdp, cfp, vp, sdp, vp, C.POINTER(C.c_longlong)]),
+        "prandtl_serve_poll": (ip, [vp, C.c_longlong, ipp, dp]),
+        "prandtl_serve_wait": (ip, [vp, C.c_longlong, C.c_double, dp]),
+        "prandtl_serve_stats_get": (ip, [vp, C.POINTER(ServeStats)]),
+        "prandtl_serve_destroy": (ip, [vp]),
+        "prandtl_serve_last_error": (C.c_char_p, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
     _LIB = L
     return L
 
 
-def check(status, handle=None):
+def check(status, handle=None, last_error=None):
+    """Raise PrandtlError for a non-OK status with the object's last error text
+    (`last_error` names the getter: prandtl_last_error by default)."""
     if status != PRANDTL_OK:
-        msg = load().prandtl_last_error(handle).decode(errors="replace")
+        getter = getattr(load(), last_error or "prandtl_last_error")
+        msg = getter(handle).decode(errors="replace")
         raise PrandtlError(status, msg)

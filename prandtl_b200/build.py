@@ -4,6 +4,8 @@ Usage: python -m prandtl_b200.build [--verbose-ptxas]
 """
 from __future__ import annotations
 
+import concurrent.futures
+import glob
 import os
 import subprocess
 import sys
@@ -11,7 +13,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libprandtl_b200.so")
-SOURCES = ["dgsem_kernels.cu", "prandtl_api.cu", "prandtl_noalloc.cu"]
+SOURCES = (["dgsem_kernels.cu", "prandtl_api.cu", "prandtl_noalloc.cu", "prandtl_batch.cu", "prandtl_serve.cu"] +
+           sorted(os.path.basename(p) for p in glob.glob(os.path.join(CSRC, "dgsem_inst_*.cu"))))
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -36,17 +39,30 @@ def build(verbose_ptxas: bool = False, force: bool = False, lib: str = LIB, defi
     are extra -D flags (launch-shape overrides used when tuning)."""
     if not force and lib == LIB and not needs_build():
         return LIB
-    objs = []
-    for src in SOURCES:
-        obj = os.path.join(CSRC, src.replace(".cu", ".o"))
-        obj = obj if lib == LIB else obj.replace(".o", f".{abs(hash(lib)) % 100000}.o")
+    tag = "" if lib == LIB else f".{abs(hash(lib)) % 100000}"
+
+    def compile_one(src):
+        obj = os.path.join(CSRC, src.replace(".cu", f"{tag}.o"))
         cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                "--expt-relaxed-constexpr", *[f"-D{d}" for d in defines],
                "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose_ptxas:
             cmd += ["-Xptxas", "-v"]
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return src, obj, r
+
+    # heaviest translation units first so the parallel build ends together
+    order = sorted(SOURCES, key=lambda f: (not f.startswith("dgsem_inst_d3"), f))
+    objs, failed = [], []
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+        for src, obj, r in ex.map(compile_one, order):
+            if r.stdout or r.stderr:
+                sys.stderr.write(r.stdout + r.stderr)
+            if r.returncode != 0:
+                failed.append(src)
+            objs.append(obj)
+    if failed:
+        raise RuntimeError("nvcc failed for " + ", ".join(failed))
     cmd = [nvcc(), *ARCH, "-shared", "-o", lib, *objs, "-lcudart"]
     subprocess.run(cmd, check=True)
     for o in objs:

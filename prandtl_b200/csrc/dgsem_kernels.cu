@@ -1,869 +1,98 @@
-// dgsem_kernels.cu -- element-per-thread-group DGSEM RHS kernels for sm_100a.
-//
-// One thread per volume node; EPB elements per CTA.  Everything an element
-// needs stays in shared memory for the whole RHS evaluation:
-//   load state -> (blending coefficient) -> two-point volume fluxes of all
-//   unique node pairs -> flux differencing -> (subcell FV) -> surface fluxes of
-//   the element's own faces (neighbour traces read from global/L2) -> epilogue
-//   (store dudt, or fuse the Runge-Kutta stage update).
-// Each interior face flux is evaluated by both neighbouring elements with the
-// same operands in the same order, so both sides see bit-identical fluxes and
-// no atomics or face buffers are needed.
+// dgsem_kernels.cu -- dispatch of the DGSEM kernels by dimension, working
+// precision and physics to the dgsem_inst_*.cu translation units, and the
+// batch step-end kernel.
 #include "dgsem_kernels.cuh"
 
 namespace prandtl {
-
-namespace {
-
-constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
-constexpr int cmax(int a, int b) { return a > b ? a : b; }
-
-template <int DIM, int NP>
-struct Shape {
-    static constexpr int ND = ipow(NP, DIM);            // nodes per element
-    static constexpr int NF = DIM + 2;                  // conserved fields
-    static constexpr int NLINE = ND / NP;               // lines per direction
-    static constexpr int PPL = NP * (NP - 1) / 2;       // unique pairs per line
-    static constexpr int NFN = ND / NP;                 // nodes per face
-    static constexpr int NFACE = 2 * DIM;
-    static constexpr int NFI = NFACE * NFN;             // face-node items
-    static constexpr int EPB = cmax(1, 128 / ND);       // elements per CTA
-    static constexpr int THREADS = EPB * ND;
-    static constexpr int TAB = 4 * NP * NP + 2 * NP;    // D, Dhat, Dhat2, Vinv, w, x
-};
-
-// Node coordinates (i, j, k) of element-local node n (x fastest).
-template <int NP>
-__device__ __forceinline__ void node_coords(int n, int c[3]) {
-    c[0] = n % NP;
-    c[1] = (n / NP) % NP;
-    c[2] = n / (NP * NP);
-}
-
-// Line containing node coordinates c in direction dir, and its base/stride.
-template <int DIM, int NP>
-__device__ __forceinline__ int line_index(int dir, const int c[3]) {
-    if (DIM == 2) return dir == 0 ? c[1] : c[0];
-    return dir == 0 ? c[2] * NP + c[1] : (dir == 1 ? c[2] * NP + c[0] : c[1] * NP + c[0]);
-}
-template <int DIM, int NP>
-__device__ __forceinline__ void line_base(int dir, int ln, int &base, int &stride) {
-    if (DIM == 2) {
-        if (dir == 0) { base = ln * NP; stride = 1; }
-        else { base = ln; stride = NP; }
-    } else {
-        if (dir == 0) { base = ln * NP; stride = 1; }
-        else if (dir == 1) { base = (ln / NP) * NP * NP + ln % NP; stride = NP; }
-        else { base = ln; stride = NP * NP; }
-    }
-}
-// Unique pair (a < b) <-> index, a-major.
-template <int NP>
-__device__ __forceinline__ int pair_index(int a, int b) {
-    return a * NP - a * (a + 1) / 2 + (b - a - 1);
-}
-template <int NP>
-__device__ __forceinline__ void pair_decode(int pp, int &a, int &b) {
-    a = 0;
-#pragma unroll
-    for (int q = 0; q < NP - 1; ++q) {
-        if (pp >= NP - 1 - a) { pp -= NP - 1 - a; ++a; }
-    }
-    b = a + 1 + pp;
-}
-// Element-local node of face node `a` on local face lf = 2*dir + side.
-template <int DIM, int NP>
-__device__ __forceinline__ int face_node(int lf, int a) {
-    const int d = lf >> 1, s = lf & 1;
-    int c[3] = {0, 0, 0};
-    c[d] = s * (NP - 1);
-    if (DIM == 2) {
-        c[1 - d] = a;
-        return c[1] * NP + c[0];
-    }
-    const int t0 = (d == 0) ? 1 : 0, t1 = (d == 2) ? 1 : 2;
-    c[t0] = a % NP;
-    c[t1] = a / NP;
-    return (c[2] * NP + c[1]) * NP + c[0];
-}
-template <int DIM, int NP>
-__device__ __forceinline__ int face_tangential(int d, const int c[3]) {
-    if (DIM == 2) return c[1 - d];
-    const int t0 = (d == 0) ? 1 : 0, t1 = (d == 2) ? 1 : 2;
-    return c[t0] + NP * c[t1];
-}
-
-template <int NP, typename Real>
-__device__ __forceinline__ void load_tables(const OpTables &T, Real *sT, int tid, int nthreads) {
-    for (int q = tid; q < NP * NP; q += nthreads) {
-        const int i = q / NP, l = q % NP;
-        sT[q] = Real(T.D[i * NP + l]);
-        sT[NP * NP + q] = Real(T.Dhat[i * NP + l]);
-        sT[2 * NP * NP + q] = Real(T.Dhat2[i * NP + l]);
-        sT[3 * NP * NP + q] = Real(T.Vinv[i * NP + l]);
-    }
-    for (int q = tid; q < NP; q += nthreads) {
-        sT[4 * NP * NP + q] = Real(T.w[q]);
-        sT[4 * NP * NP + NP + q] = Real(T.x[q]);
-    }
-}
-
-__device__ __forceinline__ void atomic_max_pos(unsigned long long *dst, double v) {
-    // v >= 0 (or NaN): non-negative doubles order like their bit patterns.
-    if (!(v >= 0.0)) v = __longlong_as_double(0x7ff0000000000000ll);   // NaN/negative -> +inf
-    atomicMax(dst, (unsigned long long)__double_as_longlong(v));
-}
-
-// Block-wide max of per-thread values, one atomic per CTA.
-template <int THREADS>
-__device__ __forceinline__ void block_max_to(unsigned long long *dst, double v, double *sred) {
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __syncthreads();
-    if (lane == 0) sred[w] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double m = sred[0];
-        for (int q = 1; q < (THREADS + 31) / 32; ++q) m = fmax(m, sred[q]);
-        atomic_max_pos(dst, m);
-    }
-}
-
-// Hoisted per-node primitive table in shared memory: H[k*ND + node].
-template <int DIM>
-struct HIdx {
-    static constexpr int RHO = 0, RRHO = 1, V = 2, VSQ = 2 + DIM, BETA = 3 + DIM, RBETA = 4 + DIM,
-                         LAM = 5 + DIM, K = 6 + DIM;
-};
-template <int DIM, int ND, typename Real>
-__device__ __forceinline__ Prim<DIM, Real> load_prim(const Real *sH, int n) {
-    using I = HIdx<DIM>;
-    Prim<DIM, Real> q;
-    q.rho = sH[I::RHO * ND + n];
-    q.rrho = sH[I::RRHO * ND + n];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) q.v[d] = sH[(I::V + d) * ND + n];
-    q.vsq = sH[I::VSQ * ND + n];
-    q.beta = sH[I::BETA * ND + n];
-    q.rbeta = sH[I::RBETA * ND + n];
-    q.lam = sH[I::LAM * ND + n];
-    return q;
-}
-template <int DIM, int ND, typename Real>
-__device__ __forceinline__ void store_prim(Real *sH, int n, const Prim<DIM, double> &q) {
-    using I = HIdx<DIM>;
-    sH[I::RHO * ND + n] = Real(q.rho);
-    sH[I::RRHO * ND + n] = Real(q.rrho);
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) sH[(I::V + d) * ND + n] = Real(q.v[d]);
-    sH[I::VSQ * ND + n] = Real(q.vsq);
-    sH[I::BETA * ND + n] = Real(q.beta);
-    sH[I::RBETA * ND + n] = Real(q.rbeta);
-    sH[I::LAM * ND + n] = Real(q.lam);
-}
-// Working-precision copy of primitives computed in FP64.
-template <int DIM, typename Real>
-__device__ __forceinline__ Prim<DIM, Real> cast_prim(const Prim<DIM, double> &q) {
-    Prim<DIM, Real> r;
-    r.rho = Real(q.rho);
-    r.rrho = Real(q.rrho);
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) r.v[d] = Real(q.v[d]);
-    r.vsq = Real(q.vsq);
-    r.beta = Real(q.beta);
-    r.rbeta = Real(q.rbeta);
-    r.lam = Real(q.lam);
-    return r;
-}
-
-constexpr int next_pow2(int v) { return v <= 1 ? 1 : 2 * next_pow2((v + 1) / 2); }
-
-// Launch shape of the RHS kernel: warps per CTA and the minimum CTAs per SM the
-// register allocation must allow (launch bounds).
-#ifndef PRANDTL_NS_WARPS
-#define PRANDTL_NS_WARPS 4
-#endif
-#ifndef PRANDTL_NS_MINB
-#define PRANDTL_NS_MINB 3
-#endif
-#ifndef PRANDTL_EULER_WARPS
-#define PRANDTL_EULER_WARPS 4
-#endif
-#ifndef PRANDTL_EULER_MINB
-#define PRANDTL_EULER_MINB 5
-#endif
-#ifndef PRANDTL_NS32_MINB
-#define PRANDTL_NS32_MINB 4
-#endif
-#ifndef PRANDTL_EULER32_MINB
-#define PRANDTL_EULER32_MINB 6
-#endif
-
-// Warp-per-element layout of the RHS kernel: one group of GS lanes owns one
-// element (GS = 32, or the next power of two >= Np^d for small elements, so
-// a warp then holds several elements); lane `li` of a group owns the nodes
-// li, li+GS, ... and the pair / face / subcell items of the same stride.
-// Groups synchronise with __syncwarp only.
-template <int DIM, int NP, bool NS, typename Real>
-struct RhsLayout {
-    using S = Shape<DIM, NP>;
-    static constexpr int ND = S::ND, NF = S::NF, NLINE = S::NLINE, PPL = S::PPL;
-    static constexpr int GS = ND >= 32 ? 32 : next_pow2(ND);
-    static constexpr int EPW = 32 / GS;                 // elements per warp
-    static constexpr int NPL = (ND + GS - 1) / GS;      // nodes per lane
-    static constexpr int NPD = NLINE * PPL;             // pairs per direction
-    static constexpr int NID = NLINE * (NP - 1);        // subcell interfaces per direction
-    static constexpr int BUF = cmax(cmax(NPD, S::NFI), cmax(NID, (5 * ND + NF - 1) / NF)) * NF;
-    static constexpr int K = HIdx<DIM>::K;
-    static constexpr int PER_ELEM = K * ND + BUF + (NS ? DIM * NF * ND : 0);
-    // warps per CTA: the configured count, reduced so the CTA's elements fit the
-    // 227 KB shared-memory limit
-    static constexpr int SMEM_MAX = 227 * 1024;
-    static constexpr int FIT = (SMEM_MAX / (int)sizeof(Real) - S::TAB) / (PER_ELEM * EPW);
-    static constexpr int WARPS_CFG = NS ? PRANDTL_NS_WARPS : PRANDTL_EULER_WARPS;
-    static constexpr int WARPS = cmax(1, FIT < WARPS_CFG ? FIT : WARPS_CFG);
-    static constexpr int EPB = WARPS * EPW;             // elements per CTA
-    static constexpr int THREADS = WARPS * 32;
-    static constexpr bool F64 = sizeof(Real) == 8;
-    static constexpr int MIN_BLOCKS = NS ? (F64 ? PRANDTL_NS_MINB : PRANDTL_NS32_MINB)
-                                         : (F64 ? PRANDTL_EULER_MINB : PRANDTL_EULER32_MINB);
-};
-
-// ------------------------------------------------------------------- RHS
-// Real is the working precision of the O(Np^{d+1}) work (two-point fluxes,
-// flux differencing, surface fluxes, gradients): double for the plain FP64
-// path, float for the FP32-bulk form.  Per-node primitives are always formed
-// in FP64 from the FP64 state, and the RK stage update is FP64.
-template <int DIM, int NP, bool NS, typename Real>
-__global__ void __launch_bounds__(RhsLayout<DIM, NP, NS, Real>::THREADS, (RhsLayout<DIM, NP, NS, Real>::MIN_BLOCKS))
-rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_constant__ OpTables T) {
-    using S = Shape<DIM, NP>;
-    using LY = RhsLayout<DIM, NP, NS, Real>;
-    constexpr int ND = S::ND, NF = S::NF, PPL = S::PPL;
-    constexpr int NFN = S::NFN, NFI = S::NFI, GS = LY::GS, NPL = LY::NPL;
-    constexpr int NPD = LY::NPD, NID = LY::NID;
-
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Real *smem = reinterpret_cast<Real *>(smem_raw);
-    Real *sT = smem;
-    const Real *sDh = sT + NP * NP, *sDh2 = sT + 2 * NP * NP, *sVinv = sT + 3 * NP * NP;
-    const Real *sW = sT + 4 * NP * NP;
-    load_tables<NP, Real>(T, sT, threadIdx.x, LY::THREADS);
-    __syncthreads();
-
-    const int lane = threadIdx.x & 31;
-    const int grp = threadIdx.x / GS;          // element slot within the CTA
-    const int li = threadIdx.x - grp * GS;     // lane within the group
-    const int e_raw = blockIdx.x * LY::EPB + grp;
-    const bool active = e_raw < m.E;
-    const int e = active ? e_raw : m.E - 1;
-    Real *sH = smem + S::TAB + grp * LY::PER_ELEM;   // hoisted primitives [K][ND]
-    Real *sF = sH + LY::K * ND;                       // pairs / subcell / face items / modes
-    Real *sV = sF + LY::BUF;                          // NS: contravariant viscous fluxes [DIM][NF][ND]
-    const Real *grad = nullptr;
-    if constexpr (NS) grad = LY::F64 ? reinterpret_cast<const Real *>(a.grad) : reinterpret_cast<const Real *>(a.grad32);
-
-    const long long Ndof = m.Ndof;
-    const double gamma = P.gamma, gm1 = P.gammaM1;
-    const Real gm1i = Real(P.gammaM1Inverse);
-    const double *geo = m.geo + (long long)e * (DIM * DIM + 1);
-    Real adj[DIM][DIM];
-#pragma unroll
-    for (int r = 0; r < DIM; ++r)
-#pragma unroll
-        for (int c2 = 0; c2 < DIM; ++c2) adj[r][c2] = Real(__ldg(geo + r * DIM + c2));
-    const double J = __ldg(geo + DIM * DIM);
-    const Real mJ = Real(1.0 / J);
-
-    // ---- own nodes: hoisted primitives (formed in FP64); largest |V|+c
-    double lam = 0.0;
-#pragma unroll
-    for (int k = 0; k < NPL; ++k) {
-        const int n = li + k * GS;
-        if (n < ND) {
-            double st[NF];
-#pragma unroll
-            for (int f = 0; f < NF; ++f) st[f] = __ldg(a.u + f * Ndof + (long long)e * ND + n);
-            const Prim<DIM, double> q = primitives<DIM, double>(st, gamma, gm1);
-            store_prim<DIM, ND, Real>(sH, n, q);
-            lam = fmax(lam, q.lam);
-        }
-    }
-    if (a.lambda) {
-        double v = active ? lam : 0.0;
-        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if (lane == 0) atomic_max_pos(a.lambda, v);
-    }
-    __syncwarp();
-
-    // ---- blending coefficient (PerssonPeraireIndicator.cpp:21-58, DGSEMOperator.cpp:60-80)
-    Real alpha = 0;
-    if (P.blending) {
-        Real *b0 = sF, *b1 = sF + ND;
-#pragma unroll
-        for (int k = 0; k < NPL; ++k) {
-            const int n = li + k * GS;
-            if (n < ND) {
-                // rho * ComputePressure(state) with v = m * (1/rho)
-                const Prim<DIM, Real> q = load_prim<DIM, ND, Real>(sH, n);
-                b0[n] = q.rho * (Real(0.5) * q.rbeta * q.rho);
-            }
-        }
-        __syncwarp();
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) {   // modes = V^-1 (rho p), one direction per pass
-            const Real *in = (d & 1) ? b1 : b0;
-            Real *out = (d & 1) ? b0 : b1;
-#pragma unroll
-            for (int k = 0; k < NPL; ++k) {
-                const int n = li + k * GS;
-                if (n < ND) {
-                    int c[3];
-                    node_coords<NP>(n, c);
-                    int base, stride;
-                    line_base<DIM, NP>(d, line_index<DIM, NP>(d, c), base, stride);
-                    Real s = 0;
-#pragma unroll
-                    for (int l = 0; l < NP; ++l) s += sVinv[c[d] * NP + l] * in[base + l * stride];
-                    out[n] = s;
-                }
-            }
-            __syncwarp();
-        }
-        double e0 = 0, e1 = 0, e2 = 0;
-#pragma unroll
-        for (int k = 0; k < NPL; ++k) {
-            const int n = li + k * GS;
-            if (n < ND) {
-                int c[3];
-                node_coords<NP>(n, c);
-                const double md = double(((DIM & 1) ? b1 : b0)[n]);
-                int mx = c[0];
-#pragma unroll
-                for (int d = 1; d < DIM; ++d) mx = max(mx, c[d]);
-                e0 += md * md;
-                if (mx <= NP - 2) e1 += md * md;
-                if (mx <= NP - 3) e2 += md * md;
-            }
-        }
-        for (int o = GS / 2; o > 0; o >>= 1) {
-            e0 += __shfl_xor_sync(0xffffffffu, e0, o);
-            e1 += __shfl_xor_sync(0xffffffffu, e1, o);
-            e2 += __shfl_xor_sync(0xffffffffu, e2, o);
-        }
-        double eta = 1.0 - e1 / e0;
-        eta = fmax(eta, 1.0 - e2 / e1);
-        const double thr = P.modal_threshold;
-        double al = 1.0 / (1.0 + exp(-9.21024 * (eta - thr) / thr));
-        if (al < P.alpha_min) al = 0.0;
-        else if (al > 1.0 - P.alpha_min) al = 1.0;
-        al = fmin(al, P.alpha_max);
-        alpha = Real(al);
-        if (li == 0 && a.alpha && active) a.alpha[e] = al;
-        __syncwarp();
-    }
-
-    // ---- NS: contravariant viscous flux of every own node (flux_mat = adj * Fv^T, :632)
-    if constexpr (NS) {
-#pragma unroll
-        for (int k = 0; k < NPL; ++k) {
-            const int n = li + k * GS;
-            if (n < ND) {
-                Real dq[DIM][NF];
-#pragma unroll
-                for (int d = 0; d < DIM; ++d)
-#pragma unroll
-                    for (int f = 0; f < NF; ++f)
-                        dq[d][f] = __ldg(grad + (d * NF + f) * Ndof + (long long)e * ND + n);
-                // Q1 (DGSEMIntegrator.cpp:620): the reference evaluates the volume
-                // viscous flux with the state of node Np^d-1 (stale member id1).
-                const int src = (P.quirks == 0) ? ND - 1 : n;
-                const Prim<DIM, Real> q = load_prim<DIM, ND, Real>(sH, src);
-                Real Vc[DIM][NF];
-#pragma unroll
-                for (int r = 0; r < DIM; ++r)
-#pragma unroll
-                    for (int f = 0; f < NF; ++f) Vc[r][f] = 0;
-                viscous_flux<DIM, Real>(q.rho, q.rrho, q.v, Real(0.5) * q.rbeta * q.rho, dq, P,
-                                        [&](int f, int cc, Real val) {
-#pragma unroll
-                                            for (int r = 0; r < DIM; ++r) Vc[r][f] += adj[r][cc] * val;
-                                        });
-#pragma unroll
-                for (int r = 0; r < DIM; ++r)
-#pragma unroll
-                    for (int f = 0; f < NF; ++f) sV[(r * NF + f) * ND + n] = Vc[r][f];
-            }
-        }
-        __syncwarp();
-    }
-
-    // ---- flux differencing, one direction at a time:
-    //      sum_l Dhat2(i,l) F#(i,l) (F#(i,i) = 0) and, for NS, sum_l Dhat(i,l) Fv_l
-    Real dUi[NPL][NF], dUv[NPL][NF];
-#pragma unroll
-    for (int k = 0; k < NPL; ++k)
-#pragma unroll
-        for (int f = 0; f < NF; ++f) { dUi[k][f] = 0; dUv[k][f] = 0; }
-#pragma unroll
-    for (int dir = 0; dir < DIM; ++dir) {
-        Real mt[DIM];
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) mt[q] = adj[dir][q];
-        for (int p = li; p < NPD; p += GS) {
-            const int ln = p / PPL, pp = p - ln * PPL;
-            int pa, pb, base, stride;
-            pair_decode<NP>(pp, pa, pb);
-            line_base<DIM, NP>(dir, ln, base, stride);
-            Real F[NF];
-            volume_flux<DIM, Real>(load_prim<DIM, ND, Real>(sH, base + pa * stride),
-                                   load_prim<DIM, ND, Real>(sH, base + pb * stride), mt, gm1i, F);
-#pragma unroll
-            for (int f = 0; f < NF; ++f) sF[f * NPD + p] = F[f];
-        }
-        __syncwarp();
-#pragma unroll
-        for (int k = 0; k < NPL; ++k) {
-            const int n = li + k * GS;
-            if (n < ND) {
-                int c[3];
-                node_coords<NP>(n, c);
-                const int pos = c[dir];
-                const int ln = line_index<DIM, NP>(dir, c);
-#pragma unroll
-                for (int l = 0; l < NP; ++l) {
-                    if (l == pos) continue;
-                    const Real dh = sDh2[pos * NP + l];
-                    if (NS && DIM == 3 && dir == 2 && l < pos && P.quirks == 0) {
-                        // Q2 (DGSEMIntegrator.cpp:702): H(id2)(:,k) = g, the last
-                        // eta-pair flux of node (i,j,l): the pair (j, Np-1) on the
-                        // eta line through (i, ., l); zero when j == Np-1.
-                        if (c[1] != NP - 1) {
-                            Real F[NF], mg[DIM];
-#pragma unroll
-                            for (int q = 0; q < DIM; ++q) mg[q] = adj[1][q];
-                            volume_flux<DIM, Real>(load_prim<DIM, ND, Real>(sH, (l * NP + c[1]) * NP + c[0]),
-                                                   load_prim<DIM, ND, Real>(sH, (l * NP + NP - 1) * NP + c[0]), mg,
-                                                   gm1i, F);
-#pragma unroll
-                            for (int f = 0; f < NF; ++f) dUi[k][f] += dh * F[f];
-                        }
-                    } else {
-                        const int pidx = ln * PPL + (l < pos ? pair_index<NP>(l, pos) : pair_index<NP>(pos, l));
-#pragma unroll
-                        for (int f = 0; f < NF; ++f) dUi[k][f] += dh * sF[f * NPD + pidx];
-                    }
-                }
-                if constexpr (NS) {
-                    int base, stride;
-                    line_base<DIM, NP>(dir, ln, base, stride);
-#pragma unroll
-                    for (int l = 0; l < NP; ++l) {
-                        const Real dh = sDh[pos * NP + l];
-#pragma unroll
-                        for (int f = 0; f < NF; ++f) dUv[k][f] += sV[(dir * NF + f) * ND + base + l * stride] * dh;
-                    }
-                }
-            }
-        }
-        __syncwarp();
-    }
-    Real acc[NPL][NF];
-#pragma unroll
-    for (int k = 0; k < NPL; ++k)
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            Real v = -dUi[k][f];
-            if (P.blending) v *= (Real(1) - alpha);
-            if (NS) v += dUv[k][f];
-            acc[k][f] = v * mJ;
-        }
-
-    // ---- subcell first-order FV (DGSEMIntegrator.cpp:972-1196), skipped when alpha == 0
-    if (P.blending && alpha != Real(0)) {
-        Real fv[NPL][NF];
-#pragma unroll
-        for (int dir = 0; dir < DIM; ++dir) {
-            Real nor[DIM];
-#pragma unroll
-            for (int q = 0; q < DIM; ++q) nor[q] = adj[dir][q];
-            for (int it = li; it < NID; it += GS) {
-                const int ln = it / (NP - 1), ii = it - ln * (NP - 1);
-                int base, stride;
-                line_base<DIM, NP>(dir, ln, base, stride);
-                const int n1 = base + ii * stride, n2 = n1 + stride;
-                const Prim<DIM, Real> q1 = load_prim<DIM, ND, Real>(sH, n1), q2 = load_prim<DIM, ND, Real>(sH, n2);
-                Real s1[NF], s2[NF], F[NF];
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) { s1[1 + d] = q1.rho * q1.v[d]; s2[1 + d] = q2.rho * q2.v[d]; }
-                face_flux<DIM, Real>(s1, q1, s2, q2, nor, gm1i, P.quirks == 0, true, F);
-#pragma unroll
-                for (int f = 0; f < NF; ++f) sF[f * NID + it] = F[f];
-            }
-            __syncwarp();
-#pragma unroll
-            for (int k = 0; k < NPL; ++k) {
-                const int n = li + k * GS;
-                if (n < ND) {
-                    int c[3];
-                    node_coords<NP>(n, c);
-                    const int pos = c[dir];
-                    const int ib = line_index<DIM, NP>(dir, c) * (NP - 1);
-                    const Real mw = Real(1.0 / (J * double(sW[pos])));
-#pragma unroll
-                    for (int f = 0; f < NF; ++f) {
-                        Real v;
-                        if (pos == 0) v = -sF[f * NID + ib];
-                        else if (pos == NP - 1) v = sF[f * NID + ib + pos - 1];
-                        else v = sF[f * NID + ib + pos - 1] - sF[f * NID + ib + pos];
-                        v *= mw;
-                        fv[k][f] = (dir == 0) ? v : fv[k][f] + v;
-                    }
-                }
-            }
-            __syncwarp();
-        }
-#pragma unroll
-        for (int k = 0; k < NPL; ++k)
-#pragma unroll
-            for (int f = 0; f < NF; ++f) acc[k][f] = fv[k][f] * alpha + acc[k][f];
-    }
-
-    // ---- surface fluxes of the element's own faces; neighbour traces from global/L2
-    const Real aw = Real(1.0 / (double(sW[0]) * J));
-    for (int it = li; it < NFI; it += GS) {
-        const int lf = it / NFN, fa = it - lf * NFN;
-        const int no = face_node<DIM, NP>(lf, fa);
-        const int4 t = __ldg(m.nbr + (long long)e * (2 * DIM) + lf);
-        const long long gn = (long long)t.x * ND + face_node<DIM, NP>(t.y, fa);
-        const long long go = (long long)e * ND + no;
-        const bool own_is_1 = (t.w == 0);
-        double so[NF], sn[NF];
-        Real nor[DIM], flux[NF], fn[NF], mo[NF], mn[NF];
-#pragma unroll
-        for (int f = 0; f < NF; ++f) { so[f] = __ldg(a.u + f * Ndof + go); sn[f] = __ldg(a.u + f * Ndof + gn); }
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) nor[q] = Real(__ldg(m.fnor + (long long)t.z * DIM + q));
-        Prim<DIM, Real> po = load_prim<DIM, ND, Real>(sH, no);
-        const Prim<DIM, double> pn64 = primitives<DIM, double>(sn, gamma, gm1);
-        Prim<DIM, Real> pn = cast_prim<DIM, Real>(pn64);
-#pragma unroll
-        for (int f = 0; f < NF; ++f) fn[f] = 0;
-        if constexpr (NS) {
-            // DGSEMIntegrator.cpp:435-549: 0.5 (Fv1 + Fv2) . n from each trace's
-            // own state and lifted gradients
-#pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                const long long g = side == 0 ? go : gn;
-                const Prim<DIM, Real> &q = side == 0 ? po : pn;
-                Real dq[DIM][NF];
-#pragma unroll
-                for (int d = 0; d < DIM; ++d)
-#pragma unroll
-                    for (int f = 0; f < NF; ++f) dq[d][f] = __ldg(grad + (d * NF + f) * Ndof + g);
-                viscous_flux<DIM, Real>(q.rho, q.rrho, q.v, Real(0.5) * q.rbeta * q.rho, dq, P,
-                                        [&](int f, int cc, Real val) { fn[f] += (Real(0.5) * val) * nor[cc]; });
-            }
-            if (P.quirks == 0) {
-                // Q8 (BasicOperations.cpp:33-34 via NavierStokesFlux.cpp:14): the face
-                // Riemann flux reads states whose momentum slots now hold velocity.
-                const Prim<DIM, double> po64 = primitives<DIM, double>(so, gamma, gm1);
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) { so[1 + d] *= po64.rrho; sn[1 + d] *= pn64.rrho; }
-                po = cast_prim<DIM, Real>(primitives<DIM, double>(so, gamma, gm1));
-                pn = cast_prim<DIM, Real>(primitives<DIM, double>(sn, gamma, gm1));
-            }
-        }
-#pragma unroll
-        for (int f = 0; f < NF; ++f) { mo[f] = Real(so[f]); mn[f] = Real(sn[f]); }
-        if (own_is_1)
-            face_flux<DIM, Real>(mo, po, mn, pn, nor, gm1i, P.quirks == 0, P.dissipation != 0, flux);
-        else
-            face_flux<DIM, Real>(mn, pn, mo, po, nor, gm1i, P.quirks == 0, P.dissipation != 0, flux);
-#pragma unroll
-        for (int f = 0; f < NF; ++f) sF[f * NFI + it] = aw * (own_is_1 ? (fn[f] - flux[f]) : (flux[f] - fn[f]));
-    }
-    __syncwarp();
-
-    // ---- gather face terms, epilogue (FP64 state update)
-    if (!active) return;
-#pragma unroll
-    for (int k = 0; k < NPL; ++k) {
-        const int n = li + k * GS;
-        if (n >= ND) continue;
-        int c[3];
-        node_coords<NP>(n, c);
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            int lf = -1;
-            if (c[d] == 0) lf = 2 * d;
-            else if (c[d] == NP - 1) lf = 2 * d + 1;
-            if (lf >= 0) {
-                const int it = lf * NFN + face_tangential<DIM, NP>(d, c);
-#pragma unroll
-                for (int f = 0; f < NF; ++f) acc[k][f] += sF[f * NFI + it];
-            }
-        }
-        const long long gnode = (long long)e * ND + n;
-        switch (a.mode) {
-        case EPI_STORE:
-#pragma unroll
-            for (int f = 0; f < NF; ++f) a.dudt[f * Ndof + gnode] = double(acc[k][f]);
-            break;
-        case EPI_LSRK:
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const long long g = f * Ndof + gnode;
-                const double L = double(acc[k][f]);
-                const double dv = (a.rkA == 0.0) ? a.dt * L : a.rkA * a.du[g] + a.dt * L;
-                a.du[g] = dv;
-                a.u_out[g] = __ldg(a.u + g) + a.rkB * dv;
-            }
-            break;
-        case EPI_SSP1:
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const long long g = f * Ndof + gnode;
-                a.u_out[g] = __ldg(a.u + g) + a.dt * double(acc[k][f]);
-            }
-            break;
-        case EPI_SSP2:
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const long long g = f * Ndof + gnode;
-                const double y = __ldg(a.u + g) + a.dt * double(acc[k][f]);
-                a.u_out[g] = 3. / 4 * a.x0[g] + 1. / 4 * y;
-            }
-            break;
-        case EPI_SSP3:
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const long long g = f * Ndof + gnode;
-                const double y = __ldg(a.u + g) + a.dt * double(acc[k][f]);
-                a.u_out[g] = 1. / 3 * a.x0[g] + 2. / 3 * y;
-            }
-            break;
-        default:
-            break;
-        }
-    }
-}
-
-// ------------------------------------------------------------ BR1 lifting
-// Entropy variables (BasicOperations.cpp:81-104), element gradient
-// (LiftingBR1.cpp:156-272), face lifting 1/2 (v2 - v1) n (LiftingBR1.cpp:10-115)
-// and the chain rule to primitive gradients (BasicOperations.cpp:126-170).
-// The arithmetic is FP64 in both forms (it is per node and cheap); the lifted
-// gradients are stored in the working precision Out (double, or float for the
-// FP32-bulk form).
-template <int DIM, int NP, typename Out>
-__global__ void __launch_bounds__(Shape<DIM, NP>::THREADS, 4)
-lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_constant__ OpTables T) {
-    using S = Shape<DIM, NP>;
-    constexpr int ND = S::ND, NF = S::NF, NFN = S::NFN, NFI = S::NFI;
-    constexpr int PER_ELEM = 2 * NF * ND + DIM * NF * NFI;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *smem = reinterpret_cast<double *>(smem_raw);
-    double *sT = smem;
-    const double *sD = sT, *sW = sT + 4 * NP * NP;
-    load_tables<NP, double>(T, sT, threadIdx.x, S::THREADS);
-    Out *gout = sizeof(Out) == 8 ? reinterpret_cast<Out *>(a.grad) : reinterpret_cast<Out *>(a.grad32);
-
-    const int el = threadIdx.x / ND;
-    const int n = threadIdx.x - el * ND;
-    const int e_raw = blockIdx.x * S::EPB + el;
-    const bool active = e_raw < m.E;
-    const int e = active ? e_raw : m.E - 1;
-    double *sU = smem + S::TAB + el * PER_ELEM;
-    double *sVe = sU + NF * ND;
-    double *sS = sVe + NF * ND;
-    const long long Ndof = m.Ndof;
-    const long long gnode = (long long)e * ND + n;
-    double st[NF], v[NF];
-#pragma unroll
-    for (int f = 0; f < NF; ++f) {
-        st[f] = __ldg(a.u + f * Ndof + gnode);
-        sU[f * ND + n] = st[f];
-    }
-    conserv2entropy<DIM, double>(st, P, v);
-#pragma unroll
-    for (int f = 0; f < NF; ++f) sVe[f * ND + n] = v[f];
-    const double *geo = m.geo + (long long)e * (DIM * DIM + 1);
-    double adj[DIM][DIM];
-#pragma unroll
-    for (int r = 0; r < DIM; ++r)
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) adj[r][q] = __ldg(geo + r * DIM + q);
-    const double J = __ldg(geo + DIM * DIM);
-    int c[3];
-    node_coords<NP>(n, c);
-
-    // face part first (its neighbour loads overlap the element part):
-    // +1/(w0 J) * 1/2 (v_elem2 - v_elem1) * n_c on both sides
-    __syncthreads();   // tables and entropy variables complete
-    const double aw = 1.0 / (sW[0] * J);
-    for (int it = n; it < NFI; it += ND) {
-        const int lf = it / NFN, fa = it - lf * NFN;
-        const int no = face_node<DIM, NP>(lf, fa);
-        const int4 t = __ldg(m.nbr + (long long)e * (2 * DIM) + lf);
-        const int nn = face_node<DIM, NP>(t.y, fa);
-        const long long gn = (long long)t.x * ND + nn;
-        double sn[NF], vn[NF], nor[DIM];
-#pragma unroll
-        for (int f = 0; f < NF; ++f) sn[f] = __ldg(a.u + f * Ndof + gn);
-        conserv2entropy<DIM, double>(sn, P, vn);
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) nor[q] = __ldg(m.fnor + (long long)t.z * DIM + q);
-        const bool own_is_1 = (t.w == 0);
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            const double vo = sVe[f * ND + no];
-            const double jf = own_is_1 ? 0.5 * (vn[f] - vo) : 0.5 * (vo - vn[f]);
-#pragma unroll
-            for (int q = 0; q < DIM; ++q) sS[(q * NF + f) * NFI + it] = aw * (jf * nor[q]);
-        }
-    }
-
-    // element part: g1(f, r) = sum_l D(pos_r, l) v_l along direction r
-    double g1[NF][DIM];
-#pragma unroll
-    for (int f = 0; f < NF; ++f)
-#pragma unroll
-        for (int r = 0; r < DIM; ++r) g1[f][r] = 0.0;
-#pragma unroll
-    for (int r = 0; r < DIM; ++r) {
-        int base, stride;
-        line_base<DIM, NP>(r, line_index<DIM, NP>(r, c), base, stride);
-#pragma unroll
-        for (int l = 0; l < NP; ++l) {
-            const double dl = sD[c[r] * NP + l];
-#pragma unroll
-            for (int f = 0; f < NF; ++f) g1[f][r] += sVe[f * ND + base + l * stride] * dl;
-        }
-    }
-    // grad_mat2 = grad_mat1 * adj, times 1/J (LiftingBR1.cpp:205-206)
-    const double mJ = 1.0 / J;
-    double g[DIM][NF];
-#pragma unroll
-    for (int q = 0; q < DIM; ++q)
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            double s = 0.0;
-#pragma unroll
-            for (int r = 0; r < DIM; ++r) s += g1[f][r] * adj[r][q];
-            g[q][f] = s * mJ;
-        }
-    __syncthreads();
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-        int lf = -1;
-        if (c[d] == 0) lf = 2 * d;
-        else if (c[d] == NP - 1) lf = 2 * d + 1;
-        if (lf >= 0) {
-            const int it = lf * NFN + face_tangential<DIM, NP>(d, c);
-#pragma unroll
-            for (int q = 0; q < DIM; ++q)
-#pragma unroll
-                for (int f = 0; f < NF; ++f) g[q][f] += sS[(q * NF + f) * NFI + it];
-        }
-    }
-    if (!active) return;
-#pragma unroll
-    for (int q = 0; q < DIM; ++q) {
-        entropygrad2primgrad<DIM, double>(st, P, g[q]);
-#pragma unroll
-        for (int f = 0; f < NF; ++f) gout[(q * NF + f) * Ndof + gnode] = Out(g[q][f]);
-    }
-}
-
-template <int DIM, int NP, bool NS, typename Real>
-size_t rhs_smem() {
-    using LY = RhsLayout<DIM, NP, NS, Real>;
-    return sizeof(Real) * (Shape<DIM, NP>::TAB + (size_t)LY::EPB * LY::PER_ELEM);
-}
-template <int DIM, int NP>
-size_t lift_smem() {
-    using S = Shape<DIM, NP>;
-    constexpr int PER_ELEM = 2 * S::NF * S::ND + DIM * S::NF * S::NFI;
-    return sizeof(double) * (S::TAB + (size_t)S::EPB * PER_ELEM);
-}
-
-template <int DIM, int NP, bool NS, typename Real>
-cudaError_t rhs_launch_ns(const MeshDev &m, const RhsArgs &a, const PhysParams &P, const OpTables &T,
-                          cudaStream_t s) {
-    using LY = RhsLayout<DIM, NP, NS, Real>;
-    const int grid = (m.E + LY::EPB - 1) / LY::EPB;
-    const size_t sm = rhs_smem<DIM, NP, NS, Real>();
-    cudaError_t err = cudaFuncSetAttribute(rhs_kernel<DIM, NP, NS, Real>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (err != cudaSuccess) return err;
-    rhs_kernel<DIM, NP, NS, Real><<<grid, LY::THREADS, sm, s>>>(m, a, P, T);
-    return cudaGetLastError();
-}
-template <int DIM, int NP, typename Real>
-cudaError_t rhs_launch_t(bool ns, const MeshDev &m, const RhsArgs &a, const PhysParams &P,
-                         const OpTables &T, cudaStream_t s) {
-    return ns ? rhs_launch_ns<DIM, NP, true, Real>(m, a, P, T, s) : rhs_launch_ns<DIM, NP, false, Real>(m, a, P, T, s);
-}
-template <int DIM, int NP, typename Out>
-cudaError_t lift_launch_t(const MeshDev &m, const LiftArgs &a, const PhysParams &P,
-                          const OpTables &T, cudaStream_t s) {
-    using S = Shape<DIM, NP>;
-    const int grid = (m.E + S::EPB - 1) / S::EPB;
-    const size_t sm = lift_smem<DIM, NP>();
-    cudaError_t err = cudaFuncSetAttribute(lift_kernel<DIM, NP, Out>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (err != cudaSuccess) return err;
-    lift_kernel<DIM, NP, Out><<<grid, S::THREADS, sm, s>>>(m, a, P, T);
-    return cudaGetLastError();
-}
-
-}   // namespace
 
 bool order_supported(int dim, int order) {
     return (dim == 2 || dim == 3) && order >= 1 && order <= 5;
 }
 
-#define PRANDTL_DISPATCH(DIMV, FN, REAL, ...)                            \
-    switch (order) {                                                     \
-    case 1: return FN<DIMV, 2, REAL>(__VA_ARGS__);                       \
-    case 2: return FN<DIMV, 3, REAL>(__VA_ARGS__);                       \
-    case 3: return FN<DIMV, 4, REAL>(__VA_ARGS__);                       \
-    case 4: return FN<DIMV, 5, REAL>(__VA_ARGS__);                       \
-    case 5: return FN<DIMV, 6, REAL>(__VA_ARGS__);                       \
-    default: return cudaErrorInvalidValue;                               \
-    }
+#define PRANDTL_DIM_NS(FN, REAL, ...)                                              \
+    do {                                                                           \
+        if (dim == 2) return ns ? FN<2, REAL, true>(__VA_ARGS__) : FN<2, REAL, false>(__VA_ARGS__); \
+        if (dim == 3) return ns ? FN<3, REAL, true>(__VA_ARGS__) : FN<3, REAL, false>(__VA_ARGS__); \
+        return cudaErrorInvalidValue;                                              \
+    } while (0)
+#define PRANDTL_DIM(FN, OUT, ...)                                                  \
+    do {                                                                           \
+        if (dim == 2) return FN<2, OUT>(__VA_ARGS__);                              \
+        if (dim == 3) return FN<3, OUT>(__VA_ARGS__);                              \
+        return cudaErrorInvalidValue;                                              \
+    } while (0)
 
 cudaError_t launch_rhs(int dim, int order, bool ns, const MeshDev &m, const RhsArgs &a,
                        const PhysParams &P, const OpTables &T, cudaStream_t s) {
     if (m.E <= 0) return cudaSuccess;
-    if (dim == 2) { PRANDTL_DISPATCH(2, rhs_launch_t, double, ns, m, a, P, T, s) }
-    if (dim == 3) { PRANDTL_DISPATCH(3, rhs_launch_t, double, ns, m, a, P, T, s) }
-    return cudaErrorInvalidValue;
+    PRANDTL_DIM_NS(rhs_dispatch, double, order, m, a, P, T, s);
 }
-
-cudaError_t launch_lift(int dim, int order, const MeshDev &m, const LiftArgs &a,
-                        const PhysParams &P, const OpTables &T, cudaStream_t s) {
-    if (m.E <= 0) return cudaSuccess;
-    if (dim == 2) { PRANDTL_DISPATCH(2, lift_launch_t, double, m, a, P, T, s) }
-    if (dim == 3) { PRANDTL_DISPATCH(3, lift_launch_t, double, m, a, P, T, s) }
-    return cudaErrorInvalidValue;
-}
-
 cudaError_t launch_rhs_fp32(int dim, int order, bool ns, const MeshDev &m, const RhsArgs &a,
                             const PhysParams &P, const OpTables &T, cudaStream_t s) {
     if (m.E <= 0) return cudaSuccess;
-    if (dim == 2) { PRANDTL_DISPATCH(2, rhs_launch_t, float, ns, m, a, P, T, s) }
-    if (dim == 3) { PRANDTL_DISPATCH(3, rhs_launch_t, float, ns, m, a, P, T, s) }
-    return cudaErrorInvalidValue;
+    PRANDTL_DIM_NS(rhs_dispatch, float, order, m, a, P, T, s);
 }
-
+cudaError_t launch_lift(int dim, int order, const MeshDev &m, const LiftArgs &a,
+                        const PhysParams &P, const OpTables &T, cudaStream_t s) {
+    if (m.E <= 0) return cudaSuccess;
+    PRANDTL_DIM(lift_dispatch, double, order, m, a, P, T, s);
+}
 cudaError_t launch_lift_fp32(int dim, int order, const MeshDev &m, const LiftArgs &a,
                              const PhysParams &P, const OpTables &T, cudaStream_t s) {
     if (m.E <= 0) return cudaSuccess;
-    if (dim == 2) { PRANDTL_DISPATCH(2, lift_launch_t, float, m, a, P, T, s) }
-    if (dim == 3) { PRANDTL_DISPATCH(3, lift_launch_t, float, m, a, P, T, s) }
-    return cudaErrorInvalidValue;
+    PRANDTL_DIM(lift_dispatch, float, order, m, a, P, T, s);
+}
+
+int batch_num_variants() { return 3; }
+
+cudaError_t batch_prepare_rhs(int dim, int order, bool ns, bool fp32, int variant, BatchKernelInfo *info) {
+    if (fp32) PRANDTL_DIM_NS(rhs_batch_prepare, float, order, variant, info);
+    PRANDTL_DIM_NS(rhs_batch_prepare, double, order, variant, info);
+}
+cudaError_t batch_prepare_lift(int dim, int order, bool fp32, BatchKernelInfo *info) {
+    if (fp32) PRANDTL_DIM(lift_batch_prepare, float, order, info);
+    PRANDTL_DIM(lift_batch_prepare, double, order, info);
+}
+cudaError_t batch_launch_rhs(int dim, int order, bool ns, bool fp32, int variant, int grid,
+                             const BatchClassDev &c, const BatchStage &st, const OpTables &T, cudaStream_t s) {
+    if (fp32) PRANDTL_DIM_NS(rhs_batch_launch, float, order, variant, grid, c, st, T, s);
+    PRANDTL_DIM_NS(rhs_batch_launch, double, order, variant, grid, c, st, T, s);
+}
+cudaError_t batch_launch_lift(int dim, int order, bool fp32, int grid, const BatchClassDev &c,
+                              const BatchStage &st, const OpTables &T, cudaStream_t s) {
+    if (fp32) PRANDTL_DIM(lift_batch_launch, float, order, grid, c, st, T, s);
+    PRANDTL_DIM(lift_batch_launch, double, order, grid, c, st, T, s);
+}
+
+namespace {
+// Simulation.cpp:1013-1018: dt = cfl * hmin / (lambda_max * (N+1)^2), here per
+// solve from the largest |V|+c seen during its last step.
+__global__ void batch_step_end_kernel(BatchInst *tab, const int *live, const int *n_live, int flip, int *left) {
+    const int n = *n_live;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int id = live[q];
+        BatchInst &I = tab[id];
+        if (I.steps_left <= 0) continue;
+        I.steps_left -= 1;
+        left[id] = I.steps_left;
+        I.steps_done += 1;
+        I.cur ^= flip;
+        const unsigned long long bits = I.lambda;
+        I.lambda_last = bits;
+        I.lambda = 0ull;
+        const double lam = __longlong_as_double((long long)bits);
+        if (I.cfl > 0.0 && lam > 0.0 && lam < 1e300) {
+            const double np = double(I.order + 1);
+            I.dt = I.cfl * I.hmin / (lam * np * np);
+        }
+    }
+}
+}   // namespace
+
+cudaError_t batch_launch_step_end(BatchInst *tab, const int *live, const int *n_live, int flip, int *left,
+                                  cudaStream_t s) {
+    batch_step_end_kernel<<<8, 256, 0, s>>>(tab, live, n_live, flip, left);
+    return cudaGetLastError();
 }
 
 }   // namespace prandtl

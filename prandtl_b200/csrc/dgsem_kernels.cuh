@@ -44,6 +44,51 @@ struct LiftArgs {
     float *grad32;          // FP32-bulk form
 };
 
+// ---------------------------------------------------------------- batches
+// Device record of one resident solve in a batch.  The host writes it on
+// admission; the step kernel advances steps_left / cur / dt; the RHS kernels
+// fold max |V|+c into lambda.
+enum BatchScheme : int { BATCH_SSPRK3 = 0, BATCH_LSRK45 = 1 };
+constexpr int BATCH_CHUNK = 64;   // per-solve element ranges are padded to this in the work prefix
+
+struct BatchInst {
+    PhysParams P;
+    const double *geo;          // [E][DIM*DIM + 1]
+    const int4 *nbr;            // [E][2*DIM] (solve-local element and face ids)
+    const double *fnor;         // [F][DIM]
+    double *u[3];               // LSRK: state ping-pong u[0], u[1] and the register u[2];
+                                // SSP-RK3: x, y1, y2
+    void *grad;                 // NS gradients (double or float)
+    double *alpha;              // [E] or null
+    long long Ndof;             // E * Np^DIM
+    int E, order;
+    double dt;                  // current time step
+    double cfl, hmin;           // cfl > 0: dt = cfl hmin / (lambda (N+1)^2) after every step
+    int steps_left;             // > 0: the solve advances; 0: frozen
+    int steps_done;
+    int cur;                    // LSRK: u[cur] holds the state at the start of the step
+    int pad;
+    unsigned long long lambda;  // max |V|+c over the current step's stages (ordered bits)
+    unsigned long long lambda_last;   // ... of the last completed step
+};
+// One (dim, order, physics) class of a batch: its solves and the padded
+// element prefix over them (prefix[s+1] - prefix[s] = E of slot s rounded up
+// to BATCH_CHUNK).  hdr[0] = number of slots.
+struct BatchClassDev {
+    BatchInst *tab;
+    const int *ids;
+    const int *prefix;
+    const int *hdr;
+};
+struct BatchStage {
+    int scheme;                 // BatchScheme
+    int stage;                  // stage index within the step
+    double rkA, rkB;            // LSRK coefficients of the stage
+};
+struct BatchKernelInfo {
+    int blocks_per_sm, threads, smem, regs, elems_per_item;
+};
+
 // Launchers (dispatch on dim and order).  Return cudaSuccess or the launch error.
 cudaError_t launch_rhs(int dim, int order, bool ns, const MeshDev &m, const RhsArgs &a,
                        const PhysParams &P, const OpTables &T, cudaStream_t s);
@@ -55,5 +100,38 @@ cudaError_t launch_rhs_fp32(int dim, int order, bool ns, const MeshDev &m, const
 cudaError_t launch_lift_fp32(int dim, int order, const MeshDev &m, const LiftArgs &a,
                              const PhysParams &P, const OpTables &T, cudaStream_t s);
 bool order_supported(int dim, int order);
+
+// Batch kernels of one class.  `variant` in [0, batch_num_variants()) picks the
+// RHS launch shape.  prepare_* must run outside stream capture.
+int batch_num_variants();
+cudaError_t batch_prepare_rhs(int dim, int order, bool ns, bool fp32, int variant, BatchKernelInfo *info);
+cudaError_t batch_prepare_lift(int dim, int order, bool fp32, BatchKernelInfo *info);
+cudaError_t batch_launch_rhs(int dim, int order, bool ns, bool fp32, int variant, int grid,
+                             const BatchClassDev &c, const BatchStage &st, const OpTables &T, cudaStream_t s);
+cudaError_t batch_launch_lift(int dim, int order, bool fp32, int grid, const BatchClassDev &c,
+                              const BatchStage &st, const OpTables &T, cudaStream_t s);
+// End of a batch step: every live solve with steps left advances its counters,
+// flips its LSRK parity, (cfl > 0) takes its next dt from lambda, and writes
+// its remaining step count to left[id].
+cudaError_t batch_launch_step_end(BatchInst *tab, const int *live, const int *n_live, int flip, int *left,
+                                  cudaStream_t s);
+
+// Per-(dim, working precision, physics) dispatchers, one translation unit each.
+template <int DIM, typename Real, bool NS>
+cudaError_t rhs_dispatch(int order, const MeshDev &m, const RhsArgs &a, const PhysParams &P,
+                         const OpTables &T, cudaStream_t s);
+template <int DIM, typename Out>
+cudaError_t lift_dispatch(int order, const MeshDev &m, const LiftArgs &a, const PhysParams &P,
+                          const OpTables &T, cudaStream_t s);
+template <int DIM, typename Real, bool NS>
+cudaError_t rhs_batch_prepare(int order, int variant, BatchKernelInfo *info);
+template <int DIM, typename Real, bool NS>
+cudaError_t rhs_batch_launch(int order, int variant, int grid, const BatchClassDev &c, const BatchStage &st,
+                             const OpTables &T, cudaStream_t s);
+template <int DIM, typename Out>
+cudaError_t lift_batch_prepare(int order, BatchKernelInfo *info);
+template <int DIM, typename Out>
+cudaError_t lift_batch_launch(int order, int grid, const BatchClassDev &c, const BatchStage &st,
+                              const OpTables &T, cudaStream_t s);
 
 }   // namespace prandtl

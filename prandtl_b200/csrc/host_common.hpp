@@ -1,0 +1,187 @@
+// host_common.hpp -- host-side helpers shared by the operator handle, the
+// no-allocation entry point and batches: the 1D operator tables, the physics
+// constants and the validation of a mesh descriptor into the neighbour table.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/prandtl_b200.h"
+#include "dgsem_kernels.cuh"
+
+namespace prandtl {
+namespace host {
+
+// ---- 1D tables (mirrors DGSEMIntegrator.cpp:41-82 and ModalBasis.cpp:110-135)
+inline long double legendre_ld(int n, long double x, long double *dp) {
+    long double p0 = 1.0L, p1 = x, dp0 = 0.0L, dp1 = 1.0L;
+    if (n == 0) { *dp = 0.0L; return 1.0L; }
+    for (int k = 1; k < n; ++k) {
+        long double p2 = ((2 * k + 1) * x * p1 - k * p0) / (k + 1);
+        long double dp2 = dp0 + (2 * k + 1) * p1;
+        p0 = p1; p1 = p2; dp0 = dp1; dp1 = dp2;
+    }
+    *dp = dp1;
+    return p1;
+}
+
+inline void build_tables(int N, OpTables &T) {
+    const int Np = N + 1;
+    std::memset(&T, 0, sizeof(T));
+    // Gauss-Lobatto nodes/weights on [0,1]
+    const long double pi = 3.14159265358979323846264338327950288L;
+    std::vector<long double> xs(Np);
+    for (int i = 0; i < Np; ++i) {
+        long double xi = -cosl(pi * i / N);
+        if (i > 0 && i < N)
+            for (int it = 0; it < 100; ++it) {
+                long double dP, P = legendre_ld(N, xi, &dP);
+                long double dx = ((1.0L - xi * xi) * dP) / (-(long double)N * (N + 1) * P);
+                xi -= dx;
+                if (fabsl(dx) < 1e-30L) break;
+            }
+        xs[i] = xi;
+    }
+    for (int i = 0; i < Np; ++i) {
+        long double dP, P = legendre_ld(N, xs[i], &dP);
+        T.x[i] = (double)((xs[i] + 1.0L) * 0.5L);
+        T.w[i] = (double)(2.0L / ((long double)N * (N + 1) * P * P) * 0.5L);
+    }
+    T.x[0] = 0.0;
+    T.x[N] = 1.0;
+    // barycentric differentiation matrix
+    std::vector<double> wb(Np, 1.0);
+    for (int i = 1; i < Np; ++i)
+        for (int j = 0; j < i; ++j) {
+            wb[j] *= (T.x[j] - T.x[i]);
+            wb[i] *= (T.x[i] - T.x[j]);
+        }
+    for (int i = 0; i < Np; ++i) wb[i] = 1.0 / wb[i];
+    for (int iL = 0; iL < Np; ++iL)
+        for (int i = 0; i < Np; ++i)
+            if (iL != i) {
+                T.D[i * Np + iL] = wb[iL] / wb[i] / (T.x[i] - T.x[iL]);
+                T.D[i * Np + i] -= T.D[i * Np + iL];
+            }
+    for (int q = 0; q < Np * Np; ++q) {
+        T.Dhat[q] = T.D[q];
+        T.Dhat2[q] = 2.0 * T.D[q];
+    }
+    T.Dhat[0] += 1.0 / T.w[0];
+    T.Dhat[(Np - 1) * Np + Np - 1] -= 1.0 / T.w[Np - 1];
+    T.Dhat2[0] += 1.0 / T.w[0];
+    T.Dhat2[(Np - 1) * Np + Np - 1] -= 1.0 / T.w[Np - 1];
+    // 1D Vandermonde of shifted Legendre P_a(2x-1): V[l][a], inverted (Gauss-Jordan)
+    std::vector<double> V(Np * Np), I(Np * Np, 0.0);
+    for (int l = 0; l < Np; ++l) {
+        double u[8], z = 2.0 * T.x[l] - 1.0;
+        u[0] = 1.0;
+        if (N >= 1) u[1] = z;
+        for (int n = 1; n < N; ++n) u[n + 1] = ((2 * n + 1) * z * u[n] - n * u[n - 1]) / (n + 1);
+        for (int a = 0; a < Np; ++a) V[l * Np + a] = u[a];
+    }
+    for (int i = 0; i < Np; ++i) I[i * Np + i] = 1.0;
+    for (int c = 0; c < Np; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < Np; ++r)
+            if (std::fabs(V[r * Np + c]) > std::fabs(V[piv * Np + c])) piv = r;
+        for (int k = 0; k < Np; ++k) {
+            std::swap(V[c * Np + k], V[piv * Np + k]);
+            std::swap(I[c * Np + k], I[piv * Np + k]);
+        }
+        const double d = 1.0 / V[c * Np + c];
+        for (int k = 0; k < Np; ++k) { V[c * Np + k] *= d; I[c * Np + k] *= d; }
+        for (int r = 0; r < Np; ++r) {
+            if (r == c) continue;
+            const double f = V[r * Np + c];
+            for (int k = 0; k < Np; ++k) { V[r * Np + k] -= f * V[c * Np + k]; I[r * Np + k] -= f * I[c * Np + k]; }
+        }
+    }
+    // I = V^{-1}: I[a][l] maps nodal values (l) to mode a
+    for (int q = 0; q < Np * Np; ++q) T.Vinv[q] = I[q];
+}
+
+inline void build_phys(const prandtl_config &c, int N, PhysParams &P) {
+    P.gamma = c.gamma;
+    P.gammaM1 = c.gamma - 1.0;
+    P.gammaM1Inverse = 1.0 / P.gammaM1;
+    P.PrInverse = 1.0 / c.Pr;
+    P.mu = c.mu;
+    P.mu_bulk = 2.0 / 3.0;     // Physics.hpp:34
+    P.R_gas = c.R_gas;
+    P.mu0 = 1.716e-5;          // Physics.hpp:35-37
+    P.T0 = 273.15;
+    P.Ts = 110.4;
+    P.T0pTs = P.T0 + P.Ts;
+    P.alpha_max = c.alpha_max;
+    P.alpha_min = c.alpha_min;
+    P.modal_threshold = 0.5 * std::pow(10.0, -1.8 * std::pow((double)N, 0.25));   // DGSEMOperator.cpp:25
+    P.sutherland = c.sutherland;
+    P.quirks = c.quirks;
+    P.dissipation = c.surface_dissipation;
+    P.blending = c.blending;
+}
+
+
+// Checks a mesh descriptor and builds the neighbour table nbr[e][lf] =
+// {neighbour element, its local face, face id, role (0: e is Elem1)}.  Every
+// element face must be an interior face exactly once, with the traces aligned
+// (local faces 2*dir and 2*dir+1 of the same direction).
+inline prandtl_status validate_mesh(const prandtl_mesh_desc *md, std::vector<int4> &nbr, std::string &msg) {
+    if (md->dim != 2 && md->dim != 3) { msg = "dim must be 2 or 3"; return PRANDTL_EUNSUPPORTED; }
+    if (!order_supported(md->dim, md->order)) { msg = "order must be in 1..5"; return PRANDTL_EUNSUPPORTED; }
+    if (md->num_elements <= 0 || md->num_faces < 0) { msg = "bad sizes"; return PRANDTL_EINVAL; }
+    if (!md->elem_adj || !md->elem_detj || (md->num_faces > 0 && (!md->face_elems || !md->face_nor))) {
+        msg = "mesh arrays missing";
+        return PRANDTL_EINVAL;
+    }
+    const int NFACE = 2 * md->dim, E = md->num_elements, F = md->num_faces;
+    nbr.assign((size_t)E * NFACE, make_int4(-1, -1, -1, -1));
+    for (int f = 0; f < F; ++f) {
+        const int *fe = md->face_elems + 4 * f;
+        const int e1 = fe[0], l1 = fe[1], e2 = fe[2], l2 = fe[3];
+        if (e1 < 0 || e1 >= E || e2 < 0 || e2 >= E || l1 < 0 || l1 >= NFACE || l2 < 0 || l2 >= NFACE) {
+            msg = "face " + std::to_string(f) + " out of range";
+            return PRANDTL_EINVAL;
+        }
+        if ((l1 >> 1) != (l2 >> 1) || (l1 ^ l2) != 1) {
+            msg = "face " + std::to_string(f) + ": only aligned opposite faces are supported";
+            return PRANDTL_EUNSUPPORTED;
+        }
+        int4 &a = nbr[(size_t)e1 * NFACE + l1];
+        int4 &b = nbr[(size_t)e2 * NFACE + l2];
+        if (a.x >= 0 || b.x >= 0) {
+            msg = "element face listed twice (face " + std::to_string(f) + ")";
+            return PRANDTL_EINVAL;
+        }
+        a = make_int4(e2, l2, f, 0);
+        b = make_int4(e1, l1, f, 1);
+    }
+    for (size_t q = 0; q < nbr.size(); ++q)
+        if (nbr[q].x < 0) {
+            msg = "element " + std::to_string(q / NFACE) + " has a boundary face; only periodic meshes are built";
+            return PRANDTL_EUNSUPPORTED;
+        }
+    for (int e = 0; e < E; ++e)
+        if (!(md->elem_detj[e] > 0.0)) { msg = "non-positive det J"; return PRANDTL_EINVAL; }
+    return PRANDTL_OK;
+}
+
+// Geometry rows [E][dim*dim + 1]: adj(J) row-major, then det J.
+inline std::vector<double> geometry_rows(const prandtl_mesh_desc *md) {
+    const int dim = md->dim, GEO = dim * dim + 1, E = md->num_elements;
+    std::vector<double> geo((size_t)E * GEO);
+    for (int e = 0; e < E; ++e) {
+        for (int q = 0; q < dim * dim; ++q) geo[(size_t)e * GEO + q] = md->elem_adj[(size_t)e * dim * dim + q];
+        geo[(size_t)e * GEO + dim * dim] = md->elem_detj[e];
+    }
+    return geo;
+}
+
+}   // namespace host
+}   // namespace prandtl

@@ -16,8 +16,10 @@
 
 #include "../../include/prandtl_b200.h"
 #include "dgsem_kernels.cuh"
+#include "host_common.hpp"
 
 using namespace prandtl;
+using namespace prandtl::host;
 
 struct prandtl_handle {
     int dim = 0, order = 0, Np = 0, nd = 0, nf = 0, E = 0, F = 0;
@@ -72,116 +74,6 @@ prandtl_status cuda_fail(prandtl_handle *h, cudaError_t e, const char *what) {
         cudaError_t _e = (call);                            \
         if (_e != cudaSuccess) return cuda_fail(h, _e, what); \
     } while (0)
-
-// ---- 1D tables (mirrors DGSEMIntegrator.cpp:41-82 and ModalBasis.cpp:110-135)
-long double legendre_ld(int n, long double x, long double *dp) {
-    long double p0 = 1.0L, p1 = x, dp0 = 0.0L, dp1 = 1.0L;
-    if (n == 0) { *dp = 0.0L; return 1.0L; }
-    for (int k = 1; k < n; ++k) {
-        long double p2 = ((2 * k + 1) * x * p1 - k * p0) / (k + 1);
-        long double dp2 = dp0 + (2 * k + 1) * p1;
-        p0 = p1; p1 = p2; dp0 = dp1; dp1 = dp2;
-    }
-    *dp = dp1;
-    return p1;
-}
-
-void build_tables(int N, OpTables &T) {
-    const int Np = N + 1;
-    std::memset(&T, 0, sizeof(T));
-    // Gauss-Lobatto nodes/weights on [0,1]
-    const long double pi = 3.14159265358979323846264338327950288L;
-    std::vector<long double> xs(Np);
-    for (int i = 0; i < Np; ++i) {
-        long double xi = -cosl(pi * i / N);
-        if (i > 0 && i < N)
-            for (int it = 0; it < 100; ++it) {
-                long double dP, P = legendre_ld(N, xi, &dP);
-                long double dx = ((1.0L - xi * xi) * dP) / (-(long double)N * (N + 1) * P);
-                xi -= dx;
-                if (fabsl(dx) < 1e-30L) break;
-            }
-        xs[i] = xi;
-    }
-    for (int i = 0; i < Np; ++i) {
-        long double dP, P = legendre_ld(N, xs[i], &dP);
-        T.x[i] = (double)((xs[i] + 1.0L) * 0.5L);
-        T.w[i] = (double)(2.0L / ((long double)N * (N + 1) * P * P) * 0.5L);
-    }
-    T.x[0] = 0.0;
-    T.x[N] = 1.0;
-    // barycentric differentiation matrix
-    std::vector<double> wb(Np, 1.0);
-    for (int i = 1; i < Np; ++i)
-        for (int j = 0; j < i; ++j) {
-            wb[j] *= (T.x[j] - T.x[i]);
-            wb[i] *= (T.x[i] - T.x[j]);
-        }
-    for (int i = 0; i < Np; ++i) wb[i] = 1.0 / wb[i];
-    for (int iL = 0; iL < Np; ++iL)
-        for (int i = 0; i < Np; ++i)
-            if (iL != i) {
-                T.D[i * Np + iL] = wb[iL] / wb[i] / (T.x[i] - T.x[iL]);
-                T.D[i * Np + i] -= T.D[i * Np + iL];
-            }
-    for (int q = 0; q < Np * Np; ++q) {
-        T.Dhat[q] = T.D[q];
-        T.Dhat2[q] = 2.0 * T.D[q];
-    }
-    T.Dhat[0] += 1.0 / T.w[0];
-    T.Dhat[(Np - 1) * Np + Np - 1] -= 1.0 / T.w[Np - 1];
-    T.Dhat2[0] += 1.0 / T.w[0];
-    T.Dhat2[(Np - 1) * Np + Np - 1] -= 1.0 / T.w[Np - 1];
-    // 1D Vandermonde of shifted Legendre P_a(2x-1): V[l][a], inverted (Gauss-Jordan)
-    std::vector<double> V(Np * Np), I(Np * Np, 0.0);
-    for (int l = 0; l < Np; ++l) {
-        double u[8], z = 2.0 * T.x[l] - 1.0;
-        u[0] = 1.0;
-        if (N >= 1) u[1] = z;
-        for (int n = 1; n < N; ++n) u[n + 1] = ((2 * n + 1) * z * u[n] - n * u[n - 1]) / (n + 1);
-        for (int a = 0; a < Np; ++a) V[l * Np + a] = u[a];
-    }
-    for (int i = 0; i < Np; ++i) I[i * Np + i] = 1.0;
-    for (int c = 0; c < Np; ++c) {
-        int piv = c;
-        for (int r = c + 1; r < Np; ++r)
-            if (std::fabs(V[r * Np + c]) > std::fabs(V[piv * Np + c])) piv = r;
-        for (int k = 0; k < Np; ++k) {
-            std::swap(V[c * Np + k], V[piv * Np + k]);
-            std::swap(I[c * Np + k], I[piv * Np + k]);
-        }
-        const double d = 1.0 / V[c * Np + c];
-        for (int k = 0; k < Np; ++k) { V[c * Np + k] *= d; I[c * Np + k] *= d; }
-        for (int r = 0; r < Np; ++r) {
-            if (r == c) continue;
-            const double f = V[r * Np + c];
-            for (int k = 0; k < Np; ++k) { V[r * Np + k] -= f * V[c * Np + k]; I[r * Np + k] -= f * I[c * Np + k]; }
-        }
-    }
-    // I = V^{-1}: I[a][l] maps nodal values (l) to mode a
-    for (int q = 0; q < Np * Np; ++q) T.Vinv[q] = I[q];
-}
-
-void build_phys(const prandtl_config &c, int N, PhysParams &P) {
-    P.gamma = c.gamma;
-    P.gammaM1 = c.gamma - 1.0;
-    P.gammaM1Inverse = 1.0 / P.gammaM1;
-    P.PrInverse = 1.0 / c.Pr;
-    P.mu = c.mu;
-    P.mu_bulk = 2.0 / 3.0;     // Physics.hpp:34
-    P.R_gas = c.R_gas;
-    P.mu0 = 1.716e-5;          // Physics.hpp:35-37
-    P.T0 = 273.15;
-    P.Ts = 110.4;
-    P.T0pTs = P.T0 + P.Ts;
-    P.alpha_max = c.alpha_max;
-    P.alpha_min = c.alpha_min;
-    P.modal_threshold = 0.5 * std::pow(10.0, -1.8 * std::pow((double)N, 0.25));   // DGSEMOperator.cpp:25
-    P.sutherland = c.sutherland;
-    P.quirks = c.quirks;
-    P.dissipation = c.surface_dissipation;
-    P.blending = c.blending;
-}
 
 prandtl_status wait_stream(prandtl_handle *h) {
     cudaError_t e = cudaEventRecord(h->done, h->stream);
@@ -299,40 +191,17 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
     if (!out) return fail(nullptr, PRANDTL_EINVAL, "out is NULL");
     *out = nullptr;
     if (!md || !cfg) return fail(nullptr, PRANDTL_EINVAL, "mesh or config is NULL");
-    if (md->dim != 2 && md->dim != 3) return fail(nullptr, PRANDTL_EUNSUPPORTED, "dim must be 2 or 3");
-    if (!order_supported(md->dim, md->order))
-        return fail(nullptr, PRANDTL_EUNSUPPORTED, "order must be in 1..5");
-    if (md->num_elements <= 0 || md->num_faces < 0) return fail(nullptr, PRANDTL_EINVAL, "bad sizes");
-    if (!md->elem_adj || !md->elem_detj || (md->num_faces > 0 && (!md->face_elems || !md->face_nor)))
-        return fail(nullptr, PRANDTL_EINVAL, "mesh arrays missing");
     if (cfg->precision != 0 && cfg->precision != 1)
         return fail(nullptr, PRANDTL_EUNSUPPORTED, "precision must be 0 (FP64) or 1 (FP32 bulk)");
     if (!(cfg->gamma > 1.0) || !(cfg->Pr > 0.0)) return fail(nullptr, PRANDTL_EINVAL, "bad gamma/Pr");
 
-    const int dim = md->dim, NFACE = 2 * dim, E = md->num_elements, F = md->num_faces;
-    // neighbour table: every element face must be an interior face exactly once
-    std::vector<int4> nbr((size_t)E * NFACE, make_int4(-1, -1, -1, -1));
-    for (int f = 0; f < F; ++f) {
-        const int *fe = md->face_elems + 4 * f;
-        const int e1 = fe[0], l1 = fe[1], e2 = fe[2], l2 = fe[3];
-        if (e1 < 0 || e1 >= E || e2 < 0 || e2 >= E || l1 < 0 || l1 >= NFACE || l2 < 0 || l2 >= NFACE)
-            return fail(nullptr, PRANDTL_EINVAL, "face " + std::to_string(f) + " out of range");
-        if ((l1 >> 1) != (l2 >> 1) || (l1 ^ l2) != 1)
-            return fail(nullptr, PRANDTL_EUNSUPPORTED,
-                        "face " + std::to_string(f) + ": only aligned opposite faces are supported");
-        int4 &a = nbr[(size_t)e1 * NFACE + l1];
-        int4 &b = nbr[(size_t)e2 * NFACE + l2];
-        if (a.x >= 0 || b.x >= 0)
-            return fail(nullptr, PRANDTL_EINVAL, "element face listed twice (face " + std::to_string(f) + ")");
-        a = make_int4(e2, l2, f, 0);
-        b = make_int4(e1, l1, f, 1);
+    const int dim = md->dim, E = md->num_elements, F = md->num_faces;
+    std::vector<int4> nbr;
+    {
+        std::string msg;
+        const prandtl_status vst = validate_mesh(md, nbr, msg);
+        if (vst != PRANDTL_OK) return fail(nullptr, vst, msg);
     }
-    for (size_t q = 0; q < nbr.size(); ++q)
-        if (nbr[q].x < 0)
-            return fail(nullptr, PRANDTL_EUNSUPPORTED,
-                        "element " + std::to_string(q / NFACE) + " has a boundary face; only periodic meshes are built");
-    for (int e = 0; e < E; ++e)
-        if (!(md->elem_detj[e] > 0.0)) return fail(nullptr, PRANDTL_EINVAL, "non-positive det J");
 
     int ndev = 0;
     cudaError_t ce = cudaGetDeviceCount(&ndev);
@@ -383,11 +252,7 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
     if ((st = dalloc(h, &h->d_alpha, (size_t)E, "alpha")) != PRANDTL_OK) return bail(st);
     if ((st = dalloc(h, &h->d_lambda, 1, "lambda")) != PRANDTL_OK) return bail(st);
 
-    std::vector<double> geo((size_t)E * GEO);
-    for (int e = 0; e < E; ++e) {
-        for (int q = 0; q < dim * dim; ++q) geo[(size_t)e * GEO + q] = md->elem_adj[(size_t)e * dim * dim + q];
-        geo[(size_t)e * GEO + dim * dim] = md->elem_detj[e];
-    }
+    const std::vector<double> geo = geometry_rows(md);
     if ((ce = cudaMemcpy(h->d_geo, geo.data(), geo.size() * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess)
         return bail(cuda_fail(h, ce, "upload geometry"));
     if ((ce = cudaMemcpy(h->d_nbr, nbr.data(), nbr.size() * sizeof(int4), cudaMemcpyHostToDevice)) != cudaSuccess)

@@ -37,6 +37,41 @@ def _ptr(a):
     raise TypeError(f"unsupported array type {type(a)}")
 
 
+class MeshArrays:
+    """The C-ABI mesh descriptor of a Mesh, with the arrays it points into kept alive."""
+
+    def __init__(self, mesh: Mesh):
+        self.adj = np.ascontiguousarray(mesh.elem_adj, dtype=np.float64)
+        self.detj = np.ascontiguousarray(mesh.elem_detj, dtype=np.float64)
+        self.faces = np.ascontiguousarray(mesh.face_elems, dtype=np.int32)
+        self.nor = np.ascontiguousarray(mesh.face_nor, dtype=np.float64)
+        dp = C.POINTER(C.c_double)
+        self.desc = _lib.MeshDesc(mesh.dim, mesh.order, mesh.num_elements, mesh.num_faces,
+                                  self.adj.ctypes.data_as(dp), self.detj.ctypes.data_as(dp),
+                                  self.faces.ctypes.data_as(C.POINTER(C.c_int)),
+                                  self.nor.ctypes.data_as(dp))
+
+
+def make_config(*, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05, parabolic=False, blending=False,
+                sutherland=False, alpha_max=0.5, alpha_min=0.001, quirks="reference",
+                surface_dissipation=True, precision="fp64", timeout_s=120.0) -> _lib.Config:
+    """prandtl_config from the DGSEMOperator keyword arguments."""
+    cfg = _lib.Config()
+    _lib.load().prandtl_config_default(C.byref(cfg))
+    cfg.gamma, cfg.Pr, cfg.mu, cfg.R_gas = gamma, Pr, mu, R_gas
+    cfg.alpha_max, cfg.alpha_min = alpha_max, alpha_min
+    cfg.parabolic, cfg.blending, cfg.sutherland = int(parabolic), int(blending), int(sutherland)
+    if quirks not in ("reference", "fixed", 0, 1):
+        raise ValueError("quirks must be 'reference' or 'fixed'")
+    cfg.quirks = 1 if quirks in ("fixed", 1) else 0
+    cfg.surface_dissipation = int(bool(surface_dissipation))
+    if precision not in ("fp64", "fp32"):
+        raise ValueError("precision must be 'fp64' or 'fp32' (FP32 bulk, FP64 RK state)")
+    cfg.precision = 1 if precision == "fp32" else 0
+    cfg.timeout_s = timeout_s
+    return cfg
+
+
 class DGSEMOperator:
     def __init__(self, mesh: Mesh, *, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05,
                  parabolic=False, blending=False, sutherland=False, alpha_max=0.5,
@@ -44,28 +79,12 @@ class DGSEMOperator:
                  precision="fp64", timeout_s=120.0):
         L = _lib.load()
         self.mesh = mesh
-        self._adj = np.ascontiguousarray(mesh.elem_adj, dtype=np.float64)
-        self._detj = np.ascontiguousarray(mesh.elem_detj, dtype=np.float64)
-        self._faces = np.ascontiguousarray(mesh.face_elems, dtype=np.int32)
-        self._nor = np.ascontiguousarray(mesh.face_nor, dtype=np.float64)
-        dp = C.POINTER(C.c_double)
-        desc = _lib.MeshDesc(mesh.dim, mesh.order, mesh.num_elements, mesh.num_faces,
-                             self._adj.ctypes.data_as(dp), self._detj.ctypes.data_as(dp),
-                             self._faces.ctypes.data_as(C.POINTER(C.c_int)),
-                             self._nor.ctypes.data_as(dp))
-        cfg = _lib.Config()
-        L.prandtl_config_default(C.byref(cfg))
-        cfg.gamma, cfg.Pr, cfg.mu, cfg.R_gas = gamma, Pr, mu, R_gas
-        cfg.alpha_max, cfg.alpha_min = alpha_max, alpha_min
-        cfg.parabolic, cfg.blending, cfg.sutherland = int(parabolic), int(blending), int(sutherland)
-        if quirks not in ("reference", "fixed", 0, 1):
-            raise ValueError("quirks must be 'reference' or 'fixed'")
-        cfg.quirks = 1 if quirks in ("fixed", 1) else 0
-        cfg.surface_dissipation = int(bool(surface_dissipation))
-        if precision not in ("fp64", "fp32"):
-            raise ValueError("precision must be 'fp64' or 'fp32' (FP32 bulk, FP64 RK state)")
-        cfg.precision = 1 if precision == "fp32" else 0
-        cfg.timeout_s = timeout_s
+        self._arrays = MeshArrays(mesh)
+        desc = self._arrays.desc
+        cfg = make_config(gamma=gamma, Pr=Pr, mu=mu, R_gas=R_gas, parabolic=parabolic,
+                          blending=blending, sutherland=sutherland, alpha_max=alpha_max,
+                          alpha_min=alpha_min, quirks=quirks, surface_dissipation=surface_dissipation,
+                          precision=precision, timeout_s=timeout_s)
         h = C.c_void_p()
         _lib.check(L.prandtl_create(C.byref(desc), C.byref(cfg), C.byref(h)), None)
         self._h = h
