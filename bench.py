@@ -1,22 +1,45 @@
 #!/usr/bin/env python
-"""Benchmark: DGSEM time steps of the 3D Navier-Stokes Taylor-Green vortex.
+"""Benchmark: the batched FP32-bulk DGSEM form against the plain FP64 path.
 
-Workload (default): periodic 32^3 hexahedral mesh on [0, 2pi]^3, N = 3 on
-Gauss-Lobatto nodes (128^3 nodes, 5 conserved fields), Mach 0.1, Re 1600,
-Pr 0.71, gamma 1.4, Chandrashekar flux differencing with the reference's
-surface flux, BR1 lifting, Carpenter-Kennedy LSRK4(5), FP64, seeded-free
-synthetic initial condition (the standard TGV).  One "step" is one full RK
-time step (5 RHS evaluations with fused stage updates).
+Headline workload ("tgv_ensemble_512"): 512 independent 3D Navier-Stokes
+Taylor-Green vortices drawn with numpy PCG64(20261203).  Each member has n^3
+periodic hexes on [0,2pi]^3 with n ~ U{4..16}, N ~ U{2,3,4,5},
+Mach ~ U[0.05,0.3] and Re ~ logU[100,3200] (Pr 0.71, gamma 1.4); the total is
+about 0.43 G DOF.  Each member takes Carpenter-Kennedy LSRK4(5) steps with
+its own fixed dt (CFL 0.1 on the initial max |V|+c).  The inputs are
+synthetic: the standard TGV initial condition, no dataset.  One "step"
+advances every member by one RK step.  Per stage and per order class there is
+one persistent lifting launch and one persistent RHS + stage-update launch,
+replayed from a CUDA graph.
 
-metric: DOF-updates/s = nodes * fields * steps / device time (whole job over
-all ranks).  Every rank runs an independent replica (no collectives on the
-data path); the timed region is bracketed by a barrier and synchronisation
-and the maximum over ranks is used.
+Keys of the JSON line:
+  value       DOF-updates/s of the FP32-bulk batch: sum(nodes*fields) * K
+              over the device time of K steps (CUDA events on the batch's
+              stream).
+  fp64_plain  the same metric for members advanced one at a time through the
+              one-operator FP64 path (DGSEMOperator.Step) on every 8th member.
+  error       FP32-batched vs FP64-plain states of those members after W+K
+              steps: relative L2 and Linf of density, momentum (as a vector)
+              and energy.
+  tgv32       the 32^3 N=3 TGV (one solve) through the plain FP64 path, with
+              its RHS kernel's FP64 roofline.
+  serving     Poisson request stream through prandtl_serve_*: p50/p99
+              time-to-solution and throughput.
+  e2e         the headline metric through the C ABI with pinned host buffers:
+              admission (H2D), tuning, W+K steps and reading every result
+              (D2H), by wall clock.
+  roofline    the dominant launch (the N=5 class RHS): FP32 CUDA-core FLOP/s
+              against the FP32 SGEMM rate measured live in this run, with the
+              launch's HBM bytes alongside.
+
+Every rank runs an independent replica: no collectives on the data path, a
+barrier and device synchronisation around the timed region, and the maximum
+time over ranks.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
---impl reference times the CPU implementation of the same path on the host
-cores (all threads) on a bounded sample of the workload; under torchrun only
+--impl reference times the reference's own DGSEM sources (oracle/_ref) on all
+host cores, on a bounded sample of the same ensemble; under torchrun only
 rank 0 runs it.
 """
 from __future__ import annotations
@@ -27,86 +50,75 @@ import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-L2_BYTES = 126 * 2 ** 20
+WORKLOAD = "tgv_ensemble_512"
+CFL = 0.1
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=200)
-    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--n", type=int, default=32, help="elements per direction")
-    p.add_argument("--order", type=int, default=3)
-    p.add_argument("--quirks", choices=["reference", "fixed"], default="fixed")
+    p.add_argument("--ensemble", type=int, default=512, help="members of the ensemble")
+    p.add_argument("--plain-every", type=int, default=8, help="FP64-plain subsample stride")
+    p.add_argument("--serve-requests", type=int, default=150)
+    p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--no-tgv32", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--no-fp64-peak", action="store_true")
+    p.add_argument("--no-peaks", action="store_true", help="skip the live SGEMM/DGEMM peak runs")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--profile-case", choices=["batch", "tgv32"], default=None,
+                   help="run only this part and print nothing (for ncu captures)")
     return p.parse_args()
 
 
-def workload_name(n, order):
-    return f"tgv3d_navier_stokes_{n}^3_N{order}_lsrk45_fp64"
-
-
-def physics():
-    return dict(parabolic=True, blending=False, mu=1.0 / 1600.0, Pr=0.71, gamma=1.4)
-
-
-def load_peaks():
-    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+def load_hbm_peak():
     try:
-        with open(path) as f:
-            pk = json.load(f)
-        return float(pk["hbm_gbs"]), "measured"
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
     except Exception:
         return 6650.0, "fallback"
 
 
 # ---------------------------------------------------------------- algorithmic cost
-def algorithmic_bytes(mesh, kernel):
-    """Compulsory DRAM bytes of one launch: every input read once, every output
-    written once (FP64).  S = one state vector."""
-    S = mesh.num_fields * mesh.ndof * 8
-    dim, E = mesh.dim, mesh.num_elements
-    tables = E * (dim * dim + 1) * 8 + E * 2 * dim * 16 + mesh.num_faces * dim * 8
-    if kernel == "lift":      # read u, write dim gradient vectors
-        return S + dim * S + tables
-    # rhs with LSRK epilogue: read u, gradients, du; write du, u_out
-    return S + dim * S + S + S + S + tables
-
-
-def flops_per_launch(mesh, kernel):
-    """FP64 operations of one launch from the operation counts of the
-    point-wise routines (add/mul/div/sqrt/log = 1, FMA = 2)."""
-    Np, dim, E = mesh.order + 1, mesh.dim, mesh.num_elements
-    nd = Np ** dim
-    nf = dim + 2
+def flops_per_element(dim, order, ns=True):
+    """Floating-point operations of one RHS launch per element, from the
+    operation counts of the point-wise routines (add/mul/div/sqrt/log = 1,
+    FMA = 2): two-point volume fluxes of every unique node pair with their two
+    D-weighted accumulations, surface fluxes of the element's face nodes,
+    node-wise viscous fluxes and their differencing (NS), epilogue."""
+    Np = order + 1
+    nd, nf = Np ** dim, dim + 2
     pairs = dim * Np ** (dim - 1) * Np * (Np - 1) // 2
     faces = 2 * dim * Np ** (dim - 1)
-    if kernel == "lift":
-        ent = 40            # entropy variables incl. log and pow as 1 each
-        per = (nd + faces) * ent + nd * dim * Np * nf * 2 + nd * dim * dim * nf * 2 + nd * dim * 35
-        return E * per
-    vol_pair = 123 + 2 * nf * 2      # Chandrashekar volume flux + two D-weighted accumulations
-    face_item = 150 + 2 * 60 + dim * nf * 2 + nf * 2
-    visc_node = 60 + dim * dim * nf * 2 + dim * Np * nf * 2
-    per = pairs * vol_pair + faces * face_item + nd * visc_node + nd * nf * 6
-    return E * per
+    vol_pair = 123 + 2 * nf * 2
+    face_item = 150 + (2 * 60 if ns else 0) + dim * nf * 2 + nf * 2
+    visc_node = (60 + dim * dim * nf * 2 + dim * Np * nf * 2) if ns else 0
+    return pairs * vol_pair + faces * face_item + nd * visc_node + nd * nf * 6
+
+
+def rhs_bytes_per_element(dim, order, grad_bytes, ns=True):
+    """Compulsory DRAM bytes of one RHS + LSRK launch per element: u read, the
+    gradients read (NS), du read and written, the next state written, and the
+    geometry rows."""
+    nd, nf = (order + 1) ** dim, dim + 2
+    per_dof = 8 + (dim * grad_bytes if ns else 0) + 8 + 8 + 8
+    return nd * nf * per_dof + (dim * dim + 1) * 8 + 2 * dim * 16
 
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
-    def __init__(self, index):
+    def __init__(self, index, tag):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{tag}_rank{index}.csv")
 
     def __enter__(self):
         try:
@@ -117,7 +129,7 @@ class ClockSampler:
                  "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "50"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=self.f, stderr=subprocess.DEVNULL)
             time.sleep(0.3)
         except Exception:
@@ -165,78 +177,73 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- CPU side
 def _cpu_worker(job):
-    """One CPU replica: LSRK4(5) steps of the TGV sample mesh.  kind 'reference'
-    runs the reference's own integrator sources (oracle/_ref), kind 'port' the
-    oracle restatement.  Returns (DOF updates, seconds)."""
-    kind, n_cpu, order, steps, seconds, threads = job
+    """One CPU process: LSRK4(5) steps of one ensemble member (order, Mach,
+    Re as drawn) on a 3^3-element mesh.  kind 'reference' runs the
+    reference's own DGSEM sources (oracle/_ref), kind 'port' the oracle
+    restatement.  Returns (DOF updates, seconds, steps)."""
+    kind, order, mach, re, steps, seconds, threads = job
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
     import pyoracle
     from prandtl_b200 import cases
+    from prandtl_b200.ensemble import fixed_dt
     from prandtl_b200.mesh import periodic_box
-    mesh = periodic_box(3, n_cpu, order, 0.0, 2 * np.pi)
-    u = cases.taylor_green(mesh)
-    kw = dict(parabolic=1, blending=0, mu=1.0 / 1600.0, Pr=0.71, gamma=1.4)
+    mesh = periodic_box(3, 3, order, 0.0, 2 * np.pi)
+    u = cases.taylor_green(mesh, mach=mach)
+    kw = dict(parabolic=1, blending=0, mu=1.0 / re, Pr=0.71, gamma=1.4, quirks=1)
     cls = pyoracle.RefOperator if kind == "reference" else pyoracle.Oracle
     op = cls(mesh, nthreads=threads, **kw)
-    lam = pyoracle.Oracle(mesh, nthreads=1, **kw).rhs(u)["lambda_max"]
-    dt = 0.1 * mesh.hmin / (lam * (order + 1) ** 2)
+    dt = fixed_dt(mesh, u, CFL)
     u = op.step(u, dt, scheme=1, nsteps=1)   # warm-up
     done, t0 = 0, time.perf_counter()
     while True:
         u = op.step(u, dt, scheme=1, nsteps=1)
         done += 1
         el = time.perf_counter() - t0
-        if (steps is not None and done >= steps) or (steps is None and el >= seconds):
+        if (steps is not None and done >= steps) or el >= seconds:
             break
     return mesh.ndof * mesh.num_fields * done, el, done
 
 
-def cpu_rate(order, steps=None, seconds=12.0):
-    """DOF-updates/s of the CPU path on the host cores.
-
-    With the reference's own sources built (oracle/_ref) this is the
-    reference: one process per core, each advancing its own 4^3-element TGV
-    sample (the reference scales over cores by MPI domain decomposition,
-    run.sh `mpiexec -n`).  Otherwise the oracle port runs 8^3 elements with one
-    OpenMP thread per core."""
+def cpu_rate(steps=None, seconds=12.0):
+    """DOF-updates/s of the CPU path on all host cores.  With the reference's
+    own sources built (oracle/_ref) this is the reference: one process per core
+    (the reference scales by MPI domain decomposition, run.sh `mpiexec -n`),
+    process i advancing ensemble member i on a 3^3-element mesh.  Otherwise the
+    oracle restatement runs the same sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import multiprocessing as mp
     import pyoracle
+    from prandtl_b200.ensemble import tgv_ensemble
     cores = os.cpu_count() or 1
-    if pyoracle.ref_available():
-        n_cpu, kind = 4, "reference"
-        jobs = [(kind, n_cpu, order, steps, seconds, 1)] * cores
-        with mp.get_context("spawn").Pool(cores) as pool:
-            res = pool.map(_cpu_worker, jobs)
-        upd = sum(r[0] for r in res)
-        el = max(r[1] for r in res)
-        nstep = res[0][2]
-        sample = (f"reference DGSEM sources (oracle/_ref, -O2) x {cores} processes, each TGV "
-                  f"{n_cpu}^3 elements N={order}, {nstep} LSRK4(5) steps")
-    else:
-        n_cpu, kind = 8, "port"
-        with mp.get_context("spawn").Pool(1) as pool:
-            upd, el, nstep = pool.map(_cpu_worker, [(kind, n_cpu, order, steps, seconds, cores)])[0]
-        sample = (f"oracle C++ restatement -O2, {cores} OpenMP threads, TGV {n_cpu}^3 elements "
-                  f"N={order}, {nstep} LSRK4(5) steps")
-    return upd / el, dict(kind=kind, cores=cores, steps=nstep, seconds=el, sample=sample)
+    kind = "reference" if pyoracle.ref_available() else "port"
+    ens = tgv_ensemble(max(cores, 4))
+    jobs = [(kind, m.order, m.mach, m.re, steps, seconds, 1) for m in ens[:cores]]
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_cpu_worker, jobs)
+    upd = sum(r[0] for r in res)
+    el = max(r[1] for r in res)
+    nsteps = min(r[2] for r in res)
+    src = "reference DGSEM sources (oracle/_ref, -O2)" if kind == "reference" else "oracle C++ restatement -O2"
+    sample = (f"{src} x {cores} processes; process i advances ensemble member i (its N, Mach, Re) "
+              f"on 3^3 elements with LSRK4(5), >= {nsteps} steps each in {el:.1f} s")
+    return upd / el, dict(kind=kind, cores=cores, steps=nsteps, seconds=el, sample=sample)
 
 
 def run_reference(args, rank):
     if rank != 0:
         return
-    # W warm-up steps, then K timed steps of the sample workload
-    cpu_rate(args.order, steps=max(1, args.warmup))
-    rate, info = cpu_rate(args.order, steps=max(1, args.steps))
+    budget = max(10.0, min(120.0, 0.6 * (args.steps + args.warmup)))
+    cpu_rate(steps=max(1, args.warmup), seconds=budget / 4)
+    rate, info = cpu_rate(steps=max(1, args.steps), seconds=budget)
     line = {
         "metric": "DOF-updates/s/GPU", "value": rate, "unit": "DOF-updates/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * info["seconds"] / max(1, info["steps"]),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (standard TGV initial condition)",
-        "config": {"workload": workload_name(args.n, args.order), "order": args.order,
-                   "scheme": "LSRK45", "quirks": "reference (the reference's own code)"},
+        "config": {"workload": WORKLOAD, "scheme": "LSRK45", "cfl": CFL,
+                   "sample": "each host core advances one ensemble member on 3^3 elements"},
         "cpu_baseline": {"value": rate, "unit": "DOF-updates/s", "cores": info["cores"],
                          "kind": info["kind"], "sample": info["sample"]},
         "e2e": {"value": rate, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -245,9 +252,12 @@ def run_reference(args, rank):
 
 
 # ---------------------------------------------------------------- GPU side
-def fp64_peak_tflops(torch):
-    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
-    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+def gemm_tflops(torch, dtype, n=8192):
+    """Best-of-5 cuBLAS GEMM rate (TF32 off for float32: CUDA-core FP32)."""
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(n, n, dtype=dtype, device="cuda")
+    b = torch.randn(n, n, dtype=dtype, device="cuda")
     for _ in range(2):
         torch.matmul(a, b)
     torch.cuda.synchronize()
@@ -259,8 +269,212 @@ def fp64_peak_tflops(torch):
         e1.record()
         torch.cuda.synchronize()
         best = min(best, e0.elapsed_time(e1) / 1e3)
+    torch.backends.cuda.matmul.allow_tf32 = old
     del a, b
-    return 2 * 8192 ** 3 / best / 1e12
+    return 2 * n ** 3 / best / 1e12
+
+
+def rel_errors(a, b, nf):
+    """Relative L2 and Linf of density, momentum (vector) and energy."""
+    import numpy as np
+    a, b = a.reshape(nf, -1), b.reshape(nf, -1)
+    out = {}
+    for name, g in (("rho", [0]), ("momentum", list(range(1, nf - 1))), ("energy", [nf - 1])):
+        d = a[g] - b[g]
+        out[name] = (float(np.linalg.norm(d) / np.linalg.norm(b[g])), float(np.abs(d).max() / np.abs(b[g]).max()))
+    return out
+
+
+def build_items(members):
+    from prandtl_b200.ensemble import fixed_dt
+    items = []
+    for m in members:
+        mesh = m.mesh()
+        u0 = m.initial_state(mesh)
+        items.append((m, mesh, u0, fixed_dt(mesh, u0, CFL)))
+    return items
+
+
+def run_batch(torch, items, K, W, barrier, local):
+    """FP32-bulk batch over all members.  The wall-clock window (e2e) spans
+    admission from pinned host memory, tuning, W+K steps and reading every
+    state back; the device window (value) spans the last K steps."""
+    from prandtl_b200.batch import Batch
+    pinned = [torch.from_numpy(u0).pin_memory() for _, _, u0, _ in items]
+    outs = [torch.empty(p.shape, dtype=torch.float64).pin_memory() for p in pinned]
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    b = Batch("fp32", "LSRK45")
+    ids = [b.add(mesh, pinned[k], dt=dt, nsteps=W + K, **m.physics()) for k, (m, mesh, _, dt) in enumerate(items)]
+    b.tune(reps=2)
+    b.advance(W)
+    b.sync()
+    stream = torch.cuda.ExternalStream(b.stream)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = b.kernel_launches
+    with ClockSampler(local, "batch") as clk:
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        b.advance(K)
+        ev1.record(stream)
+        ev1.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+    device_s = ev0.elapsed_time(ev1) / 1e3
+    launches = b.kernel_launches - launches0
+    for k, sid in enumerate(ids):
+        b.read(sid, outs[k])
+    wall = time.perf_counter() - t0
+    classes = {}
+    for order in sorted({m.order for m, _, _, _ in items}):
+        v, ms, lift = b.class_info(3, order, True)
+        classes[order] = {"variant": v, "rhs_ms_per_variant": ms, "lift_ms": lift}
+    info = {"device_s": device_s, "wall_s": wall, "launches": launches, "device_bytes": b.device_bytes,
+            "classes": classes, "clocks": clk.summary()}
+    b.close()
+    return [o.numpy() for o in outs], info
+
+
+def run_plain(torch, items, K, W):
+    """Members one at a time through the one-operator FP64 path: W untimed and
+    K timed steps each (CUDA events on the current stream)."""
+    from prandtl_b200.operator import DGSEMOperator
+    stream = torch.cuda.current_stream()
+    total_s, dofs, states, launches = 0.0, 0, [], 0
+    for m, mesh, u0, dt in items:
+        op = DGSEMOperator(mesh, **m.physics())
+        op.set_stream(stream.cuda_stream)
+        u = torch.from_numpy(u0).cuda()
+        op.Step(u, dt, scheme="LSRK45", nsteps=W)
+        l0 = op.kernel_launches
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        op.Step(u, dt, scheme="LSRK45", nsteps=K)
+        e1.record(stream)
+        e1.synchronize()
+        total_s += e0.elapsed_time(e1) / 1e3
+        launches += op.kernel_launches - l0
+        dofs += u0.size
+        states.append(u.cpu().numpy())
+        op.close()
+    return states, {"device_s": total_s, "dof": dofs, "launches": launches}
+
+
+def run_tgv32(torch, steps):
+    """The 32^3 N=3 TGV (one solve) through the plain FP64 path with per-kernel
+    CUDA-event times."""
+    import numpy as np
+    from prandtl_b200 import cases
+    from prandtl_b200.mesh import periodic_box
+    from prandtl_b200.operator import DGSEMOperator
+    mesh = periodic_box(3, 32, 3, 0.0, 2 * np.pi)
+    u0 = cases.taylor_green(mesh)
+    op = DGSEMOperator(mesh, parabolic=True, mu=1.0 / 1600.0, Pr=0.71, quirks="fixed")
+    stream = torch.cuda.current_stream()
+    op.set_stream(stream.cuda_stream)
+    u = torch.from_numpy(u0).cuda()
+    d = torch.empty_like(u)
+    op.Mult(u, d)
+    dt = op.cfl_dt(CFL, op.GetMaxCharSpeed())
+    for _ in range(3):
+        op.Step(u, dt, scheme="LSRK45")
+    torch.cuda.synchronize()
+    op.profile(True)
+    op.profile_reset()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    op.Step(u, dt, scheme="LSRK45", nsteps=steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    prof = op.profile_read()
+    op.profile(False)
+    op.close()
+    dof = mesh.ndof * mesh.num_fields
+    rhs_ms = prof["rhs"][0] / prof["rhs"][1]
+    lift_ms = prof["lift"][0] / prof["lift"][1]
+    E = mesh.num_elements
+    return {"workload": "tgv3d_navier_stokes_32^3_N3_lsrk45_fp64", "dof": dof,
+            "value": dof * steps / el, "unit": "DOF-updates/s", "ms_per_step": 1e3 * el / steps,
+            "rhs_ms": rhs_ms, "lift_ms": lift_ms,
+            "rhs_flops": E * flops_per_element(3, 3), "rhs_bytes": E * rhs_bytes_per_element(3, 3, 8)}
+
+
+def run_serving(torch, n_req):
+    """Calibrate the server's capacity with a closed burst, then replay a
+    Poisson stream at 80 % of it.  Requests are FP32-bulk solves."""
+    import numpy as np
+    from prandtl_b200.batch import Server
+    from prandtl_b200.ensemble import fixed_dt, serving_stream
+
+    def prep(reqs):
+        out = []
+        for m in reqs:
+            mesh = m.mesh()
+            u0 = m.initial_state(mesh)
+            out.append((m, mesh, u0, fixed_dt(mesh, u0, 0.3 if m.kind == "ivortex" else CFL)))
+        return out
+
+    burst = prep(serving_stream(48, seed=7, rate=1.0))
+    s = Server("fp32", steps_per_tick=4)
+    t0 = time.perf_counter()
+    tickets = [s.submit(mesh, u0, dt=dt, nsteps=m.nsteps, **m.physics()) for m, mesh, u0, dt in burst]
+    for t in tickets:
+        s.wait(t, 600.0)
+    cap_s = time.perf_counter() - t0
+    s.close()
+    capacity = len(burst) / cap_s
+    rate = 0.8 * capacity
+    reqs = prep(serving_stream(n_req, seed=20261204, rate=rate))
+    s = Server("fp32", steps_per_tick=4)
+    tickets = [None] * len(reqs)
+
+    def submitter():
+        start = time.perf_counter()
+        for k, (m, mesh, u0, dt) in enumerate(reqs):
+            delay = m.arrival - (time.perf_counter() - start)
+            if delay > 0:
+                time.sleep(delay)
+            tickets[k] = s.submit(mesh, u0, dt=dt, nsteps=m.nsteps, **m.physics())
+
+    th = threading.Thread(target=submitter)
+    t_start = time.perf_counter()
+    th.start()
+    th.join()
+    lat, results = [], []
+    for k, t in enumerate(tickets):
+        u, sec = s.wait(t, 600.0)
+        lat.append(sec)
+        results.append(u)
+    t_end = time.perf_counter()
+    st = s.stats()
+    s.close()
+    # every 15th result against the FP64 plain path
+    from prandtl_b200.operator import DGSEMOperator
+    worst = 0.0
+    checked = 0
+    for k in range(0, len(reqs), 15):
+        m, mesh, u0, dt = reqs[k]
+        op = DGSEMOperator(mesh, **m.physics())
+        ref = u0.copy()
+        op.Step(ref, dt, scheme="LSRK45", nsteps=m.nsteps)
+        op.close()
+        e = rel_errors(results[k], ref, mesh.num_fields)
+        worst = max(worst, max(v[0] for v in e.values()))
+        checked += 1
+    lat_ms = np.array(lat) * 1e3
+    return {"requests": len(reqs), "precision": "fp32-bulk",
+            "arrivals": f"Poisson at {rate:.2f}/s = 0.8 x capacity {capacity:.2f}/s (closed burst of 48)",
+            "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
+            "mean_ms": float(lat_ms.mean()),
+            "throughput_dof_updates_per_s": st["dof_updates"] / (t_end - t_start),
+            "busy_dof_updates_per_s": st["dof_updates"] / max(st["busy_s"], 1e-9),
+            "batch_steps": st["steps"], "checked_vs_fp64_plain": checked,
+            "max_rel_l2_vs_fp64_plain": worst,
+            "mix": "50% 2D Euler isentropic vortex (16^2..128^2, N 3|4), 50% 3D NS TGV (8^3..24^3, N 2|3), "
+                   "50..500 steps"}
 
 
 def main():
@@ -274,141 +488,125 @@ def main():
 
     import numpy as np
     import torch
-    from prandtl_b200 import cases
-    from prandtl_b200.mesh import periodic_box
-    from prandtl_b200.operator import DGSEMOperator
+    from prandtl_b200.ensemble import tgv_ensemble
 
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    mesh = periodic_box(3, args.n, args.order, 0.0, 2 * np.pi)
-    u0 = cases.taylor_green(mesh)
-    op = DGSEMOperator(mesh, quirks=args.quirks, **physics())
-    stream = torch.cuda.current_stream()
-    op.set_stream(stream.cuda_stream)
-    u = torch.from_numpy(u0).cuda()
-    dudt = torch.empty_like(u)
-    op.Mult(u, dudt)
-    lam = op.GetMaxCharSpeed()
-    dt = op.cfl_dt(0.1, lam)    # CFL 0.1 as the reference TGV case (Simulation.cpp:906)
-
-    for _ in range(args.warmup):
-        op.Step(u, dt, scheme="LSRK45")
-    torch.cuda.synchronize()
-
-    op.profile(True)
-    op.profile_reset()
-    launches0 = op.kernel_launches
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        barrier()
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        for _ in range(args.steps):
-            op.Step(u, dt, scheme="LSRK45")
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-    elapsed = ev0.elapsed_time(ev1) / 1e3
-    launches = op.kernel_launches - launches0
-    prof = op.profile_read()
-    op.profile(False)
-    if dist is not None:
-        t = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
-    finite = bool(torch.isfinite(u).all().item())
+        return float(t.item())
 
-    dof = mesh.ndof * mesh.num_fields
-    value = dof * args.steps * world / elapsed
+    K, W = args.steps, args.warmup
+    if args.profile_case == "tgv32":
+        run_tgv32(torch, K)
+        return
+    members = tgv_ensemble(args.ensemble)
+    items = build_items(members)
+    dof = sum(u0.size for _, _, u0, _ in items)
 
-    # ---- end to end through the public API with pinned host buffers
-    e2e = None
-    if not args.no_e2e:
-        host = torch.from_numpy(u0.copy()).pin_memory()
-        for _ in range(2):
-            op.Step(host, dt, scheme="LSRK45")
-        torch.cuda.synchronize()
-        ke = max(3, min(args.steps, 50))
-        barrier()
-        t0 = time.perf_counter()
-        for _ in range(ke):
-            op.Step(host, dt, scheme="LSRK45")   # H2D u, 5 fused stages, D2H u, wait
-        torch.cuda.synchronize()
-        el = time.perf_counter() - t0
-        if dist is not None:
-            t = torch.tensor([el], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
-        e2e = {"value": dof * ke * world / el, "unit": "DOF-updates/s",
-               "h2d_bytes_per_step": dof * 8, "d2h_bytes_per_step": dof * 8, "steps": ke}
+    states, binfo = run_batch(torch, items, K, W, barrier, local)
+    if args.profile_case == "batch":
+        return
+    device_s = max_over_ranks(binfo["device_s"])
+    wall_s = max_over_ranks(binfo["wall_s"])
+    value = dof * K * world / device_s
 
-    # ---- roofline of the dominant kernel (device time measured with events above)
-    hbm_peak, peak_kind = load_peaks()
-    dom = max(prof, key=lambda k: prof[k][0])
-    ms, n = prof[dom]
-    t_launch = ms / 1e3 / max(1, n)
-    ab = algorithmic_bytes(mesh, dom)
-    fl = flops_per_launch(mesh, dom)
-    fp64_peak = fp64_peak_tflops(torch) if (rank == 0 and not args.no_fp64_peak) else None
-    gbs = ab / t_launch / 1e9
-    tfl = fl / t_launch / 1e12
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        try:
-            with open(tpath) as f:
-                traffic = json.load(f).get(f"{dom}_bytes_per_launch")
-        except Exception:
-            traffic = None
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
-                "frac": gbs / hbm_peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "traffic": traffic, "algorithmic_bytes_per_launch": ab,
-                "avg_launch_ms": t_launch * 1e3,
-                "fp64": {"achieved_tflops": tfl, "peak_tflops": fp64_peak,
-                         "frac": (tfl / fp64_peak) if fp64_peak else None,
-                         "peak_source": "measured live: cuBLAS DGEMM 8192^3 (torch.matmul float64)",
-                         "flops_per_launch": fl},
-                "kernels": {k: {"total_ms": v[0], "launches": v[1]} for k, v in prof.items()}}
-
-    cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
-        try:
-            rate, info = cpu_rate(args.order, seconds=args.cpu_seconds)
-            cpu = {"value": rate, "unit": "DOF-updates/s", "cores": info["cores"],
-                   "kind": info["kind"], "sample": info["sample"]}
-        except Exception as exc:   # the oracle build is missing on this host
-            cpu = {"value": None, "unit": "DOF-updates/s", "cores": os.cpu_count(),
-                   "kind": "port", "sample": f"unavailable: {exc}"}
-
+    line = None
     if rank == 0:
-        S = dof * 8
+        # FP64 plain path on every k-th member, and the FP32-batched error against it
+        sample = list(range(0, len(items), max(1, args.plain_every)))
+        pstates, pinfo = run_plain(torch, [items[k] for k in sample], K, W)
+        plain_rate = pinfo["dof"] * K / pinfo["device_s"]
+        errs = [rel_errors(states[k], p, 5) for k, p in zip(sample, pstates)]
+        err = {f: {"rel_l2_max": max(e[f][0] for e in errs), "rel_l2_median": statistics.median(e[f][0] for e in errs),
+                   "rel_linf_max": max(e[f][1] for e in errs)} for f in ("rho", "momentum", "energy")}
+        # roofline of the dominant launch: the class with the largest tuned RHS time
+        fp32_peak = gemm_tflops(torch, torch.float32) if not args.no_peaks else None
+        fp64_peak = gemm_tflops(torch, torch.float64) if not args.no_peaks else None
+        dom_order = max(binfo["classes"], key=lambda o: binfo["classes"][o]["rhs_ms_per_variant"][binfo["classes"][o]["variant"]])
+        dc = binfo["classes"][dom_order]
+        t_launch = dc["rhs_ms_per_variant"][dc["variant"]] / 1e3
+        E_dom = sum(mesh.num_elements for m, mesh, _, _ in items if m.order == dom_order)
+        fl = E_dom * flops_per_element(3, dom_order)
+        by = E_dom * rhs_bytes_per_element(3, dom_order, 4)
+        hbm_peak, hbm_src = load_hbm_peak()
+        tfl = fl / t_launch / 1e12
+        roofline = {
+            "bound": "compute (FP32 CUDA cores; the kernel is neither HBM- nor tensor-bound)",
+            "kernel": f"rhs_batch_kernel<3, N={dom_order}, NS, float> (all N={dom_order} members, one stage)",
+            "achieved": tfl, "peak": fp32_peak, "unit": "TFLOP/s",
+            "frac": (tfl / fp32_peak) if fp32_peak else None,
+            "peak_source": "measured live in this run: cuBLAS SGEMM 8192^3, TF32 off (torch.matmul float32)",
+            "traffic": None,
+            "flops_per_launch": fl, "avg_launch_ms": t_launch * 1e3,
+            "launch_timing": "CUDA events on the batch stream (autotuner, the launch repeated on the step's first stage)",
+            "hbm": {"algorithmic_bytes_per_launch": by, "achieved_gbs": by / t_launch / 1e9,
+                    "peak_gbs": hbm_peak, "frac": by / t_launch / 1e9 / hbm_peak, "peak_source": hbm_src},
+            "classes": {str(o): c for o, c in binfo["classes"].items()},
+        }
+        tgv32 = None
+        if not args.no_tgv32:
+            tgv32 = run_tgv32(torch, 50)
+            tf = tgv32["rhs_flops"] / (tgv32["rhs_ms"] / 1e3) / 1e12
+            tgv32["rhs_fp64_tflops"] = tf
+            tgv32["fp64_peak_tflops"] = fp64_peak
+            tgv32["rhs_fp64_frac"] = (tf / fp64_peak) if fp64_peak else None
+            tgv32["fp64_peak_source"] = "measured live: cuBLAS DGEMM 8192^3"
+        serving = None
+        if not args.no_serve:
+            serving = run_serving(torch, args.serve_requests)
+        cpu = None
+        if not args.no_cpu_baseline:
+            try:
+                rate, info = cpu_rate(seconds=args.cpu_seconds)
+                cpu = {"value": rate, "unit": "DOF-updates/s", "cores": info["cores"],
+                       "kind": info["kind"], "sample": info["sample"]}
+            except Exception as exc:
+                cpu = {"value": None, "unit": "DOF-updates/s", "cores": os.cpu_count(), "kind": "port",
+                       "sample": f"unavailable: {exc}"}
+        u_bytes = dof * 8
         line = {
             "metric": "DOF-updates/s/GPU", "value": value, "unit": "DOF-updates/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (standard TGV initial condition, no dataset)",
-            "config": {"workload": workload_name(args.n, args.order), "mesh": f"{args.n}^3 periodic hex",
-                       "order": args.order, "dof": dof, "scheme": "LSRK45", "cfl": 0.1,
-                       "quirks": args.quirks, "parallelism": f"replicas x{world}",
-                       "l2": f"no flush: working set {(7 * S) / 2**20:.0f} MiB per stage > 126 MiB L2"},
-            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
-            "finite": finite,
+            "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": 1e3 * device_s / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32-bulk/f64-state",
+            "data": "synthetic (standard TGV initial conditions, seeded ensemble; no dataset)",
+            "config": {"workload": WORKLOAD, "members": len(items), "dof": dof, "seed": 20261203,
+                       "orders": "N ~ U{2,3,4,5}", "mesh": "n^3 periodic hexes, n ~ U{4..16}",
+                       "mach": "U[0.05,0.3]", "re": "logU[100,3200]", "scheme": "LSRK45", "cfl": CFL,
+                       "form": "batched FP32 bulk, FP64 RK state; persistent per-order launches in a CUDA graph",
+                       "parallelism": f"replicas x{world}",
+                       "l2": f"no flush: working set {binfo['device_bytes'] / 2**30:.1f} GiB >> 126 MiB L2"},
+            "fp64_plain": {"value": plain_rate, "unit": "DOF-updates/s", "members": len(sample),
+                           "sample": f"every {args.plain_every}th member, each alone through DGSEMOperator.Step",
+                           "ratio_fp32_batched_over_fp64_plain": (value / world) / plain_rate},
+            "error": {"fp32_batched_vs_fp64_plain_after_steps": W + K, "members": len(sample), **err},
+            "e2e": {"value": dof * (W + K) * world / wall_s, "unit": "DOF-updates/s",
+                    "h2d_bytes_per_step": u_bytes / (W + K), "d2h_bytes_per_step": u_bytes / (W + K),
+                    "window": "admission from pinned host memory + tuning + W+K steps + every state read back; "
+                              "the states cross once per solve, bytes shown per step"},
+            "gpu_launches": binfo["launches"],
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "tgv32": tgv32,
+            "serving": serving,
+            "clocks": binfo["clocks"],
         }
-        clk_sum = clk.summary()
-        line["clocks"] = clk_sum
+    barrier()
+    if line is not None:
         print(json.dumps(line), flush=True)
-    op.close()
     if dist is not None:
         dist.destroy_process_group()
 

@@ -236,9 +236,12 @@ prandtl_status prandtl_batch_remove(prandtl_batch *b, int id);
  * keep the fastest. */
 prandtl_status prandtl_batch_tune(prandtl_batch *b, int reps);
 /* Launch shape chosen for a class and the tuned times (ms per launch, -1 when
- * not timed) of each of the *n_variants shapes; ms may be NULL. */
+ * not timed) of each of the *n_variants RHS shapes and of the lifting launch;
+ * ms and lift_ms may be NULL. */
 prandtl_status prandtl_batch_class_info(prandtl_batch *b, int dim, int order, int parabolic,
-                                        int *variant, int *n_variants, double *ms);
+                                        int *variant, int *n_variants, double *ms, double *lift_ms);
+/* The CUDA stream (cudaStream_t) the batch enqueues on, for event timing. */
+void *prandtl_batch_stream(const prandtl_batch *b);
 size_t prandtl_batch_device_bytes(const prandtl_batch *b);   /* arena + tables */
 size_t prandtl_batch_arena_bytes(const prandtl_batch *b);    /* arena only */
 long long prandtl_batch_kernel_launches(const prandtl_batch *b);

@@ -117,11 +117,18 @@ class Batch:
         self._check(self._L.prandtl_batch_tune(self._h, int(reps)))
 
     def class_info(self, dim: int, order: int, parabolic: bool):
+        """(chosen RHS launch shape, tuned ms per RHS launch of each shape, tuned ms per lifting launch)."""
         v, n = C.c_int(), C.c_int()
         ms = (C.c_double * 8)()
+        lift = C.c_double(-1.0)
         self._check(self._L.prandtl_batch_class_info(self._h, dim, order, int(parabolic), C.byref(v),
-                                                     C.byref(n), ms))
-        return v.value, list(ms[: n.value])
+                                                     C.byref(n), ms, C.byref(lift)))
+        return v.value, list(ms[: n.value]), lift.value
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of the batch (for torch.cuda.ExternalStream and event timing)."""
+        return self._L.prandtl_batch_stream(self._h) or 0
 
     @property
     def device_bytes(self) -> int:

@@ -136,6 +136,7 @@ struct Class {
     BatchKernelInfo rinfo[MAX_VARIANTS]{};
     BatchKernelInfo linfo{};
     double ms[MAX_VARIANTS];
+    double lift_ms = -1.0;
 };
 
 }   // namespace
@@ -687,9 +688,17 @@ prandtl_status prandtl_batch_tune(prandtl_batch *b, int reps) {
         Class &c = kv.second;
         if (c.ids.empty()) continue;
         if (c.ns) {
-            BCK(b, batch_launch_lift(c.dim, c.order, fp32, c.linfo.blocks_per_sm * b->num_sms, c.dev, st0, c.T,
-                                     b->stream),
-                "tune lift");
+            const int lgrid = c.linfo.blocks_per_sm * b->num_sms;
+            BCK(b, batch_launch_lift(c.dim, c.order, fp32, lgrid, c.dev, st0, c.T, b->stream), "tune lift");
+            BCK(b, cudaEventRecord(b->ev0, b->stream), "event");
+            for (int r = 0; r < reps; ++r)
+                BCK(b, batch_launch_lift(c.dim, c.order, fp32, lgrid, c.dev, st0, c.T, b->stream), "tune lift");
+            BCK(b, cudaEventRecord(b->ev1, b->stream), "event");
+            if ((st = bwait(b)) != PRANDTL_OK) return st;
+            float lms = 0.f;
+            BCK(b, cudaEventElapsedTime(&lms, b->ev0, b->ev1), "event time");
+            c.lift_ms = lms / reps;
+            b->launches += reps + 1;
         }
         int best = c.variant;
         double best_ms = 1e300;
@@ -716,7 +725,7 @@ prandtl_status prandtl_batch_tune(prandtl_batch *b, int reps) {
 }
 
 prandtl_status prandtl_batch_class_info(prandtl_batch *b, int dim, int order, int parabolic, int *variant,
-                                        int *n_variants, double *ms) {
+                                        int *n_variants, double *ms, double *lift_ms) {
     if (!b) return PRANDTL_EINVAL;
     std::lock_guard<std::mutex> lk(b->mu);
     auto it = b->classes.find(class_key(dim, order, parabolic != 0));
@@ -725,8 +734,11 @@ prandtl_status prandtl_batch_class_info(prandtl_batch *b, int dim, int order, in
     if (n_variants) *n_variants = b->nvar;
     if (ms)
         for (int v = 0; v < b->nvar; ++v) ms[v] = it->second.ms[v];
+    if (lift_ms) *lift_ms = it->second.lift_ms;
     return PRANDTL_OK;
 }
+
+void *prandtl_batch_stream(const prandtl_batch *b) { return b ? (void *)b->stream : nullptr; }
 
 size_t prandtl_batch_device_bytes(const prandtl_batch *b) { return b ? b->bytes : 0; }
 size_t prandtl_batch_arena_bytes(const prandtl_batch *b) { return b ? b->arena_bytes : 0; }

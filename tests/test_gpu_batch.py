@@ -134,8 +134,9 @@ def test_autotuner_picks_a_timed_shape_and_keeps_results():
     ids = [b.add(mesh, u0, dt=dt, nsteps=3, **m.physics()) for m, mesh, u0, dt in items]
     b.tune(reps=2)
     for m, mesh, _, _ in items:
-        v, ms = b.class_info(mesh.dim, mesh.order, m.kind == "tgv")
+        v, ms, lift_ms = b.class_info(mesh.dim, mesh.order, m.kind == "tgv")
         assert ms[v] > 0 and ms[v] == min(t for t in ms if t > 0)
+        assert (lift_ms > 0) == (m.kind == "tgv")
     b.advance(3)
     for sid, (m, mesh, u0, dt) in zip(ids, items):
         ref = plain(m, u0, dt, 3, precision="fp32")
