@@ -210,51 +210,74 @@ constexpr int next_pow2(int v) { return v <= 1 ? 1 : 2 * next_pow2((v + 1) / 2);
 #define PRANDTL_EULER32_MINB 6
 #endif
 
-// Warp-per-element layout of the RHS kernel: one group of GS lanes owns one
-// element (GS = 32, or the next power of two >= Np^d for small elements, so
-// a warp then holds several elements); lane `li` of a group owns the nodes
-// li, li+GS, ... and the pair / face / subcell items of the same stride.
-// Groups synchronise with __syncwarp only.
+// Lane-group layout of the RHS kernel: one group of GS lanes owns one
+// element.  GS = 32 (a warp), the next power of two >= Np^d for small
+// elements (a warp then holds several elements), or 64 (two warps) for large
+// ones.  Lane `li` of a group owns the nodes li, li+GS, ... and the pair /
+// face / subcell items of the same stride.  Groups synchronise with
+// __syncwarp, or with a named barrier when GS = 64.
 //
 // V selects the launch shape (the batch autotuner times all of them):
-//   V = 0: the configured warps per CTA and register budget (the one-shot kernel)
-//   V = 1: same warps, one more resident CTA per SM required (fewer registers)
-//   V = 2: half the warps per CTA, twice the resident CTAs (finer shared-memory
-//          granularity for the large elements)
+//   V = 0: the default group width (64 lanes for >= 125 nodes) and register budget
+//          (the one-shot kernel uses this one)
+//   V = 1: same width, one fewer resident CTA per SM required (more registers)
+//   V = 2: the other group width (32 <-> 64 lanes for elements of > 32 nodes)
 constexpr int NUM_VARIANTS = 3;
-constexpr int CTX_RESERVE = 1024;   // bytes of per-warp contexts reserved in every layout
+constexpr int CTX_RESERVE = 1024;   // bytes of per-item contexts reserved in every layout
 
 template <int DIM, int NP, bool NS, typename Real, int V = 0>
 struct RhsLayout {
     using S = Shape<DIM, NP>;
     static constexpr int ND = S::ND, NF = S::NF, NLINE = S::NLINE, PPL = S::PPL;
-    static constexpr int GS = ND >= 32 ? 32 : next_pow2(ND);
-    static constexpr int EPW = 32 / GS;                 // elements per warp
+    static constexpr bool WIDE_DEFAULT = ND >= 125;
+    static constexpr bool WIDE = ND > 32 && (V == 2 ? !WIDE_DEFAULT : WIDE_DEFAULT);
+    static constexpr int GS = WIDE ? 64 : (ND >= 32 ? 32 : next_pow2(ND));
+    static constexpr int EPW = GS >= 32 ? 1 : 32 / GS;  // elements per warp
+    static constexpr int WPE = GS > 32 ? GS / 32 : 1;   // warps per element
     static constexpr int NPL = (ND + GS - 1) / GS;      // nodes per lane
     static constexpr int NPD = NLINE * PPL;             // pairs per direction
     static constexpr int NID = NLINE * (NP - 1);        // subcell interfaces per direction
     static constexpr int BUF = cmax(cmax(NPD, S::NFI), cmax(NID, (5 * ND + NF - 1) / NF)) * NF;
     static constexpr int K = HIdx<DIM>::K;
-    static constexpr int PER_ELEM = K * ND + cmax(BUF, NS ? DIM * NF * ND : 0);
+    // per-element shared memory, a multiple of 4 words so every element's area
+    // stays 16-byte aligned
+    static constexpr int PER_ELEM = (K * ND + cmax(BUF, NS ? DIM * NF * ND : 0) + 3) / 4 * 4;
     static constexpr bool F64 = sizeof(Real) == 8;
     static constexpr int MINB_CFG = NS ? (F64 ? PRANDTL_NS_MINB : PRANDTL_NS32_MINB)
                                        : (F64 ? PRANDTL_EULER_MINB : PRANDTL_EULER32_MINB);
-    static constexpr int WARPS_BASE = NS ? PRANDTL_NS_WARPS : PRANDTL_EULER_WARPS;
-    static constexpr int WARPS_CFG = V == 2 ? cmax(1, WARPS_BASE / 2) : WARPS_BASE;
+    static constexpr int WARPS_CFG = NS ? PRANDTL_NS_WARPS : PRANDTL_EULER_WARPS;
     // warps per CTA: the configured count, reduced so the CTA's elements fit the
-    // 227 KB shared-memory limit
+    // 227 KB shared-memory limit (whole elements, whole warps)
     static constexpr int SMEM_MAX = 227 * 1024;
-    static constexpr int FIT = ((SMEM_MAX - CTX_RESERVE) / (int)sizeof(Real) - S::TAB) / (PER_ELEM * EPW);
-    static constexpr int WARPS = cmax(1, FIT < WARPS_CFG ? FIT : WARPS_CFG);
-    static constexpr int EPB = WARPS * EPW;             // elements per CTA
+    static constexpr int FIT_ELEMS = ((SMEM_MAX - CTX_RESERVE) / (int)sizeof(Real) - S::TAB) / PER_ELEM;
+    static constexpr int FIT_WARPS = GS > 32 ? FIT_ELEMS * WPE : FIT_ELEMS / EPW;
+    static constexpr int WARPS_FIT = FIT_WARPS < WARPS_CFG ? FIT_WARPS : WARPS_CFG;
+    static constexpr int WARPS = cmax(WPE, WARPS_FIT / WPE * WPE);
     static constexpr int THREADS = WARPS * 32;
+    static constexpr int EPB = THREADS / GS;            // elements per CTA
+    // batch work items: one warp (EPW elements) or one two-warp group (1 element)
+    static constexpr int ITEM_THREADS = GS > 32 ? GS : 32;
+    static constexpr int ITEM_ELEMS = ITEM_THREADS / GS;
+    static constexpr int ITEMS_PER_CTA = THREADS / ITEM_THREADS;
+    static_assert(GS <= 32 || EPB < 16, "named barriers 1..15 identify the lane groups");
+    static_assert(BATCH_CHUNK % ITEM_ELEMS == 0, "items must not straddle padded solve ranges");
     // resident CTAs the register budget is sized for: the variant's request,
     // capped by what shared memory admits (228 KB per SM, 1 KB reserved per CTA)
     static constexpr int CTA_SMEM = S::TAB * (int)sizeof(Real) + CTX_RESERVE + EPB * PER_ELEM * (int)sizeof(Real);
     static constexpr int SMEM_BLOCKS = cmax(1, (228 * 1024) / (CTA_SMEM + 1024));
-    static constexpr int MINB_REQ = V == 1 ? MINB_CFG + 1 : (V == 2 ? 2 * MINB_CFG : MINB_CFG);
+    static constexpr int MINB_REQ = V == 1 ? cmax(1, MINB_CFG - 1) : MINB_CFG;
     static constexpr int MIN_BLOCKS = MINB_REQ < SMEM_BLOCKS ? MINB_REQ : SMEM_BLOCKS;
 };
+
+// Synchronise the GS lanes of lane group `gid` (its index within the CTA).
+template <int GS>
+__device__ __forceinline__ void group_sync(int gid) {
+    if constexpr (GS <= 32) {
+        __syncwarp();
+    } else {
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + gid), "n"(GS) : "memory");
+    }
+}
 
 // Instance-local operands of one element evaluation (the one-shot kernels build
 // it from their arguments, the batch kernels from the solve's table entry).
@@ -357,7 +380,7 @@ __device__ __forceinline__ int batch_slot(const int *prefix, int n, int first) {
 // in FP64 from the FP64 state, and the RK stage update is FP64.
 template <int DIM, int NP, bool NS, typename Real, typename LY>
 __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P, int e, bool active,
-                                            const Real *sT, Real *sH, int li, int lane) {
+                                            const Real *sT, Real *sH, int li, int lane, int gid) {
     using S = Shape<DIM, NP>;
     constexpr int ND = S::ND, NF = S::NF, PPL = S::PPL;
     constexpr int NFN = S::NFN, NFI = S::NFI, GS = LY::GS, NPL = LY::NPL;
@@ -384,7 +407,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 
     // ---- own nodes: hoisted primitives (formed in FP64); largest |V|+c
     double lam = 0.0;
-#pragma unroll
+#pragma unroll 1
     for (int k = 0; k < NPL; ++k) {
         const int n = li + k * GS;
         if (n < ND) {
@@ -401,13 +424,13 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
         for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
         if (lane == 0) atomic_max_pos(a.lambda, v);
     }
-    __syncwarp();
+    group_sync<GS>(gid);
 
     // ---- blending coefficient (PerssonPeraireIndicator.cpp:21-58, DGSEMOperator.cpp:60-80)
     Real alpha = 0;
     if (P.blending) {
         Real *b0 = sF, *b1 = sF + ND;
-#pragma unroll
+#pragma unroll 1
         for (int k = 0; k < NPL; ++k) {
             const int n = li + k * GS;
             if (n < ND) {
@@ -416,12 +439,12 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 b0[n] = q.rho * (Real(0.5) * q.rbeta * q.rho);
             }
         }
-        __syncwarp();
+        group_sync<GS>(gid);
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {   // modes = V^-1 (rho p), one direction per pass
             const Real *in = (d & 1) ? b1 : b0;
             Real *out = (d & 1) ? b0 : b1;
-#pragma unroll
+#pragma unroll 1
             for (int k = 0; k < NPL; ++k) {
                 const int n = li + k * GS;
                 if (n < ND) {
@@ -435,10 +458,10 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                     out[n] = s;
                 }
             }
-            __syncwarp();
+            group_sync<GS>(gid);
         }
         double e0 = 0, e1 = 0, e2 = 0;
-#pragma unroll
+#pragma unroll 1
         for (int k = 0; k < NPL; ++k) {
             const int n = li + k * GS;
             if (n < ND) {
@@ -453,10 +476,24 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 if (mx <= NP - 3) e2 += md * md;
             }
         }
-        for (int o = GS / 2; o > 0; o >>= 1) {
+        for (int o = (GS < 32 ? GS : 32) / 2; o > 0; o >>= 1) {
             e0 += __shfl_xor_sync(0xffffffffu, e0, o);
             e1 += __shfl_xor_sync(0xffffffffu, e1, o);
             e2 += __shfl_xor_sync(0xffffffffu, e2, o);
+        }
+        if constexpr (GS > 32) {
+            // two warps per element: combine the warps' sums through shared
+            // memory past the two mode buffers (8-byte aligned slots)
+            double *xch = reinterpret_cast<double *>(sH + ((LY::K * ND + 2 * ND + 1) & ~1));
+            if ((li & 31) == 0) {
+                xch[3 * (li >> 5)] = e0;
+                xch[3 * (li >> 5) + 1] = e1;
+                xch[3 * (li >> 5) + 2] = e2;
+            }
+            group_sync<GS>(gid);
+            e0 = xch[0] + xch[3];
+            e1 = xch[1] + xch[4];
+            e2 = xch[2] + xch[5];
         }
         double eta = 1.0 - e1 / e0;
         eta = fmax(eta, 1.0 - e2 / e1);
@@ -467,7 +504,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
         al = fmin(al, P.alpha_max);
         alpha = Real(al);
         if (li == 0 && a.alpha && active) a.alpha[e] = al;
-        __syncwarp();
+        group_sync<GS>(gid);
     }
 
     Real dUi[NPL][NF], dUv[NPL][NF];
@@ -478,7 +515,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 
     // ---- NS: contravariant viscous flux of every own node (flux_mat = adj * Fv^T, :632)
     if constexpr (NS) {
-#pragma unroll
+#pragma unroll 1
         for (int k = 0; k < NPL; ++k) {
             const int n = li + k * GS;
             if (n < ND) {
@@ -508,7 +545,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                     for (int f = 0; f < NF; ++f) sV[(r * NF + f) * ND + n] = Vc[r][f];
             }
         }
-        __syncwarp();
+        group_sync<GS>(gid);
         // sum_l Dhat(i,l) Fv_l along each direction (:710-738)
 #pragma unroll
         for (int k = 0; k < NPL; ++k) {
@@ -530,7 +567,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 }
             }
         }
-        __syncwarp();   // the pair phase overwrites the buffer
+        group_sync<GS>(gid);   // the pair phase overwrites the buffer
     }
 
     // ---- inviscid flux differencing, one direction at a time:
@@ -551,7 +588,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 #pragma unroll
             for (int f = 0; f < NF; ++f) sF[f * NPD + p] = F[f];
         }
-        __syncwarp();
+        group_sync<GS>(gid);
 #pragma unroll
         for (int k = 0; k < NPL; ++k) {
             const int n = li + k * GS;
@@ -586,7 +623,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 }
             }
         }
-        __syncwarp();
+        group_sync<GS>(gid);
     }
     Real acc[NPL][NF];
 #pragma unroll
@@ -620,7 +657,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 #pragma unroll
                 for (int f = 0; f < NF; ++f) sF[f * NID + it] = F[f];
             }
-            __syncwarp();
+            group_sync<GS>(gid);
 #pragma unroll
             for (int k = 0; k < NPL; ++k) {
                 const int n = li + k * GS;
@@ -641,7 +678,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                     }
                 }
             }
-            __syncwarp();
+            group_sync<GS>(gid);
         }
 #pragma unroll
         for (int k = 0; k < NPL; ++k)
@@ -703,7 +740,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 #pragma unroll
         for (int f = 0; f < NF; ++f) sF[f * NFI + it] = aw * (own_is_1 ? (fn[f] - flux[f]) : (flux[f] - fn[f]));
     }
-    __syncwarp();
+    group_sync<GS>(gid);
 
     // ---- gather face terms, epilogue (FP64 state update)
     if (!active) return;
@@ -785,19 +822,20 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
     const bool active = e_raw < m.E;
     const ElemIO io = io_from_args(m, a);
     rhs_element<DIM, NP, NS, Real, LY>(io, P, active ? e_raw : m.E - 1, active, smem,
-                                       smem + Shape<DIM, NP>::TAB + grp * LY::PER_ELEM, li, lane);
+                                       smem + Shape<DIM, NP>::TAB + grp * LY::PER_ELEM, li, lane, grp);
 }
 
-// Persistent batch kernel: a fixed grid walks the class's work items (EPW
-// elements of one solve per warp) with a grid-stride loop; the item count and
-// the solves are read from device memory, so a captured graph stays valid as
-// solves are admitted and retired.  Items of finished solves and items wholly
-// inside a solve's padding are skipped (warp-uniform).
+// Persistent batch kernel: a fixed grid walks the class's work items with a
+// grid-stride loop.  An item is one warp's EPW elements, or one two-warp
+// group's element, of one solve.  The item count and the solves are read from
+// device memory, so a captured graph stays valid as solves are admitted and
+// retired.  Items of finished solves and items wholly inside a solve's padding
+// are skipped (uniformly over the item's lanes).
 template <int DIM, int NP, bool NS, typename Real, int V>
 __global__ void __launch_bounds__(RhsLayout<DIM, NP, NS, Real, V>::THREADS, (RhsLayout<DIM, NP, NS, Real, V>::MIN_BLOCKS))
 rhs_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_constant__ OpTables T) {
     using LY = RhsLayout<DIM, NP, NS, Real, V>;
-    static_assert(LY::WARPS * sizeof(WarpCtx) <= CTX_RESERVE, "per-warp contexts exceed the reserve");
+    static_assert(LY::ITEMS_PER_CTA * sizeof(WarpCtx) <= CTX_RESERVE, "per-item contexts exceed the reserve");
     constexpr int TABB = (Shape<DIM, NP>::TAB * (int)sizeof(Real) + 15) / 16 * 16;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Real *sT = reinterpret_cast<Real *>(smem_raw);
@@ -805,33 +843,35 @@ rhs_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_consta
     Real *sE = reinterpret_cast<Real *>(smem_raw + TABB + CTX_RESERVE);
     load_tables<NP, Real>(T, sT, threadIdx.x, LY::THREADS);
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int grp = threadIdx.x / LY::GS;
+    const int lane = threadIdx.x & 31;
+    const int grp = threadIdx.x / LY::GS;              // element slot (lane group) in the CTA
     const int li = threadIdx.x - grp * LY::GS;
-    const int gw = lane / LY::GS;                  // element within the warp's item
-    WarpCtx *ctx = ctxs + warp;
+    const int slot = threadIdx.x / LY::ITEM_THREADS;   // item slot in the CTA
+    const int il = threadIdx.x - slot * LY::ITEM_THREADS;
+    const int gw = il / LY::GS;                        // element within the item
+    WarpCtx *ctx = ctxs + slot;
     Real *sH = sE + grp * LY::PER_ELEM;
     const int n = c.hdr[0];
-    const int total = n > 0 ? c.prefix[n] / LY::EPW : 0;
-    for (int item = blockIdx.x * LY::WARPS + warp; item < total; item += gridDim.x * LY::WARPS) {
-        const int first = item * LY::EPW;
+    const int total = n > 0 ? c.prefix[n] / LY::ITEM_ELEMS : 0;
+    for (int item = blockIdx.x * LY::ITEMS_PER_CTA + slot; item < total; item += gridDim.x * LY::ITEMS_PER_CTA) {
+        const int first = item * LY::ITEM_ELEMS;
         const int s = batch_slot(c.prefix, n, first);
         BatchInst *Im = c.tab + __ldg(c.ids + s);
         const int E = Im->E;
         const int e0 = first - __ldg(c.prefix + s);
         if (e0 >= E || Im->steps_left <= 0) continue;
-        __syncwarp();
+        group_sync<LY::ITEM_THREADS>(slot);   // the previous item's reads of ctx are done
         {
             const int *src = reinterpret_cast<const int *>(&Im->P);
             int *dst = reinterpret_cast<int *>(&ctx->P);
-            for (int q = lane; q < (int)(sizeof(PhysParams) / 4); q += 32) dst[q] = src[q];
-            if (lane == 0) ctx->io = io_from_batch(*Im, Im, st);
+            if (il < 32)
+                for (int q = il; q < (int)(sizeof(PhysParams) / 4); q += 32) dst[q] = src[q];
+            if (il == 0) ctx->io = io_from_batch(*Im, Im, st);
         }
-        __syncwarp();
+        group_sync<LY::ITEM_THREADS>(slot);
         const int e_raw = e0 + gw;
         const bool active = e_raw < E;
-        rhs_element<DIM, NP, NS, Real, LY>(ctx->io, ctx->P, active ? e_raw : E - 1, active, sT, sH, li, lane);
-        __syncwarp();
+        rhs_element<DIM, NP, NS, Real, LY>(ctx->io, ctx->P, active ? e_raw : E - 1, active, sT, sH, li, lane, grp);
     }
 }
 
@@ -1097,7 +1137,7 @@ cudaError_t rhs_batch_prepare_np(BatchKernelInfo *info) {
     info->threads = LY::THREADS;
     info->smem = (int)sm;
     info->regs = fa.numRegs;
-    info->elems_per_item = LY::EPW;
+    info->elems_per_item = LY::ITEM_ELEMS;
     return cudaSuccess;
 }
 template <int DIM, int NP, bool NS, typename Real, int V>
