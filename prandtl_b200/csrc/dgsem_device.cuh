@@ -56,6 +56,9 @@ __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
 template <int DIM, typename Real>
 struct Prim {
     Real rho, rrho, v[DIM], vsq, beta, rbeta, lam;
+    // pressure: p itself from primitives(); in the FP32-bulk form's working
+    // copies p - p_ref, with p_ref a pressure of the evaluating element
+    Real dp;
 };
 
 // ChandrashekarFlux.cpp:22-68 per node: v = m/rho, p = (g-1)(E - rho|v|^2/2),
@@ -76,6 +79,7 @@ __device__ __forceinline__ Prim<DIM, Real> primitives(const Real *s, Real gamma,
     q.beta = Real(0.5) * q.rho * rcp(p);
     q.rbeta = Real(2) * p * q.rrho;
     q.lam = sqrt(q.vsq) + sqrt(gamma * p * q.rrho);
+    q.dp = p;
     return q;
 }
 
@@ -103,6 +107,23 @@ __device__ __forceinline__ void log_mean(Real x, Real y, Real rx, Real &mean, Re
     }
 }
 
+// Pressure term of the momentum flux.  FP64: p_hat.  FP32-bulk form: the
+// element's constant reference pressure is left out, p_hat - p_ref =
+// (beta1 dp1 + beta2 dp2) / (beta1 + beta2) with dp = p - p_ref formed in FP64
+// per node, so the O(1/Mach^2) constant that cancels in the flux differencing
+// never enters the FP32 sums.  A constant pressure contributes nothing to
+// the element's RHS (volume and surface terms cancel for affine elements),
+// so this changes only the rounding.
+template <int DIM, typename Real>
+__device__ __forceinline__ Real momentum_pressure(const Prim<DIM, Real> &a, const Prim<DIM, Real> &b, Real p_hat,
+                                                  Real rs_beta) {
+    if constexpr (sizeof(Real) == 8) {
+        return p_hat;
+    } else {
+        return fma(a.beta, a.dp, b.beta * b.dp) * rs_beta;
+    }
+}
+
 // ChandrashekarFlux.cpp:11-83 with metric1 == metric2 == m (affine element,
 // so ComputeMean returns m exactly).
 template <int DIM, typename Real>
@@ -122,9 +143,10 @@ __device__ __forceinline__ void volume_flux(const Prim<DIM, Real> &a, const Prim
     const Real p_hat = Real(0.5) * (a.rho + b.rho) * rs_beta;   // 0.5(rho1+rho2)/(beta1+beta2)
     h += Real(0.5) * gammaM1Inverse * ibeta_ln + p_hat * irho_ln;
     const Real F0 = rho_ln * Vn;
+    const Real p_mom = momentum_pressure(a, b, p_hat, rs_beta);
     F[0] = F0;
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) F[1 + d] = F0 * vm[d] + p_hat * m[d];
+    for (int d = 0; d < DIM; ++d) F[1 + d] = F0 * vm[d] + p_mom * m[d];
     F[NF - 1] = F0 * h;
 }
 
@@ -162,9 +184,10 @@ __device__ __forceinline__ void face_flux(const Real *s1, const Prim<DIM, Real> 
     diss += Real(0.5) * drho * gammaM1Inverse * ibeta_ln + Real(0.5) * rho_mean * gammaM1Inverse * (b.rbeta - a.rbeta);
     const Real hl = dissipation ? Real(0.5) * dmax(a.lam, b.lam) * sqrt(nn) : Real(0);
     const Real F0 = rho_ln * Vn;
+    const Real p_mom = momentum_pressure(a, b, p_hat, rs_beta);
     flux[0] = F0 - hl * drho;
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) flux[1 + d] = F0 * vm[d] + p_hat * nor[d] - hl * (s2[1 + d] - s1[1 + d]);
+    for (int d = 0; d < DIM; ++d) flux[1 + d] = F0 * vm[d] + p_mom * nor[d] - hl * (s2[1 + d] - s1[1 + d]);
     flux[NF - 1] = F0 * h - hl * diss;
 }
 
@@ -222,6 +245,53 @@ __device__ __forceinline__ void conserv2entropy(const Real *s, const PhysParams 
 #pragma unroll
     for (int d = 0; d < DIM; ++d) v[1 + d] = beta * vel[d];
     v[NF - 1] = -beta;
+}
+
+// FP32-bulk form: entropy variables relative to those of a reference node of
+// the evaluating element.  Constants drop out of the lifted gradients (the
+// derivative of a constant and the jump of a shared constant are zero), so
+// only the O(1) variation is carried in FP32: s - s_ref = log1p(p/p_ref - 1) -
+// gamma log1p(rho/rho_ref - 1) from ratios formed in FP64, and
+// beta v^2/2 - (beta v^2/2)_ref, beta_ref - beta in FP64 before rounding.
+struct EntropyRef {
+    double rp, rrho, beta, bvsq;   // 1/p, 1/rho, rho/p, beta |v|^2 / 2 of the reference node
+};
+template <int DIM>
+__device__ __forceinline__ EntropyRef entropy_ref(const double *s, const PhysParams &P) {
+    constexpr int NF = DIM + 2;
+    EntropyRef R;
+    R.rrho = rcp(s[0]);
+    double vv = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        const double vd = s[1 + d] * R.rrho;
+        vv += vd * vd;
+    }
+    const double p = P.gammaM1 * (s[NF - 1] - s[0] * (0.5 * vv));
+    R.rp = rcp(p);
+    R.beta = s[0] * R.rp;
+    R.bvsq = R.beta * (0.5 * vv);
+    return R;
+}
+template <int DIM>
+__device__ __forceinline__ void conserv2entropy_rel(const double *s, const PhysParams &P, const EntropyRef &R,
+                                                    float *v) {
+    constexpr int NF = DIM + 2;
+    const double minv = rcp(s[0]);
+    double vel[DIM], vv = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        vel[d] = s[1 + d] * minv;
+        vv += vel[d] * vel[d];
+    }
+    const double v_sq = 0.5 * vv;
+    const double p = P.gammaM1 * (s[NF - 1] - s[0] * v_sq);
+    const double beta = s[0] * rcp(p);
+    const float srel = log1pf(float(fma(p, R.rp, -1.0))) - float(P.gamma) * log1pf(float(fma(s[0], R.rrho, -1.0)));
+    v[0] = -srel * float(P.gammaM1Inverse) - float(fma(beta, v_sq, -R.bvsq));
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[1 + d] = float(beta * vel[d]);
+    v[NF - 1] = float(R.beta - beta);
 }
 
 // BasicOperations.cpp:126-170 for one node and one derivative direction.

@@ -141,11 +141,14 @@ __device__ __forceinline__ void block_max_to(unsigned long long *dst, double v, 
 }
 
 // Hoisted per-node primitive table in shared memory: H[k*ND + node].
+// The FP32-bulk form also keeps dp = p - p_ref (slot DP).
 template <int DIM>
 struct HIdx {
     static constexpr int RHO = 0, RRHO = 1, V = 2, VSQ = 2 + DIM, BETA = 3 + DIM, RBETA = 4 + DIM,
-                         LAM = 5 + DIM, K = 6 + DIM;
+                         LAM = 5 + DIM, K = 6 + DIM, DP = 6 + DIM;
 };
+template <int DIM, typename Real>
+constexpr int hoisted_count() { return HIdx<DIM>::K + (sizeof(Real) == 4 ? 1 : 0); }
 template <int DIM, int ND, typename Real>
 __device__ __forceinline__ Prim<DIM, Real> load_prim(const Real *sH, int n) {
     using I = HIdx<DIM>;
@@ -158,10 +161,11 @@ __device__ __forceinline__ Prim<DIM, Real> load_prim(const Real *sH, int n) {
     q.beta = sH[I::BETA * ND + n];
     q.rbeta = sH[I::RBETA * ND + n];
     q.lam = sH[I::LAM * ND + n];
+    if constexpr (sizeof(Real) == 4) q.dp = sH[I::DP * ND + n];
     return q;
 }
 template <int DIM, int ND, typename Real>
-__device__ __forceinline__ void store_prim(Real *sH, int n, const Prim<DIM, double> &q) {
+__device__ __forceinline__ void store_prim(Real *sH, int n, const Prim<DIM, double> &q, double pref) {
     using I = HIdx<DIM>;
     sH[I::RHO * ND + n] = Real(q.rho);
     sH[I::RRHO * ND + n] = Real(q.rrho);
@@ -171,10 +175,12 @@ __device__ __forceinline__ void store_prim(Real *sH, int n, const Prim<DIM, doub
     sH[I::BETA * ND + n] = Real(q.beta);
     sH[I::RBETA * ND + n] = Real(q.rbeta);
     sH[I::LAM * ND + n] = Real(q.lam);
+    if constexpr (sizeof(Real) == 4) sH[I::DP * ND + n] = Real(q.dp - pref);
 }
-// Working-precision copy of primitives computed in FP64.
+// Working-precision copy of primitives computed in FP64 (pressure relative
+// to pref in the FP32-bulk form).
 template <int DIM, typename Real>
-__device__ __forceinline__ Prim<DIM, Real> cast_prim(const Prim<DIM, double> &q) {
+__device__ __forceinline__ Prim<DIM, Real> cast_prim(const Prim<DIM, double> &q, double pref) {
     Prim<DIM, Real> r;
     r.rho = Real(q.rho);
     r.rrho = Real(q.rrho);
@@ -184,6 +190,7 @@ __device__ __forceinline__ Prim<DIM, Real> cast_prim(const Prim<DIM, double> &q)
     r.beta = Real(q.beta);
     r.rbeta = Real(q.rbeta);
     r.lam = Real(q.lam);
+    r.dp = sizeof(Real) == 4 ? Real(q.dp - pref) : Real(q.dp);
     return r;
 }
 
@@ -238,7 +245,7 @@ struct RhsLayout {
     static constexpr int NPD = NLINE * PPL;             // pairs per direction
     static constexpr int NID = NLINE * (NP - 1);        // subcell interfaces per direction
     static constexpr int BUF = cmax(cmax(NPD, S::NFI), cmax(NID, (5 * ND + NF - 1) / NF)) * NF;
-    static constexpr int K = HIdx<DIM>::K;
+    static constexpr int K = hoisted_count<DIM, Real>();
     // per-element shared memory, a multiple of 4 words so every element's area
     // stays 16-byte aligned
     static constexpr int PER_ELEM = (K * ND + cmax(BUF, NS ? DIM * NF * ND : 0) + 3) / 4 * 4;
@@ -405,6 +412,15 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
     const double J = __ldg(geo + DIM * DIM);
     const Real mJ = Real(1.0 / J);
 
+    // FP32-bulk form: reference pressure of the element (node 0), FP64
+    double pref = 0.0;
+    if constexpr (!LY::F64) {
+        double s0[NF];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) s0[f] = __ldg(a.u + f * Ndof + (long long)e * ND);
+        pref = primitives<DIM, double>(s0, gamma, gm1).dp;
+    }
+
     // ---- own nodes: hoisted primitives (formed in FP64); largest |V|+c
     double lam = 0.0;
 #pragma unroll 1
@@ -415,7 +431,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 #pragma unroll
             for (int f = 0; f < NF; ++f) st[f] = __ldg(a.u + f * Ndof + (long long)e * ND + n);
             const Prim<DIM, double> q = primitives<DIM, double>(st, gamma, gm1);
-            store_prim<DIM, ND, Real>(sH, n, q);
+            store_prim<DIM, ND, Real>(sH, n, q, pref);
             lam = fmax(lam, q.lam);
         }
     }
@@ -703,7 +719,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
         for (int q = 0; q < DIM; ++q) nor[q] = Real(__ldg(a.fnor + (long long)t.z * DIM + q));
         Prim<DIM, Real> po = load_prim<DIM, ND, Real>(sH, no);
         const Prim<DIM, double> pn64 = primitives<DIM, double>(sn, gamma, gm1);
-        Prim<DIM, Real> pn = cast_prim<DIM, Real>(pn64);
+        Prim<DIM, Real> pn = cast_prim<DIM, Real>(pn64, pref);
 #pragma unroll
         for (int f = 0; f < NF; ++f) fn[f] = 0;
         if constexpr (NS) {
@@ -727,8 +743,8 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 const Prim<DIM, double> po64 = primitives<DIM, double>(so, gamma, gm1);
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) { so[1 + d] *= po64.rrho; sn[1 + d] *= pn64.rrho; }
-                po = cast_prim<DIM, Real>(primitives<DIM, double>(so, gamma, gm1));
-                pn = cast_prim<DIM, Real>(primitives<DIM, double>(sn, gamma, gm1));
+                po = cast_prim<DIM, Real>(primitives<DIM, double>(so, gamma, gm1), pref);
+                pn = cast_prim<DIM, Real>(primitives<DIM, double>(sn, gamma, gm1), pref);
             }
         }
 #pragma unroll
@@ -878,40 +894,48 @@ rhs_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_consta
 // ------------------------------------------------------------ BR1 lifting
 // Entropy variables (BasicOperations.cpp:81-104), element gradient
 // (LiftingBR1.cpp:156-272), face lifting 1/2 (v2 - v1) n (LiftingBR1.cpp:10-115)
-// and the chain rule to primitive gradients (BasicOperations.cpp:126-170).
-// The arithmetic is FP64 in both forms (it is per node and cheap); the lifted
-// gradients are stored in the working precision Out (double, or float for the
-// FP32-bulk form).
+// and the chain rule to primitive gradients (BasicOperations.cpp:126-170), in
+// the working precision W: double, or float for the FP32-bulk form, where the
+// entropy variables are taken relative to the element's node 0 (constants
+// drop out of the gradients) and only their logarithms of FP64 ratios are
+// evaluated in FP32.
 //
 // The element function uses __syncthreads: every thread of the CTA calls it
 // with the same control flow (n = node, sElem = this element's area).
-template <int DIM, int NP, typename Out>
+template <int DIM, int NP, typename W>
 __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &P, int e, bool active,
-                                             const double *sT, double *sElem, int n) {
+                                             const W *sT, W *sElem, int n) {
     using S = Shape<DIM, NP>;
     constexpr int ND = S::ND, NF = S::NF, NFN = S::NFN, NFI = S::NFI;
-    const double *sD = sT, *sW = sT + 4 * NP * NP;
-    Out *gout = reinterpret_cast<Out *>(a.grad);
-    double *sU = sElem;
-    double *sVe = sU + NF * ND;
-    double *sS = sVe + NF * ND;
+    constexpr bool F64 = sizeof(W) == 8;
+    const W *sD = sT, *sW = sT + 4 * NP * NP;
+    W *gout = reinterpret_cast<W *>(a.grad);
+    W *sVe = sElem;                 // entropy variables [NF][ND]
+    W *sS = sVe + NF * ND;          // face terms [DIM][NF][NFI]
     const long long Ndof = a.Ndof;
     const long long gnode = (long long)e * ND + n;
-    double st[NF], v[NF];
+    double st[NF];
+    W v[NF];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) {
-        st[f] = __ldg(a.u + f * Ndof + gnode);
-        sU[f * ND + n] = st[f];
+    for (int f = 0; f < NF; ++f) st[f] = __ldg(a.u + f * Ndof + gnode);
+    EntropyRef R{};
+    if constexpr (F64) {
+        conserv2entropy<DIM, double>(st, P, reinterpret_cast<double *>(v));
+    } else {
+        double s0[NF];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) s0[f] = __ldg(a.u + f * Ndof + (long long)e * ND);
+        R = entropy_ref<DIM>(s0, P);
+        conserv2entropy_rel<DIM>(st, P, R, reinterpret_cast<float *>(v));
     }
-    conserv2entropy<DIM, double>(st, P, v);
 #pragma unroll
     for (int f = 0; f < NF; ++f) sVe[f * ND + n] = v[f];
     const double *geo = a.geo + (long long)e * (DIM * DIM + 1);
-    double adj[DIM][DIM];
+    W adj[DIM][DIM];
 #pragma unroll
     for (int r = 0; r < DIM; ++r)
 #pragma unroll
-        for (int q = 0; q < DIM; ++q) adj[r][q] = __ldg(geo + r * DIM + q);
+        for (int q = 0; q < DIM; ++q) adj[r][q] = W(__ldg(geo + r * DIM + q));
     const double J = __ldg(geo + DIM * DIM);
     int c[3];
     node_coords<NP>(n, c);
@@ -919,54 +943,56 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
     // face part first (its neighbour loads overlap the element part):
     // +1/(w0 J) * 1/2 (v_elem2 - v_elem1) * n_c on both sides
     __syncthreads();   // tables and entropy variables complete
-    const double aw = 1.0 / (sW[0] * J);
+    const W aw = W(1.0 / (double(sW[0]) * J));
     for (int it = n; it < NFI; it += ND) {
         const int lf = it / NFN, fa = it - lf * NFN;
         const int no = face_node<DIM, NP>(lf, fa);
         const int4 t = __ldg(a.nbr + (long long)e * (2 * DIM) + lf);
         const int nn = face_node<DIM, NP>(t.y, fa);
         const long long gn = (long long)t.x * ND + nn;
-        double sn[NF], vn[NF], nor[DIM];
+        double sn[NF];
+        W vn[NF], nor[DIM];
 #pragma unroll
         for (int f = 0; f < NF; ++f) sn[f] = __ldg(a.u + f * Ndof + gn);
-        conserv2entropy<DIM, double>(sn, P, vn);
+        if constexpr (F64) conserv2entropy<DIM, double>(sn, P, reinterpret_cast<double *>(vn));
+        else conserv2entropy_rel<DIM>(sn, P, R, reinterpret_cast<float *>(vn));
 #pragma unroll
-        for (int q = 0; q < DIM; ++q) nor[q] = __ldg(a.fnor + (long long)t.z * DIM + q);
+        for (int q = 0; q < DIM; ++q) nor[q] = W(__ldg(a.fnor + (long long)t.z * DIM + q));
         const bool own_is_1 = (t.w == 0);
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-            const double vo = sVe[f * ND + no];
-            const double jf = own_is_1 ? 0.5 * (vn[f] - vo) : 0.5 * (vo - vn[f]);
+            const W vo = sVe[f * ND + no];
+            const W jf = own_is_1 ? W(0.5) * (vn[f] - vo) : W(0.5) * (vo - vn[f]);
 #pragma unroll
             for (int q = 0; q < DIM; ++q) sS[(q * NF + f) * NFI + it] = aw * (jf * nor[q]);
         }
     }
 
     // element part: g1(f, r) = sum_l D(pos_r, l) v_l along direction r
-    double g1[NF][DIM];
+    W g1[NF][DIM];
 #pragma unroll
     for (int f = 0; f < NF; ++f)
 #pragma unroll
-        for (int r = 0; r < DIM; ++r) g1[f][r] = 0.0;
+        for (int r = 0; r < DIM; ++r) g1[f][r] = 0;
 #pragma unroll
     for (int r = 0; r < DIM; ++r) {
         int base, stride;
         line_base<DIM, NP>(r, line_index<DIM, NP>(r, c), base, stride);
 #pragma unroll
         for (int l = 0; l < NP; ++l) {
-            const double dl = sD[c[r] * NP + l];
+            const W dl = sD[c[r] * NP + l];
 #pragma unroll
             for (int f = 0; f < NF; ++f) g1[f][r] += sVe[f * ND + base + l * stride] * dl;
         }
     }
     // grad_mat2 = grad_mat1 * adj, times 1/J (LiftingBR1.cpp:205-206)
-    const double mJ = 1.0 / J;
-    double g[DIM][NF];
+    const W mJ = W(1.0 / J);
+    W g[DIM][NF];
 #pragma unroll
     for (int q = 0; q < DIM; ++q)
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-            double s = 0.0;
+            W s = 0;
 #pragma unroll
             for (int r = 0; r < DIM; ++r) s += g1[f][r] * adj[r][q];
             g[q][f] = s * mJ;
@@ -986,18 +1012,21 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
         }
     }
     if (!active) return;
+    W sw[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) sw[f] = W(st[f]);
 #pragma unroll
     for (int q = 0; q < DIM; ++q) {
-        entropygrad2primgrad<DIM, double>(st, P, g[q]);
+        entropygrad2primgrad<DIM, W>(sw, P, g[q]);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) gout[(q * NF + f) * Ndof + gnode] = Out(g[q][f]);
+        for (int f = 0; f < NF; ++f) gout[(q * NF + f) * Ndof + gnode] = g[q][f];
     }
 }
 
 template <int DIM, int NP>
 struct LiftLayout {
     using S = Shape<DIM, NP>;
-    static constexpr int PER_ELEM = 2 * S::NF * S::ND + DIM * S::NF * S::NFI;
+    static constexpr int PER_ELEM = S::NF * S::ND + DIM * S::NF * S::NFI;
 };
 constexpr int prev_pow2(int v) { return v <= 1 ? 1 : 2 * prev_pow2(v / 2); }
 // Batch lift CTA: a power-of-two number of elements, so an item (one CTA's
@@ -1015,8 +1044,8 @@ __global__ void __launch_bounds__(Shape<DIM, NP>::THREADS, 4)
 lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_constant__ OpTables T) {
     using S = Shape<DIM, NP>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *smem = reinterpret_cast<double *>(smem_raw);
-    load_tables<NP, double>(T, smem, threadIdx.x, S::THREADS);
+    Out *smem = reinterpret_cast<Out *>(smem_raw);
+    load_tables<NP, Out>(T, smem, threadIdx.x, S::THREADS);
     const int el = threadIdx.x / S::ND;
     const int n = threadIdx.x - el * S::ND;
     const int e_raw = blockIdx.x * S::EPB + el;
@@ -1039,12 +1068,12 @@ __global__ void __launch_bounds__(LiftBatchShape<DIM, NP>::THREADS, 4)
 lift_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_constant__ OpTables T) {
     using S = Shape<DIM, NP>;
     using LB = LiftBatchShape<DIM, NP>;
-    constexpr int TABB = (S::TAB * 8 + 15) / 16 * 16;
+    constexpr int TABB = (S::TAB * (int)sizeof(Out) + 15) / 16 * 16;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *sT = reinterpret_cast<double *>(smem_raw);
+    Out *sT = reinterpret_cast<Out *>(smem_raw);
     WarpCtx *ctx = reinterpret_cast<WarpCtx *>(smem_raw + TABB);
-    double *sE = reinterpret_cast<double *>(smem_raw + TABB + CTX_RESERVE);
-    load_tables<NP, double>(T, sT, threadIdx.x, LB::THREADS);
+    Out *sE = reinterpret_cast<Out *>(smem_raw + TABB + CTX_RESERVE);
+    load_tables<NP, Out>(T, sT, threadIdx.x, LB::THREADS);
     const int el = threadIdx.x / S::ND;
     const int nn = threadIdx.x - el * S::ND;
     const int n = c.hdr[0];
@@ -1082,16 +1111,16 @@ size_t rhs_batch_smem() {
     return (Shape<DIM, NP>::TAB * sizeof(Real) + 15) / 16 * 16 + CTX_RESERVE +
            sizeof(Real) * (size_t)LY::EPB * LY::PER_ELEM;
 }
-template <int DIM, int NP>
+template <int DIM, int NP, typename Out>
 size_t lift_smem() {
     using S = Shape<DIM, NP>;
-    return sizeof(double) * (S::TAB + (size_t)S::EPB * LiftLayout<DIM, NP>::PER_ELEM);
+    return sizeof(Out) * (S::TAB + (size_t)S::EPB * LiftLayout<DIM, NP>::PER_ELEM);
 }
-template <int DIM, int NP>
+template <int DIM, int NP, typename Out>
 size_t lift_batch_smem() {
     using S = Shape<DIM, NP>;
-    return (S::TAB * 8 + 15) / 16 * 16 + CTX_RESERVE +
-           sizeof(double) * (size_t)LiftBatchShape<DIM, NP>::EPB * LiftLayout<DIM, NP>::PER_ELEM;
+    return (S::TAB * sizeof(Out) + 15) / 16 * 16 + CTX_RESERVE +
+           sizeof(Out) * (size_t)LiftBatchShape<DIM, NP>::EPB * LiftLayout<DIM, NP>::PER_ELEM;
 }
 
 template <int DIM, int NP, bool NS, typename Real>
@@ -1111,7 +1140,7 @@ cudaError_t lift_launch_np(const MeshDev &m, const LiftArgs &a, const PhysParams
                            cudaStream_t s) {
     using S = Shape<DIM, NP>;
     const int grid = (m.E + S::EPB - 1) / S::EPB;
-    const size_t sm = lift_smem<DIM, NP>();
+    const size_t sm = lift_smem<DIM, NP, Out>();
     cudaError_t err = cudaFuncSetAttribute(lift_kernel<DIM, NP, Out>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (err != cudaSuccess) return err;
@@ -1150,7 +1179,7 @@ cudaError_t rhs_batch_launch_np(int grid, const BatchClassDev &c, const BatchSta
 template <int DIM, int NP, typename Out>
 cudaError_t lift_batch_prepare_np(BatchKernelInfo *info) {
     using S = LiftBatchShape<DIM, NP>;
-    const size_t sm = lift_batch_smem<DIM, NP>();
+    const size_t sm = lift_batch_smem<DIM, NP, Out>();
     cudaError_t err = cudaFuncSetAttribute(lift_batch_kernel<DIM, NP, Out>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (err != cudaSuccess) return err;
@@ -1170,7 +1199,7 @@ template <int DIM, int NP, typename Out>
 cudaError_t lift_batch_launch_np(int grid, const BatchClassDev &c, const BatchStage &st, const OpTables &T,
                                  cudaStream_t s) {
     using S = LiftBatchShape<DIM, NP>;
-    lift_batch_kernel<DIM, NP, Out><<<grid, S::THREADS, lift_batch_smem<DIM, NP>(), s>>>(c, st, T);
+    lift_batch_kernel<DIM, NP, Out><<<grid, S::THREADS, lift_batch_smem<DIM, NP, Out>(), s>>>(c, st, T);
     return cudaGetLastError();
 }
 
