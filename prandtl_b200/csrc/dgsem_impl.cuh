@@ -385,7 +385,7 @@ __device__ __forceinline__ int batch_slot(const int *prefix, int n, int first) {
 // flux differencing, surface fluxes, gradients): double for the plain FP64
 // path, float for the FP32-bulk form.  Per-node primitives are always formed
 // in FP64 from the FP64 state, and the RK stage update is FP64.
-template <int DIM, int NP, bool NS, typename Real, typename LY>
+template <int DIM, int NP, bool NS, bool VC, typename Real, typename LY>
 __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P, int e, bool active,
                                             const Real *sT, Real *sH, int li, int lane, int gid) {
     using S = Shape<DIM, NP>;
@@ -530,7 +530,20 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
         for (int f = 0; f < NF; ++f) { dUi[k][f] = 0; dUv[k][f] = 0; }
 
     // ---- NS: contravariant viscous flux of every own node (flux_mat = adj * Fv^T, :632)
-    if constexpr (NS) {
+    if constexpr (NS && VC) {
+        // formed by the lifting: rows f = 1..NF-1 of adj * Fv^T (the mass row is zero)
+#pragma unroll 1
+        for (int k = 0; k < NPL; ++k) {
+            const int n = li + k * GS;
+            if (n < ND) {
+#pragma unroll
+                for (int r = 0; r < DIM; ++r)
+#pragma unroll
+                    for (int f = 1; f < NF; ++f)
+                        sV[(r * NF + f) * ND + n] = __ldg(grad + (r * (NF - 1) + f - 1) * Ndof + (long long)e * ND + n);
+            }
+        }
+    } else if constexpr (NS) {
 #pragma unroll 1
         for (int k = 0; k < NPL; ++k) {
             const int n = li + k * GS;
@@ -561,8 +574,10 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                     for (int f = 0; f < NF; ++f) sV[(r * NF + f) * ND + n] = Vc[r][f];
             }
         }
+    }
+    if constexpr (NS) {
         group_sync<GS>(gid);
-        // sum_l Dhat(i,l) Fv_l along each direction (:710-738)
+        // sum_l Dhat(i,l) Fv_l along each direction (:710-738); the mass row is zero
 #pragma unroll
         for (int k = 0; k < NPL; ++k) {
             const int n = li + k * GS;
@@ -578,7 +593,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                     for (int l = 0; l < NP; ++l) {
                         const Real dh = sDh[pos * NP + l];
 #pragma unroll
-                        for (int f = 0; f < NF; ++f) dUv[k][f] += sV[(dir * NF + f) * ND + base + l * stride] * dh;
+                        for (int f = 1; f < NF; ++f) dUv[k][f] += sV[(dir * NF + f) * ND + base + l * stride] * dh;
                     }
                 }
             }
@@ -722,7 +737,21 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
         Prim<DIM, Real> pn = cast_prim<DIM, Real>(pn64, pref);
 #pragma unroll
         for (int f = 0; f < NF; ++f) fn[f] = 0;
-        if constexpr (NS) {
+        if constexpr (NS && VC) {
+            // 0.5 (Fv1 + Fv2) . n from the traces' contravariant viscous fluxes: for
+            // affine elements the outward scaled normal of local face lf is
+            // (lf odd ? +1 : -1) times row lf/2 of adj(J) (Nanson's formula), so
+            // Fv . n_out is a signed row of adj * Fv^T.  fn is taken along nor.
+            const int dd = lf >> 1, dn = t.y >> 1;
+            const Real sgo = (lf & 1) ? Real(1) : Real(-1), sgn = (t.y & 1) ? Real(1) : Real(-1);
+#pragma unroll
+            for (int f = 1; f < NF; ++f) {
+                const Real vo = __ldg(grad + (dd * (NF - 1) + f - 1) * Ndof + go);
+                const Real vn = __ldg(grad + (dn * (NF - 1) + f - 1) * Ndof + gn);
+                const Real avg = Real(0.5) * (sgo * vo - sgn * vn);
+                fn[f] = own_is_1 ? avg : -avg;
+            }
+        } else if constexpr (NS) {
             // DGSEMIntegrator.cpp:435-549: 0.5 (Fv1 + Fv2) . n from each trace's
             // own state and lifted gradients
 #pragma unroll
@@ -823,7 +852,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 }
 
 // One-shot kernel: grid = ceil(E / EPB), one element per lane group.
-template <int DIM, int NP, bool NS, typename Real>
+template <int DIM, int NP, bool NS, bool VC, typename Real>
 __global__ void __launch_bounds__(RhsLayout<DIM, NP, NS, Real>::THREADS, (RhsLayout<DIM, NP, NS, Real>::MIN_BLOCKS))
 rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_constant__ OpTables T) {
     using LY = RhsLayout<DIM, NP, NS, Real>;
@@ -837,7 +866,7 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
     const int e_raw = blockIdx.x * LY::EPB + grp;
     const bool active = e_raw < m.E;
     const ElemIO io = io_from_args(m, a);
-    rhs_element<DIM, NP, NS, Real, LY>(io, P, active ? e_raw : m.E - 1, active, smem,
+    rhs_element<DIM, NP, NS, VC, Real, LY>(io, P, active ? e_raw : m.E - 1, active, smem,
                                        smem + Shape<DIM, NP>::TAB + grp * LY::PER_ELEM, li, lane, grp);
 }
 
@@ -847,7 +876,7 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
 // device memory, so a captured graph stays valid as solves are admitted and
 // retired.  Items of finished solves and items wholly inside a solve's padding
 // are skipped (uniformly over the item's lanes).
-template <int DIM, int NP, bool NS, typename Real, int V>
+template <int DIM, int NP, bool NS, bool VC, typename Real, int V>
 __global__ void __launch_bounds__(RhsLayout<DIM, NP, NS, Real, V>::THREADS, (RhsLayout<DIM, NP, NS, Real, V>::MIN_BLOCKS))
 rhs_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_constant__ OpTables T) {
     using LY = RhsLayout<DIM, NP, NS, Real, V>;
@@ -887,7 +916,7 @@ rhs_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_consta
         group_sync<LY::ITEM_THREADS>(slot);
         const int e_raw = e0 + gw;
         const bool active = e_raw < E;
-        rhs_element<DIM, NP, NS, Real, LY>(ctx->io, ctx->P, active ? e_raw : E - 1, active, sT, sH, li, lane, grp);
+        rhs_element<DIM, NP, NS, VC, Real, LY>(ctx->io, ctx->P, active ? e_raw : E - 1, active, sT, sH, li, lane, grp);
     }
 }
 
@@ -902,7 +931,7 @@ rhs_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_consta
 //
 // The element function uses __syncthreads: every thread of the CTA calls it
 // with the same control flow (n = node, sElem = this element's area).
-template <int DIM, int NP, typename W>
+template <int DIM, int NP, typename W, bool VC>
 __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &P, int e, bool active,
                                              const W *sT, W *sElem, int n) {
     using S = Shape<DIM, NP>;
@@ -1016,10 +1045,32 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
 #pragma unroll
     for (int f = 0; f < NF; ++f) sw[f] = W(st[f]);
 #pragma unroll
-    for (int q = 0; q < DIM; ++q) {
-        entropygrad2primgrad<DIM, W>(sw, P, g[q]);
+    for (int q = 0; q < DIM; ++q) entropygrad2primgrad<DIM, W>(sw, P, g[q]);
+    if constexpr (VC) {
+        // the node's contravariant viscous flux adj * Fv^T, rows f = 1..NF-1
+        // (NavierStokesFlux.cpp:12-58 with this node's state and gradients;
+        // flux_mat of DGSEMIntegrator.cpp:632), [DIM][NF-1][Ndof]
+        const Prim<DIM, double> q64 = primitives<DIM, double>(st, P.gamma, P.gammaM1);
+        W vel[DIM], Vc[DIM][NF];
 #pragma unroll
-        for (int f = 0; f < NF; ++f) gout[(q * NF + f) * Ndof + gnode] = g[q][f];
+        for (int d = 0; d < DIM; ++d) vel[d] = W(q64.v[d]);
+#pragma unroll
+        for (int r = 0; r < DIM; ++r)
+#pragma unroll
+            for (int f = 0; f < NF; ++f) Vc[r][f] = 0;
+        viscous_flux<DIM, W>(W(q64.rho), W(q64.rrho), vel, W(q64.dp), g, P, [&](int f, int cc, W val) {
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) Vc[r][f] += adj[r][cc] * val;
+        });
+#pragma unroll
+        for (int r = 0; r < DIM; ++r)
+#pragma unroll
+            for (int f = 1; f < NF; ++f) gout[(r * (NF - 1) + f - 1) * Ndof + gnode] = Vc[r][f];
+    } else {
+#pragma unroll
+        for (int q = 0; q < DIM; ++q)
+#pragma unroll
+            for (int f = 0; f < NF; ++f) gout[(q * NF + f) * Ndof + gnode] = g[q][f];
     }
 }
 
@@ -1039,7 +1090,7 @@ struct LiftBatchShape {
     static_assert(BATCH_CHUNK % EPB == 0, "lift item must divide the padding chunk");
 };
 
-template <int DIM, int NP, typename Out>
+template <int DIM, int NP, typename Out, bool VC>
 __global__ void __launch_bounds__(Shape<DIM, NP>::THREADS, 4)
 lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_constant__ OpTables T) {
     using S = Shape<DIM, NP>;
@@ -1058,12 +1109,12 @@ lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_
     io.fnor = m.fnor;
     io.Ndof = m.Ndof;
     io.E = m.E;
-    lift_element<DIM, NP, Out>(io, P, active ? e_raw : m.E - 1, active, smem,
+    lift_element<DIM, NP, Out, VC>(io, P, active ? e_raw : m.E - 1, active, smem,
                                smem + S::TAB + el * LiftLayout<DIM, NP>::PER_ELEM, n);
 }
 
 // Persistent batch lift: CTA-level items of EPB elements of one solve.
-template <int DIM, int NP, typename Out>
+template <int DIM, int NP, typename Out, bool VC>
 __global__ void __launch_bounds__(LiftBatchShape<DIM, NP>::THREADS, 4)
 lift_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_constant__ OpTables T) {
     using S = Shape<DIM, NP>;
@@ -1095,7 +1146,7 @@ lift_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_const
         __syncthreads();
         const int e_raw = e0 + el;
         const bool active = e_raw < E;
-        lift_element<DIM, NP, Out>(ctx->io, ctx->P, active ? e_raw : E - 1, active, sT,
+        lift_element<DIM, NP, Out, VC>(ctx->io, ctx->P, active ? e_raw : E - 1, active, sT,
                                    sE + el * LiftLayout<DIM, NP>::PER_ELEM, nn);
     }
 }
@@ -1123,45 +1174,45 @@ size_t lift_batch_smem() {
            sizeof(Out) * (size_t)LiftBatchShape<DIM, NP>::EPB * LiftLayout<DIM, NP>::PER_ELEM;
 }
 
-template <int DIM, int NP, bool NS, typename Real>
+template <int DIM, int NP, bool NS, bool VC, typename Real>
 cudaError_t rhs_launch_np(const MeshDev &m, const RhsArgs &a, const PhysParams &P, const OpTables &T,
                           cudaStream_t s) {
     using LY = RhsLayout<DIM, NP, NS, Real>;
     const int grid = (m.E + LY::EPB - 1) / LY::EPB;
     const size_t sm = rhs_smem<DIM, NP, NS, Real>();
-    cudaError_t err = cudaFuncSetAttribute(rhs_kernel<DIM, NP, NS, Real>,
+    cudaError_t err = cudaFuncSetAttribute(rhs_kernel<DIM, NP, NS, VC, Real>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (err != cudaSuccess) return err;
-    rhs_kernel<DIM, NP, NS, Real><<<grid, LY::THREADS, sm, s>>>(m, a, P, T);
+    rhs_kernel<DIM, NP, NS, VC, Real><<<grid, LY::THREADS, sm, s>>>(m, a, P, T);
     return cudaGetLastError();
 }
-template <int DIM, int NP, typename Out>
+template <int DIM, int NP, typename Out, bool VC>
 cudaError_t lift_launch_np(const MeshDev &m, const LiftArgs &a, const PhysParams &P, const OpTables &T,
                            cudaStream_t s) {
     using S = Shape<DIM, NP>;
     const int grid = (m.E + S::EPB - 1) / S::EPB;
     const size_t sm = lift_smem<DIM, NP, Out>();
-    cudaError_t err = cudaFuncSetAttribute(lift_kernel<DIM, NP, Out>,
+    cudaError_t err = cudaFuncSetAttribute(lift_kernel<DIM, NP, Out, VC>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (err != cudaSuccess) return err;
-    lift_kernel<DIM, NP, Out><<<grid, S::THREADS, sm, s>>>(m, a, P, T);
+    lift_kernel<DIM, NP, Out, VC><<<grid, S::THREADS, sm, s>>>(m, a, P, T);
     return cudaGetLastError();
 }
 
 // Batch kernels: `prepare` sets the shared-memory attribute (outside any stream
 // capture) and reports the resident CTAs per SM; `launch` only launches.
-template <int DIM, int NP, bool NS, typename Real, int V>
+template <int DIM, int NP, bool NS, bool VC, typename Real, int V>
 cudaError_t rhs_batch_prepare_np(BatchKernelInfo *info) {
     using LY = RhsLayout<DIM, NP, NS, Real, V>;
     const size_t sm = rhs_batch_smem<DIM, NP, NS, Real, V>();
-    cudaError_t err = cudaFuncSetAttribute(rhs_batch_kernel<DIM, NP, NS, Real, V>,
+    cudaError_t err = cudaFuncSetAttribute(rhs_batch_kernel<DIM, NP, NS, VC, Real, V>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (err != cudaSuccess) return err;
     int nb = 0;
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rhs_batch_kernel<DIM, NP, NS, Real, V>, LY::THREADS, sm);
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rhs_batch_kernel<DIM, NP, NS, VC, Real, V>, LY::THREADS, sm);
     if (err != cudaSuccess) return err;
     cudaFuncAttributes fa{};
-    cudaFuncGetAttributes(&fa, rhs_batch_kernel<DIM, NP, NS, Real, V>);
+    cudaFuncGetAttributes(&fa, rhs_batch_kernel<DIM, NP, NS, VC, Real, V>);
     info->blocks_per_sm = nb;
     info->threads = LY::THREADS;
     info->smem = (int)sm;
@@ -1169,25 +1220,25 @@ cudaError_t rhs_batch_prepare_np(BatchKernelInfo *info) {
     info->elems_per_item = LY::ITEM_ELEMS;
     return cudaSuccess;
 }
-template <int DIM, int NP, bool NS, typename Real, int V>
+template <int DIM, int NP, bool NS, bool VC, typename Real, int V>
 cudaError_t rhs_batch_launch_np(int grid, const BatchClassDev &c, const BatchStage &st, const OpTables &T,
                                 cudaStream_t s) {
     using LY = RhsLayout<DIM, NP, NS, Real, V>;
-    rhs_batch_kernel<DIM, NP, NS, Real, V><<<grid, LY::THREADS, rhs_batch_smem<DIM, NP, NS, Real, V>(), s>>>(c, st, T);
+    rhs_batch_kernel<DIM, NP, NS, VC, Real, V><<<grid, LY::THREADS, rhs_batch_smem<DIM, NP, NS, Real, V>(), s>>>(c, st, T);
     return cudaGetLastError();
 }
-template <int DIM, int NP, typename Out>
+template <int DIM, int NP, typename Out, bool VC>
 cudaError_t lift_batch_prepare_np(BatchKernelInfo *info) {
     using S = LiftBatchShape<DIM, NP>;
     const size_t sm = lift_batch_smem<DIM, NP, Out>();
-    cudaError_t err = cudaFuncSetAttribute(lift_batch_kernel<DIM, NP, Out>,
+    cudaError_t err = cudaFuncSetAttribute(lift_batch_kernel<DIM, NP, Out, VC>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (err != cudaSuccess) return err;
     int nb = 0;
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, lift_batch_kernel<DIM, NP, Out>, S::THREADS, sm);
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, lift_batch_kernel<DIM, NP, Out, VC>, S::THREADS, sm);
     if (err != cudaSuccess) return err;
     cudaFuncAttributes fa{};
-    cudaFuncGetAttributes(&fa, lift_batch_kernel<DIM, NP, Out>);
+    cudaFuncGetAttributes(&fa, lift_batch_kernel<DIM, NP, Out, VC>);
     info->blocks_per_sm = nb;
     info->threads = S::THREADS;
     info->smem = (int)sm;
@@ -1195,11 +1246,11 @@ cudaError_t lift_batch_prepare_np(BatchKernelInfo *info) {
     info->elems_per_item = S::EPB;
     return cudaSuccess;
 }
-template <int DIM, int NP, typename Out>
+template <int DIM, int NP, typename Out, bool VC>
 cudaError_t lift_batch_launch_np(int grid, const BatchClassDev &c, const BatchStage &st, const OpTables &T,
                                  cudaStream_t s) {
     using S = LiftBatchShape<DIM, NP>;
-    lift_batch_kernel<DIM, NP, Out><<<grid, S::THREADS, lift_batch_smem<DIM, NP, Out>(), s>>>(c, st, T);
+    lift_batch_kernel<DIM, NP, Out, VC><<<grid, S::THREADS, lift_batch_smem<DIM, NP, Out>(), s>>>(c, st, T);
     return cudaGetLastError();
 }
 
@@ -1222,51 +1273,51 @@ cudaError_t lift_batch_launch_np(int grid, const BatchClassDev &c, const BatchSt
     default: return cudaErrorInvalidValue;                               \
     }
 
-template <int DIM, typename Real, bool NS>
+template <int DIM, typename Real, bool NS, bool VC>
 cudaError_t rhs_dispatch(int order, const MeshDev &m, const RhsArgs &a, const PhysParams &P,
                          const OpTables &T, cudaStream_t s) {
-    PRANDTL_ORDER_SWITCH((rhs_launch_np<DIM, NP, NS, Real>(m, a, P, T, s)))
+    PRANDTL_ORDER_SWITCH((rhs_launch_np<DIM, NP, NS, VC, Real>(m, a, P, T, s)))
 }
-template <int DIM, typename Out>
+template <int DIM, typename Out, bool VC>
 cudaError_t lift_dispatch(int order, const MeshDev &m, const LiftArgs &a, const PhysParams &P,
                           const OpTables &T, cudaStream_t s) {
-    PRANDTL_ORDER_SWITCH((lift_launch_np<DIM, NP, Out>(m, a, P, T, s)))
+    PRANDTL_ORDER_SWITCH((lift_launch_np<DIM, NP, Out, VC>(m, a, P, T, s)))
 }
-template <int DIM, typename Real, bool NS>
+template <int DIM, typename Real, bool NS, bool VC>
 cudaError_t rhs_batch_prepare(int order, int variant, BatchKernelInfo *info) {
     PRANDTL_ORDER_SWITCH(([&]() -> cudaError_t {
-        PRANDTL_VARIANT_SWITCH(return (rhs_batch_prepare_np<DIM, NP, NS, Real, VV>(info)))
+        PRANDTL_VARIANT_SWITCH(return (rhs_batch_prepare_np<DIM, NP, NS, VC, Real, VV>(info)))
     }()))
 }
-template <int DIM, typename Real, bool NS>
+template <int DIM, typename Real, bool NS, bool VC>
 cudaError_t rhs_batch_launch(int order, int variant, int grid, const BatchClassDev &c, const BatchStage &st,
                              const OpTables &T, cudaStream_t s) {
     PRANDTL_ORDER_SWITCH(([&]() -> cudaError_t {
-        PRANDTL_VARIANT_SWITCH(return (rhs_batch_launch_np<DIM, NP, NS, Real, VV>(grid, c, st, T, s)))
+        PRANDTL_VARIANT_SWITCH(return (rhs_batch_launch_np<DIM, NP, NS, VC, Real, VV>(grid, c, st, T, s)))
     }()))
 }
-template <int DIM, typename Out>
+template <int DIM, typename Out, bool VC>
 cudaError_t lift_batch_prepare(int order, BatchKernelInfo *info) {
-    PRANDTL_ORDER_SWITCH((lift_batch_prepare_np<DIM, NP, Out>(info)))
+    PRANDTL_ORDER_SWITCH((lift_batch_prepare_np<DIM, NP, Out, VC>(info)))
 }
-template <int DIM, typename Out>
+template <int DIM, typename Out, bool VC>
 cudaError_t lift_batch_launch(int order, int grid, const BatchClassDev &c, const BatchStage &st,
                               const OpTables &T, cudaStream_t s) {
-    PRANDTL_ORDER_SWITCH((lift_batch_launch_np<DIM, NP, Out>(grid, c, st, T, s)))
+    PRANDTL_ORDER_SWITCH((lift_batch_launch_np<DIM, NP, Out, VC>(grid, c, st, T, s)))
 }
 
-// One translation unit per (DIM, Real, NS) instantiates its share.
-#define PRANDTL_INSTANTIATE_RHS(DIMV, REAL, NSV)                                                        \
-    template cudaError_t rhs_dispatch<DIMV, REAL, NSV>(int, const MeshDev &, const RhsArgs &,           \
+// One translation unit per (DIM, Real, physics) instantiates its share.
+#define PRANDTL_INSTANTIATE_RHS(DIMV, REAL, NSV, VCV)                                                   \
+    template cudaError_t rhs_dispatch<DIMV, REAL, NSV, VCV>(int, const MeshDev &, const RhsArgs &,      \
+                                                            const PhysParams &, const OpTables &, cudaStream_t); \
+    template cudaError_t rhs_batch_prepare<DIMV, REAL, NSV, VCV>(int, int, BatchKernelInfo *);          \
+    template cudaError_t rhs_batch_launch<DIMV, REAL, NSV, VCV>(int, int, int, const BatchClassDev &,   \
+                                                                const BatchStage &, const OpTables &, cudaStream_t);
+#define PRANDTL_INSTANTIATE_LIFT(DIMV, OUT, VCV)                                                        \
+    template cudaError_t lift_dispatch<DIMV, OUT, VCV>(int, const MeshDev &, const LiftArgs &,          \
                                                        const PhysParams &, const OpTables &, cudaStream_t); \
-    template cudaError_t rhs_batch_prepare<DIMV, REAL, NSV>(int, int, BatchKernelInfo *);               \
-    template cudaError_t rhs_batch_launch<DIMV, REAL, NSV>(int, int, int, const BatchClassDev &,        \
-                                                           const BatchStage &, const OpTables &, cudaStream_t);
-#define PRANDTL_INSTANTIATE_LIFT(DIMV, OUT)                                                             \
-    template cudaError_t lift_dispatch<DIMV, OUT>(int, const MeshDev &, const LiftArgs &,               \
-                                                  const PhysParams &, const OpTables &, cudaStream_t);  \
-    template cudaError_t lift_batch_prepare<DIMV, OUT>(int, BatchKernelInfo *);                         \
-    template cudaError_t lift_batch_launch<DIMV, OUT>(int, int, const BatchClassDev &, const BatchStage &, \
-                                                      const OpTables &, cudaStream_t);
+    template cudaError_t lift_batch_prepare<DIMV, OUT, VCV>(int, BatchKernelInfo *);                    \
+    template cudaError_t lift_batch_launch<DIMV, OUT, VCV>(int, int, const BatchClassDev &, const BatchStage &, \
+                                                           const OpTables &, cudaStream_t);
 
 }   // namespace prandtl

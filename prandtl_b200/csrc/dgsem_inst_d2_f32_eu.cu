@@ -2,5 +2,5 @@
 #include "dgsem_impl.cuh"
 
 namespace prandtl {
-PRANDTL_INSTANTIATE_RHS(2, float, false)
+PRANDTL_INSTANTIATE_RHS(2, float, false, false)
 }   // namespace prandtl

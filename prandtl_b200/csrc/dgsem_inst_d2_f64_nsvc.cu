@@ -1,0 +1,7 @@
+// 2D, FP64, Navier-Stokes with contravariant viscous fluxes: instantiation of the DGSEM kernels.
+#include "dgsem_impl.cuh"
+
+namespace prandtl {
+PRANDTL_INSTANTIATE_RHS(2, double, true, true)
+PRANDTL_INSTANTIATE_LIFT(2, double, true)
+}   // namespace prandtl

@@ -1,7 +1,7 @@
-// 3D, FP64, Navier-Stokes: instantiation of the DGSEM kernels.
+// 3D, FP64, Navier-Stokes with lifted gradients (reference defects reproduced): instantiation of the DGSEM kernels.
 #include "dgsem_impl.cuh"
 
 namespace prandtl {
-PRANDTL_INSTANTIATE_RHS(3, double, true)
-PRANDTL_INSTANTIATE_LIFT(3, double)
+PRANDTL_INSTANTIATE_RHS(3, double, true, false)
+PRANDTL_INSTANTIATE_LIFT(3, double, false)
 }   // namespace prandtl

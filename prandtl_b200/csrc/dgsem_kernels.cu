@@ -9,59 +9,73 @@ bool order_supported(int dim, int order) {
     return (dim == 2 || dim == 3) && order >= 1 && order <= 5;
 }
 
-#define PRANDTL_DIM_NS(FN, REAL, ...)                                              \
+// Euler, Navier-Stokes with gradients, Navier-Stokes with contravariant viscous fluxes.
+#define PRANDTL_DIM_PHYS(FN, REAL, NSV, VCV, ...)                                  \
     do {                                                                           \
-        if (dim == 2) return ns ? FN<2, REAL, true>(__VA_ARGS__) : FN<2, REAL, false>(__VA_ARGS__); \
-        if (dim == 3) return ns ? FN<3, REAL, true>(__VA_ARGS__) : FN<3, REAL, false>(__VA_ARGS__); \
+        if (!(NSV)) {                                                              \
+            if (dim == 2) return FN<2, REAL, false, false>(__VA_ARGS__);           \
+            if (dim == 3) return FN<3, REAL, false, false>(__VA_ARGS__);           \
+        } else if (VCV) {                                                          \
+            if (dim == 2) return FN<2, REAL, true, true>(__VA_ARGS__);             \
+            if (dim == 3) return FN<3, REAL, true, true>(__VA_ARGS__);             \
+        } else {                                                                   \
+            if (dim == 2) return FN<2, REAL, true, false>(__VA_ARGS__);            \
+            if (dim == 3) return FN<3, REAL, true, false>(__VA_ARGS__);            \
+        }                                                                          \
         return cudaErrorInvalidValue;                                              \
     } while (0)
-#define PRANDTL_DIM(FN, OUT, ...)                                                  \
+#define PRANDTL_DIM_LIFT(FN, OUT, VCV, ...)                                        \
     do {                                                                           \
-        if (dim == 2) return FN<2, OUT>(__VA_ARGS__);                              \
-        if (dim == 3) return FN<3, OUT>(__VA_ARGS__);                              \
+        if (VCV) {                                                                 \
+            if (dim == 2) return FN<2, OUT, true>(__VA_ARGS__);                    \
+            if (dim == 3) return FN<3, OUT, true>(__VA_ARGS__);                    \
+        } else {                                                                   \
+            if (dim == 2) return FN<2, OUT, false>(__VA_ARGS__);                   \
+            if (dim == 3) return FN<3, OUT, false>(__VA_ARGS__);                   \
+        }                                                                          \
         return cudaErrorInvalidValue;                                              \
     } while (0)
 
 cudaError_t launch_rhs(int dim, int order, bool ns, const MeshDev &m, const RhsArgs &a,
                        const PhysParams &P, const OpTables &T, cudaStream_t s) {
     if (m.E <= 0) return cudaSuccess;
-    PRANDTL_DIM_NS(rhs_dispatch, double, order, m, a, P, T, s);
+    PRANDTL_DIM_PHYS(rhs_dispatch, double, ns, use_vc(P), order, m, a, P, T, s);
 }
 cudaError_t launch_rhs_fp32(int dim, int order, bool ns, const MeshDev &m, const RhsArgs &a,
                             const PhysParams &P, const OpTables &T, cudaStream_t s) {
     if (m.E <= 0) return cudaSuccess;
-    PRANDTL_DIM_NS(rhs_dispatch, float, order, m, a, P, T, s);
+    PRANDTL_DIM_PHYS(rhs_dispatch, float, ns, use_vc(P), order, m, a, P, T, s);
 }
 cudaError_t launch_lift(int dim, int order, const MeshDev &m, const LiftArgs &a,
                         const PhysParams &P, const OpTables &T, cudaStream_t s) {
     if (m.E <= 0) return cudaSuccess;
-    PRANDTL_DIM(lift_dispatch, double, order, m, a, P, T, s);
+    PRANDTL_DIM_LIFT(lift_dispatch, double, use_vc(P), order, m, a, P, T, s);
 }
 cudaError_t launch_lift_fp32(int dim, int order, const MeshDev &m, const LiftArgs &a,
                              const PhysParams &P, const OpTables &T, cudaStream_t s) {
     if (m.E <= 0) return cudaSuccess;
-    PRANDTL_DIM(lift_dispatch, float, order, m, a, P, T, s);
+    PRANDTL_DIM_LIFT(lift_dispatch, float, use_vc(P), order, m, a, P, T, s);
 }
 
 int batch_num_variants() { return 3; }
 
-cudaError_t batch_prepare_rhs(int dim, int order, bool ns, bool fp32, int variant, BatchKernelInfo *info) {
-    if (fp32) PRANDTL_DIM_NS(rhs_batch_prepare, float, order, variant, info);
-    PRANDTL_DIM_NS(rhs_batch_prepare, double, order, variant, info);
+cudaError_t batch_prepare_rhs(int dim, int order, bool ns, bool vc, bool fp32, int variant, BatchKernelInfo *info) {
+    if (fp32) PRANDTL_DIM_PHYS(rhs_batch_prepare, float, ns, vc, order, variant, info);
+    PRANDTL_DIM_PHYS(rhs_batch_prepare, double, ns, vc, order, variant, info);
 }
-cudaError_t batch_prepare_lift(int dim, int order, bool fp32, BatchKernelInfo *info) {
-    if (fp32) PRANDTL_DIM(lift_batch_prepare, float, order, info);
-    PRANDTL_DIM(lift_batch_prepare, double, order, info);
+cudaError_t batch_prepare_lift(int dim, int order, bool vc, bool fp32, BatchKernelInfo *info) {
+    if (fp32) PRANDTL_DIM_LIFT(lift_batch_prepare, float, vc, order, info);
+    PRANDTL_DIM_LIFT(lift_batch_prepare, double, vc, order, info);
 }
-cudaError_t batch_launch_rhs(int dim, int order, bool ns, bool fp32, int variant, int grid,
+cudaError_t batch_launch_rhs(int dim, int order, bool ns, bool vc, bool fp32, int variant, int grid,
                              const BatchClassDev &c, const BatchStage &st, const OpTables &T, cudaStream_t s) {
-    if (fp32) PRANDTL_DIM_NS(rhs_batch_launch, float, order, variant, grid, c, st, T, s);
-    PRANDTL_DIM_NS(rhs_batch_launch, double, order, variant, grid, c, st, T, s);
+    if (fp32) PRANDTL_DIM_PHYS(rhs_batch_launch, float, ns, vc, order, variant, grid, c, st, T, s);
+    PRANDTL_DIM_PHYS(rhs_batch_launch, double, ns, vc, order, variant, grid, c, st, T, s);
 }
-cudaError_t batch_launch_lift(int dim, int order, bool fp32, int grid, const BatchClassDev &c,
+cudaError_t batch_launch_lift(int dim, int order, bool vc, bool fp32, int grid, const BatchClassDev &c,
                               const BatchStage &st, const OpTables &T, cudaStream_t s) {
-    if (fp32) PRANDTL_DIM(lift_batch_launch, float, order, grid, c, st, T, s);
-    PRANDTL_DIM(lift_batch_launch, double, order, grid, c, st, T, s);
+    if (fp32) PRANDTL_DIM_LIFT(lift_batch_launch, float, vc, order, grid, c, st, T, s);
+    PRANDTL_DIM_LIFT(lift_batch_launch, double, vc, order, grid, c, st, T, s);
 }
 
 namespace {

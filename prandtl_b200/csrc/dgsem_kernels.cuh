@@ -102,13 +102,15 @@ cudaError_t launch_lift_fp32(int dim, int order, const MeshDev &m, const LiftArg
 bool order_supported(int dim, int order);
 
 // Batch kernels of one class.  `variant` in [0, batch_num_variants()) picks the
-// RHS launch shape.  prepare_* must run outside stream capture.
+// RHS launch shape.  `vc` selects the Navier-Stokes form that passes
+// contravariant viscous fluxes from the lifting to the RHS (quirks = 1) instead
+// of primitive gradients (quirks = 0).  prepare_* must run outside stream capture.
 int batch_num_variants();
-cudaError_t batch_prepare_rhs(int dim, int order, bool ns, bool fp32, int variant, BatchKernelInfo *info);
-cudaError_t batch_prepare_lift(int dim, int order, bool fp32, BatchKernelInfo *info);
-cudaError_t batch_launch_rhs(int dim, int order, bool ns, bool fp32, int variant, int grid,
+cudaError_t batch_prepare_rhs(int dim, int order, bool ns, bool vc, bool fp32, int variant, BatchKernelInfo *info);
+cudaError_t batch_prepare_lift(int dim, int order, bool vc, bool fp32, BatchKernelInfo *info);
+cudaError_t batch_launch_rhs(int dim, int order, bool ns, bool vc, bool fp32, int variant, int grid,
                              const BatchClassDev &c, const BatchStage &st, const OpTables &T, cudaStream_t s);
-cudaError_t batch_launch_lift(int dim, int order, bool fp32, int grid, const BatchClassDev &c,
+cudaError_t batch_launch_lift(int dim, int order, bool vc, bool fp32, int grid, const BatchClassDev &c,
                               const BatchStage &st, const OpTables &T, cudaStream_t s);
 // End of a batch step: every live solve with steps left advances its counters,
 // flips its LSRK parity, (cfl > 0) takes its next dt from lambda, and writes
@@ -117,21 +119,29 @@ cudaError_t batch_launch_step_end(BatchInst *tab, const int *live, const int *n_
                                   cudaStream_t s);
 
 // Per-(dim, working precision, physics) dispatchers, one translation unit each.
-template <int DIM, typename Real, bool NS>
+// VC (Navier-Stokes only): the lifting emits the contravariant viscous fluxes
+// adj * Fv^T, rows 1..NF-1, as [DIM][NF-1][Ndof] in the gradient buffer, and
+// the RHS reads them instead of evaluating viscous fluxes from gradients.
+template <int DIM, typename Real, bool NS, bool VC>
 cudaError_t rhs_dispatch(int order, const MeshDev &m, const RhsArgs &a, const PhysParams &P,
                          const OpTables &T, cudaStream_t s);
-template <int DIM, typename Out>
+template <int DIM, typename Out, bool VC>
 cudaError_t lift_dispatch(int order, const MeshDev &m, const LiftArgs &a, const PhysParams &P,
                           const OpTables &T, cudaStream_t s);
-template <int DIM, typename Real, bool NS>
+template <int DIM, typename Real, bool NS, bool VC>
 cudaError_t rhs_batch_prepare(int order, int variant, BatchKernelInfo *info);
-template <int DIM, typename Real, bool NS>
+template <int DIM, typename Real, bool NS, bool VC>
 cudaError_t rhs_batch_launch(int order, int variant, int grid, const BatchClassDev &c, const BatchStage &st,
                              const OpTables &T, cudaStream_t s);
-template <int DIM, typename Out>
+template <int DIM, typename Out, bool VC>
 cudaError_t lift_batch_prepare(int order, BatchKernelInfo *info);
-template <int DIM, typename Out>
+template <int DIM, typename Out, bool VC>
 cudaError_t lift_batch_launch(int order, int grid, const BatchClassDev &c, const BatchStage &st,
                               const OpTables &T, cudaStream_t s);
+
+// The Navier-Stokes form used for a configuration: contravariant viscous
+// fluxes (VC) unless the reference's defects are reproduced (quirks == 0,
+// whose volume and face viscous fluxes differ, Q1/Q8).
+inline bool use_vc(const PhysParams &P) { return P.quirks != 0; }
 
 }   // namespace prandtl

@@ -172,6 +172,34 @@ inline prandtl_status validate_mesh(const prandtl_mesh_desc *md, std::vector<int
     return PRANDTL_OK;
 }
 
+// For the Navier-Stokes form with contravariant viscous fluxes: every face's
+// scaled normal must be the outward adjugate row of both its elements
+// (Nanson's formula for affine elements): nor = s1 adj(J_e1)[d1] =
+// -s2 adj(J_e2)[d2] with s = +1 on a local face 2d+1, -1 on 2d.
+inline prandtl_status check_face_normals(const prandtl_mesh_desc *md, std::string &msg) {
+    const int dim = md->dim;
+    for (int f = 0; f < md->num_faces; ++f) {
+        const int *fe = md->face_elems + 4 * f;
+        const double *nor = md->face_nor + (size_t)f * dim;
+        for (int side = 0; side < 2; ++side) {
+            const int e = fe[2 * side], lf = fe[2 * side + 1], d = lf >> 1;
+            const double sg = ((lf & 1) ? 1.0 : -1.0) * (side == 0 ? 1.0 : -1.0);
+            const double *row = md->elem_adj + ((size_t)e * dim + d) * dim;
+            double err = 0, mag = 0;
+            for (int c = 0; c < dim; ++c) {
+                err = std::fmax(err, std::fabs(nor[c] - sg * row[c]));
+                mag = std::fmax(mag, std::fabs(row[c]));
+            }
+            if (!(err <= 1e-9 * mag)) {
+                msg = "face " + std::to_string(f) +
+                      ": scaled normal differs from the element's adjugate row (non-affine or inconsistent mesh)";
+                return PRANDTL_EUNSUPPORTED;
+            }
+        }
+    }
+    return PRANDTL_OK;
+}
+
 // Geometry rows [E][dim*dim + 1]: adj(J) row-major, then det J.
 inline std::vector<double> geometry_rows(const prandtl_mesh_desc *md) {
     const int dim = md->dim, GEO = dim * dim + 1, E = md->num_elements;

@@ -199,7 +199,8 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
     std::vector<int4> nbr;
     {
         std::string msg;
-        const prandtl_status vst = validate_mesh(md, nbr, msg);
+        prandtl_status vst = validate_mesh(md, nbr, msg);
+        if (vst == PRANDTL_OK && cfg->parabolic && cfg->quirks != 0) vst = check_face_normals(md, msg);
         if (vst != PRANDTL_OK) return fail(nullptr, vst, msg);
     }
 

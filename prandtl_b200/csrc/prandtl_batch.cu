@@ -112,7 +112,7 @@ Layout solve_layout(int dim, int order, int E, int F, bool ns, bool blending, bo
     return L;
 }
 
-int class_key(int dim, int order, bool ns) { return (dim * 16 + order) * 2 + (ns ? 1 : 0); }
+int class_key(int dim, int order, bool ns, bool vc) { return ((dim * 16 + order) * 2 + (ns ? 1 : 0)) * 2 + (vc ? 1 : 0); }
 
 struct Solve {
     bool used = false;
@@ -127,7 +127,7 @@ constexpr int MAX_VARIANTS = 8;
 
 struct Class {
     int dim = 0, order = 0;
-    bool ns = false;
+    bool ns = false, vc = false;   // vc: NS with contravariant viscous fluxes (quirks = 1)
     OpTables T{};
     std::vector<int> ids;        // slot -> solve id
     int *d_buf = nullptr;        // ids[cap] | prefix[cap + 1] | hdr[4]
@@ -235,26 +235,27 @@ prandtl_status upload_live(prandtl_batch *b) {
     return PRANDTL_OK;
 }
 
-prandtl_status get_class(prandtl_batch *b, int dim, int order, bool ns, Class **out) {
-    const int key = class_key(dim, order, ns);
+prandtl_status get_class(prandtl_batch *b, int dim, int order, bool ns, bool vc, Class **out) {
+    const int key = class_key(dim, order, ns, vc);
     auto it = b->classes.find(key);
     if (it != b->classes.end()) { *out = &it->second; return PRANDTL_OK; }
     Class c;
     c.dim = dim;
     c.order = order;
     c.ns = ns;
+    c.vc = vc;
     build_tables(order, c.T);
     const bool fp32 = b->cfg.precision == 1;
     int first_ok = -1;
     for (int v = 0; v < b->nvar; ++v) {
         c.ms[v] = -1.0;
-        BCK(b, batch_prepare_rhs(dim, order, ns, fp32, v, &c.rinfo[v]), "prepare batch rhs kernel");
+        BCK(b, batch_prepare_rhs(dim, order, ns, vc, fp32, v, &c.rinfo[v]), "prepare batch rhs kernel");
         if (c.rinfo[v].blocks_per_sm > 0 && first_ok < 0) first_ok = v;
     }
     if (first_ok < 0) return bfail(b, PRANDTL_EUNSUPPORTED, "no RHS launch shape fits this device");
     c.variant = first_ok;
     if (ns) {
-        BCK(b, batch_prepare_lift(dim, order, fp32, &c.linfo), "prepare batch lift kernel");
+        BCK(b, batch_prepare_lift(dim, order, vc, fp32, &c.linfo), "prepare batch lift kernel");
         if (c.linfo.blocks_per_sm <= 0) return bfail(b, PRANDTL_EUNSUPPORTED, "lift kernel does not fit this device");
     }
     const size_t words = 2 * (size_t)b->cap + 5;
@@ -282,10 +283,10 @@ prandtl_status enqueue_step(prandtl_batch *b, cudaStream_t s) {
             Class &c = kv.second;
             if (c.ns) {
                 const int grid = c.linfo.blocks_per_sm * b->num_sms;
-                BCK(b, batch_launch_lift(c.dim, c.order, fp32, grid, c.dev, st, c.T, s), "batch lift launch");
+                BCK(b, batch_launch_lift(c.dim, c.order, c.vc, fp32, grid, c.dev, st, c.T, s), "batch lift launch");
             }
             const int grid = c.rinfo[c.variant].blocks_per_sm * b->num_sms;
-            BCK(b, batch_launch_rhs(c.dim, c.order, c.ns, fp32, c.variant, grid, c.dev, st, c.T, s),
+            BCK(b, batch_launch_rhs(c.dim, c.order, c.ns, c.vc, fp32, c.variant, grid, c.dev, st, c.T, s),
                 "batch rhs launch");
         }
     }
@@ -472,10 +473,12 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, 
     BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
     const int dim = md->dim, order = md->order, E = md->num_elements, F = md->num_faces;
     const bool ns = cfg->parabolic != 0, fp32 = b->cfg.precision == 1, blend = cfg->blending != 0;
+    const bool vc = ns && cfg->quirks != 0;
+    if (vc && (st = check_face_normals(md, msg)) != PRANDTL_OK) return bfail(b, st, msg);
     const Layout L = solve_layout(dim, order, E, F, ns, blend, fp32);
     if (b->free_ids.empty()) return bfail(b, PRANDTL_ENOMEM, "solve table full");
     Class *c = nullptr;
-    if ((st = get_class(b, dim, order, ns, &c)) != PRANDTL_OK) return st;
+    if ((st = get_class(b, dim, order, ns, vc, &c)) != PRANDTL_OK) return st;
     size_t off = 0;
     if (!b->alloc.alloc(L.total, &off))
         return bfail(b, PRANDTL_ENOMEM, "arena has no room: need " + std::to_string(L.total) +
@@ -487,7 +490,7 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, 
     s.dim = dim;
     s.order = order;
     s.ns = ns;
-    s.key = class_key(dim, order, ns);
+    s.key = class_key(dim, order, ns, vc);
     s.E = E;
     s.nf = dim + 2;
     s.Ndof = (long long)E;
@@ -689,10 +692,10 @@ prandtl_status prandtl_batch_tune(prandtl_batch *b, int reps) {
         if (c.ids.empty()) continue;
         if (c.ns) {
             const int lgrid = c.linfo.blocks_per_sm * b->num_sms;
-            BCK(b, batch_launch_lift(c.dim, c.order, fp32, lgrid, c.dev, st0, c.T, b->stream), "tune lift");
+            BCK(b, batch_launch_lift(c.dim, c.order, c.vc, fp32, lgrid, c.dev, st0, c.T, b->stream), "tune lift");
             BCK(b, cudaEventRecord(b->ev0, b->stream), "event");
             for (int r = 0; r < reps; ++r)
-                BCK(b, batch_launch_lift(c.dim, c.order, fp32, lgrid, c.dev, st0, c.T, b->stream), "tune lift");
+                BCK(b, batch_launch_lift(c.dim, c.order, c.vc, fp32, lgrid, c.dev, st0, c.T, b->stream), "tune lift");
             BCK(b, cudaEventRecord(b->ev1, b->stream), "event");
             if ((st = bwait(b)) != PRANDTL_OK) return st;
             float lms = 0.f;
@@ -706,10 +709,10 @@ prandtl_status prandtl_batch_tune(prandtl_batch *b, int reps) {
             c.ms[v] = -1.0;
             if (c.rinfo[v].blocks_per_sm <= 0) continue;
             const int grid = c.rinfo[v].blocks_per_sm * b->num_sms;
-            BCK(b, batch_launch_rhs(c.dim, c.order, c.ns, fp32, v, grid, c.dev, st0, c.T, b->stream), "tune rhs");
+            BCK(b, batch_launch_rhs(c.dim, c.order, c.ns, c.vc, fp32, v, grid, c.dev, st0, c.T, b->stream), "tune rhs");
             BCK(b, cudaEventRecord(b->ev0, b->stream), "event");
             for (int r = 0; r < reps; ++r)
-                BCK(b, batch_launch_rhs(c.dim, c.order, c.ns, fp32, v, grid, c.dev, st0, c.T, b->stream), "tune rhs");
+                BCK(b, batch_launch_rhs(c.dim, c.order, c.ns, c.vc, fp32, v, grid, c.dev, st0, c.T, b->stream), "tune rhs");
             BCK(b, cudaEventRecord(b->ev1, b->stream), "event");
             if ((st = bwait(b)) != PRANDTL_OK) return st;
             float ms = 0.f;
@@ -728,7 +731,8 @@ prandtl_status prandtl_batch_class_info(prandtl_batch *b, int dim, int order, in
                                         int *n_variants, double *ms, double *lift_ms) {
     if (!b) return PRANDTL_EINVAL;
     std::lock_guard<std::mutex> lk(b->mu);
-    auto it = b->classes.find(class_key(dim, order, parabolic != 0));
+    auto it = b->classes.find(class_key(dim, order, parabolic != 0, parabolic != 0));
+    if (it == b->classes.end()) it = b->classes.find(class_key(dim, order, parabolic != 0, false));
     if (it == b->classes.end()) return bfail(b, PRANDTL_EINVAL, "no such class in this batch");
     if (variant) *variant = it->second.variant;
     if (n_variants) *n_variants = b->nvar;
