@@ -210,6 +210,9 @@ constexpr int next_pow2(int v) { return v <= 1 ? 1 : 2 * next_pow2((v + 1) / 2);
 #ifndef PRANDTL_EULER_MINB
 #define PRANDTL_EULER_MINB 5
 #endif
+#ifndef PRANDTL_NSVC_MINB
+#define PRANDTL_NSVC_MINB 4
+#endif
 #ifndef PRANDTL_NS32_MINB
 #define PRANDTL_NS32_MINB 4
 #endif
@@ -232,7 +235,7 @@ constexpr int next_pow2(int v) { return v <= 1 ? 1 : 2 * next_pow2((v + 1) / 2);
 constexpr int NUM_VARIANTS = 3;
 constexpr int CTX_RESERVE = 1024;   // bytes of per-item contexts reserved in every layout
 
-template <int DIM, int NP, bool NS, typename Real, int V = 0>
+template <int DIM, int NP, bool NS, typename Real, int V = 0, bool VC = false>
 struct RhsLayout {
     using S = Shape<DIM, NP>;
     static constexpr int ND = S::ND, NF = S::NF, NLINE = S::NLINE, PPL = S::PPL;
@@ -250,7 +253,9 @@ struct RhsLayout {
     // stays 16-byte aligned
     static constexpr int PER_ELEM = (K * ND + cmax(BUF, NS ? DIM * NF * ND : 0) + 3) / 4 * 4;
     static constexpr bool F64 = sizeof(Real) == 8;
-    static constexpr int MINB_CFG = NS ? (F64 ? PRANDTL_NS_MINB : PRANDTL_NS32_MINB)
+    // (the Navier-Stokes form with contravariant viscous fluxes needs fewer
+    // registers: FP64 fits one more resident CTA)
+    static constexpr int MINB_CFG = NS ? (F64 ? (VC ? PRANDTL_NSVC_MINB : PRANDTL_NS_MINB) : PRANDTL_NS32_MINB)
                                        : (F64 ? PRANDTL_EULER_MINB : PRANDTL_EULER32_MINB);
     static constexpr int WARPS_CFG = NS ? PRANDTL_NS_WARPS : PRANDTL_EULER_WARPS;
     // warps per CTA: the configured count, reduced so the CTA's elements fit the
@@ -853,9 +858,9 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 
 // One-shot kernel: grid = ceil(E / EPB), one element per lane group.
 template <int DIM, int NP, bool NS, bool VC, typename Real>
-__global__ void __launch_bounds__(RhsLayout<DIM, NP, NS, Real>::THREADS, (RhsLayout<DIM, NP, NS, Real>::MIN_BLOCKS))
+__global__ void __launch_bounds__(RhsLayout<DIM, NP, NS, Real, 0, VC>::THREADS, (RhsLayout<DIM, NP, NS, Real, 0, VC>::MIN_BLOCKS))
 rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_constant__ OpTables T) {
-    using LY = RhsLayout<DIM, NP, NS, Real>;
+    using LY = RhsLayout<DIM, NP, NS, Real, 0, VC>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Real *smem = reinterpret_cast<Real *>(smem_raw);
     load_tables<NP, Real>(T, smem, threadIdx.x, LY::THREADS);
@@ -877,9 +882,9 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
 // retired.  Items of finished solves and items wholly inside a solve's padding
 // are skipped (uniformly over the item's lanes).
 template <int DIM, int NP, bool NS, bool VC, typename Real, int V>
-__global__ void __launch_bounds__(RhsLayout<DIM, NP, NS, Real, V>::THREADS, (RhsLayout<DIM, NP, NS, Real, V>::MIN_BLOCKS))
+__global__ void __launch_bounds__(RhsLayout<DIM, NP, NS, Real, V, VC>::THREADS, (RhsLayout<DIM, NP, NS, Real, V, VC>::MIN_BLOCKS))
 rhs_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_constant__ OpTables T) {
-    using LY = RhsLayout<DIM, NP, NS, Real, V>;
+    using LY = RhsLayout<DIM, NP, NS, Real, V, VC>;
     static_assert(LY::ITEMS_PER_CTA * sizeof(WarpCtx) <= CTX_RESERVE, "per-item contexts exceed the reserve");
     constexpr int TABB = (Shape<DIM, NP>::TAB * (int)sizeof(Real) + 15) / 16 * 16;
     extern __shared__ __align__(16) unsigned char smem_raw[];
