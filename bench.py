@@ -68,7 +68,7 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--ensemble", type=int, default=512, help="members of the ensemble")
     p.add_argument("--plain-every", type=int, default=8, help="FP64-plain subsample stride")
-    p.add_argument("--serve-requests", type=int, default=150)
+    p.add_argument("--serve-requests", type=int, default=500)
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--no-tgv32", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -92,25 +92,37 @@ def flops_per_element(dim, order, ns=True):
     """Floating-point operations of one RHS launch per element, from the
     operation counts of the point-wise routines (add/mul/div/sqrt/log = 1,
     FMA = 2): two-point volume fluxes of every unique node pair with their two
-    D-weighted accumulations, surface fluxes of the element's face nodes,
-    node-wise viscous fluxes and their differencing (NS), epilogue."""
+    D-weighted accumulations, surface fluxes of the element's face nodes, the
+    Dhat-divergence of the contravariant viscous fluxes and their signed face
+    average (NS; the viscous fluxes themselves are the lifting's work), and
+    the RK epilogue."""
     Np = order + 1
     nd, nf = Np ** dim, dim + 2
     pairs = dim * Np ** (dim - 1) * Np * (Np - 1) // 2
     faces = 2 * dim * Np ** (dim - 1)
     vol_pair = 123 + 2 * nf * 2
-    face_item = 150 + (2 * 60 if ns else 0) + dim * nf * 2 + nf * 2
-    visc_node = (60 + dim * dim * nf * 2 + dim * Np * nf * 2) if ns else 0
+    face_item = 150 + dim * nf * 2 + nf * 2 + ((nf - 1) * 3 if ns else 0)
+    visc_node = dim * Np * (nf - 1) * 2 if ns else 0
     return pairs * vol_pair + faces * face_item + nd * visc_node + nd * nf * 6
 
 
-def rhs_bytes_per_element(dim, order, grad_bytes, ns=True):
+def rhs_bytes_per_element(dim, order, visc_bytes, ns=True):
     """Compulsory DRAM bytes of one RHS + LSRK launch per element: u read, the
-    gradients read (NS), du read and written, the next state written, and the
+    contravariant viscous fluxes read (NS: dim*(nf-1) values per node of
+    visc_bytes each), du read and written, the next state written, and the
     geometry rows."""
     nd, nf = (order + 1) ** dim, dim + 2
-    per_dof = 8 + (dim * grad_bytes if ns else 0) + 8 + 8 + 8
-    return nd * nf * per_dof + (dim * dim + 1) * 8 + 2 * dim * 16
+    per_node = nf * (8 + 8 + 8 + 8) + (dim * (nf - 1) * visc_bytes if ns else 0)
+    return nd * per_node + (dim * dim + 1) * 8 + 2 * dim * 16
+
+
+def measured_traffic():
+    """DRAM bytes per launch from the committed ncu summaries (profiles/)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
 
 
 # ---------------------------------------------------------------- clocks
@@ -399,7 +411,7 @@ def run_tgv32(torch, steps):
     return {"workload": "tgv3d_navier_stokes_32^3_N3_lsrk45_fp64", "dof": dof,
             "value": dof * steps / el, "unit": "DOF-updates/s", "ms_per_step": 1e3 * el / steps,
             "rhs_ms": rhs_ms, "lift_ms": lift_ms,
-            "rhs_flops": E * flops_per_element(3, 3), "rhs_bytes": E * rhs_bytes_per_element(3, 3, 8)}
+            "rhs_flops": E * flops_per_element(3, 3), "rhs_algorithmic_bytes": E * rhs_bytes_per_element(3, 3, 8)}
 
 
 def run_serving(torch, n_req):
@@ -544,13 +556,18 @@ def main():
         by = E_dom * rhs_bytes_per_element(3, dom_order, 4)
         hbm_peak, hbm_src = load_hbm_peak()
         tfl = fl / t_launch / 1e12
+        tr = measured_traffic().get(f"rhs_batch_N{dom_order}_fp32")
+        traffic = tr["bytes_per_element"] * E_dom if tr else None
         roofline = {
             "bound": "compute (FP32 CUDA cores; the kernel is neither HBM- nor tensor-bound)",
             "kernel": f"rhs_batch_kernel<3, N={dom_order}, NS, float> (all N={dom_order} members, one stage)",
             "achieved": tfl, "peak": fp32_peak, "unit": "TFLOP/s",
             "frac": (tfl / fp32_peak) if fp32_peak else None,
             "peak_source": "measured live in this run: cuBLAS SGEMM 8192^3, TF32 off (torch.matmul float32)",
-            "traffic": None,
+            "traffic": traffic,
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel on the N=5 members "
+                               "of a 24-member ensemble, scaled by elements (profiles/rhs_batch_kernel_N5_fp32_ncu.md); "
+                               "that launch was an LSRK first stage, which does not read du") if tr else None,
             "flops_per_launch": fl, "avg_launch_ms": t_launch * 1e3,
             "launch_timing": "CUDA events on the batch stream (autotuner, the launch repeated on the step's first stage)",
             "hbm": {"algorithmic_bytes_per_launch": by, "achieved_gbs": by / t_launch / 1e9,
@@ -565,6 +582,8 @@ def main():
             tgv32["fp64_peak_tflops"] = fp64_peak
             tgv32["rhs_fp64_frac"] = (tf / fp64_peak) if fp64_peak else None
             tgv32["fp64_peak_source"] = "measured live: cuBLAS DGEMM 8192^3"
+            t32 = measured_traffic().get("rhs_tgv32_fp64")
+            tgv32["rhs_traffic_bytes"] = t32["bytes_per_launch"] if t32 else None
         serving = None
         if not args.no_serve:
             serving = run_serving(torch, args.serve_requests)

@@ -101,3 +101,27 @@ def test_null_handle_calls_fail_cleanly(lib):
     assert lib.prandtl_synchronize(None) == _lib.PRANDTL_EINVAL
     assert lib.prandtl_kernel_launches(None) == 0
     assert lib.prandtl_version().startswith(b"prandtl_b200")
+
+
+def test_face_normals_must_match_the_metrics_in_fixed_navier_stokes(lib):
+    """Fixed-mode NS takes face viscous terms from the adjugate rows; a mesh whose
+    face normals disagree with them is rejected before any device work."""
+    from prandtl_b200 import _lib
+    from prandtl_b200.mesh import periodic_box
+    keep = []
+    cfg = _lib.Config()
+    lib.prandtl_config_default(C.byref(cfg))
+    cfg.parabolic, cfg.quirks = 1, 1
+    m = periodic_box(3, 2, 2, 0.0, 1.0, affine=np.array([[1.0, 0.2, 0.0], [0.0, 1.1, 0.1], [0.05, 0.0, 0.9]]))
+    h = C.c_void_p()
+    m.face_nor = np.array(m.face_nor, copy=True)
+    m.face_nor[3, 1] += 1e-3
+    d = _desc(m, keep)
+    assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EUNSUPPORTED
+    assert b"adjugate" in lib.prandtl_last_error(None)
+    cfg.quirks = 0   # reference mode evaluates viscous fluxes from gradients: no such requirement
+    st = lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h))
+    assert st in (_lib.PRANDTL_ECUDA, _lib.PRANDTL_OK)
+    if st == _lib.PRANDTL_OK:
+        lib.prandtl_destroy(h)
+
