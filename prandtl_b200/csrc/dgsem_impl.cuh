@@ -731,10 +731,17 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
         const long long gn = (long long)t.x * ND + face_node<DIM, NP>(t.y, fa);
         const long long go = (long long)e * ND + no;
         const bool own_is_1 = (t.w == 0);
+        // the own trace's conserved state is read only by the gradient form
+        // (its Q8 path rebuilds the trace from it); otherwise only its momentum
+        // enters the surface flux, formed from the hoisted rho and v
+        constexpr bool OWN_STATE = NS && !VC;
         double so[NF], sn[NF];
         Real nor[DIM], flux[NF], fn[NF], mo[NF], mn[NF];
 #pragma unroll
-        for (int f = 0; f < NF; ++f) { so[f] = __ldg(a.u + f * Ndof + go); sn[f] = __ldg(a.u + f * Ndof + gn); }
+        for (int f = 0; f < NF; ++f) {
+            if constexpr (OWN_STATE) so[f] = __ldg(a.u + f * Ndof + go);
+            sn[f] = __ldg(a.u + f * Ndof + gn);
+        }
 #pragma unroll
         for (int q = 0; q < DIM; ++q) nor[q] = Real(__ldg(a.fnor + (long long)t.z * DIM + q));
         Prim<DIM, Real> po = load_prim<DIM, ND, Real>(sH, no);
@@ -782,7 +789,16 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
             }
         }
 #pragma unroll
-        for (int f = 0; f < NF; ++f) { mo[f] = Real(so[f]); mn[f] = Real(sn[f]); }
+        for (int f = 0; f < NF; ++f) mn[f] = Real(sn[f]);
+        if constexpr (OWN_STATE) {
+#pragma unroll
+            for (int f = 0; f < NF; ++f) mo[f] = Real(so[f]);
+        } else {
+            mo[0] = po.rho;
+            mo[NF - 1] = 0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) mo[1 + d] = po.rho * po.v[d];
+        }
         if (own_is_1)
             face_flux<DIM, Real>(mo, po, mn, pn, nor, gm1i, P.quirks == 0, P.dissipation != 0, flux);
         else
@@ -974,31 +990,44 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
     int c[3];
     node_coords<NP>(n, c);
 
-    // face part first (its neighbour loads overlap the element part):
+    // face part: the neighbour traces' entropy variables are formed before the
+    // barrier (their loads overlap the own node's), the jumps after it:
     // +1/(w0 J) * 1/2 (v_elem2 - v_elem1) * n_c on both sides
+    constexpr int MAXIT = (NFI + ND - 1) / ND;   // face items per thread
+    W vn[MAXIT][NF], nor[MAXIT][DIM];
+    int no[MAXIT];
+    bool own1[MAXIT];
+#pragma unroll
+    for (int k = 0; k < MAXIT; ++k) {
+        const int it = n + k * ND;
+        if (it < NFI) {
+            const int lf = it / NFN, fa = it - lf * NFN;
+            no[k] = face_node<DIM, NP>(lf, fa);
+            const int4 t = __ldg(a.nbr + (long long)e * (2 * DIM) + lf);
+            const long long gn = (long long)t.x * ND + face_node<DIM, NP>(t.y, fa);
+            double sn[NF];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) sn[f] = __ldg(a.u + f * Ndof + gn);
+            if constexpr (F64) conserv2entropy<DIM, double>(sn, P, reinterpret_cast<double *>(vn[k]));
+            else conserv2entropy_rel<DIM>(sn, P, R, reinterpret_cast<float *>(vn[k]));
+#pragma unroll
+            for (int q = 0; q < DIM; ++q) nor[k][q] = W(__ldg(a.fnor + (long long)t.z * DIM + q));
+            own1[k] = (t.w == 0);
+        }
+    }
     __syncthreads();   // tables and entropy variables complete
     const W aw = W(1.0 / (double(sW[0]) * J));
-    for (int it = n; it < NFI; it += ND) {
-        const int lf = it / NFN, fa = it - lf * NFN;
-        const int no = face_node<DIM, NP>(lf, fa);
-        const int4 t = __ldg(a.nbr + (long long)e * (2 * DIM) + lf);
-        const int nn = face_node<DIM, NP>(t.y, fa);
-        const long long gn = (long long)t.x * ND + nn;
-        double sn[NF];
-        W vn[NF], nor[DIM];
 #pragma unroll
-        for (int f = 0; f < NF; ++f) sn[f] = __ldg(a.u + f * Ndof + gn);
-        if constexpr (F64) conserv2entropy<DIM, double>(sn, P, reinterpret_cast<double *>(vn));
-        else conserv2entropy_rel<DIM>(sn, P, R, reinterpret_cast<float *>(vn));
+    for (int k = 0; k < MAXIT; ++k) {
+        const int it = n + k * ND;
+        if (it < NFI) {
 #pragma unroll
-        for (int q = 0; q < DIM; ++q) nor[q] = W(__ldg(a.fnor + (long long)t.z * DIM + q));
-        const bool own_is_1 = (t.w == 0);
+            for (int f = 0; f < NF; ++f) {
+                const W vo = sVe[f * ND + no[k]];
+                const W jf = own1[k] ? W(0.5) * (vn[k][f] - vo) : W(0.5) * (vo - vn[k][f]);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            const W vo = sVe[f * ND + no];
-            const W jf = own_is_1 ? W(0.5) * (vn[f] - vo) : W(0.5) * (vo - vn[f]);
-#pragma unroll
-            for (int q = 0; q < DIM; ++q) sS[(q * NF + f) * NFI + it] = aw * (jf * nor[q]);
+                for (int q = 0; q < DIM; ++q) sS[(q * NF + f) * NFI + it] = aw * (jf * nor[k][q]);
+            }
         }
     }
 
