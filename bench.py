@@ -264,6 +264,17 @@ def run_reference(args, rank):
 
 
 # ---------------------------------------------------------------- GPU side
+def max_over_ranks(dist, x, device):
+    """The largest of every rank's x (each rank times its own replica; the job
+    takes as long as its slowest rank).  dist is torch.distributed or None."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def gemm_tflops(torch, dtype, n=8192):
     """Best-of-5 cuBLAS GEMM rate (TF32 off for float32: CUDA-core FP32)."""
     old = torch.backends.cuda.matmul.allow_tf32
@@ -514,13 +525,6 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     K, W = args.steps, args.warmup
     if args.profile_case == "tgv32":
         run_tgv32(torch, K)
@@ -532,8 +536,8 @@ def main():
     states, binfo = run_batch(torch, items, K, W, barrier, local)
     if args.profile_case == "batch":
         return
-    device_s = max_over_ranks(binfo["device_s"])
-    wall_s = max_over_ranks(binfo["wall_s"])
+    device_s = max_over_ranks(dist, binfo["device_s"], "cuda")
+    wall_s = max_over_ranks(dist, binfo["wall_s"], "cuda")
     value = dof * K * world / device_s
 
     line = None

@@ -171,3 +171,30 @@ def test_ensemble_members_small_sample():
     for sid, (m, mesh, u0, dt) in zip(ids, items):
         assert norm_err(b.read(sid), plain(m, u0, dt, 2), mesh.num_fields) <= 1e-12
     b.close()
+
+
+def test_blending_and_reference_mode_classes():
+    """Classes with subcell-FV blending (2D Kelvin-Helmholtz) and the
+    reference's own Navier-Stokes (quirks = reference: the gradient form) run in
+    one batch next to fixed-mode solves and match the one-operator path."""
+    from prandtl_b200.operator import DGSEMOperator
+    kh = periodic_box(2, 8, 3, -1.0, 1.0)
+    u_kh = cases.kelvin_helmholtz(kh)
+    tg = periodic_box(3, 2, 3, 0.0, 2 * np.pi)
+    u_tg = cases.taylor_green(tg)
+    runs = [(kh, u_kh, dict(blending=True, quirks="fixed")),
+            (kh, u_kh, dict(blending=True, quirks="reference")),
+            (tg, u_tg, dict(parabolic=True, mu=1 / 1600, Pr=0.71, quirks="reference")),
+            (tg, u_tg, dict(parabolic=True, mu=1 / 1600, Pr=0.71, quirks="fixed"))]
+    b = Batch("fp64", "RK3SSP", arena_bytes=1 << 28)
+    ids = []
+    for mesh, u0, kw in runs:
+        ids.append(b.add(mesh, u0, dt=fixed_dt(mesh, u0, 0.2), nsteps=3, **kw))
+    b.advance(3)
+    for sid, (mesh, u0, kw) in zip(ids, runs):
+        op = DGSEMOperator(mesh, **kw)
+        ref = u0.copy()
+        op.Step(ref, fixed_dt(mesh, u0, 0.2), scheme="RK3SSP", nsteps=3)
+        op.close()
+        assert norm_err(b.read(sid), ref, mesh.num_fields) <= 1e-12, kw
+    b.close()
