@@ -20,6 +20,8 @@
 // class.
 #pragma once
 
+#include <cstdint>
+
 #include "dgsem_kernels.cuh"
 
 namespace prandtl {
@@ -119,6 +121,23 @@ __device__ __forceinline__ void load_tables(const OpTables &T, Real *sT, int tid
     }
 }
 
+// Node pairs of the flux-differencing phase, per direction: entry dir*NPD + p
+// holds the element-local nodes (a, b), a < b along the line, of unique pair p
+// (line-major, then pair-major) as a | b << 16.  Built once per CTA, so the
+// pair loop does one shared load instead of decoding line and pair indices.
+template <int DIM, int NP>
+__device__ __forceinline__ void load_pair_table(uint32_t *sP, int tid, int nthreads) {
+    constexpr int PPL = NP * (NP - 1) / 2, NPD = ipow(NP, DIM - 1) * PPL;
+    for (int q = tid; q < DIM * NPD; q += nthreads) {
+        const int dir = q / NPD, p = q - dir * NPD;
+        const int ln = p / PPL, pp = p - ln * PPL;
+        int pa, pb, base, stride;
+        pair_decode<NP>(pp, pa, pb);
+        line_base<DIM, NP>(dir, ln, base, stride);
+        sP[q] = uint32_t(base + pa * stride) | (uint32_t(base + pb * stride) << 16);
+    }
+}
+
 __device__ __forceinline__ void atomic_max_pos(unsigned long long *dst, double v) {
     // v >= 0 (or NaN): non-negative doubles order like their bit patterns.
     if (!(v >= 0.0)) v = __longlong_as_double(0x7ff0000000000000ll);   // NaN/negative -> +inf
@@ -213,6 +232,9 @@ constexpr int next_pow2(int v) { return v <= 1 ? 1 : 2 * next_pow2((v + 1) / 2);
 #ifndef PRANDTL_NSVC_MINB
 #define PRANDTL_NSVC_MINB 4
 #endif
+#ifndef PRANDTL_NSVC32_MINB
+#define PRANDTL_NSVC32_MINB 4
+#endif
 #ifndef PRANDTL_NS32_MINB
 #define PRANDTL_NS32_MINB 4
 #endif
@@ -227,11 +249,12 @@ constexpr int next_pow2(int v) { return v <= 1 ? 1 : 2 * next_pow2((v + 1) / 2);
 // face / subcell items of the same stride.  Groups synchronise with
 // __syncwarp, or with a named barrier when GS = 64.
 //
-// V selects the launch shape (the batch autotuner times all of them):
-//   V = 0: the default group width (64 lanes for >= 125 nodes) and register budget
-//          (the one-shot kernel uses this one)
-//   V = 1: same width, one fewer resident CTA per SM required (more registers)
-//   V = 2: the other group width (32 <-> 64 lanes for elements of > 32 nodes)
+// V selects the register budget (the batch autotuner times all of them): the
+// launch bounds ask for MINB_BASE resident CTAs per SM (V = 0, also the
+// one-shot kernels), one fewer (V = 1: more registers) or one more (V = 2:
+// fewer registers, possibly spilling), always capped by what shared memory
+// admits.  The group width is fixed per element size: 64 lanes for >= 125
+// nodes (the tuner never preferred the other width).
 constexpr int NUM_VARIANTS = 3;
 constexpr int CTX_RESERVE = 1024;   // bytes of per-item contexts reserved in every layout
 
@@ -239,8 +262,7 @@ template <int DIM, int NP, bool NS, typename Real, int V = 0, bool VC = false>
 struct RhsLayout {
     using S = Shape<DIM, NP>;
     static constexpr int ND = S::ND, NF = S::NF, NLINE = S::NLINE, PPL = S::PPL;
-    static constexpr bool WIDE_DEFAULT = ND >= 125;
-    static constexpr bool WIDE = ND > 32 && (V == 2 ? !WIDE_DEFAULT : WIDE_DEFAULT);
+    static constexpr bool WIDE = ND >= 125;
     static constexpr int GS = WIDE ? 64 : (ND >= 32 ? 32 : next_pow2(ND));
     static constexpr int EPW = GS >= 32 ? 1 : 32 / GS;  // elements per warp
     static constexpr int WPE = GS > 32 ? GS / 32 : 1;   // warps per element
@@ -254,14 +276,20 @@ struct RhsLayout {
     static constexpr int PER_ELEM = (K * ND + cmax(BUF, NS ? DIM * NF * ND : 0) + 3) / 4 * 4;
     static constexpr bool F64 = sizeof(Real) == 8;
     // (the Navier-Stokes form with contravariant viscous fluxes needs fewer
-    // registers: FP64 fits one more resident CTA)
-    static constexpr int MINB_CFG = NS ? (F64 ? (VC ? PRANDTL_NSVC_MINB : PRANDTL_NS_MINB) : PRANDTL_NS32_MINB)
+    // registers; in FP32 the 216-node elements keep one CTA fewer for their
+    // longer per-lane node arrays; FP64 large elements are capped by shared
+    // memory anyway)
+    static constexpr int MINB_CFG = NS ? (F64 ? (VC ? PRANDTL_NSVC_MINB : PRANDTL_NS_MINB)
+                                              : (VC ? (ND >= 216 ? 3 : PRANDTL_NSVC32_MINB) : PRANDTL_NS32_MINB))
                                        : (F64 ? PRANDTL_EULER_MINB : PRANDTL_EULER32_MINB);
     static constexpr int WARPS_CFG = NS ? PRANDTL_NS_WARPS : PRANDTL_EULER_WARPS;
     // warps per CTA: the configured count, reduced so the CTA's elements fit the
     // 227 KB shared-memory limit (whole elements, whole warps)
     static constexpr int SMEM_MAX = 227 * 1024;
-    static constexpr int FIT_ELEMS = ((SMEM_MAX - CTX_RESERVE) / (int)sizeof(Real) - S::TAB) / PER_ELEM;
+    static constexpr int TAB_BYTES = (S::TAB * (int)sizeof(Real) + 15) / 16 * 16;
+    static constexpr int PAIR_BYTES = (DIM * NPD * 4 + 15) / 16 * 16;   // load_pair_table
+    static constexpr int FIXED_BYTES = TAB_BYTES + PAIR_BYTES + CTX_RESERVE;
+    static constexpr int FIT_ELEMS = (SMEM_MAX - FIXED_BYTES) / (PER_ELEM * (int)sizeof(Real));
     static constexpr int FIT_WARPS = GS > 32 ? FIT_ELEMS * WPE : FIT_ELEMS / EPW;
     static constexpr int WARPS_FIT = FIT_WARPS < WARPS_CFG ? FIT_WARPS : WARPS_CFG;
     static constexpr int WARPS = cmax(WPE, WARPS_FIT / WPE * WPE);
@@ -275,9 +303,9 @@ struct RhsLayout {
     static_assert(BATCH_CHUNK % ITEM_ELEMS == 0, "items must not straddle padded solve ranges");
     // resident CTAs the register budget is sized for: the variant's request,
     // capped by what shared memory admits (228 KB per SM, 1 KB reserved per CTA)
-    static constexpr int CTA_SMEM = S::TAB * (int)sizeof(Real) + CTX_RESERVE + EPB * PER_ELEM * (int)sizeof(Real);
+    static constexpr int CTA_SMEM = FIXED_BYTES + EPB * PER_ELEM * (int)sizeof(Real);
     static constexpr int SMEM_BLOCKS = cmax(1, (228 * 1024) / (CTA_SMEM + 1024));
-    static constexpr int MINB_REQ = V == 1 ? cmax(1, MINB_CFG - 1) : MINB_CFG;
+    static constexpr int MINB_REQ = V == 1 ? cmax(1, MINB_CFG - 1) : (V == 2 ? MINB_CFG + 1 : MINB_CFG);
     static constexpr int MIN_BLOCKS = MINB_REQ < SMEM_BLOCKS ? MINB_REQ : SMEM_BLOCKS;
 };
 
@@ -392,7 +420,8 @@ __device__ __forceinline__ int batch_slot(const int *prefix, int n, int first) {
 // in FP64 from the FP64 state, and the RK stage update is FP64.
 template <int DIM, int NP, bool NS, bool VC, typename Real, typename LY>
 __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P, int e, bool active,
-                                            const Real *sT, Real *sH, int li, int lane, int gid) {
+                                            const Real *sT, const uint32_t *sPair, Real *sH, int li, int lane,
+                                            int gid) {
     using S = Shape<DIM, NP>;
     constexpr int ND = S::ND, NF = S::NF, PPL = S::PPL;
     constexpr int NFN = S::NFN, NFI = S::NFI, GS = LY::GS, NPL = LY::NPL;
@@ -614,13 +643,10 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 #pragma unroll
         for (int q = 0; q < DIM; ++q) mt[q] = adj[dir][q];
         for (int p = li; p < NPD; p += GS) {
-            const int ln = p / PPL, pp = p - ln * PPL;
-            int pa, pb, base, stride;
-            pair_decode<NP>(pp, pa, pb);
-            line_base<DIM, NP>(dir, ln, base, stride);
+            const uint32_t pr = sPair[dir * NPD + p];
             Real F[NF];
-            volume_flux<DIM, Real>(load_prim<DIM, ND, Real>(sH, base + pa * stride),
-                                   load_prim<DIM, ND, Real>(sH, base + pb * stride), mt, gm1i, F);
+            volume_flux<DIM, Real>(load_prim<DIM, ND, Real>(sH, int(pr & 0xffffu)),
+                                   load_prim<DIM, ND, Real>(sH, int(pr >> 16)), mt, gm1i, F);
 #pragma unroll
             for (int f = 0; f < NF; ++f) sF[f * NPD + p] = F[f];
         }
@@ -879,7 +905,10 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
     using LY = RhsLayout<DIM, NP, NS, Real, 0, VC>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Real *smem = reinterpret_cast<Real *>(smem_raw);
+    uint32_t *sPair = reinterpret_cast<uint32_t *>(smem_raw + LY::TAB_BYTES);
+    Real *sE = reinterpret_cast<Real *>(smem_raw + LY::TAB_BYTES + LY::PAIR_BYTES);
     load_tables<NP, Real>(T, smem, threadIdx.x, LY::THREADS);
+    load_pair_table<DIM, NP>(sPair, threadIdx.x, LY::THREADS);
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int grp = threadIdx.x / LY::GS;          // element slot within the CTA
@@ -887,8 +916,8 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
     const int e_raw = blockIdx.x * LY::EPB + grp;
     const bool active = e_raw < m.E;
     const ElemIO io = io_from_args(m, a);
-    rhs_element<DIM, NP, NS, VC, Real, LY>(io, P, active ? e_raw : m.E - 1, active, smem,
-                                       smem + Shape<DIM, NP>::TAB + grp * LY::PER_ELEM, li, lane, grp);
+    rhs_element<DIM, NP, NS, VC, Real, LY>(io, P, active ? e_raw : m.E - 1, active, smem, sPair,
+                                           sE + grp * LY::PER_ELEM, li, lane, grp);
 }
 
 // Persistent batch kernel: a fixed grid walks the class's work items with a
@@ -902,12 +931,13 @@ __global__ void __launch_bounds__(RhsLayout<DIM, NP, NS, Real, V, VC>::THREADS, 
 rhs_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_constant__ OpTables T) {
     using LY = RhsLayout<DIM, NP, NS, Real, V, VC>;
     static_assert(LY::ITEMS_PER_CTA * sizeof(WarpCtx) <= CTX_RESERVE, "per-item contexts exceed the reserve");
-    constexpr int TABB = (Shape<DIM, NP>::TAB * (int)sizeof(Real) + 15) / 16 * 16;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Real *sT = reinterpret_cast<Real *>(smem_raw);
-    WarpCtx *ctxs = reinterpret_cast<WarpCtx *>(smem_raw + TABB);
-    Real *sE = reinterpret_cast<Real *>(smem_raw + TABB + CTX_RESERVE);
+    uint32_t *sPair = reinterpret_cast<uint32_t *>(smem_raw + LY::TAB_BYTES);
+    WarpCtx *ctxs = reinterpret_cast<WarpCtx *>(smem_raw + LY::TAB_BYTES + LY::PAIR_BYTES);
+    Real *sE = reinterpret_cast<Real *>(smem_raw + LY::FIXED_BYTES);
     load_tables<NP, Real>(T, sT, threadIdx.x, LY::THREADS);
+    load_pair_table<DIM, NP>(sPair, threadIdx.x, LY::THREADS);
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int grp = threadIdx.x / LY::GS;              // element slot (lane group) in the CTA
@@ -937,7 +967,8 @@ rhs_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_consta
         group_sync<LY::ITEM_THREADS>(slot);
         const int e_raw = e0 + gw;
         const bool active = e_raw < E;
-        rhs_element<DIM, NP, NS, VC, Real, LY>(ctx->io, ctx->P, active ? e_raw : E - 1, active, sT, sH, li, lane, grp);
+        rhs_element<DIM, NP, NS, VC, Real, LY>(ctx->io, ctx->P, active ? e_raw : E - 1, active, sT, sPair, sH, li,
+                                               lane, grp);
     }
 }
 
@@ -1188,13 +1219,12 @@ lift_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_const
 template <int DIM, int NP, bool NS, typename Real>
 size_t rhs_smem() {
     using LY = RhsLayout<DIM, NP, NS, Real>;
-    return sizeof(Real) * (Shape<DIM, NP>::TAB + (size_t)LY::EPB * LY::PER_ELEM);
+    return LY::TAB_BYTES + LY::PAIR_BYTES + sizeof(Real) * (size_t)LY::EPB * LY::PER_ELEM;
 }
 template <int DIM, int NP, bool NS, typename Real, int V>
 size_t rhs_batch_smem() {
     using LY = RhsLayout<DIM, NP, NS, Real, V>;
-    return (Shape<DIM, NP>::TAB * sizeof(Real) + 15) / 16 * 16 + CTX_RESERVE +
-           sizeof(Real) * (size_t)LY::EPB * LY::PER_ELEM;
+    return LY::FIXED_BYTES + sizeof(Real) * (size_t)LY::EPB * LY::PER_ELEM;
 }
 template <int DIM, int NP, typename Out>
 size_t lift_smem() {
