@@ -57,13 +57,29 @@ typedef struct prandtl_mesh_desc {
     int dim;                   /* 2 or 3 */
     int order;                 /* polynomial degree N (1..5); Np = N + 1 Gauss-Lobatto nodes */
     int num_elements;          /* E */
-    int num_faces;             /* F interior faces (periodic meshes: all faces) */
+    int num_faces;             /* F faces: interior faces, then or mixed with boundary faces */
     const double *elem_adj;    /* [E][dim][dim] adjugate of the element Jacobian, row-major */
     const double *elem_detj;   /* [E] Jacobian determinant */
     const int *face_elems;     /* [F][4] elem1, lface1, elem2, lface2; lface = 2*dir + side,
-                                  side 0 is the xi_dir = 0 face; traces aligned */
+                                  side 0 is the xi_dir = 0 face; traces aligned.  A boundary
+                                  face is {elem1, lface1, -1, bc} with bc an index into
+                                  prandtl_config.bcs (Euler only) */
     const double *face_nor;    /* [F][dim] scaled normal outward from elem1 (|n| = face measure) */
 } prandtl_mesh_desc;
+
+/* Boundary conditions of boundary faces (Euler), each the reference's
+ * boundary integrator of the same name with a constant state
+ * (src/Integrators/BoundaryConditions/): */
+#define PRANDTL_BC_STATE 0            /* SpecifiedState / SupersonicInflow: outer state = state */
+#define PRANDTL_BC_OUTFLOW 1          /* SupersonicOutflow: outer state = inner state */
+#define PRANDTL_BC_SLIP_WALL 2        /* SlipWall: pressure flux of the normal Riemann problem */
+#define PRANDTL_BC_SYMMETRY 3         /* Symmetry: inner state with reflected normal momentum */
+#define PRANDTL_BC_PRESSURE_OUTFLOW 4 /* SubsonicOutflowP: inner state at pressure p */
+typedef struct prandtl_bc {
+    int type;                  /* PRANDTL_BC_* */
+    double state[5];           /* conserved outer state (PRANDTL_BC_STATE), dim+2 used */
+    double p;                  /* outflow pressure (PRANDTL_BC_PRESSURE_OUTFLOW) */
+} prandtl_bc;
 
 /* Physics and switches.  Defaults (prandtl_config_default) match the
  * reference's Simulation::LoadConfig defaults (Simulation.cpp:153-157) and
@@ -87,6 +103,8 @@ typedef struct prandtl_config {
                                   per-node primitives, entropy variables, lambda_max and the RK
                                   state and registers in FP64 (no reference counterpart) */
     double timeout_s;          /* bound on every host-side wait; 0 selects 120 s */
+    int num_bcs;               /* boundary conditions the mesh's boundary faces index; */
+    const prandtl_bc *bcs;     /*   copied at create (0 / NULL: periodic meshes only) */
 } prandtl_config;
 
 typedef struct prandtl_handle prandtl_handle;

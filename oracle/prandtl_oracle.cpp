@@ -424,6 +424,8 @@ struct Ctx {
     const int *faces;
     Phys P;
     int parabolic, blending, quirks, dissipation;
+    int num_bcs;
+    const oracle_bc *bcs;
     double alpha_max, alpha_min, modalThreshold;
     std::vector<double> x, w, D, Dhat, Dhat2;   // Dhat, Dhat2 as [i][l]
     std::vector<double> Vinv;                   // [nd][nd] modal basis inverse
@@ -463,6 +465,8 @@ void setup(Ctx &X, const oracle_mesh *m, const oracle_config *c) {
     X.parabolic = c->parabolic;
     X.blending = c->blending;
     X.quirks = c->quirks;
+    X.num_bcs = c->num_bcs;
+    X.bcs = c->bcs;
     X.dissipation = c->surface_dissipation;
     X.alpha_max = c->alpha_max;
     X.alpha_min = c->alpha_min;
@@ -510,6 +514,81 @@ void setup(Ctx &X, const oracle_mesh *m, const oracle_config *c) {
 }
 
 inline int node_id(const Ctx &X, int i, int j, int k) { return k * X.ny() * X.nx() + j * X.nx() + i; }
+
+// Boundary-face flux of trace s1 (BdrFaceIntegrator.cpp:61-138 with the
+// integrators of src/Integrators/BoundaryConditions/).  The element receives
+// -flux / (w0 J1) at the face node.  Returns the largest |V|+c seen.
+double bdr_face_flux(const Ctx &X, const oracle_bc &bc, const double *s1_in, const double *nor, double *flux) {
+    const int dim = X.dim, nf = dim + 2;
+    const double gamma = X.P.gamma, gammaM1 = X.P.gammaM1, gammaM1Inverse = X.P.gammaM1Inverse;
+    double s1[5] = {0, 0, 0, 0, 0}, s2[5] = {0, 0, 0, 0, 0};
+    for (int f = 0; f < nf; ++f) s1[f] = s1_in[f];
+    switch (bc.type) {
+    case ORACLE_BC_STATE:   // SpecifiedStateBdrFaceIntegrator.cpp:24-36 (constant)
+        for (int f = 0; f < nf; ++f) s2[f] = bc.state[f];
+        return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
+    case ORACLE_BC_OUTFLOW:   // SupersonicOutflowBdrFaceIntegrator.cpp:11-14
+        for (int f = 0; f < nf; ++f) s2[f] = s1[f];
+        return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
+    case ORACLE_BC_SYMMETRY: {   // SymmetryBdrFaceIntegrator.cpp:11-32
+        const double nn = norml2(nor, dim);
+        if (nn == 0.0) {
+            for (int f = 0; f < nf; ++f) flux[f] = 0.0;
+            return 0.0;
+        }
+        const double rn = 1.0 / nn;
+        double un[3], mn = 0.0;
+        for (int d = 0; d < dim; ++d) un[d] = nor[d] * rn;
+        for (int f = 0; f < nf; ++f) s2[f] = s1[f];
+        for (int d = 0; d < dim; ++d) mn += s2[1 + d] * un[d];
+        for (int d = 0; d < dim; ++d) s2[1 + d] += -2.0 * mn * un[d];
+        return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
+    }
+    case ORACLE_BC_SLIP_WALL: {   // SlipWallBdrFaceIntegrator.cpp:16-59
+        const double nn = norml2(nor, dim), rn = 1.0 / nn;
+        const double gammaP1 = 1.0 + gamma, gammaP1Inverse = 1.0 / gammaP1;
+        const double rho = s1[0];
+        double mn = 0.0, vv = 0.0;
+        for (int d = 0; d < dim; ++d) {
+            mn += s1[1 + d] * (nor[d] * rn);
+            const double v = s1[1 + d] / rho;
+            vv += v * v;
+        }
+        const double u = mn / rho;   // normal velocity in the rotated frame
+        const double p = gammaM1 * (s1[nf - 1] - 0.5 * rho * vv);
+        const double an = sound_speed(p, rho, gamma);
+        double p_star;
+        if (u > 0.0)
+            p_star = p + 0.25 * u * gammaP1 * rho *
+                             (u + std::sqrt(u * u + 8.0 * gammaP1Inverse / rho * p * (gammaM1 * gammaP1Inverse + 1.0)));
+        else
+            p_star = p * std::pow(std::max(1.0 + 0.5 * gammaM1 * u / an, 0.0001), 2.0 * gamma * gammaM1Inverse);
+        for (int f = 0; f < nf; ++f) flux[f] = 0.0;
+        for (int d = 0; d < dim; ++d) flux[1 + d] = p_star * nor[d];
+        return std::sqrt(vv) + an;
+    }
+    case ORACLE_BC_PRESSURE_OUTFLOW: {   // SubsonicOutflowPBdrFaceIntegrator.cpp:17-29
+        // Q9: `Vector vel(state1.GetData() + 1, dim); vel /= state1(0);` wraps the
+        // inner trace, so (reference) both traces carry velocity in the momentum slots
+        double vel[3], vv = 0.0;
+        if (X.quirks == 0) {
+            const double r = 1.0 / s1[0];
+            for (int d = 0; d < dim; ++d) s1[1 + d] *= r;
+            for (int d = 0; d < dim; ++d) vel[d] = s1[1 + d];
+        } else {
+            const double r = 1.0 / s1[0];
+            for (int d = 0; d < dim; ++d) vel[d] = s1[1 + d] * r;
+        }
+        for (int d = 0; d < dim; ++d) vv += vel[d] * vel[d];
+        for (int f = 0; f < nf; ++f) s2[f] = s1[f];
+        s2[nf - 1] = bc.p * gammaM1Inverse + 0.5 * s1[0] * vv;
+        return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
+    }
+    default:
+        for (int f = 0; f < nf; ++f) flux[f] = 0.0;
+        return 0.0;
+    }
+}
 
 // Element-local node on local face lf (= 2*dir + side) for face node a.
 int face_node(const Ctx &X, int lf, int a) {
@@ -884,6 +963,17 @@ void run_rhs(const Ctx &X, const double *u, double *dudt, double *alpha_out, dou
             if ((fe[1] >> 1) != dir) continue;
             const int e1 = fe[0], lf1 = fe[1], e2 = fe[2], lf2 = fe[3];
             const double *nor = X.fnor + (long)fc * dim;
+            if (e2 < 0) {   // boundary face (BdrFaceIntegrator::AssembleFaceVector, Euler)
+                const double a1 = 1.0 / (w0 * X.detj[e1]);
+                for (int a = 0; a < nfn; ++a) {
+                    const long g1 = (long)e1 * nd + face_node(X, lf1, a);
+                    double s1[5], flux[5];
+                    for (int f = 0; f < nf; ++f) s1[f] = u[f * Ndof + g1];
+                    bdr_face_flux(X, X.bcs[lf2], s1, nor, flux);
+                    for (int f = 0; f < nf; ++f) dudt[f * Ndof + g1] += a1 * -flux[f];
+                }
+                continue;
+            }
             const double a1 = 1.0 / (w0 * X.detj[e1]), a2 = 1.0 / (w0 * X.detj[e2]);
             for (int a = 0; a < nfn; ++a) {
                 const int n1 = face_node(X, lf1, a), n2 = face_node(X, lf2, a);
@@ -939,6 +1029,11 @@ int oracle_rhs(const oracle_mesh *m, const oracle_config *c, const double *u, do
     if (!m || !c || !u || !dudt) return 1;
     if (m->dim < 2 || m->dim > 3 || m->order < 1 || m->order > 9) return 1;
     if (nthreads <= 0) nthreads = 1;
+    for (int f = 0; f < m->num_faces; ++f) {   // boundary faces: Euler, a valid BC index
+        const int *fe = m->face_elems + 4 * f;
+        if (fe[2] >= 0) continue;
+        if (c->parabolic || !c->bcs || fe[3] < 0 || fe[3] >= c->num_bcs) return 1;
+    }
     Ctx X;
     setup(X, m, c);
     run_rhs(X, u, dudt, alpha, lambda_max, grad, nthreads);

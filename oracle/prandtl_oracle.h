@@ -39,6 +39,21 @@ typedef struct oracle_mesh {
     const double *face_nor;   /* [F][dim] */
 } oracle_mesh;
 
+/* Boundary conditions (Euler).  A boundary face is listed in face_elems as
+ * {elem1, lface1, -1, bc} with bc an index into oracle_config.bcs. */
+enum {
+    ORACLE_BC_STATE = 0,            /* SpecifiedState / SupersonicInflow with a constant state */
+    ORACLE_BC_OUTFLOW = 1,          /* SupersonicOutflow: outer state = inner state */
+    ORACLE_BC_SLIP_WALL = 2,        /* SlipWall: pressure flux of the normal Riemann problem */
+    ORACLE_BC_SYMMETRY = 3,         /* Symmetry: inner state with reflected normal momentum */
+    ORACLE_BC_PRESSURE_OUTFLOW = 4  /* SubsonicOutflowP with a constant pressure */
+};
+typedef struct oracle_bc {
+    int type;
+    double state[5];    /* conserved outer state (ORACLE_BC_STATE) */
+    double p;           /* outflow pressure (ORACLE_BC_PRESSURE_OUTFLOW) */
+} oracle_bc;
+
 typedef struct oracle_config {
     double gamma;
     double Pr;
@@ -51,6 +66,8 @@ typedef struct oracle_config {
     int sutherland;           /* Sutherland viscosity law */
     int quirks;               /* 0: reproduce the reference exactly; 1: fixed */
     int surface_dissipation;  /* 1: as the reference; 0: EC surface flux (test switch) */
+    int num_bcs;              /* boundary conditions referenced by boundary faces */
+    const oracle_bc *bcs;
 } oracle_config;
 
 /* One RHS evaluation dudt = L(u).  alpha (may be NULL) receives the per-element

@@ -22,11 +22,34 @@ class OracleMesh(C.Structure):
                 ("face_nor", C.POINTER(C.c_double))]
 
 
+class OracleBC(C.Structure):
+    _fields_ = [("type", C.c_int), ("state", C.c_double * 5), ("p", C.c_double)]
+
+
+# boundary-condition types (prandtl_oracle.h ORACLE_BC_*)
+BC_TYPES = {"state": 0, "outflow": 1, "slip_wall": 2, "symmetry": 3, "pressure_outflow": 4}
+
+
 class OracleConfig(C.Structure):
     _fields_ = [("gamma", C.c_double), ("Pr", C.c_double), ("mu", C.c_double),
                 ("R_gas", C.c_double), ("alpha_max", C.c_double), ("alpha_min", C.c_double),
                 ("parabolic", C.c_int), ("blending", C.c_int), ("sutherland", C.c_int),
-                ("quirks", C.c_int), ("surface_dissipation", C.c_int)]
+                ("quirks", C.c_int), ("surface_dissipation", C.c_int),
+                ("num_bcs", C.c_int), ("bcs", C.POINTER(OracleBC))]
+
+
+def make_bcs(bcs):
+    """ctypes array of boundary conditions from [(type name, state or None, p or None), ...]."""
+    if not bcs:
+        return None
+    arr = (OracleBC * len(bcs))()
+    for k, b in enumerate(bcs):
+        kind, state, p = (tuple(b) + (None, None))[:3]
+        arr[k].type = BC_TYPES[kind]
+        for f, v in enumerate(state if state is not None else []):
+            arr[k].state[f] = float(v)
+        arr[k].p = float(p) if p is not None else 0.0
+    return arr
 
 
 def build():
@@ -66,7 +89,7 @@ class Oracle:
 
     def __init__(self, mesh, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05, alpha_max=0.5,
                  alpha_min=0.001, parabolic=0, blending=0, sutherland=0, quirks=0,
-                 surface_dissipation=1, nthreads=None):
+                 surface_dissipation=1, nthreads=None, bcs=None):
         self.mesh = mesh
         self._adj = np.ascontiguousarray(mesh.elem_adj, dtype=np.float64)
         self._detj = np.ascontiguousarray(mesh.elem_detj, dtype=np.float64)
@@ -75,8 +98,10 @@ class Oracle:
         self.m = OracleMesh(mesh.dim, mesh.order, mesh.num_elements, mesh.num_faces,
                             _p(self._adj), _p(self._detj),
                             self._faces.ctypes.data_as(C.POINTER(C.c_int)), _p(self._nor))
+        self._bcs = make_bcs(bcs)
         self.c = OracleConfig(gamma, Pr, mu, R_gas, alpha_max, alpha_min, parabolic, blending,
-                              sutherland, quirks, surface_dissipation)
+                              sutherland, quirks, surface_dissipation, len(bcs) if bcs else 0,
+                              self._bcs)
         self.nthreads = nthreads or os.cpu_count() or 1
 
     @property

@@ -23,6 +23,12 @@ FILES="$SRC/BasicOperations/BasicOperations.cpp $SRC/RiemannSolvers/Chandrasheka
  $SRC/Fluxes/NavierStokesFlux.cpp $SRC/Integrators/DGSEMIntegrator/DGSEMIntegrator.cpp \
  $SRC/Integrators/Lifting/LiftingScheme.cpp $SRC/Integrators/Lifting/LiftingBR1/LiftingBR1.cpp \
  $SRC/Indicators/Indicator.cpp $SRC/Indicators/PerssonPeraireIndicator.cpp $SRC/ModalBasis/ModalBasis.cpp \
+ $SRC/Integrators/BoundaryConditions/BdrFaceIntegrator.cpp \
+ $SRC/Integrators/BoundaryConditions/SpecifiedStateBdrFaceIntegrator.cpp \
+ $SRC/Integrators/BoundaryConditions/SupersonicOutflowBdrFaceIntegrator.cpp \
+ $SRC/Integrators/BoundaryConditions/SlipWallBdrFaceIntegrator.cpp \
+ $SRC/Integrators/BoundaryConditions/SymmetryBdrFaceIntegrator.cpp \
+ $SRC/Integrators/BoundaryConditions/SubsonicOutflowPBdrFaceIntegrator.cpp \
  $HERE/ref_driver.cpp"
 # -O2 -DNDEBUG as the reference's Release configuration (configure.sh)
 FLAGS="-O2 -DNDEBUG -std=c++17 -fPIC -shared -w"

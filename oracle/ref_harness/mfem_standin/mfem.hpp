@@ -37,6 +37,9 @@
         if (!(x)) throw std::runtime_error("MFEM_VERIFY failed");    \
     } while (0)
 #define MFEM_ABORT(msg) throw std::runtime_error("MFEM_ABORT");
+#define MFEM_WARNING(msg) \
+    do {                  \
+    } while (0)
 
 namespace mfem {
 
@@ -571,6 +574,7 @@ public:
 
 class FaceElementTransformations {
 public:
+    int ElementNo = -1;   // the face number
     int Elem1No = -1, Elem2No = -1;
     int lf1 = 0, lf2 = 0, dim = 0;
     ElementTransformation *T1 = nullptr, *T2 = nullptr;
@@ -583,6 +587,43 @@ public:
     const IntegrationPoint &GetElement2IntPoint() { return eip2; }
     const DenseMatrix &Jacobian() { return Jf; }
     void Transform(const IntegrationPoint &, Vector &x) { x.SetSize(dim); x = 0.0; }
+};
+
+// ------------------------------------------------------------ coefficients
+// MFEM's function coefficients: a std::function of the physical point (and,
+// with SetTime, of the time).  Boundary states here are constant, so the
+// point comes from FaceElementTransformations::Transform (zero).
+inline void mfem_error(const char *msg) { throw std::runtime_error(msg); }
+class FunctionCoefficient {
+public:
+    explicit FunctionCoefficient(std::function<real_t(const Vector &)> f) : f_(std::move(f)) {}
+    void SetTime(real_t t) { t_ = t; }
+    real_t Eval(FaceElementTransformations &T, const IntegrationPoint &ip) {
+        Vector x;
+        T.Transform(ip, x);
+        return f_(x);
+    }
+
+private:
+    std::function<real_t(const Vector &)> f_;
+    real_t t_ = 0.0;
+};
+class VectorFunctionCoefficient {
+public:
+    VectorFunctionCoefficient(int vdim, std::function<void(const Vector &, Vector &)> f)
+        : vdim_(vdim), f_(std::move(f)) {}
+    void SetTime(real_t t) { t_ = t; }
+    void Eval(Vector &v, FaceElementTransformations &T, const IntegrationPoint &ip) {
+        Vector x;
+        T.Transform(ip, x);
+        v.SetSize(vdim_);
+        f_(x, v);
+    }
+
+private:
+    int vdim_;
+    std::function<void(const Vector &, Vector &)> f_;
+    real_t t_ = 0.0;
 };
 
 // ------------------------------------------------------------ mesh / spaces

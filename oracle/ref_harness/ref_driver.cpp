@@ -9,8 +9,9 @@
 // without MFEM: the stand-in geometry, and the assembly loops of
 // DGSEMOperator::Mult (DGSEMOperator.cpp:537-591, :60-159) and
 // DGSEMNonlinearForm::Mult / MultLifting (DGSEMNonlinearForm.cpp:424-849,
-// :1070-1545), restated for serial periodic meshes (no shared or boundary
-// faces, P = identity).
+// :1070-1545), restated for serial affine meshes (no shared faces, P =
+// identity).  Boundary faces (Euler only) run the reference's own boundary
+// integrators with constant states.
 #include "mfem.hpp"
 
 #include "BasicOperations.hpp"
@@ -28,6 +29,11 @@
 #include "NavierStokesFlux.hpp"
 #include "PerssonPeraireIndicator.hpp"
 #include "Physics.hpp"
+#include "SlipWallBdrFaceIntegrator.hpp"
+#include "SpecifiedStateBdrFaceIntegrator.hpp"
+#include "SubsonicOutflowPBdrFaceIntegrator.hpp"
+#include "SupersonicOutflowBdrFaceIntegrator.hpp"
+#include "SymmetryBdrFaceIntegrator.hpp"
 #include "prandtl_oracle.h"
 
 namespace mfem {
@@ -143,9 +149,11 @@ void FaceElementTransformations::SetAllIntPoints(const IntegrationPoint *fip) {
         e.x = c[0]; e.y = c[1]; e.z = c[2];
     };
     map(lf1, eip1);
-    map(lf2, eip2);
     T1->SetIntPoint(&eip1);
-    T2->SetIntPoint(&eip2);
+    if (T2) {   // boundary faces have no element 2
+        map(lf2, eip2);
+        T2->SetIntPoint(&eip2);
+    }
 }
 
 }   // namespace mfem
@@ -180,11 +188,12 @@ std::shared_ptr<ParMesh> make_mesh(const oracle_mesh *m) {
     for (int f = 0; f < m->num_faces; ++f) {
         const int *fe = m->face_elems + 4 * f;
         auto F = std::make_unique<FaceElementTransformations>();
+        F->ElementNo = f;
         F->Elem1No = fe[0]; F->lf1 = fe[1];
         F->Elem2No = fe[2]; F->lf2 = fe[3];
         F->dim = dim;
         F->T1 = &pm->trans[fe[0]];
-        F->T2 = &pm->trans[fe[2]];
+        F->T2 = fe[2] >= 0 ? &pm->trans[fe[2]] : nullptr;
         // face Jacobian: element-1 Jacobian columns along the face's
         // tangential directions, oriented so CalcOrtho points out of elem1
         const int d = fe[1] >> 1, s = fe[1] & 1;
@@ -366,11 +375,49 @@ extern "C" int ref_rhs(const oracle_mesh *md, const oracle_config *cfg, const do
         }
         for (int i = 0; i < pmesh->GetNumFaces(); i++) {
             FaceElementTransformations *tr = pmesh->GetInteriorFaceTransformations(i);
+            if (tr->Elem2No < 0) continue;
             vfes->GetElementVDofs(tr->Elem1No, vdofs);
             vfes->GetElementVDofs(tr->Elem2No, vdofs2);
             vdofs.Append(vdofs2);
             u.GetSubVector(vdofs, el_u);
             integ.AssembleFaceVector(*fe, *fe, *tr, el_u, el_dudt);
+            dudt.AddElementVector(vdofs, el_dudt);
+        }
+        // boundary faces (DGSEMNonlinearForm.cpp:781-830): the reference's boundary
+        // integrator of each face's condition, element 1 only
+        std::vector<std::unique_ptr<BdrFaceIntegrator>> bdr;
+        const real_t time = 0.0;
+        for (int k = 0; k < cfg->num_bcs; ++k) {
+            const oracle_bc &b = cfg->bcs[k];
+            switch (b.type) {
+            case ORACLE_BC_STATE: {
+                Vector st(nf);
+                for (int f = 0; f < nf; ++f) st(f) = b.state[f];
+                bdr.emplace_back(new SpecifiedStateBdrFaceIntegrator(lifting, rsolver, Np, time, pc.gamma, st));
+                break;
+            }
+            case ORACLE_BC_OUTFLOW:
+                bdr.emplace_back(new SupersonicOutflowBdrFaceIntegrator(lifting, rsolver, Np, time, pc.gamma));
+                break;
+            case ORACLE_BC_SLIP_WALL:
+                bdr.emplace_back(new SlipWallBdrFaceIntegrator(lifting, rsolver, Np, time, pc.gamma, true, false));
+                break;
+            case ORACLE_BC_SYMMETRY:
+                bdr.emplace_back(new SymmetryBdrFaceIntegrator(lifting, rsolver, Np, time, pc.gamma, true, false));
+                break;
+            case ORACLE_BC_PRESSURE_OUTFLOW:
+                bdr.emplace_back(new SubsonicOutflowPBdrFaceIntegrator(lifting, rsolver, Np, time, pc.gamma, b.p));
+                break;
+            default:
+                throw std::runtime_error("unknown boundary condition");
+            }
+        }
+        for (int i = 0; i < pmesh->GetNumFaces(); i++) {
+            FaceElementTransformations *tr = pmesh->GetInteriorFaceTransformations(i);
+            if (tr->Elem2No >= 0) continue;
+            vfes->GetElementVDofs(tr->Elem1No, vdofs);
+            u.GetSubVector(vdofs, el_u);
+            bdr.at(tr->lf2)->AssembleFaceVector(*fe, *fe, *tr, el_u, el_dudt);
             dudt.AddElementVector(vdofs, el_dudt);
         }
 #endif

@@ -45,12 +45,19 @@ class MeshDesc(C.Structure):
                 ("face_nor", C.POINTER(C.c_double))]
 
 
+class BC(C.Structure):
+    _fields_ = [("type", C.c_int), ("state", C.c_double * 5), ("p", C.c_double)]
+
+
+BC_TYPES = {"state": 0, "outflow": 1, "slip_wall": 2, "symmetry": 3, "pressure_outflow": 4}
+
+
 class Config(C.Structure):
     _fields_ = [("gamma", C.c_double), ("Pr", C.c_double), ("mu", C.c_double),
                 ("R_gas", C.c_double), ("alpha_max", C.c_double), ("alpha_min", C.c_double),
                 ("parabolic", C.c_int), ("blending", C.c_int), ("sutherland", C.c_int),
                 ("quirks", C.c_int), ("surface_dissipation", C.c_int), ("precision", C.c_int),
-                ("timeout_s", C.c_double)]
+                ("timeout_s", C.c_double), ("num_bcs", C.c_int), ("bcs", C.POINTER(BC))]
 
 
 class BatchConfig(C.Structure):

@@ -26,6 +26,14 @@ struct PhysParams {
     int blending;
 };
 
+// A boundary condition (the layout of prandtl_bc).
+enum BcType : int { BC_STATE = 0, BC_OUTFLOW = 1, BC_SLIP_WALL = 2, BC_SYMMETRY = 3, BC_PRESSURE_OUTFLOW = 4 };
+struct BcDev {
+    int type, pad;
+    double state[5];
+    double p;
+};
+
 // 1D operator tables for one polynomial order (NP <= 8), row-major [i][l].
 struct OpTables {
     double D[64];       // D(i,l) = dL_l/dxi at node i        DGSEMIntegrator.cpp:58-69

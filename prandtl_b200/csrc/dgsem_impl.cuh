@@ -256,7 +256,7 @@ constexpr int next_pow2(int v) { return v <= 1 ? 1 : 2 * next_pow2((v + 1) / 2);
 // admits.  The group width is fixed per element size: 64 lanes for >= 125
 // nodes (the tuner never preferred the other width).
 constexpr int NUM_VARIANTS = 3;
-constexpr int CTX_RESERVE = 1024;   // bytes of per-item contexts reserved in every layout
+constexpr int CTX_RESERVE = 1280;   // bytes of per-item contexts reserved in every layout
 
 template <int DIM, int NP, bool NS, typename Real, int V = 0, bool VC = false>
 struct RhsLayout {
@@ -337,6 +337,7 @@ struct ElemIO {
     int E;
     int mode;
     double dt, rkA, rkB;
+    const BcDev *bcs;           // boundary conditions (boundary faces)
 };
 // Per-warp (rhs) or per-CTA (lift) copy of the current solve's constants.
 struct __align__(16) WarpCtx {
@@ -364,6 +365,7 @@ __device__ __forceinline__ ElemIO io_from_args(const MeshDev &m, const RhsArgs &
     io.dt = a.dt;
     io.rkA = a.rkA;
     io.rkB = a.rkB;
+    io.bcs = m.bcs;
     return io;
 }
 
@@ -386,6 +388,7 @@ __device__ __forceinline__ ElemIO io_from_batch(const BatchInst &I, BatchInst *I
     io.dt = I.dt;
     io.rkA = st.rkA;
     io.rkB = st.rkB;
+    io.bcs = I.bcs;
     if (st.scheme == BATCH_LSRK45) {
         const int in = I.cur ^ (st.stage & 1);
         io.u = I.u[in];
@@ -413,6 +416,93 @@ __device__ __forceinline__ int batch_slot(const int *prefix, int n, int first) {
     }
     return lo;
 }
+// Boundary-face flux of the inner trace s_in (FP64 conserved state) along the
+// element's outward scaled normal nor: the reference's boundary integrators
+// with constant states (src/Integrators/BoundaryConditions/; the element is
+// Elem1 and receives -flux / (w0 J), BdrFaceIntegrator.cpp:61-138).  Inviscid.
+// The outer state is formed in FP64; the Chandrashekar surface flux runs in
+// the working precision like the interior faces.
+template <int DIM, typename Real>
+__device__ __forceinline__ void boundary_flux(const BcDev &bc, const double *s_in, const double *nor,
+                                              const PhysParams &P, double pref, Real *flux) {
+    constexpr int NF = DIM + 2;
+    const double gamma = P.gamma, gm1 = P.gammaM1, gm1i = P.gammaM1Inverse;
+    double s1[NF], s2[NF], nn = 0.0;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) s1[f] = s_in[f];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) nn += nor[d] * nor[d];
+    nn = sqrt(nn);
+    if (bc.type == BC_SLIP_WALL) {   // SlipWallBdrFaceIntegrator.cpp:16-59
+        const double rn = 1.0 / nn, gp1 = 1.0 + gamma, gp1i = 1.0 / gp1;
+        const double rho = s1[0];
+        double mn = 0.0, vv = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            mn += s1[1 + d] * (nor[d] * rn);
+            const double v = s1[1 + d] / rho;
+            vv += v * v;
+        }
+        const double un = mn / rho;   // normal velocity of the rotated state
+        const double p = gm1 * (s1[NF - 1] - 0.5 * rho * vv);
+        const double an = sqrt(gamma * p / rho);
+        double p_star;
+        if (un > 0.0)
+            p_star = p + 0.25 * un * gp1 * rho * (un + sqrt(un * un + 8.0 * gp1i / rho * p * (gm1 * gp1i + 1.0)));
+        else
+            p_star = p * pow(fmax(1.0 + 0.5 * gm1 * un / an, 0.0001), 2.0 * gamma * gm1i);
+        // the FP32-bulk form carries p - pref in every momentum flux (pref = 0 in FP64)
+        flux[0] = 0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) flux[1 + d] = Real((p_star - pref) * nor[d]);
+        flux[NF - 1] = 0;
+        return;
+    }
+    if (bc.type == BC_STATE) {   // SpecifiedStateBdrFaceIntegrator.cpp:24-36
+#pragma unroll
+        for (int f = 0; f < NF; ++f) s2[f] = bc.state[f];
+    } else if (bc.type == BC_SYMMETRY) {   // SymmetryBdrFaceIntegrator.cpp:11-32
+        if (nn == 0.0) {
+#pragma unroll
+            for (int f = 0; f < NF; ++f) flux[f] = 0;
+            return;
+        }
+        const double rn = 1.0 / nn;
+        double mn = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) mn += s1[1 + d] * (nor[d] * rn);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) s2[f] = s1[f];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) s2[1 + d] += -2.0 * mn * (nor[d] * rn);
+    } else if (bc.type == BC_PRESSURE_OUTFLOW) {   // SubsonicOutflowPBdrFaceIntegrator.cpp:17-29
+        // quirks == 0 (Q9): the reference's velocity vector wraps the inner
+        // trace, so both traces carry velocity in their momentum slots
+        const double r = 1.0 / s1[0];
+        double vel[DIM], vv = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            vel[d] = s1[1 + d] * r;
+            if (P.quirks == 0) s1[1 + d] = vel[d];
+            vv += vel[d] * vel[d];
+        }
+#pragma unroll
+        for (int f = 0; f < NF; ++f) s2[f] = s1[f];
+        s2[NF - 1] = bc.p * gm1i + 0.5 * s1[0] * vv;
+    } else {   // BC_OUTFLOW, SupersonicOutflowBdrFaceIntegrator.cpp:11-14
+#pragma unroll
+        for (int f = 0; f < NF; ++f) s2[f] = s1[f];
+    }
+    Real m1[NF], m2[NF], nr[DIM];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) { m1[f] = Real(s1[f]); m2[f] = Real(s2[f]); }
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) nr[d] = Real(nor[d]);
+    face_flux<DIM, Real>(m1, cast_prim<DIM, Real>(primitives<DIM, double>(s1, gamma, gm1), pref), m2,
+                         cast_prim<DIM, Real>(primitives<DIM, double>(s2, gamma, gm1), pref), nr, Real(gm1i),
+                         P.quirks == 0, P.dissipation != 0, flux);
+}
+
 // ------------------------------------------------------------------- RHS
 // Real is the working precision of the O(Np^{d+1}) work (two-point fluxes,
 // flux differencing, surface fluxes, gradients): double for the plain FP64
@@ -754,8 +844,20 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
         const int lf = it / NFN, fa = it - lf * NFN;
         const int no = face_node<DIM, NP>(lf, fa);
         const int4 t = __ldg(a.nbr + (long long)e * (2 * DIM) + lf);
-        const long long gn = (long long)t.x * ND + face_node<DIM, NP>(t.y, fa);
         const long long go = (long long)e * ND + no;
+        if (t.x < 0) {   // boundary face: the element is Elem1; inviscid (Euler)
+            double sb[NF], nb[DIM];
+            Real fb[NF];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) sb[f] = __ldg(a.u + f * Ndof + go);
+#pragma unroll
+            for (int q = 0; q < DIM; ++q) nb[q] = __ldg(a.fnor + (long long)t.z * DIM + q);
+            boundary_flux<DIM, Real>(a.bcs[t.y], sb, nb, P, pref, fb);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) sF[f * NFI + it] = -(aw * fb[f]);
+            continue;
+        }
+        const long long gn = (long long)t.x * ND + face_node<DIM, NP>(t.y, fa);
         const bool own_is_1 = (t.w == 0);
         // the own trace's conserved state is read only by the gradient form
         // (its Q8 path rebuilds the trace from it); otherwise only its momentum

@@ -22,6 +22,7 @@ struct MeshDev {
     const double *fnor;  // [F][DIM] scaled normal, outward from elem1
     int E;
     long long Ndof;      // E * Np^DIM
+    const BcDev *bcs;    // boundary conditions (boundary faces: nbr = {-1, bc, face id, 0})
 };
 
 struct RhsArgs {
@@ -68,6 +69,7 @@ struct BatchInst {
     int steps_done;
     int cur;                    // LSRK: u[cur] holds the state at the start of the step
     int pad;
+    const BcDev *bcs;           // boundary conditions (boundary faces)
     unsigned long long lambda;  // max |V|+c over the current step's stages (ordered bits)
     unsigned long long lambda_last;   // ... of the last completed step
 };

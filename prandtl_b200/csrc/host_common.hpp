@@ -130,9 +130,12 @@ inline void build_phys(const prandtl_config &c, int N, PhysParams &P) {
 
 // Checks a mesh descriptor and builds the neighbour table nbr[e][lf] =
 // {neighbour element, its local face, face id, role (0: e is Elem1)}.  Every
-// element face must be an interior face exactly once, with the traces aligned
-// (local faces 2*dir and 2*dir+1 of the same direction).
-inline prandtl_status validate_mesh(const prandtl_mesh_desc *md, std::vector<int4> &nbr, std::string &msg) {
+// element face must be listed exactly once: as an interior face with the
+// traces aligned (local faces 2*dir and 2*dir+1 of the same direction), or as
+// a boundary face {elem1, lface1, -1, bc} with 0 <= bc < num_bcs, recorded as
+// {-1, bc, face id, 0}.
+inline prandtl_status validate_mesh(const prandtl_mesh_desc *md, std::vector<int4> &nbr, std::string &msg,
+                                    int num_bcs = 0) {
     if (md->dim != 2 && md->dim != 3) { msg = "dim must be 2 or 3"; return PRANDTL_EUNSUPPORTED; }
     if (!order_supported(md->dim, md->order)) { msg = "order must be in 1..5"; return PRANDTL_EUNSUPPORTED; }
     if (md->num_elements <= 0 || md->num_faces < 0) { msg = "bad sizes"; return PRANDTL_EINVAL; }
@@ -141,11 +144,30 @@ inline prandtl_status validate_mesh(const prandtl_mesh_desc *md, std::vector<int
         return PRANDTL_EINVAL;
     }
     const int NFACE = 2 * md->dim, E = md->num_elements, F = md->num_faces;
-    nbr.assign((size_t)E * NFACE, make_int4(-1, -1, -1, -1));
+    constexpr int UNSET = -2;
+    nbr.assign((size_t)E * NFACE, make_int4(UNSET, -1, -1, -1));
     for (int f = 0; f < F; ++f) {
         const int *fe = md->face_elems + 4 * f;
         const int e1 = fe[0], l1 = fe[1], e2 = fe[2], l2 = fe[3];
-        if (e1 < 0 || e1 >= E || e2 < 0 || e2 >= E || l1 < 0 || l1 >= NFACE || l2 < 0 || l2 >= NFACE) {
+        if (e1 < 0 || e1 >= E || l1 < 0 || l1 >= NFACE) {
+            msg = "face " + std::to_string(f) + " out of range";
+            return PRANDTL_EINVAL;
+        }
+        int4 &a = nbr[(size_t)e1 * NFACE + l1];
+        if (a.x != UNSET) {
+            msg = "element face listed twice (face " + std::to_string(f) + ")";
+            return PRANDTL_EINVAL;
+        }
+        if (e2 < 0) {   // boundary face
+            if (e2 != -1 || l2 < 0 || l2 >= num_bcs) {
+                msg = "boundary face " + std::to_string(f) + ": no boundary condition " + std::to_string(l2) +
+                      " (" + std::to_string(num_bcs) + " given)";
+                return PRANDTL_EINVAL;
+            }
+            a = make_int4(-1, l2, f, 0);
+            continue;
+        }
+        if (e2 >= E || l2 < 0 || l2 >= NFACE) {
             msg = "face " + std::to_string(f) + " out of range";
             return PRANDTL_EINVAL;
         }
@@ -153,9 +175,8 @@ inline prandtl_status validate_mesh(const prandtl_mesh_desc *md, std::vector<int
             msg = "face " + std::to_string(f) + ": only aligned opposite faces are supported";
             return PRANDTL_EUNSUPPORTED;
         }
-        int4 &a = nbr[(size_t)e1 * NFACE + l1];
         int4 &b = nbr[(size_t)e2 * NFACE + l2];
-        if (a.x >= 0 || b.x >= 0) {
+        if (b.x != UNSET) {
             msg = "element face listed twice (face " + std::to_string(f) + ")";
             return PRANDTL_EINVAL;
         }
@@ -163,12 +184,47 @@ inline prandtl_status validate_mesh(const prandtl_mesh_desc *md, std::vector<int
         b = make_int4(e1, l1, f, 1);
     }
     for (size_t q = 0; q < nbr.size(); ++q)
-        if (nbr[q].x < 0) {
-            msg = "element " + std::to_string(q / NFACE) + " has a boundary face; only periodic meshes are built";
+        if (nbr[q].x == UNSET) {
+            msg = "element " + std::to_string(q / NFACE) + " has a face that is neither interior nor a boundary face";
             return PRANDTL_EUNSUPPORTED;
         }
     for (int e = 0; e < E; ++e)
         if (!(md->elem_detj[e] > 0.0)) { msg = "non-positive det J"; return PRANDTL_EINVAL; }
+    return PRANDTL_OK;
+}
+
+inline bool has_boundary(const prandtl_mesh_desc *md) {
+    for (int f = 0; f < md->num_faces; ++f)
+        if (md->face_elems[4 * f + 2] < 0) return true;
+    return false;
+}
+
+// Device copy of the boundary conditions (BcDev has prandtl_bc's layout).
+inline std::vector<BcDev> device_bcs(const prandtl_config *cfg) {
+    static_assert(sizeof(BcDev) == sizeof(prandtl_bc), "BcDev mirrors prandtl_bc");
+    std::vector<BcDev> out((size_t)(cfg->num_bcs > 0 && cfg->bcs ? cfg->num_bcs : 0));
+    for (size_t k = 0; k < out.size(); ++k) {
+        out[k].type = cfg->bcs[k].type;
+        out[k].pad = 0;
+        for (int f = 0; f < 5; ++f) out[k].state[f] = cfg->bcs[k].state[f];
+        out[k].p = cfg->bcs[k].p;
+    }
+    return out;
+}
+
+inline prandtl_status check_bcs(const prandtl_config *cfg, std::string &msg) {
+    if (cfg->num_bcs < 0 || (cfg->num_bcs > 0 && !cfg->bcs)) { msg = "bad boundary-condition table"; return PRANDTL_EINVAL; }
+    for (int k = 0; k < cfg->num_bcs; ++k) {
+        const prandtl_bc &b = cfg->bcs[k];
+        if (b.type < PRANDTL_BC_STATE || b.type > PRANDTL_BC_PRESSURE_OUTFLOW) {
+            msg = "boundary condition " + std::to_string(k) + ": unknown type";
+            return PRANDTL_EINVAL;
+        }
+        if (b.type == PRANDTL_BC_STATE && !(b.state[0] > 0.0)) {
+            msg = "boundary condition " + std::to_string(k) + ": outer density must be positive";
+            return PRANDTL_EINVAL;
+        }
+    }
     return PRANDTL_OK;
 }
 
@@ -183,6 +239,7 @@ inline prandtl_status check_face_normals(const prandtl_mesh_desc *md, std::strin
         const double *nor = md->face_nor + (size_t)f * dim;
         for (int side = 0; side < 2; ++side) {
             const int e = fe[2 * side], lf = fe[2 * side + 1], d = lf >> 1;
+            if (e < 0) continue;   // boundary face: no element 2
             const double sg = ((lf & 1) ? 1.0 : -1.0) * (side == 0 ? 1.0 : -1.0);
             const double *row = md->elem_adj + ((size_t)e * dim + d) * dim;
             double err = 0, mag = 0;

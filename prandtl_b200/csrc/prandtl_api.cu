@@ -41,6 +41,7 @@ struct prandtl_handle {
     float *d_grad32 = nullptr;                    // NS primitive gradients (FP32-bulk form)
     double *d_alpha = nullptr;
     unsigned long long *d_lambda = nullptr;
+    BcDev *d_bcs = nullptr;                       // boundary conditions
     size_t bytes = 0;
     long long launches = 0;
     // optional per-kernel CUDA-event timing (prandtl_profile)
@@ -110,6 +111,7 @@ MeshDev mesh_dev(const prandtl_handle *h) {
     m.fnor = h->d_fnor;
     m.E = h->E;
     m.Ndof = h->Ndof;
+    m.bcs = h->d_bcs;
     return m;
 }
 
@@ -152,6 +154,7 @@ void free_all(prandtl_handle *h) {
     cudaFree(h->d_grad32);
     cudaFree(h->d_alpha);
     cudaFree(h->d_lambda);
+    cudaFree(h->d_bcs);
     if (h->done) cudaEventDestroy(h->done);
     for (auto &r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (auto ev : h->ev_pool) cudaEventDestroy(ev);
@@ -199,7 +202,12 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
     std::vector<int4> nbr;
     {
         std::string msg;
-        prandtl_status vst = validate_mesh(md, nbr, msg);
+        prandtl_status vst = check_bcs(cfg, msg);
+        if (vst == PRANDTL_OK) vst = validate_mesh(md, nbr, msg, cfg->num_bcs);
+        if (vst == PRANDTL_OK && cfg->parabolic && has_boundary(md)) {
+            msg = "boundary faces are supported for Euler (parabolic = 0)";
+            vst = PRANDTL_EUNSUPPORTED;
+        }
         if (vst == PRANDTL_OK && cfg->parabolic && cfg->quirks != 0) vst = check_face_normals(md, msg);
         if (vst != PRANDTL_OK) return fail(nullptr, vst, msg);
     }
@@ -220,6 +228,7 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
     h->F = F;
     h->Ndof = (long long)E * h->nd;
     h->cfg = *cfg;
+    h->cfg.bcs = nullptr;   // the caller's table is copied to the device below
     if (h->cfg.timeout_s <= 0) h->cfg.timeout_s = 120.0;
     build_tables(md->order, h->T);
     build_phys(h->cfg, md->order, h->P);
@@ -252,6 +261,12 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
         return bail(st);
     if ((st = dalloc(h, &h->d_alpha, (size_t)E, "alpha")) != PRANDTL_OK) return bail(st);
     if ((st = dalloc(h, &h->d_lambda, 1, "lambda")) != PRANDTL_OK) return bail(st);
+    const std::vector<BcDev> bcs = device_bcs(cfg);
+    if (!bcs.empty()) {
+        if ((st = dalloc(h, &h->d_bcs, bcs.size(), "boundary conditions")) != PRANDTL_OK) return bail(st);
+        if ((ce = cudaMemcpy(h->d_bcs, bcs.data(), bcs.size() * sizeof(BcDev), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail(cuda_fail(h, ce, "upload boundary conditions"));
+    }
 
     const std::vector<double> geo = geometry_rows(md);
     if ((ce = cudaMemcpy(h->d_geo, geo.data(), geo.size() * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess)

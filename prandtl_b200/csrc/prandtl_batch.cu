@@ -87,10 +87,10 @@ private:
 
 // Byte offsets of one solve's arrays inside its arena block.
 struct Layout {
-    size_t u[3], grad, alpha, geo, nbr, fnor, total;
+    size_t u[3], grad, alpha, geo, nbr, fnor, bcs, total;
 };
 
-Layout solve_layout(int dim, int order, int E, int F, bool ns, bool blending, bool fp32) {
+Layout solve_layout(int dim, int order, int E, int F, bool ns, bool blending, bool fp32, int num_bcs = 0) {
     long long nd = 1;
     for (int d = 0; d < dim; ++d) nd *= order + 1;
     const size_t Ndof = (size_t)E * nd, nf = dim + 2;
@@ -108,6 +108,8 @@ Layout solve_layout(int dim, int order, int E, int F, bool ns, bool blending, bo
     o += align_up((size_t)E * 2 * dim * sizeof(int4));
     L.fnor = o;
     o += align_up((size_t)std::max(F, 1) * dim * sizeof(double));
+    L.bcs = o;
+    o += align_up((size_t)std::max(num_bcs, 0) * sizeof(BcDev));
     L.total = o;
     return L;
 }
@@ -451,7 +453,7 @@ prandtl_status prandtl_batch_footprint(prandtl_batch *b, const prandtl_mesh_desc
     if ((md->dim != 2 && md->dim != 3) || !order_supported(md->dim, md->order) || md->num_elements <= 0)
         return bfail(b, PRANDTL_EUNSUPPORTED, "unsupported mesh");
     const Layout L = solve_layout(md->dim, md->order, md->num_elements, md->num_faces, cfg->parabolic != 0,
-                                  cfg->blending != 0, b->cfg.precision == 1);
+                                  cfg->blending != 0, b->cfg.precision == 1, cfg->num_bcs);
     *bytes = L.total;
     return PRANDTL_OK;
 }
@@ -468,14 +470,19 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, 
     b->err.clear();
     std::vector<int4> nbr;
     std::string msg;
-    prandtl_status st = validate_mesh(md, nbr, msg);
+    prandtl_status st = check_bcs(cfg, msg);
+    if (st == PRANDTL_OK) st = validate_mesh(md, nbr, msg, cfg->num_bcs);
+    if (st == PRANDTL_OK && cfg->parabolic && has_boundary(md)) {
+        msg = "boundary faces are supported for Euler (parabolic = 0)";
+        st = PRANDTL_EUNSUPPORTED;
+    }
     if (st != PRANDTL_OK) return bfail(b, st, msg);
     BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
     const int dim = md->dim, order = md->order, E = md->num_elements, F = md->num_faces;
     const bool ns = cfg->parabolic != 0, fp32 = b->cfg.precision == 1, blend = cfg->blending != 0;
     const bool vc = ns && cfg->quirks != 0;
     if (vc && (st = check_face_normals(md, msg)) != PRANDTL_OK) return bfail(b, st, msg);
-    const Layout L = solve_layout(dim, order, E, F, ns, blend, fp32);
+    const Layout L = solve_layout(dim, order, E, F, ns, blend, fp32, cfg->num_bcs);
     if (b->free_ids.empty()) return bfail(b, PRANDTL_ENOMEM, "solve table full");
     Class *c = nullptr;
     if ((st = get_class(b, dim, order, ns, vc, &c)) != PRANDTL_OK) return st;
@@ -515,6 +522,10 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, 
                              b->stream)) != cudaSuccess ||
         (blend && (e = cudaMemsetAsync(base + L.alpha, 0, (size_t)E * sizeof(double), b->stream)) != cudaSuccess))
         return undo(bcuda(b, e, "upload solve"));
+    const std::vector<BcDev> bcs = device_bcs(cfg);
+    if (!bcs.empty() && (e = cudaMemcpyAsync(base + L.bcs, bcs.data(), bcs.size() * sizeof(BcDev),
+                                             cudaMemcpyHostToDevice, b->stream)) != cudaSuccess)
+        return undo(bcuda(b, e, "upload boundary conditions"));
     BatchInst I;
     std::memset(&I, 0, sizeof(I));
     build_phys(*cfg, order, I.P);
@@ -524,6 +535,7 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, 
     for (int k = 0; k < 3; ++k) I.u[k] = reinterpret_cast<double *>(base + L.u[k]);
     I.grad = ns ? (void *)(base + L.grad) : nullptr;
     I.alpha = blend ? reinterpret_cast<double *>(base + L.alpha) : nullptr;
+    I.bcs = bcs.empty() ? nullptr : reinterpret_cast<const BcDev *>(base + L.bcs);
     I.Ndof = s.Ndof;
     I.E = E;
     I.order = order;

@@ -290,6 +290,7 @@ extern "C" prandtl_status prandtl_rhs_noalloc(const prandtl_mesh_desc *m, const 
     md.fnor = m->face_nor;
     md.E = E;
     md.Ndof = Ndof;
+    md.bcs = nullptr;   // periodic meshes only: boundary faces fail the check above
     if (cfg->parabolic) {
         LiftArgs la{u, grad};
         if ((e = launch_lift(dim, m->order, md, la, P, T, s)) != cudaSuccess)

@@ -141,12 +141,16 @@ class Mesh:
         return (self.elem_detj[:, None] * wn[None, :]).reshape(-1)
 
 
-def periodic_box(dim: int, n, order: int, lo=0.0, hi=1.0, affine=None) -> Mesh:
-    """Periodic box mesh [lo, hi]^dim with n elements per direction.
+def periodic_box(dim: int, n, order: int, lo=0.0, hi=1.0, affine=None, bcs=None) -> Mesh:
+    """Box mesh [lo, hi]^dim with n elements per direction, periodic unless
+    ``bcs`` says otherwise.
 
     ``n`` may be an int or a per-direction tuple; ``lo``/``hi`` scalars or
     per-direction tuples.  ``affine`` (dim x dim) maps the box afterwards,
-    x = affine @ X, keeping every element affine.
+    x = affine @ X, keeping every element affine.  ``bcs`` (length 2*dim,
+    entry 2*d + side for the side x_d = lo (0) or hi (1)) holds None for a
+    periodic direction or the boundary-condition index of that side's
+    boundary faces, listed as (elem, local face, -1, bc index).
     """
     if dim not in (2, 3):
         raise ValueError("dim must be 2 or 3")
@@ -168,6 +172,9 @@ def periodic_box(dim: int, n, order: int, lo=0.0, hi=1.0, affine=None) -> Mesh:
     strides = [int(np.prod(n[:d])) for d in range(dim)]
     order_pos = {fs: p for p, fs in enumerate(_MFEM_FACE_ORDER[dim])}
 
+    bcs = [None] * (2 * dim) if bcs is None else list(bcs)
+    if len(bcs) != 2 * dim or any((bcs[2 * d] is None) != (bcs[2 * d + 1] is None) for d in range(dim)):
+        raise ValueError("bcs: 2*dim entries, both sides of a direction periodic (None) or both bounded")
     faces = []
     normals = []
     for d in range(dim):
@@ -176,7 +183,17 @@ def periodic_box(dim: int, n, order: int, lo=0.0, hi=1.0, affine=None) -> Mesh:
         e_up = sum(up[k] * strides[k] for k in range(dim))
         for e in range(E):
             eu = int(e_up[e])
-            if n[d] >= 2:
+            if bcs[2 * d] is not None:   # bounded direction: interior faces plus two boundary sides
+                if cell[d, e] == 0:
+                    faces.append((e, 2 * d + 0, -1, int(bcs[2 * d])))
+                    normals.append(-adj[d])
+                if cell[d, e] == n[d] - 1:
+                    faces.append((e, 2 * d + 1, -1, int(bcs[2 * d + 1])))
+                    normals.append(+adj[d])
+                else:
+                    faces.append((e, 2 * d + 1, eu, 2 * d + 0))
+                    normals.append(+adj[d])
+            elif n[d] >= 2:
                 if e < eu:
                     faces.append((e, 2 * d + 1, eu, 2 * d + 0))
                     normals.append(+adj[d])

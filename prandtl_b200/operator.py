@@ -52,10 +52,26 @@ class MeshArrays:
                                   self.nor.ctypes.data_as(dp))
 
 
+def make_bcs(bcs):
+    """ctypes array of prandtl_bc from [(type name, state or None, p or None), ...]:
+    type names "state", "outflow", "slip_wall", "symmetry", "pressure_outflow"."""
+    if not bcs:
+        return None
+    arr = (_lib.BC * len(bcs))()
+    for k, b in enumerate(bcs):
+        kind, state, p = (tuple(b) + (None, None))[:3]
+        arr[k].type = _lib.BC_TYPES[kind]
+        for f, v in enumerate(state if state is not None else []):
+            arr[k].state[f] = float(v)
+        arr[k].p = float(p) if p is not None else 0.0
+    return arr
+
+
 def make_config(*, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05, parabolic=False, blending=False,
                 sutherland=False, alpha_max=0.5, alpha_min=0.001, quirks="reference",
-                surface_dissipation=True, precision="fp64", timeout_s=120.0) -> _lib.Config:
-    """prandtl_config from the DGSEMOperator keyword arguments."""
+                surface_dissipation=True, precision="fp64", timeout_s=120.0, bcs=None) -> _lib.Config:
+    """prandtl_config from the DGSEMOperator keyword arguments (the BC array is
+    kept alive on the returned object)."""
     cfg = _lib.Config()
     _lib.load().prandtl_config_default(C.byref(cfg))
     cfg.gamma, cfg.Pr, cfg.mu, cfg.R_gas = gamma, Pr, mu, R_gas
@@ -69,6 +85,9 @@ def make_config(*, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05, parabolic=False, b
         raise ValueError("precision must be 'fp64' or 'fp32' (FP32 bulk, FP64 RK state)")
     cfg.precision = 1 if precision == "fp32" else 0
     cfg.timeout_s = timeout_s
+    cfg._bcs = make_bcs(bcs)
+    cfg.num_bcs = len(bcs) if bcs else 0
+    cfg.bcs = cfg._bcs
     return cfg
 
 
@@ -76,7 +95,7 @@ class DGSEMOperator:
     def __init__(self, mesh: Mesh, *, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05,
                  parabolic=False, blending=False, sutherland=False, alpha_max=0.5,
                  alpha_min=0.001, quirks="reference", surface_dissipation=True,
-                 precision="fp64", timeout_s=120.0):
+                 precision="fp64", timeout_s=120.0, bcs=None):
         L = _lib.load()
         self.mesh = mesh
         self._arrays = MeshArrays(mesh)
@@ -84,7 +103,7 @@ class DGSEMOperator:
         cfg = make_config(gamma=gamma, Pr=Pr, mu=mu, R_gas=R_gas, parabolic=parabolic,
                           blending=blending, sutherland=sutherland, alpha_max=alpha_max,
                           alpha_min=alpha_min, quirks=quirks, surface_dissipation=surface_dissipation,
-                          precision=precision, timeout_s=timeout_s)
+                          precision=precision, timeout_s=timeout_s, bcs=bcs)
         h = C.c_void_p()
         _lib.check(L.prandtl_create(C.byref(desc), C.byref(cfg), C.byref(h)), None)
         self._h = h

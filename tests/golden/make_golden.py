@@ -1,9 +1,10 @@
 """Generate golden RHS vectors from the reference's own DGSEM sources.
 
 Runs oracle/_ref/libref_*.so (the reference's DGSEMIntegrator, LiftingBR1,
-ChandrashekarFlux, NavierStokesFlux, BasicOperations, PerssonPeraireIndicator
-and ModalBasis compiled unmodified by oracle/ref_harness/build_ref.sh) on small
-seeded cases and stores inputs and outputs in reference_rhs.npz.
+ChandrashekarFlux, NavierStokesFlux, BasicOperations, PerssonPeraireIndicator,
+ModalBasis and boundary integrators compiled unmodified by
+oracle/ref_harness/build_ref.sh) on small seeded cases and stores inputs and
+outputs in reference_rhs.npz.
 
     python tests/golden/make_golden.py
 """
@@ -33,11 +34,24 @@ CASES = [
 ]
 PHYS = dict(gamma=1.4, Pr=0.71, mu=0.01, R_gas=287.05, alpha_max=0.5, alpha_min=0.001)
 
+# Euler with boundary faces: (name, dim, n, order, blending, amplitude, seed);
+# every case uses BCS, the sides of SIDES[dim] (2*dir + side -> BCS index).
+BOUNDARY_CASES = [
+    ("euler2d_bdr_n3_N3", 2, 3, 3, 0, 0.10, 11),
+    ("euler2d_bdr_blend_n3_N2", 2, 3, 2, 1, 0.30, 12),
+    ("euler3d_bdr_n2_N3", 3, 2, 3, 0, 0.10, 13),
+    ("euler3d_bdr_blend_n2_N2", 3, 2, 2, 1, 0.30, 14),
+]
+BCS = {2: [("state", [1.3, 0.5, 0.2, 2.9]), ("outflow",), ("slip_wall",), ("symmetry",), ("pressure_outflow", None, 1.4)],
+       3: [("state", [1.3, 0.5, 0.2, -0.1, 2.9]), ("outflow",), ("slip_wall",), ("symmetry",),
+           ("pressure_outflow", None, 1.4)]}
+SIDES = {2: [0, 4, 2, 3], 3: [0, 1, 2, 3, 4, 2]}
 
-def case_inputs(dim, n, order, amp, seed):
+
+def case_inputs(dim, n, order, amp, seed, bcs=None):
     rng = np.random.default_rng(100 + seed)
     A = np.eye(dim) + 0.15 * rng.uniform(-1, 1, (dim, dim))
-    mesh = periodic_box(dim, n, order, 0.0, 1.0, affine=A)
+    mesh = periodic_box(dim, n, order, 0.0, 1.0, affine=A, bcs=bcs)
     base = cases.free_stream(mesh, rho=1.2, vel=[0.4, -0.3, 0.2][:dim], p=1.5)
     return mesh, A, cases.perturbed(mesh, base, amp=amp, seed=seed)
 
@@ -54,8 +68,15 @@ def main():
         out[f"{name}/u"] = u
         out[f"{name}/dudt"] = r["dudt"]
         out[f"{name}/alpha"] = r["alpha"]
+    for name, dim, n, order, bl, amp, seed in BOUNDARY_CASES:
+        mesh, A, u = case_inputs(dim, n, order, amp, seed, bcs=SIDES[dim])
+        r = pyoracle.RefOperator(mesh, blending=bl, bcs=BCS[dim], **PHYS).rhs(u, want_alpha=True)
+        out[f"{name}/affine"] = A
+        out[f"{name}/u"] = u
+        out[f"{name}/dudt"] = r["dudt"]
+        out[f"{name}/alpha"] = r["alpha"]
     np.savez_compressed(os.path.join(HERE, "reference_rhs.npz"), **out)
-    print(f"wrote {len(CASES)} cases")
+    print(f"wrote {len(CASES) + len(BOUNDARY_CASES)} cases")
 
 
 if __name__ == "__main__":

@@ -125,3 +125,33 @@ def test_face_normals_must_match_the_metrics_in_fixed_navier_stokes(lib):
     if st == _lib.PRANDTL_OK:
         lib.prandtl_destroy(h)
 
+
+
+def test_boundary_tables_validated_before_touching_the_device(lib):
+    """Boundary faces {e1, l1, -1, bc}: a bad BC index or type is EINVAL, boundary
+    faces in the Navier-Stokes form are EUNSUPPORTED, all before device work."""
+    from prandtl_b200 import _lib
+    from prandtl_b200.mesh import periodic_box
+    from prandtl_b200.operator import make_config
+    keep = []
+    h = C.c_void_p()
+    m = periodic_box(2, 2, 2, 0.0, 1.0, bcs=[0, 0, None, None])
+    assert (m.face_elems[:, 2] == -1).sum() == 4
+    d = _desc(m, keep)
+    cfg = make_config()    # no BC table: the faces name BC 0 of none
+    assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EINVAL
+    assert b"boundary condition" in lib.prandtl_last_error(None)
+    cfg = make_config(bcs=[("outflow",)])
+    cfg._bcs[0].type = 9
+    assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EINVAL
+    assert b"unknown type" in lib.prandtl_last_error(None)
+    cfg = make_config(bcs=[("state", [0.0, 0.1, 0.0, 2.5])])
+    assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EINVAL
+    cfg = make_config(bcs=[("outflow",)], parabolic=True)
+    assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EUNSUPPORTED
+    assert b"Euler" in lib.prandtl_last_error(None)
+    cfg = make_config(bcs=[("outflow",)])
+    st = lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h))
+    assert st in (_lib.PRANDTL_ECUDA, _lib.PRANDTL_OK)
+    if st == _lib.PRANDTL_OK:
+        lib.prandtl_destroy(h)

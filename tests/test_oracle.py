@@ -202,3 +202,33 @@ def test_rk_order(oracle_mod, scheme):
     e2 = np.abs(o.step(u0, T / 8, scheme=scheme, nsteps=8) - ref).max()
     order = np.log2(e1 / e2)
     assert order > (2.6 if scheme == 0 else 3.6)
+
+
+# ---------------------------------------------------------------- boundary faces
+def _bdr_free_stream(oracle_mod, dim, kinds, vel):
+    from prandtl_b200 import cases
+    from prandtl_b200.mesh import periodic_box
+    sides = {2: [0, 1, 2, 3], 3: [0, 1, 2, 3, 4, 5]}[dim]
+    mesh = periodic_box(dim, 3, 3, 0.0, 1.0, bcs=sides)
+    u = cases.free_stream(mesh, rho=1.2, vel=vel, p=2.0)
+    nf = dim + 2
+    state = list(u.reshape(nf, -1)[:, 0])
+    bcs = [(k, state if k == "state" else None, 2.0 if k == "pressure_outflow" else None) for k in kinds]
+    return mesh, oracle_mod.Oracle(mesh, quirks=1, bcs=bcs).rhs(u)["dudt"]
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_boundary_free_stream_preserved(oracle_mod, dim):
+    """A uniform state is kept by inflow of that state, outflow and
+    pressure outflow at its pressure on every side."""
+    for kinds in (["state"] * 2 * dim, ["outflow"] * 2 * dim, ["pressure_outflow"] * 2 * dim):
+        _, d = _bdr_free_stream(oracle_mod, dim, kinds, [0.3, -0.2, 0.1][:dim])
+        assert np.abs(d).max() < 1e-12, kinds
+
+
+def test_wall_parallel_flow_preserved(oracle_mod):
+    """Flow along x between slip walls (or symmetry planes) at y = 0, 1 is
+    kept: zero normal velocity, the wall flux is the pressure flux."""
+    for wall in ("slip_wall", "symmetry"):
+        _, d = _bdr_free_stream(oracle_mod, 2, ["outflow", "outflow", wall, wall], [0.4, 0.0])
+        assert np.abs(d).max() < 1e-12, wall

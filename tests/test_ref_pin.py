@@ -14,6 +14,8 @@ import numpy as np
 import pytest
 
 from conftest import normalized_error
+from prandtl_b200 import cases
+from prandtl_b200.mesh import periodic_box
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "golden"))
@@ -87,3 +89,32 @@ def test_golden_fixtures_come_from_the_reference(oracle_mod):
         mesh, A, u = make_golden.case_inputs(dim, n, order, amp, seed)
         r = o.RefOperator(mesh, parabolic=par, blending=bl, **make_golden.PHYS).rhs(u)
         np.testing.assert_array_equal(r["dudt"], GOLDEN[f"{name}/dudt"])
+
+
+# ---------------------------------------------------------------- boundary faces
+@pytest.mark.parametrize("case", make_golden.BOUNDARY_CASES, ids=[c[0] for c in make_golden.BOUNDARY_CASES])
+def test_oracle_boundary_matches_reference_golden(oracle_mod, case):
+    """Boundary integrators (state, outflow, slip wall, symmetry, pressure
+    outflow with the reference's Q9 aliasing) against the reference's outputs."""
+    name, dim, n, order, bl, amp, seed = case
+    mesh, _, u = make_golden.case_inputs(dim, n, order, amp, seed, bcs=make_golden.SIDES[dim])
+    gold = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_rhs.npz"))
+    o = oracle_mod.Oracle(mesh, blending=bl, quirks=0, bcs=make_golden.BCS[dim], **make_golden.PHYS).rhs(u)
+    assert normalized_error(o["dudt"], gold[f"{name}/dudt"], mesh.num_fields) <= 1e-13
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("order", [1, 2, 4])
+@pytest.mark.parametrize("kind", ["state", "outflow", "slip_wall", "symmetry", "pressure_outflow"])
+def test_oracle_boundary_matches_reference_sources(oracle_mod, dim, order, kind):
+    """One boundary condition on every bounded side, oracle vs the reference's
+    boundary integrator compiled from its own sources."""
+    _ref(oracle_mod)
+    state = [1.1, 0.3, -0.2, 0.15, 2.7][: dim + 2] if dim == 3 else [1.1, 0.3, -0.2, 2.7]
+    bcs = [(kind, state if kind == "state" else None, 1.2 if kind == "pressure_outflow" else None)]
+    sides = [0, 0, 0, 0] if dim == 2 else [0, 0, None, None, 0, 0]
+    mesh = periodic_box(dim, 2, order, 0.0, 1.0, bcs=sides, affine=np.eye(dim) + 0.1 * np.eye(dim, k=1))
+    u = cases.perturbed(mesh, cases.free_stream(mesh, rho=1.1, p=2.0), amp=0.2, seed=order)
+    o = oracle_mod.Oracle(mesh, quirks=0, bcs=bcs).rhs(u)["dudt"]
+    r = oracle_mod.RefOperator(mesh, quirks=0, bcs=bcs).rhs(u)["dudt"]
+    assert normalized_error(o, r, mesh.num_fields) <= 1e-13
