@@ -75,10 +75,19 @@ typedef struct prandtl_mesh_desc {
 #define PRANDTL_BC_SLIP_WALL 2        /* SlipWall: pressure flux of the normal Riemann problem */
 #define PRANDTL_BC_SYMMETRY 3         /* Symmetry: inner state with reflected normal momentum */
 #define PRANDTL_BC_PRESSURE_OUTFLOW 4 /* SubsonicOutflowP: inner state at pressure p */
+#define PRANDTL_BC_RIEMANN 5          /* RiemannInvariant: characteristic state from the outer
+                                         primitive state (rho, V, p) in state[] */
+#define PRANDTL_BC_INFLOW_RV 6        /* SubsonicInflowRV: density state[0], velocity state[1..dim],
+                                         inner pressure */
+#define PRANDTL_BC_INFLOW_PTTT 7      /* SubsonicInflowPtTtAng: total pressure pt, total temperature
+                                         Tt, cp, flow angles theta, phi in degrees */
 typedef struct prandtl_bc {
     int type;                  /* PRANDTL_BC_* */
-    double state[5];           /* conserved outer state (PRANDTL_BC_STATE), dim+2 used */
+    double state[5];           /* STATE: conserved outer state; RIEMANN: primitive outer state;
+                                  INFLOW_RV: rho, V (dim+2 or dim+1 used) */
     double p;                  /* outflow pressure (PRANDTL_BC_PRESSURE_OUTFLOW) */
+    double pt, Tt, cp;         /* PRANDTL_BC_INFLOW_PTTT */
+    double theta, phi;         /*   flow direction (cos t, sin t) in 2D, (cos t sin f, sin t sin f, cos f) in 3D */
 } prandtl_bc;
 
 /* Physics and switches.  Defaults (prandtl_config_default) match the

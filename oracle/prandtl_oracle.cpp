@@ -584,6 +584,80 @@ double bdr_face_flux(const Ctx &X, const oracle_bc &bc, const double *s1_in, con
         s2[nf - 1] = bc.p * gammaM1Inverse + 0.5 * s1[0] * vv;
         return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
     }
+    case ORACLE_BC_RIEMANN: {   // RiemannInvariantBdrFaceIntegrator.cpp:45-116 (constant state)
+        const double gammaInverse = 1.0 / gamma;
+        const double rho_o = bc.state[0], p_o = bc.state[nf - 1];
+        double V_o[3], un[3], V_i[3];
+        const double rn = 1.0 / norml2(nor, dim);   // Normalize: vec /= Norml2
+        for (int d = 0; d < dim; ++d) { V_o[d] = bc.state[1 + d]; un[d] = nor[d] * rn; }
+        const double r1 = 1.0 / s1[0];
+        for (int d = 0; d < dim; ++d) V_i[d] = s1[1 + d] * r1;   // V_i /= state1(0)
+        double Vn_i = 0.0, Vn_o = 0.0;
+        for (int d = 0; d < dim; ++d) { Vn_i += V_i[d] * un[d]; Vn_o += V_o[d] * un[d]; }
+        // Q10: V_i wraps state1, so the trace's momentum slots hold V_i; ComputePressure
+        // then divides that wrapped range by rho once more (V_i = m / rho^2 afterwards).
+        if (X.quirks == 0) {
+            for (int d = 0; d < dim; ++d) { V_i[d] *= r1; s1[1 + d] = V_i[d]; }
+        }
+        double vv = 0.0;
+        for (int d = 0; d < dim; ++d) vv += V_i[d] * V_i[d];
+        const double p_i = gammaM1 * (s1[nf - 1] - 0.5 * s1[0] * vv);
+        const double a_o = sound_speed(p_o, rho_o, gamma), a_i = sound_speed(p_i, s1[0], gamma);
+        const double R_minus = (std::abs(Vn_o) >= a_o && Vn_i >= 0.0) ? Vn_i - 2.0 * a_i * gammaM1Inverse
+                                                                      : Vn_o - 2.0 * a_o * gammaM1Inverse;
+        const double R_plus = (std::abs(Vn_o) >= a_o && Vn_i < 0.0) ? Vn_o + 2.0 * a_o * gammaM1Inverse
+                                                                    : Vn_i + 2.0 * a_i * gammaM1Inverse;
+        const double Vn_b = 0.5 * (R_plus + R_minus), a_b = 0.25 * gammaM1 * (R_plus - R_minus);
+        const double dVn_i = Vn_b - Vn_i, dVn_o = Vn_b - Vn_o;
+        s2[0] = (Vn_i < 0.0) ? std::pow(a_b * a_b * gammaInverse * rho_o / p_o, gammaM1Inverse) * rho_o
+                             : std::pow(a_b * a_b * gammaInverse * s1[0] / p_i, gammaM1Inverse) * s1[0];
+        s2[nf - 1] = 0.0;
+        for (int d = 0; d < dim; ++d) {
+            s2[1 + d] = (Vn_i >= 0.0) ? s2[0] * (V_i[d] + dVn_i * un[d]) : s2[0] * (V_o[d] + dVn_o * un[d]);
+            s2[nf - 1] += s2[1 + d] * s2[1 + d];
+        }
+        const double p_b = a_b * a_b * s2[0] * gammaInverse;
+        s2[nf - 1] *= (0.5 / s2[0]);
+        s2[nf - 1] += p_b * gammaM1Inverse;
+        return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
+    }
+    case ORACLE_BC_INFLOW_RV: {   // SubsonicInflowRVBdrFaceIntegrator.cpp:19-49 (constant)
+        const double r = bc.state[0];
+        double dke = 0.0, uu = 0.0;
+        s2[0] = r;
+        for (int d = 0; d < dim; ++d) {
+            s2[1 + d] = r * bc.state[1 + d];
+            dke -= s1[1 + d] * s1[1 + d];
+            uu += bc.state[1 + d] * bc.state[1 + d];
+        }
+        dke *= 0.5 / s1[0];
+        dke += 0.5 * uu * r;
+        s2[nf - 1] = s1[nf - 1] + dke;
+        return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
+    }
+    case ORACLE_BC_INFLOW_PTTT: {   // SubsonicInflowPtTtAngBdrFaceIntegrator.cpp:15-79 (constant)
+        // direction: (cos t, sin t) in 2D; in 3D the reference stores cos f one past
+        // the end of its 3-vector and leaves the z component unset (Q11); cos f is used
+        double vc[3] = {std::cos(bc.theta * M_PI / 180.0), std::sin(bc.theta * M_PI / 180.0), 0.0};
+        if (dim > 2) {
+            vc[0] *= std::sin(bc.phi * M_PI / 180.0);
+            vc[1] *= std::sin(bc.phi * M_PI / 180.0);
+            vc[2] = std::cos(bc.phi * M_PI / 180.0);
+        }
+        // ComputePressure(state1) wraps state1 (quirks 0: velocity stays in its momentum slots)
+        const double r1 = 1.0 / s1[0];
+        double v[3], vv = 0.0;
+        for (int d = 0; d < dim; ++d) { v[d] = s1[1 + d] * r1; vv += v[d] * v[d]; }
+        if (X.quirks == 0)
+            for (int d = 0; d < dim; ++d) s1[1 + d] = v[d];
+        const double p = gammaM1 * (s1[nf - 1] - 0.5 * s1[0] * vv);
+        double V_sq = 2.0 * bc.cp * bc.Tt * (1.0 - std::pow(p / bc.pt, gammaM1 / gamma));
+        V_sq = std::max(0.0, V_sq);
+        s2[0] = gamma * gammaM1Inverse * p / (bc.cp * bc.Tt - 0.5 * V_sq);
+        for (int d = 0; d < dim; ++d) s2[1 + d] = s2[0] * std::sqrt(V_sq) * vc[d];
+        s2[nf - 1] = p * gammaM1Inverse + 0.5 * s2[0] * V_sq;
+        return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
+    }
     default:
         for (int f = 0; f < nf; ++f) flux[f] = 0.0;
         return 0.0;

@@ -46,12 +46,17 @@ enum {
     ORACLE_BC_OUTFLOW = 1,          /* SupersonicOutflow: outer state = inner state */
     ORACLE_BC_SLIP_WALL = 2,        /* SlipWall: pressure flux of the normal Riemann problem */
     ORACLE_BC_SYMMETRY = 3,         /* Symmetry: inner state with reflected normal momentum */
-    ORACLE_BC_PRESSURE_OUTFLOW = 4  /* SubsonicOutflowP with a constant pressure */
+    ORACLE_BC_PRESSURE_OUTFLOW = 4, /* SubsonicOutflowP with a constant pressure */
+    ORACLE_BC_RIEMANN = 5,          /* RiemannInvariant, constant outer primitive state */
+    ORACLE_BC_INFLOW_RV = 6,        /* SubsonicInflowRV, constant density and velocity */
+    ORACLE_BC_INFLOW_PTTT = 7       /* SubsonicInflowPtTtAng, constant pt, Tt, angles */
 };
 typedef struct oracle_bc {
     int type;
-    double state[5];    /* conserved outer state (ORACLE_BC_STATE) */
+    double state[5];    /* STATE: conserved outer state; RIEMANN: primitive (rho, V, p); INFLOW_RV: rho, V */
     double p;           /* outflow pressure (ORACLE_BC_PRESSURE_OUTFLOW) */
+    double pt, Tt, cp;  /* ORACLE_BC_INFLOW_PTTT */
+    double theta, phi;  /*   flow angles in degrees */
 } oracle_bc;
 
 typedef struct oracle_config {

@@ -29,6 +29,9 @@ FILES="$SRC/BasicOperations/BasicOperations.cpp $SRC/RiemannSolvers/Chandrasheka
  $SRC/Integrators/BoundaryConditions/SlipWallBdrFaceIntegrator.cpp \
  $SRC/Integrators/BoundaryConditions/SymmetryBdrFaceIntegrator.cpp \
  $SRC/Integrators/BoundaryConditions/SubsonicOutflowPBdrFaceIntegrator.cpp \
+ $SRC/Integrators/BoundaryConditions/RiemannInvariantBdrFaceIntegrator.cpp \
+ $SRC/Integrators/BoundaryConditions/SubsonicInflowRVBdrFaceIntegrator.cpp \
+ $SRC/Integrators/BoundaryConditions/SubsonicInflowPtTtAngBdrFaceIntegrator.cpp \
  $HERE/ref_driver.cpp"
 # -O2 -DNDEBUG as the reference's Release configuration (configure.sh)
 FLAGS="-O2 -DNDEBUG -std=c++17 -fPIC -shared -w"

@@ -34,6 +34,9 @@
 #include "SubsonicOutflowPBdrFaceIntegrator.hpp"
 #include "SupersonicOutflowBdrFaceIntegrator.hpp"
 #include "SymmetryBdrFaceIntegrator.hpp"
+#include "RiemannInvariantBdrFaceIntegrator.hpp"
+#include "SubsonicInflowRVBdrFaceIntegrator.hpp"
+#include "SubsonicInflowPtTtAngBdrFaceIntegrator.hpp"
 #include "prandtl_oracle.h"
 
 namespace mfem {
@@ -407,6 +410,25 @@ extern "C" int ref_rhs(const oracle_mesh *md, const oracle_config *cfg, const do
                 break;
             case ORACLE_BC_PRESSURE_OUTFLOW:
                 bdr.emplace_back(new SubsonicOutflowPBdrFaceIntegrator(lifting, rsolver, Np, time, pc.gamma, b.p));
+                break;
+            case ORACLE_BC_RIEMANN: {
+                Vector prim(nf);
+                for (int f = 0; f < nf; ++f) prim(f) = b.state[f];
+                bdr.emplace_back(new RiemannInvariantBdrFaceIntegrator(lifting, rsolver, Np, time, pc.gamma, prim));
+                break;
+            }
+            case ORACLE_BC_INFLOW_RV: {
+                Vector V(dim);
+                for (int d = 0; d < dim; ++d) V(d) = b.state[1 + d];
+                bdr.emplace_back(new SubsonicInflowRVBdrFaceIntegrator(lifting, rsolver, Np, time, pc.gamma,
+                                                                       b.state[0], V));
+                break;
+            }
+            case ORACLE_BC_INFLOW_PTTT:
+                // the 3D constructor writes one past the end of its direction vector
+                if (dim > 2) throw std::runtime_error("SubsonicInflowPtTtAng is not constructed in 3D");
+                bdr.emplace_back(new SubsonicInflowPtTtAngBdrFaceIntegrator(lifting, rsolver, Np, time, pc.gamma, b.cp,
+                                                                            b.pt, b.Tt, b.theta, b.phi));
                 break;
             default:
                 throw std::runtime_error("unknown boundary condition");

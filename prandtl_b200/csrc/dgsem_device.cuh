@@ -27,11 +27,18 @@ struct PhysParams {
 };
 
 // A boundary condition (the layout of prandtl_bc).
-enum BcType : int { BC_STATE = 0, BC_OUTFLOW = 1, BC_SLIP_WALL = 2, BC_SYMMETRY = 3, BC_PRESSURE_OUTFLOW = 4 };
+// INFLOW_PTTT keeps pt, Tt, cp and the unit flow direction vc (formed on the
+// host from theta, phi).
+enum BcType : int {
+    BC_STATE = 0, BC_OUTFLOW = 1, BC_SLIP_WALL = 2, BC_SYMMETRY = 3, BC_PRESSURE_OUTFLOW = 4,
+    BC_RIEMANN = 5, BC_INFLOW_RV = 6, BC_INFLOW_PTTT = 7
+};
 struct BcDev {
     int type, pad;
     double state[5];
     double p;
+    double pt, Tt, cp;
+    double vc[3];
 };
 
 // 1D operator tables for one polynomial order (NP <= 8), row-major [i][l].

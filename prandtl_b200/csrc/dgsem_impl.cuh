@@ -489,6 +489,75 @@ __device__ __forceinline__ void boundary_flux(const BcDev &bc, const double *s_i
 #pragma unroll
         for (int f = 0; f < NF; ++f) s2[f] = s1[f];
         s2[NF - 1] = bc.p * gm1i + 0.5 * s1[0] * vv;
+    } else if (bc.type == BC_RIEMANN) {   // RiemannInvariantBdrFaceIntegrator.cpp:45-116
+        const double rn = 1.0 / nn, r1 = 1.0 / s1[0], gi = 1.0 / gamma;
+        const double rho_o = bc.state[0], p_o = bc.state[NF - 1];
+        double un[DIM], vi[DIM], vn_i = 0.0, vn_o = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            un[d] = nor[d] * rn;
+            vi[d] = s1[1 + d] * r1;
+            vn_i += vi[d] * un[d];
+            vn_o += bc.state[1 + d] * un[d];
+        }
+        // quirks == 0 (Q10): the inner velocity wraps the trace and the pressure
+        // helper divides it once more, so the trace and vi end as m / rho^2
+        double vv = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            if (P.quirks == 0) {
+                vi[d] *= r1;
+                s1[1 + d] = vi[d];
+            }
+            vv += vi[d] * vi[d];
+        }
+        const double p_i = gm1 * (s1[NF - 1] - 0.5 * s1[0] * vv);
+        const double a_o = sqrt(gamma * p_o / rho_o), a_i = sqrt(gamma * p_i / s1[0]);
+        const bool sup = fabs(vn_o) >= a_o;
+        const double r_minus = (sup && vn_i >= 0.0) ? vn_i - 2.0 * a_i * gm1i : vn_o - 2.0 * a_o * gm1i;
+        const double r_plus = (sup && vn_i < 0.0) ? vn_o + 2.0 * a_o * gm1i : vn_i + 2.0 * a_i * gm1i;
+        const double vn_b = 0.5 * (r_plus + r_minus), a_b = 0.25 * gm1 * (r_plus - r_minus);
+        s2[0] = vn_i < 0.0 ? pow(a_b * a_b * gi * rho_o / p_o, gm1i) * rho_o
+                           : pow(a_b * a_b * gi * s1[0] / p_i, gm1i) * s1[0];
+        double ke = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            s2[1 + d] = vn_i >= 0.0 ? s2[0] * (vi[d] + (vn_b - vn_i) * un[d])
+                                    : s2[0] * (bc.state[1 + d] + (vn_b - vn_o) * un[d]);
+            ke += s2[1 + d] * s2[1 + d];
+        }
+        s2[NF - 1] = ke * (0.5 / s2[0]) + a_b * a_b * s2[0] * gi * gm1i;
+    } else if (bc.type == BC_INFLOW_RV) {   // SubsonicInflowRVBdrFaceIntegrator.cpp:19-49
+        const double r = bc.state[0];
+        double dke = 0.0, uu = 0.0;
+        s2[0] = r;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            s2[1 + d] = r * bc.state[1 + d];
+            dke -= s1[1 + d] * s1[1 + d];
+            uu += bc.state[1 + d] * bc.state[1 + d];
+        }
+        dke *= 0.5 / s1[0];
+        dke += 0.5 * uu * r;
+        s2[NF - 1] = s1[NF - 1] + dke;
+    } else if (bc.type == BC_INFLOW_PTTT) {   // SubsonicInflowPtTtAngBdrFaceIntegrator.cpp:55-79
+        // quirks == 0: the pressure helper leaves velocity in the trace's momentum slots
+        const double r1 = 1.0 / s1[0];
+        double vv = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            const double v = s1[1 + d] * r1;
+            if (P.quirks == 0) s1[1 + d] = v;
+            vv += v * v;
+        }
+        const double p = gm1 * (s1[NF - 1] - 0.5 * s1[0] * vv);
+        double v_sq = 2.0 * bc.cp * bc.Tt * (1.0 - pow(p / bc.pt, gm1 / gamma));
+        v_sq = fmax(0.0, v_sq);
+        s2[0] = gamma * gm1i * p / (bc.cp * bc.Tt - 0.5 * v_sq);
+        const double sv = sqrt(v_sq);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) s2[1 + d] = s2[0] * sv * bc.vc[d];
+        s2[NF - 1] = p * gm1i + 0.5 * s2[0] * v_sq;
     } else {   // BC_OUTFLOW, SupersonicOutflowBdrFaceIntegrator.cpp:11-14
 #pragma unroll
         for (int f = 0; f < NF; ++f) s2[f] = s1[f];

@@ -200,28 +200,59 @@ inline bool has_boundary(const prandtl_mesh_desc *md) {
 }
 
 // Device copy of the boundary conditions (BcDev has prandtl_bc's layout).
-inline std::vector<BcDev> device_bcs(const prandtl_config *cfg) {
-    static_assert(sizeof(BcDev) == sizeof(prandtl_bc), "BcDev mirrors prandtl_bc");
+// Flow direction of SubsonicInflowPtTtAng (SubsonicInflowPtTtAngBdrFaceIntegrator.cpp
+// constructors): (cos t, sin t) in 2D, (cos t sin f, sin t sin f, cos f) in 3D,
+// angles in degrees.  The reference's 3D constructor stores cos f one slot past
+// its dim-sized vector and leaves the z component unset; the intended value is
+// used in both modes.
+inline void inflow_direction(int dim, double theta, double phi, double vc[3]) {
+    vc[0] = vc[1] = vc[2] = 0.0;
+    vc[0] = std::cos(theta * M_PI / 180.0);
+    vc[1] = std::sin(theta * M_PI / 180.0);
+    if (dim > 2) {
+        vc[0] *= std::sin(phi * M_PI / 180.0);
+        vc[1] *= std::sin(phi * M_PI / 180.0);
+        vc[2] = std::cos(phi * M_PI / 180.0);
+    }
+}
+
+inline std::vector<BcDev> device_bcs(const prandtl_config *cfg, int dim) {
     std::vector<BcDev> out((size_t)(cfg->num_bcs > 0 && cfg->bcs ? cfg->num_bcs : 0));
     for (size_t k = 0; k < out.size(); ++k) {
-        out[k].type = cfg->bcs[k].type;
-        out[k].pad = 0;
-        for (int f = 0; f < 5; ++f) out[k].state[f] = cfg->bcs[k].state[f];
-        out[k].p = cfg->bcs[k].p;
+        const prandtl_bc &b = cfg->bcs[k];
+        BcDev &o = out[k];
+        o.type = b.type;
+        o.pad = 0;
+        for (int f = 0; f < 5; ++f) o.state[f] = b.state[f];
+        o.p = b.p;
+        o.pt = b.pt;
+        o.Tt = b.Tt;
+        o.cp = b.cp;
+        inflow_direction(dim, b.theta, b.phi, o.vc);
     }
     return out;
 }
 
-inline prandtl_status check_bcs(const prandtl_config *cfg, std::string &msg) {
+inline prandtl_status check_bcs(const prandtl_config *cfg, int dim, std::string &msg) {
     if (cfg->num_bcs < 0 || (cfg->num_bcs > 0 && !cfg->bcs)) { msg = "bad boundary-condition table"; return PRANDTL_EINVAL; }
     for (int k = 0; k < cfg->num_bcs; ++k) {
         const prandtl_bc &b = cfg->bcs[k];
-        if (b.type < PRANDTL_BC_STATE || b.type > PRANDTL_BC_PRESSURE_OUTFLOW) {
-            msg = "boundary condition " + std::to_string(k) + ": unknown type";
+        const std::string tag = "boundary condition " + std::to_string(k);
+        if (b.type < PRANDTL_BC_STATE || b.type > PRANDTL_BC_INFLOW_PTTT) {
+            msg = tag + ": unknown type";
             return PRANDTL_EINVAL;
         }
-        if (b.type == PRANDTL_BC_STATE && !(b.state[0] > 0.0)) {
-            msg = "boundary condition " + std::to_string(k) + ": outer density must be positive";
+        if ((b.type == PRANDTL_BC_STATE || b.type == PRANDTL_BC_RIEMANN || b.type == PRANDTL_BC_INFLOW_RV) &&
+            !(b.state[0] > 0.0)) {
+            msg = tag + ": outer density must be positive";
+            return PRANDTL_EINVAL;
+        }
+        if (b.type == PRANDTL_BC_RIEMANN && !(b.state[dim == 3 ? 4 : 3] > 0.0)) {
+            msg = tag + ": outer pressure must be positive";
+            return PRANDTL_EINVAL;
+        }
+        if (b.type == PRANDTL_BC_INFLOW_PTTT && !(b.pt > 0.0 && b.Tt > 0.0 && b.cp > 0.0)) {
+            msg = tag + ": pt, Tt and cp must be positive";
             return PRANDTL_EINVAL;
         }
     }

@@ -202,7 +202,7 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
     std::vector<int4> nbr;
     {
         std::string msg;
-        prandtl_status vst = check_bcs(cfg, msg);
+        prandtl_status vst = check_bcs(cfg, md->dim, msg);
         if (vst == PRANDTL_OK) vst = validate_mesh(md, nbr, msg, cfg->num_bcs);
         if (vst == PRANDTL_OK && cfg->parabolic && has_boundary(md)) {
             msg = "boundary faces are supported for Euler (parabolic = 0)";
@@ -261,7 +261,7 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
         return bail(st);
     if ((st = dalloc(h, &h->d_alpha, (size_t)E, "alpha")) != PRANDTL_OK) return bail(st);
     if ((st = dalloc(h, &h->d_lambda, 1, "lambda")) != PRANDTL_OK) return bail(st);
-    const std::vector<BcDev> bcs = device_bcs(cfg);
+    const std::vector<BcDev> bcs = device_bcs(cfg, md->dim);
     if (!bcs.empty()) {
         if ((st = dalloc(h, &h->d_bcs, bcs.size(), "boundary conditions")) != PRANDTL_OK) return bail(st);
         if ((ce = cudaMemcpy(h->d_bcs, bcs.data(), bcs.size() * sizeof(BcDev), cudaMemcpyHostToDevice)) != cudaSuccess)

@@ -470,7 +470,7 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, 
     b->err.clear();
     std::vector<int4> nbr;
     std::string msg;
-    prandtl_status st = check_bcs(cfg, msg);
+    prandtl_status st = check_bcs(cfg, md->dim, msg);
     if (st == PRANDTL_OK) st = validate_mesh(md, nbr, msg, cfg->num_bcs);
     if (st == PRANDTL_OK && cfg->parabolic && has_boundary(md)) {
         msg = "boundary faces are supported for Euler (parabolic = 0)";
@@ -522,7 +522,7 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, 
                              b->stream)) != cudaSuccess ||
         (blend && (e = cudaMemsetAsync(base + L.alpha, 0, (size_t)E * sizeof(double), b->stream)) != cudaSuccess))
         return undo(bcuda(b, e, "upload solve"));
-    const std::vector<BcDev> bcs = device_bcs(cfg);
+    const std::vector<BcDev> bcs = device_bcs(cfg, md->dim);
     if (!bcs.empty() && (e = cudaMemcpyAsync(base + L.bcs, bcs.data(), bcs.size() * sizeof(BcDev),
                                              cudaMemcpyHostToDevice, b->stream)) != cudaSuccess)
         return undo(bcuda(b, e, "upload boundary conditions"));

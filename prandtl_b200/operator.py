@@ -54,15 +54,21 @@ class MeshArrays:
 
 def make_bcs(bcs):
     """ctypes array of prandtl_bc from [(type name, state or None, p or None), ...]:
-    type names "state", "outflow", "slip_wall", "symmetry", "pressure_outflow"."""
+    type names "state", "outflow", "slip_wall", "symmetry", "pressure_outflow",
+    "riemann" (state = outer primitive state), "inflow_rv" (state = rho, V) and
+    "inflow_pttt" (second item a dict of pt, Tt, cp, theta, phi)."""
     if not bcs:
         return None
     arr = (_lib.BC * len(bcs))()
     for k, b in enumerate(bcs):
         kind, state, p = (tuple(b) + (None, None))[:3]
         arr[k].type = _lib.BC_TYPES[kind]
-        for f, v in enumerate(state if state is not None else []):
-            arr[k].state[f] = float(v)
+        if isinstance(state, dict):   # inflow_pttt: pt, Tt, cp, theta, phi
+            for name, v in state.items():
+                setattr(arr[k], name, float(v))
+        else:
+            for f, v in enumerate(state if state is not None else []):
+                arr[k].state[f] = float(v)
         arr[k].p = float(p) if p is not None else 0.0
     return arr
 

@@ -47,6 +47,35 @@ BCS = {2: [("state", [1.3, 0.5, 0.2, 2.9]), ("outflow",), ("slip_wall",), ("symm
            ("pressure_outflow", None, 1.4)]}
 SIDES = {2: [0, 4, 2, 3], 3: [0, 1, 2, 3, 4, 2]}
 
+# Characteristic and subsonic-inflow conditions, same case format (CHAR_BCS on
+# the sides CHAR_SIDES).  The reference's SubsonicInflowPtTtAng constructor
+# writes past its direction vector in 3D, so 3D cases leave it out.
+PTTT = ("inflow_pttt", dict(pt=1.7, Tt=1.3, cp=3.5, theta=20.0, phi=70.0))
+CHAR_CASES = [
+    ("euler2d_char_n3_N3", 2, 3, 3, 0, 0.10, 21),
+    ("euler2d_char_blend_n2_N4", 2, 2, 4, 1, 0.30, 22),
+    ("euler3d_char_n2_N2", 3, 2, 2, 0, 0.10, 23),
+    ("euler3d_char_blend_n2_N3", 3, 2, 3, 1, 0.30, 24),
+]
+CHAR_BCS = {2: [("riemann", [1.25, 0.35, -0.1, 1.6]), ("inflow_rv", [1.15, 0.45, -0.25]), PTTT,
+                ("riemann", [1.2, 1.8, 0.1, 1.5]), ("outflow",)],
+            3: [("riemann", [1.25, 0.35, -0.1, 0.05, 1.6]), ("inflow_rv", [1.15, 0.45, -0.25, 0.15]),
+                ("riemann", [1.2, 1.8, 0.1, 0.0, 1.5]), ("outflow",)]}
+CHAR_SIDES = {2: [1, 0, 2, 3], 3: [1, 0, 2, 3, 0, 2]}
+BC_SETS = {"walls": (BOUNDARY_CASES, BCS, SIDES), "char": (CHAR_CASES, CHAR_BCS, CHAR_SIDES)}
+
+
+def bc_example(kind, dim):
+    """One condition of the given type with constant data for a dim-D case;
+    "riemann_supersonic" is the Riemann condition with a supersonic outer state."""
+    if kind == "riemann_supersonic":
+        return CHAR_BCS[dim][2 if dim == 3 else 3]
+    for bcs in (BCS[dim], CHAR_BCS[dim], [PTTT]):
+        for b in bcs:
+            if b[0] == kind:
+                return b
+    raise KeyError(kind)
+
 
 def case_inputs(dim, n, order, amp, seed, bcs=None):
     rng = np.random.default_rng(100 + seed)
@@ -68,15 +97,16 @@ def main():
         out[f"{name}/u"] = u
         out[f"{name}/dudt"] = r["dudt"]
         out[f"{name}/alpha"] = r["alpha"]
-    for name, dim, n, order, bl, amp, seed in BOUNDARY_CASES:
-        mesh, A, u = case_inputs(dim, n, order, amp, seed, bcs=SIDES[dim])
-        r = pyoracle.RefOperator(mesh, blending=bl, bcs=BCS[dim], **PHYS).rhs(u, want_alpha=True)
-        out[f"{name}/affine"] = A
-        out[f"{name}/u"] = u
-        out[f"{name}/dudt"] = r["dudt"]
-        out[f"{name}/alpha"] = r["alpha"]
+    for bcases, bcs, sides in BC_SETS.values():
+        for name, dim, n, order, bl, amp, seed in bcases:
+            mesh, A, u = case_inputs(dim, n, order, amp, seed, bcs=sides[dim])
+            r = pyoracle.RefOperator(mesh, blending=bl, bcs=bcs[dim], **PHYS).rhs(u, want_alpha=True)
+            out[f"{name}/affine"] = A
+            out[f"{name}/u"] = u
+            out[f"{name}/dudt"] = r["dudt"]
+            out[f"{name}/alpha"] = r["alpha"]
     np.savez_compressed(os.path.join(HERE, "reference_rhs.npz"), **out)
-    print(f"wrote {len(CASES) + len(BOUNDARY_CASES)} cases")
+    print(f"wrote {len(CASES) + len(BOUNDARY_CASES) + len(CHAR_CASES)} cases")
 
 
 if __name__ == "__main__":

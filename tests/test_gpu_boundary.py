@@ -42,28 +42,35 @@ def _affine(dim, seed=1):
 
 def test_boundary_rhs_matches_reference_golden():
     gold = np.load(os.path.join(HERE, "golden", "reference_rhs.npz"))
-    for name, dim, n, order, bl, amp, seed in make_golden.BOUNDARY_CASES:
-        mesh, A, u = make_golden.case_inputs(dim, n, order, amp, seed, bcs=SIDES[dim])
-        op = _op(mesh, blending=bool(bl), quirks="reference", bcs=BCS[dim], **make_golden.PHYS)
-        d = np.empty_like(u)
-        op.Mult(u, d)
-        err = normalized_error(d, gold[f"{name}/dudt"], mesh.num_fields)
-        assert err <= RHS_TOL, f"{name}: {err:.3e}"
-        np.testing.assert_allclose(op.alpha(), gold[f"{name}/alpha"], rtol=0, atol=1e-12)
-        op.close()
+    for bcases, bcs, sides in make_golden.BC_SETS.values():
+        for name, dim, n, order, bl, amp, seed in bcases:
+            mesh, A, u = make_golden.case_inputs(dim, n, order, amp, seed, bcs=sides[dim])
+            op = _op(mesh, blending=bool(bl), quirks="reference", bcs=bcs[dim], **make_golden.PHYS)
+            d = np.empty_like(u)
+            op.Mult(u, d)
+            err = normalized_error(d, gold[f"{name}/dudt"], mesh.num_fields)
+            assert err <= RHS_TOL, f"{name}: {err:.3e}"
+            np.testing.assert_allclose(op.alpha(), gold[f"{name}/alpha"], rtol=0, atol=1e-12)
+            op.close()
 
 
 @pytest.mark.parametrize("dim,n,order", [(2, 3, 1), (2, 3, 2), (2, 2, 3), (2, 2, 4), (2, 2, 5),
                                          (3, 2, 1), (3, 2, 2), (3, 2, 3), (3, 2, 4), (3, 1, 5)])
 @pytest.mark.parametrize("blending", [0, 1])
 @pytest.mark.parametrize("quirks", ["reference", "fixed"])
-def test_boundary_rhs_matches_oracle(oracle_mod, dim, n, order, blending, quirks):
-    mesh = periodic_box(dim, n, order, 0.0, 1.0, affine=_affine(dim, order), bcs=SIDES[dim])
+@pytest.mark.parametrize("bset", ["walls", "char"])
+def test_boundary_rhs_matches_oracle(oracle_mod, dim, n, order, blending, quirks, bset):
+    _, bcs, sides = make_golden.BC_SETS[bset]
+    bcs = bcs[dim] + ([make_golden.PTTT] if dim == 3 and bset == "char" else [])
+    sides = list(sides[dim])
+    if dim == 3 and bset == "char":
+        sides[3] = len(bcs) - 1   # 3D inflow_pttt (direction cos f, checked against the oracle only)
+    mesh = periodic_box(dim, n, order, 0.0, 1.0, affine=_affine(dim, order), bcs=sides)
     base = cases.free_stream(mesh, rho=1.2, vel=[0.4, -0.3, 0.2][:dim], p=1.5)
     u = cases.perturbed(mesh, base, amp=0.3 if blending else 0.1, seed=order + 7 * dim)
     q = 0 if quirks == "reference" else 1
-    ref = oracle_mod.Oracle(mesh, quirks=q, blending=blending, bcs=BCS[dim]).rhs(u, want_alpha=True)
-    op = _op(mesh, quirks=quirks, blending=bool(blending), bcs=BCS[dim])
+    ref = oracle_mod.Oracle(mesh, quirks=q, blending=blending, bcs=bcs).rhs(u, want_alpha=True)
+    op = _op(mesh, quirks=quirks, blending=bool(blending), bcs=bcs)
     d = np.empty_like(u)
     op.Mult(u, d)
     err = normalized_error(d, ref["dudt"], mesh.num_fields)
@@ -74,14 +81,15 @@ def test_boundary_rhs_matches_oracle(oracle_mod, dim, n, order, blending, quirks
     op.close()
 
 
-@pytest.mark.parametrize("kind", ["state", "outflow", "slip_wall", "symmetry", "pressure_outflow"])
+@pytest.mark.parametrize("kind", ["state", "outflow", "slip_wall", "symmetry", "pressure_outflow", "riemann",
+                                  "riemann_supersonic", "inflow_rv", "inflow_pttt"])
 def test_each_boundary_type_alone(oracle_mod, kind):
     """Every side carries the same BC type (one type per run isolates each flux)."""
     for dim in (2, 3):
         mesh = periodic_box(dim, 2, 3, 0.0, 1.0, affine=_affine(dim, 3), bcs=[0] * (2 * dim))
         base = cases.free_stream(mesh, rho=1.1, vel=[0.3, 0.2, -0.1][:dim], p=2.0)
         u = cases.perturbed(mesh, base, amp=0.2, seed=dim)
-        bc = [b for b in BCS[dim] if b[0] == kind]
+        bc = [make_golden.bc_example(kind, dim)]
         for q in (0, 1):
             ref = oracle_mod.Oracle(mesh, quirks=q, bcs=bc).rhs(u)
             op = _op(mesh, quirks=q and "fixed" or "reference", bcs=bc)
@@ -92,16 +100,19 @@ def test_each_boundary_type_alone(oracle_mod, kind):
 
 
 def test_boundary_free_stream_preserved_gpu():
-    """A uniform state is kept by inflow of that state, outflow and pressure
-    outflow at its pressure; flow along x is kept between slip walls and
-    between symmetry planes."""
+    """A uniform state is kept by inflow of that state, outflow, pressure
+    outflow at its pressure, Riemann invariants of that state and subsonic
+    inflow of its density and velocity; flow along x is kept between slip walls
+    and between symmetry planes."""
     for dim in (2, 3):
         vel = [0.3, -0.2, 0.1][:dim]
         mesh = periodic_box(dim, 3, 3, 0.0, 1.0, bcs=list(range(2 * dim)))
         u = cases.free_stream(mesh, rho=1.2, vel=vel, p=2.0)
         state = list(u.reshape(dim + 2, -1)[:, 0])
-        for kind in ("state", "outflow", "pressure_outflow"):
-            bc = [(kind, state if kind == "state" else None, 2.0 if kind == "pressure_outflow" else None)]
+        prim = [1.2] + vel + [2.0]
+        for kind in ("state", "outflow", "pressure_outflow", "riemann", "inflow_rv"):
+            data = {"state": state, "riemann": prim, "inflow_rv": prim[:-1]}.get(kind)
+            bc = [(kind, data, 2.0 if kind == "pressure_outflow" else None)]
             op = _op(mesh, quirks="fixed", bcs=bc * (2 * dim))
             d = np.empty_like(u)
             op.Mult(u, d)

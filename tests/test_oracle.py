@@ -213,17 +213,20 @@ def _bdr_free_stream(oracle_mod, dim, kinds, vel):
     u = cases.free_stream(mesh, rho=1.2, vel=vel, p=2.0)
     nf = dim + 2
     state = list(u.reshape(nf, -1)[:, 0])
-    bcs = [(k, state if k == "state" else None, 2.0 if k == "pressure_outflow" else None) for k in kinds]
+    prim = [1.2] + list(vel) + [2.0]
+    data = {"state": state, "riemann": prim, "inflow_rv": prim[:-1]}
+    bcs = [(k, data.get(k), 2.0 if k == "pressure_outflow" else None) for k in kinds]
     return mesh, oracle_mod.Oracle(mesh, quirks=1, bcs=bcs).rhs(u)["dudt"]
 
 
 @pytest.mark.parametrize("dim", [2, 3])
 def test_boundary_free_stream_preserved(oracle_mod, dim):
-    """A uniform state is kept by inflow of that state, outflow and
-    pressure outflow at its pressure on every side."""
-    for kinds in (["state"] * 2 * dim, ["outflow"] * 2 * dim, ["pressure_outflow"] * 2 * dim):
-        _, d = _bdr_free_stream(oracle_mod, dim, kinds, [0.3, -0.2, 0.1][:dim])
-        assert np.abs(d).max() < 1e-12, kinds
+    """A uniform state is kept by inflow of that state, outflow, pressure
+    outflow at its pressure, Riemann invariants of that state and subsonic
+    inflow of its density and velocity on every side."""
+    for k in ("state", "outflow", "pressure_outflow", "riemann", "inflow_rv"):
+        _, d = _bdr_free_stream(oracle_mod, dim, [k] * 2 * dim, [0.3, -0.2, 0.1][:dim])
+        assert np.abs(d).max() < 1e-12, k
 
 
 def test_wall_parallel_flow_preserved(oracle_mod):
