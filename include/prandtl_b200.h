@@ -81,6 +81,13 @@ typedef struct prandtl_mesh_desc {
                                          inner pressure */
 #define PRANDTL_BC_INFLOW_PTTT 7      /* SubsonicInflowPtTtAng: total pressure pt, total temperature
                                          Tt, cp, flow angles theta, phi in degrees */
+#define PRANDTL_BC_NOSLIP_ADIABATIC 8 /* NoSlipAdiabWall: wall velocity, normal heat flux */
+#define PRANDTL_BC_NOSLIP_ISOTHERMAL 9 /* NoSlipIsothWall: wall velocity, wall temperature */
+/* With parabolic = 1 every type but SLIP_WALL, SYMMETRY and INFLOW_PTTT is
+ * accepted (the reference defines no viscous treatment for the first two), and
+ * RIEMANN only with quirks = 1 (the reference's Riemann lifting reads a face
+ * normal that is never set for it); in the Euler form the no-slip walls act as
+ * slip walls, as in the reference. */
 typedef struct prandtl_bc {
     int type;                  /* PRANDTL_BC_* */
     double state[5];           /* STATE: conserved outer state; RIEMANN: primitive outer state;
@@ -88,6 +95,9 @@ typedef struct prandtl_bc {
     double p;                  /* outflow pressure (PRANDTL_BC_PRESSURE_OUTFLOW) */
     double pt, Tt, cp;         /* PRANDTL_BC_INFLOW_PTTT */
     double theta, phi;         /*   flow direction (cos t, sin t) in 2D, (cos t sin f, sin t sin f, cos f) in 3D */
+    double wall_vel[3];        /* NOSLIP_*: wall velocity (dim used) */
+    double heat_flux;          /* NOSLIP_ADIABATIC: normal heat flux per unit face area */
+    double wall_T;             /* NOSLIP_ISOTHERMAL: wall temperature (with the config's R_gas) */
 } prandtl_bc;
 
 /* Physics and switches.  Defaults (prandtl_config_default) match the

@@ -515,74 +515,44 @@ void setup(Ctx &X, const oracle_mesh *m, const oracle_config *c) {
 
 inline int node_id(const Ctx &X, int i, int j, int k) { return k * X.ny() * X.nx() + j * X.nx() + i; }
 
-// Boundary-face flux of trace s1 (BdrFaceIntegrator.cpp:61-138 with the
-// integrators of src/Integrators/BoundaryConditions/).  The element receives
-// -flux / (w0 J1) at the face node.  Returns the largest |V|+c seen.
-double bdr_face_flux(const Ctx &X, const oracle_bc &bc, const double *s1_in, const double *nor, double *flux) {
+// Outer state s2 of a boundary condition whose flux is the surface flux of
+// (s1, s2) (ComputeOuterInviscidState of src/Integrators/BoundaryConditions/,
+// constant data).  s1 takes the reference-mode aliasing the integrator applies
+// to its inner trace.  Not for the wall types, which have their own flux.
+void bdr_outer_state(const Ctx &X, const oracle_bc &bc, double *s1, const double *nor, double *s2) {
     const int dim = X.dim, nf = dim + 2;
     const double gamma = X.P.gamma, gammaM1 = X.P.gammaM1, gammaM1Inverse = X.P.gammaM1Inverse;
-    double s1[5] = {0, 0, 0, 0, 0}, s2[5] = {0, 0, 0, 0, 0};
-    for (int f = 0; f < nf; ++f) s1[f] = s1_in[f];
     switch (bc.type) {
     case ORACLE_BC_STATE:   // SpecifiedStateBdrFaceIntegrator.cpp:24-36 (constant)
         for (int f = 0; f < nf; ++f) s2[f] = bc.state[f];
-        return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
+        return;
     case ORACLE_BC_OUTFLOW:   // SupersonicOutflowBdrFaceIntegrator.cpp:11-14
         for (int f = 0; f < nf; ++f) s2[f] = s1[f];
-        return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
-    case ORACLE_BC_SYMMETRY: {   // SymmetryBdrFaceIntegrator.cpp:11-32
-        const double nn = norml2(nor, dim);
-        if (nn == 0.0) {
-            for (int f = 0; f < nf; ++f) flux[f] = 0.0;
-            return 0.0;
-        }
-        const double rn = 1.0 / nn;
+        return;
+    case ORACLE_BC_SYMMETRY: {   // SymmetryBdrFaceIntegrator.cpp:11-32 (|nor| > 0)
+        const double rn = 1.0 / norml2(nor, dim);
         double un[3], mn = 0.0;
         for (int d = 0; d < dim; ++d) un[d] = nor[d] * rn;
         for (int f = 0; f < nf; ++f) s2[f] = s1[f];
         for (int d = 0; d < dim; ++d) mn += s2[1 + d] * un[d];
         for (int d = 0; d < dim; ++d) s2[1 + d] += -2.0 * mn * un[d];
-        return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
-    }
-    case ORACLE_BC_SLIP_WALL: {   // SlipWallBdrFaceIntegrator.cpp:16-59
-        const double nn = norml2(nor, dim), rn = 1.0 / nn;
-        const double gammaP1 = 1.0 + gamma, gammaP1Inverse = 1.0 / gammaP1;
-        const double rho = s1[0];
-        double mn = 0.0, vv = 0.0;
-        for (int d = 0; d < dim; ++d) {
-            mn += s1[1 + d] * (nor[d] * rn);
-            const double v = s1[1 + d] / rho;
-            vv += v * v;
-        }
-        const double u = mn / rho;   // normal velocity in the rotated frame
-        const double p = gammaM1 * (s1[nf - 1] - 0.5 * rho * vv);
-        const double an = sound_speed(p, rho, gamma);
-        double p_star;
-        if (u > 0.0)
-            p_star = p + 0.25 * u * gammaP1 * rho *
-                             (u + std::sqrt(u * u + 8.0 * gammaP1Inverse / rho * p * (gammaM1 * gammaP1Inverse + 1.0)));
-        else
-            p_star = p * std::pow(std::max(1.0 + 0.5 * gammaM1 * u / an, 0.0001), 2.0 * gamma * gammaM1Inverse);
-        for (int f = 0; f < nf; ++f) flux[f] = 0.0;
-        for (int d = 0; d < dim; ++d) flux[1 + d] = p_star * nor[d];
-        return std::sqrt(vv) + an;
+        return;
     }
     case ORACLE_BC_PRESSURE_OUTFLOW: {   // SubsonicOutflowPBdrFaceIntegrator.cpp:17-29
         // Q9: `Vector vel(state1.GetData() + 1, dim); vel /= state1(0);` wraps the
         // inner trace, so (reference) both traces carry velocity in the momentum slots
         double vel[3], vv = 0.0;
+        const double r = 1.0 / s1[0];
         if (X.quirks == 0) {
-            const double r = 1.0 / s1[0];
             for (int d = 0; d < dim; ++d) s1[1 + d] *= r;
             for (int d = 0; d < dim; ++d) vel[d] = s1[1 + d];
         } else {
-            const double r = 1.0 / s1[0];
             for (int d = 0; d < dim; ++d) vel[d] = s1[1 + d] * r;
         }
         for (int d = 0; d < dim; ++d) vv += vel[d] * vel[d];
         for (int f = 0; f < nf; ++f) s2[f] = s1[f];
         s2[nf - 1] = bc.p * gammaM1Inverse + 0.5 * s1[0] * vv;
-        return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
+        return;
     }
     case ORACLE_BC_RIEMANN: {   // RiemannInvariantBdrFaceIntegrator.cpp:45-116 (constant state)
         const double gammaInverse = 1.0 / gamma;
@@ -619,7 +589,7 @@ double bdr_face_flux(const Ctx &X, const oracle_bc &bc, const double *s1_in, con
         const double p_b = a_b * a_b * s2[0] * gammaInverse;
         s2[nf - 1] *= (0.5 / s2[0]);
         s2[nf - 1] += p_b * gammaM1Inverse;
-        return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
+        return;
     }
     case ORACLE_BC_INFLOW_RV: {   // SubsonicInflowRVBdrFaceIntegrator.cpp:19-49 (constant)
         const double r = bc.state[0];
@@ -633,7 +603,7 @@ double bdr_face_flux(const Ctx &X, const oracle_bc &bc, const double *s1_in, con
         dke *= 0.5 / s1[0];
         dke += 0.5 * uu * r;
         s2[nf - 1] = s1[nf - 1] + dke;
-        return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
+        return;
     }
     case ORACLE_BC_INFLOW_PTTT: {   // SubsonicInflowPtTtAngBdrFaceIntegrator.cpp:15-79 (constant)
         // direction: (cos t, sin t) in 2D; in 3D the reference stores cos f one past
@@ -656,11 +626,130 @@ double bdr_face_flux(const Ctx &X, const oracle_bc &bc, const double *s1_in, con
         s2[0] = gamma * gammaM1Inverse * p / (bc.cp * bc.Tt - 0.5 * V_sq);
         for (int d = 0; d < dim; ++d) s2[1 + d] = s2[0] * std::sqrt(V_sq) * vc[d];
         s2[nf - 1] = p * gammaM1Inverse + 0.5 * s2[0] * V_sq;
-        return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
+        return;
     }
     default:
+        for (int f = 0; f < nf; ++f) s2[f] = s1[f];
+        return;
+    }
+}
+
+inline bool is_wall(int type) {
+    return type == ORACLE_BC_SLIP_WALL || type == ORACLE_BC_NOSLIP_ADIABATIC || type == ORACLE_BC_NOSLIP_ISOTHERMAL;
+}
+
+// Boundary-face flux of trace s1 (BdrFaceIntegrator.cpp:61-138 with the
+// integrators of src/Integrators/BoundaryConditions/).  The element receives
+// -flux / (w0 J1) at the face node.  On return s1 and s2 are the inner and outer
+// states the viscous boundary flux reads (NS).  Returns the largest |V|+c seen.
+double bdr_face_flux(const Ctx &X, const oracle_bc &bc, double *s1, double *s2, const double *nor, double *flux) {
+    const int dim = X.dim, nf = dim + 2;
+    const double gamma = X.P.gamma, gammaM1 = X.P.gammaM1, gammaM1Inverse = X.P.gammaM1Inverse;
+    if (is_wall(bc.type)) {
+        // SlipWallBdrFaceIntegrator.cpp:16-59; the no-slip walls inherit it
+        const double nn = norml2(nor, dim), rn = 1.0 / nn;
+        const double gammaP1 = 1.0 + gamma, gammaP1Inverse = 1.0 / gammaP1;
+        const double rho = s1[0];
+        double mn = 0.0, vv = 0.0;
+        for (int d = 0; d < dim; ++d) {
+            mn += s1[1 + d] * (nor[d] * rn);
+            const double v = s1[1 + d] / rho;
+            vv += v * v;
+        }
+        const double u = mn / rho;   // normal velocity in the rotated frame
+        const double p = gammaM1 * (s1[nf - 1] - 0.5 * rho * vv);
+        const double an = sound_speed(p, rho, gamma);
+        double p_star;
+        if (u > 0.0)
+            p_star = p + 0.25 * u * gammaP1 * rho *
+                             (u + std::sqrt(u * u + 8.0 * gammaP1Inverse / rho * p * (gammaM1 * gammaP1Inverse + 1.0)));
+        else
+            p_star = p * std::pow(std::max(1.0 + 0.5 * gammaM1 * u / an, 0.0001), 2.0 * gamma * gammaM1Inverse);
         for (int f = 0; f < nf; ++f) flux[f] = 0.0;
+        for (int d = 0; d < dim; ++d) flux[1 + d] = p_star * nor[d];
+        for (int f = 0; f < nf; ++f) s2[f] = s1[f];
+        return std::sqrt(vv) + an;
+    }
+    if (bc.type == ORACLE_BC_SYMMETRY && norml2(nor, dim) == 0.0) {
+        for (int f = 0; f < nf; ++f) { flux[f] = 0.0; s2[f] = s1[f]; }
         return 0.0;
+    }
+    bdr_outer_state(X, bc, s1, nor, s2);
+    return face_flux(dim, gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
+}
+
+// BasicOperations.cpp:106-124
+void entropy2conserv(int dim, const Phys &P, const double *ent, double *state) {
+    double vel[3], vv = 0.0;
+    const double beta = -ent[dim + 1];
+    const double rb = 1.0 / beta;   // vel /= beta
+    for (int d = 0; d < dim; ++d) vel[d] = ent[1 + d] * rb;
+    for (int d = 0; d < dim; ++d) vv += vel[d] * vel[d];
+    const double s = P.gamma - (ent[0] + 0.5 * beta * vv) * P.gammaM1;
+    state[0] = std::pow(std::exp(-s) / beta, P.gammaM1Inverse);
+    for (int d = 0; d < dim; ++d) state[1 + d] = state[0] * vel[d];
+    state[dim + 1] = state[0] * (1.0 / beta * P.gammaM1Inverse + 0.5 * vv);
+}
+
+// Lifting flux of a boundary face node (ComputeBdrFaceLiftingFlux): w1 is the
+// inner trace's entropy variables; the gradient receives fluxN * nor / (w0 J1).
+// Default (BdrFaceIntegrator.cpp:274-281): 1/2 (v(outer state of E2C(w1)) - w1)
+// (reference mode: Q12).
+// No-slip walls (NoSlip*WallBdrFaceIntegrator.cpp): v_wall - w1 with v_wall =
+// (w1_0, V_wall * b, -b), b = -w1_last (adiabatic) or 1/(R_gas T_wall).
+void bdr_lift_flux(const Ctx &X, const oracle_bc &bc, const double *w1, const double *nor, double *fluxN) {
+    const int dim = X.dim, nf = dim + 2;
+    if (bc.type == ORACLE_BC_NOSLIP_ADIABATIC || bc.type == ORACLE_BC_NOSLIP_ISOTHERMAL) {
+        const double v = bc.type == ORACLE_BC_NOSLIP_ADIABATIC ? -w1[nf - 1] : 1.0 / (X.P.R_gas * bc.wall_T);
+        fluxN[0] = w1[0];
+        for (int d = 0; d < dim; ++d) fluxN[1 + d] = bc.wall_vel[d] * v;
+        fluxN[nf - 1] = -v;
+        for (int f = 0; f < nf; ++f) fluxN[f] -= w1[f];
+        return;
+    }
+    double c[5] = {0, 0, 0, 0, 0}, s2[5] = {0, 0, 0, 0, 0}, w[5] = {0, 0, 0, 0, 0};
+    for (int f = 0; f < nf; ++f) w[f] = w1[f];
+    entropy2conserv(dim, X.P, w1, c);
+    // Q12: Entropy2Conserv's `vel /= beta` wraps its const input, so (reference)
+    // the trace's middle entries are velocities when `fluxN -= state1` reads them
+    if (X.quirks == 0) {
+        const double rb = 1.0 / -w1[nf - 1];
+        for (int d = 0; d < dim; ++d) w[1 + d] = w1[1 + d] * rb;
+    }
+    bdr_outer_state(X, bc, c, nor, s2);
+    conserv2entropy(nf, X.P, s2, fluxN);
+    for (int f = 0; f < nf; ++f) fluxN[f] -= w[f];
+    for (int f = 0; f < nf; ++f) fluxN[f] *= 0.5;
+}
+
+// Viscous boundary flux (ComputeBdrFaceViscousFlux) from the traces left by
+// bdr_face_flux and the inner primitive gradients q[c][f]:
+//   no-slip walls, supersonic outflow: Fv(inner state, q) . nor (outflow uses its
+//   copy of the inner state); the adiabatic wall's energy row is V_wall . (mom rows)
+//   + q_n |nor| (NoSlipAdiabWallBdrFaceIntegrator.cpp:17-31);
+//   specified state, pressure outflow, Riemann invariants, inflow (rho, V):
+//   Fv(outer state, 0) . nor = 0.
+void bdr_viscous_flux(const Ctx &X, const oracle_bc &bc, double *s1, double *s2, const double (*q)[5],
+                      const double *nor, double *fv) {
+    const int dim = X.dim, nf = dim + 2;
+    for (int f = 0; f < nf; ++f) fv[f] = 0.0;
+    if (bc.type != ORACLE_BC_NOSLIP_ADIABATIC && bc.type != ORACLE_BC_NOSLIP_ISOTHERMAL &&
+        bc.type != ORACLE_BC_OUTFLOW)
+        return;
+    double Fv[15];
+    viscous_flux(dim, X.P, bc.type == ORACLE_BC_OUTFLOW ? s2 : s1, q[0], q[1], dim > 2 ? q[2] : nullptr, Fv);
+    for (int f = 0; f < nf; ++f) {   // DenseMatrix::Mult(nor, fluxN)
+        double t = 0.0;
+        for (int c = 0; c < dim; ++c) t += Fv[f * dim + c] * nor[c];
+        fv[f] = t;
+    }
+    if (bc.type == ORACLE_BC_NOSLIP_ADIABATIC) {
+        double nn = 0.0;
+        for (int c = 0; c < dim; ++c) nn += nor[c] * nor[c];
+        const double qn = bc.heat_flux * std::sqrt(nn);
+        double e = bc.wall_vel[0] * fv[1];
+        for (int d = 1; d < dim; ++d) e += bc.wall_vel[d] * fv[1 + d];
+        fv[nf - 1] = e + qn;
     }
 }
 
@@ -958,7 +1047,7 @@ void run_rhs(const Ctx &X, const double *u, double *dudt, double *alpha_out, dou
         std::vector<double> ent((size_t)nf * Ndof);
 #pragma omp parallel for schedule(static) num_threads(nthreads)
         for (long n = 0; n < Ndof; ++n) {
-            double s[5], v[5];
+            double s[5] = {0, 0, 0, 0, 0}, v[5];
             for (int f = 0; f < nf; ++f) s[f] = u[f * Ndof + n];
             conserv2entropy(nf, X.P, s, v);
             for (int f = 0; f < nf; ++f) ent[f * Ndof + n] = v[f];
@@ -981,7 +1070,7 @@ void run_rhs(const Ctx &X, const double *u, double *dudt, double *alpha_out, dou
 #pragma omp parallel for schedule(static) num_threads(nthreads)
             for (int fc = 0; fc < X.F; ++fc) {
                 const int *fe = X.faces + 4 * fc;
-                if ((fe[1] >> 1) != dir) continue;
+                if ((fe[1] >> 1) != dir || fe[2] < 0) continue;
                 const int e1 = fe[0], lf1 = fe[1], e2 = fe[2], lf2 = fe[3];
                 const double *nor = X.fnor + (long)fc * dim;
                 const double a1 = 1.0 / (w0 * X.detj[e1]), a2 = 1.0 / (w0 * X.detj[e2]);
@@ -996,6 +1085,26 @@ void run_rhs(const Ctx &X, const double *u, double *dudt, double *alpha_out, dou
                             grad[((size_t)c * nf + f) * Ndof + g1] += a1 * t;
                             grad[((size_t)c * nf + f) * Ndof + g2] += a2 * t;
                         }
+                }
+            }
+        }
+        // boundary faces after the interior ones (DGSEMNonlinearForm.cpp:561-610 ->
+        // LiftingBR1.cpp:311-407), element 1 only, grouped by direction
+        for (int dir = 0; dir < dim; ++dir) {
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+            for (int fc = 0; fc < X.F; ++fc) {
+                const int *fe = X.faces + 4 * fc;
+                if ((fe[1] >> 1) != dir || fe[2] >= 0) continue;
+                const int e1 = fe[0], lf1 = fe[1];
+                const double *nor = X.fnor + (long)fc * dim;
+                const double a1 = 1.0 / (w0 * X.detj[e1]);
+                for (int a = 0; a < nfn; ++a) {
+                    const long g1 = (long)e1 * nd + face_node(X, lf1, a);
+                    double w1[5], fj[5];
+                    for (int f = 0; f < nf; ++f) w1[f] = ent[f * Ndof + g1];
+                    bdr_lift_flux(X, X.bcs[fe[3]], w1, nor, fj);
+                    for (int c = 0; c < dim; ++c)
+                        for (int f = 0; f < nf; ++f) grad[((size_t)c * nf + f) * Ndof + g1] += a1 * (fj[f] * nor[c]);
                 }
             }
         }
@@ -1037,14 +1146,22 @@ void run_rhs(const Ctx &X, const double *u, double *dudt, double *alpha_out, dou
             if ((fe[1] >> 1) != dir) continue;
             const int e1 = fe[0], lf1 = fe[1], e2 = fe[2], lf2 = fe[3];
             const double *nor = X.fnor + (long)fc * dim;
-            if (e2 < 0) {   // boundary face (BdrFaceIntegrator::AssembleFaceVector, Euler)
+            if (e2 < 0) {   // boundary face (BdrFaceIntegrator::AssembleFaceVector)
                 const double a1 = 1.0 / (w0 * X.detj[e1]);
                 for (int a = 0; a < nfn; ++a) {
                     const long g1 = (long)e1 * nd + face_node(X, lf1, a);
-                    double s1[5], flux[5];
+                    double s1[5] = {0, 0, 0, 0, 0}, s2[5] = {0, 0, 0, 0, 0}, flux[5], d1[5];
                     for (int f = 0; f < nf; ++f) s1[f] = u[f * Ndof + g1];
-                    bdr_face_flux(X, X.bcs[lf2], s1, nor, flux);
-                    for (int f = 0; f < nf; ++f) dudt[f * Ndof + g1] += a1 * -flux[f];
+                    bdr_face_flux(X, X.bcs[lf2], s1, s2, nor, flux);
+                    for (int f = 0; f < nf; ++f) d1[f] = -flux[f];
+                    if (X.parabolic) {   // dU = -inviscid + viscous (BdrFaceIntegrator.cpp:170-186)
+                        double q[3][5], fv[5];
+                        for (int c = 0; c < dim; ++c)
+                            for (int f = 0; f < nf; ++f) q[c][f] = grad[((size_t)c * nf + f) * Ndof + g1];
+                        bdr_viscous_flux(X, X.bcs[lf2], s1, s2, q, nor, fv);
+                        for (int f = 0; f < nf; ++f) d1[f] += fv[f];
+                    }
+                    for (int f = 0; f < nf; ++f) dudt[f * Ndof + g1] += a1 * d1[f];
                 }
                 continue;
             }
@@ -1094,6 +1211,23 @@ void run_rhs(const Ctx &X, const double *u, double *dudt, double *alpha_out, dou
     }
 }
 
+// Boundary faces need a valid BC index; the Navier-Stokes form has no viscous
+// treatment for the slip wall, symmetry and pt/Tt inflow types, and in reference
+// mode no defined Riemann-invariant lifting (RiemannInvariantBdrFaceIntegrator
+// normalises the integrator's `nor`, which AssembleLiftingBdrFaceVector never sets).
+bool bad_boundaries(const oracle_mesh *m, const oracle_config *c) {
+    for (int f = 0; f < m->num_faces; ++f) {
+        const int *fe = m->face_elems + 4 * f;
+        if (fe[2] >= 0) continue;
+        if (!c->bcs || fe[3] < 0 || fe[3] >= c->num_bcs) return true;
+        const int t = c->bcs[fe[3]].type;
+        if (c->parabolic && (t == ORACLE_BC_SLIP_WALL || t == ORACLE_BC_SYMMETRY || t == ORACLE_BC_INFLOW_PTTT))
+            return true;
+        // Q13: the reference's Riemann lifting reads a face normal only its face pass sets
+        if (c->parabolic && c->quirks == 0 && t == ORACLE_BC_RIEMANN) return true;
+    }
+    return false;
+}
 }   // namespace
 
 extern "C" {
@@ -1103,11 +1237,7 @@ int oracle_rhs(const oracle_mesh *m, const oracle_config *c, const double *u, do
     if (!m || !c || !u || !dudt) return 1;
     if (m->dim < 2 || m->dim > 3 || m->order < 1 || m->order > 9) return 1;
     if (nthreads <= 0) nthreads = 1;
-    for (int f = 0; f < m->num_faces; ++f) {   // boundary faces: Euler, a valid BC index
-        const int *fe = m->face_elems + 4 * f;
-        if (fe[2] >= 0) continue;
-        if (c->parabolic || !c->bcs || fe[3] < 0 || fe[3] >= c->num_bcs) return 1;
-    }
+    if (bad_boundaries(m, c)) return 1;
     Ctx X;
     setup(X, m, c);
     run_rhs(X, u, dudt, alpha, lambda_max, grad, nthreads);
@@ -1118,6 +1248,7 @@ int oracle_step(const oracle_mesh *m, const oracle_config *c, double *u, double 
                 int scheme, int nsteps, int nthreads) {
     if (!m || !c || !u) return 1;
     if (nthreads <= 0) nthreads = 1;
+    if (bad_boundaries(m, c)) return 1;
     Ctx X;
     setup(X, m, c);
     const long n = (long)X.nf * X.Ndof;

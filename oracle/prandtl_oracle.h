@@ -39,8 +39,10 @@ typedef struct oracle_mesh {
     const double *face_nor;   /* [F][dim] */
 } oracle_mesh;
 
-/* Boundary conditions (Euler).  A boundary face is listed in face_elems as
- * {elem1, lface1, -1, bc} with bc an index into oracle_config.bcs. */
+/* Boundary conditions.  A boundary face is listed in face_elems as
+ * {elem1, lface1, -1, bc} with bc an index into oracle_config.bcs.  With
+ * parabolic = 1 the slip wall, symmetry and SubsonicInflowPtTtAng types are
+ * rejected (the reference defines no viscous treatment for the first two). */
 enum {
     ORACLE_BC_STATE = 0,            /* SpecifiedState / SupersonicInflow with a constant state */
     ORACLE_BC_OUTFLOW = 1,          /* SupersonicOutflow: outer state = inner state */
@@ -49,7 +51,9 @@ enum {
     ORACLE_BC_PRESSURE_OUTFLOW = 4, /* SubsonicOutflowP with a constant pressure */
     ORACLE_BC_RIEMANN = 5,          /* RiemannInvariant, constant outer primitive state */
     ORACLE_BC_INFLOW_RV = 6,        /* SubsonicInflowRV, constant density and velocity */
-    ORACLE_BC_INFLOW_PTTT = 7       /* SubsonicInflowPtTtAng, constant pt, Tt, angles */
+    ORACLE_BC_INFLOW_PTTT = 7,      /* SubsonicInflowPtTtAng, constant pt, Tt, angles */
+    ORACLE_BC_NOSLIP_ADIABATIC = 8, /* NoSlipAdiabWall: wall velocity, normal heat flux */
+    ORACLE_BC_NOSLIP_ISOTHERMAL = 9 /* NoSlipIsothWall: wall velocity, wall temperature */
 };
 typedef struct oracle_bc {
     int type;
@@ -57,6 +61,9 @@ typedef struct oracle_bc {
     double p;           /* outflow pressure (ORACLE_BC_PRESSURE_OUTFLOW) */
     double pt, Tt, cp;  /* ORACLE_BC_INFLOW_PTTT */
     double theta, phi;  /*   flow angles in degrees */
+    double wall_vel[3]; /* NOSLIP_*: wall velocity */
+    double heat_flux;   /* NOSLIP_ADIABATIC: normal heat flux per unit face measure */
+    double wall_T;      /* NOSLIP_ISOTHERMAL: wall temperature (entropy variable -1/(R_gas T)) */
 } oracle_bc;
 
 typedef struct oracle_config {

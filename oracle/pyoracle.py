@@ -24,12 +24,13 @@ class OracleMesh(C.Structure):
 
 class OracleBC(C.Structure):
     _fields_ = [("type", C.c_int), ("state", C.c_double * 5), ("p", C.c_double), ("pt", C.c_double),
-                ("Tt", C.c_double), ("cp", C.c_double), ("theta", C.c_double), ("phi", C.c_double)]
+                ("Tt", C.c_double), ("cp", C.c_double), ("theta", C.c_double), ("phi", C.c_double),
+                ("wall_vel", C.c_double * 3), ("heat_flux", C.c_double), ("wall_T", C.c_double)]
 
 
 # boundary-condition types (prandtl_oracle.h ORACLE_BC_*)
 BC_TYPES = {"state": 0, "outflow": 1, "slip_wall": 2, "symmetry": 3, "pressure_outflow": 4,
-            "riemann": 5, "inflow_rv": 6, "inflow_pttt": 7}
+            "riemann": 5, "inflow_rv": 6, "inflow_pttt": 7, "noslip_adiabatic": 8, "noslip_isothermal": 9}
 
 
 class OracleConfig(C.Structure):
@@ -42,16 +43,20 @@ class OracleConfig(C.Structure):
 
 def make_bcs(bcs):
     """ctypes array of boundary conditions from [(type name, state or None, p or None), ...];
-    for inflow_pttt the second item is a dict of pt, Tt, cp, theta, phi."""
+    for inflow_pttt and the no-slip walls the second item is a dict of named fields."""
     if not bcs:
         return None
     arr = (OracleBC * len(bcs))()
     for k, b in enumerate(bcs):
         kind, state, p = (tuple(b) + (None, None))[:3]
         arr[k].type = BC_TYPES[kind]
-        if isinstance(state, dict):   # inflow_pttt: pt, Tt, cp, theta, phi
+        if isinstance(state, dict):   # inflow_pttt, noslip_*: named fields
             for name, v in state.items():
-                setattr(arr[k], name, float(v))
+                if name == "wall_vel":
+                    for d, x in enumerate(v):
+                        arr[k].wall_vel[d] = float(x)
+                else:
+                    setattr(arr[k], name, float(v))
         else:
             for f, v in enumerate(state if state is not None else []):
                 arr[k].state[f] = float(v)

@@ -32,6 +32,8 @@ FILES="$SRC/BasicOperations/BasicOperations.cpp $SRC/RiemannSolvers/Chandrasheka
  $SRC/Integrators/BoundaryConditions/RiemannInvariantBdrFaceIntegrator.cpp \
  $SRC/Integrators/BoundaryConditions/SubsonicInflowRVBdrFaceIntegrator.cpp \
  $SRC/Integrators/BoundaryConditions/SubsonicInflowPtTtAngBdrFaceIntegrator.cpp \
+ $SRC/Integrators/BoundaryConditions/NoSlipAdiabWallBdrFaceIntegrator.cpp \
+ $SRC/Integrators/BoundaryConditions/NoSlipIsothWallBdrFaceIntegrator.cpp \
  $HERE/ref_driver.cpp"
 # -O2 -DNDEBUG as the reference's Release configuration (configure.sh)
 FLAGS="-O2 -DNDEBUG -std=c++17 -fPIC -shared -w"

@@ -37,6 +37,8 @@
 #include "RiemannInvariantBdrFaceIntegrator.hpp"
 #include "SubsonicInflowRVBdrFaceIntegrator.hpp"
 #include "SubsonicInflowPtTtAngBdrFaceIntegrator.hpp"
+#include "NoSlipAdiabWallBdrFaceIntegrator.hpp"
+#include "NoSlipIsothWallBdrFaceIntegrator.hpp"
 #include "prandtl_oracle.h"
 
 namespace mfem {
@@ -288,107 +290,12 @@ extern "C" int ref_rhs(const oracle_mesh *md, const oracle_config *cfg, const do
         Vector el_u, el_dudt;
         const FiniteElement *fe = vfes->GetFE(0);
         dudt = 0.0;
-#ifdef PARABOLIC
-        {
-            // ComputeGlobalEntropyVector (DGSEMOperator.cpp:82-94)
-            Vector ent(N), el_vdofs;
-            DenseMatrix ent_mat(Ndofs, nf);
-            for (int el = 0; el < NE; el++) {
-                vfes->GetElementVDofs(el, vdofs);
-                u.GetSubVector(vdofs, el_vdofs);
-                DenseMatrix vdof_mat(el_vdofs.GetData(), Ndofs, nf);
-                Conserv2Entropy(vdof_mat, ent_mat, pc.gamma, pc.gammaM1, pc.gammaM1Inverse);
-                ent.SetSubVector(vdofs, ent_mat.GetData());
-            }
-            // MultLifting (DGSEMNonlinearForm.cpp:213-645), P = I, no boundary faces
-            std::vector<Vector> g(dim, Vector(N));
-            for (auto &v : g) v = 0.0;
-            std::vector<Vector> elg(3);
-            for (int i = 0; i < NE; i++) {
-                vfes->GetElementVDofs(i, vdofs);
-                ent.GetSubVector(vdofs, el_u);
-                if (dim == 3) integ.AssembleLiftingElementVector(*fe, *pmesh->GetElementTransformation(i), el_u, elg[0], elg[1], elg[2]);
-                else integ.AssembleLiftingElementVector(*fe, *pmesh->GetElementTransformation(i), el_u, elg[0], elg[1]);
-                for (int d = 0; d < dim; ++d) g[d].AddElementVector(vdofs, elg[d]);
-            }
-            for (int i = 0; i < pmesh->GetNumFaces(); i++) {
-                FaceElementTransformations *tr = pmesh->GetInteriorFaceTransformations(i);
-                vfes->GetElementVDofs(tr->Elem1No, vdofs);
-                vfes->GetElementVDofs(tr->Elem2No, vdofs2);
-                vdofs.Append(vdofs2);
-                ent.GetSubVector(vdofs, el_u);
-                if (dim == 3) integ.AssembleLiftingFaceVector(*fe, *fe, *tr, el_u, elg[0], elg[1], elg[2]);
-                else integ.AssembleLiftingFaceVector(*fe, *fe, *tr, el_u, elg[0], elg[1]);
-                for (int d = 0; d < dim; ++d) g[d].AddElementVector(vdofs, elg[d]);
-            }
-            // ComputeGlobalPrimitiveGradVector (DGSEMOperator.cpp:112-159)
-            Vector grad_vdofs;
-            for (int el = 0; el < NE; el++) {
-                vfes->GetElementVDofs(el, vdofs);
-                u.GetSubVector(vdofs, el_vdofs);
-                DenseMatrix vdof_mat(el_vdofs.GetData(), Ndofs, nf);
-                for (int d = 0; d < dim; ++d) {
-                    g[d].GetSubVector(vdofs, grad_vdofs);
-                    DenseMatrix grad_mat(grad_vdofs.GetData(), Ndofs, nf);
-                    EntropyGrad2PrimGrad(vdof_mat, grad_mat, pc.gammaM1, pc.gammaM1Inverse);
-                    g[d].SetSubVector(vdofs, grad_mat.GetData());
-                }
-            }
-            if (grad_out)
-                for (int d = 0; d < dim; ++d) std::memcpy(grad_out + (size_t)d * N, g[d].GetData(), sizeof(double) * N);
-            // Mult (DGSEMNonlinearForm.cpp:1070-1545)
-            Vector gx, gy, gz;
-            for (int i = 0; i < NE; i++) {
-                vfes->GetElementVDofs(i, vdofs);
-                u.GetSubVector(vdofs, el_u);
-                g[0].GetSubVector(vdofs, gx);
-                g[1].GetSubVector(vdofs, gy);
-                if (dim == 3) {
-                    g[2].GetSubVector(vdofs, gz);
-                    integ.AssembleElementVector(*fe, *pmesh->GetElementTransformation(i), el_u, gx, gy, gz, el_dudt);
-                } else {
-                    integ.AssembleElementVector(*fe, *pmesh->GetElementTransformation(i), el_u, gx, gy, el_dudt);
-                }
-                dudt.AddElementVector(vdofs, el_dudt);
-            }
-            for (int i = 0; i < pmesh->GetNumFaces(); i++) {
-                FaceElementTransformations *tr = pmesh->GetInteriorFaceTransformations(i);
-                vfes->GetElementVDofs(tr->Elem1No, vdofs);
-                vfes->GetElementVDofs(tr->Elem2No, vdofs2);
-                vdofs.Append(vdofs2);
-                u.GetSubVector(vdofs, el_u);
-                g[0].GetSubVector(vdofs, gx);
-                g[1].GetSubVector(vdofs, gy);
-                if (dim == 3) {
-                    g[2].GetSubVector(vdofs, gz);
-                    integ.AssembleFaceVector(*fe, *fe, *tr, el_u, gx, gy, gz, el_dudt);
-                } else {
-                    integ.AssembleFaceVector(*fe, *fe, *tr, el_u, gx, gy, el_dudt);
-                }
-                dudt.AddElementVector(vdofs, el_dudt);
-            }
-        }
-#else
-        // Mult (DGSEMNonlinearForm.cpp:647-849)
-        for (int i = 0; i < NE; i++) {
-            vfes->GetElementVDofs(i, vdofs);
-            u.GetSubVector(vdofs, el_u);
-            integ.AssembleElementVector(*fe, *pmesh->GetElementTransformation(i), el_u, el_dudt);
-            dudt.AddElementVector(vdofs, el_dudt);
-        }
-        for (int i = 0; i < pmesh->GetNumFaces(); i++) {
-            FaceElementTransformations *tr = pmesh->GetInteriorFaceTransformations(i);
-            if (tr->Elem2No < 0) continue;
-            vfes->GetElementVDofs(tr->Elem1No, vdofs);
-            vfes->GetElementVDofs(tr->Elem2No, vdofs2);
-            vdofs.Append(vdofs2);
-            u.GetSubVector(vdofs, el_u);
-            integ.AssembleFaceVector(*fe, *fe, *tr, el_u, el_dudt);
-            dudt.AddElementVector(vdofs, el_dudt);
-        }
-        // boundary faces (DGSEMNonlinearForm.cpp:781-830): the reference's boundary
-        // integrator of each face's condition, element 1 only
+        // the reference's boundary integrator of each condition (constant data;
+        // the adiabatic wall through coefficient functions, as Simulation::LoadConfig
+        // builds it, Simulation.cpp:540-632)
         std::vector<std::unique_ptr<BdrFaceIntegrator>> bdr;
+        std::vector<std::unique_ptr<FunctionCoefficient>> scoef;
+        std::vector<std::unique_ptr<VectorFunctionCoefficient>> vcoef;
         const real_t time = 0.0;
         for (int k = 0; k < cfg->num_bcs; ++k) {
             const oracle_bc &b = cfg->bcs[k];
@@ -430,9 +337,155 @@ extern "C" int ref_rhs(const oracle_mesh *md, const oracle_config *cfg, const do
                 bdr.emplace_back(new SubsonicInflowPtTtAngBdrFaceIntegrator(lifting, rsolver, Np, time, pc.gamma, b.cp,
                                                                             b.pt, b.Tt, b.theta, b.phi));
                 break;
+            case ORACLE_BC_NOSLIP_ADIABATIC: {
+                const double qn = b.heat_flux, v0 = b.wall_vel[0], v1 = b.wall_vel[1], v2 = b.wall_vel[2];
+                scoef.emplace_back(new FunctionCoefficient([qn](const Vector &) { return qn; }));
+                vcoef.emplace_back(new VectorFunctionCoefficient(dim, [v0, v1, v2, dim](const Vector &, Vector &v) {
+                    v(0) = v0;
+                    if (dim > 1) v(1) = v1;
+                    if (dim > 2) v(2) = v2;
+                }));
+                bdr.emplace_back(new NoSlipAdiabWallBdrFaceIntegrator(lifting, rsolver, Np, time, pc.gamma,
+                                                                      *scoef.back(), *vcoef.back(), false));
+                break;
+            }
+            case ORACLE_BC_NOSLIP_ISOTHERMAL: {
+                Vector V(dim);
+                for (int d = 0; d < dim; ++d) V(d) = b.wall_vel[d];
+                real_t T = b.wall_T;
+                bdr.emplace_back(new NoSlipIsothWallBdrFaceIntegrator(lifting, rsolver, Np, time, pc.gamma,
+                                                                      cfg->R_gas, T, V));
+                break;
+            }
             default:
                 throw std::runtime_error("unknown boundary condition");
             }
+        }
+#ifdef PARABOLIC
+        {
+            // ComputeGlobalEntropyVector (DGSEMOperator.cpp:82-94)
+            Vector ent(N), el_vdofs;
+            DenseMatrix ent_mat(Ndofs, nf);
+            for (int el = 0; el < NE; el++) {
+                vfes->GetElementVDofs(el, vdofs);
+                u.GetSubVector(vdofs, el_vdofs);
+                DenseMatrix vdof_mat(el_vdofs.GetData(), Ndofs, nf);
+                Conserv2Entropy(vdof_mat, ent_mat, pc.gamma, pc.gammaM1, pc.gammaM1Inverse);
+                ent.SetSubVector(vdofs, ent_mat.GetData());
+            }
+            // MultLifting (DGSEMNonlinearForm.cpp:213-645), P = I
+            std::vector<Vector> g(dim, Vector(N));
+            for (auto &v : g) v = 0.0;
+            std::vector<Vector> elg(3);
+            for (int i = 0; i < NE; i++) {
+                vfes->GetElementVDofs(i, vdofs);
+                ent.GetSubVector(vdofs, el_u);
+                if (dim == 3) integ.AssembleLiftingElementVector(*fe, *pmesh->GetElementTransformation(i), el_u, elg[0], elg[1], elg[2]);
+                else integ.AssembleLiftingElementVector(*fe, *pmesh->GetElementTransformation(i), el_u, elg[0], elg[1]);
+                for (int d = 0; d < dim; ++d) g[d].AddElementVector(vdofs, elg[d]);
+            }
+            for (int i = 0; i < pmesh->GetNumFaces(); i++) {
+                FaceElementTransformations *tr = pmesh->GetInteriorFaceTransformations(i);
+                if (tr->Elem2No < 0) continue;
+                vfes->GetElementVDofs(tr->Elem1No, vdofs);
+                vfes->GetElementVDofs(tr->Elem2No, vdofs2);
+                vdofs.Append(vdofs2);
+                ent.GetSubVector(vdofs, el_u);
+                if (dim == 3) integ.AssembleLiftingFaceVector(*fe, *fe, *tr, el_u, elg[0], elg[1], elg[2]);
+                else integ.AssembleLiftingFaceVector(*fe, *fe, *tr, el_u, elg[0], elg[1]);
+                for (int d = 0; d < dim; ++d) g[d].AddElementVector(vdofs, elg[d]);
+            }
+            // boundary faces (DGSEMNonlinearForm.cpp:561-610)
+            for (int i = 0; i < pmesh->GetNumFaces(); i++) {
+                FaceElementTransformations *tr = pmesh->GetInteriorFaceTransformations(i);
+                if (tr->Elem2No >= 0) continue;
+                vfes->GetElementVDofs(tr->Elem1No, vdofs);
+                ent.GetSubVector(vdofs, el_u);
+                if (dim == 3) bdr.at(tr->lf2)->AssembleLiftingFaceVector(*fe, *fe, *tr, el_u, elg[0], elg[1], elg[2]);
+                else bdr.at(tr->lf2)->AssembleLiftingFaceVector(*fe, *fe, *tr, el_u, elg[0], elg[1]);
+                for (int d = 0; d < dim; ++d) g[d].AddElementVector(vdofs, elg[d]);
+            }
+            // ComputeGlobalPrimitiveGradVector (DGSEMOperator.cpp:112-159)
+            Vector grad_vdofs;
+            for (int el = 0; el < NE; el++) {
+                vfes->GetElementVDofs(el, vdofs);
+                u.GetSubVector(vdofs, el_vdofs);
+                DenseMatrix vdof_mat(el_vdofs.GetData(), Ndofs, nf);
+                for (int d = 0; d < dim; ++d) {
+                    g[d].GetSubVector(vdofs, grad_vdofs);
+                    DenseMatrix grad_mat(grad_vdofs.GetData(), Ndofs, nf);
+                    EntropyGrad2PrimGrad(vdof_mat, grad_mat, pc.gammaM1, pc.gammaM1Inverse);
+                    g[d].SetSubVector(vdofs, grad_mat.GetData());
+                }
+            }
+            if (grad_out)
+                for (int d = 0; d < dim; ++d) std::memcpy(grad_out + (size_t)d * N, g[d].GetData(), sizeof(double) * N);
+            // Mult (DGSEMNonlinearForm.cpp:1070-1545)
+            Vector gx, gy, gz;
+            for (int i = 0; i < NE; i++) {
+                vfes->GetElementVDofs(i, vdofs);
+                u.GetSubVector(vdofs, el_u);
+                g[0].GetSubVector(vdofs, gx);
+                g[1].GetSubVector(vdofs, gy);
+                if (dim == 3) {
+                    g[2].GetSubVector(vdofs, gz);
+                    integ.AssembleElementVector(*fe, *pmesh->GetElementTransformation(i), el_u, gx, gy, gz, el_dudt);
+                } else {
+                    integ.AssembleElementVector(*fe, *pmesh->GetElementTransformation(i), el_u, gx, gy, el_dudt);
+                }
+                dudt.AddElementVector(vdofs, el_dudt);
+            }
+            for (int i = 0; i < pmesh->GetNumFaces(); i++) {
+                FaceElementTransformations *tr = pmesh->GetInteriorFaceTransformations(i);
+                if (tr->Elem2No < 0) continue;
+                vfes->GetElementVDofs(tr->Elem1No, vdofs);
+                vfes->GetElementVDofs(tr->Elem2No, vdofs2);
+                vdofs.Append(vdofs2);
+                u.GetSubVector(vdofs, el_u);
+                g[0].GetSubVector(vdofs, gx);
+                g[1].GetSubVector(vdofs, gy);
+                if (dim == 3) {
+                    g[2].GetSubVector(vdofs, gz);
+                    integ.AssembleFaceVector(*fe, *fe, *tr, el_u, gx, gy, gz, el_dudt);
+                } else {
+                    integ.AssembleFaceVector(*fe, *fe, *tr, el_u, gx, gy, el_dudt);
+                }
+                dudt.AddElementVector(vdofs, el_dudt);
+            }
+            // boundary faces (DGSEMNonlinearForm.cpp:1480-1525)
+            for (int i = 0; i < pmesh->GetNumFaces(); i++) {
+                FaceElementTransformations *tr = pmesh->GetInteriorFaceTransformations(i);
+                if (tr->Elem2No >= 0) continue;
+                vfes->GetElementVDofs(tr->Elem1No, vdofs);
+                u.GetSubVector(vdofs, el_u);
+                g[0].GetSubVector(vdofs, gx);
+                g[1].GetSubVector(vdofs, gy);
+                if (dim == 3) {
+                    g[2].GetSubVector(vdofs, gz);
+                    bdr.at(tr->lf2)->AssembleFaceVector(*fe, *fe, *tr, el_u, gx, gy, gz, el_dudt);
+                } else {
+                    bdr.at(tr->lf2)->AssembleFaceVector(*fe, *fe, *tr, el_u, gx, gy, el_dudt);
+                }
+                dudt.AddElementVector(vdofs, el_dudt);
+            }
+        }
+#else
+        // Mult (DGSEMNonlinearForm.cpp:647-849)
+        for (int i = 0; i < NE; i++) {
+            vfes->GetElementVDofs(i, vdofs);
+            u.GetSubVector(vdofs, el_u);
+            integ.AssembleElementVector(*fe, *pmesh->GetElementTransformation(i), el_u, el_dudt);
+            dudt.AddElementVector(vdofs, el_dudt);
+        }
+        for (int i = 0; i < pmesh->GetNumFaces(); i++) {
+            FaceElementTransformations *tr = pmesh->GetInteriorFaceTransformations(i);
+            if (tr->Elem2No < 0) continue;
+            vfes->GetElementVDofs(tr->Elem1No, vdofs);
+            vfes->GetElementVDofs(tr->Elem2No, vdofs2);
+            vdofs.Append(vdofs2);
+            u.GetSubVector(vdofs, el_u);
+            integ.AssembleFaceVector(*fe, *fe, *tr, el_u, el_dudt);
+            dudt.AddElementVector(vdofs, el_dudt);
         }
         for (int i = 0; i < pmesh->GetNumFaces(); i++) {
             FaceElementTransformations *tr = pmesh->GetInteriorFaceTransformations(i);

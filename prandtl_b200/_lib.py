@@ -47,11 +47,12 @@ class MeshDesc(C.Structure):
 
 class BC(C.Structure):
     _fields_ = [("type", C.c_int), ("state", C.c_double * 5), ("p", C.c_double), ("pt", C.c_double),
-                ("Tt", C.c_double), ("cp", C.c_double), ("theta", C.c_double), ("phi", C.c_double)]
+                ("Tt", C.c_double), ("cp", C.c_double), ("theta", C.c_double), ("phi", C.c_double),
+                ("wall_vel", C.c_double * 3), ("heat_flux", C.c_double), ("wall_T", C.c_double)]
 
 
 BC_TYPES = {"state": 0, "outflow": 1, "slip_wall": 2, "symmetry": 3, "pressure_outflow": 4,
-            "riemann": 5, "inflow_rv": 6, "inflow_pttt": 7}
+            "riemann": 5, "inflow_rv": 6, "inflow_pttt": 7, "noslip_adiabatic": 8, "noslip_isothermal": 9}
 
 
 class Config(C.Structure):

@@ -28,10 +28,11 @@ struct PhysParams {
 
 // A boundary condition (the layout of prandtl_bc).
 // INFLOW_PTTT keeps pt, Tt, cp and the unit flow direction vc (formed on the
-// host from theta, phi).
+// host from theta, phi); the no-slip walls keep the wall velocity, the normal
+// heat flux and vT = 1 / (R_gas T_wall).
 enum BcType : int {
     BC_STATE = 0, BC_OUTFLOW = 1, BC_SLIP_WALL = 2, BC_SYMMETRY = 3, BC_PRESSURE_OUTFLOW = 4,
-    BC_RIEMANN = 5, BC_INFLOW_RV = 6, BC_INFLOW_PTTT = 7
+    BC_RIEMANN = 5, BC_INFLOW_RV = 6, BC_INFLOW_PTTT = 7, BC_NOSLIP_ADIABATIC = 8, BC_NOSLIP_ISOTHERMAL = 9
 };
 struct BcDev {
     int type, pad;
@@ -39,6 +40,8 @@ struct BcDev {
     double p;
     double pt, Tt, cp;
     double vc[3];
+    double wall_vel[3];
+    double heat_flux, vT;
 };
 
 // 1D operator tables for one polynomial order (NP <= 8), row-major [i][l].

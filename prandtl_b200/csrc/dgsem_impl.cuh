@@ -416,57 +416,23 @@ __device__ __forceinline__ int batch_slot(const int *prefix, int n, int first) {
     }
     return lo;
 }
-// Boundary-face flux of the inner trace s_in (FP64 conserved state) along the
-// element's outward scaled normal nor: the reference's boundary integrators
-// with constant states (src/Integrators/BoundaryConditions/; the element is
-// Elem1 and receives -flux / (w0 J), BdrFaceIntegrator.cpp:61-138).  Inviscid.
-// The outer state is formed in FP64; the Chandrashekar surface flux runs in
-// the working precision like the interior faces.
-template <int DIM, typename Real>
-__device__ __forceinline__ void boundary_flux(const BcDev &bc, const double *s_in, const double *nor,
-                                              const PhysParams &P, double pref, Real *flux) {
+__device__ __forceinline__ bool bc_is_wall(int type) {
+    return type == BC_SLIP_WALL || type == BC_NOSLIP_ADIABATIC || type == BC_NOSLIP_ISOTHERMAL;
+}
+
+// Outer state s2 of the conditions whose flux is the surface flux of (s1, s2)
+// (ComputeOuterInviscidState of src/Integrators/BoundaryConditions/, constant
+// data), in FP64.  s1 takes the reference-mode aliasing the integrator applies
+// to its inner trace.  nn = |nor|.  Not for the wall types.
+template <int DIM>
+__device__ __forceinline__ void bc_outer_state(const BcDev &bc, double *s1, const double *nor, double nn,
+                                               const PhysParams &P, double *s2) {
     constexpr int NF = DIM + 2;
     const double gamma = P.gamma, gm1 = P.gammaM1, gm1i = P.gammaM1Inverse;
-    double s1[NF], s2[NF], nn = 0.0;
-#pragma unroll
-    for (int f = 0; f < NF; ++f) s1[f] = s_in[f];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) nn += nor[d] * nor[d];
-    nn = sqrt(nn);
-    if (bc.type == BC_SLIP_WALL) {   // SlipWallBdrFaceIntegrator.cpp:16-59
-        const double rn = 1.0 / nn, gp1 = 1.0 + gamma, gp1i = 1.0 / gp1;
-        const double rho = s1[0];
-        double mn = 0.0, vv = 0.0;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            mn += s1[1 + d] * (nor[d] * rn);
-            const double v = s1[1 + d] / rho;
-            vv += v * v;
-        }
-        const double un = mn / rho;   // normal velocity of the rotated state
-        const double p = gm1 * (s1[NF - 1] - 0.5 * rho * vv);
-        const double an = sqrt(gamma * p / rho);
-        double p_star;
-        if (un > 0.0)
-            p_star = p + 0.25 * un * gp1 * rho * (un + sqrt(un * un + 8.0 * gp1i / rho * p * (gm1 * gp1i + 1.0)));
-        else
-            p_star = p * pow(fmax(1.0 + 0.5 * gm1 * un / an, 0.0001), 2.0 * gamma * gm1i);
-        // the FP32-bulk form carries p - pref in every momentum flux (pref = 0 in FP64)
-        flux[0] = 0;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) flux[1 + d] = Real((p_star - pref) * nor[d]);
-        flux[NF - 1] = 0;
-        return;
-    }
     if (bc.type == BC_STATE) {   // SpecifiedStateBdrFaceIntegrator.cpp:24-36
 #pragma unroll
         for (int f = 0; f < NF; ++f) s2[f] = bc.state[f];
-    } else if (bc.type == BC_SYMMETRY) {   // SymmetryBdrFaceIntegrator.cpp:11-32
-        if (nn == 0.0) {
-#pragma unroll
-            for (int f = 0; f < NF; ++f) flux[f] = 0;
-            return;
-        }
+    } else if (bc.type == BC_SYMMETRY) {   // SymmetryBdrFaceIntegrator.cpp:11-32 (|nor| > 0)
         const double rn = 1.0 / nn;
         double mn = 0.0;
 #pragma unroll
@@ -562,6 +528,56 @@ __device__ __forceinline__ void boundary_flux(const BcDev &bc, const double *s_i
 #pragma unroll
         for (int f = 0; f < NF; ++f) s2[f] = s1[f];
     }
+}
+
+// Boundary-face flux of the inner trace s_in (FP64 conserved state) along the
+// element's outward scaled normal nor: the reference's boundary integrators
+// with constant states (src/Integrators/BoundaryConditions/; the element is
+// Elem1 and receives -flux / (w0 J), BdrFaceIntegrator.cpp:61-138).  Inviscid.
+// The outer state is formed in FP64; the Chandrashekar surface flux runs in
+// the working precision like the interior faces.
+template <int DIM, typename Real>
+__device__ __forceinline__ void boundary_flux(const BcDev &bc, const double *s_in, const double *nor,
+                                              const PhysParams &P, double pref, Real *flux) {
+    constexpr int NF = DIM + 2;
+    const double gamma = P.gamma, gm1 = P.gammaM1, gm1i = P.gammaM1Inverse;
+    double s1[NF], s2[NF], nn = 0.0;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) s1[f] = s_in[f];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) nn += nor[d] * nor[d];
+    nn = sqrt(nn);
+    if (bc_is_wall(bc.type)) {   // SlipWallBdrFaceIntegrator.cpp:16-59 (the no-slip walls inherit it)
+        const double rn = 1.0 / nn, gp1 = 1.0 + gamma, gp1i = 1.0 / gp1;
+        const double rho = s1[0];
+        double mn = 0.0, vv = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            mn += s1[1 + d] * (nor[d] * rn);
+            const double v = s1[1 + d] / rho;
+            vv += v * v;
+        }
+        const double un = mn / rho;   // normal velocity of the rotated state
+        const double p = gm1 * (s1[NF - 1] - 0.5 * rho * vv);
+        const double an = sqrt(gamma * p / rho);
+        double p_star;
+        if (un > 0.0)
+            p_star = p + 0.25 * un * gp1 * rho * (un + sqrt(un * un + 8.0 * gp1i / rho * p * (gm1 * gp1i + 1.0)));
+        else
+            p_star = p * pow(fmax(1.0 + 0.5 * gm1 * un / an, 0.0001), 2.0 * gamma * gm1i);
+        // the FP32-bulk form carries p - pref in every momentum flux (pref = 0 in FP64)
+        flux[0] = 0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) flux[1 + d] = Real((p_star - pref) * nor[d]);
+        flux[NF - 1] = 0;
+        return;
+    }
+    if (bc.type == BC_SYMMETRY && nn == 0.0) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f) flux[f] = 0;
+        return;
+    }
+    bc_outer_state<DIM>(bc, s1, nor, nn, P, s2);
     Real m1[NF], m2[NF], nr[DIM];
 #pragma unroll
     for (int f = 0; f < NF; ++f) { m1[f] = Real(s1[f]); m2[f] = Real(s2[f]); }
@@ -605,13 +621,18 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
     const double J = __ldg(geo + DIM * DIM);
     const Real mJ = Real(1.0 / J);
 
-    // FP32-bulk form: reference pressure of the element (node 0), FP64
+    // FP32-bulk form: reference pressure of the element (node 0), FP64.  The
+    // shift cancels only where the volume operator annihilates a constant flux;
+    // the reference's 3D Navier-Stokes volume term (quirks == 0) stores the eta
+    // flux in the symmetric zeta slot (DGSEMIntegrator.cpp:702), so there pref = 0.
     double pref = 0.0;
     if constexpr (!LY::F64) {
-        double s0[NF];
+        if (!(DIM == 3 && NS && P.quirks == 0)) {
+            double s0[NF];
 #pragma unroll
-        for (int f = 0; f < NF; ++f) s0[f] = __ldg(a.u + f * Ndof + (long long)e * ND);
-        pref = primitives<DIM, double>(s0, gamma, gm1).dp;
+            for (int f = 0; f < NF; ++f) s0[f] = __ldg(a.u + f * Ndof + (long long)e * ND);
+            pref = primitives<DIM, double>(s0, gamma, gm1).dp;
+        }
     }
 
     // ---- own nodes: hoisted primitives (formed in FP64); largest |V|+c
@@ -914,16 +935,53 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
         const int no = face_node<DIM, NP>(lf, fa);
         const int4 t = __ldg(a.nbr + (long long)e * (2 * DIM) + lf);
         const long long go = (long long)e * ND + no;
-        if (t.x < 0) {   // boundary face: the element is Elem1; inviscid (Euler)
+        if (t.x < 0) {   // boundary face: the element is Elem1 (BdrFaceIntegrator.cpp:61-186)
             double sb[NF], nb[DIM];
-            Real fb[NF];
+            Real fb[NF], fv[NF];
 #pragma unroll
             for (int f = 0; f < NF; ++f) sb[f] = __ldg(a.u + f * Ndof + go);
 #pragma unroll
             for (int q = 0; q < DIM; ++q) nb[q] = __ldg(a.fnor + (long long)t.z * DIM + q);
-            boundary_flux<DIM, Real>(a.bcs[t.y], sb, nb, P, pref, fb);
+            const BcDev &bc = a.bcs[t.y];
+            boundary_flux<DIM, Real>(bc, sb, nb, P, pref, fb);
 #pragma unroll
-            for (int f = 0; f < NF; ++f) sF[f * NFI + it] = -(aw * fb[f]);
+            for (int f = 0; f < NF; ++f) fv[f] = 0;
+            if constexpr (NS) {
+                // viscous boundary flux (ComputeBdrFaceViscousFlux): Fv(inner state,
+                // inner gradients) . n for the no-slip walls and supersonic outflow;
+                // the other accepted types evaluate Fv with zero gradients, i.e. 0
+                if (bc.type == BC_NOSLIP_ADIABATIC || bc.type == BC_NOSLIP_ISOTHERMAL || bc.type == BC_OUTFLOW) {
+                    if constexpr (VC) {
+                        // n = sgo * row lf/2 of adj(J): Fv . n is a signed row of adj * Fv^T
+                        const int dd = lf >> 1;
+                        const Real sgo = (lf & 1) ? Real(1) : Real(-1);
+#pragma unroll
+                        for (int f = 1; f < NF; ++f) fv[f] = sgo * __ldg(grad + (dd * (NF - 1) + f - 1) * Ndof + go);
+                    } else {
+                        const Prim<DIM, Real> q = load_prim<DIM, ND, Real>(sH, no);
+                        Real dq[DIM][NF], nr[DIM];
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) {
+                            nr[d] = Real(nb[d]);
+#pragma unroll
+                            for (int f = 0; f < NF; ++f) dq[d][f] = __ldg(grad + (d * NF + f) * Ndof + go);
+                        }
+                        viscous_flux<DIM, Real>(q.rho, q.rrho, q.v, Real(0.5) * q.rbeta * q.rho, dq, P,
+                                                [&](int f, int cc, Real val) { fv[f] += val * nr[cc]; });
+                    }
+                    if (bc.type == BC_NOSLIP_ADIABATIC) {   // NoSlipAdiabWallBdrFaceIntegrator.cpp:17-31
+                        double nn = 0.0;
+#pragma unroll
+                        for (int q = 0; q < DIM; ++q) nn += nb[q] * nb[q];
+                        Real e = 0;
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) e += Real(bc.wall_vel[d]) * fv[1 + d];
+                        fv[NF - 1] = e + Real(bc.heat_flux * sqrt(nn));
+                    }
+                }
+            }
+#pragma unroll
+            for (int f = 0; f < NF; ++f) sF[f * NFI + it] = aw * (fv[f] - fb[f]);
             continue;
         }
         const long long gn = (long long)t.x * ND + face_node<DIM, NP>(t.y, fa);
@@ -1154,6 +1212,62 @@ rhs_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_consta
 //
 // The element function uses __syncthreads: every thread of the CTA calls it
 // with the same control flow (n = node, sElem = this element's area).
+// BR1 lifting at a boundary face node (LiftingBR1.cpp:311-407 with
+// ComputeBdrFaceLiftingFlux): the gradient receives lf * nor / (w0 J) with
+//   default: lf = 1/2 (v(outer state) - v1) (BdrFaceIntegrator.cpp:274-281),
+//            the outer state formed from the trace itself (the reference forms
+//            it from Entropy2Conserv(v1), the same state up to rounding);
+//            reference mode (Q12): Entropy2Conserv's `vel /= beta` wraps v1, so
+//            the middle entries of v1 in the jump are velocities;
+//   no-slip walls: lf = v_wall - v1, v_wall = (v1_0, V_wall b, -b) with b = beta1
+//            (adiabatic) or 1 / (R_gas T_wall) (NoSlip*WallBdrFaceIntegrator.cpp).
+// The element's jump is 1/2 (vn - v1), so vn = v1 + 2 lf is returned (entropy
+// variables of the lift's working form: absolute in FP64, relative to the
+// element's node 0 in FP32 with absolute middle entries).
+template <int DIM, typename W>
+__device__ __forceinline__ void boundary_lift_trace(const ElemIO &a, const PhysParams &P, const EntropyRef &R,
+                                                    long long g, const int4 t, W *vn) {
+    constexpr int NF = DIM + 2;
+    constexpr bool F64 = sizeof(W) == 8;
+    const BcDev &bc = a.bcs[t.y];
+    double s1[NF], nb[DIM], nn = 0.0;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) s1[f] = __ldg(a.u + f * a.Ndof + g);
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) {
+        nb[q] = __ldg(a.fnor + (long long)t.z * DIM + q);
+        nn += nb[q] * nb[q];
+    }
+    nn = sqrt(nn);
+    W v1[NF];
+    if constexpr (F64) conserv2entropy<DIM, double>(s1, P, reinterpret_cast<double *>(v1));
+    else conserv2entropy_rel<DIM>(s1, P, R, reinterpret_cast<float *>(v1));
+    const double rr = 1.0 / s1[0];
+    if (bc.type == BC_NOSLIP_ADIABATIC || bc.type == BC_NOSLIP_ISOTHERMAL) {
+        double vv = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) vv += (s1[1 + d] * rr) * (s1[1 + d] * rr);
+        const double beta1 = s1[0] * rcp(P.gammaM1 * (s1[NF - 1] - s1[0] * (0.5 * vv)));
+        const bool adiab = bc.type == BC_NOSLIP_ADIABATIC;
+        const double b = adiab ? beta1 : bc.vT;
+        vn[0] = v1[0];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) vn[1 + d] = W(2.0 * (bc.wall_vel[d] * b)) - v1[1 + d];
+        vn[NF - 1] = adiab ? v1[NF - 1] : W(2.0 * (F64 ? -bc.vT : R.beta - bc.vT)) - v1[NF - 1];
+        return;
+    }
+    double c[NF], s2[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) c[f] = s1[f];
+    bc_outer_state<DIM>(bc, c, nb, nn, P, s2);
+    if constexpr (F64) conserv2entropy<DIM, double>(s2, P, reinterpret_cast<double *>(vn));
+    else conserv2entropy_rel<DIM>(s2, P, R, reinterpret_cast<float *>(vn));
+    if (P.quirks == 0) {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) vn[1 + d] += v1[1 + d] - W(s1[1 + d] * rr);
+    }
+}
+
 template <int DIM, int NP, typename W, bool VC>
 __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &P, int e, bool active,
                                              const W *sT, W *sElem, int n) {
@@ -1206,15 +1320,19 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
             const int lf = it / NFN, fa = it - lf * NFN;
             no[k] = face_node<DIM, NP>(lf, fa);
             const int4 t = __ldg(a.nbr + (long long)e * (2 * DIM) + lf);
+#pragma unroll
+            for (int q = 0; q < DIM; ++q) nor[k][q] = W(__ldg(a.fnor + (long long)t.z * DIM + q));
+            own1[k] = (t.w == 0);
+            if (t.x < 0) {
+                boundary_lift_trace<DIM, W>(a, P, R, e * (long long)ND + no[k], t, vn[k]);
+                continue;
+            }
             const long long gn = (long long)t.x * ND + face_node<DIM, NP>(t.y, fa);
             double sn[NF];
 #pragma unroll
             for (int f = 0; f < NF; ++f) sn[f] = __ldg(a.u + f * Ndof + gn);
             if constexpr (F64) conserv2entropy<DIM, double>(sn, P, reinterpret_cast<double *>(vn[k]));
             else conserv2entropy_rel<DIM>(sn, P, R, reinterpret_cast<float *>(vn[k]));
-#pragma unroll
-            for (int q = 0; q < DIM; ++q) nor[k][q] = W(__ldg(a.fnor + (long long)t.z * DIM + q));
-            own1[k] = (t.w == 0);
         }
     }
     __syncthreads();   // tables and entropy variables complete
@@ -1345,6 +1463,7 @@ lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_
     io.fnor = m.fnor;
     io.Ndof = m.Ndof;
     io.E = m.E;
+    io.bcs = m.bcs;
     lift_element<DIM, NP, Out, VC>(io, P, active ? e_raw : m.E - 1, active, smem,
                                smem + S::TAB + el * LiftLayout<DIM, NP>::PER_ELEM, n);
 }

@@ -193,11 +193,6 @@ inline prandtl_status validate_mesh(const prandtl_mesh_desc *md, std::vector<int
     return PRANDTL_OK;
 }
 
-inline bool has_boundary(const prandtl_mesh_desc *md) {
-    for (int f = 0; f < md->num_faces; ++f)
-        if (md->face_elems[4 * f + 2] < 0) return true;
-    return false;
-}
 
 // Device copy of the boundary conditions (BcDev has prandtl_bc's layout).
 // Flow direction of SubsonicInflowPtTtAng (SubsonicInflowPtTtAngBdrFaceIntegrator.cpp
@@ -229,6 +224,9 @@ inline std::vector<BcDev> device_bcs(const prandtl_config *cfg, int dim) {
         o.Tt = b.Tt;
         o.cp = b.cp;
         inflow_direction(dim, b.theta, b.phi, o.vc);
+        for (int d = 0; d < 3; ++d) o.wall_vel[d] = b.wall_vel[d];
+        o.heat_flux = b.heat_flux;
+        o.vT = b.type == PRANDTL_BC_NOSLIP_ISOTHERMAL ? 1.0 / (cfg->R_gas * b.wall_T) : 0.0;
     }
     return out;
 }
@@ -238,7 +236,7 @@ inline prandtl_status check_bcs(const prandtl_config *cfg, int dim, std::string 
     for (int k = 0; k < cfg->num_bcs; ++k) {
         const prandtl_bc &b = cfg->bcs[k];
         const std::string tag = "boundary condition " + std::to_string(k);
-        if (b.type < PRANDTL_BC_STATE || b.type > PRANDTL_BC_INFLOW_PTTT) {
+        if (b.type < PRANDTL_BC_STATE || b.type > PRANDTL_BC_NOSLIP_ISOTHERMAL) {
             msg = tag + ": unknown type";
             return PRANDTL_EINVAL;
         }
@@ -254,6 +252,34 @@ inline prandtl_status check_bcs(const prandtl_config *cfg, int dim, std::string 
         if (b.type == PRANDTL_BC_INFLOW_PTTT && !(b.pt > 0.0 && b.Tt > 0.0 && b.cp > 0.0)) {
             msg = tag + ": pt, Tt and cp must be positive";
             return PRANDTL_EINVAL;
+        }
+        if (b.type == PRANDTL_BC_NOSLIP_ISOTHERMAL && !(b.wall_T > 0.0 && cfg->R_gas > 0.0)) {
+            msg = tag + ": wall temperature and R_gas must be positive";
+            return PRANDTL_EINVAL;
+        }
+    }
+    return PRANDTL_OK;
+}
+
+// The Navier-Stokes form has no treatment for the slip wall, symmetry and
+// pt/Tt inflow (the reference defines none for the first two), and reference
+// mode has no defined Riemann-invariant lifting: RiemannInvariantBdrFaceIntegrator
+// normalises the integrator's face normal, which only its face pass sets.
+// Checks the conditions boundary faces use (after validate_mesh).
+inline prandtl_status check_viscous_bcs(const prandtl_mesh_desc *md, const prandtl_config *cfg, std::string &msg) {
+    if (!cfg->parabolic) return PRANDTL_OK;
+    for (int f = 0; f < md->num_faces; ++f) {
+        const int *fe = md->face_elems + 4 * f;
+        if (fe[2] >= 0) continue;
+        const int t = cfg->bcs[fe[3]].type;
+        const std::string tag = "boundary condition " + std::to_string(fe[3]);
+        if (t == PRANDTL_BC_SLIP_WALL || t == PRANDTL_BC_SYMMETRY || t == PRANDTL_BC_INFLOW_PTTT) {
+            msg = tag + ": slip wall, symmetry and pt/Tt inflow have no viscous treatment (parabolic = 1)";
+            return PRANDTL_EUNSUPPORTED;
+        }
+        if (cfg->quirks == 0 && t == PRANDTL_BC_RIEMANN) {
+            msg = tag + ": the reference's Riemann-invariant lifting is undefined (use quirks = 1)";
+            return PRANDTL_EUNSUPPORTED;
         }
     }
     return PRANDTL_OK;

@@ -204,10 +204,7 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
         std::string msg;
         prandtl_status vst = check_bcs(cfg, md->dim, msg);
         if (vst == PRANDTL_OK) vst = validate_mesh(md, nbr, msg, cfg->num_bcs);
-        if (vst == PRANDTL_OK && cfg->parabolic && has_boundary(md)) {
-            msg = "boundary faces are supported for Euler (parabolic = 0)";
-            vst = PRANDTL_EUNSUPPORTED;
-        }
+        if (vst == PRANDTL_OK) vst = check_viscous_bcs(md, cfg, msg);
         if (vst == PRANDTL_OK && cfg->parabolic && cfg->quirks != 0) vst = check_face_normals(md, msg);
         if (vst != PRANDTL_OK) return fail(nullptr, vst, msg);
     }

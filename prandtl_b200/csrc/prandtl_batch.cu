@@ -472,10 +472,7 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, 
     std::string msg;
     prandtl_status st = check_bcs(cfg, md->dim, msg);
     if (st == PRANDTL_OK) st = validate_mesh(md, nbr, msg, cfg->num_bcs);
-    if (st == PRANDTL_OK && cfg->parabolic && has_boundary(md)) {
-        msg = "boundary faces are supported for Euler (parabolic = 0)";
-        st = PRANDTL_EUNSUPPORTED;
-    }
+    if (st == PRANDTL_OK) st = check_viscous_bcs(md, cfg, msg);
     if (st != PRANDTL_OK) return bfail(b, st, msg);
     BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
     const int dim = md->dim, order = md->order, E = md->num_elements, F = md->num_faces;

@@ -56,16 +56,21 @@ def make_bcs(bcs):
     """ctypes array of prandtl_bc from [(type name, state or None, p or None), ...]:
     type names "state", "outflow", "slip_wall", "symmetry", "pressure_outflow",
     "riemann" (state = outer primitive state), "inflow_rv" (state = rho, V) and
-    "inflow_pttt" (second item a dict of pt, Tt, cp, theta, phi)."""
+    "inflow_pttt" (second item a dict of pt, Tt, cp, theta, phi), "noslip_adiabatic"
+    (dict of wall_vel, heat_flux) and "noslip_isothermal" (dict of wall_vel, wall_T)."""
     if not bcs:
         return None
     arr = (_lib.BC * len(bcs))()
     for k, b in enumerate(bcs):
         kind, state, p = (tuple(b) + (None, None))[:3]
         arr[k].type = _lib.BC_TYPES[kind]
-        if isinstance(state, dict):   # inflow_pttt: pt, Tt, cp, theta, phi
+        if isinstance(state, dict):   # inflow_pttt, noslip_*: named fields
             for name, v in state.items():
-                setattr(arr[k], name, float(v))
+                if name == "wall_vel":
+                    for d, x in enumerate(v):
+                        arr[k].wall_vel[d] = float(x)
+                else:
+                    setattr(arr[k], name, float(v))
         else:
             for f, v in enumerate(state if state is not None else []):
                 arr[k].state[f] = float(v)

@@ -22,6 +22,8 @@ def normalized_error(g, r, nf):
     """
     g = np.asarray(g).reshape(nf, -1)
     r = np.asarray(r).reshape(nf, -1)
+    if not (np.isfinite(g).all() and np.isfinite(r).all()):
+        return float("inf")   # a NaN must never compare as small
     out = []
     for f in range(nf):
         scale = np.maximum(np.abs(r[f]), np.abs(r[f]).max())

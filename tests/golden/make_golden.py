@@ -62,7 +62,36 @@ CHAR_BCS = {2: [("riemann", [1.25, 0.35, -0.1, 1.6]), ("inflow_rv", [1.15, 0.45,
             3: [("riemann", [1.25, 0.35, -0.1, 0.05, 1.6]), ("inflow_rv", [1.15, 0.45, -0.25, 0.15]),
                 ("riemann", [1.2, 1.8, 0.1, 0.0, 1.5]), ("outflow",)]}
 CHAR_SIDES = {2: [1, 0, 2, 3], 3: [1, 0, 2, 3, 0, 2]}
-BC_SETS = {"walls": (BOUNDARY_CASES, BCS, SIDES), "char": (CHAR_CASES, CHAR_BCS, CHAR_SIDES)}
+
+# Navier-Stokes with boundary faces (parabolic = 1): no-slip walls (a moving
+# adiabatic lid with a heat flux, an isothermal wall), outflow and the
+# inflow/outflow types whose viscous boundary flux vanishes.  Slip wall,
+# symmetry and pt/Tt inflow have no viscous treatment in the reference, and its
+# Riemann-invariant lifting reads an unset face normal (NaN here), so the
+# golden cases leave those out.
+NS_BCS = {d: [("noslip_adiabatic", dict(wall_vel=[0.3, 0.0, 0.1][:d], heat_flux=0.01)),
+              ("noslip_isothermal", dict(wall_vel=[0.0, 0.05, 0.0][:d], wall_T=0.0045)),
+              ("outflow",),
+              ("state", [1.3, 0.5, 0.2, 2.9] if d == 2 else [1.3, 0.5, 0.2, -0.1, 2.9]),
+              ("pressure_outflow", None, 1.4),
+              ("riemann", [1.25, 0.35, -0.1, 1.6] if d == 2 else [1.25, 0.35, -0.1, 0.05, 1.6]),
+              ("inflow_rv", [1.15, 0.45, -0.25, 0.15][: d + 1])] for d in (2, 3)}
+NS_WALL_SIDES = {2: [3, 2, 1, 0], 3: [3, 2, 1, 0, 0, 1]}
+NS_CHAR_SIDES = {2: [2, 4, 6, 0], 3: [2, 4, 6, 0, 1, 3]}
+NS_WALL_CASES = [
+    ("ns2d_walls_n3_N3", 2, 3, 3, 0, 0.10, 31),
+    ("ns2d_walls_blend_n2_N4", 2, 2, 4, 1, 0.30, 32),
+    ("ns3d_walls_n2_N2", 3, 2, 2, 0, 0.10, 33),
+    ("ns3d_walls_blend_n2_N3", 3, 2, 3, 1, 0.30, 34),
+]
+NS_CHAR_CASES = [
+    ("ns2d_char_n3_N2", 2, 3, 2, 0, 0.10, 41),
+    ("ns3d_char_n2_N3", 3, 2, 3, 1, 0.30, 42),
+]
+# name -> (cases, BC tables, sides, parabolic)
+BC_SETS = {"walls": (BOUNDARY_CASES, BCS, SIDES, 0), "char": (CHAR_CASES, CHAR_BCS, CHAR_SIDES, 0),
+           "ns_walls": (NS_WALL_CASES, NS_BCS, NS_WALL_SIDES, 1),
+           "ns_char": (NS_CHAR_CASES, NS_BCS, NS_CHAR_SIDES, 1)}
 
 
 def bc_example(kind, dim):
@@ -70,7 +99,7 @@ def bc_example(kind, dim):
     "riemann_supersonic" is the Riemann condition with a supersonic outer state."""
     if kind == "riemann_supersonic":
         return CHAR_BCS[dim][2 if dim == 3 else 3]
-    for bcs in (BCS[dim], CHAR_BCS[dim], [PTTT]):
+    for bcs in (BCS[dim], CHAR_BCS[dim], [PTTT], NS_BCS[dim]):
         for b in bcs:
             if b[0] == kind:
                 return b
@@ -97,16 +126,16 @@ def main():
         out[f"{name}/u"] = u
         out[f"{name}/dudt"] = r["dudt"]
         out[f"{name}/alpha"] = r["alpha"]
-    for bcases, bcs, sides in BC_SETS.values():
+    for bcases, bcs, sides, par in BC_SETS.values():
         for name, dim, n, order, bl, amp, seed in bcases:
             mesh, A, u = case_inputs(dim, n, order, amp, seed, bcs=sides[dim])
-            r = pyoracle.RefOperator(mesh, blending=bl, bcs=bcs[dim], **PHYS).rhs(u, want_alpha=True)
+            r = pyoracle.RefOperator(mesh, parabolic=par, blending=bl, bcs=bcs[dim], **PHYS).rhs(u, want_alpha=True)
             out[f"{name}/affine"] = A
             out[f"{name}/u"] = u
             out[f"{name}/dudt"] = r["dudt"]
             out[f"{name}/alpha"] = r["alpha"]
     np.savez_compressed(os.path.join(HERE, "reference_rhs.npz"), **out)
-    print(f"wrote {len(CASES) + len(BOUNDARY_CASES) + len(CHAR_CASES)} cases")
+    print(f"wrote {len(CASES) + sum(len(v[0]) for v in BC_SETS.values())} cases")
 
 
 if __name__ == "__main__":

@@ -128,8 +128,9 @@ def test_face_normals_must_match_the_metrics_in_fixed_navier_stokes(lib):
 
 
 def test_boundary_tables_validated_before_touching_the_device(lib):
-    """Boundary faces {e1, l1, -1, bc}: a bad BC index or type is EINVAL, boundary
-    faces in the Navier-Stokes form are EUNSUPPORTED, all before device work."""
+    """Boundary faces {e1, l1, -1, bc}: a bad BC index, type or datum is EINVAL;
+    Navier-Stokes with a condition that has no viscous treatment is
+    EUNSUPPORTED; all before device work."""
     from prandtl_b200 import _lib
     from prandtl_b200.mesh import periodic_box
     from prandtl_b200.operator import make_config
@@ -142,16 +143,24 @@ def test_boundary_tables_validated_before_touching_the_device(lib):
     assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EINVAL
     assert b"boundary condition" in lib.prandtl_last_error(None)
     cfg = make_config(bcs=[("outflow",)])
-    cfg._bcs[0].type = 9
+    cfg._bcs[0].type = 42
     assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EINVAL
     assert b"unknown type" in lib.prandtl_last_error(None)
     cfg = make_config(bcs=[("state", [0.0, 0.1, 0.0, 2.5])])
     assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EINVAL
-    cfg = make_config(bcs=[("outflow",)], parabolic=True)
+    for kind in ("slip_wall", "symmetry"):   # no viscous treatment in the reference
+        cfg = make_config(bcs=[(kind,)], parabolic=True)
+        assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EUNSUPPORTED
+        assert b"viscous" in lib.prandtl_last_error(None)
+    cfg = make_config(bcs=[("riemann", [1.2, 0.3, 0.0, 1.5])], parabolic=True, quirks="reference")
     assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EUNSUPPORTED
-    assert b"Euler" in lib.prandtl_last_error(None)
-    cfg = make_config(bcs=[("outflow",)])
-    st = lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h))
-    assert st in (_lib.PRANDTL_ECUDA, _lib.PRANDTL_OK)
-    if st == _lib.PRANDTL_OK:
-        lib.prandtl_destroy(h)
+    cfg = make_config(bcs=[("noslip_isothermal", dict(wall_T=0.0))], parabolic=True)
+    assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EINVAL
+    for kw in (dict(bcs=[("outflow",)]), dict(bcs=[("outflow",)], parabolic=True),
+               dict(bcs=[("noslip_adiabatic", dict(wall_vel=[1.0, 0.0]))], parabolic=True),
+               dict(bcs=[("riemann", [1.2, 0.3, 0.0, 1.5])], parabolic=True, quirks="fixed")):
+        cfg = make_config(**kw)
+        st = lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h))
+        assert st in (_lib.PRANDTL_ECUDA, _lib.PRANDTL_OK), kw
+        if st == _lib.PRANDTL_OK:
+            lib.prandtl_destroy(h)

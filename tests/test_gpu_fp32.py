@@ -43,6 +43,19 @@ def test_fp32_rhs_tgv(order):
     assert max(errs) <= 2e-3, errs
 
 
+@pytest.mark.parametrize("dim", [2, 3])
+def test_fp32_rhs_reference_mode_navier_stokes(dim):
+    """Reference-mode NS (gradient form, the reference's defects kept) in FP32."""
+    mesh = periodic_box(dim, 3, 3, 0.0, 1.0, affine=np.eye(dim) + 0.1 * np.eye(dim, k=1))
+    base = cases.free_stream(mesh, rho=1.2, vel=[0.4, -0.3, 0.2][:dim], p=1.5)
+    u = cases.perturbed(mesh, base, amp=0.1, seed=4)
+    kw = dict(parabolic=True, mu=0.01, Pr=0.71, quirks="reference")
+    d64, d32 = np.empty_like(u), np.empty_like(u)
+    _op(mesh, **kw).Mult(u, d64)
+    _op(mesh, precision="fp32", **kw).Mult(u, d32)
+    assert max(rel_l2(d32, d64, mesh.num_fields)) <= 2e-3
+
+
 def test_fp32_rhs_euler_blended():
     mesh = periodic_box(2, 16, 3, -1.0, 1.0)
     u = cases.kelvin_helmholtz(mesh)

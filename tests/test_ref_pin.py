@@ -92,19 +92,20 @@ def test_golden_fixtures_come_from_the_reference(oracle_mod):
 
 
 # ---------------------------------------------------------------- boundary faces
-GOLD_BDR = [(c, st) for st, (cs, _, _) in make_golden.BC_SETS.items() for c in cs]
+GOLD_BDR = [(c, st) for st, (cs, _, _, _) in make_golden.BC_SETS.items() for c in cs]
 
 
 @pytest.mark.parametrize("case,bset", GOLD_BDR, ids=[c[0] for c, _ in GOLD_BDR])
 def test_oracle_boundary_matches_reference_golden(oracle_mod, case, bset):
     """Boundary integrators (state, outflow, slip wall, symmetry, pressure outflow
     with the reference's Q9 aliasing, Riemann invariants with Q10, subsonic
-    inflows) against the reference's outputs."""
+    inflows; in the Navier-Stokes form the no-slip walls, BR1 boundary lifting
+    with Q12 and the viscous boundary fluxes) against the reference's outputs."""
     name, dim, n, order, bl, amp, seed = case
-    _, bcs, sides = make_golden.BC_SETS[bset]
+    _, bcs, sides, par = make_golden.BC_SETS[bset]
     mesh, _, u = make_golden.case_inputs(dim, n, order, amp, seed, bcs=sides[dim])
     gold = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_rhs.npz"))
-    o = oracle_mod.Oracle(mesh, blending=bl, quirks=0, bcs=bcs[dim], **make_golden.PHYS).rhs(u)
+    o = oracle_mod.Oracle(mesh, parabolic=par, blending=bl, quirks=0, bcs=bcs[dim], **make_golden.PHYS).rhs(u)
     assert normalized_error(o["dudt"], gold[f"{name}/dudt"], mesh.num_fields) <= 1e-13
 
 
@@ -129,3 +130,47 @@ def test_oracle_boundary_matches_reference_sources(oracle_mod, dim, order, kind)
     o = oracle_mod.Oracle(mesh, quirks=0, bcs=bcs).rhs(u)["dudt"]
     r = oracle_mod.RefOperator(mesh, quirks=0, bcs=bcs).rhs(u)["dudt"]
     assert normalized_error(o, r, mesh.num_fields) <= 1e-13
+
+
+NS_KINDS = ["noslip_adiabatic", "noslip_isothermal", "outflow", "state", "pressure_outflow", "inflow_rv"]
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("order", [1, 2, 4])
+@pytest.mark.parametrize("bl", [0, 1])
+@pytest.mark.parametrize("kind", NS_KINDS)
+def test_oracle_ns_boundary_matches_reference_sources(oracle_mod, dim, order, bl, kind):
+    """Navier-Stokes: one condition on every bounded side; lifting and viscous
+    boundary terms of the reference's integrators compiled from its sources."""
+    _ref(oracle_mod)
+    bcs = [make_golden.bc_example(kind, dim)]
+    sides = [0, 0, 0, 0] if dim == 2 else [0, 0, None, None, 0, 0]
+    mesh = periodic_box(dim, 2, order, 0.0, 1.0, bcs=sides, affine=np.eye(dim) + 0.1 * np.eye(dim, k=1))
+    base = cases.free_stream(mesh, rho=1.1, vel=[0.35, -0.2, 0.1][:dim], p=1.6)
+    u = cases.perturbed(mesh, base, amp=0.2, seed=order)
+    kw = dict(parabolic=1, blending=bl, quirks=0, bcs=bcs, **make_golden.PHYS)
+    o = oracle_mod.Oracle(mesh, **kw).rhs(u, want_grad=True)
+    r = oracle_mod.RefOperator(mesh, **kw).rhs(u, want_grad=True)
+    assert normalized_error(o["dudt"], r["dudt"], mesh.num_fields) <= 1e-13
+    assert normalized_error(o["grad"], r["grad"], mesh.num_fields * dim) <= 1e-13
+
+
+def test_oracle_rejects_ns_boundaries_without_viscous_treatment(oracle_mod):
+    mesh = periodic_box(2, 2, 2, 0.0, 1.0, bcs=[0, 0, None, None])
+    u = cases.free_stream(mesh)
+    for kind in ("slip_wall", "symmetry", "inflow_pttt"):
+        with pytest.raises(RuntimeError):
+            oracle_mod.Oracle(mesh, parabolic=1, bcs=[make_golden.bc_example(kind, 2)]).rhs(u)
+    with pytest.raises(RuntimeError):   # Q13: reference-mode Riemann lifting is undefined
+        oracle_mod.Oracle(mesh, parabolic=1, quirks=0, bcs=[make_golden.bc_example("riemann", 2)]).rhs(u)
+    oracle_mod.Oracle(mesh, parabolic=1, quirks=1, bcs=[make_golden.bc_example("riemann", 2)]).rhs(u)
+
+
+def test_reference_riemann_lifting_reads_an_unset_normal(oracle_mod):
+    """Q13 as observed: the reference's NS operator with a Riemann-invariant
+    boundary returns non-finite values (its lifting normalises a zero normal)."""
+    _ref(oracle_mod)
+    mesh = periodic_box(2, 2, 2, 0.0, 1.0, bcs=[0, 0, 0, 0])
+    u = cases.perturbed(mesh, cases.free_stream(mesh, rho=1.1, vel=[0.35, -0.2], p=1.6), amp=0.2, seed=1)
+    r = oracle_mod.RefOperator(mesh, parabolic=1, bcs=[make_golden.bc_example("riemann", 2)]).rhs(u)
+    assert not np.isfinite(r["dudt"]).all()
