@@ -188,6 +188,40 @@ const char *prandtl_last_error(const prandtl_handle *h);
 
 const char *prandtl_version(void);
 
+/* ---- Mesh ingestion (host only) ----
+ * Replaces the reference's mesh setup, Simulation.cpp:271-336: `new
+ * Mesh(file)` for MFEM v1.0 meshes (with a `nodes` section of L2_T1 corner
+ * nodes, MFEM's form of periodic meshes) and Gmsh 2.2 ASCII meshes,
+ * `UniformRefinement()` per `ser_ref_levels`, and "mesh_ordering": "Hilbert".
+ * Quadrilaterals / hexahedra, affine, of structured topology: each element's
+ * local frame is chosen so that neighbouring faces are aligned; other meshes
+ * get PRANDTL_EUNSUPPORTED with the reason in prandtl_mesh_last_error(). */
+typedef struct prandtl_mesh prandtl_mesh;
+prandtl_status prandtl_mesh_read(const char *path, int order, int refine_levels, int hilbert,
+                                 prandtl_mesh **out);
+/* Descriptor arrays, valid until prandtl_mesh_destroy.  Boundary faces are
+ * {elem1, lface1, -1, attribute - 1} until prandtl_mesh_set_boundary_conditions.
+ * hmin (may be NULL): smallest singular value of the element Jacobians, as
+ * MFEM's GetElementSize(e, 1). */
+prandtl_status prandtl_mesh_describe(const prandtl_mesh *m, prandtl_mesh_desc *desc, double *hmin);
+/* Boundary attribute of each descriptor face (0 for interior faces and for
+ * boundary faces no boundary element names), num_faces entries. */
+prandtl_status prandtl_mesh_face_attributes(const prandtl_mesh *m, int *attr);
+/* Element attributes, num_elements entries. */
+prandtl_status prandtl_mesh_element_attributes(const prandtl_mesh *m, int *attr);
+/* Boundary faces of attribute a (1..num_attributes) take BC index
+ * bc_of_attribute[a-1]; others take -1 (which prandtl_create rejects). */
+prandtl_status prandtl_mesh_set_boundary_conditions(prandtl_mesh *m, const int *bc_of_attribute,
+                                                    int num_attributes);
+/* Attribute of a Gmsh physical group by entity dimension and name, -1 if none
+ * (the reference's boundary names in "boundary_conditions"). */
+int prandtl_mesh_attribute(const prandtl_mesh *m, int entity_dim, const char *name);
+/* Physical coordinates of every node, [dim][E * (order+1)^dim], byNODES. */
+prandtl_status prandtl_mesh_node_coords(const prandtl_mesh *m, double *xyz);
+void prandtl_mesh_destroy(prandtl_mesh *m);
+/* Text of this thread's last mesh-function error. */
+const char *prandtl_mesh_last_error(void);
+
 /* ---- RHS without any memory allocation (no counterpart in the reference) ----
  * For callers that cannot call cudaMalloc: code that runs inside another
  * framework's memory pool, embeddings with a fixed device footprint, or code

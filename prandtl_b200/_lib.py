@@ -35,7 +35,11 @@ EXPORTS = ["prandtl_config_default", "prandtl_create", "prandtl_destroy", "prand
            "prandtl_batch_kernel_launches", "prandtl_batch_last_error",
            "prandtl_serve_create", "prandtl_serve_submit", "prandtl_serve_poll",
            "prandtl_serve_wait", "prandtl_serve_stats_get", "prandtl_serve_destroy",
-           "prandtl_serve_last_error"]
+           "prandtl_serve_last_error",
+           "prandtl_mesh_read", "prandtl_mesh_describe", "prandtl_mesh_face_attributes",
+           "prandtl_mesh_element_attributes", "prandtl_mesh_set_boundary_conditions",
+           "prandtl_mesh_attribute", "prandtl_mesh_node_coords", "prandtl_mesh_destroy",
+           "prandtl_mesh_last_error"]
 
 
 class MeshDesc(C.Structure):
@@ -160,6 +164,15 @@ def load():
         "prandtl_serve_stats_get": (ip, [vp, C.POINTER(ServeStats)]),
         "prandtl_serve_destroy": (ip, [vp]),
         "prandtl_serve_last_error": (C.c_char_p, [vp]),
+        "prandtl_mesh_read": (ip, [C.c_char_p, ip, ip, ip, C.POINTER(vp)]),
+        "prandtl_mesh_describe": (ip, [vp, mdp, dp]),
+        "prandtl_mesh_face_attributes": (ip, [vp, ipp]),
+        "prandtl_mesh_element_attributes": (ip, [vp, ipp]),
+        "prandtl_mesh_set_boundary_conditions": (ip, [vp, ipp, ip]),
+        "prandtl_mesh_attribute": (ip, [vp, ip, C.c_char_p]),
+        "prandtl_mesh_node_coords": (ip, [vp, dp]),
+        "prandtl_mesh_destroy": (None, [vp]),
+        "prandtl_mesh_last_error": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

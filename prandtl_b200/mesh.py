@@ -105,6 +105,8 @@ class Mesh:
     hmin: float               # min element size (MFEM GetElementSize(e, 1))
     nodes_1d: np.ndarray = field(default=None)
     weights_1d: np.ndarray = field(default=None)
+    face_attr: np.ndarray = field(default=None)   # (F,) boundary attribute per face (read meshes)
+    elem_attr: np.ndarray = field(default=None)   # (E,) element attribute (read meshes)
 
     @property
     def Np(self) -> int:
@@ -219,3 +221,60 @@ def periodic_box(dim: int, n, order: int, lo=0.0, hi=1.0, affine=None, bcs=None)
     return Mesh(dim=dim, order=order, n=n, elem_adj=elem_adj, elem_detj=elem_detj,
                 face_elems=face_elems, face_nor=face_nor, coords=coords, hmin=hmin,
                 nodes_1d=x1, weights_1d=w1)
+
+
+def read_mesh(path: str, order: int, refine: int = 0, hilbert: bool = False, boundary_conditions=None) -> Mesh:
+    """Read an MFEM v1.0 or Gmsh 2.2 ASCII mesh through the native reader
+    (``prandtl_mesh_read``: quadrilaterals / hexahedra, affine, aligned frames).
+
+    ``refine`` uniform refinements and ``hilbert`` element ordering follow the
+    reference's ``ser_ref_levels`` and ``"mesh_ordering": "Hilbert"``.
+    ``boundary_conditions`` maps a boundary attribute (int) or a Gmsh physical
+    name to a BC index; boundary faces default to BC index attribute - 1.
+    """
+    import ctypes as C
+    from . import _lib
+    L = _lib.load()
+    h = C.c_void_p()
+    st = L.prandtl_mesh_read(str(path).encode(), int(order), int(refine), int(bool(hilbert)), C.byref(h))
+    if st != _lib.PRANDTL_OK:
+        raise _lib.PrandtlError(st, L.prandtl_mesh_last_error().decode(errors="replace"))
+    try:
+        dim_probe = _lib.MeshDesc()
+        hmin = C.c_double()
+        L.prandtl_mesh_describe(h, C.byref(dim_probe), C.byref(hmin))
+        F = dim_probe.num_faces
+        fattr = np.zeros(F, dtype=np.int32)
+        L.prandtl_mesh_face_attributes(h, fattr.ctypes.data_as(C.POINTER(C.c_int)))
+        if boundary_conditions:
+            amax = int(fattr.max(initial=0))
+            table = np.full(max(amax, 1), -1, dtype=np.int32)
+            for a in range(1, amax + 1):
+                table[a - 1] = a - 1
+            for key, bc in boundary_conditions.items():
+                a = key if isinstance(key, (int, np.integer)) else \
+                    L.prandtl_mesh_attribute(h, dim_probe.dim - 1, str(key).encode())
+                if a < 1:
+                    raise KeyError(f"no boundary attribute named {key!r}")
+                if a > amax:
+                    continue
+                table[a - 1] = int(bc)
+            L.prandtl_mesh_set_boundary_conditions(h, table.ctypes.data_as(C.POINTER(C.c_int)), int(table.size))
+        d = _lib.MeshDesc()
+        L.prandtl_mesh_describe(h, C.byref(d), None)
+        dim, E = d.dim, d.num_elements
+        adj = np.ctypeslib.as_array(d.elem_adj, shape=(E * dim * dim,)).reshape(E, dim, dim).copy()
+        detj = np.ctypeslib.as_array(d.elem_detj, shape=(E,)).copy()
+        faces = np.ctypeslib.as_array(d.face_elems, shape=(F * 4,)).reshape(F, 4).copy()
+        nor = np.ctypeslib.as_array(d.face_nor, shape=(F * dim,)).reshape(F, dim).copy()
+        Np = order + 1
+        coords = np.empty((dim, E * Np ** dim))
+        L.prandtl_mesh_node_coords(h, coords.ctypes.data_as(C.POINTER(C.c_double)))
+        eattr = np.empty(E, dtype=np.int32)
+        L.prandtl_mesh_element_attributes(h, eattr.ctypes.data_as(C.POINTER(C.c_int)))
+    finally:
+        L.prandtl_mesh_destroy(h)
+    x, w = gauss_lobatto(order)
+    return Mesh(dim=dim, order=order, n=(E,), elem_adj=adj, elem_detj=detj, face_elems=faces.astype(np.int32),
+                face_nor=nor, coords=coords, hmin=float(hmin.value), nodes_1d=x, weights_1d=w,
+                face_attr=fattr, elem_attr=eattr)
