@@ -222,6 +222,29 @@ void prandtl_mesh_destroy(prandtl_mesh *m);
 /* Text of this thread's last mesh-function error. */
 const char *prandtl_mesh_last_error(void);
 
+/* ---- Checkpoint/resume and ParaView output (host only) ----
+ * The reference's checkpoint files (Simulation.cpp:1084-1116 save, :350-384
+ * load): <folder>/Cycle<ti>/checkpoint_cycle_<ti>.<rank, 8 digits>.chk, an MFEM
+ * GridFunction in text (L2_T1_<dim>D_P<order>, VDim dim+2), and
+ * checkpoint_cycle_<ti>.json with {"time", "cycle"} (rank 0 writes it).
+ * Values are written with 17 significant digits (exact round trip); the
+ * loader accepts byNODES and byVDIM orderings and checks the meta file's
+ * cycle.  u is byNODES, ndof nodes per field. */
+prandtl_status prandtl_checkpoint_save(const char *folder, int cycle, double time, int rank, int dim, int order,
+                                       long long ndof, const double *u);
+prandtl_status prandtl_checkpoint_load(const char *folder, int cycle, int rank, int dim, int order,
+                                       long long ndof, double *u, double *time);
+/* ParaView collection as the reference's ParaViewDataCollection writes it
+ * (Simulation.cpp:389-410, high-order output at the mesh order):
+ * <dir>/<name>/<name>.pvd and Cycle<6 digits>/{data.pvtu, proc000000.vtu} with
+ * VTK Lagrange cells and point fields Density, Horizontal/Vertical/Normal V,
+ * Pressure, Blending Coeff.  coords: [dim][Ndof] node coordinates (as
+ * prandtl_mesh_node_coords); alpha: per element or NULL; binary: base64 data. */
+prandtl_status prandtl_paraview_save(const char *dir, const char *name, int cycle, double time, int dim, int order,
+                                     int num_elements, const double *coords, const double *u, const double *alpha,
+                                     double gamma, int binary);
+const char *prandtl_io_last_error(void);
+
 /* ---- RHS without any memory allocation (no counterpart in the reference) ----
  * For callers that cannot call cudaMalloc: code that runs inside another
  * framework's memory pool, embeddings with a fixed device footprint, or code

@@ -39,7 +39,8 @@ EXPORTS = ["prandtl_config_default", "prandtl_create", "prandtl_destroy", "prand
            "prandtl_mesh_read", "prandtl_mesh_describe", "prandtl_mesh_face_attributes",
            "prandtl_mesh_element_attributes", "prandtl_mesh_set_boundary_conditions",
            "prandtl_mesh_attribute", "prandtl_mesh_node_coords", "prandtl_mesh_destroy",
-           "prandtl_mesh_last_error"]
+           "prandtl_mesh_last_error", "prandtl_checkpoint_save", "prandtl_checkpoint_load",
+           "prandtl_paraview_save", "prandtl_io_last_error"]
 
 
 class MeshDesc(C.Structure):
@@ -173,6 +174,11 @@ def load():
         "prandtl_mesh_node_coords": (ip, [vp, dp]),
         "prandtl_mesh_destroy": (None, [vp]),
         "prandtl_mesh_last_error": (C.c_char_p, []),
+        "prandtl_checkpoint_save": (ip, [C.c_char_p, ip, C.c_double, ip, ip, ip, C.c_longlong, dp]),
+        "prandtl_checkpoint_load": (ip, [C.c_char_p, ip, ip, ip, ip, C.c_longlong, dp, dp]),
+        "prandtl_paraview_save": (ip, [C.c_char_p, C.c_char_p, ip, C.c_double, ip, ip, ip, dp, dp, dp,
+                                       C.c_double, ip]),
+        "prandtl_io_last_error": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

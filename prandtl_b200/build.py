@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libprandtl_b200.so")
 SOURCES = (["dgsem_kernels.cu", "prandtl_api.cu", "prandtl_noalloc.cu", "prandtl_batch.cu", "prandtl_serve.cu",
-            "prandtl_mesh.cu"] +
+            "prandtl_mesh.cu", "prandtl_io.cu"] +
            sorted(os.path.basename(p) for p in glob.glob(os.path.join(CSRC, "dgsem_inst_*.cu"))))
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
