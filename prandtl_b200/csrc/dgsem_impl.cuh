@@ -637,16 +637,22 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 
     // ---- own nodes: hoisted primitives (formed in FP64); largest |V|+c
     double lam = 0.0;
-#pragma unroll 1
-    for (int k = 0; k < NPL; ++k) {
-        const int n = li + k * GS;
-        if (n < ND) {
-            double st[NF];
+    {
+        double st[NPL][NF];   // every load in flight before the first use
 #pragma unroll
-            for (int f = 0; f < NF; ++f) st[f] = __ldg(a.u + f * Ndof + (long long)e * ND + n);
-            const Prim<DIM, double> q = primitives<DIM, double>(st, gamma, gm1);
-            store_prim<DIM, ND, Real>(sH, n, q, pref);
-            lam = fmax(lam, q.lam);
+        for (int k = 0; k < NPL; ++k) {
+            const int n = li + k * GS;
+#pragma unroll
+            for (int f = 0; f < NF; ++f) st[k][f] = n < ND ? __ldg(a.u + f * Ndof + (long long)e * ND + n) : 1.0;
+        }
+#pragma unroll
+        for (int k = 0; k < NPL; ++k) {
+            const int n = li + k * GS;
+            if (n < ND) {
+                const Prim<DIM, double> q = primitives<DIM, double>(st[k], gamma, gm1);
+                store_prim<DIM, ND, Real>(sH, n, q, pref);
+                lam = fmax(lam, q.lam);
+            }
         }
     }
     if (a.lambda) {
@@ -745,16 +751,26 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 
     // ---- NS: contravariant viscous flux of every own node (flux_mat = adj * Fv^T, :632)
     if constexpr (NS && VC) {
-        // formed by the lifting: rows f = 1..NF-1 of adj * Fv^T (the mass row is zero)
-#pragma unroll 1
+        // formed by the lifting: rows f = 1..NF-1 of adj * Fv^T (the mass row is zero);
+        // each lane's loads are all issued before the stores
+        Real vrow[NPL][DIM][NF - 1];
+#pragma unroll
+        for (int k = 0; k < NPL; ++k) {
+            const int n = li + k * GS;
+#pragma unroll
+            for (int r = 0; r < DIM; ++r)
+#pragma unroll
+                for (int f = 1; f < NF; ++f)
+                    vrow[k][r][f - 1] = n < ND ? __ldg(grad + (r * (NF - 1) + f - 1) * Ndof + (long long)e * ND + n) : Real(0);
+        }
+#pragma unroll
         for (int k = 0; k < NPL; ++k) {
             const int n = li + k * GS;
             if (n < ND) {
 #pragma unroll
                 for (int r = 0; r < DIM; ++r)
 #pragma unroll
-                    for (int f = 1; f < NF; ++f)
-                        sV[(r * NF + f) * ND + n] = __ldg(grad + (r * (NF - 1) + f - 1) * Ndof + (long long)e * ND + n);
+                    for (int f = 1; f < NF; ++f) sV[(r * NF + f) * ND + n] = vrow[k][r][f - 1];
             }
         }
     } else if constexpr (NS) {
@@ -928,20 +944,56 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
             for (int f = 0; f < NF; ++f) acc[k][f] = fv[k][f] * alpha + acc[k][f];
     }
 
-    // ---- surface fluxes of the element's own faces; neighbour traces from global/L2
+    // ---- surface fluxes of the element's own faces; neighbour traces from global/L2.
+    //      For N >= 3 a lane's face items go in pairs: both items' loads are in
+    //      flight before either is evaluated.
     const Real aw = Real(1.0 / (double(sW[0]) * J));
-    for (int it = li; it < NFI; it += GS) {
+    struct FaceIn {
+        int4 t;
+        double s[NF];                  // neighbour trace (interior face) or own trace (boundary)
+        double nb[DIM];                // scaled normal
+        Real vo[NF - 1], vn[NF - 1];   // VC form: own / neighbour contravariant viscous rows
+    };
+    auto face_load = [&](int it, FaceIn &x) {
+        const int lf = it / NFN, fa = it - lf * NFN;
+        const long long go = (long long)e * ND + face_node<DIM, NP>(lf, fa);
+        x.t = __ldg(a.nbr + (long long)e * (2 * DIM) + lf);
+        const long long gs = x.t.x < 0 ? go : (long long)x.t.x * ND + face_node<DIM, NP>(x.t.y, fa);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) x.s[f] = __ldg(a.u + f * Ndof + gs);
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) x.nb[q] = __ldg(a.fnor + (long long)x.t.z * DIM + q);
+        if constexpr (NS && VC) {
+            const int dd = lf >> 1, dn = x.t.x < 0 ? dd : x.t.y >> 1;
+#pragma unroll
+            for (int f = 1; f < NF; ++f) {
+                x.vo[f - 1] = __ldg(grad + (dd * (NF - 1) + f - 1) * Ndof + go);
+                x.vn[f - 1] = __ldg(grad + (dn * (NF - 1) + f - 1) * Ndof + gs);
+            }
+        }
+    };
+    constexpr int FB = NP >= 4 ? 2 : 1;   // face items whose loads go together
+    for (int it0 = li; it0 < NFI; it0 += FB * GS) {
+      FaceIn xin[FB];
+#pragma unroll
+      for (int q2 = 0; q2 < FB; ++q2)
+          if (it0 + q2 * GS < NFI) face_load(it0 + q2 * GS, xin[q2]);
+#pragma unroll
+      for (int q2 = 0; q2 < FB; ++q2) {
+        const int it = it0 + q2 * GS;
+        if (it >= NFI) break;
+        const FaceIn &x = xin[q2];
         const int lf = it / NFN, fa = it - lf * NFN;
         const int no = face_node<DIM, NP>(lf, fa);
-        const int4 t = __ldg(a.nbr + (long long)e * (2 * DIM) + lf);
+        const int4 t = x.t;
         const long long go = (long long)e * ND + no;
         if (t.x < 0) {   // boundary face: the element is Elem1 (BdrFaceIntegrator.cpp:61-186)
             double sb[NF], nb[DIM];
             Real fb[NF], fv[NF];
 #pragma unroll
-            for (int f = 0; f < NF; ++f) sb[f] = __ldg(a.u + f * Ndof + go);
+            for (int f = 0; f < NF; ++f) sb[f] = x.s[f];
 #pragma unroll
-            for (int q = 0; q < DIM; ++q) nb[q] = __ldg(a.fnor + (long long)t.z * DIM + q);
+            for (int q = 0; q < DIM; ++q) nb[q] = x.nb[q];
             const BcDev &bc = a.bcs[t.y];
             boundary_flux<DIM, Real>(bc, sb, nb, P, pref, fb);
 #pragma unroll
@@ -953,10 +1005,9 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 if (bc.type == BC_NOSLIP_ADIABATIC || bc.type == BC_NOSLIP_ISOTHERMAL || bc.type == BC_OUTFLOW) {
                     if constexpr (VC) {
                         // n = sgo * row lf/2 of adj(J): Fv . n is a signed row of adj * Fv^T
-                        const int dd = lf >> 1;
                         const Real sgo = (lf & 1) ? Real(1) : Real(-1);
 #pragma unroll
-                        for (int f = 1; f < NF; ++f) fv[f] = sgo * __ldg(grad + (dd * (NF - 1) + f - 1) * Ndof + go);
+                        for (int f = 1; f < NF; ++f) fv[f] = sgo * x.vo[f - 1];
                     } else {
                         const Prim<DIM, Real> q = load_prim<DIM, ND, Real>(sH, no);
                         Real dq[DIM][NF], nr[DIM];
@@ -995,10 +1046,10 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
             if constexpr (OWN_STATE) so[f] = __ldg(a.u + f * Ndof + go);
-            sn[f] = __ldg(a.u + f * Ndof + gn);
+            sn[f] = x.s[f];
         }
 #pragma unroll
-        for (int q = 0; q < DIM; ++q) nor[q] = Real(__ldg(a.fnor + (long long)t.z * DIM + q));
+        for (int q = 0; q < DIM; ++q) nor[q] = Real(x.nb[q]);
         Prim<DIM, Real> po = load_prim<DIM, ND, Real>(sH, no);
         const Prim<DIM, double> pn64 = primitives<DIM, double>(sn, gamma, gm1);
         Prim<DIM, Real> pn = cast_prim<DIM, Real>(pn64, pref);
@@ -1009,12 +1060,11 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
             // affine elements the outward scaled normal of local face lf is
             // (lf odd ? +1 : -1) times row lf/2 of adj(J) (Nanson's formula), so
             // Fv . n_out is a signed row of adj * Fv^T.  fn is taken along nor.
-            const int dd = lf >> 1, dn = t.y >> 1;
             const Real sgo = (lf & 1) ? Real(1) : Real(-1), sgn = (t.y & 1) ? Real(1) : Real(-1);
 #pragma unroll
             for (int f = 1; f < NF; ++f) {
-                const Real vo = __ldg(grad + (dd * (NF - 1) + f - 1) * Ndof + go);
-                const Real vn = __ldg(grad + (dn * (NF - 1) + f - 1) * Ndof + gn);
+                const Real vo = x.vo[f - 1];
+                const Real vn = x.vn[f - 1];
                 const Real avg = Real(0.5) * (sgo * vo - sgn * vn);
                 fn[f] = own_is_1 ? avg : -avg;
             }
@@ -1060,69 +1110,86 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
             face_flux<DIM, Real>(mn, pn, mo, po, nor, gm1i, P.quirks == 0, P.dissipation != 0, flux);
 #pragma unroll
         for (int f = 0; f < NF; ++f) sF[f * NFI + it] = aw * (own_is_1 ? (fn[f] - flux[f]) : (flux[f] - fn[f]));
+      }
     }
     group_sync<GS>(gid);
 
-    // ---- gather face terms, epilogue (FP64 state update)
+    // ---- gather face terms, epilogue (FP64 state update).  The stage's global
+    //      operands of a lane's nodes (up to 4) are in flight before the gather.
     if (!active) return;
+    const int mode = a.mode;
+    const bool need_b = (mode == EPI_LSRK && a.rkA != 0.0) || mode == EPI_SSP2 || mode == EPI_SSP3;
+    const double *pb = mode == EPI_LSRK ? a.du : a.x0;
+    constexpr int KB = NPL <= 4 ? NPL : 1;   // nodes whose operands load together
 #pragma unroll
-    for (int k = 0; k < NPL; ++k) {
-        const int n = li + k * GS;
-        if (n >= ND) continue;
-        int c[3];
-        node_coords<NP>(n, c);
+    for (int k0 = 0; k0 < NPL; k0 += KB) {
+        double ua[KB][NF], ub[KB][NF];
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            int lf = -1;
-            if (c[d] == 0) lf = 2 * d;
-            else if (c[d] == NP - 1) lf = 2 * d + 1;
-            if (lf >= 0) {
-                const int it = lf * NFN + face_tangential<DIM, NP>(d, c);
+        for (int kk = 0; kk < KB; ++kk) {
+            const int n = li + (k0 + kk) * GS;
+            const long long gnode = (long long)e * ND + n;
 #pragma unroll
-                for (int f = 0; f < NF; ++f) acc[k][f] += sF[f * NFI + it];
+            for (int f = 0; f < NF; ++f) {
+                const long long g = f * Ndof + gnode;
+                ua[kk][f] = (k0 + kk < NPL && n < ND && mode != EPI_STORE) ? __ldg(a.u + g) : 0.0;
+                ub[kk][f] = (k0 + kk < NPL && n < ND && need_b) ? pb[g] : 0.0;
             }
         }
-        const long long gnode = (long long)e * ND + n;
-        switch (a.mode) {
-        case EPI_STORE:
 #pragma unroll
-            for (int f = 0; f < NF; ++f) a.dudt[f * Ndof + gnode] = double(acc[k][f]);
-            break;
-        case EPI_LSRK:
+        for (int kk = 0; kk < KB; ++kk) {
+            const int k = k0 + kk;
+            const int n = li + k * GS;
+            if (k >= NPL || n >= ND) continue;
+            int c[3];
+            node_coords<NP>(n, c);
 #pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const long long g = f * Ndof + gnode;
-                const double L = double(acc[k][f]);
-                const double dv = (a.rkA == 0.0) ? a.dt * L : a.rkA * a.du[g] + a.dt * L;
-                a.du[g] = dv;
-                a.u_out[g] = __ldg(a.u + g) + a.rkB * dv;
+            for (int d = 0; d < DIM; ++d) {
+                int lf = -1;
+                if (c[d] == 0) lf = 2 * d;
+                else if (c[d] == NP - 1) lf = 2 * d + 1;
+                if (lf >= 0) {
+                    const int it = lf * NFN + face_tangential<DIM, NP>(d, c);
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) acc[k][f] += sF[f * NFI + it];
+                }
             }
-            break;
-        case EPI_SSP1:
+            const long long gnode = (long long)e * ND + n;
+            switch (mode) {
+            case EPI_STORE:
 #pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const long long g = f * Ndof + gnode;
-                a.u_out[g] = __ldg(a.u + g) + a.dt * double(acc[k][f]);
-            }
-            break;
-        case EPI_SSP2:
+                for (int f = 0; f < NF; ++f) a.dudt[f * Ndof + gnode] = double(acc[k][f]);
+                break;
+            case EPI_LSRK:
 #pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const long long g = f * Ndof + gnode;
-                const double y = __ldg(a.u + g) + a.dt * double(acc[k][f]);
-                a.u_out[g] = 3. / 4 * a.x0[g] + 1. / 4 * y;
-            }
-            break;
-        case EPI_SSP3:
+                for (int f = 0; f < NF; ++f) {
+                    const long long g = f * Ndof + gnode;
+                    const double L = double(acc[k][f]);
+                    const double dv = (a.rkA == 0.0) ? a.dt * L : a.rkA * ub[kk][f] + a.dt * L;
+                    a.du[g] = dv;
+                    a.u_out[g] = ua[kk][f] + a.rkB * dv;
+                }
+                break;
+            case EPI_SSP1:
 #pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const long long g = f * Ndof + gnode;
-                const double y = __ldg(a.u + g) + a.dt * double(acc[k][f]);
-                a.u_out[g] = 1. / 3 * a.x0[g] + 2. / 3 * y;
+                for (int f = 0; f < NF; ++f) a.u_out[f * Ndof + gnode] = ua[kk][f] + a.dt * double(acc[k][f]);
+                break;
+            case EPI_SSP2:
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    const double y = ua[kk][f] + a.dt * double(acc[k][f]);
+                    a.u_out[f * Ndof + gnode] = 3. / 4 * ub[kk][f] + 1. / 4 * y;
+                }
+                break;
+            case EPI_SSP3:
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    const double y = ua[kk][f] + a.dt * double(acc[k][f]);
+                    a.u_out[f * Ndof + gnode] = 1. / 3 * ub[kk][f] + 2. / 3 * y;
+                }
+                break;
+            default:
+                break;
             }
-            break;
-        default:
-            break;
         }
     }
 }
