@@ -107,6 +107,36 @@ __device__ __forceinline__ Prim<DIM, Real> primitives(const Real *s, Real gamma,
     return q;
 }
 
+// FP32-bulk form: the same primitives in FP32, with the pressure relative to
+// pref (dp = p - pref) formed in FP64 from the FP64 state, since it carries the
+// low-Mach cancellation: 1/rho and |m|^2/(2 rho) in FP64, everything that only
+// enters the O(Np^{d+1}) fluxes (v, beta, 1/beta, |v| + c) in FP32.
+template <int DIM>
+__device__ __forceinline__ Prim<DIM, float> primitives_mixed(const double *s, double gamma, double gammaM1,
+                                                             double pref) {
+    constexpr int NF = DIM + 2;
+    Prim<DIM, float> q;
+    const double rr = rcp(s[0]);
+    double mm = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) mm += s[1 + d] * s[1 + d];
+    const double p = gammaM1 * (s[NF - 1] - 0.5 * mm * rr);
+    q.dp = float(p - pref);
+    q.rho = float(s[0]);
+    q.rrho = float(rr);
+    q.vsq = 0.0f;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        q.v[d] = float(s[1 + d] * rr);
+        q.vsq += q.v[d] * q.v[d];
+    }
+    const float pf = float(p);
+    q.beta = 0.5f * q.rho * rcp(pf);
+    q.rbeta = 2.0f * pf * q.rrho;
+    q.lam = sqrtf(q.vsq) + sqrtf(float(gamma) * pf * q.rrho);
+    return q;
+}
+
 // BasicOperations.cpp:6-12.  Logarithmic mean of x, y > 0 and its inverse.
 // With f = (y-x)/(y+x) and u = f^2 the mean is ((x+y)/2) / P(u),
 // P(u) = 1 + u/3 + u^2/5 + u^3/7, on the reference's series branch u < 1e-4

@@ -196,6 +196,19 @@ __device__ __forceinline__ void store_prim(Real *sH, int n, const Prim<DIM, doub
     sH[I::LAM * ND + n] = Real(q.lam);
     if constexpr (sizeof(Real) == 4) sH[I::DP * ND + n] = Real(q.dp - pref);
 }
+template <int DIM, int ND, typename Real>
+__device__ __forceinline__ void store_prim_w(Real *sH, int n, const Prim<DIM, Real> &q) {
+    using I = HIdx<DIM>;
+    sH[I::RHO * ND + n] = q.rho;
+    sH[I::RRHO * ND + n] = q.rrho;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) sH[(I::V + d) * ND + n] = q.v[d];
+    sH[I::VSQ * ND + n] = q.vsq;
+    sH[I::BETA * ND + n] = q.beta;
+    sH[I::RBETA * ND + n] = q.rbeta;
+    sH[I::LAM * ND + n] = q.lam;
+    if constexpr (sizeof(Real) == 4) sH[I::DP * ND + n] = q.dp;
+}
 // Working-precision copy of primitives computed in FP64 (pressure relative
 // to pref in the FP32-bulk form).
 template <int DIM, typename Real>
@@ -649,9 +662,15 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
         for (int k = 0; k < NPL; ++k) {
             const int n = li + k * GS;
             if (n < ND) {
-                const Prim<DIM, double> q = primitives<DIM, double>(st[k], gamma, gm1);
-                store_prim<DIM, ND, Real>(sH, n, q, pref);
-                lam = fmax(lam, q.lam);
+                if constexpr (!LY::F64) {
+                    const Prim<DIM, float> q = primitives_mixed<DIM>(st[k], gamma, gm1, pref);
+                    store_prim_w<DIM, ND, Real>(sH, n, q);
+                    lam = fmax(lam, double(q.lam));
+                } else {
+                    const Prim<DIM, double> q = primitives<DIM, double>(st[k], gamma, gm1);
+                    store_prim<DIM, ND, Real>(sH, n, q, pref);
+                    lam = fmax(lam, q.lam);
+                }
             }
         }
     }
@@ -1051,8 +1070,14 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 #pragma unroll
         for (int q = 0; q < DIM; ++q) nor[q] = Real(x.nb[q]);
         Prim<DIM, Real> po = load_prim<DIM, ND, Real>(sH, no);
-        const Prim<DIM, double> pn64 = primitives<DIM, double>(sn, gamma, gm1);
-        Prim<DIM, Real> pn = cast_prim<DIM, Real>(pn64, pref);
+        Prim<DIM, double> pn64;
+        Prim<DIM, Real> pn;
+        if constexpr (!LY::F64 && !(NS && !VC)) {
+            pn = primitives_mixed<DIM>(sn, gamma, gm1, pref);
+        } else {
+            pn64 = primitives<DIM, double>(sn, gamma, gm1);
+            pn = cast_prim<DIM, Real>(pn64, pref);
+        }
 #pragma unroll
         for (int f = 0; f < NF; ++f) fn[f] = 0;
         if constexpr (NS && VC) {
