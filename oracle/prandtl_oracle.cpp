@@ -29,6 +29,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <cstring>
 #include <vector>
 #ifdef _OPENMP
@@ -426,6 +427,10 @@ struct Ctx {
     int parabolic, blending, quirks, dissipation;
     int num_bcs;
     const oracle_bc *bcs;
+    int axi;                       // axisymmetric (z, r) form
+    const double *xy;              // [dim][Ndof] node coordinates
+    std::vector<char> on_axis;     // [Ndof] axis nodes (DGSEMOperator::BuildAxisIndexFromMarker)
+    double r(long g) const { return xy[Ndof + g]; }
     double alpha_max, alpha_min, modalThreshold;
     std::vector<double> x, w, D, Dhat, Dhat2;   // Dhat, Dhat2 as [i][l]
     std::vector<double> Vinv;                   // [nd][nd] modal basis inverse
@@ -467,6 +472,19 @@ void setup(Ctx &X, const oracle_mesh *m, const oracle_config *c) {
     X.quirks = c->quirks;
     X.num_bcs = c->num_bcs;
     X.bcs = c->bcs;
+    X.axi = c->axisymmetric;
+    X.xy = c->node_coords;
+    if (X.axi) {   // DGSEMOperator.cpp:482-518: nodes at |r| <= 1e-14 of elements on "axis" boundaries
+        X.on_axis.assign(X.Ndof, 0);
+        for (int f = 0; f < X.F; ++f) {
+            const int *fe = X.faces + 4 * f;
+            if (fe[2] >= 0 || X.bcs[fe[3]].type != ORACLE_BC_AXIS) continue;
+            for (int n = 0; n < X.nd; ++n) {
+                const long g = (long)fe[0] * X.nd + n;
+                if (std::abs(X.r(g)) <= 1e-14) X.on_axis[g] = 1;
+            }
+        }
+    }
     X.dissipation = c->surface_dissipation;
     X.alpha_max = c->alpha_max;
     X.alpha_min = c->alpha_min;
@@ -529,6 +547,7 @@ void bdr_outer_state(const Ctx &X, const oracle_bc &bc, double *s1, const double
     case ORACLE_BC_OUTFLOW:   // SupersonicOutflowBdrFaceIntegrator.cpp:11-14
         for (int f = 0; f < nf; ++f) s2[f] = s1[f];
         return;
+    case ORACLE_BC_AXIS:
     case ORACLE_BC_SYMMETRY: {   // SymmetryBdrFaceIntegrator.cpp:11-32 (|nor| > 0)
         const double rn = 1.0 / norml2(nor, dim);
         double un[3], mn = 0.0;
@@ -670,7 +689,7 @@ double bdr_face_flux(const Ctx &X, const oracle_bc &bc, double *s1, double *s2, 
         for (int f = 0; f < nf; ++f) s2[f] = s1[f];
         return std::sqrt(vv) + an;
     }
-    if (bc.type == ORACLE_BC_SYMMETRY && norml2(nor, dim) == 0.0) {
+    if ((bc.type == ORACLE_BC_SYMMETRY || bc.type == ORACLE_BC_AXIS) && norml2(nor, dim) == 0.0) {
         for (int f = 0; f < nf; ++f) { flux[f] = 0.0; s2[f] = s1[f]; }
         return 0.0;
     }
@@ -839,6 +858,10 @@ void fv_fluxes(const Ctx &X, int e, const double *el, double alpha, double *el_d
             for (int f = 0; f < nf; ++f) s2[f] = el[id2 * nf + f];
             subcell_normal(X, e, dir, i + 1, nor);
             face_flux(X.dim, X.P.gamma, X.quirks, 1, s1, s2, nor, flux);
+            if (X.axi) {   // DGSEMIntegrator.cpp:979-1031: times r at the nodes' reference midpoint
+                const double rh = 0.5 * (X.r((long)e * X.nd + id1) + X.r((long)e * X.nd + id2));
+                for (int f = 0; f < nf; ++f) flux[f] *= rh;
+            }
             for (int f = 0; f < nf; ++f) dU[f] -= flux[f];
             const double m = 1.0 / (J * X.w[i]);
             for (int f = 0; f < nf; ++f) dU[f] *= m;
@@ -918,6 +941,10 @@ void element_volume(const Ctx &X, int e, const double *el, const double *gq, dou
                     const int id2 = node_id(X, m, j, k);
                     for (int q = 0; q < nf; ++q) s2[q] = el[id2 * nf + q];
                     volume_flux(dim, X.P.gamma, s1, s2, m0, m0, f);
+                    if (X.axi) {   // DGSEMIntegrator.cpp:273-291: f *= r at the reference midpoint
+                        const double rh = 0.5 * (X.r((long)e * nd + id1) + X.r((long)e * nd + id2));
+                        for (int q = 0; q < nf; ++q) f[q] *= rh;
+                    }
                     setcol(Fi, id1, m, f);
                     setcol(Fi, id2, i, f);
                 }
@@ -928,6 +955,10 @@ void element_volume(const Ctx &X, int e, const double *el, const double *gq, dou
                         const int id2 = node_id(X, i, m, k);
                         for (int q = 0; q < nf; ++q) s2[q] = el[id2 * nf + q];
                         volume_flux(dim, X.P.gamma, s1, s2, m1r, m1r, g);
+                        if (X.axi) {   // :319-338
+                            const double rh = 0.5 * (X.r((long)e * nd + id1) + X.r((long)e * nd + id2));
+                            for (int q = 0; q < nf; ++q) g[q] *= rh;
+                        }
                         setcol(Gi, id1, m, g);
                         setcol(Gi, id2, j, g);
                     }
@@ -973,6 +1004,11 @@ void element_volume(const Ctx &X, int e, const double *el, const double *gq, dou
                 if (X.blending)
                     for (int q = 0; q < nf; ++q) dUi[q] *= (1.0 - alpha);
                 const double mJ = 1.0 / J;
+                if (X.axi) {   // DGSEMIntegrator.cpp:411-428: + p on the radial momentum
+                    const double *st = el + id1 * nf;
+                    const double ke = 0.5 * ((st[1] * st[1] + st[2] * st[2]) / st[0]);
+                    el_dudt[id1 * nf + 2] += X.P.gammaM1 * (st[3] - ke);
+                }
                 if (ns) {
                     for (int q = 0; q < nf; ++q) el_dudt[id1 * nf + q] += (dUi[q] + dUv[q]) * mJ;
                 } else {
@@ -1015,10 +1051,95 @@ void element_lift(const Ctx &X, int e, const double *v, double *gout /*[dim][nd]
             }
 }
 
-void run_rhs(const Ctx &X, const double *u, double *dudt, double *alpha_out, double *lambda_out,
+// DGSEMOperator::RecoverStateFromWeighted (DGSEMOperator.cpp:161-470): U from
+// the weighted state rU.  Off the axis U = rU / r.  At an axis node the
+// reference's "axis" boundaries also select the low-order reconstruction
+// (Simulation.cpp:520-530 sets SetLowOrderAxis(true)), so its high-order
+// shape-derivative branch is never taken: U(0) = d(rU)/dr from the two nearest
+// off-axis nodes at the same z (else the two nearest overall), a least-squares
+// slope through the origin limited by minmod against theta_lim times each
+// node's slope and clamped to cap = 10 |f1| / r1; one node: its slope; none:
+// 0.  A non-finite or too small density or non-finite energy copies the
+// nearest off-axis node's U instead.  Radial momentum is 0 on the axis.
+int recover_weighted(const Ctx &X, const double *rU, double *U) {
+    const int nd = X.nd, nf = X.nf;
+    const long Ndof = X.Ndof;
+    const double tiny = 1e-14, cap_mult = 10.0, z_tol = 1e-12, theta_lim = 1.5, rho_floor = 1e-12;
+    const double inf = std::numeric_limits<double>::infinity();
+    auto sign = [](double a) { return (double)((a > 0) - (a < 0)); };
+    auto minmod = [&](double a, double b) { return a * b <= 0.0 ? 0.0 : sign(a) * std::min(std::abs(a), std::abs(b)); };
+    auto clamp = [&](double x, double m) {
+        if (!std::isfinite(x)) return 0.0;
+        return std::abs(x) <= m ? x : sign(x) * m;
+    };
+    int bad = 0;
+    for (int e = 0; e < X.E; ++e) {
+        const long g0 = (long)e * nd;
+        for (int ld = 0; ld < nd; ++ld) {
+            const long g = g0 + ld;
+            const double r = X.r(g);
+            if (!X.on_axis[g] && r > 0.0) {
+                for (int f = 0; f < nf; ++f) U[f * Ndof + g] = rU[f * Ndof + g] / r;
+                continue;
+            }
+            const double z_axis = X.xy[g];
+            // nearest off-axis nodes at the same z, else overall (the same for every field)
+            int j1 = -1, j2 = -1;
+            double r1 = inf, r2 = inf;
+            for (int pass = 0; pass < 2 && j1 < 0; ++pass)
+                for (int j = 0; j < nd; ++j) {
+                    const double rj = X.r(g0 + j);
+                    if (!(rj > 0.0)) continue;
+                    if (pass == 0 && !(std::abs(X.xy[g0 + j] - z_axis) <= z_tol)) continue;
+                    if (rj < r1) { r2 = r1; j2 = j1; r1 = rj; j1 = j; }
+                    else if (rj < r2) { r2 = rj; j2 = j; }
+                }
+            auto d_dr = [&](int f) {
+                const double *fe = rU + f * Ndof + g0;
+                const double f_ref = j1 >= 0 ? std::abs(fe[j1]) : 0.0;
+                const double cap = (j1 >= 0 && !(f_ref < 1e-12)) ? cap_mult * f_ref / std::max(r1, tiny) : inf;
+                if (j1 >= 0 && j2 >= 0 && std::isfinite(r1) && std::isfinite(r2) && r1 > 0.0 && r2 > 0.0) {
+                    const double f1 = fe[j1], f2 = fe[j2];
+                    const double m = (r1 * f1 + r2 * f2) / std::max(r1 * r1 + r2 * r2, tiny);
+                    const double s1 = f1 / r1, s2 = f2 / r2;
+                    return clamp(minmod(m, minmod(theta_lim * s1, theta_lim * s2)), cap);
+                }
+                if (j1 >= 0 && std::isfinite(r1) && r1 > 0.0) return clamp(fe[j1] / r1, cap);
+                return 0.0;
+            };
+            const double rho_axis = d_dr(0), mz_axis = d_dr(1), E_axis = d_dr(3);
+            if (!std::isfinite(rho_axis) || rho_axis < rho_floor || !std::isfinite(E_axis)) {
+                int nb = -1;
+                double rn = -1.0;
+                for (int j = 0; j < nd; ++j) {
+                    const double rj = X.r(g0 + j);
+                    if (rj > 0.0 && (nb == -1 || rj < rn)) { rn = rj; nb = j; }
+                }
+                if (nb < 0) { ++bad; continue; }
+                for (int f = 0; f < nf; ++f) U[f * Ndof + g] = rU[f * Ndof + g0 + nb] / rn;
+                U[2 * Ndof + g] = 0.0;
+            } else {
+                U[g] = rho_axis;
+                U[Ndof + g] = mz_axis;
+                U[2 * Ndof + g] = 0.0;
+                U[3 * Ndof + g] = E_axis;
+            }
+        }
+    }
+    return bad;
+}
+
+void run_rhs(const Ctx &X, const double *u_in, double *dudt, double *alpha_out, double *lambda_out,
              double *grad_out, int nthreads) {
     const int nf = X.nf, nd = X.nd, dim = X.dim, E = X.E;
     const long Ndof = X.Ndof;
+    std::vector<double> Urec;
+    const double *u = u_in;
+    if (X.axi) {   // DGSEMOperator::Mult evaluates the fluxes on U recovered from rU
+        Urec.assign((size_t)nf * Ndof, 0.0);
+        recover_weighted(X, u_in, Urec.data());
+        u = Urec.data();
+    }
     std::vector<double> alpha(E, 0.0);
     if (X.blending) {
 #pragma omp parallel for schedule(static) num_threads(nthreads)
@@ -1153,6 +1274,8 @@ void run_rhs(const Ctx &X, const double *u, double *dudt, double *alpha_out, dou
                     double s1[5] = {0, 0, 0, 0, 0}, s2[5] = {0, 0, 0, 0, 0}, flux[5], d1[5];
                     for (int f = 0; f < nf; ++f) s1[f] = u[f * Ndof + g1];
                     bdr_face_flux(X, X.bcs[lf2], s1, s2, nor, flux);
+                    if (X.axi)   // BdrFaceIntegrator.cpp:109-111: dU_face1 *= r
+                        for (int f = 0; f < nf; ++f) flux[f] *= X.r(g1);
                     for (int f = 0; f < nf; ++f) d1[f] = -flux[f];
                     if (X.parabolic) {   // dU = -inviscid + viscous (BdrFaceIntegrator.cpp:170-186)
                         double q[3][5], fv[5];
@@ -1173,6 +1296,8 @@ void run_rhs(const Ctx &X, const double *u, double *dudt, double *alpha_out, dou
                 for (int f = 0; f < nf; ++f) { s1[f] = u[f * Ndof + g1]; s2[f] = u[f * Ndof + g2]; }
                 if (!X.parabolic) {
                     face_flux(dim, X.P.gamma, X.quirks, X.dissipation, s1, s2, nor, flux);
+                    if (X.axi)   // DGSEMIntegrator.cpp:190-207: flux_num *= r at the face point
+                        for (int f = 0; f < nf; ++f) flux[f] *= X.r(g1);
                     for (int f = 0; f < nf; ++f) { d1[f] = -flux[f]; d2[f] = flux[f]; }
                 } else {
                     double q1[3][5], q2[3][5], fv1[15], fv2[15];
@@ -1209,6 +1334,9 @@ void run_rhs(const Ctx &X, const double *u, double *dudt, double *alpha_out, dou
             }
         }
     }
+    if (X.axi)   // DGSEMOperator::ZeroAxisRadialMom (DGSEMOperator.cpp:520-533)
+        for (long g = 0; g < Ndof; ++g)
+            if (X.on_axis[g]) dudt[2 * Ndof + g] = 0.0;
 }
 
 // Boundary faces need a valid BC index; the Navier-Stokes form has no viscous
@@ -1225,6 +1353,7 @@ bool bad_boundaries(const oracle_mesh *m, const oracle_config *c) {
             return true;
         // Q13: the reference's Riemann lifting reads a face normal only its face pass sets
         if (c->parabolic && c->quirks == 0 && t == ORACLE_BC_RIEMANN) return true;
+        if (t == ORACLE_BC_AXIS && !c->axisymmetric) return true;
     }
     return false;
 }
@@ -1238,10 +1367,19 @@ int oracle_rhs(const oracle_mesh *m, const oracle_config *c, const double *u, do
     if (m->dim < 2 || m->dim > 3 || m->order < 1 || m->order > 9) return 1;
     if (nthreads <= 0) nthreads = 1;
     if (bad_boundaries(m, c)) return 1;
+    if (c->axisymmetric && (m->dim != 2 || c->parabolic || !c->node_coords)) return 1;
     Ctx X;
     setup(X, m, c);
     run_rhs(X, u, dudt, alpha, lambda_max, grad, nthreads);
     return 0;
+}
+
+int oracle_recover_weighted(const oracle_mesh *m, const oracle_config *c, const double *rU, double *U) {
+    if (!m || !c || !rU || !U || !c->axisymmetric || !c->node_coords || m->dim != 2) return 1;
+    if (bad_boundaries(m, c)) return 1;
+    Ctx X;
+    setup(X, m, c);
+    return recover_weighted(X, rU, U) == 0 ? 0 : 1;
 }
 
 int oracle_step(const oracle_mesh *m, const oracle_config *c, double *u, double t, double dt,
@@ -1249,6 +1387,7 @@ int oracle_step(const oracle_mesh *m, const oracle_config *c, double *u, double 
     if (!m || !c || !u) return 1;
     if (nthreads <= 0) nthreads = 1;
     if (bad_boundaries(m, c)) return 1;
+    if (c->axisymmetric && (m->dim != 2 || c->parabolic || !c->node_coords)) return 1;
     Ctx X;
     setup(X, m, c);
     const long n = (long)X.nf * X.Ndof;

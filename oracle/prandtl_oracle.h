@@ -53,7 +53,8 @@ enum {
     ORACLE_BC_INFLOW_RV = 6,        /* SubsonicInflowRV, constant density and velocity */
     ORACLE_BC_INFLOW_PTTT = 7,      /* SubsonicInflowPtTtAng, constant pt, Tt, angles */
     ORACLE_BC_NOSLIP_ADIABATIC = 8, /* NoSlipAdiabWall: wall velocity, normal heat flux */
-    ORACLE_BC_NOSLIP_ISOTHERMAL = 9 /* NoSlipIsothWall: wall velocity, wall temperature */
+    ORACLE_BC_NOSLIP_ISOTHERMAL = 9,/* NoSlipIsothWall: wall velocity, wall temperature */
+    ORACLE_BC_AXIS = 10             /* "axis": the symmetry flux; its nodes at r = 0 are axis nodes */
 };
 typedef struct oracle_bc {
     int type;
@@ -80,7 +81,13 @@ typedef struct oracle_config {
     int surface_dissipation;  /* 1: as the reference; 0: EC surface flux (test switch) */
     int num_bcs;              /* boundary conditions referenced by boundary faces */
     const oracle_bc *bcs;
+    int axisymmetric;         /* 2D Euler in (z, r): u is r U (AXISYMMETRIC build of the reference) */
+    const double *node_coords;/* [dim][Ndof] node coordinates (axisymmetric: r = coordinate 1) */
 } oracle_config;
+
+/* Axisymmetric form: U recovered from the weighted state rU (the input every
+ * axisymmetric oracle_rhs call takes).  Returns 0 on success. */
+int oracle_recover_weighted(const oracle_mesh *m, const oracle_config *c, const double *rU, double *U);
 
 /* One RHS evaluation dudt = L(u).  alpha (may be NULL) receives the per-element
  * blending coefficient, lambda_max (may be NULL) the largest |V|+c of any state

@@ -30,7 +30,8 @@ class OracleBC(C.Structure):
 
 # boundary-condition types (prandtl_oracle.h ORACLE_BC_*)
 BC_TYPES = {"state": 0, "outflow": 1, "slip_wall": 2, "symmetry": 3, "pressure_outflow": 4,
-            "riemann": 5, "inflow_rv": 6, "inflow_pttt": 7, "noslip_adiabatic": 8, "noslip_isothermal": 9}
+            "riemann": 5, "inflow_rv": 6, "inflow_pttt": 7, "noslip_adiabatic": 8, "noslip_isothermal": 9,
+            "axis": 10}
 
 
 class OracleConfig(C.Structure):
@@ -38,7 +39,8 @@ class OracleConfig(C.Structure):
                 ("R_gas", C.c_double), ("alpha_max", C.c_double), ("alpha_min", C.c_double),
                 ("parabolic", C.c_int), ("blending", C.c_int), ("sutherland", C.c_int),
                 ("quirks", C.c_int), ("surface_dissipation", C.c_int),
-                ("num_bcs", C.c_int), ("bcs", C.POINTER(OracleBC))]
+                ("num_bcs", C.c_int), ("bcs", C.POINTER(OracleBC)),
+                ("axisymmetric", C.c_int), ("node_coords", C.POINTER(C.c_double))]
 
 
 def make_bcs(bcs):
@@ -81,6 +83,8 @@ def lib():
         L.oracle_step.argtypes = [C.POINTER(OracleMesh), C.POINTER(OracleConfig), dp, C.c_double,
                                   C.c_double, C.c_int, C.c_int, C.c_int]
         L.oracle_step.restype = C.c_int
+        L.oracle_recover_weighted.argtypes = [C.POINTER(OracleMesh), C.POINTER(OracleConfig), dp, dp]
+        L.oracle_recover_weighted.restype = C.c_int
         L.oracle_gl.argtypes = [C.c_int, dp, dp, dp]
         L.oracle_log_mean.argtypes = [C.c_double, C.c_double]
         L.oracle_log_mean.restype = C.c_double
@@ -101,7 +105,7 @@ class Oracle:
 
     def __init__(self, mesh, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05, alpha_max=0.5,
                  alpha_min=0.001, parabolic=0, blending=0, sutherland=0, quirks=0,
-                 surface_dissipation=1, nthreads=None, bcs=None):
+                 surface_dissipation=1, nthreads=None, bcs=None, axisymmetric=0):
         self.mesh = mesh
         self._adj = np.ascontiguousarray(mesh.elem_adj, dtype=np.float64)
         self._detj = np.ascontiguousarray(mesh.elem_detj, dtype=np.float64)
@@ -111,9 +115,10 @@ class Oracle:
                             _p(self._adj), _p(self._detj),
                             self._faces.ctypes.data_as(C.POINTER(C.c_int)), _p(self._nor))
         self._bcs = make_bcs(bcs)
+        self._xy = np.ascontiguousarray(mesh.coords, dtype=np.float64)
         self.c = OracleConfig(gamma, Pr, mu, R_gas, alpha_max, alpha_min, parabolic, blending,
                               sutherland, quirks, surface_dissipation, len(bcs) if bcs else 0,
-                              self._bcs)
+                              self._bcs, int(axisymmetric), _p(self._xy))
         self.nthreads = nthreads or os.cpu_count() or 1
 
     @property
@@ -158,7 +163,8 @@ def gl(order):
 # The reference's own integrator sources, compiled by ref_harness/build_ref.sh
 # into _ref/ (only where the reference checkout is present).
 _REF_LIBS = {}
-_REF_VARIANTS = {(0, 0): "euler", (0, 1): "euler_blend", (1, 0): "ns", (1, 1): "ns_blend"}
+_REF_VARIANTS = {(0, 0, 0): "euler", (0, 1, 0): "euler_blend", (1, 0, 0): "ns", (1, 1, 0): "ns_blend",
+                 (0, 0, 1): "euler_axi", (0, 1, 1): "euler_blend_axi"}
 
 
 def ref_available():
@@ -169,8 +175,8 @@ def build_ref():
     subprocess.run(["bash", os.path.join(_HERE, "ref_harness", "build_ref.sh")], check=True)
 
 
-def ref_lib(parabolic, blending):
-    key = (int(bool(parabolic)), int(bool(blending)))
+def ref_lib(parabolic, blending, axisymmetric=0):
+    key = (int(bool(parabolic)), int(bool(blending)), int(bool(axisymmetric)))
     if key not in _REF_LIBS:
         L = C.CDLL(os.path.join(_HERE, "_ref", f"libref_{_REF_VARIANTS[key]}.so"))
         dp = C.POINTER(C.c_double)
@@ -189,9 +195,14 @@ class RefOperator(Oracle):
     physics switches select the compile-time variant."""
 
     def rhs(self, u, want_alpha=False, want_grad=False):
-        L = ref_lib(self.c.parabolic, self.c.blending)
+        L = ref_lib(self.c.parabolic, self.c.blending, self.c.axisymmetric)
         u = np.ascontiguousarray(u, dtype=np.float64)
         dudt = np.empty_like(u)
+        if self.c.axisymmetric:   # the integrators see U recovered from r U (restated in the oracle)
+            U = np.empty_like(u)
+            if lib().oracle_recover_weighted(C.byref(self.m), C.byref(self.c), _p(u), _p(U)) != 0:
+                raise RuntimeError("oracle_recover_weighted failed")
+            u = U
         alpha = np.empty(self.mesh.num_elements) if want_alpha else None
         grad = np.empty(self.mesh.dim * u.size) if want_grad else None
         rc = L.ref_rhs(C.byref(self.m), C.byref(self.c), _p(u), _p(dudt),

@@ -45,4 +45,6 @@ build euler
 build euler_blend -DSUBCELL_FV_BLENDING
 build ns -DPARABOLIC
 build ns_blend -DPARABOLIC -DSUBCELL_FV_BLENDING
+build euler_axi -DAXISYMMETRIC
+build euler_blend_axi -DSUBCELL_FV_BLENDING -DAXISYMMETRIC
 echo "built $(ls "$OUT"/libref_*.so | wc -l) reference libraries in $OUT"

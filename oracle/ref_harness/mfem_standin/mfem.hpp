@@ -586,13 +586,13 @@ public:
     const IntegrationPoint &GetElement1IntPoint() { return eip1; }
     const IntegrationPoint &GetElement2IntPoint() { return eip2; }
     const DenseMatrix &Jacobian() { return Jf; }
-    void Transform(const IntegrationPoint &, Vector &x) { x.SetSize(dim); x = 0.0; }
+    // the physical point of the face point last set by SetAllIntPoints
+    void Transform(const IntegrationPoint &, Vector &x) { T1->Transform(eip1, x); }
 };
 
 // ------------------------------------------------------------ coefficients
 // MFEM's function coefficients: a std::function of the physical point (and,
-// with SetTime, of the time).  Boundary states here are constant, so the
-// point comes from FaceElementTransformations::Transform (zero).
+// with SetTime, of the time), from FaceElementTransformations::Transform.
 inline void mfem_error(const char *msg) { throw std::runtime_error(msg); }
 class FunctionCoefficient {
 public:

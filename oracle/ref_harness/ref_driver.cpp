@@ -169,7 +169,7 @@ using namespace Prandtl;
 namespace {
 
 // Stand-in ParMesh of an affine periodic mesh from the oracle descriptor.
-std::shared_ptr<ParMesh> make_mesh(const oracle_mesh *m) {
+std::shared_ptr<ParMesh> make_mesh(const oracle_mesh *m, const double *coords = nullptr) {
     auto pm = std::make_shared<ParMesh>();
     const int dim = m->dim;
     pm->dim = dim;
@@ -189,6 +189,12 @@ std::shared_ptr<ParMesh> make_mesh(const oracle_mesh *m) {
         inv.Invert();
         for (int r = 0; r < dim; ++r)
             for (int c = 0; c < dim; ++c) T.J(r, c) = T.detJ * inv(r, c);
+        if (coords) {   // origin = node 0 of the element (xi = 0)
+            int nd = 1;
+            for (int d = 0; d < dim; ++d) nd *= m->order + 1;
+            const long Ndof = (long)m->num_elements * nd;
+            for (int d = 0; d < dim; ++d) T.x0[d] = coords[d * Ndof + (long)e * nd];
+        }
     }
     for (int f = 0; f < m->num_faces; ++f) {
         const int *fe = m->face_elems + 4 * f;
@@ -250,7 +256,7 @@ extern "C" int ref_rhs(const oracle_mesh *md, const oracle_config *cfg, const do
 #ifdef PARABOLIC
         lifting = std::make_shared<LiftingBR1>();
 #endif
-        auto pmesh = make_mesh(md);
+        auto pmesh = make_mesh(md, cfg->node_coords);
         DG_FECollection fec(order, dim, BasisType::GaussLobatto), fec0(0, dim);
         auto vfes = std::make_shared<ParFiniteElementSpace>(pmesh.get(), &fec, nf);
         auto fes0 = std::make_shared<ParFiniteElementSpace>(pmesh.get(), &fec0, 1);
@@ -313,6 +319,7 @@ extern "C" int ref_rhs(const oracle_mesh *md, const oracle_config *cfg, const do
                 bdr.emplace_back(new SlipWallBdrFaceIntegrator(lifting, rsolver, Np, time, pc.gamma, true, false));
                 break;
             case ORACLE_BC_SYMMETRY:
+            case ORACLE_BC_AXIS:   // Simulation.cpp:520-530: "axis" adds the symmetry integrator
                 bdr.emplace_back(new SymmetryBdrFaceIntegrator(lifting, rsolver, Np, time, pc.gamma, true, false));
                 break;
             case ORACLE_BC_PRESSURE_OUTFLOW:
@@ -494,6 +501,19 @@ extern "C" int ref_rhs(const oracle_mesh *md, const oracle_config *cfg, const do
             u.GetSubVector(vdofs, el_u);
             bdr.at(tr->lf2)->AssembleFaceVector(*fe, *fe, *tr, el_u, el_dudt);
             dudt.AddElementVector(vdofs, el_dudt);
+        }
+#endif
+#ifdef AXISYMMETRIC
+        // u is the state recovered from r U (DGSEMOperator::Mult, restated by the
+        // caller); DGSEMOperator::ZeroAxisRadialMom: zero radial-momentum rate at
+        // the |r| <= 1e-14 nodes of elements on "axis" boundaries
+        for (int f = 0; f < md->num_faces; ++f) {
+            const int *fe4 = md->face_elems + 4 * f;
+            if (fe4[2] >= 0 || cfg->bcs[fe4[3]].type != ORACLE_BC_AXIS) continue;
+            for (int n = 0; n < Ndofs; ++n) {
+                const long g = (long)fe4[0] * Ndofs + n;
+                if (std::abs(cfg->node_coords[(long)NE * Ndofs + g]) <= 1e-14) dudt(2 * (long)NE * Ndofs + g) = 0.0;
+            }
         }
 #endif
         (void)grad_out;

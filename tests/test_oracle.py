@@ -235,3 +235,33 @@ def test_wall_parallel_flow_preserved(oracle_mod):
     for wall in ("slip_wall", "symmetry"):
         _, d = _bdr_free_stream(oracle_mod, 2, ["outflow", "outflow", wall, wall], [0.4, 0.0])
         assert np.abs(d).max() < 1e-12, wall
+
+
+# ---------------------------------------------------------------- axisymmetric (z, r)
+def test_axisymmetric_free_stream_and_recovery(oracle_mod):
+    """Uniform axial flow between the axis and a slip wall is kept (the r-weighted
+    pressure flux balances the source); off the axis U = rU / r exactly; on the
+    axis the radial momentum and its rate are zero."""
+    import ctypes as C
+    from prandtl_b200 import cases
+    from prandtl_b200.mesh import periodic_box
+    for N in (1, 2, 3, 4):
+        mesh = periodic_box(2, (4, 3), N, (0.0, 0.0), (2.0, 1.0), bcs=[0, 0, 1, 2])
+        bcs = [("outflow",), ("axis",), ("slip_wall",)]
+        U = cases.free_stream(mesh, rho=1.2, vel=[0.3, 0.0], p=1.5).reshape(4, -1)
+        r = mesh.coords[1]
+        orc = oracle_mod.Oracle(mesh, quirks=1, bcs=bcs, axisymmetric=1)
+        d = orc.rhs((U * r[None, :]).reshape(-1))["dudt"]
+        assert np.abs(d).max() < 1e-12, N
+        Up = cases.perturbed(mesh, cases.free_stream(mesh, rho=1.2, vel=[0.3, 0.1], p=1.5), amp=0.1, seed=N)
+        Up = Up.reshape(4, -1)
+        rUp = (Up * r[None, :]).reshape(-1)
+        rec = np.empty_like(rUp)
+        dp = C.POINTER(C.c_double)
+        assert oracle_mod.lib().oracle_recover_weighted(C.byref(orc.m), C.byref(orc.c), rUp.ctypes.data_as(dp),
+                                                        rec.ctypes.data_as(dp)) == 0
+        rec = rec.reshape(4, -1)
+        off = r > 1e-14
+        np.testing.assert_allclose(rec[:, off], Up[:, off], rtol=1e-14)
+        assert (rec[2, ~off] == 0).all() and (rec[0, ~off] > 0).all()
+        assert (orc.rhs(rUp)["dudt"].reshape(4, -1)[2, ~off] == 0).all()
