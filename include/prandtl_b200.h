@@ -83,6 +83,8 @@ typedef struct prandtl_mesh_desc {
                                          Tt, cp, flow angles theta, phi in degrees */
 #define PRANDTL_BC_NOSLIP_ADIABATIC 8 /* NoSlipAdiabWall: wall velocity, normal heat flux */
 #define PRANDTL_BC_NOSLIP_ISOTHERMAL 9 /* NoSlipIsothWall: wall velocity, wall temperature */
+#define PRANDTL_BC_AXIS 10            /* the r = 0 axis of the axisymmetric form: the symmetry
+                                         flux; marks the axis nodes (axisymmetric = 1 only) */
 /* With parabolic = 1 every type but SLIP_WALL, SYMMETRY and INFLOW_PTTT is
  * accepted (the reference defines no viscous treatment for the first two), and
  * RIEMANN only with quirks = 1 (the reference's Riemann lifting reads a face
@@ -124,6 +126,10 @@ typedef struct prandtl_config {
     double timeout_s;          /* bound on every host-side wait; 0 selects 120 s */
     int num_bcs;               /* boundary conditions the mesh's boundary faces index; */
     const prandtl_bc *bcs;     /*   copied at create (0 / NULL: periodic meshes only) */
+    int axisymmetric;          /* 1: 2D Euler in (z, r) = (x, y) (AXISYMMETRIC): the state is r U,
+                                  fluxes carry r, + p on the radial momentum; 0: planar */
+    const double *node_coords; /* axisymmetric: [dim][Ndof] node coordinates (byNODES, the state's
+                                  node order), copied at create; else ignored */
 } prandtl_config;
 
 typedef struct prandtl_handle prandtl_handle;

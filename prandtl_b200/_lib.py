@@ -57,7 +57,8 @@ class BC(C.Structure):
 
 
 BC_TYPES = {"state": 0, "outflow": 1, "slip_wall": 2, "symmetry": 3, "pressure_outflow": 4,
-            "riemann": 5, "inflow_rv": 6, "inflow_pttt": 7, "noslip_adiabatic": 8, "noslip_isothermal": 9}
+            "riemann": 5, "inflow_rv": 6, "inflow_pttt": 7, "noslip_adiabatic": 8, "noslip_isothermal": 9,
+            "axis": 10}
 
 
 class Config(C.Structure):
@@ -65,7 +66,8 @@ class Config(C.Structure):
                 ("R_gas", C.c_double), ("alpha_max", C.c_double), ("alpha_min", C.c_double),
                 ("parabolic", C.c_int), ("blending", C.c_int), ("sutherland", C.c_int),
                 ("quirks", C.c_int), ("surface_dissipation", C.c_int), ("precision", C.c_int),
-                ("timeout_s", C.c_double), ("num_bcs", C.c_int), ("bcs", C.POINTER(BC))]
+                ("timeout_s", C.c_double), ("num_bcs", C.c_int), ("bcs", C.POINTER(BC)),
+                ("axisymmetric", C.c_int), ("node_coords", C.POINTER(C.c_double))]
 
 
 class BatchConfig(C.Structure):

@@ -32,7 +32,8 @@ struct PhysParams {
 // heat flux and vT = 1 / (R_gas T_wall).
 enum BcType : int {
     BC_STATE = 0, BC_OUTFLOW = 1, BC_SLIP_WALL = 2, BC_SYMMETRY = 3, BC_PRESSURE_OUTFLOW = 4,
-    BC_RIEMANN = 5, BC_INFLOW_RV = 6, BC_INFLOW_PTTT = 7, BC_NOSLIP_ADIABATIC = 8, BC_NOSLIP_ISOTHERMAL = 9
+    BC_RIEMANN = 5, BC_INFLOW_RV = 6, BC_INFLOW_PTTT = 7, BC_NOSLIP_ADIABATIC = 8, BC_NOSLIP_ISOTHERMAL = 9,
+    BC_AXIS = 10
 };
 struct BcDev {
     int type, pad;

@@ -351,6 +351,10 @@ struct ElemIO {
     int mode;
     double dt, rkA, rkB;
     const BcDev *bcs;           // boundary conditions (boundary faces)
+    // axisymmetric (z, r) form, 2D Euler only; null otherwise
+    const double *u_rk;         // the RK state r U (u is the U recovered from it)
+    const double *rad;          // [Ndof] node radius r
+    const unsigned char *axis;  // [Ndof] axis nodes
 };
 // Per-warp (rhs) or per-CTA (lift) copy of the current solve's constants.
 struct __align__(16) WarpCtx {
@@ -379,6 +383,9 @@ __device__ __forceinline__ ElemIO io_from_args(const MeshDev &m, const RhsArgs &
     io.rkA = a.rkA;
     io.rkB = a.rkB;
     io.bcs = m.bcs;
+    io.u_rk = a.u_rk;
+    io.rad = m.rad;
+    io.axis = m.axis;
     return io;
 }
 
@@ -414,6 +421,9 @@ __device__ __forceinline__ ElemIO io_from_batch(const BatchInst &I, BatchInst *I
         io.x0 = I.u[0];
         io.mode = st.stage == 0 ? EPI_SSP1 : (st.stage == 1 ? EPI_SSP2 : EPI_SSP3);
     }
+    io.u_rk = nullptr;
+    io.rad = nullptr;
+    io.axis = nullptr;
     return io;
 }
 
@@ -445,7 +455,7 @@ __device__ __forceinline__ void bc_outer_state(const BcDev &bc, double *s1, cons
     if (bc.type == BC_STATE) {   // SpecifiedStateBdrFaceIntegrator.cpp:24-36
 #pragma unroll
         for (int f = 0; f < NF; ++f) s2[f] = bc.state[f];
-    } else if (bc.type == BC_SYMMETRY) {   // SymmetryBdrFaceIntegrator.cpp:11-32 (|nor| > 0)
+    } else if (bc.type == BC_SYMMETRY || bc.type == BC_AXIS) {   // SymmetryBdrFaceIntegrator.cpp:11-32 (|nor| > 0)
         const double rn = 1.0 / nn;
         double mn = 0.0;
 #pragma unroll
@@ -585,7 +595,7 @@ __device__ __forceinline__ void boundary_flux(const BcDev &bc, const double *s_i
         flux[NF - 1] = 0;
         return;
     }
-    if (bc.type == BC_SYMMETRY && nn == 0.0) {
+    if ((bc.type == BC_SYMMETRY || bc.type == BC_AXIS) && nn == 0.0) {
 #pragma unroll
         for (int f = 0; f < NF; ++f) flux[f] = 0;
         return;
@@ -638,9 +648,13 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
     // shift cancels only where the volume operator annihilates a constant flux;
     // the reference's 3D Navier-Stokes volume term (quirks == 0) stores the eta
     // flux in the symmetric zeta slot (DGSEMIntegrator.cpp:702), so there pref = 0.
+    // axisymmetric (z, r) form (DGSEMIntegrator.cpp AXISYMMETRIC parts): fluxes
+    // weighted by r, a pressure source; r-weighting also breaks the constant-
+    // pressure cancellation, so the FP32 shift is off there
+    const double *rad = (DIM == 2 && !NS) ? a.rad : nullptr;
     double pref = 0.0;
     if constexpr (!LY::F64) {
-        if (!(DIM == 3 && NS && P.quirks == 0)) {
+        if (!(DIM == 3 && NS && P.quirks == 0) && !rad) {
             double s0[NF];
 #pragma unroll
             for (int f = 0; f < NF; ++f) s0[f] = __ldg(a.u + f * Ndof + (long long)e * ND);
@@ -862,6 +876,12 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
             Real F[NF];
             volume_flux<DIM, Real>(load_prim<DIM, ND, Real>(sH, int(pr & 0xffffu)),
                                    load_prim<DIM, ND, Real>(sH, int(pr >> 16)), mt, gm1i, F);
+            if (rad) {   // f *= r at the pair's reference midpoint (:273-291, :319-338)
+                const Real rh = Real(0.5 * (__ldg(rad + (long long)e * ND + int(pr & 0xffffu)) +
+                                            __ldg(rad + (long long)e * ND + int(pr >> 16))));
+#pragma unroll
+                for (int f = 0; f < NF; ++f) F[f] *= rh;
+            }
 #pragma unroll
             for (int f = 0; f < NF; ++f) sF[f * NPD + p] = F[f];
         }
@@ -912,6 +932,17 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
             if (NS) v += dUv[k][f];
             acc[k][f] = v * mJ;
         }
+    if (rad) {   // + p on the radial momentum (DGSEMIntegrator.cpp:411-428), not blended
+#pragma unroll
+        for (int k = 0; k < NPL; ++k) {
+            const int n = li + k * GS;
+            if (n < ND) {
+                const Prim<DIM, Real> q = load_prim<DIM, ND, Real>(sH, n);
+                if constexpr (LY::F64) acc[k][2] += Real(0.5) * q.rbeta * q.rho;
+                else acc[k][2] += q.dp;   // pref = 0 here: dp is p
+            }
+        }
+    }
 
     // ---- subcell first-order FV (DGSEMIntegrator.cpp:972-1196), skipped when alpha == 0
     if (P.blending && alpha != Real(0)) {
@@ -931,6 +962,11 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) { s1[1 + d] = q1.rho * q1.v[d]; s2[1 + d] = q2.rho * q2.v[d]; }
                 face_flux<DIM, Real>(s1, q1, s2, q2, nor, gm1i, P.quirks == 0, true, F);
+                if (rad) {   // DGSEMIntegrator.cpp:979-1031, 1096-1111
+                    const Real rh = Real(0.5 * (__ldg(rad + (long long)e * ND + n1) + __ldg(rad + (long long)e * ND + n2)));
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) F[f] *= rh;
+                }
 #pragma unroll
                 for (int f = 0; f < NF; ++f) sF[f * NID + it] = F[f];
             }
@@ -1015,6 +1051,11 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
             for (int q = 0; q < DIM; ++q) nb[q] = x.nb[q];
             const BcDev &bc = a.bcs[t.y];
             boundary_flux<DIM, Real>(bc, sb, nb, P, pref, fb);
+            if (rad) {   // BdrFaceIntegrator.cpp:109-111
+                const Real rr = Real(__ldg(rad + go));
+#pragma unroll
+                for (int f = 0; f < NF; ++f) fb[f] *= rr;
+            }
 #pragma unroll
             for (int f = 0; f < NF; ++f) fv[f] = 0;
             if constexpr (NS) {
@@ -1133,6 +1174,11 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
             face_flux<DIM, Real>(mo, po, mn, pn, nor, gm1i, P.quirks == 0, P.dissipation != 0, flux);
         else
             face_flux<DIM, Real>(mn, pn, mo, po, nor, gm1i, P.quirks == 0, P.dissipation != 0, flux);
+        if (rad) {   // DGSEMIntegrator.cpp:190-207: r at the face point, from element 1
+            const Real rr = Real(__ldg(rad + (own_is_1 ? go : gn)));
+#pragma unroll
+            for (int f = 0; f < NF; ++f) flux[f] *= rr;
+        }
 #pragma unroll
         for (int f = 0; f < NF; ++f) sF[f * NFI + it] = aw * (own_is_1 ? (fn[f] - flux[f]) : (flux[f] - fn[f]));
       }
@@ -1156,7 +1202,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 const long long g = f * Ndof + gnode;
-                ua[kk][f] = (k0 + kk < NPL && n < ND && mode != EPI_STORE) ? __ldg(a.u + g) : 0.0;
+                ua[kk][f] = (k0 + kk < NPL && n < ND && mode != EPI_STORE) ? __ldg((a.u_rk ? a.u_rk : a.u) + g) : 0.0;
                 ub[kk][f] = (k0 + kk < NPL && n < ND && need_b) ? pb[g] : 0.0;
             }
         }
@@ -1179,6 +1225,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 }
             }
             const long long gnode = (long long)e * ND + n;
+            if (rad && a.axis && a.axis[gnode]) acc[k][2] = 0;   // DGSEMOperator::ZeroAxisRadialMom
             switch (mode) {
             case EPI_STORE:
 #pragma unroll
@@ -1556,6 +1603,9 @@ lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_
     io.Ndof = m.Ndof;
     io.E = m.E;
     io.bcs = m.bcs;
+    io.u_rk = nullptr;
+    io.rad = nullptr;
+    io.axis = nullptr;
     lift_element<DIM, NP, Out, VC>(io, P, active ? e_raw : m.E - 1, active, smem,
                                smem + S::TAB + el * LiftLayout<DIM, NP>::PER_ELEM, n);
 }

@@ -101,7 +101,98 @@ __global__ void batch_step_end_kernel(BatchInst *tab, const int *live, const int
         }
     }
 }
+
+// DGSEMOperator::RecoverStateFromWeighted (DGSEMOperator.cpp:161-470) with the
+// low-order axis reconstruction the reference selects for "axis" boundaries
+// (Simulation.cpp:520-530).  One thread per node: off the axis U = rU / r; at
+// an axis node (or r <= 0) each field is d(rU)/dr from the two nearest
+// off-axis nodes of the element at the same z (else the two nearest overall):
+// the least-squares slope through the origin, limited by minmod against 1.5x
+// each node's own slope and clamped to 10 |f1| / r1 (one node: its slope).  A
+// non-finite or too small density or non-finite energy takes the nearest
+// off-axis node's U instead; radial momentum is 0 there.  Products and sums
+// are rounded separately (no contraction) so the result is the host's bit
+// for bit.
+__device__ __forceinline__ double axi_sign(double a) { return (double)((a > 0) - (a < 0)); }
+__device__ __forceinline__ double axi_minmod(double a, double b) {
+    return __dmul_rn(a, b) <= 0.0 ? 0.0 : axi_sign(a) * fmin(fabs(a), fabs(b));
+}
+__device__ __forceinline__ double axi_clamp(double x, double m) {
+    if (!isfinite(x)) return 0.0;
+    return fabs(x) <= m ? x : axi_sign(x) * m;
+}
+
+__global__ void axi_recover_kernel(const double *__restrict__ rU, double *__restrict__ U,
+                                   const double *__restrict__ xy, const unsigned char *__restrict__ axis,
+                                   long long Ndof, int ND) {
+    constexpr int NF = 4;
+    const double inf = __longlong_as_double(0x7ff0000000000000ll);
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < Ndof;
+         g += (long long)gridDim.x * blockDim.x) {
+        const double *rr = xy + Ndof;
+        const double r = rr[g];
+        if (!axis[g] && r > 0.0) {
+#pragma unroll
+            for (int f = 0; f < NF; ++f) U[f * Ndof + g] = rU[f * Ndof + g] / r;
+            continue;
+        }
+        const long long g0 = (g / ND) * ND;
+        const double z_axis = xy[g];
+        int j1 = -1, j2 = -1;
+        double r1 = inf, r2 = inf;
+        for (int pass = 0; pass < 2 && j1 < 0; ++pass)
+            for (int j = 0; j < ND; ++j) {
+                const double rj = rr[g0 + j];
+                if (!(rj > 0.0)) continue;
+                if (pass == 0 && !(fabs(xy[g0 + j] - z_axis) <= 1e-12)) continue;
+                if (rj < r1) { r2 = r1; j2 = j1; r1 = rj; j1 = j; }
+                else if (rj < r2) { r2 = rj; j2 = j; }
+            }
+        double d[NF];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            const double *fe = rU + f * Ndof + g0;
+            const double f_ref = j1 >= 0 ? fabs(fe[j1]) : 0.0;
+            const double cap = (j1 >= 0 && !(f_ref < 1e-12)) ? __dmul_rn(10.0, f_ref) / fmax(r1, 1e-14) : inf;
+            double v = 0.0;
+            if (j1 >= 0 && j2 >= 0 && isfinite(r1) && isfinite(r2) && r1 > 0.0 && r2 > 0.0) {
+                const double f1 = fe[j1], f2 = fe[j2];
+                const double m = __dadd_rn(__dmul_rn(r1, f1), __dmul_rn(r2, f2)) /
+                                 fmax(__dadd_rn(__dmul_rn(r1, r1), __dmul_rn(r2, r2)), 1e-14);
+                const double s1 = f1 / r1, s2 = f2 / r2;
+                v = axi_clamp(axi_minmod(m, axi_minmod(__dmul_rn(1.5, s1), __dmul_rn(1.5, s2))), cap);
+            } else if (j1 >= 0 && isfinite(r1) && r1 > 0.0) {
+                v = axi_clamp(fe[j1] / r1, cap);
+            }
+            d[f] = v;
+        }
+        if (!isfinite(d[0]) || d[0] < 1e-12 || !isfinite(d[3])) {
+            int nb = -1;
+            double rn = -1.0;
+            for (int j = 0; j < ND; ++j) {
+                const double rj = rr[g0 + j];
+                if (rj > 0.0 && (nb == -1 || rj < rn)) { rn = rj; nb = j; }
+            }
+#pragma unroll
+            for (int f = 0; f < NF; ++f) U[f * Ndof + g] = nb < 0 ? 0.0 : rU[f * Ndof + g0 + nb] / rn;
+            U[2 * Ndof + g] = 0.0;
+        } else {
+            U[g] = d[0];
+            U[Ndof + g] = d[1];
+            U[2 * Ndof + g] = 0.0;
+            U[3 * Ndof + g] = d[3];
+        }
+    }
+}
 }   // namespace
+
+cudaError_t launch_axi_recover(const double *rU, double *U, const double *xy, const unsigned char *axis,
+                               long long Ndof, int ND, cudaStream_t s) {
+    if (Ndof <= 0) return cudaSuccess;
+    const long long blocks = (Ndof + 255) / 256;
+    axi_recover_kernel<<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, s>>>(rU, U, xy, axis, Ndof, ND);
+    return cudaGetLastError();
+}
 
 cudaError_t batch_launch_step_end(BatchInst *tab, const int *live, const int *n_live, int flip, int *left,
                                   cudaStream_t s) {

@@ -23,6 +23,9 @@ struct MeshDev {
     int E;
     long long Ndof;      // E * Np^DIM
     const BcDev *bcs;    // boundary conditions (boundary faces: nbr = {-1, bc, face id, 0})
+    // axisymmetric (z, r) form, 2D Euler (null otherwise)
+    const double *rad;            // [Ndof] node radius
+    const unsigned char *axis;    // [Ndof] 1 at axis nodes
 };
 
 struct RhsArgs {
@@ -37,6 +40,7 @@ struct RhsArgs {
     double dt, rkA, rkB;
     int mode;
     const float *grad32;    // NS: primitive gradients, FP32-bulk form
+    const double *u_rk;     // axisymmetric: the RK state r U (u holds the recovered U); else null
 };
 
 struct LiftArgs {
@@ -117,6 +121,9 @@ cudaError_t batch_launch_lift(int dim, int order, bool vc, bool fp32, int grid, 
 // End of a batch step: every live solve with steps left advances its counters,
 // flips its LSRK parity, (cfl > 0) takes its next dt from lambda, and writes
 // its remaining step count to left[id].
+// Axisymmetric form: U recovered from the weighted state rU (2D, 4 fields).
+cudaError_t launch_axi_recover(const double *rU, double *U, const double *xy, const unsigned char *axis,
+                               long long Ndof, int ND, cudaStream_t s);
 cudaError_t batch_launch_step_end(BatchInst *tab, const int *live, const int *n_live, int flip, int *left,
                                   cudaStream_t s);
 

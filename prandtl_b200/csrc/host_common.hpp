@@ -236,9 +236,13 @@ inline prandtl_status check_bcs(const prandtl_config *cfg, int dim, std::string 
     for (int k = 0; k < cfg->num_bcs; ++k) {
         const prandtl_bc &b = cfg->bcs[k];
         const std::string tag = "boundary condition " + std::to_string(k);
-        if (b.type < PRANDTL_BC_STATE || b.type > PRANDTL_BC_NOSLIP_ISOTHERMAL) {
+        if (b.type < PRANDTL_BC_STATE || b.type > PRANDTL_BC_AXIS) {
             msg = tag + ": unknown type";
             return PRANDTL_EINVAL;
+        }
+        if (b.type == PRANDTL_BC_AXIS && !cfg->axisymmetric) {
+            msg = tag + ": the axis condition needs the axisymmetric form";
+            return PRANDTL_EUNSUPPORTED;
         }
         if ((b.type == PRANDTL_BC_STATE || b.type == PRANDTL_BC_RIEMANN || b.type == PRANDTL_BC_INFLOW_RV) &&
             !(b.state[0] > 0.0)) {

@@ -42,6 +42,11 @@ struct prandtl_handle {
     double *d_alpha = nullptr;
     unsigned long long *d_lambda = nullptr;
     BcDev *d_bcs = nullptr;                       // boundary conditions
+    // axisymmetric form: node coordinates [2][Ndof], axis-node flags, and the
+    // state U recovered from the r-weighted RK state before each RHS
+    double *d_xy = nullptr;
+    unsigned char *d_axis = nullptr;
+    double *d_U = nullptr;
     size_t bytes = 0;
     long long launches = 0;
     // optional per-kernel CUDA-event timing (prandtl_profile)
@@ -112,6 +117,8 @@ MeshDev mesh_dev(const prandtl_handle *h) {
     m.E = h->E;
     m.Ndof = h->Ndof;
     m.bcs = h->d_bcs;
+    m.rad = h->d_xy ? h->d_xy + h->Ndof : nullptr;
+    m.axis = h->d_axis;
     return m;
 }
 
@@ -119,6 +126,13 @@ MeshDev mesh_dev(const prandtl_handle *h) {
 prandtl_status run_rhs(prandtl_handle *h, const double *u, RhsArgs a) {
     const MeshDev m = mesh_dev(h);
     a.u = u;
+    if (h->d_U) {   // axisymmetric: fluxes of U, the RK update of r U (DGSEMOperator::Mult)
+        cudaError_t e = launch_axi_recover(u, h->d_U, h->d_xy, h->d_axis, h->Ndof, h->nd, h->stream);
+        if (e != cudaSuccess) return cuda_fail(h, e, "axisymmetric recovery launch");
+        h->launches++;
+        a.u = h->d_U;
+        a.u_rk = u;
+    }
     const bool ns = h->cfg.parabolic != 0;
     const bool fp32 = h->cfg.precision == 1;
     if (ns) {
@@ -155,6 +169,9 @@ void free_all(prandtl_handle *h) {
     cudaFree(h->d_alpha);
     cudaFree(h->d_lambda);
     cudaFree(h->d_bcs);
+    cudaFree(h->d_xy);
+    cudaFree(h->d_axis);
+    cudaFree(h->d_U);
     if (h->done) cudaEventDestroy(h->done);
     for (auto &r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (auto ev : h->ev_pool) cudaEventDestroy(ev);
@@ -197,6 +214,10 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
     if (cfg->precision != 0 && cfg->precision != 1)
         return fail(nullptr, PRANDTL_EUNSUPPORTED, "precision must be 0 (FP64) or 1 (FP32 bulk)");
     if (!(cfg->gamma > 1.0) || !(cfg->Pr > 0.0)) return fail(nullptr, PRANDTL_EINVAL, "bad gamma/Pr");
+    if (cfg->axisymmetric && (md->dim != 2 || cfg->parabolic))
+        return fail(nullptr, PRANDTL_EUNSUPPORTED, "the axisymmetric form is 2D Euler");
+    if (cfg->axisymmetric && !cfg->node_coords)
+        return fail(nullptr, PRANDTL_EINVAL, "the axisymmetric form needs node_coords");
 
     const int dim = md->dim, E = md->num_elements, F = md->num_faces;
     std::vector<int4> nbr;
@@ -226,6 +247,7 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
     h->Ndof = (long long)E * h->nd;
     h->cfg = *cfg;
     h->cfg.bcs = nullptr;   // the caller's table is copied to the device below
+    h->cfg.node_coords = nullptr;   // likewise the axisymmetric node coordinates
     if (h->cfg.timeout_s <= 0) h->cfg.timeout_s = 120.0;
     build_tables(md->order, h->T);
     build_phys(h->cfg, md->order, h->P);
@@ -275,6 +297,27 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
         return bail(cuda_fail(h, ce, "upload normals"));
     if ((ce = cudaMemset(h->d_alpha, 0, (size_t)E * sizeof(double))) != cudaSuccess)
         return bail(cuda_fail(h, ce, "memset alpha"));
+    if (cfg->axisymmetric) {
+        // DGSEMOperator::BuildAxisIndexFromMarker (DGSEMOperator.cpp:482-518):
+        // nodes at |r| <= 1e-14 of the elements on axis boundary faces
+        std::vector<unsigned char> axis((size_t)h->Ndof, 0);
+        for (int f = 0; f < F; ++f) {
+            const int *fe = md->face_elems + 4 * f;
+            if (fe[2] >= 0 || cfg->bcs[fe[3]].type != PRANDTL_BC_AXIS) continue;
+            for (int n = 0; n < h->nd; ++n) {
+                const long long g = (long long)fe[0] * h->nd + n;
+                if (std::abs(cfg->node_coords[h->Ndof + g]) <= 1e-14) axis[(size_t)g] = 1;
+            }
+        }
+        if ((st = dalloc(h, &h->d_xy, (size_t)2 * h->Ndof, "node coordinates")) != PRANDTL_OK) return bail(st);
+        if ((st = dalloc(h, &h->d_axis, (size_t)h->Ndof, "axis nodes")) != PRANDTL_OK) return bail(st);
+        if ((st = dalloc(h, &h->d_U, S, "recovered state")) != PRANDTL_OK) return bail(st);
+        if ((ce = cudaMemcpy(h->d_xy, cfg->node_coords, (size_t)2 * h->Ndof * sizeof(double),
+                             cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail(cuda_fail(h, ce, "upload node coordinates"));
+        if ((ce = cudaMemcpy(h->d_axis, axis.data(), axis.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail(cuda_fail(h, ce, "upload axis nodes"));
+    }
     *out = h;
     return PRANDTL_OK;
 }

@@ -473,6 +473,10 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, 
     prandtl_status st = check_bcs(cfg, md->dim, msg);
     if (st == PRANDTL_OK) st = validate_mesh(md, nbr, msg, cfg->num_bcs);
     if (st == PRANDTL_OK) st = check_viscous_bcs(md, cfg, msg);
+    if (st == PRANDTL_OK && cfg->axisymmetric) {
+        st = PRANDTL_EUNSUPPORTED;
+        msg = "the axisymmetric form runs on a prandtl_create operator, not in a batch";
+    }
     if (st != PRANDTL_OK) return bfail(b, st, msg);
     BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
     const int dim = md->dim, order = md->order, E = md->num_elements, F = md->num_faces;

@@ -218,6 +218,7 @@ extern "C" prandtl_status prandtl_rhs_noalloc(const prandtl_mesh_desc *m, const 
     if (!m->elem_adj || !m->elem_detj || !m->face_elems || !m->face_nor)
         return fail(PRANDTL_EINVAL, "mesh arrays missing");
     if (cfg->precision != 0) return fail(PRANDTL_EUNSUPPORTED, "only precision 0 (FP64) is built");
+    if (cfg->axisymmetric) return fail(PRANDTL_EUNSUPPORTED, "the axisymmetric form needs prandtl_create");
     if (!(cfg->gamma > 1.0) || !(cfg->Pr > 0.0)) return fail(PRANDTL_EINVAL, "bad gamma/Pr");
 
     const int dim = m->dim, E = m->num_elements, F = m->num_faces, NFACE = 2 * dim;
@@ -284,7 +285,7 @@ extern "C" prandtl_status prandtl_rhs_noalloc(const prandtl_mesh_desc *m, const 
     P.dissipation = cfg->surface_dissipation;
     P.blending = cfg->blending;
 
-    MeshDev md;
+    MeshDev md{};
     md.geo = geo;
     md.nbr = nbr;
     md.fnor = m->face_nor;

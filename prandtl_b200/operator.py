@@ -80,9 +80,11 @@ def make_bcs(bcs):
 
 def make_config(*, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05, parabolic=False, blending=False,
                 sutherland=False, alpha_max=0.5, alpha_min=0.001, quirks="reference",
-                surface_dissipation=True, precision="fp64", timeout_s=120.0, bcs=None) -> _lib.Config:
-    """prandtl_config from the DGSEMOperator keyword arguments (the BC array is
-    kept alive on the returned object)."""
+                surface_dissipation=True, precision="fp64", timeout_s=120.0, bcs=None,
+                axisymmetric=False, node_coords=None) -> _lib.Config:
+    """prandtl_config from the DGSEMOperator keyword arguments (the BC array
+    and the axisymmetric node coordinates are kept alive on the returned
+    object)."""
     cfg = _lib.Config()
     _lib.load().prandtl_config_default(C.byref(cfg))
     cfg.gamma, cfg.Pr, cfg.mu, cfg.R_gas = gamma, Pr, mu, R_gas
@@ -99,6 +101,10 @@ def make_config(*, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05, parabolic=False, b
     cfg._bcs = make_bcs(bcs)
     cfg.num_bcs = len(bcs) if bcs else 0
     cfg.bcs = cfg._bcs
+    cfg.axisymmetric = int(bool(axisymmetric))
+    if axisymmetric and node_coords is not None:
+        cfg._xy = np.ascontiguousarray(node_coords, dtype=np.float64)
+        cfg.node_coords = cfg._xy.ctypes.data_as(C.POINTER(C.c_double))
     return cfg
 
 
@@ -106,7 +112,9 @@ class DGSEMOperator:
     def __init__(self, mesh: Mesh, *, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05,
                  parabolic=False, blending=False, sutherland=False, alpha_max=0.5,
                  alpha_min=0.001, quirks="reference", surface_dissipation=True,
-                 precision="fp64", timeout_s=120.0, bcs=None):
+                 precision="fp64", timeout_s=120.0, bcs=None, axisymmetric=False):
+        """axisymmetric: the reference's AXISYMMETRIC build -- 2D Euler in
+        (z, r) = (x, y); Mult takes and returns the r-weighted state r U."""
         L = _lib.load()
         self.mesh = mesh
         self._arrays = MeshArrays(mesh)
@@ -114,7 +122,8 @@ class DGSEMOperator:
         cfg = make_config(gamma=gamma, Pr=Pr, mu=mu, R_gas=R_gas, parabolic=parabolic,
                           blending=blending, sutherland=sutherland, alpha_max=alpha_max,
                           alpha_min=alpha_min, quirks=quirks, surface_dissipation=surface_dissipation,
-                          precision=precision, timeout_s=timeout_s, bcs=bcs)
+                          precision=precision, timeout_s=timeout_s, bcs=bcs,
+                          axisymmetric=axisymmetric, node_coords=mesh.coords if axisymmetric else None)
         h = C.c_void_p()
         _lib.check(L.prandtl_create(C.byref(desc), C.byref(cfg), C.byref(h)), None)
         self._h = h

@@ -94,6 +94,27 @@ BC_SETS = {"walls": (BOUNDARY_CASES, BCS, SIDES, 0), "char": (CHAR_CASES, CHAR_B
            "ns_char": (NS_CHAR_CASES, NS_BCS, NS_CHAR_SIDES, 1)}
 
 
+# Axisymmetric (z, r) Euler (the reference built with AXISYMMETRIC): state r U
+# on a sheared box over 0 <= r <= 1 with the axis at r = 0;
+# (name, n, order, blending, amplitude, seed).
+AXI_BCS = [("state", [1.3, 0.5, 0.0, 2.9]), ("outflow",), ("axis",), ("slip_wall",)]
+AXI_SIDES = [0, 1, 2, 3]
+AXI_CASES = [
+    ("axi2d_n4x3_N1", (4, 3), 1, 0, 0.10, 31),
+    ("axi2d_n4x3_N3", (4, 3), 3, 0, 0.10, 32),
+    ("axi2d_blend_n4x3_N2", (4, 3), 2, 1, 0.30, 33),
+    ("axi2d_blend_n3x2_N4", (3, 2), 4, 1, 0.30, 34),
+]
+
+
+def axi_inputs(n, order, blending, amp, seed):
+    mesh = periodic_box(2, n, order, (0.0, 0.0), (2.0, 1.0), bcs=AXI_SIDES,
+                        affine=np.array([[1.0, 0.1], [0.0, 1.0]]))
+    U = cases.perturbed(mesh, cases.free_stream(mesh, rho=1.2, vel=[0.3, 0.05], p=1.5),
+                        amp=amp, seed=seed).reshape(4, -1)
+    return mesh, (U * mesh.coords[1][None, :]).reshape(-1)
+
+
 def bc_example(kind, dim):
     """One condition of the given type with constant data for a dim-D case;
     "riemann_supersonic" is the Riemann condition with a supersonic outer state."""
@@ -134,8 +155,14 @@ def main():
             out[f"{name}/u"] = u
             out[f"{name}/dudt"] = r["dudt"]
             out[f"{name}/alpha"] = r["alpha"]
+    for name, n, order, bl, amp, seed in AXI_CASES:
+        mesh, u = axi_inputs(n, order, bl, amp, seed)
+        r = pyoracle.RefOperator(mesh, blending=bl, bcs=AXI_BCS, axisymmetric=1).rhs(u, want_alpha=True)
+        out[f"{name}/u"] = u
+        out[f"{name}/dudt"] = r["dudt"]
+        out[f"{name}/alpha"] = r["alpha"]
     np.savez_compressed(os.path.join(HERE, "reference_rhs.npz"), **out)
-    print(f"wrote {len(CASES) + sum(len(v[0]) for v in BC_SETS.values())} cases")
+    print(f"wrote {len(CASES) + sum(len(v[0]) for v in BC_SETS.values()) + len(AXI_CASES)} cases")
 
 
 if __name__ == "__main__":

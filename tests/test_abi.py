@@ -164,3 +164,36 @@ def test_boundary_tables_validated_before_touching_the_device(lib):
         assert st in (_lib.PRANDTL_ECUDA, _lib.PRANDTL_OK), kw
         if st == _lib.PRANDTL_OK:
             lib.prandtl_destroy(h)
+
+
+def test_axisymmetric_configuration_checked_before_the_device(lib):
+    """The axisymmetric form is 2D Euler with node coordinates; the axis
+    condition needs it; the no-alloc entry point leaves it to prandtl_create.
+    All checked before device work."""
+    from prandtl_b200 import _lib
+    from prandtl_b200.mesh import periodic_box
+    from prandtl_b200.operator import make_config
+    keep = []
+    h = C.c_void_p()
+    m = periodic_box(2, (3, 2), 2, (0.0, 0.0), (1.0, 1.0), bcs=[0, 0, 1, 0])
+    d = _desc(m, keep)
+    bcs = [("outflow",), ("axis",)]
+    cfg = make_config(bcs=bcs)   # axis without the axisymmetric form
+    assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EUNSUPPORTED
+    assert b"axisymmetric" in lib.prandtl_last_error(None)
+    cfg = make_config(bcs=bcs, axisymmetric=True)   # no node coordinates
+    assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EINVAL
+    cfg = make_config(bcs=bcs, axisymmetric=True, node_coords=m.coords, parabolic=True)
+    assert lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EUNSUPPORTED
+    m3 = periodic_box(3, 2, 2)
+    d3 = _desc(m3, keep)
+    cfg = make_config(axisymmetric=True, node_coords=m3.coords)
+    assert lib.prandtl_create(C.byref(d3), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EUNSUPPORTED
+    cfg = make_config(bcs=bcs, axisymmetric=True, node_coords=m.coords)
+    st = lib.prandtl_create(C.byref(d), C.byref(cfg), C.byref(h))
+    assert st in (_lib.PRANDTL_ECUDA, _lib.PRANDTL_OK)
+    if st == _lib.PRANDTL_OK:
+        lib.prandtl_destroy(h)
+    u = np.zeros(m.num_fields * m.ndof)
+    assert lib.prandtl_rhs_noalloc(C.byref(d), C.byref(cfg), u.ctypes.data, u.ctypes.data, None) == \
+        _lib.PRANDTL_EUNSUPPORTED

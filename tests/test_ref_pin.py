@@ -198,3 +198,17 @@ def test_oracle_axisymmetric_matches_reference_sources(oracle_mod, order, bl):
     o = oracle_mod.Oracle(mesh, **kw).rhs(rU)["dudt"]
     r = oracle_mod.RefOperator(mesh, **kw).rhs(rU)["dudt"]
     assert normalized_error(o, r, 4) <= 1e-13
+
+
+@pytest.mark.parametrize("case", make_golden.AXI_CASES, ids=[c[0] for c in make_golden.AXI_CASES])
+def test_oracle_axisymmetric_matches_reference_golden(oracle_mod, case):
+    """The committed outputs of the reference's AXISYMMETRIC build (runs on any
+    host: no reference sources needed)."""
+    name, n, order, bl, amp, seed = case
+    mesh, u = make_golden.axi_inputs(n, order, bl, amp, seed)
+    np.testing.assert_array_equal(u, GOLDEN[f"{name}/u"])
+    r = oracle_mod.Oracle(mesh, quirks=0, blending=bl, bcs=make_golden.AXI_BCS, axisymmetric=1).rhs(u, want_alpha=True)
+    assert normalized_error(r["dudt"], GOLDEN[f"{name}/dudt"], mesh.num_fields) <= PIN_TOL
+    np.testing.assert_allclose(r["alpha"], GOLDEN[f"{name}/alpha"], rtol=0, atol=1e-14)
+    if bl:
+        assert (r["alpha"] > 0).any()
