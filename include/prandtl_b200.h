@@ -130,6 +130,9 @@ typedef struct prandtl_config {
                                   fluxes carry r, + p on the radial momentum; 0: planar */
     const double *node_coords; /* axisymmetric: [dim][Ndof] node coordinates (byNODES, the state's
                                   node order), copied at create; else ignored */
+    double axis_rho_floor;     /* axisymmetric: density floor of the axis reconstruction; 0 selects
+                                  1e-12 (DGSEMOperator.hpp:44).  The reference's driver raises it to
+                                  max(1e-12, 1e-8 rho_inf) (SetAxisFloorsFromFreestream) */
 } prandtl_config;
 
 typedef struct prandtl_handle prandtl_handle;
@@ -161,6 +164,13 @@ prandtl_status prandtl_step(prandtl_handle *h, double *u, double t, double dt, i
 /* Per-element blending coefficient of the last RHS evaluation ([E] values;
  * the reference's `alpha` ParGridFunction on fes0). */
 prandtl_status prandtl_get_alpha(prandtl_handle *h, double *alpha, int ptr_flags);
+
+/* Axisymmetric form: the conserved state U recovered from the r-weighted state
+ * rU ([4][Ndof] each), as every RHS evaluation sees it
+ * (DGSEMOperator::RecoverStateFromWeighted, DGSEMOperator.cpp:161-470; the
+ * reference's output fields are the primitives of this U, Simulation.cpp:1041-1044).
+ * PRANDTL_EUNSUPPORTED for a planar operator. */
+prandtl_status prandtl_recover_state(prandtl_handle *h, const double *rU, double *U, int ptr_flags);
 
 /* CFL step dt = cfl*hmin/(lambda_max*(N+1)^2) (Simulation.cpp:906,1017). */
 double prandtl_cfl_dt(double cfl, double hmin, double lambda_max, int order);

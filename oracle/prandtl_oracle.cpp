@@ -429,6 +429,7 @@ struct Ctx {
     const oracle_bc *bcs;
     int axi;                       // axisymmetric (z, r) form
     const double *xy;              // [dim][Ndof] node coordinates
+    double axis_rho_floor;         // DGSEMOperator.hpp:44 rho_floor_abs
     std::vector<char> on_axis;     // [Ndof] axis nodes (DGSEMOperator::BuildAxisIndexFromMarker)
     double r(long g) const { return xy[Ndof + g]; }
     double alpha_max, alpha_min, modalThreshold;
@@ -474,6 +475,7 @@ void setup(Ctx &X, const oracle_mesh *m, const oracle_config *c) {
     X.bcs = c->bcs;
     X.axi = c->axisymmetric;
     X.xy = c->node_coords;
+    X.axis_rho_floor = c->axis_rho_floor > 0.0 ? c->axis_rho_floor : 1e-12;
     if (X.axi) {   // DGSEMOperator.cpp:482-518: nodes at |r| <= 1e-14 of elements on "axis" boundaries
         X.on_axis.assign(X.Ndof, 0);
         for (int f = 0; f < X.F; ++f) {
@@ -1064,7 +1066,8 @@ void element_lift(const Ctx &X, int e, const double *v, double *gout /*[dim][nd]
 int recover_weighted(const Ctx &X, const double *rU, double *U) {
     const int nd = X.nd, nf = X.nf;
     const long Ndof = X.Ndof;
-    const double tiny = 1e-14, cap_mult = 10.0, z_tol = 1e-12, theta_lim = 1.5, rho_floor = 1e-12;
+    const double tiny = 1e-14, cap_mult = 10.0, z_tol = 1e-12, theta_lim = 1.5;
+    const double rho_floor = X.axis_rho_floor;
     const double inf = std::numeric_limits<double>::infinity();
     auto sign = [](double a) { return (double)((a > 0) - (a < 0)); };
     auto minmod = [&](double a, double b) { return a * b <= 0.0 ? 0.0 : sign(a) * std::min(std::abs(a), std::abs(b)); };

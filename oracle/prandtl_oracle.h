@@ -83,6 +83,7 @@ typedef struct oracle_config {
     const oracle_bc *bcs;
     int axisymmetric;         /* 2D Euler in (z, r): u is r U (AXISYMMETRIC build of the reference) */
     const double *node_coords;/* [dim][Ndof] node coordinates (axisymmetric: r = coordinate 1) */
+    double axis_rho_floor;    /* axis density floor of the recovery; <= 0 selects 1e-12 */
 } oracle_config;
 
 /* Axisymmetric form: U recovered from the weighted state rU (the input every

@@ -40,7 +40,8 @@ class OracleConfig(C.Structure):
                 ("parabolic", C.c_int), ("blending", C.c_int), ("sutherland", C.c_int),
                 ("quirks", C.c_int), ("surface_dissipation", C.c_int),
                 ("num_bcs", C.c_int), ("bcs", C.POINTER(OracleBC)),
-                ("axisymmetric", C.c_int), ("node_coords", C.POINTER(C.c_double))]
+                ("axisymmetric", C.c_int), ("node_coords", C.POINTER(C.c_double)),
+                ("axis_rho_floor", C.c_double)]
 
 
 def make_bcs(bcs):
@@ -105,7 +106,8 @@ class Oracle:
 
     def __init__(self, mesh, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05, alpha_max=0.5,
                  alpha_min=0.001, parabolic=0, blending=0, sutherland=0, quirks=0,
-                 surface_dissipation=1, nthreads=None, bcs=None, axisymmetric=0):
+                 surface_dissipation=1, nthreads=None, bcs=None, axisymmetric=0,
+                 axis_rho_floor=0.0):
         self.mesh = mesh
         self._adj = np.ascontiguousarray(mesh.elem_adj, dtype=np.float64)
         self._detj = np.ascontiguousarray(mesh.elem_detj, dtype=np.float64)
@@ -118,7 +120,7 @@ class Oracle:
         self._xy = np.ascontiguousarray(mesh.coords, dtype=np.float64)
         self.c = OracleConfig(gamma, Pr, mu, R_gas, alpha_max, alpha_min, parabolic, blending,
                               sutherland, quirks, surface_dissipation, len(bcs) if bcs else 0,
-                              self._bcs, int(axisymmetric), _p(self._xy))
+                              self._bcs, int(axisymmetric), _p(self._xy), float(axis_rho_floor))
         self.nthreads = nthreads or os.cpu_count() or 1
 
     @property

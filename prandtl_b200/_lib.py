@@ -25,7 +25,7 @@ EXPORTS = ["prandtl_config_default", "prandtl_create", "prandtl_destroy", "prand
            "prandtl_step", "prandtl_get_alpha", "prandtl_cfl_dt", "prandtl_set_stream",
            "prandtl_synchronize", "prandtl_kernel_launches", "prandtl_profile",
            "prandtl_profile_read", "prandtl_profile_reset", "prandtl_device_bytes",
-           "prandtl_last_error", "prandtl_version", "prandtl_rhs_noalloc",
+           "prandtl_last_error", "prandtl_version", "prandtl_rhs_noalloc", "prandtl_recover_state",
            "prandtl_batch_config_default", "prandtl_batch_create", "prandtl_batch_destroy",
            "prandtl_batch_footprint", "prandtl_batch_add", "prandtl_batch_advance",
            "prandtl_batch_sync", "prandtl_batch_finished", "prandtl_batch_query",
@@ -67,7 +67,8 @@ class Config(C.Structure):
                 ("parabolic", C.c_int), ("blending", C.c_int), ("sutherland", C.c_int),
                 ("quirks", C.c_int), ("surface_dissipation", C.c_int), ("precision", C.c_int),
                 ("timeout_s", C.c_double), ("num_bcs", C.c_int), ("bcs", C.POINTER(BC)),
-                ("axisymmetric", C.c_int), ("node_coords", C.POINTER(C.c_double))]
+                ("axisymmetric", C.c_int), ("node_coords", C.POINTER(C.c_double)),
+                ("axis_rho_floor", C.c_double)]
 
 
 class BatchConfig(C.Structure):
@@ -116,6 +117,8 @@ def load():
     L.prandtl_step.restype = ip
     L.prandtl_get_alpha.argtypes = [vp, vp, ip]
     L.prandtl_get_alpha.restype = ip
+    L.prandtl_recover_state.argtypes = [vp, vp, vp, ip]
+    L.prandtl_recover_state.restype = ip
     L.prandtl_cfl_dt.argtypes = [C.c_double, C.c_double, C.c_double, ip]
     L.prandtl_cfl_dt.restype = C.c_double
     L.prandtl_set_stream.argtypes = [vp, vp]

@@ -41,7 +41,11 @@ def load_checkpoint(folder: str, cycle: int, mesh: Mesh, rank: int = 0):
 
 def save_paraview(folder: str, name: str, cycle: int, time: float, mesh: Mesh, u: np.ndarray, alpha=None,
                   gamma: float = 1.4, binary: bool = True):
-    """ParaView collection ``<folder>/<name>/<name>.pvd`` with this cycle added."""
+    """ParaView collection ``<folder>/<name>/<name>.pvd`` with this cycle added.
+
+    u is the conserved state; for the axisymmetric form pass the recovered U
+    (``DGSEMOperator.recover_state(rU)``), as the reference writes its fields
+    from it (Simulation.cpp:1041-1044)."""
     u = np.ascontiguousarray(u, dtype=np.float64)
     coords = np.ascontiguousarray(mesh.coords, dtype=np.float64)
     a = None if alpha is None else np.ascontiguousarray(alpha, dtype=np.float64)

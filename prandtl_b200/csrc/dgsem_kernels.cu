@@ -109,8 +109,8 @@ __global__ void batch_step_end_kernel(BatchInst *tab, const int *live, const int
 // off-axis nodes of the element at the same z (else the two nearest overall):
 // the least-squares slope through the origin, limited by minmod against 1.5x
 // each node's own slope and clamped to 10 |f1| / r1 (one node: its slope).  A
-// non-finite or too small density or non-finite energy takes the nearest
-// off-axis node's U instead; radial momentum is 0 there.  Products and sums
+// density that is non-finite or below rho_floor, or a non-finite energy, takes
+// the nearest off-axis node's U instead; radial momentum is 0 there.  Products and sums
 // are rounded separately (no contraction) so the result is the host's bit
 // for bit.
 __device__ __forceinline__ double axi_sign(double a) { return (double)((a > 0) - (a < 0)); }
@@ -124,7 +124,7 @@ __device__ __forceinline__ double axi_clamp(double x, double m) {
 
 __global__ void axi_recover_kernel(const double *__restrict__ rU, double *__restrict__ U,
                                    const double *__restrict__ xy, const unsigned char *__restrict__ axis,
-                                   long long Ndof, int ND) {
+                                   long long Ndof, int ND, double rho_floor) {
     constexpr int NF = 4;
     const double inf = __longlong_as_double(0x7ff0000000000000ll);
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < Ndof;
@@ -166,7 +166,7 @@ __global__ void axi_recover_kernel(const double *__restrict__ rU, double *__rest
             }
             d[f] = v;
         }
-        if (!isfinite(d[0]) || d[0] < 1e-12 || !isfinite(d[3])) {
+        if (!isfinite(d[0]) || d[0] < rho_floor || !isfinite(d[3])) {
             int nb = -1;
             double rn = -1.0;
             for (int j = 0; j < ND; ++j) {
@@ -187,10 +187,10 @@ __global__ void axi_recover_kernel(const double *__restrict__ rU, double *__rest
 }   // namespace
 
 cudaError_t launch_axi_recover(const double *rU, double *U, const double *xy, const unsigned char *axis,
-                               long long Ndof, int ND, cudaStream_t s) {
+                               long long Ndof, int ND, double rho_floor, cudaStream_t s) {
     if (Ndof <= 0) return cudaSuccess;
     const long long blocks = (Ndof + 255) / 256;
-    axi_recover_kernel<<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, s>>>(rU, U, xy, axis, Ndof, ND);
+    axi_recover_kernel<<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, s>>>(rU, U, xy, axis, Ndof, ND, rho_floor);
     return cudaGetLastError();
 }
 

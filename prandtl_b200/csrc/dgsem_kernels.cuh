@@ -123,7 +123,7 @@ cudaError_t batch_launch_lift(int dim, int order, bool vc, bool fp32, int grid, 
 // its remaining step count to left[id].
 // Axisymmetric form: U recovered from the weighted state rU (2D, 4 fields).
 cudaError_t launch_axi_recover(const double *rU, double *U, const double *xy, const unsigned char *axis,
-                               long long Ndof, int ND, cudaStream_t s);
+                               long long Ndof, int ND, double rho_floor, cudaStream_t s);
 cudaError_t batch_launch_step_end(BatchInst *tab, const int *live, const int *n_live, int flip, int *left,
                                   cudaStream_t s);
 

@@ -127,7 +127,9 @@ prandtl_status run_rhs(prandtl_handle *h, const double *u, RhsArgs a) {
     const MeshDev m = mesh_dev(h);
     a.u = u;
     if (h->d_U) {   // axisymmetric: fluxes of U, the RK update of r U (DGSEMOperator::Mult)
-        cudaError_t e = launch_axi_recover(u, h->d_U, h->d_xy, h->d_axis, h->Ndof, h->nd, h->stream);
+        cudaError_t e = launch_axi_recover(u, h->d_U, h->d_xy, h->d_axis, h->Ndof, h->nd,
+                                           h->cfg.axis_rho_floor > 0.0 ? h->cfg.axis_rho_floor : 1e-12,
+                                           h->stream);
         if (e != cudaSuccess) return cuda_fail(h, e, "axisymmetric recovery launch");
         h->launches++;
         a.u = h->d_U;
@@ -446,6 +448,27 @@ prandtl_status prandtl_get_alpha(prandtl_handle *h, double *alpha, int ptr_flags
     CK(h, cudaMemcpyAsync(alpha, h->d_alpha, (size_t)h->E * sizeof(double),
                           dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream),
        "copy alpha");
+    return wait_stream(h);
+}
+
+prandtl_status prandtl_recover_state(prandtl_handle *h, const double *rU, double *U, int ptr_flags) {
+    if (!h || !rU || !U) return h ? fail(h, PRANDTL_EINVAL, "null pointer") : PRANDTL_EINVAL;
+    std::lock_guard<std::mutex> lk(h->mu);
+    h->err.clear();
+    if (!h->d_U) return fail(h, PRANDTL_EUNSUPPORTED, "not an axisymmetric operator");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    const size_t bytes = (size_t)h->nf * h->Ndof * sizeof(double);
+    const bool dev = (ptr_flags & PRANDTL_PTR_DEVICE) != 0;
+    const double *src = rU;
+    if (!dev) {
+        CK(h, cudaMemcpyAsync(h->d_in, rU, bytes, cudaMemcpyHostToDevice, h->stream), "H2D rU");
+        src = h->d_in;
+    }
+    CK(h, launch_axi_recover(src, dev ? U : h->d_out, h->d_xy, h->d_axis, h->Ndof, h->nd,
+                             h->cfg.axis_rho_floor > 0.0 ? h->cfg.axis_rho_floor : 1e-12, h->stream),
+       "axisymmetric recovery launch");
+    h->launches++;
+    if (!dev) CK(h, cudaMemcpyAsync(U, h->d_out, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H U");
     return wait_stream(h);
 }
 

@@ -81,7 +81,7 @@ def make_bcs(bcs):
 def make_config(*, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05, parabolic=False, blending=False,
                 sutherland=False, alpha_max=0.5, alpha_min=0.001, quirks="reference",
                 surface_dissipation=True, precision="fp64", timeout_s=120.0, bcs=None,
-                axisymmetric=False, node_coords=None) -> _lib.Config:
+                axisymmetric=False, node_coords=None, axis_rho_floor=0.0) -> _lib.Config:
     """prandtl_config from the DGSEMOperator keyword arguments (the BC array
     and the axisymmetric node coordinates are kept alive on the returned
     object)."""
@@ -102,6 +102,7 @@ def make_config(*, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05, parabolic=False, b
     cfg.num_bcs = len(bcs) if bcs else 0
     cfg.bcs = cfg._bcs
     cfg.axisymmetric = int(bool(axisymmetric))
+    cfg.axis_rho_floor = float(axis_rho_floor)
     if axisymmetric and node_coords is not None:
         cfg._xy = np.ascontiguousarray(node_coords, dtype=np.float64)
         cfg.node_coords = cfg._xy.ctypes.data_as(C.POINTER(C.c_double))
@@ -112,9 +113,10 @@ class DGSEMOperator:
     def __init__(self, mesh: Mesh, *, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05,
                  parabolic=False, blending=False, sutherland=False, alpha_max=0.5,
                  alpha_min=0.001, quirks="reference", surface_dissipation=True,
-                 precision="fp64", timeout_s=120.0, bcs=None, axisymmetric=False):
+                 precision="fp64", timeout_s=120.0, bcs=None, axisymmetric=False, axis_rho_floor=0.0):
         """axisymmetric: the reference's AXISYMMETRIC build -- 2D Euler in
-        (z, r) = (x, y); Mult takes and returns the r-weighted state r U."""
+        (z, r) = (x, y); Mult takes and returns the r-weighted state r U.
+        axis_rho_floor: density floor of its axis reconstruction (0: 1e-12)."""
         L = _lib.load()
         self.mesh = mesh
         self._arrays = MeshArrays(mesh)
@@ -123,7 +125,8 @@ class DGSEMOperator:
                           blending=blending, sutherland=sutherland, alpha_max=alpha_max,
                           alpha_min=alpha_min, quirks=quirks, surface_dissipation=surface_dissipation,
                           precision=precision, timeout_s=timeout_s, bcs=bcs,
-                          axisymmetric=axisymmetric, node_coords=mesh.coords if axisymmetric else None)
+                          axisymmetric=axisymmetric, node_coords=mesh.coords if axisymmetric else None,
+                          axis_rho_floor=axis_rho_floor)
         h = C.c_void_p()
         _lib.check(L.prandtl_create(C.byref(desc), C.byref(cfg), C.byref(h)), None)
         self._h = h
@@ -164,6 +167,23 @@ class DGSEMOperator:
         out = np.empty(self.mesh.num_elements)
         _lib.check(self._L.prandtl_get_alpha(self._h, out.ctypes.data, _lib.PTR_HOST), self._h)
         return out
+
+    def recover_state(self, rU, U=None):
+        """Axisymmetric form: the conserved U that the fluxes see, recovered
+        from the r-weighted state rU (the reference writes its output fields
+        from this U)."""
+        if U is None:
+            if isinstance(rU, np.ndarray):
+                U = np.empty_like(rU)
+            else:
+                import torch
+                U = torch.empty_like(rU)
+        pr, fr = _ptr(rU)
+        pU, fU = _ptr(U)
+        if fr != fU:
+            raise ValueError("rU and U must both be host or both be device arrays")
+        _lib.check(self._L.prandtl_recover_state(self._h, pr, pU, fr), self._h)
+        return U
 
     def cfl_dt(self, cfl: float, lambda_max: float | None = None) -> float:
         lam = self.max_char_speed if lambda_max is None else lambda_max

@@ -106,3 +106,41 @@ def test_axisymmetric_fp32_rhs():
     op.Mult(u, d32)
     op.close()
     assert max(rel_l2(d32, d64, 4)) <= 2e-3
+
+
+def test_axisymmetric_density_floor_matches_oracle(oracle_mod):
+    """A raised axis density floor (the reference driver's 1e-8 rho_inf rule,
+    here far above the density) sends every axis node to the nearest-node copy."""
+    mesh, u = make_golden.axi_inputs((4, 3), 3, 1, 0.3, 71)
+    for floor in (0.0, 100.0):
+        ref = oracle_mod.Oracle(mesh, quirks=0, blending=1, bcs=BCS, axisymmetric=1,
+                                axis_rho_floor=floor).rhs(u)["dudt"]
+        op = _op(mesh, quirks="reference", blending=True, bcs=BCS, axis_rho_floor=floor)
+        d = np.empty_like(u)
+        op.Mult(u, d)
+        assert normalized_error(d, ref, 4) <= RHS_TOL, floor
+        op.close()
+
+
+def test_recover_state_matches_oracle(oracle_mod):
+    """The U behind the reference's axisymmetric output fields, host and device
+    pointers; a planar operator refuses."""
+    import ctypes as C
+    import torch
+    from prandtl_b200 import _lib
+    mesh, u = make_golden.axi_inputs((4, 3), 4, 1, 0.3, 81)
+    orc = oracle_mod.Oracle(mesh, quirks=0, bcs=BCS, axisymmetric=1)
+    ref = np.empty_like(u)
+    dp = C.POINTER(C.c_double)
+    assert oracle_mod.lib().oracle_recover_weighted(C.byref(orc.m), C.byref(orc.c), u.ctypes.data_as(dp),
+                                                    ref.ctypes.data_as(dp)) == 0
+    op = _op(mesh, quirks="reference", bcs=BCS)
+    np.testing.assert_array_equal(op.recover_state(u), ref)
+    ud = torch.from_numpy(u).cuda()
+    np.testing.assert_array_equal(op.recover_state(ud).cpu().numpy(), ref)
+    op.close()
+    from prandtl_b200.operator import DGSEMOperator
+    planar = DGSEMOperator(periodic_box(2, 2, 2))
+    with pytest.raises(_lib.PrandtlError):
+        planar.recover_state(np.zeros(4 * planar.mesh.ndof))
+    planar.close()

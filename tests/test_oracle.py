@@ -265,3 +265,32 @@ def test_axisymmetric_free_stream_and_recovery(oracle_mod):
         np.testing.assert_allclose(rec[:, off], Up[:, off], rtol=1e-14)
         assert (rec[2, ~off] == 0).all() and (rec[0, ~off] > 0).all()
         assert (orc.rhs(rUp)["dudt"].reshape(4, -1)[2, ~off] == 0).all()
+
+
+def test_axisymmetric_density_floor_takes_the_nearest_node(oracle_mod):
+    """Above the axis density floor (the reference's driver raises it to
+    1e-8 rho_inf) the axis node copies the nearest off-axis node's U with zero
+    radial momentum."""
+    import ctypes as C
+    from prandtl_b200 import cases
+    from prandtl_b200.mesh import periodic_box
+    mesh = periodic_box(2, (3, 2), 3, (0.0, 0.0), (2.0, 1.0), bcs=[0, 0, 1, 2])
+    bcs = [("outflow",), ("axis",), ("slip_wall",)]
+    U = cases.perturbed(mesh, cases.free_stream(mesh, rho=1.2, vel=[0.3, 0.1], p=1.5), amp=0.1, seed=3)
+    r = mesh.coords[1]
+    rU = (U.reshape(4, -1) * r[None, :]).reshape(-1)
+    dp = C.POINTER(C.c_double)
+    nd = (mesh.order + 1) ** 2
+    for floor, copied in ((0.0, False), (100.0, True)):
+        orc = oracle_mod.Oracle(mesh, quirks=1, bcs=bcs, axisymmetric=1, axis_rho_floor=floor)
+        rec = np.empty_like(rU)
+        assert oracle_mod.lib().oracle_recover_weighted(C.byref(orc.m), C.byref(orc.c), rU.ctypes.data_as(dp),
+                                                        rec.ctypes.data_as(dp)) == 0
+        rec = rec.reshape(4, -1)
+        for g in np.flatnonzero(np.abs(r) <= 1e-14):
+            e0 = (g // nd) * nd
+            re = r[e0:e0 + nd]
+            j = e0 + int(np.argmin(np.where(re > 0, re, np.inf)))
+            want = U.reshape(4, -1)[:, j].copy()
+            want[2] = 0.0
+            assert np.allclose(rec[:, g], want, rtol=1e-14) == copied
