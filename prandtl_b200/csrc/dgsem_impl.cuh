@@ -251,32 +251,39 @@ constexpr int next_pow2(int v) { return v <= 1 ? 1 : 2 * next_pow2((v + 1) / 2);
 #ifndef PRANDTL_NS32_MINB
 #define PRANDTL_NS32_MINB 4
 #endif
+#ifndef PRANDTL_LINE_MAX_NP
+#define PRANDTL_LINE_MAX_NP 4
+#endif
 #ifndef PRANDTL_EULER32_MINB
 #define PRANDTL_EULER32_MINB 6
 #endif
 
 // Lane-group layout of the RHS kernel: one group of GS lanes owns one
 // element.  GS = 32 (a warp), the next power of two >= Np^d for small
-// elements (a warp then holds several elements), or 64 (two warps) for large
-// ones.  Lane `li` of a group owns the nodes li, li+GS, ... and the pair /
-// face / subcell items of the same stride.  Groups synchronise with
-// __syncwarp, or with a named barrier when GS = 64.
+// elements (a warp then holds several elements), 64 (two warps) for large
+// ones, or 128 for the FP32 Navier-Stokes 216-node elements.  Lane `li` of a
+// group owns the nodes li, li+GS, ... and the pair / line / face / subcell
+// items of the same stride.  Groups synchronise with __syncwarp, or with a
+// named barrier when GS > 32.
 //
 // V selects the register budget (the batch autotuner times all of them): the
 // launch bounds ask for MINB_BASE resident CTAs per SM (V = 0, also the
 // one-shot kernels), one fewer (V = 1: more registers) or one more (V = 2:
 // fewer registers, possibly spilling), always capped by what shared memory
-// admits.  The group width is fixed per element size: 64 lanes for >= 125
-// nodes (the tuner never preferred the other width).
+// admits.  The group width is fixed per element size and form (measured:
+// 64 lanes for >= 125 nodes, 128 for the FP32 Navier-Stokes 216-node form).
 constexpr int NUM_VARIANTS = 3;
 constexpr int CTX_RESERVE = 1280;   // bytes of per-item contexts reserved in every layout
 
-template <int DIM, int NP, bool NS, typename Real, int V = 0, bool VC = false>
+template <int DIM, int NP, bool NS, typename Real, int V, bool VC>
 struct RhsLayout {
     using S = Shape<DIM, NP>;
     static constexpr int ND = S::ND, NF = S::NF, NLINE = S::NLINE, PPL = S::PPL;
     static constexpr bool WIDE = ND >= 125;
-    static constexpr int GS = WIDE ? 64 : (ND >= 32 ? 32 : next_pow2(ND));
+    // FP32-bulk Navier-Stokes with contravariant viscous fluxes at Np = 6: 128
+    // lanes, so that the 3 x 36 line tasks of the volume terms take one round
+    static constexpr bool TASK128 = NS && VC && sizeof(Real) == 4 && ND >= 216;
+    static constexpr int GS = TASK128 ? 128 : (WIDE ? 64 : (ND >= 32 ? 32 : next_pow2(ND)));
     static constexpr int EPW = GS >= 32 ? 1 : 32 / GS;  // elements per warp
     static constexpr int WPE = GS > 32 ? GS / 32 : 1;   // warps per element
     static constexpr int NPL = (ND + GS - 1) / GS;      // nodes per lane
@@ -289,11 +296,11 @@ struct RhsLayout {
     static constexpr int PER_ELEM = (K * ND + cmax(BUF, NS ? DIM * NF * ND : 0) + 3) / 4 * 4;
     static constexpr bool F64 = sizeof(Real) == 8;
     // (the Navier-Stokes form with contravariant viscous fluxes needs fewer
-    // registers; in FP32 the 216-node elements keep one CTA fewer for their
-    // longer per-lane node arrays; FP64 large elements are capped by shared
+    // registers; in FP32 the 216-node elements of 128 lanes fit 4 CTAs of
+    // 128 registers a thread; FP64 large elements are capped by shared
     // memory anyway)
     static constexpr int MINB_CFG = NS ? (F64 ? (VC ? PRANDTL_NSVC_MINB : PRANDTL_NS_MINB)
-                                              : (VC ? (ND >= 216 ? 3 : PRANDTL_NSVC32_MINB) : PRANDTL_NS32_MINB))
+                                              : (VC ? (TASK128 ? 4 : PRANDTL_NSVC32_MINB) : PRANDTL_NS32_MINB))
                                        : (F64 ? PRANDTL_EULER_MINB : PRANDTL_EULER32_MINB);
     static constexpr int WARPS_CFG = NS ? PRANDTL_NS_WARPS : PRANDTL_EULER_WARPS;
     // warps per CTA: the configured count, reduced so the CTA's elements fit the
@@ -320,6 +327,12 @@ struct RhsLayout {
     static constexpr int SMEM_BLOCKS = cmax(1, (228 * 1024) / (CTA_SMEM + 1024));
     static constexpr int MINB_REQ = V == 1 ? cmax(1, MINB_CFG - 1) : (V == 2 ? MINB_CFG + 1 : MINB_CFG);
     static constexpr int MIN_BLOCKS = MINB_REQ < SMEM_BLOCKS ? MINB_REQ : SMEM_BLOCKS;
+    // volume terms by line tasks (Navier-Stokes: the viscous-flux buffer holds
+    // the per-direction results) or by pairs and node-wise sums.  Line tasks
+    // were measured faster in the FP32-bulk form up to Np = 4 (3-4 %) and with
+    // the 128-lane groups at Np = 6 (17 %); slower in FP64 and at Np = 5 (75
+    // tasks over 64 or 128 lanes).
+    static constexpr bool LINE = NS && !F64 && (NP <= PRANDTL_LINE_MAX_NP || TASK128);
 };
 
 // Synchronise the GS lanes of lane group `gid` (its index within the CTA).
@@ -751,8 +764,8 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
             e2 += __shfl_xor_sync(0xffffffffu, e2, o);
         }
         if constexpr (GS > 32) {
-            // two warps per element: combine the warps' sums through shared
-            // memory past the two mode buffers (8-byte aligned slots)
+            // several warps per element: combine the warps' sums through
+            // shared memory past the two mode buffers (8-byte aligned slots)
             double *xch = reinterpret_cast<double *>(sH + ((LY::K * ND + 2 * ND + 1) & ~1));
             if ((li & 31) == 0) {
                 xch[3 * (li >> 5)] = e0;
@@ -760,9 +773,15 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 xch[3 * (li >> 5) + 2] = e2;
             }
             group_sync<GS>(gid);
-            e0 = xch[0] + xch[3];
-            e1 = xch[1] + xch[4];
-            e2 = xch[2] + xch[5];
+            e0 = xch[0];
+            e1 = xch[1];
+            e2 = xch[2];
+#pragma unroll
+            for (int w = 1; w < GS / 32; ++w) {
+                e0 += xch[3 * w];
+                e1 += xch[3 * w + 1];
+                e2 += xch[3 * w + 2];
+            }
         }
         double eta = 1.0 - e1 / e0;
         eta = fmax(eta, 1.0 - e2 / e1);
@@ -838,100 +857,184 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
             }
         }
     }
-    if constexpr (NS) {
+    Real acc[NPL][NF];
+    if constexpr (LY::LINE) {
+        // ---- line tasks (DGSEMIntegrator.cpp:601-750): one lane per (direction,
+        //      line) evaluates the line's Np(Np-1)/2 two-point fluxes once and
+        //      accumulates both nodes' Dhat2 terms in registers, partners in
+        //      ascending order as in the node-wise sum; adds the line's Dhat sums
+        //      of the contravariant viscous fluxes and writes the direction's
+        //      total over the line's own slots of that buffer (no other task
+        //      reads them).  Q2 (quirks == 0, 3D): a zeta-line node's partners
+        //      below it contribute the eta flux G(l) of DGSEMIntegrator.cpp:702.
         group_sync<GS>(gid);
-        // sum_l Dhat(i,l) Fv_l along each direction (:710-738); the mass row is zero
+        const Real blend = P.blending ? Real(1) - alpha : Real(1);
+        for (int t = li; t < DIM * S::NLINE; t += GS) {
+            const int dir = t / S::NLINE, ln = t - dir * S::NLINE;
+            int base, stride;
+            line_base<DIM, NP>(dir, ln, base, stride);
+            Real mt[DIM], mg[DIM];
+#pragma unroll
+            for (int q = 0; q < DIM; ++q) {
+                mt[q] = dir == 0 ? adj[0][q] : (dir == 1 ? adj[1][q] : adj[DIM - 1][q]);
+                mg[q] = adj[1][q];
+            }
+            const bool useG = DIM == 3 && P.quirks == 0 && dir == 2;
+            const bool gzero = ln / NP == NP - 1;   // zeta line at j = Np-1: G = 0
+            Real al[NP][NF];
+#pragma unroll
+            for (int i = 0; i < NP; ++i)
+#pragma unroll
+                for (int f = 0; f < NF; ++f) al[i][f] = 0;
+#pragma unroll
+            for (int i = 0; i < NP; ++i) {
+                const Prim<DIM, Real> qi = load_prim<DIM, ND, Real>(sH, base + i * stride);
+                Real G[NF];
+#pragma unroll
+                for (int f = 0; f < NF; ++f) G[f] = 0;
+                if (i < NP - 1 && useG && !gzero)
+                    volume_flux<DIM, Real>(qi, load_prim<DIM, ND, Real>(sH, ln % NP + (NP - 1) * NP + i * NP * NP),
+                                           mg, gm1i, G);
+#pragma unroll
+                for (int l = i + 1; l < NP; ++l) {
+                    Real F[NF];
+                    volume_flux<DIM, Real>(qi, load_prim<DIM, ND, Real>(sH, base + l * stride), mt, gm1i, F);
+                    const Real dil = sDh2[i * NP + l], dli = sDh2[l * NP + i];
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) {
+                        al[i][f] += dil * F[f];
+                        al[l][f] += dli * (useG ? G[f] : F[f]);
+                    }
+                }
+            }
+            Real vv[NP][NF - 1];
+#pragma unroll
+            for (int l = 0; l < NP; ++l)
+#pragma unroll
+                for (int f = 1; f < NF; ++f) vv[l][f - 1] = sV[(dir * NF + f) * ND + base + l * stride];
+#pragma unroll
+            for (int i = 0; i < NP; ++i) {
+                Real *out = sV + dir * NF * ND + base + i * stride;
+                out[0] = -blend * al[i][0];
+#pragma unroll
+                for (int f = 1; f < NF; ++f) {
+                    Real sv = 0;
+#pragma unroll
+                    for (int l = 0; l < NP; ++l) sv += vv[l][f - 1] * sDh[i * NP + l];
+                    out[f * ND] = sv - blend * al[i][f];
+                }
+            }
+        }
+        group_sync<GS>(gid);
 #pragma unroll
         for (int k = 0; k < NPL; ++k) {
             const int n = li + k * GS;
-            if (n < ND) {
-                int c[3];
-                node_coords<NP>(n, c);
 #pragma unroll
-                for (int dir = 0; dir < DIM; ++dir) {
+            for (int f = 0; f < NF; ++f) {
+                Real v = 0;
+                if (n < ND) {
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) v += sV[(d * NF + f) * ND + n];
+                }
+                acc[k][f] = v * mJ;
+            }
+        }
+        group_sync<GS>(gid);   // later phases overwrite the buffer
+    } else {
+        if constexpr (NS) {
+            group_sync<GS>(gid);
+            // sum_l Dhat(i,l) Fv_l along each direction (:710-738); the mass row is zero
+#pragma unroll
+            for (int k = 0; k < NPL; ++k) {
+                const int n = li + k * GS;
+                if (n < ND) {
+                    int c[3];
+                    node_coords<NP>(n, c);
+#pragma unroll
+                    for (int dir = 0; dir < DIM; ++dir) {
+                        const int pos = c[dir];
+                        int base, stride;
+                        line_base<DIM, NP>(dir, line_index<DIM, NP>(dir, c), base, stride);
+#pragma unroll
+                        for (int l = 0; l < NP; ++l) {
+                            const Real dh = sDh[pos * NP + l];
+#pragma unroll
+                            for (int f = 1; f < NF; ++f) dUv[k][f] += sV[(dir * NF + f) * ND + base + l * stride] * dh;
+                        }
+                    }
+                }
+            }
+            group_sync<GS>(gid);   // the pair phase overwrites the buffer
+        }
+
+        // ---- inviscid flux differencing, one direction at a time:
+        //      sum_l Dhat2(i,l) F#(i,l) with F#(i,i) = 0
+#pragma unroll
+        for (int dir = 0; dir < DIM; ++dir) {
+            Real mt[DIM];
+#pragma unroll
+            for (int q = 0; q < DIM; ++q) mt[q] = adj[dir][q];
+            for (int p = li; p < NPD; p += GS) {
+                const uint32_t pr = sPair[dir * NPD + p];
+                Real F[NF];
+                volume_flux<DIM, Real>(load_prim<DIM, ND, Real>(sH, int(pr & 0xffffu)),
+                                       load_prim<DIM, ND, Real>(sH, int(pr >> 16)), mt, gm1i, F);
+                if (rad) {   // f *= r at the pair's reference midpoint (:273-291, :319-338)
+                    const Real rh = Real(0.5 * (__ldg(rad + (long long)e * ND + int(pr & 0xffffu)) +
+                                                __ldg(rad + (long long)e * ND + int(pr >> 16))));
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) F[f] *= rh;
+                }
+#pragma unroll
+                for (int f = 0; f < NF; ++f) sF[f * NPD + p] = F[f];
+            }
+            group_sync<GS>(gid);
+#pragma unroll
+            for (int k = 0; k < NPL; ++k) {
+                const int n = li + k * GS;
+                if (n < ND) {
+                    int c[3];
+                    node_coords<NP>(n, c);
                     const int pos = c[dir];
-                    int base, stride;
-                    line_base<DIM, NP>(dir, line_index<DIM, NP>(dir, c), base, stride);
+                    const int ln = line_index<DIM, NP>(dir, c);
 #pragma unroll
                     for (int l = 0; l < NP; ++l) {
-                        const Real dh = sDh[pos * NP + l];
+                        if (l == pos) continue;
+                        const Real dh = sDh2[pos * NP + l];
+                        if (NS && DIM == 3 && dir == 2 && l < pos && P.quirks == 0) {
+                            // Q2 (DGSEMIntegrator.cpp:702): H(id2)(:,k) = g, the last
+                            // eta-pair flux of node (i,j,l): the pair (j, Np-1) on the
+                            // eta line through (i, ., l); zero when j == Np-1.
+                            if (c[1] != NP - 1) {
+                                Real F[NF], mg[DIM];
 #pragma unroll
-                        for (int f = 1; f < NF; ++f) dUv[k][f] += sV[(dir * NF + f) * ND + base + l * stride] * dh;
-                    }
-                }
-            }
-        }
-        group_sync<GS>(gid);   // the pair phase overwrites the buffer
-    }
-
-    // ---- inviscid flux differencing, one direction at a time:
-    //      sum_l Dhat2(i,l) F#(i,l) with F#(i,i) = 0
+                                for (int q = 0; q < DIM; ++q) mg[q] = adj[1][q];
+                                volume_flux<DIM, Real>(load_prim<DIM, ND, Real>(sH, (l * NP + c[1]) * NP + c[0]),
+                                                       load_prim<DIM, ND, Real>(sH, (l * NP + NP - 1) * NP + c[0]), mg,
+                                                       gm1i, F);
 #pragma unroll
-    for (int dir = 0; dir < DIM; ++dir) {
-        Real mt[DIM];
+                                for (int f = 0; f < NF; ++f) dUi[k][f] += dh * F[f];
+                            }
+                        } else {
+                            const int pidx = ln * PPL + (l < pos ? pair_index<NP>(l, pos) : pair_index<NP>(pos, l));
 #pragma unroll
-        for (int q = 0; q < DIM; ++q) mt[q] = adj[dir][q];
-        for (int p = li; p < NPD; p += GS) {
-            const uint32_t pr = sPair[dir * NPD + p];
-            Real F[NF];
-            volume_flux<DIM, Real>(load_prim<DIM, ND, Real>(sH, int(pr & 0xffffu)),
-                                   load_prim<DIM, ND, Real>(sH, int(pr >> 16)), mt, gm1i, F);
-            if (rad) {   // f *= r at the pair's reference midpoint (:273-291, :319-338)
-                const Real rh = Real(0.5 * (__ldg(rad + (long long)e * ND + int(pr & 0xffffu)) +
-                                            __ldg(rad + (long long)e * ND + int(pr >> 16))));
-#pragma unroll
-                for (int f = 0; f < NF; ++f) F[f] *= rh;
-            }
-#pragma unroll
-            for (int f = 0; f < NF; ++f) sF[f * NPD + p] = F[f];
-        }
-        group_sync<GS>(gid);
-#pragma unroll
-        for (int k = 0; k < NPL; ++k) {
-            const int n = li + k * GS;
-            if (n < ND) {
-                int c[3];
-                node_coords<NP>(n, c);
-                const int pos = c[dir];
-                const int ln = line_index<DIM, NP>(dir, c);
-#pragma unroll
-                for (int l = 0; l < NP; ++l) {
-                    if (l == pos) continue;
-                    const Real dh = sDh2[pos * NP + l];
-                    if (NS && DIM == 3 && dir == 2 && l < pos && P.quirks == 0) {
-                        // Q2 (DGSEMIntegrator.cpp:702): H(id2)(:,k) = g, the last
-                        // eta-pair flux of node (i,j,l): the pair (j, Np-1) on the
-                        // eta line through (i, ., l); zero when j == Np-1.
-                        if (c[1] != NP - 1) {
-                            Real F[NF], mg[DIM];
-#pragma unroll
-                            for (int q = 0; q < DIM; ++q) mg[q] = adj[1][q];
-                            volume_flux<DIM, Real>(load_prim<DIM, ND, Real>(sH, (l * NP + c[1]) * NP + c[0]),
-                                                   load_prim<DIM, ND, Real>(sH, (l * NP + NP - 1) * NP + c[0]), mg,
-                                                   gm1i, F);
-#pragma unroll
-                            for (int f = 0; f < NF; ++f) dUi[k][f] += dh * F[f];
+                            for (int f = 0; f < NF; ++f) dUi[k][f] += dh * sF[f * NPD + pidx];
                         }
-                    } else {
-                        const int pidx = ln * PPL + (l < pos ? pair_index<NP>(l, pos) : pair_index<NP>(pos, l));
-#pragma unroll
-                        for (int f = 0; f < NF; ++f) dUi[k][f] += dh * sF[f * NPD + pidx];
                     }
                 }
             }
+            group_sync<GS>(gid);
         }
-        group_sync<GS>(gid);
+#pragma unroll
+        for (int k = 0; k < NPL; ++k)
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                Real v = -dUi[k][f];
+                if (P.blending) v *= (Real(1) - alpha);
+                if (NS) v += dUv[k][f];
+                acc[k][f] = v * mJ;
+            }
     }
-    Real acc[NPL][NF];
-#pragma unroll
-    for (int k = 0; k < NPL; ++k)
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            Real v = -dUi[k][f];
-            if (P.blending) v *= (Real(1) - alpha);
-            if (NS) v += dUv[k][f];
-            acc[k][f] = v * mJ;
-        }
     if (rad) {   // + p on the radial momentum (DGSEMIntegrator.cpp:411-428), not blended
 #pragma unroll
         for (int k = 0; k < NPL; ++k) {
@@ -1648,14 +1751,14 @@ lift_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_const
     }
 }
 
-template <int DIM, int NP, bool NS, typename Real>
+template <int DIM, int NP, bool NS, bool VC, typename Real>
 size_t rhs_smem() {
-    using LY = RhsLayout<DIM, NP, NS, Real>;
+    using LY = RhsLayout<DIM, NP, NS, Real, 0, VC>;
     return LY::TAB_BYTES + LY::PAIR_BYTES + sizeof(Real) * (size_t)LY::EPB * LY::PER_ELEM;
 }
-template <int DIM, int NP, bool NS, typename Real, int V>
+template <int DIM, int NP, bool NS, bool VC, typename Real, int V>
 size_t rhs_batch_smem() {
-    using LY = RhsLayout<DIM, NP, NS, Real, V>;
+    using LY = RhsLayout<DIM, NP, NS, Real, V, VC>;
     return LY::FIXED_BYTES + sizeof(Real) * (size_t)LY::EPB * LY::PER_ELEM;
 }
 template <int DIM, int NP, typename Out>
@@ -1673,9 +1776,9 @@ size_t lift_batch_smem() {
 template <int DIM, int NP, bool NS, bool VC, typename Real>
 cudaError_t rhs_launch_np(const MeshDev &m, const RhsArgs &a, const PhysParams &P, const OpTables &T,
                           cudaStream_t s) {
-    using LY = RhsLayout<DIM, NP, NS, Real>;
+    using LY = RhsLayout<DIM, NP, NS, Real, 0, VC>;
     const int grid = (m.E + LY::EPB - 1) / LY::EPB;
-    const size_t sm = rhs_smem<DIM, NP, NS, Real>();
+    const size_t sm = rhs_smem<DIM, NP, NS, VC, Real>();
     cudaError_t err = cudaFuncSetAttribute(rhs_kernel<DIM, NP, NS, VC, Real>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (err != cudaSuccess) return err;
@@ -1699,8 +1802,8 @@ cudaError_t lift_launch_np(const MeshDev &m, const LiftArgs &a, const PhysParams
 // capture) and reports the resident CTAs per SM; `launch` only launches.
 template <int DIM, int NP, bool NS, bool VC, typename Real, int V>
 cudaError_t rhs_batch_prepare_np(BatchKernelInfo *info) {
-    using LY = RhsLayout<DIM, NP, NS, Real, V>;
-    const size_t sm = rhs_batch_smem<DIM, NP, NS, Real, V>();
+    using LY = RhsLayout<DIM, NP, NS, Real, V, VC>;
+    const size_t sm = rhs_batch_smem<DIM, NP, NS, VC, Real, V>();
     cudaError_t err = cudaFuncSetAttribute(rhs_batch_kernel<DIM, NP, NS, VC, Real, V>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (err != cudaSuccess) return err;
@@ -1719,8 +1822,8 @@ cudaError_t rhs_batch_prepare_np(BatchKernelInfo *info) {
 template <int DIM, int NP, bool NS, bool VC, typename Real, int V>
 cudaError_t rhs_batch_launch_np(int grid, const BatchClassDev &c, const BatchStage &st, const OpTables &T,
                                 cudaStream_t s) {
-    using LY = RhsLayout<DIM, NP, NS, Real, V>;
-    rhs_batch_kernel<DIM, NP, NS, VC, Real, V><<<grid, LY::THREADS, rhs_batch_smem<DIM, NP, NS, Real, V>(), s>>>(c, st, T);
+    using LY = RhsLayout<DIM, NP, NS, Real, V, VC>;
+    rhs_batch_kernel<DIM, NP, NS, VC, Real, V><<<grid, LY::THREADS, rhs_batch_smem<DIM, NP, NS, VC, Real, V>(), s>>>(c, st, T);
     return cudaGetLastError();
 }
 template <int DIM, int NP, typename Out, bool VC>
