@@ -1519,7 +1519,8 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
     const W *sD = sT, *sW = sT + 4 * NP * NP;
     W *gout = reinterpret_cast<W *>(a.grad);
     W *sVe = sElem;                 // entropy variables [NF][ND]
-    W *sS = sVe + NF * ND;          // face terms [DIM][NF][NFI]
+    W *sS = sVe + NF * ND;          // face jumps [NF][NFI]
+    W *sN = sS + NF * NFI;          // face normals [2 DIM][DIM] (one per local face)
     const long long Ndof = a.Ndof;
     const long long gnode = (long long)e * ND + n;
     double st[NF];
@@ -1579,6 +1580,8 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
     }
     __syncthreads();   // tables and entropy variables complete
     const W aw = W(1.0 / (double(sW[0]) * J));
+    // the jumps per face node and the normal per face; the face's nodes form
+    // aw * (jump * n_q) themselves
 #pragma unroll
     for (int k = 0; k < MAXIT; ++k) {
         const int it = n + k * ND;
@@ -1586,9 +1589,11 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 const W vo = sVe[f * ND + no[k]];
-                const W jf = own1[k] ? W(0.5) * (vn[k][f] - vo) : W(0.5) * (vo - vn[k][f]);
+                sS[f * NFI + it] = own1[k] ? W(0.5) * (vn[k][f] - vo) : W(0.5) * (vo - vn[k][f]);
+            }
+            if (it % NFN == 0) {
 #pragma unroll
-                for (int q = 0; q < DIM; ++q) sS[(q * NF + f) * NFI + it] = aw * (jf * nor[k][q]);
+                for (int q = 0; q < DIM; ++q) sN[(it / NFN) * DIM + q] = nor[k][q];
             }
         }
     }
@@ -1630,10 +1635,15 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
         else if (c[d] == NP - 1) lf = 2 * d + 1;
         if (lf >= 0) {
             const int it = lf * NFN + face_tangential<DIM, NP>(d, c);
+            W jf[NF], nq[DIM];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) jf[f] = sS[f * NFI + it];
+#pragma unroll
+            for (int q = 0; q < DIM; ++q) nq[q] = sN[lf * DIM + q];
 #pragma unroll
             for (int q = 0; q < DIM; ++q)
 #pragma unroll
-                for (int f = 0; f < NF; ++f) g[q][f] += sS[(q * NF + f) * NFI + it];
+                for (int f = 0; f < NF; ++f) g[q][f] += aw * (jf[f] * nq[q]);
         }
     }
     if (!active) return;
@@ -1673,7 +1683,7 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
 template <int DIM, int NP>
 struct LiftLayout {
     using S = Shape<DIM, NP>;
-    static constexpr int PER_ELEM = S::NF * S::ND + DIM * S::NF * S::NFI;
+    static constexpr int PER_ELEM = S::NF * S::ND + S::NF * S::NFI + 2 * DIM * DIM;
 };
 constexpr int prev_pow2(int v) { return v <= 1 ? 1 : 2 * prev_pow2(v / 2); }
 // Batch lift CTA: a power-of-two number of elements, so an item (one CTA's
