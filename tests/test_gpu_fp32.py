@@ -69,6 +69,25 @@ def test_fp32_rhs_euler_blended():
     assert max(rel_l2(d32, d64, 4)) <= 2e-3
 
 
+@pytest.mark.parametrize("order", [2, 3, 4, 5])
+def test_fp32_rhs_navier_stokes_blended(order):
+    """Navier-Stokes with blending on a perturbed box: the line-task volume
+    terms (N <= 3 and N = 5) and the indicator's cross-warp reduction (N >= 4)
+    against the FP64 path."""
+    mesh = periodic_box(3, 3, order, 0.0, 1.0, affine=np.eye(3) + 0.1 * np.eye(3, k=1))
+    base = cases.free_stream(mesh, rho=1.2, vel=[0.4, -0.3, 0.2], p=1.5)
+    u = cases.perturbed(mesh, base, amp=0.3, seed=order)
+    kw = dict(parabolic=True, blending=True, mu=0.01, Pr=0.71, quirks="fixed")
+    d64, d32 = np.empty_like(u), np.empty_like(u)
+    op64 = _op(mesh, **kw)
+    op64.Mult(u, d64)
+    op32 = _op(mesh, precision="fp32", **kw)
+    op32.Mult(u, d32)
+    assert (op64.alpha() > 0).any()
+    np.testing.assert_allclose(op32.alpha(), op64.alpha(), rtol=0, atol=1e-5)
+    assert max(rel_l2(d32, d64, mesh.num_fields)) <= 2e-3
+
+
 @pytest.mark.parametrize("case", ["tgv", "ivortex"])
 def test_fp32_trajectory_error(case):
     if case == "tgv":
