@@ -1523,6 +1523,30 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
     W *sN = sS + NF * NFI;          // face normals [2 DIM][DIM] (one per local face)
     const long long Ndof = a.Ndof;
     const long long gnode = (long long)e * ND + n;
+    // FP64: this thread's face items' neighbour-table entries and interior
+    // neighbour traces are loaded with the own state (measured 4 % faster).
+    // The FP32 form loads them after the own entropy variables: earlier, the
+    // longer live ranges spill and cost 10-20 %.
+    constexpr int MAXIT = (NFI + ND - 1) / ND;   // face items per thread
+    int4 tk[MAXIT];
+    double snk[MAXIT][NF];
+    if constexpr (F64) {
+#pragma unroll
+        for (int k = 0; k < MAXIT; ++k) {
+            const int it = n + k * ND;
+            tk[k] = it < NFI ? __ldg(a.nbr + (long long)e * (2 * DIM) + it / NFN) : make_int4(-1, 0, 0, 0);
+        }
+#pragma unroll
+        for (int k = 0; k < MAXIT; ++k) {
+            const int it = n + k * ND;
+            if (it < NFI && tk[k].x >= 0) {
+                const int fa = it - (it / NFN) * NFN;
+                const long long gn = (long long)tk[k].x * ND + face_node<DIM, NP>(tk[k].y, fa);
+#pragma unroll
+                for (int f = 0; f < NF; ++f) snk[k][f] = __ldg(a.u + f * Ndof + gn);
+            }
+        }
+    }
     double st[NF];
     W v[NF];
 #pragma unroll
@@ -1552,7 +1576,6 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
     // face part: the neighbour traces' entropy variables are formed before the
     // barrier (their loads overlap the own node's), the jumps after it:
     // +1/(w0 J) * 1/2 (v_elem2 - v_elem1) * n_c on both sides
-    constexpr int MAXIT = (NFI + ND - 1) / ND;   // face items per thread
     W vn[MAXIT][NF], nor[MAXIT][DIM];
     int no[MAXIT];
     bool own1[MAXIT];
@@ -1562,7 +1585,7 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
         if (it < NFI) {
             const int lf = it / NFN, fa = it - lf * NFN;
             no[k] = face_node<DIM, NP>(lf, fa);
-            const int4 t = __ldg(a.nbr + (long long)e * (2 * DIM) + lf);
+            const int4 t = F64 ? tk[k] : __ldg(a.nbr + (long long)e * (2 * DIM) + lf);
 #pragma unroll
             for (int q = 0; q < DIM; ++q) nor[k][q] = W(__ldg(a.fnor + (long long)t.z * DIM + q));
             own1[k] = (t.w == 0);
@@ -1570,12 +1593,15 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
                 boundary_lift_trace<DIM, W>(a, P, R, e * (long long)ND + no[k], t, vn[k]);
                 continue;
             }
-            const long long gn = (long long)t.x * ND + face_node<DIM, NP>(t.y, fa);
-            double sn[NF];
+            if constexpr (F64) {
+                conserv2entropy<DIM, double>(snk[k], P, reinterpret_cast<double *>(vn[k]));
+            } else {
+                const long long gn = (long long)t.x * ND + face_node<DIM, NP>(t.y, fa);
+                double sn[NF];
 #pragma unroll
-            for (int f = 0; f < NF; ++f) sn[f] = __ldg(a.u + f * Ndof + gn);
-            if constexpr (F64) conserv2entropy<DIM, double>(sn, P, reinterpret_cast<double *>(vn[k]));
-            else conserv2entropy_rel<DIM>(sn, P, R, reinterpret_cast<float *>(vn[k]));
+                for (int f = 0; f < NF; ++f) sn[f] = __ldg(a.u + f * Ndof + gn);
+                conserv2entropy_rel<DIM>(sn, P, R, reinterpret_cast<float *>(vn[k]));
+            }
         }
     }
     __syncthreads();   // tables and entropy variables complete
