@@ -360,13 +360,15 @@ def run_batch(torch, items, K, W, barrier, local):
     return [o.numpy() for o in outs], info
 
 
-def run_plain(torch, items, K, W):
+def run_plain(torch, items, K, W, batch_states=None):
     """Members one at a time through the one-operator FP64 path: W untimed and
-    K timed steps each (CUDA events on the current stream)."""
+    K timed steps each (CUDA events on the current stream).  Outside the timed
+    region, the FP64 device budgets (mass, energy, entropy) of the initial
+    state, the final FP64 state and the member's final FP32-batched state."""
     from prandtl_b200.operator import DGSEMOperator
     stream = torch.cuda.current_stream()
-    total_s, dofs, states, launches = 0.0, 0, [], 0
-    for m, mesh, u0, dt in items:
+    total_s, dofs, states, launches, budgets = 0.0, 0, [], 0, []
+    for k, (m, mesh, u0, dt) in enumerate(items):
         op = DGSEMOperator(mesh, **m.physics())
         op.set_stream(stream.cuda_stream)
         u = torch.from_numpy(u0).cuda()
@@ -381,8 +383,33 @@ def run_plain(torch, items, K, W):
         launches += op.kernel_launches - l0
         dofs += u0.size
         states.append(u.cpu().numpy())
+        b0 = op.budgets(torch.from_numpy(u0).cuda())
+        bp = op.budgets(u)
+        bb = op.budgets(torch.from_numpy(batch_states[k]).cuda()) if batch_states is not None else None
+        budgets.append((b0, bp, bb))
         op.close()
-    return states, {"device_s": total_s, "dof": dofs, "launches": launches}
+    return states, {"device_s": total_s, "dof": dofs, "launches": launches, "budgets": budgets}
+
+
+def budget_summary(budgets, steps):
+    """Largest relative drifts of mass and energy over the run, per path, and
+    the FP32-batched vs FP64-plain entropy difference (relative to the initial
+    entropy)."""
+    def drift(b0, b1, f):
+        return abs(b1["conserved"][f] - b0["conserved"][f]) / abs(b0["conserved"][f])
+    out = {"members": len(budgets), "steps": steps,
+           "reduction": "FP64 on the device, node weights w_i w_j w_k |J|, fixed-order two-pass sum"}
+    for name, j in (("fp64_plain", 1), ("fp32_batched", 2)):
+        if any(b[j] is None for b in budgets):
+            continue
+        out[name] = {"mass_rel_drift_max": max(drift(b[0], b[j], 0) for b in budgets),
+                     "energy_rel_drift_max": max(drift(b[0], b[j], 4) for b in budgets),
+                     "entropy_rel_change_max": max(abs(b[j]["entropy"] - b[0]["entropy"]) / abs(b[0]["entropy"])
+                                                   for b in budgets)}
+    if all(b[2] is not None for b in budgets):
+        out["entropy_fp32_vs_fp64_rel_max"] = max(abs(b[2]["entropy"] - b[1]["entropy"]) / abs(b[0]["entropy"])
+                                                  for b in budgets)
+    return out
 
 
 def run_tgv32(torch, steps):
@@ -544,7 +571,7 @@ def main():
     if rank == 0:
         # FP64 plain path on every k-th member, and the FP32-batched error against it
         sample = list(range(0, len(items), max(1, args.plain_every)))
-        pstates, pinfo = run_plain(torch, [items[k] for k in sample], K, W)
+        pstates, pinfo = run_plain(torch, [items[k] for k in sample], K, W, [states[k] for k in sample])
         plain_rate = pinfo["dof"] * K / pinfo["device_s"]
         errs = [rel_errors(states[k], p, 5) for k, p in zip(sample, pstates)]
         err = {f: {"rel_l2_max": max(e[f][0] for e in errs), "rel_l2_median": statistics.median(e[f][0] for e in errs),
@@ -616,6 +643,7 @@ def main():
                            "sample": f"every {args.plain_every}th member, each alone through DGSEMOperator.Step",
                            "ratio_fp32_batched_over_fp64_plain": (value / world) / plain_rate},
             "error": {"fp32_batched_vs_fp64_plain_after_steps": W + K, "members": len(sample), **err},
+            "budgets": budget_summary(pinfo["budgets"], W + K),
             "e2e": {"value": dof * (W + K) * world / wall_s, "unit": "DOF-updates/s",
                     "h2d_bytes_per_step": u_bytes / (W + K), "d2h_bytes_per_step": u_bytes / (W + K),
                     "window": "admission from pinned host memory + tuning + W+K steps + every state read back; "

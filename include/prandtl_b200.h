@@ -172,6 +172,18 @@ prandtl_status prandtl_get_alpha(prandtl_handle *h, double *alpha, int ptr_flags
  * PRANDTL_EUNSUPPORTED for a planar operator. */
 prandtl_status prandtl_recover_state(prandtl_handle *h, const double *rU, double *U, int ptr_flags);
 
+/* FP64 budgets of a state on the device (planar forms): with nf = dim + 2,
+ *   out[0 .. nf-1]       integrals of the conserved fields (mass, momentum, energy),
+ *   out[nf]              integral of the entropy function U = -rho s / (gamma - 1),
+ *                        s = ln(p rho^-gamma) (the entropy pair of the Chandrashekar flux),
+ *   out[nf+1 .. 2nf]     integrals of dudt_f,
+ *   out[2nf+1]           integral of v . dudt (v the entropy variables: the entropy production),
+ * with the node weights w_i w_j (w_k) |J|; the last nf + 1 are 0 when dudt is NULL.
+ * u and dudt follow ptr_flags; out is host memory of 2 nf + 2 doubles.  The sums are
+ * deterministic (fixed-order two-pass reduction).  EUNSUPPORTED for the axisymmetric form. */
+prandtl_status prandtl_budgets(prandtl_handle *h, const double *u, const double *dudt, double *out,
+                               int ptr_flags);
+
 /* CFL step dt = cfl*hmin/(lambda_max*(N+1)^2) (Simulation.cpp:906,1017). */
 double prandtl_cfl_dt(double cfl, double hmin, double lambda_max, int order);
 

@@ -26,6 +26,7 @@ EXPORTS = ["prandtl_config_default", "prandtl_create", "prandtl_destroy", "prand
            "prandtl_synchronize", "prandtl_kernel_launches", "prandtl_profile",
            "prandtl_profile_read", "prandtl_profile_reset", "prandtl_device_bytes",
            "prandtl_last_error", "prandtl_version", "prandtl_rhs_noalloc", "prandtl_recover_state",
+           "prandtl_budgets",
            "prandtl_batch_config_default", "prandtl_batch_create", "prandtl_batch_destroy",
            "prandtl_batch_footprint", "prandtl_batch_add", "prandtl_batch_advance",
            "prandtl_batch_sync", "prandtl_batch_finished", "prandtl_batch_query",
@@ -119,6 +120,8 @@ def load():
     L.prandtl_get_alpha.restype = ip
     L.prandtl_recover_state.argtypes = [vp, vp, vp, ip]
     L.prandtl_recover_state.restype = ip
+    L.prandtl_budgets.argtypes = [vp, vp, vp, vp, ip]
+    L.prandtl_budgets.restype = ip
     L.prandtl_cfl_dt.argtypes = [C.c_double, C.c_double, C.c_double, ip]
     L.prandtl_cfl_dt.restype = C.c_double
     L.prandtl_set_stream.argtypes = [vp, vp]

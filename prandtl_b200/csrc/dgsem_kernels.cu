@@ -186,6 +186,101 @@ __global__ void axi_recover_kernel(const double *__restrict__ rU, double *__rest
 }
 }   // namespace
 
+namespace {
+struct Weights1D {
+    double w[8];
+};
+
+// One thread per node (grid-stride), FP64 throughout; warp shuffles, then the
+// block's warps in order, give one partial per block and output.
+template <int NOUT>
+__global__ void __launch_bounds__(BUDGET_THREADS) budget_kernel(const double *__restrict__ u,
+                                                               const double *__restrict__ dudt,
+                                                               const double *__restrict__ geo, Weights1D W,
+                                                               int dim, int np, int E, double gamma,
+                                                               double *__restrict__ partials) {
+    constexpr int MAXF = (NOUT - 2) / 2;
+    const int nf = dim + 2, nd = dim == 2 ? np * np : np * np * np;
+    const long long Ndof = (long long)E * nd;
+    double acc[NOUT];
+#pragma unroll
+    for (int q = 0; q < NOUT; ++q) acc[q] = 0.0;
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < Ndof;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int e = (int)(g / nd), n = (int)(g - (long long)e * nd);
+        double wn = W.w[n % np] * W.w[(n / np) % np];
+        if (dim == 3) wn *= W.w[n / (np * np)];
+        const double wJ = wn * fabs(geo[(long long)e * (dim * dim + 1) + dim * dim]);
+        double s[MAXF], r[MAXF];
+#pragma unroll
+        for (int f = 0; f < MAXF; ++f) {
+            s[f] = f < nf ? u[f * Ndof + g] : 0.0;
+            r[f] = (f < nf && dudt) ? dudt[f * Ndof + g] : 0.0;
+        }
+        const double rho = s[0], E_ = s[nf - 1];
+        double vv = 0.0;
+#pragma unroll
+        for (int d = 0; d < MAXF - 2; ++d)
+            if (d < dim) vv += (s[1 + d] / rho) * (s[1 + d] / rho);
+        const double p = (gamma - 1.0) * (E_ - 0.5 * rho * vv);
+        const double ent = log(p) - gamma * log(rho);
+        const double beta = rho / p;
+#pragma unroll
+        for (int f = 0; f < MAXF; ++f)
+            if (f < nf) {
+                acc[f] += wJ * s[f];
+                acc[MAXF + 1 + f] += wJ * r[f];
+            }
+        acc[MAXF] += wJ * (-rho * ent / (gamma - 1.0));
+        double vd = ((gamma - ent) / (gamma - 1.0) - 0.5 * beta * vv) * r[0] - beta * r[nf - 1];
+#pragma unroll
+        for (int d = 0; d < MAXF - 2; ++d)
+            if (d < dim) vd += beta * (s[1 + d] / rho) * r[1 + d];
+        acc[NOUT - 1] += wJ * vd;
+    }
+    __shared__ double red[BUDGET_THREADS / 32][NOUT];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NOUT; ++q) {
+        double v = acc[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[wid][q] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < NOUT) {
+        double v = 0.0;
+        for (int k = 0; k < BUDGET_THREADS / 32; ++k) v += red[k][threadIdx.x];
+        partials[blockIdx.x * NOUT + threadIdx.x] = v;
+    }
+}
+
+__global__ void budget_final_kernel(const double *__restrict__ partials, int blocks, int nout,
+                                    double *__restrict__ out) {
+    const int q = threadIdx.x;
+    if (q >= nout) return;
+    double v = 0.0;
+    for (int b = 0; b < blocks; ++b) v += partials[b * nout + q];   // fixed order: deterministic
+    out[q] = v;
+}
+}   // namespace
+
+cudaError_t launch_budgets(const double *u, const double *dudt, const double *geo, const double *w1d, int dim,
+                           int np, int E, double gamma, double *partials, double *out, cudaStream_t s) {
+    if (np < 2 || np > 8 || (dim != 2 && dim != 3) || E <= 0) return cudaErrorInvalidValue;
+    Weights1D W{};
+    for (int i = 0; i < np; ++i) W.w[i] = w1d[i];
+    const long long Ndof = (long long)E * (dim == 2 ? np * np : np * np * np);
+    long long blocks = (Ndof + BUDGET_THREADS - 1) / BUDGET_THREADS;
+    if (blocks > BUDGET_BLOCKS) blocks = BUDGET_BLOCKS;
+    // outputs: nf conserved integrals, entropy, nf rate integrals, entropy rate
+    constexpr int NOUT = 2 * 5 + 2;
+    budget_kernel<NOUT><<<(unsigned)blocks, BUDGET_THREADS, 0, s>>>(u, dudt, geo, W, dim, np, E, gamma, partials);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    budget_final_kernel<<<1, 32, 0, s>>>(partials, (int)blocks, NOUT, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_axi_recover(const double *rU, double *U, const double *xy, const unsigned char *axis,
                                long long Ndof, int ND, double rho_floor, cudaStream_t s) {
     if (Ndof <= 0) return cudaSuccess;

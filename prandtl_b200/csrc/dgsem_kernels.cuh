@@ -121,6 +121,16 @@ cudaError_t batch_launch_lift(int dim, int order, bool vc, bool fp32, int grid, 
 // End of a batch step: every live solve with steps left advances its counters,
 // flips its LSRK parity, (cfl > 0) takes its next dt from lambda, and writes
 // its remaining step count to left[id].
+// FP64 budgets over the mesh (node weights w_i w_j (w_k) |J|): the integrals
+// of the nf conserved fields and of the entropy function U = -rho s / (g-1),
+// s = ln(p rho^-g); with dudt also the integrals of dudt_f and of v . dudt
+// (v the entropy variables).  nout = 2 nf + 2 values; deterministic two-pass
+// reduction through `partials` ([BUDGET_BLOCKS][nout]).
+constexpr int BUDGET_BLOCKS = 592;
+constexpr int BUDGET_THREADS = 256;
+cudaError_t launch_budgets(const double *u, const double *dudt, const double *geo, const double *w1d, int dim,
+                           int np, int E, double gamma, double *partials, double *out, cudaStream_t s);
+
 // Axisymmetric form: U recovered from the weighted state rU (2D, 4 fields).
 cudaError_t launch_axi_recover(const double *rU, double *U, const double *xy, const unsigned char *axis,
                                long long Ndof, int ND, double rho_floor, cudaStream_t s);

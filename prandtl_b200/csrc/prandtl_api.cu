@@ -47,6 +47,7 @@ struct prandtl_handle {
     double *d_xy = nullptr;
     unsigned char *d_axis = nullptr;
     double *d_U = nullptr;
+    double *d_budget = nullptr;                   // budget partials [BUDGET_BLOCKS][12] + totals [12]
     size_t bytes = 0;
     long long launches = 0;
     // optional per-kernel CUDA-event timing (prandtl_profile)
@@ -174,6 +175,7 @@ void free_all(prandtl_handle *h) {
     cudaFree(h->d_xy);
     cudaFree(h->d_axis);
     cudaFree(h->d_U);
+    cudaFree(h->d_budget);
     if (h->done) cudaEventDestroy(h->done);
     for (auto &r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (auto ev : h->ev_pool) cudaEventDestroy(ev);
@@ -282,6 +284,7 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
         return bail(st);
     if ((st = dalloc(h, &h->d_alpha, (size_t)E, "alpha")) != PRANDTL_OK) return bail(st);
     if ((st = dalloc(h, &h->d_lambda, 1, "lambda")) != PRANDTL_OK) return bail(st);
+    if ((st = dalloc(h, &h->d_budget, (size_t)(BUDGET_BLOCKS + 1) * 12, "budgets")) != PRANDTL_OK) return bail(st);
     const std::vector<BcDev> bcs = device_bcs(cfg, md->dim);
     if (!bcs.empty()) {
         if ((st = dalloc(h, &h->d_bcs, bcs.size(), "boundary conditions")) != PRANDTL_OK) return bail(st);
@@ -470,6 +473,42 @@ prandtl_status prandtl_recover_state(prandtl_handle *h, const double *rU, double
     h->launches++;
     if (!dev) CK(h, cudaMemcpyAsync(U, h->d_out, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H U");
     return wait_stream(h);
+}
+
+prandtl_status prandtl_budgets(prandtl_handle *h, const double *u, const double *dudt, double *out, int ptr_flags) {
+    if (!h || !u || !out) return h ? fail(h, PRANDTL_EINVAL, "null pointer") : PRANDTL_EINVAL;
+    std::lock_guard<std::mutex> lk(h->mu);
+    h->err.clear();
+    if (h->d_U) return fail(h, PRANDTL_EUNSUPPORTED, "budgets are defined for the planar forms");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    const size_t bytes = (size_t)h->nf * h->Ndof * sizeof(double);
+    const bool dev = (ptr_flags & PRANDTL_PTR_DEVICE) != 0;
+    const double *ud = u, *dd = dudt;
+    if (!dev) {
+        CK(h, cudaMemcpyAsync(h->d_in, u, bytes, cudaMemcpyHostToDevice, h->stream), "H2D u");
+        ud = h->d_in;
+        if (dudt) {
+            CK(h, cudaMemcpyAsync(h->d_out, dudt, bytes, cudaMemcpyHostToDevice, h->stream), "H2D dudt");
+            dd = h->d_out;
+        }
+    }
+    double *tot = h->d_budget + (size_t)BUDGET_BLOCKS * 12;
+    CK(h, launch_budgets(ud, dd, h->d_geo, h->T.w, h->dim, h->Np, h->E, h->cfg.gamma, h->d_budget, tot, h->stream),
+       "budget kernel launch");
+    h->launches += 2;
+    double buf[12];
+    CK(h, cudaMemcpyAsync(buf, tot, sizeof(buf), cudaMemcpyDeviceToHost, h->stream), "D2H budgets");
+    prandtl_status st = wait_stream(h);
+    if (st != PRANDTL_OK) return st;
+    // device slots: conserved [0..4], entropy [5], rates [6..10], entropy rate [11]
+    const int nf = h->nf;
+    for (int f = 0; f < nf; ++f) {
+        out[f] = buf[f];
+        out[nf + 1 + f] = dudt ? buf[6 + f] : 0.0;
+    }
+    out[nf] = buf[5];
+    out[2 * nf + 1] = dudt ? buf[11] : 0.0;
+    return PRANDTL_OK;
 }
 
 double prandtl_cfl_dt(double cfl, double hmin, double lambda_max, int order) {

@@ -185,6 +185,22 @@ class DGSEMOperator:
         _lib.check(self._L.prandtl_recover_state(self._h, pr, pU, fr), self._h)
         return U
 
+    def budgets(self, u, dudt=None) -> dict:
+        """FP64 integrals over the mesh, reduced on the device: the conserved
+        fields, the entropy function -rho s / (gamma - 1), and with dudt their
+        rates and the entropy production (integral of v . dudt)."""
+        pu, fu = _ptr(u)
+        pd = None
+        if dudt is not None:
+            pd, fd = _ptr(dudt)
+            if fd != fu:
+                raise ValueError("u and dudt must both be host or both be device arrays")
+        nf = self.mesh.num_fields
+        out = np.zeros(2 * nf + 2)
+        _lib.check(self._L.prandtl_budgets(self._h, pu, pd, out.ctypes.data, fu), self._h)
+        return {"conserved": out[:nf].copy(), "entropy": float(out[nf]),
+                "rates": out[nf + 1:2 * nf + 1].copy(), "entropy_rate": float(out[2 * nf + 1])}
+
     def cfl_dt(self, cfl: float, lambda_max: float | None = None) -> float:
         lam = self.max_char_speed if lambda_max is None else lambda_max
         return self._L.prandtl_cfl_dt(cfl, self.mesh.hmin, lam, self.mesh.order)
