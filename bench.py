@@ -605,6 +605,19 @@ def main():
                     "peak_gbs": hbm_peak, "frac": by / t_launch / 1e9 / hbm_peak, "peak_source": hbm_src},
             "classes": {str(o): c for o, c in binfo["classes"].items()},
         }
+        # the same class's lifting launch: HBM-bound by design (u read, FP32 viscous rows written)
+        t_lift = dc["lift_ms"] / 1e3
+        nd_dom = (dom_order + 1) ** 3
+        lby = E_dom * nd_dom * (5 * 8 + 3 * 4 * 4)
+        ltr = measured_traffic().get(f"lift_batch_N{dom_order}_fp32")
+        roofline["lift"] = {
+            "kernel": f"lift_batch_kernel<3, N={dom_order}, float> (all N={dom_order} members, one stage)",
+            "bound": "hbm", "algorithmic_bytes_per_launch": lby, "avg_launch_ms": t_lift * 1e3,
+            "achieved_gbs": lby / t_lift / 1e9, "peak_gbs": hbm_peak, "frac": lby / t_lift / 1e9 / hbm_peak,
+            "peak_source": hbm_src,
+            "traffic": ltr["bytes_per_element"] * E_dom if ltr else None,
+            "traffic_source": ("ncu dram bytes of this kernel on the N=5 members of a 24-member ensemble, scaled by "
+                               "elements (profiles/lift_batch_kernel_N5_fp32_ncu.md)") if ltr else None}
         tgv32 = None
         if not args.no_tgv32:
             tgv32 = run_tgv32(torch, 50)
