@@ -1719,9 +1719,10 @@ struct LiftBatchShape {
     static constexpr int ND = Shape<DIM, NP>::ND;
     static constexpr int EPB = prev_pow2(cmax(1, 128 / ND));
     static constexpr int THREADS = EPB * ND;
-    // resident CTAs the register budget is sized for (measured on the FP32 3D
-    // Navier-Stokes classes: 5 beats 4 by up to 13 %; 6 is better still at Np = 5, N = 4)
-    static constexpr int MIN_BLOCKS = (DIM == 3 && NP == 5) ? 6 : 5;
+    // resident CTAs the FP32 lift's register budget is sized for (measured on the
+    // 3D Navier-Stokes classes: 5 beats 4 by up to 13 %; 6 is better still at
+    // Np = 5, N = 4); the FP64 lift keeps 4
+    static constexpr int MIN_BLOCKS32 = (DIM == 3 && NP == 5) ? 6 : 5;
     static_assert(BATCH_CHUNK % EPB == 0, "lift item must divide the padding chunk");
 };
 
@@ -1760,7 +1761,8 @@ lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_
 
 // Persistent batch lift: CTA-level items of EPB elements of one solve.
 template <int DIM, int NP, typename Out, bool VC>
-__global__ void __launch_bounds__(LiftBatchShape<DIM, NP>::THREADS, LiftBatchShape<DIM, NP>::MIN_BLOCKS)
+__global__ void __launch_bounds__(LiftBatchShape<DIM, NP>::THREADS,
+                                  sizeof(Out) == 8 ? 4 : LiftBatchShape<DIM, NP>::MIN_BLOCKS32)
 lift_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_constant__ OpTables T) {
     using S = Shape<DIM, NP>;
     using LB = LiftBatchShape<DIM, NP>;
