@@ -351,6 +351,10 @@ prandtl_status prandtl_batch_query(prandtl_batch *b, int id, int *steps_left, in
                                    double *dt, double *lambda_max);
 /* Waits, then copies the solve's current state (byNODES) out. */
 prandtl_status prandtl_batch_read(prandtl_batch *b, int id, double *u, int ptr_flags);
+/* Waits, then the FP64 budgets of the solve's current state, reduced on the device where it
+ * resides: out[0 .. nf-1] the integrals of the conserved fields, out[nf] the integral of the
+ * entropy function (host memory, nf + 1 doubles; as prandtl_budgets without the rates). */
+prandtl_status prandtl_batch_budgets(prandtl_batch *b, int id, double *out);
 /* Retire a solve and free its arena range (after the enqueued work). */
 prandtl_status prandtl_batch_remove(prandtl_batch *b, int id);
 /* Autotuner: per class with resident solves, time `reps` launches of each RHS

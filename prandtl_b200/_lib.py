@@ -26,7 +26,7 @@ EXPORTS = ["prandtl_config_default", "prandtl_create", "prandtl_destroy", "prand
            "prandtl_synchronize", "prandtl_kernel_launches", "prandtl_profile",
            "prandtl_profile_read", "prandtl_profile_reset", "prandtl_device_bytes",
            "prandtl_last_error", "prandtl_version", "prandtl_rhs_noalloc", "prandtl_recover_state",
-           "prandtl_budgets",
+           "prandtl_budgets", "prandtl_batch_budgets",
            "prandtl_batch_config_default", "prandtl_batch_create", "prandtl_batch_destroy",
            "prandtl_batch_footprint", "prandtl_batch_add", "prandtl_batch_advance",
            "prandtl_batch_sync", "prandtl_batch_finished", "prandtl_batch_query",
@@ -158,6 +158,7 @@ def load():
         "prandtl_batch_finished": (ip, [vp, ipp, ip, ipp]),
         "prandtl_batch_query": (ip, [vp, ip, ipp, ipp, dp, dp]),
         "prandtl_batch_read": (ip, [vp, ip, vp, ip]),
+        "prandtl_batch_budgets": (ip, [vp, ip, vp]),
         "prandtl_batch_remove": (ip, [vp, ip]),
         "prandtl_batch_tune": (ip, [vp, ip]),
         "prandtl_batch_class_info": (ip, [vp, ip, ip, ip, ipp, ipp, dp, dp]),

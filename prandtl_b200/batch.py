@@ -59,6 +59,7 @@ class Batch:
         self._h = h
         self.precision, self.scheme = precision, scheme
         self._shape = {}
+        self._nf = {}
 
     def _check(self, st):
         _lib.check(st, self._h, "prandtl_batch_last_error")
@@ -80,6 +81,7 @@ class Batch:
         self._check(self._L.prandtl_batch_add(self._h, C.byref(arr.desc), C.byref(cfg), p, flag,
                                               C.byref(sd), C.byref(sid)))
         self._shape[sid.value] = (mesh.num_fields * mesh.ndof,)
+        self._nf[sid.value] = mesh.num_fields
         return sid.value
 
     def advance(self, nsteps: int):
@@ -108,6 +110,14 @@ class Batch:
         p, flag = _ptr(out)
         self._check(self._L.prandtl_batch_read(self._h, int(sid), p, flag))
         return out
+
+    def budgets(self, sid: int) -> dict:
+        """FP64 integrals of the solve's resident state, reduced on the device:
+        the conserved fields and the entropy function."""
+        nf = self._nf[sid]
+        out = np.zeros(nf + 1)
+        self._check(self._L.prandtl_batch_budgets(self._h, int(sid), out.ctypes.data))
+        return {"conserved": out[:nf].copy(), "entropy": float(out[nf])}
 
     def remove(self, sid: int):
         self._check(self._L.prandtl_batch_remove(self._h, int(sid)))

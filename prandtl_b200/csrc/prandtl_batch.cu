@@ -120,6 +120,7 @@ struct Solve {
     bool used = false;
     int dim = 0, order = 0, key = 0, E = 0, nf = 0;
     bool ns = false;
+    double gamma = 1.4;
     long long Ndof = 0;
     size_t off = 0;
     Layout L{};
@@ -155,6 +156,7 @@ struct prandtl_batch {
     int *d_live = nullptr;       // live ids [cap] | count
     int *d_left = nullptr;       // steps left per solve id, written by the step-end kernel
     int *h_left = nullptr;       // pinned copy
+    double *d_budget = nullptr;  // budget partials [BUDGET_BLOCKS][12] + totals [12]
     std::vector<Solve> solves;
     std::vector<int> free_ids;
     std::vector<int> live;
@@ -346,6 +348,7 @@ void free_batch(prandtl_batch *b) {
     cudaFree(b->d_live);
     cudaFree(b->d_left);
     if (b->h_left) cudaFreeHost(b->h_left);
+    cudaFree(b->d_budget);
     if (b->done) cudaEventDestroy(b->done);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
@@ -425,6 +428,8 @@ prandtl_status prandtl_batch_create(const prandtl_batch_config *cin, prandtl_bat
         return bail(bcuda(b, ce, "steps-left table"));
     if ((ce = cudaMallocHost(&b->h_left, (size_t)b->cap * sizeof(int))) != cudaSuccess)
         return bail(bcuda(b, ce, "pinned steps-left"));
+    if ((ce = cudaMalloc(&b->d_budget, (size_t)(BUDGET_BLOCKS + 1) * 12 * sizeof(double))) != cudaSuccess)
+        return bail(bcuda(b, ce, "budgets"));
     b->bytes = arena + (size_t)b->cap * (sizeof(BatchInst) + 2 * sizeof(int)) + sizeof(int);
     b->solves.resize(b->cap);
     for (int q = b->cap - 1; q >= 0; --q) b->free_ids.push_back(q);
@@ -501,6 +506,7 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, 
     s.key = class_key(dim, order, ns, vc);
     s.E = E;
     s.nf = dim + 2;
+    s.gamma = cfg->gamma;
     s.Ndof = (long long)E;
     for (int d = 0; d < dim; ++d) s.Ndof *= order + 1;
     s.off = off;
@@ -665,6 +671,38 @@ prandtl_status prandtl_batch_read(prandtl_batch *b, int id, double *u, int ptr_f
                            b->stream),
         "copy state");
     return bwait(b);
+}
+
+prandtl_status prandtl_batch_budgets(prandtl_batch *b, int id, double *out) {
+    if (!b) return PRANDTL_EINVAL;
+    if (!out) return bfail(b, PRANDTL_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (id < 0 || id >= b->cap || !b->solves[id].used) return bfail(b, PRANDTL_EINVAL, "unknown solve id");
+    BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
+    const Solve &s = b->solves[id];
+    int cur = 0;
+    if (b->cfg.scheme == PRANDTL_LSRK45) {
+        BCK(b, cudaMemcpyAsync(&cur, reinterpret_cast<char *>(b->d_tab + id) + offsetof(BatchInst, cur), sizeof(int),
+                               cudaMemcpyDeviceToHost, b->stream),
+            "D2H parity");
+        prandtl_status st = bwait(b);
+        if (st != PRANDTL_OK) return st;
+    }
+    const char *base = b->arena + s.off;
+    const OpTables &T = b->classes.at(s.key).T;
+    double *tot = b->d_budget + (size_t)BUDGET_BLOCKS * 12;
+    BCK(b, launch_budgets(reinterpret_cast<const double *>(base + s.L.u[cur & 1]), nullptr,
+                          reinterpret_cast<const double *>(base + s.L.geo), T.w, s.dim, s.order + 1, s.E, s.gamma,
+                          b->d_budget, tot, b->stream),
+        "budget kernel launch");
+    b->launches += 2;
+    double buf[12];
+    BCK(b, cudaMemcpyAsync(buf, tot, sizeof(buf), cudaMemcpyDeviceToHost, b->stream), "D2H budgets");
+    prandtl_status st = bwait(b);
+    if (st != PRANDTL_OK) return st;
+    for (int f = 0; f < s.nf; ++f) out[f] = buf[f];   // device slots: conserved [0..4], entropy [5]
+    out[s.nf] = buf[5];
+    return PRANDTL_OK;
 }
 
 prandtl_status prandtl_batch_remove(prandtl_batch *b, int id) {

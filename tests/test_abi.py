@@ -100,6 +100,7 @@ def test_null_handle_calls_fail_cleanly(lib):
     assert lib.prandtl_step(None, None, 0.0, 0.1, 0, 1, 0) == _lib.PRANDTL_EINVAL
     assert lib.prandtl_synchronize(None) == _lib.PRANDTL_EINVAL
     assert lib.prandtl_budgets(None, None, None, None, 0) == _lib.PRANDTL_EINVAL
+    assert lib.prandtl_batch_budgets(None, 0, None) == _lib.PRANDTL_EINVAL
     assert lib.prandtl_recover_state(None, None, None, 0) == _lib.PRANDTL_EINVAL
     assert lib.prandtl_kernel_launches(None) == 0
     assert lib.prandtl_version().startswith(b"prandtl_b200")

@@ -90,3 +90,28 @@ def test_budgets_over_a_trajectory(precision):
     assert max(drift) <= tol, drift
     assert -1e-6 <= dS <= 0.0, dS
     op.close()
+
+
+def test_batch_budgets_match_the_operator():
+    """A batch solve's budgets read in place equal the operator's on the same
+    state, before and after steps (FP32-bulk batch: mass and energy kept)."""
+    from prandtl_b200.batch import Batch
+    mesh = periodic_box(3, 3, 3, 0.0, 2 * np.pi)
+    u0 = cases.taylor_green(mesh, mach=0.2)
+    phys = dict(parabolic=True, mu=1 / 400, Pr=0.71, quirks="fixed")
+    b = Batch("fp32", "LSRK45", arena_bytes=1 << 28)
+    sid = b.add(mesh, u0, dt=2e-3, nsteps=10, **phys)
+    op = _op(mesh, **phys)
+    b0 = b.budgets(sid)
+    r0 = op.budgets(u0)
+    np.testing.assert_array_equal(b0["conserved"], r0["conserved"])
+    assert b0["entropy"] == r0["entropy"]
+    b.advance(10)
+    b1 = b.budgets(sid)
+    r1 = op.budgets(b.read(sid))
+    np.testing.assert_array_equal(b1["conserved"], r1["conserved"])
+    for f in (0, 4):
+        assert abs(b1["conserved"][f] - b0["conserved"][f]) <= 1e-9 * abs(b0["conserved"][f])
+    assert b1["entropy"] <= b0["entropy"]
+    op.close()
+    b.close()
