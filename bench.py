@@ -597,7 +597,7 @@ def main():
             "peak_source": "measured live in this run: cuBLAS SGEMM 8192^3, TF32 off (torch.matmul float32)",
             "traffic": traffic,
             "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel on the N=5 members "
-                               "of a 24-member ensemble, scaled by elements (profiles/rhs_batch_kernel_N5_fp32_ncu.md); "
+                               "of a 24-member ensemble, scaled by elements (ncu summary rhs_batch_kernel_N5_fp32_ncu under profiles/); "
                                "that launch was an LSRK first stage, which does not read du") if tr else None,
             "flops_per_launch": fl, "avg_launch_ms": t_launch * 1e3,
             "launch_timing": "CUDA events on the batch stream (autotuner, the launch repeated on the step's first stage)",
@@ -617,7 +617,7 @@ def main():
             "peak_source": hbm_src,
             "traffic": ltr["bytes_per_element"] * E_dom if ltr else None,
             "traffic_source": ("ncu dram bytes of this kernel on the N=5 members of a 24-member ensemble, scaled by "
-                               "elements (profiles/lift_batch_kernel_N5_fp32_ncu.md)") if ltr else None}
+                               "elements (ncu summary lift_batch_kernel_N5_fp32_ncu under profiles/)") if ltr else None}
         tgv32 = None
         if not args.no_tgv32:
             tgv32 = run_tgv32(torch, 50)

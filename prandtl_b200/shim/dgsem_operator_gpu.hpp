@@ -4,8 +4,10 @@
 // the same mfem::TimeDependentOperator surface (Mult, GetMaxCharSpeed,
 // GetTimeRef), so Simulation's ODESolver::Init / Step (Simulation.cpp:807,
 // :1010) drive the sm_100a kernels unchanged.  The caller builds the
-// prandtl_mesh_desc from its mesh; mfem::Vector data are
-// host arrays in Ordering::byNODES, exactly the layout the kernels use.
+// prandtl_mesh_desc from its mesh: per element the adjugate and determinant of
+// the affine Jacobian, per face Elem1/Elem2, their local faces and the
+// CalcOrtho scaled normal.  mfem::Vector data are host arrays in
+// Ordering::byNODES, exactly the layout the kernels use.
 #pragma once
 
 #include <stdexcept>
