@@ -126,7 +126,7 @@ cudaError_t batch_launch_lift(int dim, int order, bool vc, bool fp32, int grid, 
 // s = ln(p rho^-g); with dudt also the integrals of dudt_f and of v . dudt
 // (v the entropy variables).  nout = 2 nf + 2 values; deterministic two-pass
 // reduction through `partials` ([BUDGET_BLOCKS][nout]).
-constexpr int BUDGET_BLOCKS = 592;
+constexpr int BUDGET_BLOCKS = 592;    // 4 per SM on 148 SMs (grid-stride beyond)
 constexpr int BUDGET_THREADS = 256;
 cudaError_t launch_budgets(const double *u, const double *dudt, const double *geo, const double *w1d, int dim,
                            int np, int E, double gamma, double *partials, double *out, cudaStream_t s);
