@@ -71,6 +71,7 @@ def parse():
     p.add_argument("--serve-requests", type=int, default=500)
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--no-tgv32", action="store_true")
+    p.add_argument("--no-configs", action="store_true", help="skip the 2D vortex and Kelvin-Helmholtz keys")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-peaks", action="store_true", help="skip the live SGEMM/DGEMM peak runs")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -127,10 +128,15 @@ def measured_traffic():
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
+    """nvidia-smi clock/throttle samples every 100 ms while the block runs; the
+    CSV goes to PRANDTL_BENCH_CLOCKS_DIR if set, else a temporary folder."""
+
     def __init__(self, index, tag):
+        import tempfile
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{tag}_rank{index}.csv")
+        folder = os.environ.get("PRANDTL_BENCH_CLOCKS_DIR") or tempfile.mkdtemp(prefix="prandtl_clocks_")
+        self.path = os.path.join(folder, f"clocks_{tag}_rank{index}.csv")
 
     def __enter__(self):
         try:
@@ -189,73 +195,90 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- CPU side
 def _cpu_worker(job):
-    """One CPU process: LSRK4(5) steps of one ensemble member (order, Mach,
-    Re as drawn) on a 3^3-element mesh.  kind 'reference' runs the
+    """One CPU process advances one ensemble member on its own mesh (the same
+    n^3 elements, N, Mach and Re as in the GPU batch) with LSRK4(5) stages for
+    a fixed wall-clock window, stage by stage.  kind 'reference' runs the
     reference's own DGSEM sources (oracle/_ref), kind 'port' the oracle
-    restatement.  Returns (DOF updates, seconds, steps)."""
-    kind, order, mach, re, steps, seconds, threads = job
+    restatement.  Returns (DOF updates, seconds, stages, elements, order)."""
+    kind, index, seconds, threads = job
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
     import pyoracle
-    from prandtl_b200 import cases
-    from prandtl_b200.ensemble import fixed_dt
-    from prandtl_b200.mesh import periodic_box
-    mesh = periodic_box(3, 3, order, 0.0, 2 * np.pi)
-    u = cases.taylor_green(mesh, mach=mach)
-    kw = dict(parabolic=1, blending=0, mu=1.0 / re, Pr=0.71, gamma=1.4, quirks=1)
+    from prandtl_b200.ensemble import fixed_dt, tgv_ensemble
+    m = tgv_ensemble(index + 1)[index]
+    mesh = m.mesh()
+    u = m.initial_state(mesh)
+    kw = dict(parabolic=1, blending=0, mu=1.0 / m.re, Pr=0.71, gamma=1.4, quirks=1)
     cls = pyoracle.RefOperator if kind == "reference" else pyoracle.Oracle
     op = cls(mesh, nthreads=threads, **kw)
     dt = fixed_dt(mesh, u, CFL)
-    u = op.step(u, dt, scheme=1, nsteps=1)   # warm-up
-    done, t0 = 0, time.perf_counter()
+    A, B = pyoracle._LSRK_A, pyoracle._LSRK_B
+    du = np.zeros_like(u)
+    op.rhs(u)   # warm-up
+    stages, t0 = 0, time.perf_counter()
     while True:
-        u = op.step(u, dt, scheme=1, nsteps=1)
-        done += 1
+        k = stages % 5
+        du = A[k] * du + dt * op.rhs(u)["dudt"]
+        u = u + B[k] * du
+        stages += 1
         el = time.perf_counter() - t0
-        if (steps is not None and done >= steps) or el >= seconds:
+        if el >= seconds:
             break
-    return mesh.ndof * mesh.num_fields * done, el, done
+    return mesh.ndof * mesh.num_fields * stages / 5.0, el, stages, mesh.num_elements, m.order
 
 
-def cpu_rate(steps=None, seconds=12.0):
-    """DOF-updates/s of the CPU path on all host cores.  With the reference's
-    own sources built (oracle/_ref) this is the reference: one process per core
+def cpu_rate(seconds=12.0, single_core=True):
+    """DOF-updates/s of the CPU path on all host cores: with the reference's own
+    sources built (oracle/_ref) this is the reference, one process per core
     (the reference scales by MPI domain decomposition, run.sh `mpiexec -n`),
-    process i advancing ensemble member i on a 3^3-element mesh.  Otherwise the
-    oracle restatement runs the same sample."""
+    process i advancing ensemble member i on its own mesh; otherwise the
+    oracle restatement runs the same sample.  Every process runs for the same
+    wall-clock window, so no core idles, and the rate is the sum of the
+    processes' own rates.  With single_core, member 0 is also timed alone on
+    one core."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import multiprocessing as mp
     import pyoracle
-    from prandtl_b200.ensemble import tgv_ensemble
     cores = os.cpu_count() or 1
     kind = "reference" if pyoracle.ref_available() else "port"
-    ens = tgv_ensemble(max(cores, 4))
-    jobs = [(kind, m.order, m.mach, m.re, steps, seconds, 1) for m in ens[:cores]]
-    with mp.get_context("spawn").Pool(cores) as pool:
-        res = pool.map(_cpu_worker, jobs)
-    upd = sum(r[0] for r in res)
-    el = max(r[1] for r in res)
-    nsteps = min(r[2] for r in res)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_cpu_worker, [(kind, i, seconds, 1) for i in range(cores)])
+    rate = sum(r[0] / r[1] for r in res)
+    one = None
+    if single_core:
+        # the sampled member of median size, alone on one core
+        order = sorted(range(len(res)), key=lambda i: res[i][0] / max(1, res[i][2]))
+        mid = order[len(order) // 2]
+        with ctx.Pool(1) as pool:
+            r1 = pool.map(_cpu_worker, [(kind, mid, seconds, 1)])[0]
+        one = {"value": r1[0] / r1[1], "unit": "DOF-updates/s", "cores": 1,
+               "sample": f"ensemble member {mid} ({r1[3]} elements, N={r1[4]}, the sample's median size) "
+                         f"alone on one core, {r1[2]} LSRK stages in {r1[1]:.1f} s"}
     src = "reference DGSEM sources (oracle/_ref, -O2)" if kind == "reference" else "oracle C++ restatement -O2"
-    sample = (f"{src} x {cores} processes; process i advances ensemble member i (its N, Mach, Re) "
-              f"on 3^3 elements with LSRK4(5), >= {nsteps} steps each in {el:.1f} s")
-    return upd / el, dict(kind=kind, cores=cores, steps=nsteps, seconds=el, sample=sample)
+    elems = sorted({(r[3], r[4]) for r in res})
+    sample = (f"{src} x {cores} processes, each for {seconds:.0f} s of wall clock: process i advances "
+              f"ensemble member i on its own mesh (the batch's sizes: {len(res)} members, "
+              f"{min(e for e, _ in elems)}..{max(e for e, _ in elems)} elements, N "
+              f"{sorted({o for _, o in elems})}) with LSRK4(5) stages; rate = sum of the processes' rates; "
+              f"{min(r[2] for r in res)}..{max(r[2] for r in res)} stages each")
+    return rate, dict(kind=kind, cores=cores, seconds=max(r[1] for r in res),
+                      stages=sum(r[2] for r in res), sample=sample, single_core=one)
 
 
 def run_reference(args, rank):
     if rank != 0:
         return
     budget = max(10.0, min(120.0, 0.6 * (args.steps + args.warmup)))
-    cpu_rate(steps=max(1, args.warmup), seconds=budget / 4)
-    rate, info = cpu_rate(steps=max(1, args.steps), seconds=budget)
+    rate, info = cpu_rate(seconds=budget, single_core=False)
     line = {
         "metric": "DOF-updates/s/GPU", "value": rate, "unit": "DOF-updates/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * info["seconds"] / max(1, info["steps"]),
+        "ms_per_step": 1e3 * info["seconds"] * 5.0 * info["cores"] / max(1, info["stages"]),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (standard TGV initial condition)",
         "config": {"workload": WORKLOAD, "scheme": "LSRK45", "cfl": CFL,
-                   "sample": "each host core advances one ensemble member on 3^3 elements"},
+                   "sample": "each host core advances one ensemble member on its own mesh for the same window"},
         "cpu_baseline": {"value": rate, "unit": "DOF-updates/s", "cores": info["cores"],
                          "kind": info["kind"], "sample": info["sample"]},
         "e2e": {"value": rate, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -412,16 +435,21 @@ def budget_summary(budgets, steps):
     return out
 
 
-def run_tgv32(torch, steps):
-    """The 32^3 N=3 TGV (one solve) through the plain FP64 path with per-kernel
-    CUDA-event times."""
+def run_tgv32(torch, steps, fp32_steps=200, extras=True):
+    """BASELINE config 2, the 32^3 N=3 TGV (one solve), through the plain FP64
+    path: per-kernel CUDA-event times of `steps` LSRK steps; the drop-in call
+    pattern (DGSEMOperator::Mult on host vectors, one call per RK stage:
+    pageable H2D, lift + RHS, D2H) by wall clock; and the FP32-bulk form against
+    FP64 after `fp32_steps` steps at CFL 0.5 (L2 / Linf of rho, momentum, energy)."""
     import numpy as np
     from prandtl_b200 import cases
+    from prandtl_b200.ensemble import fixed_dt
     from prandtl_b200.mesh import periodic_box
     from prandtl_b200.operator import DGSEMOperator
     mesh = periodic_box(3, 32, 3, 0.0, 2 * np.pi)
     u0 = cases.taylor_green(mesh)
-    op = DGSEMOperator(mesh, parabolic=True, mu=1.0 / 1600.0, Pr=0.71, quirks="fixed")
+    phys = dict(parabolic=True, mu=1.0 / 1600.0, Pr=0.71, quirks="fixed")
+    op = DGSEMOperator(mesh, **phys)
     stream = torch.cuda.current_stream()
     op.set_stream(stream.cuda_stream)
     u = torch.from_numpy(u0).cuda()
@@ -441,15 +469,137 @@ def run_tgv32(torch, steps):
     el = e0.elapsed_time(e1) / 1e3
     prof = op.profile_read()
     op.profile(False)
+    if not extras:
+        op.close()
+        return None
+    # drop-in pattern: Mult with host (pageable) vectors, as mfem::ODESolver calls it
+    uh = u.cpu().numpy()
+    dh = np.empty_like(uh)
+    op.Mult(uh, dh)
+    reps = 10
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        op.Mult(uh, dh)
+    mult_s = (time.perf_counter() - t0) / reps
     op.close()
     dof = mesh.ndof * mesh.num_fields
     rhs_ms = prof["rhs"][0] / prof["rhs"][1]
     lift_ms = prof["lift"][0] / prof["lift"][1]
     E = mesh.num_elements
+    # FP32 bulk vs FP64 after fp32_steps steps at CFL 0.5
+    dt5 = fixed_dt(mesh, u0, 0.5)
+    fin, ftime = {}, {}
+    for prec in ("fp64", "fp32"):
+        o = DGSEMOperator(mesh, precision=prec, **phys)
+        o.set_stream(stream.cuda_stream)
+        x = torch.from_numpy(u0).cuda()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        o.Step(x, dt5, scheme="LSRK45", nsteps=fp32_steps)
+        b.record(stream)
+        o.synchronize()
+        ftime[prec] = a.elapsed_time(b) / 1e3
+        fin[prec] = x.cpu().numpy()
+        o.close()
     return {"workload": "tgv3d_navier_stokes_32^3_N3_lsrk45_fp64", "dof": dof,
             "value": dof * steps / el, "unit": "DOF-updates/s", "ms_per_step": 1e3 * el / steps,
             "rhs_ms": rhs_ms, "lift_ms": lift_ms,
-            "rhs_flops": E * flops_per_element(3, 3), "rhs_algorithmic_bytes": E * rhs_bytes_per_element(3, 3, 8)}
+            "rhs_flops": E * flops_per_element(3, 3), "rhs_algorithmic_bytes": E * rhs_bytes_per_element(3, 3, 8),
+            "dropin_mult_host": {
+                "ms_per_call": 1e3 * mult_s, "kernels_ms": rhs_ms + lift_ms,
+                "dof_rhs_per_s": dof / mult_s, "bytes_per_call": 2 * dof * 8,
+                "pattern": "DGSEMOperator.Mult(u, dudt) on pageable numpy vectors: H2D of u, lift + RHS "
+                           "kernels, D2H of dudt, wait; one call per RK stage as mfem::ODESolver::Step makes"},
+            "fp32_vs_fp64": {"steps": fp32_steps, "cfl": 0.5, "scheme": "LSRK45",
+                             **rel_errors(fin["fp32"], fin["fp64"], mesh.num_fields),
+                             "fp64_dof_updates_per_s": dof * fp32_steps / ftime["fp64"],
+                             "fp32_dof_updates_per_s": dof * fp32_steps / ftime["fp32"],
+                             "format": "per field: [relative L2, relative Linf]"}}
+
+
+def run_ivortex32(torch, steps=100):
+    """2D Euler isentropic vortex 32^2 N=3 (plain method,
+    FP64), SSP-RK3 at CFL 0.5 (dt from the initial lambda_max), `steps` steps."""
+    from prandtl_b200 import cases
+    from prandtl_b200.ensemble import fixed_dt
+    from prandtl_b200.operator import DGSEMOperator
+    mesh, u0, _ = cases.make_case("ivortex", 32, 3)
+    op = DGSEMOperator(mesh, quirks="reference")
+    stream = torch.cuda.current_stream()
+    op.set_stream(stream.cuda_stream)
+    u = torch.from_numpy(u0).cuda()
+    dt = fixed_dt(mesh, u0, 0.5)
+    op.Step(u, dt, scheme="RK3SSP", nsteps=3)
+    op.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    op.Step(u, dt, scheme="RK3SSP", nsteps=steps)
+    b.record(stream)
+    op.synchronize()
+    el = a.elapsed_time(b) / 1e3
+    dof = mesh.ndof * mesh.num_fields
+    op.close()
+    return {"workload": "ivortex2d_euler_32^2_N3_ssprk3_fp64", "steps": steps, "dof": dof,
+            "value": dof * steps / el, "unit": "DOF-updates/s", "ms_per_step": 1e3 * el / steps,
+            "note": "65,536 DOF: far too small to fill a B200 (launch- and latency-bound)"}
+
+
+def run_kh256(torch, t_final=3.0, precisions=("fp64", "fp32")):
+    """2D Euler Kelvin-Helmholtz 256^2 N=3 with the modal
+    indicator and subcell FV blending (alpha_max 0.5), SSP-RK3 with
+    dt = 0.4 hmin / (lambda_max (N+1)^2) after every step (on the device), to
+    t = 3, one batch solve per precision.  Every stage checks every node
+    (non-finite, rho <= 0, p <= 0); mass and energy budgets on the device;
+    the blending field at t = 3 from one RHS of the final state."""
+    import numpy as np
+    from prandtl_b200 import cases
+    from prandtl_b200.batch import Batch
+    from prandtl_b200.ensemble import fixed_dt
+    from prandtl_b200.operator import DGSEMOperator
+    mesh, u0, _ = cases.make_case("kh", 256, 3)
+    phys = dict(blending=True, alpha_max=0.5, quirks="reference")
+    out = {"workload": "kh2d_euler_256^2_N3_blended_ssprk3_cfl0.4_to_t3", "dof": mesh.ndof * mesh.num_fields}
+    for prec in precisions:
+        b = Batch(prec, "RK3SSP", arena_bytes=2 << 30)
+        sid = b.add(mesh, u0, dt=fixed_dt(mesh, u0, 0.4), nsteps=1 << 30, cfl=0.4, t_final=t_final, **phys)
+        b0 = b.budgets(sid)
+        stream = torch.cuda.ExternalStream(b.stream)
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        status = "ok"
+        a.record(stream)
+        try:
+            while sid not in b.finished():
+                b.advance(2000)
+                b.query(sid)
+        except Exception as exc:   # a failed state check (PRANDTL_ENONFINITE) ends the run
+            status = str(exc)
+        e.record(stream)
+        b.sync()
+        dev_s = a.elapsed_time(e) / 1e3
+        q = b.query(sid) if status == "ok" else {}
+        t = b.time(sid)
+        b1 = b.budgets(sid)
+        u = b.read(sid) if status == "ok" else None
+        b.close()
+        rec = {"status": status, "t": t, "steps": q.get("steps_done"), "device_s": dev_s,
+               "dof_updates_per_s": out["dof"] * q.get("steps_done", 0) / dev_s if q else None,
+               "state_check": "every node of every stage: finite, rho > 0, p > 0" + (" - passed" if status == "ok"
+                                                                                         else " - FAILED"),
+               "mass_rel_drift": abs(b1["conserved"][0] - b0["conserved"][0]) / abs(b0["conserved"][0]),
+               "energy_rel_drift": abs(b1["conserved"][3] - b0["conserved"][3]) / abs(b0["conserved"][3])}
+        if u is not None:
+            v = u.reshape(4, -1)
+            p = 0.4 * (v[3] - 0.5 * (v[1] ** 2 + v[2] ** 2) / v[0])
+            rec["min_rho"], rec["min_p"] = float(v[0].min()), float(p.min())
+            op = DGSEMOperator(mesh, **phys)
+            d = np.empty_like(u)
+            op.Mult(u, d)
+            al = op.alpha()
+            op.close()
+            rec["alpha_at_t"] = {"elements_blended": int((al > 0).sum()), "fraction": float((al > 0).mean()),
+                                 "max": float(al.max()), "mean": float(al.mean())}
+        out[prec] = rec
+    return out
 
 
 def run_serving(torch, n_req):
@@ -554,7 +704,7 @@ def main():
 
     K, W = args.steps, args.warmup
     if args.profile_case == "tgv32":
-        run_tgv32(torch, K)
+        run_tgv32(torch, K, extras=False)
         return
     members = tgv_ensemble(args.ensemble)
     items = build_items(members)
@@ -618,6 +768,8 @@ def main():
             "traffic": ltr["bytes_per_element"] * E_dom if ltr else None,
             "traffic_source": ("ncu dram bytes of this kernel on the N=5 members of a 24-member ensemble, scaled by "
                                "elements (ncu summary lift_batch_kernel_N5_fp32_ncu under profiles/)") if ltr else None}
+        ivortex32 = run_ivortex32(torch) if not args.no_configs else None
+        kh256 = run_kh256(torch) if not args.no_configs else None
         tgv32 = None
         if not args.no_tgv32:
             tgv32 = run_tgv32(torch, 50)
@@ -636,7 +788,7 @@ def main():
             try:
                 rate, info = cpu_rate(seconds=args.cpu_seconds)
                 cpu = {"value": rate, "unit": "DOF-updates/s", "cores": info["cores"],
-                       "kind": info["kind"], "sample": info["sample"]}
+                       "kind": info["kind"], "sample": info["sample"], "single_core": info["single_core"]}
             except Exception as exc:
                 cpu = {"value": None, "unit": "DOF-updates/s", "cores": os.cpu_count(), "kind": "port",
                        "sample": f"unavailable: {exc}"}
@@ -665,6 +817,8 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "tgv32": tgv32,
+            "ivortex32": ivortex32,
+            "kh256": kh256,
             "serving": serving,
             "clocks": binfo["clocks"],
         }

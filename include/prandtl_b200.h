@@ -34,12 +34,21 @@ typedef enum prandtl_status {
     PRANDTL_OK = 0,
     PRANDTL_EINVAL = 1,        /* bad argument or descriptor */
     PRANDTL_ENOMEM = 2,        /* device allocation failed */
-    PRANDTL_ENONFINITE = 3,    /* non-finite state detected (NaN check) */
+    PRANDTL_ENONFINITE = 3,    /* the RK state left the admissible set: a non-finite value, or
+                                  density or pressure <= 0 (the reference's NaN check,
+                                  Simulation.cpp:1024-1035, extended to positivity) */
     PRANDTL_ETIMEDOUT = 4,     /* a bounded wait ran out */
     PRANDTL_ECUDA = 5,         /* CUDA runtime error (text in prandtl_last_error) */
     PRANDTL_EUNSUPPORTED = 6,  /* valid input outside what this build implements */
     PRANDTL_ETOOLARGE = 7      /* input larger than a fixed-size limit (prandtl_rhs_noalloc) */
 } prandtl_status;
+
+/* State-check bits behind PRANDTL_ENONFINITE: every RK stage checks every
+ * node of the state it writes (the axisymmetric form checks finiteness only,
+ * since its RK state r U vanishes on the axis). */
+#define PRANDTL_HEALTH_NONFINITE 1u
+#define PRANDTL_HEALTH_DENSITY 2u
+#define PRANDTL_HEALTH_PRESSURE 4u
 
 /* Pointer-location flags for the u / dudt arguments. */
 #define PRANDTL_PTR_HOST 0     /* host memory: staged through the handle's device buffers */
@@ -157,7 +166,13 @@ prandtl_status prandtl_rhs(prandtl_handle *h, const double *u, double *dudt, dou
                            double *lambda_max, int ptr_flags);
 
 /* nsteps steps of size dt applied to u in place (ODESolver::Step,
- * Simulation.cpp:1010); each stage fuses the RK update into the RHS kernel. */
+ * Simulation.cpp:1010); each stage fuses the RK update into the RHS kernel.
+ * Every stage checks the state it writes (PRANDTL_HEALTH_*) into a sticky
+ * device flag of the handle.  With host pointers the call waits and returns
+ * PRANDTL_ENONFINITE (state still copied back, reason in prandtl_last_error)
+ * when any stage of these steps failed the check; with device pointers it
+ * returns without waiting and the next prandtl_synchronize reports the flag.
+ * Reporting clears the flag. */
 prandtl_status prandtl_step(prandtl_handle *h, double *u, double t, double dt, int scheme,
                             int nsteps, int ptr_flags);
 
@@ -190,7 +205,8 @@ double prandtl_cfl_dt(double cfl, double hmin, double lambda_max, int order);
 /* Use a caller-owned cudaStream_t (passed as void*) instead of the handle's. */
 prandtl_status prandtl_set_stream(prandtl_handle *h, void *cuda_stream);
 
-/* Wait for all work on the handle's stream, at most cfg->timeout_s. */
+/* Wait for all work on the handle's stream, at most cfg->timeout_s; then
+ * PRANDTL_ENONFINITE if a step since the last report failed the state check. */
 prandtl_status prandtl_synchronize(prandtl_handle *h);
 
 /* Number of kernels this handle has launched (instrumentation). */
@@ -211,7 +227,8 @@ prandtl_status prandtl_profile_reset(prandtl_handle *h);
 size_t prandtl_device_bytes(const prandtl_handle *h);
 
 /* Text of the last error on this handle ("" if none); h may be NULL for the
- * last error of a failed prandtl_create on this thread. */
+ * last error of a failed prandtl_create or prandtl_rhs_noalloc on this thread
+ * (kept in a fixed thread-local buffer). */
 const char *prandtl_last_error(const prandtl_handle *h);
 
 const char *prandtl_version(void);
@@ -287,13 +304,18 @@ const char *prandtl_io_last_error(void);
  * to 256 bytes (3D N=3: about 4,200 elements); larger meshes return
  * PRANDTL_ETOOLARGE before any device work.
  * The first call on a device looks up the array's device address while that
- * device is current; make that first call before any stream capture.  The
- * call validates the mesh on the device, waits (bounded by cfg->timeout_s) for
- * that check, then enqueues the kernels on `cuda_stream` (a cudaStream_t, NULL
- * for the default stream) and returns without waiting for them.  All calls
- * share the scratch array, which keeps the last call's contents; calls that
- * overlap on the GPU (other streams or host threads on the same device) race.
- * No lambda_max or blending-coefficient output. */
+ * device is current and creates the one CUDA event the call waits on; make
+ * that first call before any stream capture.  Every call validates the mesh
+ * on the device (faces in range, aligned, each element face listed once,
+ * det J > 0), records that event behind the check on `cuda_stream` (a
+ * cudaStream_t, NULL for the default stream) and waits for it on the host,
+ * bounded by cfg->timeout_s (PRANDTL_ETIMEDOUT), reads the check's 4-byte
+ * result, then enqueues the RHS kernels and returns without waiting for them.
+ * A failed check returns PRANDTL_EUNSUPPORTED with the reason in
+ * prandtl_last_error(NULL).  All calls share the scratch array, which keeps
+ * the last call's contents; calls that overlap on the GPU (other streams or
+ * host threads on the same device) race.  No lambda_max or
+ * blending-coefficient output. */
 #define PRANDTL_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 prandtl_status prandtl_rhs_noalloc(const prandtl_mesh_desc *mesh_dev, const prandtl_config *cfg,
                                    const double *u_dev, double *dudt_dev, void *cuda_stream);
@@ -327,7 +349,10 @@ typedef struct {
     double cfl;             /* > 0: after each step dt = cfl*hmin/(lambda_max (N+1)^2),
                                lambda_max over that step's stages (Simulation.cpp:1013-1018) */
     double hmin;            /* smallest element size, for cfl > 0 */
-    int nsteps;             /* steps to take */
+    int nsteps;             /* steps to take (at most, with t_final) */
+    double t_final;         /* > 0: end time; each step takes min(dt, t_final - t) and the solve
+                               stops once t >= t_final - 1e-8 dt (Simulation.cpp:1007-1024);
+                               0: no end time */
 } prandtl_solve_desc;
 
 void prandtl_batch_config_default(prandtl_batch_config *c);
@@ -344,12 +369,19 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *mesh
 prandtl_status prandtl_batch_advance(prandtl_batch *b, int nsteps);
 /* Wait (bounded) for the enqueued work. */
 prandtl_status prandtl_batch_sync(prandtl_batch *b);
-/* Waits, then lists up to `cap` resident solves with no steps left. */
+/* Waits, then lists up to `cap` resident solves with no steps left (including
+ * solves stopped by a failed state check). */
 prandtl_status prandtl_batch_finished(prandtl_batch *b, int *ids, int cap, int *count);
-/* Waits, then reports one solve's progress, current dt and last-step lambda_max. */
+/* Waits, then reports one solve's progress, current dt and last-step lambda_max;
+ * PRANDTL_ENONFINITE (outputs still filled) when an RK stage of the solve failed
+ * the state check (PRANDTL_HEALTH_*): that solve alone stopped at the end of the
+ * step, the others go on. */
 prandtl_status prandtl_batch_query(prandtl_batch *b, int id, int *steps_left, int *steps_done,
                                    double *dt, double *lambda_max);
-/* Waits, then copies the solve's current state (byNODES) out. */
+/* Waits, then reports the solve's simulated time (the sum of its steps' dt). */
+prandtl_status prandtl_batch_time(prandtl_batch *b, int id, double *t);
+/* Waits, then copies the solve's current state (byNODES) out; PRANDTL_ENONFINITE
+ * (state still copied) for a solve stopped by the state check. */
 prandtl_status prandtl_batch_read(prandtl_batch *b, int id, double *u, int ptr_flags);
 /* Waits, then the FP64 budgets of the solve's current state, reduced on the device where it
  * resides: out[0 .. nf-1] the integrals of the conserved fields, out[nf] the integral of the

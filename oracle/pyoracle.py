@@ -154,6 +154,77 @@ class Oracle:
         return u
 
 
+# ---------------------------------------------------------------------------
+# The same restatement evaluated in x87 long double (liboracle_ld.so, built by
+# the Makefile from a copy of prandtl_oracle.cpp with every double lifted):
+# the near-exact operator against which both FP64 evaluations, the oracle's and
+# the GPU's, are measured when their own rounding of large cancelling terms
+# exceeds the 1e-12 budget.
+_LD = None
+_LDP = C.POINTER(C.c_longdouble)
+
+
+class _MeshLD(C.Structure):
+    _fields_ = [("dim", C.c_int), ("order", C.c_int), ("num_elements", C.c_int), ("num_faces", C.c_int),
+                ("elem_adj", _LDP), ("elem_detj", _LDP), ("face_elems", C.POINTER(C.c_int)), ("face_nor", _LDP)]
+
+
+class _ConfigLD(C.Structure):
+    _fields_ = [("gamma", C.c_longdouble), ("Pr", C.c_longdouble), ("mu", C.c_longdouble),
+                ("R_gas", C.c_longdouble), ("alpha_max", C.c_longdouble), ("alpha_min", C.c_longdouble),
+                ("parabolic", C.c_int), ("blending", C.c_int), ("sutherland", C.c_int),
+                ("quirks", C.c_int), ("surface_dissipation", C.c_int),
+                ("num_bcs", C.c_int), ("bcs", C.c_void_p),
+                ("axisymmetric", C.c_int), ("node_coords", _LDP), ("axis_rho_floor", C.c_longdouble)]
+
+
+def lib_ld():
+    global _LD
+    if _LD is None:
+        path = os.path.join(_HERE, "liboracle_ld.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        L.oracle_rhs.argtypes = [C.POINTER(_MeshLD), C.POINTER(_ConfigLD), _LDP, _LDP, _LDP, _LDP, _LDP, C.c_int]
+        L.oracle_rhs.restype = C.c_int
+        _LD = L
+    return _LD
+
+
+class LongDoubleOracle:
+    """Periodic meshes, planar forms: rhs(u) in long double (u may be float64)."""
+
+    def __init__(self, mesh, gamma=1.4, Pr=0.72, mu=0.02, R_gas=287.05, alpha_max=0.5, alpha_min=0.001,
+                 parabolic=0, blending=0, sutherland=0, quirks=0, surface_dissipation=1, nthreads=None):
+        ld = np.longdouble
+        self.mesh = mesh
+        self._adj = np.ascontiguousarray(mesh.elem_adj, dtype=ld)
+        self._detj = np.ascontiguousarray(mesh.elem_detj, dtype=ld)
+        self._faces = np.ascontiguousarray(mesh.face_elems, dtype=np.int32)
+        self._nor = np.ascontiguousarray(mesh.face_nor, dtype=ld)
+        self.m = _MeshLD(mesh.dim, mesh.order, mesh.num_elements, mesh.num_faces,
+                         self._adj.ctypes.data_as(_LDP), self._detj.ctypes.data_as(_LDP),
+                         self._faces.ctypes.data_as(C.POINTER(C.c_int)), self._nor.ctypes.data_as(_LDP))
+        self.c = _ConfigLD(gamma, Pr, mu, R_gas, alpha_max, alpha_min, parabolic, blending, sutherland, quirks,
+                           surface_dissipation, 0, None, 0, None, 0.0)
+        self.nthreads = nthreads or os.cpu_count() or 1
+
+    def rhs(self, u, want_alpha=False):
+        u = np.ascontiguousarray(u, dtype=np.longdouble)
+        dudt = np.empty_like(u)
+        alpha = np.empty(self.mesh.num_elements, dtype=np.longdouble) if want_alpha else None
+        lam = np.zeros(1, dtype=np.longdouble)
+        rc = lib_ld().oracle_rhs(C.byref(self.m), C.byref(self.c), u.ctypes.data_as(_LDP),
+                                 dudt.ctypes.data_as(_LDP), alpha.ctypes.data_as(_LDP) if alpha is not None else None,
+                                 lam.ctypes.data_as(_LDP), None, self.nthreads)
+        if rc != 0:
+            raise RuntimeError(f"oracle_rhs (long double) failed ({rc})")
+        out = {"dudt": dudt, "lambda_max": lam[0]}
+        if alpha is not None:
+            out["alpha"] = alpha
+        return out
+
+
 def gl(order):
     n = order + 1
     x, w, D = np.empty(n), np.empty(n), np.empty(n * n)

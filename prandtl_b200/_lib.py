@@ -32,7 +32,7 @@ EXPORTS = ["prandtl_config_default", "prandtl_create", "prandtl_destroy", "prand
            "prandtl_batch_sync", "prandtl_batch_finished", "prandtl_batch_query",
            "prandtl_batch_read", "prandtl_batch_remove", "prandtl_batch_tune",
            "prandtl_batch_class_info", "prandtl_batch_stream", "prandtl_batch_device_bytes",
-           "prandtl_batch_arena_bytes",
+           "prandtl_batch_arena_bytes", "prandtl_batch_time",
            "prandtl_batch_kernel_launches", "prandtl_batch_last_error",
            "prandtl_serve_create", "prandtl_serve_submit", "prandtl_serve_poll",
            "prandtl_serve_wait", "prandtl_serve_stats_get", "prandtl_serve_destroy",
@@ -79,7 +79,8 @@ class BatchConfig(C.Structure):
 
 
 class SolveDesc(C.Structure):
-    _fields_ = [("dt", C.c_double), ("cfl", C.c_double), ("hmin", C.c_double), ("nsteps", C.c_int)]
+    _fields_ = [("dt", C.c_double), ("cfl", C.c_double), ("hmin", C.c_double), ("nsteps", C.c_int),
+                ("t_final", C.c_double)]
 
 
 class ServeStats(C.Structure):
@@ -158,6 +159,7 @@ def load():
         "prandtl_batch_finished": (ip, [vp, ipp, ip, ipp]),
         "prandtl_batch_query": (ip, [vp, ip, ipp, ipp, dp, dp]),
         "prandtl_batch_read": (ip, [vp, ip, vp, ip]),
+        "prandtl_batch_time": (ip, [vp, ip, dp]),
         "prandtl_batch_budgets": (ip, [vp, ip, vp]),
         "prandtl_batch_remove": (ip, [vp, ip]),
         "prandtl_batch_tune": (ip, [vp, ip]),

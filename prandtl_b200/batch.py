@@ -43,8 +43,9 @@ def _batch_config(precision, scheme, arena_bytes, max_solves, steps_per_graph, u
     return c
 
 
-def _solve_desc(mesh: Mesh, dt, nsteps, cfl, hmin):
-    return _lib.SolveDesc(float(dt), float(cfl), float(mesh.hmin if hmin is None else hmin), int(nsteps))
+def _solve_desc(mesh: Mesh, dt, nsteps, cfl, hmin, t_final=0.0):
+    return _lib.SolveDesc(float(dt), float(cfl), float(mesh.hmin if hmin is None else hmin), int(nsteps),
+                          float(t_final))
 
 
 class Batch:
@@ -71,12 +72,14 @@ class Batch:
         self._check(self._L.prandtl_batch_footprint(self._h, C.byref(arr.desc), C.byref(cfg), C.byref(n)))
         return n.value
 
-    def add(self, mesh: Mesh, u0, *, dt, nsteps, cfl=0.0, hmin=None, **phys) -> int:
-        """Admit a solve; raises PrandtlError(ENOMEM) when the arena has no room."""
+    def add(self, mesh: Mesh, u0, *, dt, nsteps, cfl=0.0, hmin=None, t_final=0.0, **phys) -> int:
+        """Admit a solve; raises PrandtlError(ENOMEM) when the arena has no room.
+        cfl > 0 updates dt from each step's lambda_max; t_final > 0 stops the
+        solve at that time (the last step shortened to reach it)."""
         arr = MeshArrays(mesh)
         cfg = make_config(**phys)
         p, flag = _ptr(u0)
-        sd = _solve_desc(mesh, dt, nsteps, cfl, hmin)
+        sd = _solve_desc(mesh, dt, nsteps, cfl, hmin, t_final)
         sid = C.c_int(-1)
         self._check(self._L.prandtl_batch_add(self._h, C.byref(arr.desc), C.byref(cfg), p, flag,
                                               C.byref(sd), C.byref(sid)))
@@ -103,6 +106,12 @@ class Batch:
         self._check(self._L.prandtl_batch_query(self._h, int(sid), C.byref(left), C.byref(done),
                                                 C.byref(dt), C.byref(lam)))
         return {"steps_left": left.value, "steps_done": done.value, "dt": dt.value, "lambda_max": lam.value}
+
+    def time(self, sid: int) -> float:
+        """Simulated time of the solve (the sum of its steps' dt)."""
+        t = C.c_double()
+        self._check(self._L.prandtl_batch_time(self._h, int(sid), C.byref(t)))
+        return t.value
 
     def read(self, sid: int, out=None):
         if out is None:

@@ -257,6 +257,12 @@ constexpr int next_pow2(int v) { return v <= 1 ? 1 : 2 * next_pow2((v + 1) / 2);
 #ifndef PRANDTL_EULER32_MINB
 #define PRANDTL_EULER32_MINB 6
 #endif
+#ifndef PRANDTL_WIDE_MIN_ND
+#define PRANDTL_WIDE_MIN_ND 125
+#endif
+#ifndef PRANDTL_LIFT64_MINB
+#define PRANDTL_LIFT64_MINB 5
+#endif
 
 // Lane-group layout of the RHS kernel: one group of GS lanes owns one
 // element.  GS = 32 (a warp), the next power of two >= Np^d for small
@@ -279,7 +285,7 @@ template <int DIM, int NP, bool NS, typename Real, int V, bool VC>
 struct RhsLayout {
     using S = Shape<DIM, NP>;
     static constexpr int ND = S::ND, NF = S::NF, NLINE = S::NLINE, PPL = S::PPL;
-    static constexpr bool WIDE = ND >= 125;
+    static constexpr bool WIDE = ND >= PRANDTL_WIDE_MIN_ND;
     // FP32-bulk Navier-Stokes with contravariant viscous fluxes at Np = 6: 128
     // lanes, so that the 3 x 36 line tasks of the volume terms take one round
     static constexpr bool TASK128 = NS && VC && sizeof(Real) == 4 && ND >= 216;
@@ -291,9 +297,13 @@ struct RhsLayout {
     static constexpr int NID = NLINE * (NP - 1);        // subcell interfaces per direction
     static constexpr int BUF = cmax(cmax(NPD, S::NFI), cmax(NID, (5 * ND + NF - 1) / NF)) * NF;
     static constexpr int K = hoisted_count<DIM, Real>();
-    // per-element shared memory, a multiple of 4 words so every element's area
-    // stays 16-byte aligned
-    static constexpr int PER_ELEM = (K * ND + cmax(BUF, NS ? DIM * NF * ND : 0) + 3) / 4 * 4;
+    // per-element shared memory, in Real units: the hoisted primitives and the
+    // work buffer (BODY, padded to 16 bytes), then the element's neighbour-table
+    // entries (2 DIM int4), and the whole a multiple of 4 words so every
+    // element's area stays 16-byte aligned
+    static constexpr int BODY = (K * ND + cmax(BUF, NS ? DIM * NF * ND : 0) + 3) / 4 * 4;
+    static constexpr int NBR_REALS = 2 * DIM * 16 / (int)sizeof(Real);
+    static constexpr int PER_ELEM = (BODY + NBR_REALS + 3) / 4 * 4;
     static constexpr bool F64 = sizeof(Real) == 8;
     // (the Navier-Stokes form with contravariant viscous fluxes needs fewer
     // registers; in FP32 the 216-node elements of 128 lanes fit 4 CTAs of
@@ -368,6 +378,7 @@ struct ElemIO {
     const double *u_rk;         // the RK state r U (u is the U recovered from it)
     const double *rad;          // [Ndof] node radius r
     const unsigned char *axis;  // [Ndof] axis nodes
+    unsigned int *health;       // RK modes: state-check bits (PRANDTL_HEALTH_*), may be null
 };
 // Per-warp (rhs) or per-CTA (lift) copy of the current solve's constants.
 struct __align__(16) WarpCtx {
@@ -399,6 +410,7 @@ __device__ __forceinline__ ElemIO io_from_args(const MeshDev &m, const RhsArgs &
     io.u_rk = a.u_rk;
     io.rad = m.rad;
     io.axis = m.axis;
+    io.health = a.health;
     return io;
 }
 
@@ -437,6 +449,7 @@ __device__ __forceinline__ ElemIO io_from_batch(const BatchInst &I, BatchInst *I
     io.u_rk = nullptr;
     io.rad = nullptr;
     io.axis = nullptr;
+    io.health = &Im->health;
     return io;
 }
 
@@ -624,6 +637,26 @@ __device__ __forceinline__ void boundary_flux(const BcDev &bc, const double *s_i
                          P.quirks == 0, P.dissipation != 0, flux);
 }
 
+// State check of one node's new RK state: bit 0 a non-finite value, bit 1
+// rho <= 0, bit 2 p <= 0 (the last two only where `positivity`: the
+// axisymmetric RK state r U vanishes on the axis).
+template <int DIM>
+__device__ __forceinline__ unsigned state_health(const double *s, double gm1, bool positivity) {
+    constexpr int NF = DIM + 2;
+    bool finite = true;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) finite = finite && isfinite(s[f]);
+    unsigned bad = finite ? 0u : 1u;
+    if (positivity && finite) {
+        double mm = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) mm += s[1 + d] * s[1 + d];
+        if (!(s[0] > 0.0)) bad |= 2u;
+        else if (!(gm1 * (s[NF - 1] - 0.5 * mm / s[0]) > 0.0)) bad |= 4u;
+    }
+    return bad;
+}
+
 // ------------------------------------------------------------------- RHS
 // Real is the working precision of the O(Np^{d+1}) work (two-point fluxes,
 // flux differencing, surface fluxes, gradients): double for the plain FP64
@@ -675,9 +708,14 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
         }
     }
 
-    // ---- own nodes: hoisted primitives (formed in FP64); largest |V|+c
+    // ---- own nodes: hoisted primitives (formed in FP64); largest |V|+c.  The
+    //      element's neighbour-table entries are loaded with the own state and
+    //      kept in shared memory, so the face phase's neighbour-trace loads do
+    //      not wait on a table load first.
+    int4 *sNbr = reinterpret_cast<int4 *>(sH + LY::BODY);
     double lam = 0.0;
     {
+        const int4 tn = li < 2 * DIM ? __ldg(a.nbr + (long long)e * (2 * DIM) + li) : make_int4(0, 0, 0, 0);
         double st[NPL][NF];   // every load in flight before the first use
 #pragma unroll
         for (int k = 0; k < NPL; ++k) {
@@ -700,6 +738,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 }
             }
         }
+        if (li < 2 * DIM) sNbr[li] = tn;
     }
     if (a.lambda) {
         double v = active ? lam : 0.0;
@@ -1115,7 +1154,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
     auto face_load = [&](int it, FaceIn &x) {
         const int lf = it / NFN, fa = it - lf * NFN;
         const long long go = (long long)e * ND + face_node<DIM, NP>(lf, fa);
-        x.t = __ldg(a.nbr + (long long)e * (2 * DIM) + lf);
+        x.t = sNbr[lf];
         const long long gs = x.t.x < 0 ? go : (long long)x.t.x * ND + face_node<DIM, NP>(x.t.y, fa);
 #pragma unroll
         for (int f = 0; f < NF; ++f) x.s[f] = __ldg(a.u + f * Ndof + gs);
@@ -1329,41 +1368,37 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
             }
             const long long gnode = (long long)e * ND + n;
             if (rad && a.axis && a.axis[gnode]) acc[k][2] = 0;   // DGSEMOperator::ZeroAxisRadialMom
-            switch (mode) {
-            case EPI_STORE:
+            if (mode == EPI_STORE) {
 #pragma unroll
                 for (int f = 0; f < NF; ++f) a.dudt[f * Ndof + gnode] = double(acc[k][f]);
-                break;
-            case EPI_LSRK:
+                continue;
+            }
+            double nv[NF];   // the node's new RK state
 #pragma unroll
-                for (int f = 0; f < NF; ++f) {
-                    const long long g = f * Ndof + gnode;
-                    const double L = double(acc[k][f]);
+            for (int f = 0; f < NF; ++f) {
+                const long long g = f * Ndof + gnode;
+                const double L = double(acc[k][f]);
+                if (mode == EPI_LSRK) {
                     const double dv = (a.rkA == 0.0) ? a.dt * L : a.rkA * ub[kk][f] + a.dt * L;
                     a.du[g] = dv;
-                    a.u_out[g] = ua[kk][f] + a.rkB * dv;
+                    nv[f] = ua[kk][f] + a.rkB * dv;
+                } else if (mode == EPI_SSP1) {
+                    nv[f] = ua[kk][f] + a.dt * L;
+                } else if (mode == EPI_SSP2) {
+                    const double y = ua[kk][f] + a.dt * L;
+                    nv[f] = 3. / 4 * ub[kk][f] + 1. / 4 * y;
+                } else {
+                    const double y = ua[kk][f] + a.dt * L;
+                    nv[f] = 1. / 3 * ub[kk][f] + 2. / 3 * y;
                 }
-                break;
-            case EPI_SSP1:
-#pragma unroll
-                for (int f = 0; f < NF; ++f) a.u_out[f * Ndof + gnode] = ua[kk][f] + a.dt * double(acc[k][f]);
-                break;
-            case EPI_SSP2:
-#pragma unroll
-                for (int f = 0; f < NF; ++f) {
-                    const double y = ua[kk][f] + a.dt * double(acc[k][f]);
-                    a.u_out[f * Ndof + gnode] = 3. / 4 * ub[kk][f] + 1. / 4 * y;
-                }
-                break;
-            case EPI_SSP3:
-#pragma unroll
-                for (int f = 0; f < NF; ++f) {
-                    const double y = ua[kk][f] + a.dt * double(acc[k][f]);
-                    a.u_out[f * Ndof + gnode] = 1. / 3 * ub[kk][f] + 2. / 3 * y;
-                }
-                break;
-            default:
-                break;
+                a.u_out[g] = nv[f];
+            }
+            // state check (Simulation.cpp:1024-1035 checks rho for NaN): non-finite
+            // values anywhere, and (planar form) rho <= 0 or p <= 0; one atomic
+            // per violating node, none on healthy states
+            if (a.health) {
+                const unsigned bad = state_health<DIM>(nv, gm1, rad == nullptr);
+                if (bad) atomicOr(a.health, bad);
             }
         }
     }
@@ -1730,7 +1765,7 @@ struct LiftBatchShape {
 // 3D N=3: 5 beats 4 by 3.5 % in FP64, 6 beats 4 by 11 % in FP32; larger
 // elements keep 4).
 template <int NP, typename Out>
-constexpr int lift_min_blocks() { return NP <= 4 ? (sizeof(Out) == 8 ? 5 : 6) : 4; }
+constexpr int lift_min_blocks() { return NP <= 4 ? (sizeof(Out) == 8 ? PRANDTL_LIFT64_MINB : 6) : 4; }
 
 template <int DIM, int NP, typename Out, bool VC>
 __global__ void __launch_bounds__(Shape<DIM, NP>::THREADS, lift_min_blocks<NP, Out>())

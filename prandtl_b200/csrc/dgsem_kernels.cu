@@ -87,10 +87,15 @@ __global__ void batch_step_end_kernel(BatchInst *tab, const int *live, const int
         const int id = live[q];
         BatchInst &I = tab[id];
         if (I.steps_left <= 0) continue;
+        if (I.health != 0u) {   // the state left the admissible set: stop here
+            I.steps_left = 0;
+            left[id] = 0;
+            continue;
+        }
         I.steps_left -= 1;
-        left[id] = I.steps_left;
         I.steps_done += 1;
         I.cur ^= flip;
+        I.t += I.dt;
         const unsigned long long bits = I.lambda;
         I.lambda_last = bits;
         I.lambda = 0ull;
@@ -99,6 +104,11 @@ __global__ void batch_step_end_kernel(BatchInst *tab, const int *live, const int
             const double np = double(I.order + 1);
             I.dt = I.cfl * I.hmin / (lam * np * np);
         }
+        if (I.t_final > 0.0) {   // dt_real = min(dt, t_final - t); done at t >= t_final - 1e-8 dt
+            if (I.t >= I.t_final - 1e-8 * I.dt) I.steps_left = 0;
+            else I.dt = fmin(I.dt, I.t_final - I.t);
+        }
+        left[id] = I.steps_left;
     }
 }
 

@@ -41,6 +41,7 @@ struct RhsArgs {
     int mode;
     const float *grad32;    // NS: primitive gradients, FP32-bulk form
     const double *u_rk;     // axisymmetric: the RK state r U (u holds the recovered U); else null
+    unsigned int *health;   // RK modes: OR of the state-check bits of the new state (may be null)
 };
 
 struct LiftArgs {
@@ -72,10 +73,12 @@ struct BatchInst {
     int steps_left;             // > 0: the solve advances; 0: frozen
     int steps_done;
     int cur;                    // LSRK: u[cur] holds the state at the start of the step
-    int pad;
+    unsigned int health;        // state-check bits of the RK stages (sticky); non-zero freezes the solve
     const BcDev *bcs;           // boundary conditions (boundary faces)
     unsigned long long lambda;  // max |V|+c over the current step's stages (ordered bits)
     unsigned long long lambda_last;   // ... of the last completed step
+    double t;                   // simulated time: the sum of the completed steps' dt
+    double t_final;             // > 0: end time (the last step is shortened to reach it)
 };
 // One (dim, order, physics) class of a batch: its solves and the padded
 // element prefix over them (prefix[s+1] - prefix[s] = E of slot s rounded up
@@ -120,7 +123,10 @@ cudaError_t batch_launch_lift(int dim, int order, bool vc, bool fp32, int grid, 
                               const BatchStage &st, const OpTables &T, cudaStream_t s);
 // End of a batch step: every live solve with steps left advances its counters,
 // flips its LSRK parity, (cfl > 0) takes its next dt from lambda, and writes
-// its remaining step count to left[id].
+// its remaining step count to left[id]; a solve whose state check failed
+// (health != 0) is frozen instead: steps_left = 0.  With an end time the
+// solve's time advances by the step's dt, the next dt is cut to reach t_final
+// and the solve stops there (Simulation.cpp:1007-1024).
 // FP64 budgets over the mesh (node weights w_i w_j (w_k) |J|): the integrals
 // of the nf conserved fields and of the entropy function U = -rho s / (g-1),
 // s = ln(p rho^-g); with dudt also the integrals of dudt_f and of v . dudt

@@ -30,12 +30,14 @@ inline long double legendre_ld(int n, long double x, long double *dp) {
     return p1;
 }
 
+// Fixed-size arrays only (Np <= 8): the allocation-free entry point builds
+// its tables with this function too.
 inline void build_tables(int N, OpTables &T) {
     const int Np = N + 1;
     std::memset(&T, 0, sizeof(T));
     // Gauss-Lobatto nodes/weights on [0,1]
     const long double pi = 3.14159265358979323846264338327950288L;
-    std::vector<long double> xs(Np);
+    long double xs[8];
     for (int i = 0; i < Np; ++i) {
         long double xi = -cosl(pi * i / N);
         if (i > 0 && i < N)
@@ -55,7 +57,8 @@ inline void build_tables(int N, OpTables &T) {
     T.x[0] = 0.0;
     T.x[N] = 1.0;
     // barycentric differentiation matrix
-    std::vector<double> wb(Np, 1.0);
+    double wb[8];
+    for (int i = 0; i < Np; ++i) wb[i] = 1.0;
     for (int i = 1; i < Np; ++i)
         for (int j = 0; j < i; ++j) {
             wb[j] *= (T.x[j] - T.x[i]);
@@ -77,7 +80,8 @@ inline void build_tables(int N, OpTables &T) {
     T.Dhat2[0] += 1.0 / T.w[0];
     T.Dhat2[(Np - 1) * Np + Np - 1] -= 1.0 / T.w[Np - 1];
     // 1D Vandermonde of shifted Legendre P_a(2x-1): V[l][a], inverted (Gauss-Jordan)
-    std::vector<double> V(Np * Np), I(Np * Np, 0.0);
+    double V[64], I[64];
+    for (int q = 0; q < Np * Np; ++q) I[q] = 0.0;
     for (int l = 0; l < Np; ++l) {
         double u[8], z = 2.0 * T.x[l] - 1.0;
         u[0] = 1.0;
@@ -104,6 +108,24 @@ inline void build_tables(int N, OpTables &T) {
     }
     // I = V^{-1}: I[a][l] maps nodal values (l) to mode a
     for (int q = 0; q < Np * Np; ++q) T.Vinv[q] = I[q];
+}
+
+// Text of the calling thread's last failure outside a handle (prandtl_create,
+// prandtl_rhs_noalloc), kept in a fixed thread-local buffer (no allocation);
+// prandtl_last_error(NULL) returns it.  Defined in prandtl_api.cu.
+void set_unbound_error(const char *msg);
+const char *unbound_error();
+
+// Room in a batch for one more solve of `bytes` (defined in prandtl_batch.cu).
+bool batch_has_room(prandtl_batch *b, size_t bytes);
+
+// Text for the state-check bits the RK epilogue sets (PRANDTL_HEALTH_*).
+inline std::string health_text(unsigned bits) {
+    std::string t = "the state left the admissible set:";
+    if (bits & PRANDTL_HEALTH_NONFINITE) t += " non-finite values;";
+    if (bits & PRANDTL_HEALTH_DENSITY) t += " density <= 0;";
+    if (bits & PRANDTL_HEALTH_PRESSURE) t += " pressure <= 0;";
+    return t;
 }
 
 inline void build_phys(const prandtl_config &c, int N, PhysParams &P) {

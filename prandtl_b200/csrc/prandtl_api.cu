@@ -41,6 +41,8 @@ struct prandtl_handle {
     float *d_grad32 = nullptr;                    // NS primitive gradients (FP32-bulk form)
     double *d_alpha = nullptr;
     unsigned long long *d_lambda = nullptr;
+    unsigned int *d_health = nullptr;             // sticky state-check bits of the RK stages
+    unsigned int *h_health = nullptr;             // pinned host copy of d_health
     BcDev *d_bcs = nullptr;                       // boundary conditions
     // axisymmetric form: node coordinates [2][Ndof], axis-node flags, and the
     // state U recovered from the r-weighted RK state before each RHS
@@ -63,11 +65,11 @@ struct prandtl_handle {
 
 namespace {
 
-thread_local std::string g_create_error;
+thread_local char g_unbound_error[512];
 
 prandtl_status fail(prandtl_handle *h, prandtl_status st, const std::string &msg) {
     if (h) h->err = msg;
-    else g_create_error = msg;
+    else set_unbound_error(msg.c_str());
     return st;
 }
 
@@ -95,6 +97,22 @@ prandtl_status wait_stream(prandtl_handle *h) {
         if (el > limit) return fail(h, PRANDTL_ETIMEDOUT, "wait for the handle's stream timed out");
         std::this_thread::sleep_for(std::chrono::microseconds(50));
     }
+}
+
+// Copies the sticky state-check flag to the pinned host word, waits (bounded),
+// clears the device flag and reports PRANDTL_ENONFINITE when it was set.
+prandtl_status wait_and_report_health(prandtl_handle *h) {
+    cudaError_t e = cudaMemcpyAsync(h->h_health, h->d_health, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                                    h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "D2H state check flag");
+    e = cudaMemsetAsync(h->d_health, 0, sizeof(unsigned int), h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "clear state check flag");
+    prandtl_status st = wait_stream(h);
+    if (st != PRANDTL_OK) return st;
+    const unsigned bits = *h->h_health;
+    *h->h_health = 0u;
+    if (bits) return fail(h, PRANDTL_ENONFINITE, health_text(bits));
+    return PRANDTL_OK;
 }
 
 // Event pair around one launch when profiling; returns the stop event or null.
@@ -171,6 +189,8 @@ void free_all(prandtl_handle *h) {
     cudaFree(h->d_grad32);
     cudaFree(h->d_alpha);
     cudaFree(h->d_lambda);
+    cudaFree(h->d_health);
+    if (h->h_health) cudaFreeHost(h->h_health);
     cudaFree(h->d_bcs);
     cudaFree(h->d_xy);
     cudaFree(h->d_axis);
@@ -211,7 +231,7 @@ void prandtl_config_default(prandtl_config *c) {
 
 prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config *cfg,
                               prandtl_handle **out) {
-    g_create_error.clear();
+    set_unbound_error("");
     if (!out) return fail(nullptr, PRANDTL_EINVAL, "out is NULL");
     *out = nullptr;
     if (!md || !cfg) return fail(nullptr, PRANDTL_EINVAL, "mesh or config is NULL");
@@ -258,7 +278,7 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
     cudaGetDevice(&h->device);
 
     auto bail = [&](prandtl_status st) {
-        g_create_error = h->err;
+        set_unbound_error(h->err.c_str());
         free_all(h);
         delete h;
         return st;
@@ -284,6 +304,12 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
         return bail(st);
     if ((st = dalloc(h, &h->d_alpha, (size_t)E, "alpha")) != PRANDTL_OK) return bail(st);
     if ((st = dalloc(h, &h->d_lambda, 1, "lambda")) != PRANDTL_OK) return bail(st);
+    if ((st = dalloc(h, &h->d_health, 1, "state check flag")) != PRANDTL_OK) return bail(st);
+    if ((ce = cudaMemset(h->d_health, 0, sizeof(unsigned int))) != cudaSuccess)
+        return bail(cuda_fail(h, ce, "memset state check flag"));
+    if ((ce = cudaMallocHost(&h->h_health, sizeof(unsigned int))) != cudaSuccess)
+        return bail(cuda_fail(h, ce, "pinned state check flag"));
+    *h->h_health = 0u;
     if ((st = dalloc(h, &h->d_budget, (size_t)(BUDGET_BLOCKS + 1) * 12, "budgets")) != PRANDTL_OK) return bail(st);
     const std::vector<BcDev> bcs = device_bcs(cfg, md->dim);
     if (!bcs.empty()) {
@@ -401,6 +427,7 @@ prandtl_status prandtl_step(prandtl_handle *h, double *u, double t, double dt, i
             RhsArgs a{};
             a.dt = dt;
             a.x0 = x;
+            a.health = h->d_health;
             a.mode = EPI_SSP1; a.u_out = y1;
             if ((st = run_rhs(h, x, a)) != PRANDTL_OK) break;
             a.mode = EPI_SSP2; a.u_out = y2;
@@ -424,6 +451,7 @@ prandtl_status prandtl_step(prandtl_handle *h, double *u, double t, double dt, i
             for (int k = 0; k < 5; ++k) {
                 RhsArgs a{};
                 a.mode = EPI_LSRK;
+                a.health = h->d_health;
                 a.dt = dt;
                 a.rkA = A[k];
                 a.rkB = B[k];
@@ -438,7 +466,7 @@ prandtl_status prandtl_step(prandtl_handle *h, double *u, double t, double dt, i
     if (st != PRANDTL_OK) return st;
     if (!dev) {
         CK(h, cudaMemcpyAsync(u, x, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H u");
-        st = wait_stream(h);
+        st = wait_and_report_health(h);
     }
     return st;
 }
@@ -531,7 +559,9 @@ prandtl_status prandtl_set_stream(prandtl_handle *h, void *cuda_stream) {
 prandtl_status prandtl_synchronize(prandtl_handle *h) {
     if (!h) return PRANDTL_EINVAL;
     std::lock_guard<std::mutex> lk(h->mu);
-    return wait_stream(h);
+    h->err.clear();
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    return wait_and_report_health(h);
 }
 
 long long prandtl_kernel_launches(const prandtl_handle *h) { return h ? h->launches : 0; }
@@ -584,9 +614,18 @@ prandtl_status prandtl_profile_reset(prandtl_handle *h) {
 size_t prandtl_device_bytes(const prandtl_handle *h) { return h ? h->bytes : 0; }
 
 const char *prandtl_last_error(const prandtl_handle *h) {
-    return h ? h->err.c_str() : g_create_error.c_str();
+    return h ? h->err.c_str() : unbound_error();
 }
 
 const char *prandtl_version(void) { return "prandtl_b200 0.2 (sm_100a, FP64 + FP32-bulk)"; }
 
 }   // extern "C"
+
+namespace prandtl {
+namespace host {
+void set_unbound_error(const char *msg) {
+    std::snprintf(g_unbound_error, sizeof(g_unbound_error), "%s", msg ? msg : "");
+}
+const char *unbound_error() { return g_unbound_error; }
+}   // namespace host
+}   // namespace prandtl

@@ -357,6 +357,17 @@ void free_batch(prandtl_batch *b) {
 
 }   // namespace
 
+namespace prandtl {
+namespace host {
+// Room for one more solve of `bytes` (arena range and a table slot); the
+// serving loop asks before it tries an admission.
+bool batch_has_room(prandtl_batch *b, size_t bytes) {
+    std::lock_guard<std::mutex> lk(b->mu);
+    return !b->free_ids.empty() && b->alloc.largest() >= bytes;
+}
+}   // namespace host
+}   // namespace prandtl
+
 extern "C" {
 
 void prandtl_batch_config_default(prandtl_batch_config *c) {
@@ -468,8 +479,9 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, 
     if (!b) return PRANDTL_EINVAL;
     if (!md || !cfg || !u0 || !sd || !id) return bfail(b, PRANDTL_EINVAL, "null argument");
     if (sd->nsteps < 0 || !std::isfinite(sd->dt) || (sd->nsteps > 0 && !(sd->dt > 0.0)) ||
-        !std::isfinite(sd->cfl) || (sd->cfl > 0.0 && !(sd->hmin > 0.0)))
-        return bfail(b, PRANDTL_EINVAL, "bad solve description (dt, cfl, hmin, nsteps)");
+        !std::isfinite(sd->cfl) || (sd->cfl > 0.0 && !(sd->hmin > 0.0)) || !std::isfinite(sd->t_final) ||
+        sd->t_final < 0.0)
+        return bfail(b, PRANDTL_EINVAL, "bad solve description (dt, cfl, hmin, nsteps, t_final)");
     if (!(cfg->gamma > 1.0) || !(cfg->Pr > 0.0)) return bfail(b, PRANDTL_EINVAL, "bad gamma/Pr");
     std::lock_guard<std::mutex> lk(b->mu);
     b->err.clear();
@@ -546,7 +558,9 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, 
     I.Ndof = s.Ndof;
     I.E = E;
     I.order = order;
-    I.dt = sd->dt;
+    I.dt = sd->t_final > 0.0 ? std::min(sd->dt, sd->t_final) : sd->dt;
+    I.t = 0.0;
+    I.t_final = sd->t_final > 0.0 ? sd->t_final : 0.0;
     I.cfl = sd->cfl > 0.0 ? sd->cfl : 0.0;
     I.hmin = sd->hmin;
     I.steps_left = sd->nsteps;
@@ -646,7 +660,23 @@ prandtl_status prandtl_batch_query(prandtl_batch *b, int id, int *steps_left, in
         std::memcpy(&v, &I.lambda_last, sizeof(v));
         *lambda_max = v;
     }
+    if (I.health) return bfail(b, PRANDTL_ENONFINITE, "solve " + std::to_string(id) + ": " + health_text(I.health));
     return PRANDTL_OK;
+}
+
+prandtl_status prandtl_batch_time(prandtl_batch *b, int id, double *t) {
+    if (!b) return PRANDTL_EINVAL;
+    if (!t) return bfail(b, PRANDTL_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (id < 0 || id >= b->cap || !b->solves[id].used) return bfail(b, PRANDTL_EINVAL, "unknown solve id");
+    BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
+    double v = 0.0;
+    BCK(b, cudaMemcpyAsync(&v, reinterpret_cast<char *>(b->d_tab + id) + offsetof(BatchInst, t), sizeof(v),
+                           cudaMemcpyDeviceToHost, b->stream),
+        "D2H time");
+    prandtl_status st = bwait(b);
+    if (st == PRANDTL_OK) *t = v;
+    return st;
 }
 
 prandtl_status prandtl_batch_read(prandtl_batch *b, int id, double *u, int ptr_flags) {
@@ -656,21 +686,25 @@ prandtl_status prandtl_batch_read(prandtl_batch *b, int id, double *u, int ptr_f
     if (id < 0 || id >= b->cap || !b->solves[id].used) return bfail(b, PRANDTL_EINVAL, "unknown solve id");
     BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
     const Solve &s = b->solves[id];
-    int cur = 0;
-    if (b->cfg.scheme == PRANDTL_LSRK45) {
-        BCK(b, cudaMemcpyAsync(&cur, reinterpret_cast<char *>(b->d_tab + id) + offsetof(BatchInst, cur), sizeof(int),
-                               cudaMemcpyDeviceToHost, b->stream),
-            "D2H parity");
-        prandtl_status st = bwait(b);
-        if (st != PRANDTL_OK) return st;
-    }
+    // the LSRK parity and the state-check bits sit next to each other in the record
+    static_assert(offsetof(BatchInst, health) == offsetof(BatchInst, cur) + sizeof(int), "record layout");
+    int words[2] = {0, 0};
+    BCK(b, cudaMemcpyAsync(words, reinterpret_cast<char *>(b->d_tab + id) + offsetof(BatchInst, cur), sizeof(words),
+                           cudaMemcpyDeviceToHost, b->stream),
+        "D2H parity and state check");
+    prandtl_status st = bwait(b);
+    if (st != PRANDTL_OK) return st;
+    const int cur = b->cfg.scheme == PRANDTL_LSRK45 ? words[0] : 0;
     const char *src = b->arena + s.off + s.L.u[cur & 1];
     const size_t S = (size_t)s.nf * s.Ndof * sizeof(double);
     BCK(b, cudaMemcpyAsync(u, src, S,
                            (ptr_flags & PRANDTL_PTR_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                            b->stream),
         "copy state");
-    return bwait(b);
+    st = bwait(b);
+    if (st == PRANDTL_OK && words[1] != 0)
+        return bfail(b, PRANDTL_ENONFINITE, "solve " + std::to_string(id) + ": " + health_text((unsigned)words[1]));
+    return st;
 }
 
 prandtl_status prandtl_batch_budgets(prandtl_batch *b, int id, double *out) {

@@ -7,8 +7,13 @@
 //   -> wait -> copy out and retire the solves that finished,
 // so requests that arrive while others run join at the next tick and share
 // their stage launches.  Requests larger than the whole arena are rejected at
-// submit time; a request that does not fit yet waits at the head of the queue
-// until retirements free room (first come, first served, no overtaking).
+// submit time.  Admission scans the queue in arrival order: a request that
+// does not fit yet stays queued and later, smaller requests may be admitted
+// past it, but each queued request can be overtaken at most
+// kMaxOvertakes times; after that nothing behind it is admitted until it fits
+// (so it cannot starve).  A solve that fails its state check (a non-finite
+// value, density or pressure <= 0) stops alone: its request completes with
+// PRANDTL_ENONFINITE and the others go on.
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -22,9 +27,18 @@
 
 #include "../../include/prandtl_b200.h"
 
+namespace prandtl {
+namespace host {
+bool batch_has_room(prandtl_batch *b, size_t bytes);
+}
+}   // namespace prandtl
+
 namespace {
 
 using Clock = std::chrono::steady_clock;
+
+// Admissions past one queued request before it must go next.
+constexpr int kMaxOvertakes = 64;
 
 struct Request {
     long long ticket = 0;
@@ -36,8 +50,11 @@ struct Request {
     double *u_out = nullptr;
     Clock::time_point t_submit, t_done;
     int state = 0;              // 0 queued, 1 resident, 2 done, 3 failed
+    prandtl_status status = PRANDTL_OK;   // of a failed request
     int batch_id = -1;
     double dofs = 0;            // nodes * fields
+    size_t need = 0;            // arena bytes (prandtl_batch_footprint)
+    int overtaken = 0;          // admissions past this request while it waited
     std::string err;
 };
 
@@ -63,27 +80,47 @@ struct prandtl_server {
 
 namespace {
 
-// Admit in arrival order; stops at the first request that does not fit yet.
+// Admit in arrival order, letting requests that fit pass queued ones that do
+// not fit yet, within the overtaking bound.
 void admit(prandtl_server *s, std::unique_lock<std::mutex> &lk) {
-    while (!s->queue.empty()) {
-        Request *r = s->reqs.at(s->queue.front()).get();
-        lk.unlock();
+    std::vector<Request *> waiting;   // skipped so far in this scan
+    for (size_t q = 0; q < s->queue.size();) {
+        Request *r = s->reqs.at(s->queue[q]).get();
+        const bool nothing_resident = s->resident.empty();
+        bool try_add = nothing_resident;
+        if (!try_add) {
+            lk.unlock();
+            try_add = prandtl::host::batch_has_room(s->b, r->need);
+            lk.lock();
+        }
+        prandtl_status st = PRANDTL_ENOMEM;
+        std::string msg;
         int id = -1;
-        const prandtl_status st = prandtl_batch_add(s->b, &r->md, &r->cfg, r->u0.data(), PRANDTL_PTR_HOST,
-                                                    &r->solve, &id);
-        const std::string msg = st == PRANDTL_OK ? std::string() : prandtl_batch_last_error(s->b);
-        lk.lock();
-        // no room yet: wait for retirements, unless nothing is resident (then it never fits)
-        if (st == PRANDTL_ENOMEM && !s->resident.empty()) return;
-        s->queue.pop_front();
+        if (try_add) {
+            lk.unlock();
+            st = prandtl_batch_add(s->b, &r->md, &r->cfg, r->u0.data(), PRANDTL_PTR_HOST, &r->solve, &id);
+            if (st != PRANDTL_OK) msg = prandtl_batch_last_error(s->b);
+            lk.lock();
+        }
+        if (st == PRANDTL_ENOMEM && !s->resident.empty()) {
+            // no room yet: it waits; nothing behind it may pass once it has
+            // been overtaken kMaxOvertakes times
+            if (r->overtaken >= kMaxOvertakes) return;
+            waiting.push_back(r);
+            ++q;
+            continue;
+        }
+        s->queue.erase(s->queue.begin() + (long)q);
         if (st != PRANDTL_OK) {
             r->state = 3;
+            r->status = st;
             r->err = msg;
             r->t_done = Clock::now();
             s->stats.rejected++;
             s->cv_done.notify_all();
             continue;
         }
+        for (Request *w : waiting) w->overtaken++;
         r->state = 1;
         r->batch_id = id;
         std::vector<double>().swap(r->u0);
@@ -143,6 +180,7 @@ void worker_loop(prandtl_server *s) {
             for (auto &kv : s->resident) {
                 Request *r = s->reqs.at(kv.second).get();
                 r->state = 3;
+                r->status = st;
                 r->err = berr;
                 r->t_done = Clock::now();
             }
@@ -150,6 +188,7 @@ void worker_loop(prandtl_server *s) {
             for (long long t : s->queue) {
                 Request *r = s->reqs.at(t).get();
                 r->state = 3;
+                r->status = st;
                 r->err = berr;
                 r->t_done = Clock::now();
             }
@@ -171,7 +210,9 @@ void worker_loop(prandtl_server *s) {
                 s->stats.dof_updates += r->dofs * r->solve.nsteps;
             } else {
                 r->state = 3;
-                r->err = "read of the final state failed";
+                r->status = d.second;
+                r->err = d.second == PRANDTL_ENONFINITE ? "the solve failed its state check (stopped early)"
+                                                        : "read of the final state failed";
             }
         }
         s->stats.resident = (int)s->resident.size();
@@ -232,6 +273,7 @@ prandtl_status prandtl_serve_submit(prandtl_server *s, const prandtl_mesh_desc *
     r->solve = *solve;
     r->u_out = u_out;
     r->dofs = (double)S;
+    r->need = need;
     r->t_submit = Clock::now();
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) return PRANDTL_ECUDA;
@@ -256,7 +298,7 @@ prandtl_status prandtl_serve_poll(prandtl_server *s, long long ticket, int *done
     const Request &r = *it->second;
     *done = r.state >= 2 ? 1 : 0;
     if (seconds) *seconds = r.state >= 2 ? std::chrono::duration<double>(r.t_done - r.t_submit).count() : -1.0;
-    if (r.state == 3) return PRANDTL_ECUDA;
+    if (r.state == 3) return r.status != PRANDTL_OK ? r.status : PRANDTL_ECUDA;
     return PRANDTL_OK;
 }
 
@@ -269,7 +311,8 @@ prandtl_status prandtl_serve_wait(prandtl_server *s, long long ticket, double ti
     const auto limit = std::chrono::duration<double>(timeout_s > 0 ? timeout_s : s->timeout_s);
     if (!s->cv_done.wait_for(lk, limit, [&] { return r->state >= 2; })) return PRANDTL_ETIMEDOUT;
     if (seconds) *seconds = std::chrono::duration<double>(r->t_done - r->t_submit).count();
-    return r->state == 2 ? PRANDTL_OK : PRANDTL_ECUDA;
+    if (r->state == 2) return PRANDTL_OK;
+    return r->status != PRANDTL_OK ? r->status : PRANDTL_ECUDA;
 }
 
 prandtl_status prandtl_serve_stats_get(prandtl_server *s, prandtl_serve_stats *st) {

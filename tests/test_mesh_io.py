@@ -19,7 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 MESHES = os.path.join(HERE, "golden", "meshes")
 SHEAR2 = np.array([[1.0, 0.2], [0.0, 1.1]])
 SHEAR3 = np.array([[1.0, 0.1, 0.0], [0.0, 1.05, 0.15], [0.05, 0.0, 0.95]])
-REF_CASES = "/root/reference/TestCases"
+# the reference checkout (REF, as for oracle/ref_harness/build_ref.sh)
+REF_CASES = os.path.join(os.environ.get("REF", "/root/reference"), "TestCases")
 
 
 def smooth_state(mesh):

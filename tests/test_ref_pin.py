@@ -40,7 +40,7 @@ def test_oracle_matches_reference_golden(oracle_mod, case):
 
 def _ref(oracle_mod):
     if not oracle_mod.ref_available():
-        if not os.path.isdir("/root/reference/src"):
+        if not os.path.isdir(os.path.join(os.environ.get("REF", "/root/reference"), "src")):
             pytest.skip("reference sources not present on this host")
         oracle_mod.build_ref()
     return oracle_mod
