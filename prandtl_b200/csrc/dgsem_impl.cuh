@@ -346,9 +346,17 @@ struct RhsLayout {
 };
 
 // Synchronise the GS lanes of lane group `gid` (its index within the CTA).
+// A group narrower than a warp synchronises its own lanes only: groups of one
+// warp take different paths (one element's subcell FV phase runs while its
+// warp-mate's is skipped, and an inactive group returns early), so a
+// full-warp mask would pair barriers of different groups and, once a group
+// has exited, no longer order the other group's shared-memory accesses.
 template <int GS>
 __device__ __forceinline__ void group_sync(int gid) {
-    if constexpr (GS <= 32) {
+    if constexpr (GS < 32) {
+        const unsigned base = (threadIdx.x & 31u) & ~unsigned(GS - 1);
+        __syncwarp(((1u << GS) - 1u) << base);
+    } else if constexpr (GS == 32) {
         __syncwarp();
     } else {
         asm volatile("bar.sync %0, %1;" ::"r"(1 + gid), "n"(GS) : "memory");

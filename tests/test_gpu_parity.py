@@ -184,3 +184,41 @@ def test_rhs_matches_reference_golden():
         err = normalized_error(d, gold[f"{name}/dudt"], mesh.num_fields)
         assert err <= RHS_TOL, f"{name}: {err:.3e}"
         np.testing.assert_allclose(op.alpha(), gold[f"{name}/alpha"], rtol=0, atol=1e-12)
+
+
+def _checkerboard_state(mesh, seed):
+    """Smooth flow in even elements, nodal noise in odd ones: the two 16-lane
+    groups of a warp (elements 2k, 2k+1 of the 2D N = 2, 3 meshes) take the
+    subcell FV branch in one element and skip it in the other.  (At N = 1 the
+    indicator blends every element, so no warp diverges there.)"""
+    nf, nd = mesh.num_fields, mesh.nodes_per_elem
+    u = _state(mesh, seed=seed, amp=0.0).reshape(nf, -1).copy()
+    rng = np.random.default_rng(seed)
+    e = np.repeat(np.arange(mesh.num_elements), nd)
+    rough = (e % 2) == 1
+    u[0, rough] *= 1.0 + 0.4 * rng.uniform(-1, 1, rough.sum())
+    u[-1, rough] *= 1.0 + 0.4 * rng.uniform(-1, 1, rough.sum())
+    return u.reshape(-1)
+
+
+@pytest.mark.parametrize("dim,n,order", [(2, 8, 3), (2, 8, 2)])
+def test_blending_in_alternate_elements_of_a_warp(oracle_mod, dim, n, order):
+    """Regression: lane groups narrower than a warp synchronise only their own
+    lanes, so an element that runs the subcell FV phase while its warp-mate
+    skips it (and exits) still orders its shared-memory accesses.  Repeated
+    evaluations on states where every other element is blended must match the
+    oracle every time."""
+    mesh = periodic_box(dim, n, order, 0.0, 1.0)
+    kw = dict(parabolic=0, blending=1)
+    op = _op(mesh, quirks="reference", **kw)
+    for seed in range(6):
+        u = _checkerboard_state(mesh, seed)
+        ref = oracle_mod.Oracle(mesh, quirks=0, **kw).rhs(u, want_alpha=True)
+        alpha = ref["alpha"]
+        assert (alpha[1::2] > 0).all() and (alpha[0::2] == 0).all()
+        d = np.empty_like(u)
+        for _ in range(5):
+            op.Mult(u, d)
+            assert normalized_error(d, ref["dudt"], mesh.num_fields) <= RHS_TOL
+            np.testing.assert_allclose(op.alpha(), alpha, rtol=0, atol=1e-12)
+    op.close()
