@@ -649,7 +649,7 @@ __device__ __forceinline__ void boundary_flux(const BcDev &bc, const double *s_i
 // rho <= 0, bit 2 p <= 0 (the last two only where `positivity`: the
 // axisymmetric RK state r U vanishes on the axis).
 template <int DIM>
-__device__ __forceinline__ unsigned state_health(const double *s, double gm1, bool positivity) {
+__device__ __forceinline__ unsigned state_health(const double *s, bool positivity) {
     constexpr int NF = DIM + 2;
     bool finite = true;
 #pragma unroll
@@ -659,8 +659,9 @@ __device__ __forceinline__ unsigned state_health(const double *s, double gm1, bo
         double mm = 0.0;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) mm += s[1 + d] * s[1 + d];
+        // p = (gamma - 1)(E - |m|^2 / (2 rho)) > 0  <=>  2 rho E - |m|^2 > 0 for rho > 0
         if (!(s[0] > 0.0)) bad |= 2u;
-        else if (!(gm1 * (s[NF - 1] - 0.5 * mm / s[0]) > 0.0)) bad |= 4u;
+        else if (!(2.0 * s[0] * s[NF - 1] - mm > 0.0)) bad |= 4u;
     }
     return bad;
 }
@@ -1405,7 +1406,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
             // values anywhere, and (planar form) rho <= 0 or p <= 0; one atomic
             // per violating node, none on healthy states
             if (a.health) {
-                const unsigned bad = state_health<DIM>(nv, gm1, rad == nullptr);
+                const unsigned bad = state_health<DIM>(nv, rad == nullptr);
                 if (bad) atomicOr(a.health, bad);
             }
         }

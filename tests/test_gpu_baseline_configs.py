@@ -196,3 +196,37 @@ def test_c3_kh256_to_t3_stays_admissible(precision):
     op.Mult(u, d)
     assert (op.alpha() > 0).sum() > 1000
     op.close()
+
+
+def test_kh128_trajectory_matches_oracle_through_blending_onset():
+    """8000 SSP-RK3 steps of the Kelvin-Helmholtz flow on 128^2 elements at a
+    fixed dt (t ~ 1.38; the indicator starts blending near step 7000), against
+    the oracle's trajectory (tests/golden/kh128_trajectory.npz, made by
+    tests/golden/make_kh_trajectory.py): sampled DOFs within 1e-11 of the field
+    maximum, full-state L2 norms within 1e-12, the same number of blended
+    elements at the end."""
+    import os
+    torch = pytest.importorskip("torch")
+    golden = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "kh128_trajectory.npz"))
+    mesh, u0, _ = cases.make_case("kh", 128, 3)
+    dt = float(golden["dt"])
+    assert dt == fixed_dt(mesh, u0, 0.4)
+    idx = golden["index"]
+    op = DGSEMOperator(mesh, **KH)
+    ut = torch.from_numpy(u0).cuda()
+    done = 0
+    for s in (4000, 7000, 8000):
+        op.Step(ut, dt, scheme="RK3SSP", nsteps=s - done)
+        op.synchronize()
+        done = s
+        u = ut.cpu().numpy()
+        ref = golden[f"u{s}"]
+        fmax = np.abs(u.reshape(4, -1)).max(axis=1)
+        field = idx // mesh.ndof
+        assert (np.abs(u[idx] - ref) / fmax[field]).max() <= 1e-11, s
+        norms = np.linalg.norm(u.reshape(4, -1), axis=1)
+        np.testing.assert_allclose(norms, golden[f"norm{s}"], rtol=1e-12, atol=0)
+    d = np.empty_like(u)
+    op.Mult(u, d)
+    assert int((op.alpha() > 0).sum()) == int(golden["blended8000"])
+    op.close()
