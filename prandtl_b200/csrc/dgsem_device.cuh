@@ -178,6 +178,41 @@ __device__ __forceinline__ void log_mean(Real x, Real y, Real rx, Real &mean, Re
     }
 }
 
+// ---- FP32-bulk form: two two-point fluxes at once on packed pairs of FP32
+// lanes (the paired FADD2 / FMUL2 / FFMA2 instructions of sm_100: one issue
+// slot for both).  The arithmetic is that of log_mean / volume_flux below for
+// Real = float, applied to (x0, y0) and (x1, y1) side by side.
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// Logarithmic means of (x.x, y.x) and (x.y, y.y) with their inverses and
+// 1/(x+y): the series branch packed when both lanes take it, else each lane
+// through the scalar log_mean.
+__device__ __forceinline__ void log_mean2(float2 x, float2 y, float2 rx, float2 &mean, float2 &inv_mean, float2 &rs) {
+    const float2 s = add2(x, y), d = sub2(y, x);
+    rs = f2(rcp(s.x), rcp(s.y));
+    const float2 f = mul2(d, rs);
+    const float2 u = mul2(f, f);
+    if (u.x < 0.04f && u.y < 0.04f) {
+        const float2 a = mul2(u, fma2(u, fma2(u, fma2(u, fma2(u, f2(1.0f / 11), f2(1.0f / 9)), f2(1.0f / 7)),
+                                               f2(1.0f / 5)), f2(1.0f / 3)));
+        const float2 one_a = add2(f2(1.0f), a);
+        inv_mean = mul2(mul2(f2(2.0f), rs), one_a);
+        mean = mul2(mul2(f2(0.5f), s), f2(rcp(one_a.x), rcp(one_a.y)));
+        return;
+    }
+    float m0, i0, r0, m1, i1, r1;
+    log_mean<float>(x.x, y.x, rx.x, m0, i0, r0);
+    log_mean<float>(x.y, y.y, rx.y, m1, i1, r1);
+    mean = f2(m0, m1);
+    inv_mean = f2(i0, i1);
+    rs = f2(r0, r1);
+}
+
 // Pressure term of the momentum flux.  FP64: p_hat.  FP32-bulk form: the
 // element's constant reference pressure is left out, p_hat - p_ref =
 // (beta1 dp1 + beta2 dp2) / (beta1 + beta2) with dp = p - p_ref formed in FP64
@@ -219,6 +254,43 @@ __device__ __forceinline__ void volume_flux(const Prim<DIM, Real> &a, const Prim
 #pragma unroll
     for (int d = 0; d < DIM; ++d) F[1 + d] = F0 * vm[d] + p_mom * m[d];
     F[NF - 1] = F0 * h;
+}
+
+// volume_flux (FP32-bulk form) of the pairs (a0, b0) and (a1, b1), each along
+// the metric row m, on packed lanes.
+template <int DIM>
+__device__ __forceinline__ void volume_flux2(const Prim<DIM, float> &a0, const Prim<DIM, float> &b0,
+                                             const Prim<DIM, float> &a1, const Prim<DIM, float> &b1,
+                                             const float *m, float gammaM1Inverse, float *F0, float *F1) {
+    constexpr int NF = DIM + 2;
+    const float2 ar = f2(a0.rho, a1.rho), br = f2(b0.rho, b1.rho);
+    const float2 ab = f2(a0.beta, a1.beta), bb = f2(b0.beta, b1.beta);
+    float2 rho_ln, irho_ln, rs_rho, beta_ln, ibeta_ln, rs_beta;
+    log_mean2(ar, br, f2(a0.rrho, a1.rrho), rho_ln, irho_ln, rs_rho);
+    log_mean2(ab, bb, f2(a0.rbeta, a1.rbeta), beta_ln, ibeta_ln, rs_beta);
+    float2 vm[DIM], Vn = f2(0.0f), h = mul2(f2(-0.25f), add2(f2(a0.vsq, a1.vsq), f2(b0.vsq, b1.vsq)));
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        vm[d] = mul2(f2(0.5f), add2(f2(a0.v[d], a1.v[d]), f2(b0.v[d], b1.v[d])));
+        Vn = fma2(vm[d], f2(m[d]), Vn);
+        h = fma2(vm[d], vm[d], h);
+    }
+    const float2 p_hat = mul2(mul2(f2(0.5f), add2(ar, br)), rs_beta);
+    h = add2(h, fma2(mul2(f2(0.5f), f2(gammaM1Inverse)), ibeta_ln, mul2(p_hat, irho_ln)));
+    const float2 Fm = mul2(rho_ln, Vn);
+    // momentum_pressure (FP32): (beta1 dp1 + beta2 dp2) / (beta1 + beta2)
+    const float2 p_mom = mul2(fma2(ab, f2(a0.dp, a1.dp), mul2(bb, f2(b0.dp, b1.dp))), rs_beta);
+    F0[0] = Fm.x;
+    F1[0] = Fm.y;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        const float2 Fd = fma2(Fm, vm[d], mul2(p_mom, f2(m[d])));
+        F0[1 + d] = Fd.x;
+        F1[1 + d] = Fd.y;
+    }
+    const float2 Fe = mul2(Fm, h);
+    F0[NF - 1] = Fe.x;
+    F1[NF - 1] = Fe.y;
 }
 
 // ChandrashekarFlux.cpp:85-161: entropy-conservative flux minus

@@ -298,11 +298,11 @@ struct RhsLayout {
     static constexpr int BUF = cmax(cmax(NPD, S::NFI), cmax(NID, (5 * ND + NF - 1) / NF)) * NF;
     static constexpr int K = hoisted_count<DIM, Real>();
     // per-element shared memory, in Real units: the hoisted primitives and the
-    // work buffer (BODY, padded to 16 bytes), then the element's neighbour-table
-    // entries (2 DIM int4), and the whole a multiple of 4 words so every
-    // element's area stays 16-byte aligned
+    // work buffer (BODY, padded to 16 bytes), then (FP64) the element's
+    // neighbour-table entries (2 DIM int4), and the whole a multiple of 4 words
+    // so every element's area stays 16-byte aligned
     static constexpr int BODY = (K * ND + cmax(BUF, NS ? DIM * NF * ND : 0) + 3) / 4 * 4;
-    static constexpr int NBR_REALS = 2 * DIM * 16 / (int)sizeof(Real);
+    static constexpr int NBR_REALS = sizeof(Real) == 8 ? 2 * DIM * 16 / (int)sizeof(Real) : 0;
     static constexpr int PER_ELEM = (BODY + NBR_REALS + 3) / 4 * 4;
     static constexpr bool F64 = sizeof(Real) == 8;
     // (the Navier-Stokes form with contravariant viscous fluxes needs fewer
@@ -717,14 +717,19 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
         }
     }
 
-    // ---- own nodes: hoisted primitives (formed in FP64); largest |V|+c.  The
-    //      element's neighbour-table entries are loaded with the own state and
-    //      kept in shared memory, so the face phase's neighbour-trace loads do
-    //      not wait on a table load first.
+    // ---- own nodes: hoisted primitives (formed in FP64); largest |V|+c.  FP64:
+    //      the element's neighbour-table entries are loaded with the own state
+    //      and kept in shared memory, so the face phase's neighbour-trace loads
+    //      do not wait on a table load first (C2 RHS -0.6 %).  FP32: the face
+    //      phase loads them itself; holding the entry across the hoisting
+    //      raised the N=4 kernels' spills (168-register budget: 12 -> 144 B)
+    //      and their time by 11-40 %.
+    constexpr bool NBR_SMEM = LY::F64;
     int4 *sNbr = reinterpret_cast<int4 *>(sH + LY::BODY);
     double lam = 0.0;
     {
-        const int4 tn = li < 2 * DIM ? __ldg(a.nbr + (long long)e * (2 * DIM) + li) : make_int4(0, 0, 0, 0);
+        const int4 tn = NBR_SMEM && li < 2 * DIM ? __ldg(a.nbr + (long long)e * (2 * DIM) + li)
+                                                 : make_int4(0, 0, 0, 0);
         double st[NPL][NF];   // every load in flight before the first use
 #pragma unroll
         for (int k = 0; k < NPL; ++k) {
@@ -747,7 +752,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 }
             }
         }
-        if (li < 2 * DIM) sNbr[li] = tn;
+        if (NBR_SMEM && li < 2 * DIM) sNbr[li] = tn;
     }
     if (a.lambda) {
         double v = active ? lam : 0.0;
@@ -943,8 +948,30 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 if (i < NP - 1 && useG && !gzero)
                     volume_flux<DIM, Real>(qi, load_prim<DIM, ND, Real>(sH, ln % NP + (NP - 1) * NP + i * NP * NP),
                                            mg, gm1i, G);
+                // FP32: partners l, l+1 on packed lanes (volume_flux2)
+                constexpr int LSTEP = LY::F64 ? 1 : 2;
 #pragma unroll
-                for (int l = i + 1; l < NP; ++l) {
+                for (int l = i + 1; l < NP; l += LSTEP) {
+                    if constexpr (!LY::F64) {
+                        if (l + 1 < NP) {
+                            Real F[NF], F1[NF];
+                            volume_flux2<DIM>(qi, load_prim<DIM, ND, Real>(sH, base + l * stride), qi,
+                                              load_prim<DIM, ND, Real>(sH, base + (l + 1) * stride), mt, gm1i, F, F1);
+                            const Real dil = sDh2[i * NP + l], dli = sDh2[l * NP + i];
+                            const Real dil1 = sDh2[i * NP + l + 1], dl1i = sDh2[(l + 1) * NP + i];
+#pragma unroll
+                            for (int f = 0; f < NF; ++f) {
+                                al[i][f] += dil * F[f];
+                                al[l][f] += dli * (useG ? G[f] : F[f]);
+                            }
+#pragma unroll
+                            for (int f = 0; f < NF; ++f) {
+                                al[i][f] += dil1 * F1[f];
+                                al[l + 1][f] += dl1i * (useG ? G[f] : F1[f]);
+                            }
+                            continue;
+                        }
+                    }
                     Real F[NF];
                     volume_flux<DIM, Real>(qi, load_prim<DIM, ND, Real>(sH, base + l * stride), mt, gm1i, F);
                     const Real dil = sDh2[i * NP + l], dli = sDh2[l * NP + i];
@@ -1163,7 +1190,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
     auto face_load = [&](int it, FaceIn &x) {
         const int lf = it / NFN, fa = it - lf * NFN;
         const long long go = (long long)e * ND + face_node<DIM, NP>(lf, fa);
-        x.t = sNbr[lf];
+        x.t = NBR_SMEM ? sNbr[lf] : __ldg(a.nbr + (long long)e * (2 * DIM) + lf);
         const long long gs = x.t.x < 0 ? go : (long long)x.t.x * ND + face_node<DIM, NP>(x.t.y, fa);
 #pragma unroll
         for (int f = 0; f < NF; ++f) x.s[f] = __ldg(a.u + f * Ndof + gs);
