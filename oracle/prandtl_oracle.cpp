@@ -422,6 +422,8 @@ struct Ctx {
     int dim, N, Np, nd, nf, E, F;
     long Ndof;
     const double *adj, *detj, *fnor;
+    const double *nadj, *ndetj, *fnn;   // per node / face node (multilinear elements), or null
+    int nfn;                            // nodes per face
     const int *faces;
     Phys P;
     int parabolic, blending, quirks, dissipation;
@@ -440,6 +442,12 @@ struct Ctx {
     int ny() const { return dim > 1 ? Np : 1; }
     int nz() const { return dim > 2 ? Np : 1; }
     const double *A(int e) const { return adj + (long)e * dim * dim; }
+    // the transformation at node n of element e (Tr.SetIntPoint + AdjugateJacobian /
+    // Weight) and the scaled normal at face node a of face fc (CalcOrtho at the
+    // face point); affine meshes have one value per element / face
+    const double *An(int e, int n) const { return nadj ? nadj + ((long)e * nd + n) * dim * dim : A(e); }
+    double Jn(int e, int n) const { return ndetj ? ndetj[(long)e * nd + n] : detj[e]; }
+    const double *Nf(int fc, int a) const { return fnn ? fnn + ((long)fc * nfn + a) * dim : fnor + (long)fc * dim; }
 };
 
 void setup(Ctx &X, const oracle_mesh *m, const oracle_config *c) {
@@ -455,6 +463,10 @@ void setup(Ctx &X, const oracle_mesh *m, const oracle_config *c) {
     X.adj = m->elem_adj;
     X.detj = m->elem_detj;
     X.fnor = m->face_nor;
+    X.nadj = m->node_adj;
+    X.ndetj = m->node_detj;
+    X.fnn = m->face_node_nor;
+    X.nfn = (X.dim == 2) ? X.Np : X.Np * X.Np;
     X.faces = m->face_elems;
     X.P.gamma = c->gamma;
     X.P.gammaM1 = c->gamma - 1.0;
@@ -830,17 +842,21 @@ double element_alpha(const Ctx &X, const double *el) {
 }
 
 // ----------------------------------------------------------- subcell FV
-// DGSEMIntegrator.cpp:1199-1304: subcell interface normal for direction dir
-// at interface index i (0..Np) on an affine element.
-void subcell_normal(const Ctx &X, int e, int dir, int i, double *nor) {
+// DGSEMIntegrator.cpp:1199-1304: subcell interface normal for direction dir at
+// interface index i (0..Np) of the line whose nodes are base + m * stride:
+// Ja_dir at the line's first node plus sum_{l<i} w_l sum_m D(l,m) Ja_dir(node m)
+// (on an affine element the sums vanish and the normal is Ja_dir).
+void subcell_normal(const Ctx &X, int e, int dir, int base, int stride, int i, double *nor) {
     const int dim = X.dim, Np = X.Np;
-    const double *Ja = X.A(e) + dir * dim;
+    const double *Ja0 = X.An(e, base) + dir * dim;
     double tmp[3];
-    for (int c = 0; c < dim; ++c) nor[c] = Ja[c];
+    for (int c = 0; c < dim; ++c) nor[c] = Ja0[c];
     for (int l = 0; l < i; ++l) {
         for (int c = 0; c < dim; ++c) tmp[c] = 0.0;
-        for (int m = 0; m < Np; ++m)
+        for (int m = 0; m < Np; ++m) {
+            const double *Ja = X.An(e, base + m * stride) + dir * dim;
             for (int c = 0; c < dim; ++c) tmp[c] += Ja[c] * X.D[l * Np + m];
+        }
         for (int c = 0; c < dim; ++c) tmp[c] *= X.w[l];
         for (int c = 0; c < dim; ++c) nor[c] += tmp[c];
     }
@@ -849,7 +865,6 @@ void subcell_normal(const Ctx &X, int e, int dir, int i, double *nor) {
 // DGSEMIntegrator.cpp:972-1196
 void fv_fluxes(const Ctx &X, int e, const double *el, double alpha, double *el_dudt) {
     const int nf = X.nf, Np = X.Np;
-    const double J = X.detj[e];
     double s1[5], s2[5], nor[3], flux[5], dU[5];
     auto line = [&](int dir, int base, int stride, bool set) {
         for (int f = 0; f < nf; ++f) dU[f] = 0.0;
@@ -858,14 +873,14 @@ void fv_fluxes(const Ctx &X, int e, const double *el, double alpha, double *el_d
         for (int i = 0; i < Np - 1; ++i) {
             int id2 = id1 + stride;
             for (int f = 0; f < nf; ++f) s2[f] = el[id2 * nf + f];
-            subcell_normal(X, e, dir, i + 1, nor);
+            subcell_normal(X, e, dir, base, stride, i + 1, nor);
             face_flux(X.dim, X.P.gamma, X.quirks, 1, s1, s2, nor, flux);
             if (X.axi) {   // DGSEMIntegrator.cpp:979-1031: times r at the nodes' reference midpoint
                 const double rh = 0.5 * (X.r((long)e * X.nd + id1) + X.r((long)e * X.nd + id2));
                 for (int f = 0; f < nf; ++f) flux[f] *= rh;
             }
             for (int f = 0; f < nf; ++f) dU[f] -= flux[f];
-            const double m = 1.0 / (J * X.w[i]);
+            const double m = 1.0 / (X.Jn(e, id1) * X.w[i]);   // Tr.Weight() at id1
             for (int f = 0; f < nf; ++f) dU[f] *= m;
             for (int f = 0; f < nf; ++f) {
                 if (set) el_dudt[id1 * nf + f] = dU[f];
@@ -874,7 +889,7 @@ void fv_fluxes(const Ctx &X, int e, const double *el, double alpha, double *el_d
             for (int f = 0; f < nf; ++f) { dU[f] = flux[f]; s1[f] = s2[f]; }
             id1 = id2;
         }
-        const double m = 1.0 / (J * X.w[Np - 1]);
+        const double m = 1.0 / (X.Jn(e, id1) * X.w[Np - 1]);
         for (int f = 0; f < nf; ++f) dU[f] *= m;
         for (int f = 0; f < nf; ++f) {
             if (set) el_dudt[id1 * nf + f] = dU[f];
@@ -902,8 +917,6 @@ void element_volume(const Ctx &X, int e, const double *el, const double *gq, dou
     const bool ns = X.parabolic != 0;
     for (int n = 0; n < nd * nf; ++n) el_dudt[n] = 0.0;
     if (X.blending) fv_fluxes(X, e, el, alpha, el_dudt);
-    const double *adj = X.A(e);
-    const double J = X.detj[e];
     // F/G/H_inviscid(node)(f, l): [node][f][l]
     std::vector<double> Fi(nd * nf * Np, 0.0), Gi(nd * nf * Np, 0.0), Hi(nd * nf * Np, 0.0);
     std::vector<double> Fv(nf * nd, 0.0), Gv(nf * nd, 0.0), Hv(nf * nd, 0.0);   // [f][node]
@@ -915,6 +928,7 @@ void element_volume(const Ctx &X, int e, const double *el, const double *gq, dou
         const int idq1 = nd - 1;   // Q1: stale member id1 == Np^d - 1
         for (int i = 0; i < nd; ++i) {
             double state[5], fv[15];
+            const double *adj = X.An(e, i);   // Tr.SetIntPoint(ip(i)), AdjugateJacobian
             const int src = (X.quirks == 0) ? idq1 : i;
             for (int f = 0; f < nf; ++f) state[f] = el[src * nf + f];
             const double *dqx = gq + (0 * nd + i) * nf;
@@ -930,7 +944,8 @@ void element_volume(const Ctx &X, int e, const double *el, const double *gq, dou
                 }
         }
     }
-    const double *m0 = adj + 0 * dim, *m1r = adj + 1 * dim, *m2r = (dim > 2) ? adj + 2 * dim : nullptr;
+    // metric row r at node n: adj1 / adj2 .GetRow(r) of the pair's nodes (ComputeMean in volume_flux)
+    auto mrow = [&](int n, int r) { return X.An(e, n) + r * dim; };
     double f[5], g[5], h[5], s1[5], s2[5], dUi[5], dUv[5];
     for (int k = 0; k < X.nz(); ++k)
         for (int j = 0; j < X.ny(); ++j)
@@ -942,7 +957,7 @@ void element_volume(const Ctx &X, int e, const double *el, const double *gq, dou
                 for (int m = i + 1; m < Np; ++m) {
                     const int id2 = node_id(X, m, j, k);
                     for (int q = 0; q < nf; ++q) s2[q] = el[id2 * nf + q];
-                    volume_flux(dim, X.P.gamma, s1, s2, m0, m0, f);
+                    volume_flux(dim, X.P.gamma, s1, s2, mrow(id1, 0), mrow(id2, 0), f);
                     if (X.axi) {   // DGSEMIntegrator.cpp:273-291: f *= r at the reference midpoint
                         const double rh = 0.5 * (X.r((long)e * nd + id1) + X.r((long)e * nd + id2));
                         for (int q = 0; q < nf; ++q) f[q] *= rh;
@@ -956,7 +971,7 @@ void element_volume(const Ctx &X, int e, const double *el, const double *gq, dou
                     for (int m = j + 1; m < Np; ++m) {
                         const int id2 = node_id(X, i, m, k);
                         for (int q = 0; q < nf; ++q) s2[q] = el[id2 * nf + q];
-                        volume_flux(dim, X.P.gamma, s1, s2, m1r, m1r, g);
+                        volume_flux(dim, X.P.gamma, s1, s2, mrow(id1, 1), mrow(id2, 1), g);
                         if (X.axi) {   // :319-338
                             const double rh = 0.5 * (X.r((long)e * nd + id1) + X.r((long)e * nd + id2));
                             for (int q = 0; q < nf; ++q) g[q] *= rh;
@@ -970,7 +985,7 @@ void element_volume(const Ctx &X, int e, const double *el, const double *gq, dou
                         for (int m = k + 1; m < Np; ++m) {
                             const int id2 = node_id(X, i, j, m);
                             for (int q = 0; q < nf; ++q) s2[q] = el[id2 * nf + q];
-                            volume_flux(dim, X.P.gamma, s1, s2, m2r, m2r, h);
+                            volume_flux(dim, X.P.gamma, s1, s2, mrow(id1, 2), mrow(id2, 2), h);
                             setcol(Hi, id1, m, h);
                             setcol(Hi, id2, k, (ns && X.quirks == 0) ? g : h);   // Q2
                         }
@@ -1005,7 +1020,7 @@ void element_volume(const Ctx &X, int e, const double *el, const double *gq, dou
                 for (int q = 0; q < nf; ++q) dUi[q] = -dUi[q];
                 if (X.blending)
                     for (int q = 0; q < nf; ++q) dUi[q] *= (1.0 - alpha);
-                const double mJ = 1.0 / J;
+                const double mJ = 1.0 / X.Jn(e, id1);   // J = Tr.Weight() at id1
                 if (X.axi) {   // DGSEMIntegrator.cpp:411-428: + p on the radial momentum
                     const double *st = el + id1 * nf;
                     const double ke = 0.5 * ((st[1] * st[1] + st[2] * st[2]) / st[0]);
@@ -1023,8 +1038,6 @@ void element_volume(const Ctx &X, int e, const double *el, const double *gq, dou
 // LiftingBR1.cpp:156-272 (element part), entropy variables in `v` [nd][nf].
 void element_lift(const Ctx &X, int e, const double *v, double *gout /*[dim][nd][nf]*/) {
     const int nf = X.nf, Np = X.Np, nd = X.nd, dim = X.dim;
-    const double *adj = X.A(e);
-    const double J = X.detj[e];
     for (int k = 0; k < X.nz(); ++k)
         for (int j = 0; j < X.ny(); ++j)
             for (int i = 0; i < X.nx(); ++i) {
@@ -1043,7 +1056,8 @@ void element_lift(const Ctx &X, int e, const double *v, double *gout /*[dim][nd]
                         for (int q = 0; q < nf; ++q) g1[q][2] += c[q] * X.D[k * Np + l];
                     }
                 }
-                const double mJ = 1.0 / J;
+                const double *adj = X.An(e, id);   // LiftingBR1.cpp:184-186: J, adj at the node
+                const double mJ = 1.0 / X.Jn(e, id);
                 for (int c = 0; c < dim; ++c)
                     for (int q = 0; q < nf; ++q) {
                         double s = 0.0;
@@ -1196,11 +1210,12 @@ void run_rhs(const Ctx &X, const double *u_in, double *dudt, double *alpha_out, 
                 const int *fe = X.faces + 4 * fc;
                 if ((fe[1] >> 1) != dir || fe[2] < 0) continue;
                 const int e1 = fe[0], lf1 = fe[1], e2 = fe[2], lf2 = fe[3];
-                const double *nor = X.fnor + (long)fc * dim;
-                const double a1 = 1.0 / (w0 * X.detj[e1]), a2 = 1.0 / (w0 * X.detj[e2]);
                 for (int a = 0; a < nfn; ++a) {
                     const int n1 = face_node(X, lf1, a), n2 = face_node(X, lf2, a);
                     const long g1 = (long)e1 * nd + n1, g2 = (long)e2 * nd + n2;
+                    // LiftingBR1.cpp:40-49: J1, J2 at the face point, CalcOrtho there
+                    const double *nor = X.Nf(fc, a);
+                    const double a1 = 1.0 / (w0 * X.Jn(e1, n1)), a2 = 1.0 / (w0 * X.Jn(e2, n2));
                     double fj[5];
                     for (int f = 0; f < nf; ++f) fj[f] = 0.5 * (ent[f * Ndof + g2] - ent[f * Ndof + g1]);
                     for (int c = 0; c < dim; ++c)
@@ -1220,10 +1235,11 @@ void run_rhs(const Ctx &X, const double *u_in, double *dudt, double *alpha_out, 
                 const int *fe = X.faces + 4 * fc;
                 if ((fe[1] >> 1) != dir || fe[2] >= 0) continue;
                 const int e1 = fe[0], lf1 = fe[1];
-                const double *nor = X.fnor + (long)fc * dim;
-                const double a1 = 1.0 / (w0 * X.detj[e1]);
                 for (int a = 0; a < nfn; ++a) {
-                    const long g1 = (long)e1 * nd + face_node(X, lf1, a);
+                    const int n1 = face_node(X, lf1, a);
+                    const long g1 = (long)e1 * nd + n1;
+                    const double *nor = X.Nf(fc, a);
+                    const double a1 = 1.0 / (w0 * X.Jn(e1, n1));
                     double w1[5], fj[5];
                     for (int f = 0; f < nf; ++f) w1[f] = ent[f * Ndof + g1];
                     bdr_lift_flux(X, X.bcs[fe[3]], w1, nor, fj);
@@ -1269,11 +1285,12 @@ void run_rhs(const Ctx &X, const double *u_in, double *dudt, double *alpha_out, 
             const int *fe = X.faces + 4 * fc;
             if ((fe[1] >> 1) != dir) continue;
             const int e1 = fe[0], lf1 = fe[1], e2 = fe[2], lf2 = fe[3];
-            const double *nor = X.fnor + (long)fc * dim;
             if (e2 < 0) {   // boundary face (BdrFaceIntegrator::AssembleFaceVector)
-                const double a1 = 1.0 / (w0 * X.detj[e1]);
                 for (int a = 0; a < nfn; ++a) {
-                    const long g1 = (long)e1 * nd + face_node(X, lf1, a);
+                    const int n1 = face_node(X, lf1, a);
+                    const long g1 = (long)e1 * nd + n1;
+                    const double *nor = X.Nf(fc, a);
+                    const double a1 = 1.0 / (w0 * X.Jn(e1, n1));
                     double s1[5] = {0, 0, 0, 0, 0}, s2[5] = {0, 0, 0, 0, 0}, flux[5], d1[5];
                     for (int f = 0; f < nf; ++f) s1[f] = u[f * Ndof + g1];
                     bdr_face_flux(X, X.bcs[lf2], s1, s2, nor, flux);
@@ -1291,10 +1308,12 @@ void run_rhs(const Ctx &X, const double *u_in, double *dudt, double *alpha_out, 
                 }
                 continue;
             }
-            const double a1 = 1.0 / (w0 * X.detj[e1]), a2 = 1.0 / (w0 * X.detj[e2]);
             for (int a = 0; a < nfn; ++a) {
                 const int n1 = face_node(X, lf1, a), n2 = face_node(X, lf2, a);
                 const long g1 = (long)e1 * nd + n1, g2 = (long)e2 * nd + n2;
+                // DGSEMIntegrator.cpp:151-222: J1, J2 at the face point, CalcOrtho there
+                const double *nor = X.Nf(fc, a);
+                const double a1 = 1.0 / (w0 * X.Jn(e1, n1)), a2 = 1.0 / (w0 * X.Jn(e2, n2));
                 double s1[5], s2[5], flux[5], d1[5], d2[5];
                 for (int f = 0; f < nf; ++f) { s1[f] = u[f * Ndof + g1]; s2[f] = u[f * Ndof + g2]; }
                 if (!X.parabolic) {

@@ -8,8 +8,9 @@
  *
  * Parity status: pinned at the integrator level against the reference's own
  * sources compiled under oracle/_ref (see oracle/ref_harness/).  The MFEM
- * geometry pieces (Gauss-Lobatto rule, affine transformations, face normals)
- * are restated from their mathematics on both sides.
+ * geometry pieces (Gauss-Lobatto rule, affine and multilinear element
+ * transformations, face normals) are restated from their mathematics on both
+ * sides.
  *
  * Layout conventions (identical to the product's C-ABI):
  *   state u: MFEM Ordering::byNODES, u[f*Ndof + e*Np^dim + node], node
@@ -37,6 +38,15 @@ typedef struct oracle_mesh {
     const double *elem_detj;  /* [E] Jacobian determinant */
     const int *face_elems;    /* [F][4] elem1, lface1, elem2, lface2 */
     const double *face_nor;   /* [F][dim] */
+    /* Non-affine (multilinear) elements; all three NULL for affine meshes.
+     * MFEM evaluates the element transformation at every Gauss-Lobatto node
+     * (ElementTransformation::SetIntPoint + AdjugateJacobian / Weight,
+     * DGSEMIntegrator.cpp:254-267) and the face transformation at every face
+     * point (CalcOrtho, DGSEMIntegrator.cpp:151-222). */
+    const double *node_adj;   /* [E][Np^dim][dim][dim] adjugate at each node */
+    const double *node_detj;  /* [E][Np^dim] Jacobian determinant at each node */
+    const double *face_node_nor; /* [F][Np^(dim-1)][dim] scaled normal at each face node
+                                    (face node order of elem1's local face) */
 } oracle_mesh;
 
 /* Boundary conditions.  A boundary face is listed in face_elems as

@@ -19,7 +19,16 @@ class OracleMesh(C.Structure):
     _fields_ = [("dim", C.c_int), ("order", C.c_int), ("num_elements", C.c_int),
                 ("num_faces", C.c_int), ("elem_adj", C.POINTER(C.c_double)),
                 ("elem_detj", C.POINTER(C.c_double)), ("face_elems", C.POINTER(C.c_int)),
-                ("face_nor", C.POINTER(C.c_double))]
+                ("face_nor", C.POINTER(C.c_double)), ("node_adj", C.POINTER(C.c_double)),
+                ("node_detj", C.POINTER(C.c_double)), ("face_node_nor", C.POINTER(C.c_double))]
+
+
+def _node_geometry(mesh, dtype):
+    """Per-node adjugates / determinants and per-face-node normals of a mesh with
+    non-affine elements (None for affine meshes)."""
+    if getattr(mesh, "node_adj", None) is None:
+        return None
+    return tuple(np.ascontiguousarray(a, dtype=dtype) for a in (mesh.node_adj, mesh.node_detj, mesh.face_node_nor))
 
 
 class OracleBC(C.Structure):
@@ -113,9 +122,11 @@ class Oracle:
         self._detj = np.ascontiguousarray(mesh.elem_detj, dtype=np.float64)
         self._faces = np.ascontiguousarray(mesh.face_elems, dtype=np.int32)
         self._nor = np.ascontiguousarray(mesh.face_nor, dtype=np.float64)
+        self._ngeo = _node_geometry(mesh, np.float64)
+        ng = [_p(a) for a in self._ngeo] if self._ngeo else [None, None, None]
         self.m = OracleMesh(mesh.dim, mesh.order, mesh.num_elements, mesh.num_faces,
                             _p(self._adj), _p(self._detj),
-                            self._faces.ctypes.data_as(C.POINTER(C.c_int)), _p(self._nor))
+                            self._faces.ctypes.data_as(C.POINTER(C.c_int)), _p(self._nor), *ng)
         self._bcs = make_bcs(bcs)
         self._xy = np.ascontiguousarray(mesh.coords, dtype=np.float64)
         self.c = OracleConfig(gamma, Pr, mu, R_gas, alpha_max, alpha_min, parabolic, blending,
@@ -166,7 +177,8 @@ _LDP = C.POINTER(C.c_longdouble)
 
 class _MeshLD(C.Structure):
     _fields_ = [("dim", C.c_int), ("order", C.c_int), ("num_elements", C.c_int), ("num_faces", C.c_int),
-                ("elem_adj", _LDP), ("elem_detj", _LDP), ("face_elems", C.POINTER(C.c_int)), ("face_nor", _LDP)]
+                ("elem_adj", _LDP), ("elem_detj", _LDP), ("face_elems", C.POINTER(C.c_int)), ("face_nor", _LDP),
+                ("node_adj", _LDP), ("node_detj", _LDP), ("face_node_nor", _LDP)]
 
 
 class _ConfigLD(C.Structure):
@@ -202,9 +214,11 @@ class LongDoubleOracle:
         self._detj = np.ascontiguousarray(mesh.elem_detj, dtype=ld)
         self._faces = np.ascontiguousarray(mesh.face_elems, dtype=np.int32)
         self._nor = np.ascontiguousarray(mesh.face_nor, dtype=ld)
+        self._ngeo = _node_geometry(mesh, ld)
+        ng = [a.ctypes.data_as(_LDP) for a in self._ngeo] if self._ngeo else [None, None, None]
         self.m = _MeshLD(mesh.dim, mesh.order, mesh.num_elements, mesh.num_faces,
                          self._adj.ctypes.data_as(_LDP), self._detj.ctypes.data_as(_LDP),
-                         self._faces.ctypes.data_as(C.POINTER(C.c_int)), self._nor.ctypes.data_as(_LDP))
+                         self._faces.ctypes.data_as(C.POINTER(C.c_int)), self._nor.ctypes.data_as(_LDP), *ng)
         self.c = _ConfigLD(gamma, Pr, mu, R_gas, alpha_max, alpha_min, parabolic, blending, sutherland, quirks,
                            surface_dissipation, 0, None, 0, None, 0.0)
         self.nthreads = nthreads or os.cpu_count() or 1

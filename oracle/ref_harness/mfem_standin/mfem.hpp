@@ -15,7 +15,8 @@
 // reciprocal, DenseMatrix is column-major and its products accumulate in
 // MFEM's kernel order, CalcOrtho and AddMult_a_VWt follow MFEM's formulas, and
 // Gauss-Lobatto rules/basis are on [0,1] with nodes lexicographic, x fastest.
-// Only affine elements of periodic meshes with aligned faces are modelled.
+// Affine and multilinear (bilinear quadrilateral / trilinear hexahedron)
+// elements with aligned faces are modelled.
 #pragma once
 
 #include <algorithm>
@@ -548,6 +549,10 @@ public:
 };
 
 // ------------------------------------------------------- transformations
+// The element map is affine (x = x0 + J xi) or multilinear in the element's
+// corners (MFEM's IsoparametricTransformation with the order-1 H1 basis):
+// SetIntPoint evaluates J = dx/dxi there and, as MFEM does on demand, its
+// adjugate (CalcAdjugate) and determinant (Weight).
 class ElementTransformation {
 public:
     int ElementNo = 0;
@@ -555,8 +560,13 @@ public:
     DenseMatrix J, adj;
     real_t detJ = 0.0;
     real_t x0[3] = {0, 0, 0};
+    bool multilinear = false;
+    real_t corner[8][3] = {};          // corner b at reference vertex (b & 1, b >> 1 & 1, b >> 2 & 1)
     const IntegrationPoint *ip = nullptr;
-    void SetIntPoint(const IntegrationPoint *p) { ip = p; }
+    void SetIntPoint(const IntegrationPoint *p) {
+        ip = p;
+        if (multilinear) eval(*p);
+    }
     const IntegrationPoint &GetIntPoint() const { return *ip; }
     real_t Weight() { return detJ; }
     const DenseMatrix &Jacobian() { return J; }
@@ -564,10 +574,49 @@ public:
     void Transform(const IntegrationPoint &p, Vector &x) {
         real_t xi[3] = {p.x, p.y, p.z};
         x.SetSize(dim);
+        if (multilinear) {
+            for (int r = 0; r < dim; ++r) x(r) = 0.0;
+            for (int b = 0; b < (1 << dim); ++b) {
+                real_t phi = 1.0;
+                for (int q = 0; q < dim; ++q) phi *= ((b >> q) & 1) ? xi[q] : 1.0 - xi[q];
+                for (int r = 0; r < dim; ++r) x(r) += phi * corner[b][r];
+            }
+            return;
+        }
         for (int r = 0; r < dim; ++r) {
             real_t s = x0[r];
             for (int c = 0; c < dim; ++c) s += J(r, c) * xi[c];
             x(r) = s;
+        }
+    }
+
+private:
+    void eval(const IntegrationPoint &p) {
+        const real_t xi[3] = {p.x, p.y, p.z};
+        for (int r = 0; r < dim; ++r)
+            for (int c = 0; c < dim; ++c) J(r, c) = 0.0;
+        for (int b = 0; b < (1 << dim); ++b)
+            for (int c = 0; c < dim; ++c) {
+                real_t dphi = ((b >> c) & 1) ? 1.0 : -1.0;
+                for (int q = 0; q < dim; ++q)
+                    if (q != c) dphi *= ((b >> q) & 1) ? xi[q] : 1.0 - xi[q];
+                for (int r = 0; r < dim; ++r) J(r, c) += dphi * corner[b][r];
+            }
+        if (dim == 2) {   // CalcAdjugate, DenseMatrix::Det
+            adj(0, 0) = J(1, 1); adj(0, 1) = -J(0, 1);
+            adj(1, 0) = -J(1, 0); adj(1, 1) = J(0, 0);
+            detJ = J(0, 0) * J(1, 1) - J(0, 1) * J(1, 0);
+        } else {
+            adj(0, 0) = J(1, 1) * J(2, 2) - J(1, 2) * J(2, 1);
+            adj(0, 1) = J(0, 2) * J(2, 1) - J(0, 1) * J(2, 2);
+            adj(0, 2) = J(0, 1) * J(1, 2) - J(0, 2) * J(1, 1);
+            adj(1, 0) = J(1, 2) * J(2, 0) - J(1, 0) * J(2, 2);
+            adj(1, 1) = J(0, 0) * J(2, 2) - J(0, 2) * J(2, 0);
+            adj(1, 2) = J(0, 2) * J(1, 0) - J(0, 0) * J(1, 2);
+            adj(2, 0) = J(1, 0) * J(2, 1) - J(1, 1) * J(2, 0);
+            adj(2, 1) = J(0, 1) * J(2, 0) - J(0, 0) * J(2, 1);
+            adj(2, 2) = J(0, 0) * J(1, 1) - J(0, 1) * J(1, 0);
+            detJ = J(0, 0) * adj(0, 0) + J(0, 1) * adj(1, 0) + J(0, 2) * adj(2, 0);
         }
     }
 };
@@ -577,9 +626,12 @@ public:
     int ElementNo = -1;   // the face number
     int Elem1No = -1, Elem2No = -1;
     int lf1 = 0, lf2 = 0, dim = 0;
+    real_t orient = 1.0;  // sign that makes CalcOrtho point out of elem1
     ElementTransformation *T1 = nullptr, *T2 = nullptr;
     DenseMatrix Jf;
     IntegrationPoint eip1, eip2;
+    // maps the face point into both elements, sets their transformations there
+    // and the face Jacobian (element 1's tangential columns, oriented)
     void SetAllIntPoints(const IntegrationPoint *face_ip);
     ElementTransformation &GetElement1Transformation() { return *T1; }
     ElementTransformation &GetElement2Transformation() { return *T2; }

@@ -159,6 +159,14 @@ void FaceElementTransformations::SetAllIntPoints(const IntegrationPoint *fip) {
         map(lf2, eip2);
         T2->SetIntPoint(&eip2);
     }
+    const int d = lf1 >> 1;
+    Jf.SetSize(dim, dim - 1);
+    if (dim == 2) {
+        for (int r = 0; r < 2; ++r) Jf(r, 0) = orient * T1->J(r, 1 - d);
+    } else {
+        const int t0 = (d == 0) ? 1 : 0, t1 = (d == 2) ? 1 : 2;
+        for (int r = 0; r < 3; ++r) { Jf(r, 0) = orient * T1->J(r, t0); Jf(r, 1) = T1->J(r, t1); }
+    }
 }
 
 }   // namespace mfem
@@ -168,10 +176,18 @@ using namespace Prandtl;
 
 namespace {
 
-// Stand-in ParMesh of an affine periodic mesh from the oracle descriptor.
+// Stand-in ParMesh from the oracle descriptor: affine elements from the
+// per-element adjugates, or (descriptor with per-node geometry) multilinear
+// elements from their corner nodes, which the Gauss-Lobatto node coordinates
+// include.
 std::shared_ptr<ParMesh> make_mesh(const oracle_mesh *m, const double *coords = nullptr) {
     auto pm = std::make_shared<ParMesh>();
-    const int dim = m->dim;
+    const int dim = m->dim, Np = m->order + 1;
+    int nd = 1;
+    for (int d = 0; d < dim; ++d) nd *= Np;
+    const long Ndof = (long)m->num_elements * nd;
+    const bool multi = m->node_adj != nullptr;
+    if (multi && !coords) throw std::runtime_error("multilinear elements need the node coordinates");
     pm->dim = dim;
     pm->trans.resize(m->num_elements);
     for (int e = 0; e < m->num_elements; ++e) {
@@ -180,6 +196,14 @@ std::shared_ptr<ParMesh> make_mesh(const oracle_mesh *m, const double *coords = 
         T.dim = dim;
         T.adj.SetSize(dim);
         T.J.SetSize(dim);
+        if (multi) {
+            T.multilinear = true;
+            for (int b = 0; b < (1 << dim); ++b) {
+                const int n = ((b & 1) + Np * ((b >> 1) & 1) + Np * Np * ((b >> 2) & 1)) * (Np - 1);
+                for (int d = 0; d < dim; ++d) T.corner[b][d] = coords[d * Ndof + (long)e * nd + n];
+            }
+            continue;
+        }
         const double *a = m->elem_adj + (size_t)e * dim * dim;
         for (int r = 0; r < dim; ++r)
             for (int c = 0; c < dim; ++c) T.adj(r, c) = a[r * dim + c];
@@ -189,12 +213,8 @@ std::shared_ptr<ParMesh> make_mesh(const oracle_mesh *m, const double *coords = 
         inv.Invert();
         for (int r = 0; r < dim; ++r)
             for (int c = 0; c < dim; ++c) T.J(r, c) = T.detJ * inv(r, c);
-        if (coords) {   // origin = node 0 of the element (xi = 0)
-            int nd = 1;
-            for (int d = 0; d < dim; ++d) nd *= m->order + 1;
-            const long Ndof = (long)m->num_elements * nd;
+        if (coords)   // origin = node 0 of the element (xi = 0)
             for (int d = 0; d < dim; ++d) T.x0[d] = coords[d * Ndof + (long)e * nd];
-        }
     }
     for (int f = 0; f < m->num_faces; ++f) {
         const int *fe = m->face_elems + 4 * f;
@@ -205,23 +225,19 @@ std::shared_ptr<ParMesh> make_mesh(const oracle_mesh *m, const double *coords = 
         F->dim = dim;
         F->T1 = &pm->trans[fe[0]];
         F->T2 = fe[2] >= 0 ? &pm->trans[fe[2]] : nullptr;
-        // face Jacobian: element-1 Jacobian columns along the face's
-        // tangential directions, oriented so CalcOrtho points out of elem1
+        // orientation: CalcOrtho of element 1's tangential columns at the face
+        // centre against the outward adjugate row there
         const int d = fe[1] >> 1, s = fe[1] & 1;
-        const DenseMatrix &J = F->T1->J;
-        F->Jf.SetSize(dim, dim - 1);
-        if (dim == 2) {
-            for (int r = 0; r < 2; ++r) F->Jf(r, 0) = J(r, 1 - d);
-        } else {
-            const int t0 = (d == 0) ? 1 : 0, t1 = (d == 2) ? 1 : 2;
-            for (int r = 0; r < 3; ++r) { F->Jf(r, 0) = J(r, t0); F->Jf(r, 1) = J(r, t1); }
-        }
+        IntegrationPoint c;
+        c.x = 0.5; c.y = 0.5; c.z = 0.0;
+        F->orient = 1.0;
+        F->SetAllIntPoints(&c);
         Vector n(dim);
         CalcOrtho(F->Jf, n);
         real_t dot = 0.0;
-        for (int c = 0; c < dim; ++c) dot += n(c) * F->T1->adj(d, c) * (s ? 1.0 : -1.0);
-        if (dot < 0)
-            for (int r = 0; r < dim; ++r) F->Jf(r, 0) = -F->Jf(r, 0);
+        for (int q = 0; q < dim; ++q) dot += n(q) * F->T1->adj(d, q) * (s ? 1.0 : -1.0);
+        if (dot < 0) F->orient = -1.0;
+        F->SetAllIntPoints(&c);
         pm->faces.push_back(std::move(F));
     }
     return pm;

@@ -107,6 +107,16 @@ class Mesh:
     weights_1d: np.ndarray = field(default=None)
     face_attr: np.ndarray = field(default=None)   # (F,) boundary attribute per face (read meshes)
     elem_attr: np.ndarray = field(default=None)   # (E,) element attribute (read meshes)
+    # non-affine (multilinear) elements: the transformation at every node and the
+    # scaled normal at every face node (None for affine meshes, whose elem_adj /
+    # elem_detj / face_nor hold for every node)
+    node_adj: np.ndarray = field(default=None)        # (E, Np^dim, dim, dim)
+    node_detj: np.ndarray = field(default=None)       # (E, Np^dim)
+    face_node_nor: np.ndarray = field(default=None)   # (F, Np^(dim-1), dim), elem1's face node order
+
+    @property
+    def affine(self) -> bool:
+        return self.node_adj is None
 
     @property
     def Np(self) -> int:
@@ -140,16 +150,69 @@ class Mesh:
             wn = np.outer(w, w).reshape(-1)          # [j][i] -> node j*Np+i
         else:
             wn = np.einsum("k,j,i->kji", w, w, w).reshape(-1)
-        return (self.elem_detj[:, None] * wn[None, :]).reshape(-1)
+        detj = self.elem_detj[:, None] if self.node_detj is None else self.node_detj
+        return (detj * wn[None, :]).reshape(-1)
 
 
-def periodic_box(dim: int, n, order: int, lo=0.0, hi=1.0, affine=None, bcs=None) -> Mesh:
+def face_node(dim: int, Np: int, lf: int, a: int) -> int:
+    """Element-local node of face node a on local face lf = 2*dir + side (face
+    nodes lexicographic over the remaining directions, lower direction fastest)."""
+    d, s = lf >> 1, lf & 1
+    c = [0, 0, 0]
+    c[d] = s * (Np - 1)
+    if dim == 2:
+        c[1 - d] = a
+    else:
+        t0 = 1 if d == 0 else 0
+        t1 = 1 if d == 2 else 2
+        c[t0], c[t1] = a % Np, a // Np
+    return c[0] + Np * c[1] + Np * Np * c[2]
+
+
+def multilinear_geometry(corners: np.ndarray, x1: np.ndarray):
+    """Node coordinates, Jacobian adjugates and determinants of multilinear
+    elements (MFEM's bilinear quadrilateral / trilinear hexahedron map) at the
+    tensor Gauss-Lobatto nodes x1.
+
+    corners: (E, 2^dim, dim), corner b at reference vertex (b & 1, b >> 1 & 1,
+    b >> 2 & 1).  Returns coords (dim, E*Np^dim), adj (E, Np^dim, dim, dim),
+    detj (E, Np^dim), with J[i][r] = dx_i / dxi_r."""
+    E, nc, dim = corners.shape
+    Np = len(x1)
+    grids = np.meshgrid(*([x1] * dim), indexing="ij")
+    ref = np.stack([g.transpose().reshape(-1) for g in grids], axis=1)   # (nd, dim), x fastest
+    nd = ref.shape[0]
+    bits = np.array([[(b >> r) & 1 for r in range(dim)] for b in range(nc)], dtype=np.float64)   # (nc, dim)
+    # phi_b(xi) = prod_r (xi_r if bit else 1 - xi_r); dphi_b / dxi_r
+    fac = np.where(bits[None, :, :] > 0, ref[:, None, :], 1.0 - ref[:, None, :])   # (nd, nc, dim)
+    phi = fac.prod(axis=2)                                                       # (nd, nc)
+    dphi = np.empty((nd, nc, dim))
+    for r in range(dim):
+        others = np.prod(np.delete(fac, r, axis=2), axis=2) if dim > 1 else 1.0
+        dphi[:, :, r] = np.where(bits[None, :, r] > 0, 1.0, -1.0) * others
+    X = np.einsum("kb,ebi->eki", phi, corners)            # (E, nd, dim)
+    J = np.einsum("kbr,ebi->ekir", dphi, corners)         # (E, nd, dim, dim)
+    adj = np.empty_like(J)
+    detj = np.empty(J.shape[:2])
+    for e in range(E):
+        for k in range(nd):
+            adj[e, k] = _adjugate(J[e, k])
+            detj[e, k] = _det(J[e, k])
+    coords = np.ascontiguousarray(X.transpose(2, 0, 1).reshape(dim, E * nd))
+    return coords, adj, detj
+
+
+def periodic_box(dim: int, n, order: int, lo=0.0, hi=1.0, affine=None, bcs=None, warp=None) -> Mesh:
     """Box mesh [lo, hi]^dim with n elements per direction, periodic unless
     ``bcs`` says otherwise.
 
     ``n`` may be an int or a per-direction tuple; ``lo``/``hi`` scalars or
     per-direction tuples.  ``affine`` (dim x dim) maps the box afterwards,
-    x = affine @ X, keeping every element affine.  ``bcs`` (length 2*dim,
+    x = affine @ X, keeping every element affine.  ``warp`` (a function of the
+    box coordinates X, shape (dim, npts), returning displacements of the same
+    shape; periodic in the periodic directions) moves every element corner to
+    affine @ X + warp(X): the elements become multilinear (non-affine) and the
+    mesh carries per-node geometry.  ``bcs`` (length 2*dim,
     entry 2*d + side for the side x_d = lo (0) or hi (1)) holds None for a
     periodic direction or the boundary-condition index of that side's
     boundary faces, listed as (elem, local face, -1, bc index).
@@ -218,9 +281,53 @@ def periodic_box(dim: int, n, order: int, lo=0.0, hi=1.0, affine=None, bcs=None)
     coords = np.einsum("ab,bek->aek", M, X).reshape(dim, -1)
     # GetElementSize(e, 1): smallest singular value of J
     hmin = float(np.linalg.svd(J, compute_uv=False).min())
-    return Mesh(dim=dim, order=order, n=n, elem_adj=elem_adj, elem_detj=elem_detj,
+    mesh = Mesh(dim=dim, order=order, n=n, elem_adj=elem_adj, elem_detj=elem_detj,
                 face_elems=face_elems, face_nor=face_nor, coords=coords, hmin=hmin,
                 nodes_1d=x1, weights_1d=w1)
+    if warp is not None:
+        nc = 1 << dim
+        bits = np.array([[(b >> r) & 1 for r in range(dim)] for b in range(nc)])   # (nc, dim)
+        Xc = lo[None, None, :] + (cell.T[:, None, :] + bits[None, :, :]) * h[None, None, :]   # (E, nc, dim)
+        flat = Xc.reshape(-1, dim).T
+        corners = (M @ flat + np.asarray(warp(flat), dtype=np.float64)).T.reshape(E, nc, dim)
+        set_multilinear(mesh, corners)
+    return mesh
+
+
+def set_multilinear(mesh: Mesh, corners: np.ndarray) -> None:
+    """Give ``mesh`` the geometry of multilinear elements with these corners
+    ((E, 2^dim, dim), corner b at reference vertex bits of b, in each element's
+    local frame): node coordinates, per-node adjugates and determinants, the
+    scaled normal at every face node (outward from elem1: +/- the adjugate row
+    of the face direction at elem1's face node, which is MFEM's CalcOrtho of the
+    face Jacobian), element values at the centre, and hmin as MFEM's
+    GetElementSize(e, 1) (smallest singular value of J at the centre)."""
+    dim, Np = mesh.dim, mesh.order + 1
+    x1 = mesh.nodes_1d
+    coords, adj, detj = multilinear_geometry(corners, x1)
+    if not (detj > 0).all():
+        raise ValueError("inverted element (det J <= 0 at a node)")
+    _, cadj, cdet = multilinear_geometry(corners, np.array([0.5]))
+    nfn = Np ** (dim - 1)
+    F = mesh.num_faces
+    fnn = np.empty((F, nfn, dim))
+    for fc in range(F):
+        e1, lf1 = int(mesh.face_elems[fc, 0]), int(mesh.face_elems[fc, 1])
+        d, sgn = lf1 >> 1, (1.0 if lf1 & 1 else -1.0)
+        for a in range(nfn):
+            fnn[fc, a] = sgn * adj[e1, face_node(dim, Np, lf1, a), d]
+    Jc = np.array([[[0.0] * dim] * dim] * corners.shape[0])
+    # centre Jacobian from the centre adjugate: J = adj(adj) / det^(dim-2)
+    for e in range(corners.shape[0]):
+        Jc[e] = _adjugate(cadj[e, 0]) / (cdet[e, 0] ** (dim - 2))
+    mesh.coords = coords
+    mesh.node_adj = adj
+    mesh.node_detj = detj
+    mesh.face_node_nor = fnn
+    mesh.elem_adj = np.ascontiguousarray(cadj[:, 0])
+    mesh.elem_detj = np.ascontiguousarray(cdet[:, 0])
+    mesh.face_nor = np.ascontiguousarray(fnn.mean(axis=1))
+    mesh.hmin = float(min(np.linalg.svd(Jc[e], compute_uv=False).min() for e in range(corners.shape[0])))
 
 
 def read_mesh(path: str, order: int, refine: int = 0, hilbert: bool = False, boundary_conditions=None) -> Mesh:

@@ -115,6 +115,59 @@ def axi_inputs(n, order, blending, amp, seed):
     return mesh, (U * mesh.coords[1][None, :]).reshape(-1)
 
 
+# Non-affine (multilinear) elements: the box's element corners moved by a
+# smooth displacement (periodic on the unit box), so every element is a
+# general bilinear quadrilateral / trilinear hexahedron with per-node metrics;
+# (name, dim, n, order, parabolic, blending, amplitude, seed, boundary set or None).
+CURVED_CASES = [
+    ("curved_euler2d_blend_n3_N3", 2, 3, 3, 0, 1, 0.30, 51, None),
+    ("curved_euler2d_n3_N1", 2, 3, 1, 0, 0, 0.10, 52, None),
+    ("curved_ns2d_n3_N2", 2, 3, 2, 1, 0, 0.10, 53, None),
+    ("curved_euler3d_n3_N2", 3, 3, 2, 0, 0, 0.10, 54, None),
+    ("curved_ns3d_blend_n3_N2", 3, 3, 2, 1, 1, 0.30, 55, None),
+    ("curved_euler2d_bdr_blend_n3_N2", 2, 3, 2, 0, 1, 0.30, 56, "walls"),
+    ("curved_ns2d_walls_n3_N3", 2, 3, 3, 1, 0, 0.10, 57, "ns_walls"),
+    ("curved_euler3d_char_n3_N2", 3, 3, 2, 0, 0, 0.10, 58, "char"),
+]
+CURVED_AXI_CASES = [
+    ("curved_axi2d_n4x3_N1", (4, 3), 1, 0, 0.10, 61),
+    ("curved_axi2d_blend_n4x3_N2", (4, 3), 2, 1, 0.30, 62),
+]
+
+
+def warp_field(dim, amp):
+    """Corner displacement on the unit box, periodic in every direction."""
+    def w(X):
+        s = [np.sin(2 * np.pi * X[d]) for d in range(dim)]
+        c = [np.cos(2 * np.pi * X[d]) for d in range(dim)]
+        if dim == 2:
+            return amp * np.stack([s[1] * (0.6 + 0.4 * s[0]), s[0] * (0.5 + 0.5 * c[1])])
+        return amp * np.stack([s[1] * s[2] + 0.3 * s[0] * c[1], s[0] * s[2] + 0.3 * s[1] * c[2],
+                               s[0] * s[1] + 0.3 * s[2] * c[0]])
+    return w
+
+
+def axi_warp(X):
+    """Displacement of the (z, r) box [0,2] x [0,1] that keeps the axis r = 0 and
+    the other sides straight."""
+    z, r = X[0], X[1]
+    return np.stack([0.06 * np.sin(np.pi * r) * np.sin(np.pi * z), 0.05 * np.sin(np.pi * r) * np.sin(0.5 * np.pi * z)])
+
+
+def curved_inputs(dim, n, order, amp, seed, bset=None):
+    sides = BC_SETS[bset][2][dim] if bset else None
+    mesh = periodic_box(dim, n, order, 0.0, 1.0, bcs=sides, warp=warp_field(dim, 0.06))
+    base = cases.free_stream(mesh, rho=1.2, vel=[0.4, -0.3, 0.2][:dim], p=1.5)
+    return mesh, cases.perturbed(mesh, base, amp=amp, seed=seed)
+
+
+def curved_axi_inputs(n, order, blending, amp, seed):
+    mesh = periodic_box(2, n, order, (0.0, 0.0), (2.0, 1.0), bcs=AXI_SIDES, warp=axi_warp)
+    U = cases.perturbed(mesh, cases.free_stream(mesh, rho=1.2, vel=[0.3, 0.05], p=1.5),
+                        amp=amp, seed=seed).reshape(4, -1)
+    return mesh, (U * mesh.coords[1][None, :]).reshape(-1)
+
+
 def bc_example(kind, dim):
     """One condition of the given type with constant data for a dim-D case;
     "riemann_supersonic" is the Riemann condition with a supersonic outer state."""
@@ -161,8 +214,21 @@ def main():
         out[f"{name}/u"] = u
         out[f"{name}/dudt"] = r["dudt"]
         out[f"{name}/alpha"] = r["alpha"]
+    for name, dim, n, order, par, bl, amp, seed, bset in CURVED_CASES:
+        mesh, u = curved_inputs(dim, n, order, amp, seed, bset)
+        bcs = BC_SETS[bset][1][dim] if bset else None
+        r = pyoracle.RefOperator(mesh, parabolic=par, blending=bl, bcs=bcs, **PHYS).rhs(u, want_alpha=True)
+        out[f"{name}/u"] = u
+        out[f"{name}/dudt"] = r["dudt"]
+        out[f"{name}/alpha"] = r["alpha"]
+    for name, n, order, bl, amp, seed in CURVED_AXI_CASES:
+        mesh, u = curved_axi_inputs(n, order, bl, amp, seed)
+        r = pyoracle.RefOperator(mesh, blending=bl, bcs=AXI_BCS, axisymmetric=1).rhs(u, want_alpha=True)
+        out[f"{name}/u"] = u
+        out[f"{name}/dudt"] = r["dudt"]
+        out[f"{name}/alpha"] = r["alpha"]
     np.savez_compressed(os.path.join(HERE, "reference_rhs.npz"), **out)
-    print(f"wrote {len(CASES) + sum(len(v[0]) for v in BC_SETS.values()) + len(AXI_CASES)} cases")
+    print(f"wrote {len(CASES) + sum(len(v[0]) for v in BC_SETS.values()) + len(AXI_CASES)+ len(CURVED_CASES) + len(CURVED_AXI_CASES)} cases")
 
 
 if __name__ == "__main__":

@@ -212,3 +212,84 @@ def test_oracle_axisymmetric_matches_reference_golden(oracle_mod, case):
     np.testing.assert_allclose(r["alpha"], GOLDEN[f"{name}/alpha"], rtol=0, atol=1e-14)
     if bl:
         assert (r["alpha"] > 0).any()
+
+
+# ---------------------------------------------------------------- multilinear (non-affine) elements
+@pytest.mark.parametrize("case", make_golden.CURVED_CASES, ids=[c[0] for c in make_golden.CURVED_CASES])
+def test_oracle_curved_matches_reference_golden(oracle_mod, case):
+    """Per-node metrics in the volume flux averages, per-node J, subcell metrics
+    integrated along each line, per-face-node normals and J on both sides
+    (DGSEMIntegrator.cpp:254-267, :1199-1304; LiftingBR1.cpp:40-49, :184-186):
+    the oracle against the committed outputs of the reference's sources."""
+    name, dim, n, order, par, bl, amp, seed, bset = case
+    mesh, u = make_golden.curved_inputs(dim, n, order, amp, seed, bset)
+    assert not mesh.affine
+    np.testing.assert_array_equal(u, GOLDEN[f"{name}/u"])
+    bcs = make_golden.BC_SETS[bset][1][dim] if bset else None
+    r = oracle_mod.Oracle(mesh, parabolic=par, blending=bl, quirks=0, bcs=bcs, **make_golden.PHYS).rhs(u, want_alpha=True)
+    assert normalized_error(r["dudt"], GOLDEN[f"{name}/dudt"], mesh.num_fields) <= PIN_TOL
+    np.testing.assert_allclose(r["alpha"], GOLDEN[f"{name}/alpha"], rtol=0, atol=1e-14)
+    if bl:
+        assert (r["alpha"] > 0).any()
+
+
+@pytest.mark.parametrize("case", make_golden.CURVED_AXI_CASES, ids=[c[0] for c in make_golden.CURVED_AXI_CASES])
+def test_oracle_curved_axisymmetric_matches_reference_golden(oracle_mod, case):
+    name, n, order, bl, amp, seed = case
+    mesh, u = make_golden.curved_axi_inputs(n, order, bl, amp, seed)
+    np.testing.assert_array_equal(u, GOLDEN[f"{name}/u"])
+    r = oracle_mod.Oracle(mesh, quirks=0, blending=bl, bcs=make_golden.AXI_BCS, axisymmetric=1).rhs(u, want_alpha=True)
+    assert normalized_error(r["dudt"], GOLDEN[f"{name}/dudt"], mesh.num_fields) <= PIN_TOL
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("par", [0, 1])
+@pytest.mark.parametrize("bl", [0, 1])
+@pytest.mark.parametrize("order", [1, 2, 3, 4])
+def test_oracle_curved_matches_reference_sources(oracle_mod, dim, par, bl, order):
+    o = _ref(oracle_mod)
+    mesh = periodic_box(dim, 3, order, 0.0, 1.0, warp=make_golden.warp_field(dim, 0.05 + 0.01 * order))
+    base = cases.free_stream(mesh, rho=1.1, vel=[0.2, 0.5, -0.3][:dim], p=1.3)
+    u = cases.perturbed(mesh, base, amp=0.3 if bl else 0.1, seed=order)
+    kw = dict(parabolic=par, blending=bl, mu=0.01, Pr=0.71)
+    a = o.Oracle(mesh, quirks=0, **kw).rhs(u, want_alpha=True, want_grad=bool(par))
+    b = o.RefOperator(mesh, **kw).rhs(u, want_alpha=True, want_grad=bool(par))
+    assert normalized_error(a["dudt"], b["dudt"], mesh.num_fields) <= PIN_TOL
+    np.testing.assert_allclose(a["alpha"], b["alpha"], rtol=0, atol=1e-14)
+    if par:
+        assert normalized_error(a["grad"], b["grad"], dim * mesh.num_fields) <= PIN_TOL
+
+
+@pytest.mark.parametrize("order", [1, 2, 4])
+@pytest.mark.parametrize("kind", ["state", "outflow", "slip_wall", "symmetry", "riemann", "inflow_rv"])
+def test_oracle_curved_boundary_matches_reference_sources(oracle_mod, order, kind):
+    """Boundary faces of multilinear elements: the face-node normals and J."""
+    _ref(oracle_mod)
+    bcs = [make_golden.bc_example(kind, 2)]
+    mesh = periodic_box(2, 3, order, 0.0, 1.0, bcs=[0, 0, 0, 0], warp=make_golden.warp_field(2, 0.06))
+    u = cases.perturbed(mesh, cases.free_stream(mesh, rho=1.1, vel=[0.35, -0.2], p=1.6), amp=0.2, seed=order)
+    o = oracle_mod.Oracle(mesh, quirks=0, bcs=bcs).rhs(u)["dudt"]
+    r = oracle_mod.RefOperator(mesh, quirks=0, bcs=bcs).rhs(u)["dudt"]
+    assert normalized_error(o, r, mesh.num_fields) <= 1e-13
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("bl", [0, 1])
+def test_oracle_curved_axisymmetric_matches_reference_sources(oracle_mod, order, bl):
+    _ref(oracle_mod)
+    mesh, u = make_golden.curved_axi_inputs((4, 3), order, bl, 0.3 if bl else 0.1, order)
+    kw = dict(quirks=0, bcs=make_golden.AXI_BCS, axisymmetric=1, blending=bl)
+    o = oracle_mod.Oracle(mesh, **kw).rhs(u)["dudt"]
+    r = oracle_mod.RefOperator(mesh, **kw).rhs(u)["dudt"]
+    assert normalized_error(o, r, 4) <= 1e-13
+
+
+@pytest.mark.parametrize("dim,order", [(2, 1), (2, 3), (3, 2), (3, 3)])
+def test_oracle_curved_free_stream(oracle_mod, dim, order):
+    """A uniform state on multilinear elements stays uniform (the metric
+    identities hold for the nodal adjugates: 2D for N >= 1, 3D for N >= 2)."""
+    mesh = periodic_box(dim, 3, order, 0.0, 1.0, warp=make_golden.warp_field(dim, 0.06))
+    u = cases.free_stream(mesh, rho=1.2, vel=[0.3, -0.2, 0.1][:dim], p=1.5)
+    for par in (0, 1):
+        d = oracle_mod.Oracle(mesh, quirks=1, parabolic=par).rhs(u)["dudt"]
+        assert np.abs(d).max() < 1e-12
