@@ -61,7 +61,8 @@ typedef enum prandtl_status {
 /* Mesh in the form the DGSEM kernels consume.  Built by the caller from its
  * mfem::ParMesh (per element: ElementTransformation::AdjugateJacobian and
  * Weight of the affine map from [0,1]^dim; per interior face:
- * FaceElementTransformations Elem1No/Elem2No, local faces and CalcOrtho). */
+ * FaceElementTransformations Elem1No/Elem2No, local faces and CalcOrtho;
+ * non-affine elements add the per-node values below). */
 typedef struct prandtl_mesh_desc {
     int dim;                   /* 2 or 3 */
     int order;                 /* polynomial degree N (1..5); Np = N + 1 Gauss-Lobatto nodes */
@@ -74,6 +75,19 @@ typedef struct prandtl_mesh_desc {
                                   face is {elem1, lface1, -1, bc} with bc an index into
                                   prandtl_config.bcs (Euler only) */
     const double *face_nor;    /* [F][dim] scaled normal outward from elem1 (|n| = face measure) */
+    /* Non-affine (multilinear) elements: all three set, or all three NULL for
+     * affine meshes.  MFEM evaluates the transformation at every Gauss-Lobatto
+     * node (ElementTransformation::SetIntPoint + AdjugateJacobian / Weight,
+     * DGSEMIntegrator.cpp:254-267, LiftingBR1.cpp:184-186) and CalcOrtho at
+     * every face point (DGSEMIntegrator.cpp:151-222); these arrays hold those
+     * values.  Only FP64 handles (prandtl_create, precision 0) take them:
+     * FP32-bulk handles, batches and prandtl_rhs_noalloc return
+     * PRANDTL_EUNSUPPORTED.  elem_adj / elem_detj / face_nor are still read
+     * (validation, the element size) and may hold the element-centre values. */
+    const double *node_adj;    /* [E][Np^dim][dim][dim] adj(J) at each node, row-major */
+    const double *node_detj;   /* [E][Np^dim] det J at each node (> 0) */
+    const double *face_node_nor; /* [F][Np^(dim-1)][dim] scaled normal at each face node,
+                                    outward from elem1, in elem1's face node order */
 } prandtl_mesh_desc;
 
 /* Boundary conditions of boundary faces (Euler), each the reference's
@@ -238,16 +252,20 @@ const char *prandtl_version(void);
  * Mesh(file)` for MFEM v1.0 meshes (with a `nodes` section of L2_T1 corner
  * nodes, MFEM's form of periodic meshes) and Gmsh 2.2 ASCII meshes,
  * `UniformRefinement()` per `ser_ref_levels`, and "mesh_ordering": "Hilbert".
- * Quadrilaterals / hexahedra, affine, of structured topology: each element's
- * local frame is chosen so that neighbouring faces are aligned; other meshes
- * get PRANDTL_EUNSUPPORTED with the reason in prandtl_mesh_last_error(). */
+ * Quadrilaterals / hexahedra of structured topology: each element's local
+ * frame is chosen so that neighbouring faces are aligned; other meshes get
+ * PRANDTL_EUNSUPPORTED with the reason in prandtl_mesh_last_error().  A mesh
+ * with any element that is not a parallelogram / parallelepiped is read with
+ * multilinear elements (MFEM's order-1 map of the corners): the descriptor
+ * then carries the per-node arrays (node_adj, node_detj, face_node_nor);
+ * refinement splits each element in its reference coordinates. */
 typedef struct prandtl_mesh prandtl_mesh;
 prandtl_status prandtl_mesh_read(const char *path, int order, int refine_levels, int hilbert,
                                  prandtl_mesh **out);
 /* Descriptor arrays, valid until prandtl_mesh_destroy.  Boundary faces are
  * {elem1, lface1, -1, attribute - 1} until prandtl_mesh_set_boundary_conditions.
- * hmin (may be NULL): smallest singular value of the element Jacobians, as
- * MFEM's GetElementSize(e, 1). */
+ * hmin (may be NULL): smallest singular value of the element Jacobians at the
+ * element centre, as MFEM's GetElementSize(e, 1). */
 prandtl_status prandtl_mesh_describe(const prandtl_mesh *m, prandtl_mesh_desc *desc, double *hmin);
 /* Boundary attribute of each descriptor face (0 for interior faces and for
  * boundary faces no boundary element names), num_faces entries. */

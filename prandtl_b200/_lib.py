@@ -48,7 +48,8 @@ class MeshDesc(C.Structure):
     _fields_ = [("dim", C.c_int), ("order", C.c_int), ("num_elements", C.c_int),
                 ("num_faces", C.c_int), ("elem_adj", C.POINTER(C.c_double)),
                 ("elem_detj", C.POINTER(C.c_double)), ("face_elems", C.POINTER(C.c_int)),
-                ("face_nor", C.POINTER(C.c_double))]
+                ("face_nor", C.POINTER(C.c_double)), ("node_adj", C.POINTER(C.c_double)),
+                ("node_detj", C.POINTER(C.c_double)), ("face_node_nor", C.POINTER(C.c_double))]
 
 
 class BC(C.Structure):

@@ -387,6 +387,8 @@ struct ElemIO {
     const double *rad;          // [Ndof] node radius r
     const unsigned char *axis;  // [Ndof] axis nodes
     unsigned int *health;       // RK modes: state-check bits (PRANDTL_HEALTH_*), may be null
+    // non-affine elements (one-shot FP64 kernels; MeshDev), null otherwise
+    const double *ngeo, *fnn, *snor;
 };
 // Per-warp (rhs) or per-CTA (lift) copy of the current solve's constants.
 struct __align__(16) WarpCtx {
@@ -419,6 +421,9 @@ __device__ __forceinline__ ElemIO io_from_args(const MeshDev &m, const RhsArgs &
     io.rad = m.rad;
     io.axis = m.axis;
     io.health = a.health;
+    io.ngeo = m.ngeo;
+    io.fnn = m.fnn;
+    io.snor = m.snor;
     return io;
 }
 
@@ -458,6 +463,7 @@ __device__ __forceinline__ ElemIO io_from_batch(const BatchInst &I, BatchInst *I
     io.rad = nullptr;
     io.axis = nullptr;
     io.health = &Im->health;
+    io.ngeo = io.fnn = io.snor = nullptr;
     return io;
 }
 
@@ -671,10 +677,11 @@ __device__ __forceinline__ unsigned state_health(const double *s, bool positivit
 // flux differencing, surface fluxes, gradients): double for the plain FP64
 // path, float for the FP32-bulk form.  Per-node primitives are always formed
 // in FP64 from the FP64 state, and the RK stage update is FP64.
-template <int DIM, int NP, bool NS, bool VC, typename Real, typename LY>
+template <int DIM, int NP, bool NS, bool VC, typename Real, typename LY, bool CURV = false>
 __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P, int e, bool active,
                                             const Real *sT, const uint32_t *sPair, Real *sH, int li, int lane,
                                             int gid) {
+    static_assert(!CURV || sizeof(Real) == 8, "non-affine elements: FP64 kernels only");
     using S = Shape<DIM, NP>;
     constexpr int ND = S::ND, NF = S::NF, PPL = S::PPL;
     constexpr int NFN = S::NFN, NFI = S::NFI, GS = LY::GS, NPL = LY::NPL;
@@ -698,6 +705,10 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
         for (int c2 = 0; c2 < DIM; ++c2) adj[r][c2] = Real(__ldg(geo + r * DIM + c2));
     const double J = __ldg(geo + DIM * DIM);
     const Real mJ = Real(1.0 / J);
+    // non-affine elements: the transformation at node n, component c = r DIM + q
+    // of adj(J) or c = DIM^2 for det J (Tr.SetIntPoint at the node,
+    // DGSEMIntegrator.cpp:254-267); the affine path uses adj / J above
+    auto ngeo = [&](int n, int c) -> double { return __ldg(a.ngeo + (long long)c * Ndof + (long long)e * ND + n); };
 
     // FP32-bulk form: reference pressure of the element (node 0), FP64.  The
     // shift cancels only where the volume operator annihilates a constant flux;
@@ -893,7 +904,11 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 // viscous flux with the state of node Np^d-1 (stale member id1).
                 const int src = (P.quirks == 0) ? ND - 1 : n;
                 const Prim<DIM, Real> q = load_prim<DIM, ND, Real>(sH, src);
-                Real Vc[DIM][NF];
+                Real Vc[DIM][NF], an[DIM][DIM];   // adj(J) at node n (:620-633)
+#pragma unroll
+                for (int r = 0; r < DIM; ++r)
+#pragma unroll
+                    for (int c2 = 0; c2 < DIM; ++c2) an[r][c2] = CURV ? Real(ngeo(n, r * DIM + c2)) : adj[r][c2];
 #pragma unroll
                 for (int r = 0; r < DIM; ++r)
 #pragma unroll
@@ -901,7 +916,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 viscous_flux<DIM, Real>(q.rho, q.rrho, q.v, Real(0.5) * q.rbeta * q.rho, dq, P,
                                         [&](int f, int cc, Real val) {
 #pragma unroll
-                                            for (int r = 0; r < DIM; ++r) Vc[r][f] += adj[r][cc] * val;
+                                            for (int r = 0; r < DIM; ++r) Vc[r][f] += an[r][cc] * val;
                                         });
 #pragma unroll
                 for (int r = 0; r < DIM; ++r)
@@ -1051,9 +1066,18 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
             for (int q = 0; q < DIM; ++q) mt[q] = adj[dir][q];
             for (int p = li; p < NPD; p += GS) {
                 const uint32_t pr = sPair[dir * NPD + p];
-                Real F[NF];
+                Real F[NF], mp[DIM];
+                if constexpr (CURV) {   // ComputeMean(metric1, metric2) of the pair's nodes
+#pragma unroll
+                    for (int q = 0; q < DIM; ++q)
+                        mp[q] = (Real(ngeo(int(pr & 0xffffu), dir * DIM + q)) + Real(ngeo(int(pr >> 16), dir * DIM + q))) *
+                                Real(0.5);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < DIM; ++q) mp[q] = mt[q];
+                }
                 volume_flux<DIM, Real>(load_prim<DIM, ND, Real>(sH, int(pr & 0xffffu)),
-                                       load_prim<DIM, ND, Real>(sH, int(pr >> 16)), mt, gm1i, F);
+                                       load_prim<DIM, ND, Real>(sH, int(pr >> 16)), mp, gm1i, F);
                 if (rad) {   // f *= r at the pair's reference midpoint (:273-291, :319-338)
                     const Real rh = Real(0.5 * (__ldg(rad + (long long)e * ND + int(pr & 0xffffu)) +
                                                 __ldg(rad + (long long)e * ND + int(pr >> 16))));
@@ -1082,11 +1106,13 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                             // eta line through (i, ., l); zero when j == Np-1.
                             if (c[1] != NP - 1) {
                                 Real F[NF], mg[DIM];
+                                const int na = (l * NP + c[1]) * NP + c[0], nb = (l * NP + NP - 1) * NP + c[0];
 #pragma unroll
-                                for (int q = 0; q < DIM; ++q) mg[q] = adj[1][q];
-                                volume_flux<DIM, Real>(load_prim<DIM, ND, Real>(sH, (l * NP + c[1]) * NP + c[0]),
-                                                       load_prim<DIM, ND, Real>(sH, (l * NP + NP - 1) * NP + c[0]), mg,
-                                                       gm1i, F);
+                                for (int q = 0; q < DIM; ++q)
+                                    mg[q] = CURV ? (Real(ngeo(na, DIM + q)) + Real(ngeo(nb, DIM + q))) * Real(0.5)
+                                                 : adj[1][q];
+                                volume_flux<DIM, Real>(load_prim<DIM, ND, Real>(sH, na),
+                                                       load_prim<DIM, ND, Real>(sH, nb), mg, gm1i, F);
 #pragma unroll
                                 for (int f = 0; f < NF; ++f) dUi[k][f] += dh * F[f];
                             }
@@ -1101,14 +1127,18 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
             group_sync<GS>(gid);
         }
 #pragma unroll
-        for (int k = 0; k < NPL; ++k)
+        for (int k = 0; k < NPL; ++k) {
+            const int n = li + k * GS;
+            // J = Tr.Weight() at the node (dU /= J)
+            const Real mJn = CURV ? Real(1.0 / (n < ND ? ngeo(n, DIM * DIM) : 1.0)) : mJ;
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 Real v = -dUi[k][f];
                 if (P.blending) v *= (Real(1) - alpha);
                 if (NS) v += dUv[k][f];
-                acc[k][f] = v * mJ;
+                acc[k][f] = v * mJn;
             }
+        }
     }
     if (rad) {   // + p on the radial momentum (DGSEMIntegrator.cpp:411-428), not blended
 #pragma unroll
@@ -1136,10 +1166,14 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 line_base<DIM, NP>(dir, ln, base, stride);
                 const int n1 = base + ii * stride, n2 = n1 + stride;
                 const Prim<DIM, Real> q1 = load_prim<DIM, ND, Real>(sH, n1), q2 = load_prim<DIM, ND, Real>(sH, n2);
-                Real s1[NF], s2[NF], F[NF];
+                Real s1[NF], s2[NF], F[NF], ni[DIM];
+#pragma unroll
+                for (int q = 0; q < DIM; ++q)   // non-affine: ComputeSubcellMetrics (:1199-1304)
+                    ni[q] = CURV ? Real(__ldg(a.snor + (((long long)e * DIM + dir) * S::NLINE * (NP - 1) + it) * DIM + q))
+                                 : nor[q];
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) { s1[1 + d] = q1.rho * q1.v[d]; s2[1 + d] = q2.rho * q2.v[d]; }
-                face_flux<DIM, Real>(s1, q1, s2, q2, nor, gm1i, P.quirks == 0, true, F);
+                face_flux<DIM, Real>(s1, q1, s2, q2, ni, gm1i, P.quirks == 0, true, F);
                 if (rad) {   // DGSEMIntegrator.cpp:979-1031, 1096-1111
                     const Real rh = Real(0.5 * (__ldg(rad + (long long)e * ND + n1) + __ldg(rad + (long long)e * ND + n2)));
 #pragma unroll
@@ -1157,7 +1191,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                     node_coords<NP>(n, c);
                     const int pos = c[dir];
                     const int ib = line_index<DIM, NP>(dir, c) * (NP - 1);
-                    const Real mw = Real(1.0 / (J * double(sW[pos])));
+                    const Real mw = Real(1.0 / ((CURV ? ngeo(n, DIM * DIM) : J) * double(sW[pos])));
 #pragma unroll
                     for (int f = 0; f < NF; ++f) {
                         Real v;
@@ -1195,7 +1229,9 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 #pragma unroll
         for (int f = 0; f < NF; ++f) x.s[f] = __ldg(a.u + f * Ndof + gs);
 #pragma unroll
-        for (int q = 0; q < DIM; ++q) x.nb[q] = __ldg(a.fnor + (long long)x.t.z * DIM + q);
+        for (int q = 0; q < DIM; ++q)   // non-affine: CalcOrtho at the face point
+            x.nb[q] = CURV ? __ldg(a.fnn + ((long long)x.t.z * NFN + fa) * DIM + q)
+                           : __ldg(a.fnor + (long long)x.t.z * DIM + q);
         if constexpr (NS && VC) {
             const int dd = lf >> 1, dn = x.t.x < 0 ? dd : x.t.y >> 1;
 #pragma unroll
@@ -1220,6 +1256,8 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
         const int no = face_node<DIM, NP>(lf, fa);
         const int4 t = x.t;
         const long long go = (long long)e * ND + no;
+        // 1 / (w0 J): non-affine elements take J at the face point (Elem1/Elem2 Weight())
+        const Real awn = CURV ? Real(1.0 / (double(sW[0]) * ngeo(no, DIM * DIM))) : aw;
         if (t.x < 0) {   // boundary face: the element is Elem1 (BdrFaceIntegrator.cpp:61-186)
             double sb[NF], nb[DIM];
             Real fb[NF], fv[NF];
@@ -1270,7 +1308,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 }
             }
 #pragma unroll
-            for (int f = 0; f < NF; ++f) sF[f * NFI + it] = aw * (fv[f] - fb[f]);
+            for (int f = 0; f < NF; ++f) sF[f * NFI + it] = awn * (fv[f] - fb[f]);
             continue;
         }
         const long long gn = (long long)t.x * ND + face_node<DIM, NP>(t.y, fa);
@@ -1358,7 +1396,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
             for (int f = 0; f < NF; ++f) flux[f] *= rr;
         }
 #pragma unroll
-        for (int f = 0; f < NF; ++f) sF[f * NFI + it] = aw * (own_is_1 ? (fn[f] - flux[f]) : (flux[f] - fn[f]));
+        for (int f = 0; f < NF; ++f) sF[f * NFI + it] = awn * (own_is_1 ? (fn[f] - flux[f]) : (flux[f] - fn[f]));
       }
     }
     group_sync<GS>(gid);
@@ -1440,8 +1478,9 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
     }
 }
 
-// One-shot kernel: grid = ceil(E / EPB), one element per lane group.
-template <int DIM, int NP, bool NS, bool VC, typename Real>
+// One-shot kernel: grid = ceil(E / EPB), one element per lane group.  CURV:
+// non-affine elements (per-node geometry, FP64).
+template <int DIM, int NP, bool NS, bool VC, typename Real, bool CURV>
 __global__ void __launch_bounds__(RhsLayout<DIM, NP, NS, Real, 0, VC>::THREADS, (RhsLayout<DIM, NP, NS, Real, 0, VC>::MIN_BLOCKS))
 rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_constant__ OpTables T) {
     using LY = RhsLayout<DIM, NP, NS, Real, 0, VC>;
@@ -1458,8 +1497,8 @@ rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_co
     const int e_raw = blockIdx.x * LY::EPB + grp;
     const bool active = e_raw < m.E;
     const ElemIO io = io_from_args(m, a);
-    rhs_element<DIM, NP, NS, VC, Real, LY>(io, P, active ? e_raw : m.E - 1, active, smem, sPair,
-                                           sE + grp * LY::PER_ELEM, li, lane, grp);
+    rhs_element<DIM, NP, NS, VC, Real, LY, CURV>(io, P, active ? e_raw : m.E - 1, active, smem, sPair,
+                                                 sE + grp * LY::PER_ELEM, li, lane, grp);
 }
 
 // Persistent batch kernel: a fixed grid walks the class's work items with a
@@ -1539,7 +1578,7 @@ rhs_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_consta
 // element's node 0 in FP32 with absolute middle entries).
 template <int DIM, typename W>
 __device__ __forceinline__ void boundary_lift_trace(const ElemIO &a, const PhysParams &P, const EntropyRef &R,
-                                                    long long g, const int4 t, W *vn) {
+                                                    long long g, const int4 t, W *vn, const double *nor) {
     constexpr int NF = DIM + 2;
     constexpr bool F64 = sizeof(W) == 8;
     const BcDev &bc = a.bcs[t.y];
@@ -1547,8 +1586,8 @@ __device__ __forceinline__ void boundary_lift_trace(const ElemIO &a, const PhysP
 #pragma unroll
     for (int f = 0; f < NF; ++f) s1[f] = __ldg(a.u + f * a.Ndof + g);
 #pragma unroll
-    for (int q = 0; q < DIM; ++q) {
-        nb[q] = __ldg(a.fnor + (long long)t.z * DIM + q);
+    for (int q = 0; q < DIM; ++q) {   // nor: the face's scaled normal (per face node on non-affine meshes)
+        nb[q] = __ldg(nor + q);
         nn += nb[q] * nb[q];
     }
     nn = sqrt(nn);
@@ -1581,17 +1620,19 @@ __device__ __forceinline__ void boundary_lift_trace(const ElemIO &a, const PhysP
     }
 }
 
-template <int DIM, int NP, typename W, bool VC>
+template <int DIM, int NP, typename W, bool VC, bool CURV = false>
 __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &P, int e, bool active,
                                              const W *sT, W *sElem, int n) {
     using S = Shape<DIM, NP>;
     constexpr int ND = S::ND, NF = S::NF, NFN = S::NFN, NFI = S::NFI;
     constexpr bool F64 = sizeof(W) == 8;
+    static_assert(!CURV || F64, "non-affine elements: FP64 kernels only");
     const W *sD = sT, *sW = sT + 4 * NP * NP;
     W *gout = reinterpret_cast<W *>(a.grad);
     W *sVe = sElem;                 // entropy variables [NF][ND]
     W *sS = sVe + NF * ND;          // face jumps [NF][NFI]
-    W *sN = sS + NF * NFI;          // face normals [2 DIM][DIM] (one per local face)
+    W *sN = sS + NF * NFI;          // face normals [2 DIM][DIM] (one per local face);
+                                    // non-affine: [NFI][DIM] (one per face node)
     const long long Ndof = a.Ndof;
     const long long gnode = (long long)e * ND + n;
     // FP64: this thread's face items' neighbour-table entries and interior
@@ -1634,13 +1675,16 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
     }
 #pragma unroll
     for (int f = 0; f < NF; ++f) sVe[f * ND + n] = v[f];
+    // the transformation: per element, or (non-affine) at this thread's node
+    // (LiftingBR1.cpp:184-186: Tr.SetIntPoint, Weight, AdjugateJacobian)
     const double *geo = a.geo + (long long)e * (DIM * DIM + 1);
     W adj[DIM][DIM];
 #pragma unroll
     for (int r = 0; r < DIM; ++r)
 #pragma unroll
-        for (int q = 0; q < DIM; ++q) adj[r][q] = W(__ldg(geo + r * DIM + q));
-    const double J = __ldg(geo + DIM * DIM);
+        for (int q = 0; q < DIM; ++q)
+            adj[r][q] = W(CURV ? __ldg(a.ngeo + (long long)(r * DIM + q) * Ndof + gnode) : __ldg(geo + r * DIM + q));
+    const double J = CURV ? __ldg(a.ngeo + (long long)(DIM * DIM) * Ndof + gnode) : __ldg(geo + DIM * DIM);
     int c[3];
     node_coords<NP>(n, c);
 
@@ -1657,11 +1701,13 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
             const int lf = it / NFN, fa = it - lf * NFN;
             no[k] = face_node<DIM, NP>(lf, fa);
             const int4 t = F64 ? tk[k] : __ldg(a.nbr + (long long)e * (2 * DIM) + lf);
+            // the scaled normal: per face, or (non-affine) CalcOrtho at this face point
+            const double *fn = CURV ? a.fnn + ((long long)t.z * NFN + fa) * DIM : a.fnor + (long long)t.z * DIM;
 #pragma unroll
-            for (int q = 0; q < DIM; ++q) nor[k][q] = W(__ldg(a.fnor + (long long)t.z * DIM + q));
+            for (int q = 0; q < DIM; ++q) nor[k][q] = W(__ldg(fn + q));
             own1[k] = (t.w == 0);
             if (t.x < 0) {
-                boundary_lift_trace<DIM, W>(a, P, R, e * (long long)ND + no[k], t, vn[k]);
+                boundary_lift_trace<DIM, W>(a, P, R, e * (long long)ND + no[k], t, vn[k], fn);
                 continue;
             }
             if constexpr (F64) {
@@ -1688,9 +1734,9 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
                 const W vo = sVe[f * ND + no[k]];
                 sS[f * NFI + it] = own1[k] ? W(0.5) * (vn[k][f] - vo) : W(0.5) * (vo - vn[k][f]);
             }
-            if (it % NFN == 0) {
+            if (CURV || it % NFN == 0) {
 #pragma unroll
-                for (int q = 0; q < DIM; ++q) sN[(it / NFN) * DIM + q] = nor[k][q];
+                for (int q = 0; q < DIM; ++q) sN[(CURV ? it : it / NFN) * DIM + q] = nor[k][q];
             }
         }
     }
@@ -1736,7 +1782,7 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
 #pragma unroll
             for (int f = 0; f < NF; ++f) jf[f] = sS[f * NFI + it];
 #pragma unroll
-            for (int q = 0; q < DIM; ++q) nq[q] = sN[lf * DIM + q];
+            for (int q = 0; q < DIM; ++q) nq[q] = sN[(CURV ? it : lf) * DIM + q];
 #pragma unroll
             for (int q = 0; q < DIM; ++q)
 #pragma unroll
@@ -1777,10 +1823,10 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
     }
 }
 
-template <int DIM, int NP>
+template <int DIM, int NP, bool CURV = false>
 struct LiftLayout {
     using S = Shape<DIM, NP>;
-    static constexpr int PER_ELEM = S::NF * S::ND + S::NF * S::NFI + 2 * DIM * DIM;
+    static constexpr int PER_ELEM = S::NF * S::ND + S::NF * S::NFI + (CURV ? S::NFI * DIM : 2 * DIM * DIM);
 };
 constexpr int prev_pow2(int v) { return v <= 1 ? 1 : 2 * prev_pow2(v / 2); }
 // Batch lift CTA: a power-of-two number of elements, so an item (one CTA's
@@ -1803,7 +1849,7 @@ struct LiftBatchShape {
 template <int NP, typename Out>
 constexpr int lift_min_blocks() { return NP <= 4 ? (sizeof(Out) == 8 ? PRANDTL_LIFT64_MINB : 6) : 4; }
 
-template <int DIM, int NP, typename Out, bool VC>
+template <int DIM, int NP, typename Out, bool VC, bool CURV>
 __global__ void __launch_bounds__(Shape<DIM, NP>::THREADS, lift_min_blocks<NP, Out>())
 lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_constant__ OpTables T) {
     using S = Shape<DIM, NP>;
@@ -1826,8 +1872,11 @@ lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_
     io.u_rk = nullptr;
     io.rad = nullptr;
     io.axis = nullptr;
-    lift_element<DIM, NP, Out, VC>(io, P, active ? e_raw : m.E - 1, active, smem,
-                               smem + S::TAB + el * LiftLayout<DIM, NP>::PER_ELEM, n);
+    io.ngeo = m.ngeo;
+    io.fnn = m.fnn;
+    io.snor = nullptr;
+    lift_element<DIM, NP, Out, VC, CURV>(io, P, active ? e_raw : m.E - 1, active, smem,
+                                         smem + S::TAB + el * LiftLayout<DIM, NP, CURV>::PER_ELEM, n);
 }
 
 // Persistent batch lift: CTA-level items of EPB elements of one solve.
@@ -1879,10 +1928,10 @@ size_t rhs_batch_smem() {
     using LY = RhsLayout<DIM, NP, NS, Real, V, VC>;
     return LY::FIXED_BYTES + sizeof(Real) * (size_t)LY::EPB * LY::PER_ELEM;
 }
-template <int DIM, int NP, typename Out>
+template <int DIM, int NP, typename Out, bool CURV>
 size_t lift_smem() {
     using S = Shape<DIM, NP>;
-    return sizeof(Out) * (S::TAB + (size_t)S::EPB * LiftLayout<DIM, NP>::PER_ELEM);
+    return sizeof(Out) * (S::TAB + (size_t)S::EPB * LiftLayout<DIM, NP, CURV>::PER_ELEM);
 }
 template <int DIM, int NP, typename Out>
 size_t lift_batch_smem() {
@@ -1891,29 +1940,48 @@ size_t lift_batch_smem() {
            sizeof(Out) * (size_t)LiftBatchShape<DIM, NP>::EPB * LiftLayout<DIM, NP>::PER_ELEM;
 }
 
-template <int DIM, int NP, bool NS, bool VC, typename Real>
+template <int DIM, int NP, bool NS, bool VC, typename Real, bool CURV>
 cudaError_t rhs_launch_np(const MeshDev &m, const RhsArgs &a, const PhysParams &P, const OpTables &T,
                           cudaStream_t s) {
     using LY = RhsLayout<DIM, NP, NS, Real, 0, VC>;
     const int grid = (m.E + LY::EPB - 1) / LY::EPB;
     const size_t sm = rhs_smem<DIM, NP, NS, VC, Real>();
-    cudaError_t err = cudaFuncSetAttribute(rhs_kernel<DIM, NP, NS, VC, Real>,
+    cudaError_t err = cudaFuncSetAttribute(rhs_kernel<DIM, NP, NS, VC, Real, CURV>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (err != cudaSuccess) return err;
-    rhs_kernel<DIM, NP, NS, VC, Real><<<grid, LY::THREADS, sm, s>>>(m, a, P, T);
+    rhs_kernel<DIM, NP, NS, VC, Real, CURV><<<grid, LY::THREADS, sm, s>>>(m, a, P, T);
     return cudaGetLastError();
 }
-template <int DIM, int NP, typename Out, bool VC>
+// non-affine meshes (m.ngeo set) run the per-node-geometry kernels, FP64 only
+template <int DIM, int NP, bool NS, bool VC, typename Real>
+cudaError_t rhs_launch_any(const MeshDev &m, const RhsArgs &a, const PhysParams &P, const OpTables &T,
+                           cudaStream_t s) {
+    if (m.ngeo) {
+        if constexpr (sizeof(Real) == 8) return rhs_launch_np<DIM, NP, NS, VC, Real, true>(m, a, P, T, s);
+        else return cudaErrorNotSupported;
+    }
+    return rhs_launch_np<DIM, NP, NS, VC, Real, false>(m, a, P, T, s);
+}
+template <int DIM, int NP, typename Out, bool VC, bool CURV>
 cudaError_t lift_launch_np(const MeshDev &m, const LiftArgs &a, const PhysParams &P, const OpTables &T,
                            cudaStream_t s) {
     using S = Shape<DIM, NP>;
     const int grid = (m.E + S::EPB - 1) / S::EPB;
-    const size_t sm = lift_smem<DIM, NP, Out>();
-    cudaError_t err = cudaFuncSetAttribute(lift_kernel<DIM, NP, Out, VC>,
+    const size_t sm = lift_smem<DIM, NP, Out, CURV>();
+    cudaError_t err = cudaFuncSetAttribute(lift_kernel<DIM, NP, Out, VC, CURV>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (err != cudaSuccess) return err;
-    lift_kernel<DIM, NP, Out, VC><<<grid, S::THREADS, sm, s>>>(m, a, P, T);
+    lift_kernel<DIM, NP, Out, VC, CURV><<<grid, S::THREADS, sm, s>>>(m, a, P, T);
     return cudaGetLastError();
+}
+template <int DIM, int NP, typename Out, bool VC>
+cudaError_t lift_launch_any(const MeshDev &m, const LiftArgs &a, const PhysParams &P, const OpTables &T,
+                            cudaStream_t s) {
+    if (m.ngeo) {
+        if constexpr (sizeof(Out) == 8) return lift_launch_np<DIM, NP, Out, VC, true>(m, a, P, T, s);
+        else return cudaErrorNotSupported;
+    }
+    return lift_launch_np<DIM, NP, Out, VC, false>(m, a, P, T, s);
 }
 
 // Batch kernels: `prepare` sets the shared-memory attribute (outside any stream
@@ -1993,12 +2061,12 @@ cudaError_t lift_batch_launch_np(int grid, const BatchClassDev &c, const BatchSt
 template <int DIM, typename Real, bool NS, bool VC>
 cudaError_t rhs_dispatch(int order, const MeshDev &m, const RhsArgs &a, const PhysParams &P,
                          const OpTables &T, cudaStream_t s) {
-    PRANDTL_ORDER_SWITCH((rhs_launch_np<DIM, NP, NS, VC, Real>(m, a, P, T, s)))
+    PRANDTL_ORDER_SWITCH((rhs_launch_any<DIM, NP, NS, VC, Real>(m, a, P, T, s)))
 }
 template <int DIM, typename Out, bool VC>
 cudaError_t lift_dispatch(int order, const MeshDev &m, const LiftArgs &a, const PhysParams &P,
                           const OpTables &T, cudaStream_t s) {
-    PRANDTL_ORDER_SWITCH((lift_launch_np<DIM, NP, Out, VC>(m, a, P, T, s)))
+    PRANDTL_ORDER_SWITCH((lift_launch_any<DIM, NP, Out, VC>(m, a, P, T, s)))
 }
 template <int DIM, typename Real, bool NS, bool VC>
 cudaError_t rhs_batch_prepare(int order, int variant, BatchKernelInfo *info) {

@@ -206,7 +206,8 @@ struct Weights1D {
 template <int NOUT>
 __global__ void __launch_bounds__(BUDGET_THREADS) budget_kernel(const double *__restrict__ u,
                                                                const double *__restrict__ dudt,
-                                                               const double *__restrict__ geo, Weights1D W,
+                                                               const double *__restrict__ geo,
+                                                               const double *__restrict__ ndetj, Weights1D W,
                                                                int dim, int np, int E, double gamma,
                                                                double *__restrict__ partials) {
     constexpr int MAXF = (NOUT - 2) / 2;
@@ -220,7 +221,7 @@ __global__ void __launch_bounds__(BUDGET_THREADS) budget_kernel(const double *__
         const int e = (int)(g / nd), n = (int)(g - (long long)e * nd);
         double wn = W.w[n % np] * W.w[(n / np) % np];
         if (dim == 3) wn *= W.w[n / (np * np)];
-        const double wJ = wn * fabs(geo[(long long)e * (dim * dim + 1) + dim * dim]);
+        const double wJ = wn * fabs(ndetj ? ndetj[g] : geo[(long long)e * (dim * dim + 1) + dim * dim]);
         double s[MAXF], r[MAXF];
 #pragma unroll
         for (int f = 0; f < MAXF; ++f) {
@@ -274,8 +275,9 @@ __global__ void budget_final_kernel(const double *__restrict__ partials, int blo
 }
 }   // namespace
 
-cudaError_t launch_budgets(const double *u, const double *dudt, const double *geo, const double *w1d, int dim,
-                           int np, int E, double gamma, double *partials, double *out, cudaStream_t s) {
+cudaError_t launch_budgets(const double *u, const double *dudt, const double *geo, const double *ndetj,
+                           const double *w1d, int dim, int np, int E, double gamma, double *partials, double *out,
+                           cudaStream_t s) {
     if (np < 2 || np > 8 || (dim != 2 && dim != 3) || E <= 0) return cudaErrorInvalidValue;
     Weights1D W{};
     for (int i = 0; i < np; ++i) W.w[i] = w1d[i];
@@ -284,7 +286,7 @@ cudaError_t launch_budgets(const double *u, const double *dudt, const double *ge
     if (blocks > BUDGET_BLOCKS) blocks = BUDGET_BLOCKS;
     // outputs: nf conserved integrals, entropy, nf rate integrals, entropy rate
     constexpr int NOUT = 2 * 5 + 2;
-    budget_kernel<NOUT><<<(unsigned)blocks, BUDGET_THREADS, 0, s>>>(u, dudt, geo, W, dim, np, E, gamma, partials);
+    budget_kernel<NOUT><<<(unsigned)blocks, BUDGET_THREADS, 0, s>>>(u, dudt, geo, ndetj, W, dim, np, E, gamma, partials);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     budget_final_kernel<<<1, 32, 0, s>>>(partials, (int)blocks, NOUT, out);

@@ -26,6 +26,14 @@ struct MeshDev {
     // axisymmetric (z, r) form, 2D Euler (null otherwise)
     const double *rad;            // [Ndof] node radius
     const unsigned char *axis;    // [Ndof] 1 at axis nodes
+    // non-affine (multilinear) elements, FP64 one-shot kernels (null otherwise):
+    // the transformation at every node, [DIM*DIM + 1][Ndof] (adj(J) row-major,
+    // then det J); the scaled normal at every face node, [F][Np^(DIM-1)][DIM]
+    // (elem1's face node order); the subcell interface normals of every line,
+    // [E][DIM][Np^(DIM-1)][Np-1][DIM] (interior interfaces 1..Np-1)
+    const double *ngeo;
+    const double *fnn;
+    const double *snor;
 };
 
 struct RhsArgs {
@@ -131,11 +139,13 @@ cudaError_t batch_launch_lift(int dim, int order, bool vc, bool fp32, int grid, 
 // of the nf conserved fields and of the entropy function U = -rho s / (g-1),
 // s = ln(p rho^-g); with dudt also the integrals of dudt_f and of v . dudt
 // (v the entropy variables).  nout = 2 nf + 2 values; deterministic two-pass
-// reduction through `partials` ([BUDGET_BLOCKS][nout]).
+// reduction through `partials` ([BUDGET_BLOCKS][nout]).  ndetj (non-affine
+// elements, may be null): det J at every node instead of the element's.
 constexpr int BUDGET_BLOCKS = 592;    // 4 per SM on 148 SMs (grid-stride beyond)
 constexpr int BUDGET_THREADS = 256;
-cudaError_t launch_budgets(const double *u, const double *dudt, const double *geo, const double *w1d, int dim,
-                           int np, int E, double gamma, double *partials, double *out, cudaStream_t s);
+cudaError_t launch_budgets(const double *u, const double *dudt, const double *geo, const double *ndetj,
+                           const double *w1d, int dim, int np, int E, double gamma, double *partials, double *out,
+                           cudaStream_t s);
 
 // Axisymmetric form: U recovered from the weighted state rU (2D, 4 fields).
 cudaError_t launch_axi_recover(const double *rU, double *U, const double *xy, const unsigned char *axis,

@@ -340,6 +340,142 @@ inline prandtl_status check_face_normals(const prandtl_mesh_desc *md, std::strin
     return PRANDTL_OK;
 }
 
+// ---- non-affine (multilinear) elements: per-node geometry
+inline bool mesh_curved(const prandtl_mesh_desc *md) { return md->node_adj != nullptr; }
+
+// All three per-node arrays or none; det J > 0 and every value finite.
+inline prandtl_status check_curved(const prandtl_mesh_desc *md, std::string &msg) {
+    const int n = (md->node_adj != nullptr) + (md->node_detj != nullptr) + (md->face_node_nor != nullptr);
+    if (n == 0) return PRANDTL_OK;
+    if (n != 3) {
+        msg = "node_adj, node_detj and face_node_nor: all three or none";
+        return PRANDTL_EINVAL;
+    }
+    const int dim = md->dim, Np = md->order + 1;
+    int nd = 1;
+    for (int d = 0; d < dim; ++d) nd *= Np;
+    const int nfn = nd / Np;
+    const size_t N = (size_t)md->num_elements * nd;
+    for (size_t i = 0; i < N; ++i)
+        if (!(md->node_detj[i] > 0.0) || !std::isfinite(md->node_detj[i])) {
+            msg = "node_detj[" + std::to_string(i) + "] is not a positive finite value (inverted element)";
+            return PRANDTL_EINVAL;
+        }
+    for (size_t i = 0; i < N * dim * dim; ++i)
+        if (!std::isfinite(md->node_adj[i])) {
+            msg = "node_adj holds a non-finite value";
+            return PRANDTL_EINVAL;
+        }
+    for (size_t i = 0; i < (size_t)md->num_faces * nfn * dim; ++i)
+        if (!std::isfinite(md->face_node_nor[i])) {
+            msg = "face_node_nor holds a non-finite value";
+            return PRANDTL_EINVAL;
+        }
+    return PRANDTL_OK;
+}
+
+// Element-local node of face node a on local face lf = 2 dir + side (face nodes
+// lexicographic over the remaining directions, the lower one fastest).
+inline int host_face_node(int dim, int Np, int lf, int a) {
+    const int d = lf >> 1, s = lf & 1;
+    int c[3] = {0, 0, 0};
+    c[d] = s * (Np - 1);
+    if (dim == 2) {
+        c[1 - d] = a;
+    } else {
+        const int t0 = (d == 0) ? 1 : 0, t1 = (d == 2) ? 1 : 2;
+        c[t0] = a % Np;
+        c[t1] = a / Np;
+    }
+    return c[0] + Np * (c[1] + Np * c[2]);
+}
+
+// Per-node geometry, structure of arrays [dim*dim + 1][Ndof]: adj(J) entries
+// (row-major index r*dim + q), then det J.
+inline std::vector<double> node_geometry_soa(const prandtl_mesh_desc *md) {
+    const int dim = md->dim, Np = md->order + 1, G = dim * dim + 1;
+    int nd = 1;
+    for (int d = 0; d < dim; ++d) nd *= Np;
+    const size_t Ndof = (size_t)md->num_elements * nd;
+    std::vector<double> g(G * Ndof);
+    for (size_t n = 0; n < Ndof; ++n) {
+        for (int c = 0; c < dim * dim; ++c) g[c * Ndof + n] = md->node_adj[n * dim * dim + c];
+        g[(size_t)(dim * dim) * Ndof + n] = md->node_detj[n];
+    }
+    return g;
+}
+
+// Subcell interface normals (DGSEMIntegrator.cpp:1199-1304): for direction dir
+// and line ln (the kernels' line_base numbering), interface i = 1..Np-1 has
+// Ja_dir(first node) + sum_{l<i} w_l sum_m D(l,m) Ja_dir(node m), Ja_dir = row
+// dir of adj(J).  Layout [E][dim][Np^(dim-1)][Np-1][dim].
+inline std::vector<double> subcell_normals(const prandtl_mesh_desc *md, const OpTables &T) {
+    const int dim = md->dim, Np = md->order + 1;
+    int nd = 1;
+    for (int d = 0; d < dim; ++d) nd *= Np;
+    const int nline = nd / Np;
+    std::vector<double> out((size_t)md->num_elements * dim * nline * (Np - 1) * dim);
+    size_t o = 0;
+    for (int e = 0; e < md->num_elements; ++e)
+        for (int dir = 0; dir < dim; ++dir)
+            for (int ln = 0; ln < nline; ++ln) {
+                int base, stride;
+                if (dir == 0) { base = ln * Np; stride = 1; }
+                else if (dim == 2) { base = ln; stride = Np; }
+                else if (dir == 1) { base = (ln / Np) * Np * Np + ln % Np; stride = Np; }
+                else { base = ln; stride = Np * Np; }
+                auto Ja = [&](int m, int c) {
+                    return md->node_adj[(((size_t)e * nd + base + m * stride) * dim + dir) * dim + c];
+                };
+                for (int i = 1; i < Np; ++i) {
+                    double nor[3], tmp[3];
+                    for (int c = 0; c < dim; ++c) nor[c] = Ja(0, c);
+                    for (int l = 0; l < i; ++l) {
+                        for (int c = 0; c < dim; ++c) tmp[c] = 0.0;
+                        for (int m = 0; m < Np; ++m)
+                            for (int c = 0; c < dim; ++c) tmp[c] += Ja(m, c) * T.D[l * Np + m];
+                        for (int c = 0; c < dim; ++c) nor[c] += tmp[c] * T.w[l];
+                    }
+                    for (int c = 0; c < dim; ++c) out[o++] = nor[c];
+                }
+            }
+    return out;
+}
+
+// The contravariant viscous form takes Fv . n at a face node from the node's
+// row of adj(J) Fv^T, which needs the face normal to be that row (Nanson's
+// formula) on both sides: per face node on non-affine meshes.
+inline prandtl_status check_face_node_normals(const prandtl_mesh_desc *md, std::string &msg) {
+    const int dim = md->dim, Np = md->order + 1;
+    int nd = 1;
+    for (int d = 0; d < dim; ++d) nd *= Np;
+    const int nfn = nd / Np;
+    for (int f = 0; f < md->num_faces; ++f) {
+        const int *fe = md->face_elems + 4 * f;
+        for (int a = 0; a < nfn; ++a) {
+            const double *nor = md->face_node_nor + ((size_t)f * nfn + a) * dim;
+            for (int side = 0; side < 2; ++side) {
+                const int e = fe[2 * side], lf = fe[2 * side + 1], d = lf >> 1;
+                if (e < 0) continue;
+                const double sg = ((lf & 1) ? 1.0 : -1.0) * (side == 0 ? 1.0 : -1.0);
+                const int n = host_face_node(dim, Np, lf, a);
+                const double *row = md->node_adj + (((size_t)e * nd + n) * dim + d) * dim;
+                double err = 0, mag = 0;
+                for (int c = 0; c < dim; ++c) {
+                    err = std::fmax(err, std::fabs(nor[c] - sg * row[c]));
+                    mag = std::fmax(mag, std::fabs(row[c]));
+                }
+                if (!(err <= 1e-9 * mag)) {
+                    msg = "face " + std::to_string(f) + " node " + std::to_string(a) +
+                          ": scaled normal differs from the element's adjugate row there";
+                    return PRANDTL_EUNSUPPORTED;
+                }
+            }
+        }
+    }
+    return PRANDTL_OK;
+}
+
 // Geometry rows [E][dim*dim + 1]: adj(J) row-major, then det J.
 inline std::vector<double> geometry_rows(const prandtl_mesh_desc *md) {
     const int dim = md->dim, GEO = dim * dim + 1, E = md->num_elements;

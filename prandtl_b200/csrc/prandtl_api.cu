@@ -50,6 +50,9 @@ struct prandtl_handle {
     unsigned char *d_axis = nullptr;
     double *d_U = nullptr;
     double *d_budget = nullptr;                   // budget partials [BUDGET_BLOCKS][12] + totals [12]
+    // non-affine elements: per-node geometry [dim*dim + 1][Ndof], per-face-node
+    // normals [F][Np^(dim-1)][dim], subcell interface normals (blending)
+    double *d_ngeo = nullptr, *d_fnn = nullptr, *d_snor = nullptr;
     size_t bytes = 0;
     long long launches = 0;
     // optional per-kernel CUDA-event timing (prandtl_profile)
@@ -138,6 +141,9 @@ MeshDev mesh_dev(const prandtl_handle *h) {
     m.bcs = h->d_bcs;
     m.rad = h->d_xy ? h->d_xy + h->Ndof : nullptr;
     m.axis = h->d_axis;
+    m.ngeo = h->d_ngeo;
+    m.fnn = h->d_fnn;
+    m.snor = h->d_snor;
     return m;
 }
 
@@ -196,6 +202,9 @@ void free_all(prandtl_handle *h) {
     cudaFree(h->d_axis);
     cudaFree(h->d_U);
     cudaFree(h->d_budget);
+    cudaFree(h->d_ngeo);
+    cudaFree(h->d_fnn);
+    cudaFree(h->d_snor);
     if (h->done) cudaEventDestroy(h->done);
     for (auto &r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (auto ev : h->ev_pool) cudaEventDestroy(ev);
@@ -250,7 +259,13 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
         prandtl_status vst = check_bcs(cfg, md->dim, msg);
         if (vst == PRANDTL_OK) vst = validate_mesh(md, nbr, msg, cfg->num_bcs);
         if (vst == PRANDTL_OK) vst = check_viscous_bcs(md, cfg, msg);
-        if (vst == PRANDTL_OK && cfg->parabolic && cfg->quirks != 0) vst = check_face_normals(md, msg);
+        if (vst == PRANDTL_OK) vst = check_curved(md, msg);
+        if (vst == PRANDTL_OK && mesh_curved(md) && cfg->precision != 0) {
+            msg = "non-affine elements run in the FP64 form only (precision 0)";
+            vst = PRANDTL_EUNSUPPORTED;
+        }
+        if (vst == PRANDTL_OK && cfg->parabolic && cfg->quirks != 0)
+            vst = mesh_curved(md) ? check_face_node_normals(md, msg) : check_face_normals(md, msg);
         if (vst != PRANDTL_OK) return fail(nullptr, vst, msg);
     }
 
@@ -328,6 +343,23 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
         return bail(cuda_fail(h, ce, "upload normals"));
     if ((ce = cudaMemset(h->d_alpha, 0, (size_t)E * sizeof(double))) != cudaSuccess)
         return bail(cuda_fail(h, ce, "memset alpha"));
+    if (mesh_curved(md)) {   // per-node geometry of non-affine elements
+        const std::vector<double> ng = node_geometry_soa(md);
+        const size_t nfn_all = (size_t)(F > 0 ? F : 1) * (h->nd / h->Np) * dim;
+        if ((st = dalloc(h, &h->d_ngeo, ng.size(), "node geometry")) != PRANDTL_OK) return bail(st);
+        if ((st = dalloc(h, &h->d_fnn, nfn_all, "face node normals")) != PRANDTL_OK) return bail(st);
+        if ((ce = cudaMemcpy(h->d_ngeo, ng.data(), ng.size() * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail(cuda_fail(h, ce, "upload node geometry"));
+        if (F > 0 && (ce = cudaMemcpy(h->d_fnn, md->face_node_nor, (size_t)F * (h->nd / h->Np) * dim * sizeof(double),
+                                      cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail(cuda_fail(h, ce, "upload face node normals"));
+        if (cfg->blending) {
+            const std::vector<double> sn = subcell_normals(md, h->T);
+            if ((st = dalloc(h, &h->d_snor, sn.size(), "subcell normals")) != PRANDTL_OK) return bail(st);
+            if ((ce = cudaMemcpy(h->d_snor, sn.data(), sn.size() * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess)
+                return bail(cuda_fail(h, ce, "upload subcell normals"));
+        }
+    }
     if (cfg->axisymmetric) {
         // DGSEMOperator::BuildAxisIndexFromMarker (DGSEMOperator.cpp:482-518):
         // nodes at |r| <= 1e-14 of the elements on axis boundary faces
@@ -521,7 +553,9 @@ prandtl_status prandtl_budgets(prandtl_handle *h, const double *u, const double 
         }
     }
     double *tot = h->d_budget + (size_t)BUDGET_BLOCKS * 12;
-    CK(h, launch_budgets(ud, dd, h->d_geo, h->T.w, h->dim, h->Np, h->E, h->cfg.gamma, h->d_budget, tot, h->stream),
+    const double *ndetj = h->d_ngeo ? h->d_ngeo + (size_t)(h->dim * h->dim) * h->Ndof : nullptr;
+    CK(h, launch_budgets(ud, dd, h->d_geo, ndetj, h->T.w, h->dim, h->Np, h->E, h->cfg.gamma, h->d_budget, tot,
+                         h->stream),
        "budget kernel launch");
     h->launches += 2;
     double buf[12];

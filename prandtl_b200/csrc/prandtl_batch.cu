@@ -494,6 +494,10 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, 
         st = PRANDTL_EUNSUPPORTED;
         msg = "the axisymmetric form runs on a prandtl_create operator, not in a batch";
     }
+    if (st == PRANDTL_OK && (md->node_adj || md->node_detj || md->face_node_nor)) {
+        st = PRANDTL_EUNSUPPORTED;
+        msg = "non-affine elements run on a prandtl_create FP64 operator, not in a batch";
+    }
     if (st != PRANDTL_OK) return bfail(b, st, msg);
     BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
     const int dim = md->dim, order = md->order, E = md->num_elements, F = md->num_faces;
@@ -726,7 +730,8 @@ prandtl_status prandtl_batch_budgets(prandtl_batch *b, int id, double *out) {
     const OpTables &T = b->classes.at(s.key).T;
     double *tot = b->d_budget + (size_t)BUDGET_BLOCKS * 12;
     BCK(b, launch_budgets(reinterpret_cast<const double *>(base + s.L.u[cur & 1]), nullptr,
-                          reinterpret_cast<const double *>(base + s.L.geo), T.w, s.dim, s.order + 1, s.E, s.gamma,
+                          reinterpret_cast<const double *>(base + s.L.geo), nullptr, T.w, s.dim, s.order + 1, s.E,
+                          s.gamma,
                           b->d_budget, tot, b->stream),
         "budget kernel launch");
     b->launches += 2;

@@ -19,9 +19,13 @@
 //    the same tangential axes.  A breadth-first walk fixes each neighbour's
 //    frame from the shared face's vertex ids; meshes without such a frame (not
 //    structured-topology) are rejected.
-//  * geometry: affine elements only (parallelograms / parallelepipeds); the
-//    scaled face normal of an affine element is the signed adjugate row of its
-//    face direction (Nanson), which is what MFEM's CalcOrtho returns there.
+//  * geometry: affine elements (parallelograms / parallelepipeds) give one
+//    adjugate and determinant per element; any other quadrilateral /
+//    hexahedron is the multilinear map of its corners (MFEM's order-1
+//    transformation), evaluated at every Gauss-Lobatto node.  The scaled face
+//    normal is the signed adjugate row of the face direction (Nanson), per
+//    face or, on multilinear elements, per face node: what MFEM's CalcOrtho
+//    returns there.
 //  * uniform refinement (2^dim children per element, the aligned frames carry
 //    over) and Hilbert-curve element ordering of the element centroids.
 //
@@ -46,6 +50,11 @@ struct prandtl_mesh {
     int dim = 0, order = 0;
     // oriented affine elements: x = X0 + J xi, xi in [0,1]^dim
     std::vector<double> X0, J;   // [E][dim], [E][dim][dim] with J[i][r] = dx_i / dxi_r
+    // multilinear elements (some element is not affine): the oriented corners
+    // [E][2^dim][dim], corner b at reference vertex (b & 1, b >> 1 & 1, b >> 2 & 1)
+    bool multilinear = false;
+    std::vector<double> Xc;
+    std::vector<double> nadj, ndetj, fnn;   // descriptor per-node arrays (multilinear)
     std::vector<int> attr;       // element attributes
     // neighbour of local face lf = 2d+s: element (or -1) and its local face, or
     // the boundary attribute (0 = a boundary face no boundary element names)
@@ -478,9 +487,13 @@ prandtl_status orient(const Raw &R, prandtl_mesh &M) {
             }
         }
     }
-    // geometry in the chosen frames
+    // geometry in the chosen frames: X0 + J xi from corners 0 and 1 << r, and
+    // the corners themselves for the multilinear map when any element is not
+    // a parallelogram / parallelepiped
     M.X0.assign((size_t)E * dim, 0.0);
     M.J.assign((size_t)E * dim * dim, 0.0);
+    M.Xc.assign((size_t)E * nc * dim, 0.0);
+    M.multilinear = false;
     for (int e = 0; e < E; ++e) {
         const Frame &F = frames[fr[e]];
         auto X = [&](int b, int i) { return corner_x(e, F, b, i); };
@@ -494,17 +507,63 @@ prandtl_status orient(const Raw &R, prandtl_mesh &M) {
             }
         for (int b = 0; b < nc; ++b)
             for (int i = 0; i < dim; ++i) {
+                M.Xc[((size_t)e * nc + b) * dim + i] = X(b, i);
                 double x = x0[i];
                 for (int r = 0; r < dim; ++r) x += ((b >> r) & 1) * J[i * dim + r];
-                if (std::fabs(x - X(b, i)) > 1e-9 * scale)
-                    return mesh_fail(PRANDTL_EUNSUPPORTED, "element " + std::to_string(e) +
-                                                               " is not affine (a parallelogram / parallelepiped)");
+                if (std::fabs(x - X(b, i)) > 1e-9 * scale) M.multilinear = true;
             }
         if (!(determinant(dim, J) > 0.0))
             return mesh_fail(PRANDTL_EINVAL, "element " + std::to_string(e) + " is inverted");
     }
     M.attr = R.el_attr;
     return PRANDTL_OK;
+}
+
+// Multilinear map of corners Xc (2^dim of them) at reference point xi: the
+// position x and the Jacobian J[i][r] = dx_i / dxi_r (MFEM's order-1 H1
+// transformation of a quadrilateral / hexahedron).
+void multilinear_eval(int dim, const double *Xc, const double *xi, double *x, double *J) {
+    const int nc = 1 << dim;
+    for (int i = 0; i < dim; ++i) {
+        if (x) x[i] = 0.0;
+        if (J)
+            for (int r = 0; r < dim; ++r) J[i * dim + r] = 0.0;
+    }
+    for (int b = 0; b < nc; ++b) {
+        double phi = 1.0;
+        for (int q = 0; q < dim; ++q) phi *= ((b >> q) & 1) ? xi[q] : 1.0 - xi[q];
+        for (int i = 0; i < dim; ++i)
+            if (x) x[i] += phi * Xc[b * dim + i];
+        if (!J) continue;
+        for (int r = 0; r < dim; ++r) {
+            double dphi = ((b >> r) & 1) ? 1.0 : -1.0;
+            for (int q = 0; q < dim; ++q)
+                if (q != r) dphi *= ((b >> q) & 1) ? xi[q] : 1.0 - xi[q];
+            for (int i = 0; i < dim; ++i) J[i * dim + r] += dphi * Xc[b * dim + i];
+        }
+    }
+}
+
+// Gauss-Lobatto nodes on [0, 1]: roots of (1 - x^2) P'_N (Newton in long double).
+std::vector<double> gl_nodes(int N) {
+    std::vector<double> xi(N + 1);
+    for (int i = 0; i <= N; ++i) {
+        long double x = -std::cos((long double)M_PI * i / N);
+        if (i > 0 && i < N)
+            for (int it = 0; it < 100; ++it) {
+                long double p0 = 1, p1 = x, d0 = 0, d1 = 1;
+                for (int k = 1; k < N; ++k) {
+                    const long double p2 = ((2 * k + 1) * x * p1 - k * p0) / (k + 1);
+                    const long double d2 = d0 + (2 * k + 1) * p1;
+                    p0 = p1, p1 = p2, d0 = d1, d1 = d2;
+                }
+                const long double dx = (1 - x * x) * d1 / (-(long double)(N * (N + 1)) * p1);
+                x -= dx;
+                if (std::fabs((double)dx) < 1e-30) break;
+            }
+        xi[i] = i == 0 ? 0.0 : i == N ? 1.0 : (double)((x + 1) * 0.5L);
+    }
+    return xi;
 }
 
 // one level of uniform refinement: child c of element e has bits c along the
@@ -548,6 +607,19 @@ void refine(prandtl_mesh &M) {
                 C.nb_f[(size_t)ce * nfl + lf] = nf;
             }
         }
+    if (M.multilinear) {   // child corners: the parent's map at (c + b) / 2
+        const int nc = 1 << dim;
+        C.Xc.resize((size_t)E * nch * nc * dim);
+        for (int e = 0; e < E; ++e)
+            for (int c = 0; c < nch; ++c)
+                for (int b = 0; b < nc; ++b) {
+                    double xi[3] = {0, 0, 0};
+                    for (int r = 0; r < dim; ++r) xi[r] = 0.5 * (((c >> r) & 1) + ((b >> r) & 1));
+                    multilinear_eval(dim, &M.Xc[(size_t)e * nc * dim], xi,
+                                     &C.Xc[(((size_t)e * nch + c) * nc + b) * dim], nullptr);
+                }
+        M.Xc.swap(C.Xc);
+    }
     M.X0.swap(C.X0);
     M.J.swap(C.J);
     M.attr.swap(C.attr);
@@ -586,10 +658,17 @@ void hilbert_reorder(prandtl_mesh &M) {
     const int dim = M.dim, nfl = 2 * dim, E = (int)M.attr.size();
     const int bits = dim == 2 ? 20 : 16;
     std::vector<double> c((size_t)E * dim), lo(dim, 1e300), hi(dim, -1e300);
+    const int nc = 1 << dim;
     for (int e = 0; e < E; ++e)
         for (int i = 0; i < dim; ++i) {
             double x = M.X0[(size_t)e * dim + i];
-            for (int r = 0; r < dim; ++r) x += 0.5 * M.J[((size_t)e * dim + i) * dim + r];
+            if (M.multilinear) {   // the map at the reference centre: the corners' mean
+                x = 0.0;
+                for (int b = 0; b < nc; ++b) x += M.Xc[((size_t)e * nc + b) * dim + i];
+                x /= nc;
+            } else {
+                for (int r = 0; r < dim; ++r) x += 0.5 * M.J[((size_t)e * dim + i) * dim + r];
+            }
             c[(size_t)e * dim + i] = x;
             lo[i] = std::min(lo[i], x);
             hi[i] = std::max(hi[i], x);
@@ -612,10 +691,12 @@ void hilbert_reorder(prandtl_mesh &M) {
     C.attr.resize(E);
     C.nb_e.resize(M.nb_e.size());
     C.nb_f.resize(M.nb_f.size());
+    if (M.multilinear) C.Xc.resize(M.Xc.size());
     for (int k = 0; k < E; ++k) {
         const int e = key[k].second;
         std::copy_n(&M.X0[(size_t)e * dim], dim, &C.X0[(size_t)k * dim]);
         std::copy_n(&M.J[(size_t)e * dim * dim], dim * dim, &C.J[(size_t)k * dim * dim]);
+        if (M.multilinear) std::copy_n(&M.Xc[(size_t)e * nc * dim], nc * dim, &C.Xc[(size_t)k * nc * dim]);
         C.attr[k] = M.attr[e];
         for (int lf = 0; lf < nfl; ++lf) {
             const int ne = M.nb_e[(size_t)e * nfl + lf];
@@ -623,6 +704,7 @@ void hilbert_reorder(prandtl_mesh &M) {
             C.nb_f[(size_t)k * nfl + lf] = M.nb_f[(size_t)e * nfl + lf];
         }
     }
+    if (M.multilinear) M.Xc.swap(C.Xc);
     M.X0.swap(C.X0);
     M.J.swap(C.J);
     M.attr.swap(C.attr);
@@ -630,8 +712,23 @@ void hilbert_reorder(prandtl_mesh &M) {
     M.nb_f.swap(C.nb_f);
 }
 
+// Element-local node of face node a on local face lf = 2 dir + side.
+int face_node_of(int dim, int Np, int lf, int a) {
+    const int d = lf >> 1, s = lf & 1;
+    int c[3] = {0, 0, 0};
+    c[d] = s * (Np - 1);
+    if (dim == 2) {
+        c[1 - d] = a;
+    } else {
+        const int t0 = (d == 0) ? 1 : 0, t1 = (d == 2) ? 1 : 2;
+        c[t0] = a % Np;
+        c[t1] = a / Np;
+    }
+    return c[0] + Np * (c[1] + Np * c[2]);
+}
+
 // descriptor arrays; boundary faces carry BC index attribute - 1
-void describe(prandtl_mesh &M) {
+prandtl_status describe(prandtl_mesh &M) {
     const int dim = M.dim, nfl = 2 * dim, E = (int)M.attr.size();
     M.adj.resize((size_t)E * dim * dim);
     M.detj.resize(E);
@@ -639,12 +736,40 @@ void describe(prandtl_mesh &M) {
     M.nor.clear();
     M.face_attr.clear();
     M.hmin = 1e300;
+    const int nc = 1 << dim, Np = M.order + 1;
+    int nd = 1;
+    for (int d = 0; d < dim; ++d) nd *= Np;
+    const int nfn = nd / Np;
     for (int e = 0; e < E; ++e) {
+        double Jc[9];
         const double *J = &M.J[(size_t)e * dim * dim];
+        if (M.multilinear) {   // element values at the reference centre
+            const double mid[3] = {0.5, 0.5, 0.5};
+            multilinear_eval(dim, &M.Xc[(size_t)e * nc * dim], mid, nullptr, Jc);
+            J = Jc;
+        }
         adjugate(dim, J, &M.adj[(size_t)e * dim * dim]);
         M.detj[e] = determinant(dim, J);
-        M.hmin = std::min(M.hmin, min_singular(dim, J));
+        M.hmin = std::min(M.hmin, min_singular(dim, J));   // MFEM GetElementSize(e, 1), at the centre
     }
+    if (M.multilinear) {   // the transformation at every Gauss-Lobatto node
+        const std::vector<double> xi = gl_nodes(M.order);
+        M.nadj.resize((size_t)E * nd * dim * dim);
+        M.ndetj.resize((size_t)E * nd);
+        for (int e = 0; e < E; ++e)
+            for (int n = 0; n < nd; ++n) {
+                const double p[3] = {xi[n % Np], xi[(n / Np) % Np], dim > 2 ? xi[n / (Np * Np)] : 0.0};
+                double J[9];
+                multilinear_eval(dim, &M.Xc[(size_t)e * nc * dim], p, nullptr, J);
+                adjugate(dim, J, &M.nadj[((size_t)e * nd + n) * dim * dim]);
+                const double dj = determinant(dim, J);
+                if (!(dj > 0.0))
+                    return mesh_fail(PRANDTL_EINVAL, "element " + std::to_string(e) + " is inverted at node " +
+                                                         std::to_string(n));
+                M.ndetj[(size_t)e * nd + n] = dj;
+            }
+    }
+    M.fnn.clear();
     for (int e = 0; e < E; ++e)
         for (int lf = 0; lf < nfl; ++lf) {
             const int ne = M.nb_e[(size_t)e * nfl + lf], nf = M.nb_f[(size_t)e * nfl + lf];
@@ -658,8 +783,22 @@ void describe(prandtl_mesh &M) {
                 M.faces.insert(M.faces.end(), {e, lf, ne, nf});
                 M.face_attr.push_back(0);
             }
-            for (int c = 0; c < dim; ++c) M.nor.push_back(sg * M.adj[((size_t)e * dim + d) * dim + c]);
+            if (M.multilinear) {   // per face node, and their mean as the face's value
+                double mean[3] = {0, 0, 0};
+                for (int a = 0; a < nfn; ++a) {
+                    const int n = face_node_of(dim, Np, lf, a);
+                    for (int c = 0; c < dim; ++c) {
+                        const double v = sg * M.nadj[(((size_t)e * nd + n) * dim + d) * dim + c];
+                        M.fnn.push_back(v);
+                        mean[c] += v / nfn;
+                    }
+                }
+                for (int c = 0; c < dim; ++c) M.nor.push_back(mean[c]);
+            } else {
+                for (int c = 0; c < dim; ++c) M.nor.push_back(sg * M.adj[((size_t)e * dim + d) * dim + c]);
+            }
         }
+    return PRANDTL_OK;
 }
 
 }   // namespace
@@ -698,7 +837,10 @@ prandtl_status prandtl_mesh_read(const char *path, int order, int refine_levels,
     }
     for (int l = 0; l < refine_levels; ++l) refine(*M);
     if (hilbert) hilbert_reorder(*M);
-    describe(*M);
+    if ((st = describe(*M)) != PRANDTL_OK) {
+        delete M;
+        return st;
+    }
     *out = M;
     return PRANDTL_OK;
 }
@@ -713,6 +855,9 @@ prandtl_status prandtl_mesh_describe(const prandtl_mesh *m, prandtl_mesh_desc *d
     desc->elem_detj = m->detj.data();
     desc->face_elems = m->faces.data();
     desc->face_nor = m->nor.data();
+    desc->node_adj = m->multilinear ? m->nadj.data() : nullptr;
+    desc->node_detj = m->multilinear ? m->ndetj.data() : nullptr;
+    desc->face_node_nor = m->multilinear ? m->fnn.data() : nullptr;
     if (hmin) *hmin = m->hmin;
     return PRANDTL_OK;
 }
@@ -749,30 +894,19 @@ int prandtl_mesh_attribute(const prandtl_mesh *m, int entity_dim, const char *na
 
 prandtl_status prandtl_mesh_node_coords(const prandtl_mesh *m, double *xyz) {
     if (!m || !xyz) return mesh_fail(PRANDTL_EINVAL, "null pointer");
-    const int dim = m->dim, Np = m->order + 1;
-    // Gauss-Lobatto nodes on [0, 1]: roots of (1 - x^2) P'_N (Newton in long double)
-    std::vector<double> xi(Np);
-    const int N = m->order;
-    for (int i = 0; i < Np; ++i) {
-        long double x = -std::cos((long double)M_PI * i / N);
-        if (i > 0 && i < N)
-            for (int it = 0; it < 100; ++it) {
-                long double p0 = 1, p1 = x, d0 = 0, d1 = 1;
-                for (int k = 1; k < N; ++k) {
-                    const long double p2 = ((2 * k + 1) * x * p1 - k * p0) / (k + 1);
-                    const long double d2 = d0 + (2 * k + 1) * p1;
-                    p0 = p1, p1 = p2, d0 = d1, d1 = d2;
-                }
-                const long double dx = (1 - x * x) * d1 / (-(long double)(N * (N + 1)) * p1);
-                x -= dx;
-                if (std::fabs((double)dx) < 1e-30) break;
-            }
-        xi[i] = i == 0 ? 0.0 : i == N ? 1.0 : (double)((x + 1) * 0.5L);
-    }
+    const int dim = m->dim, Np = m->order + 1, nc = 1 << dim;
+    const std::vector<double> xi = gl_nodes(m->order);
     const size_t E = m->attr.size(), ND = (size_t)std::pow(Np, dim), Ndof = E * ND;
     for (size_t e = 0; e < E; ++e)
         for (size_t n = 0; n < ND; ++n) {
             const int c[3] = {(int)(n % Np), (int)((n / Np) % Np), (int)(n / (Np * Np))};
+            if (m->multilinear) {
+                const double p[3] = {xi[c[0]], xi[c[1]], dim > 2 ? xi[c[2]] : 0.0};
+                double x[3];
+                multilinear_eval(dim, &m->Xc[e * nc * dim], p, x, nullptr);
+                for (int i = 0; i < dim; ++i) xyz[(size_t)i * Ndof + e * ND + n] = x[i];
+                continue;
+            }
             for (int i = 0; i < dim; ++i) {
                 double x = m->X0[e * dim + i];
                 for (int r = 0; r < dim; ++r) x += m->J[(e * dim + i) * dim + r] * xi[c[r]];

@@ -152,6 +152,8 @@ extern "C" prandtl_status prandtl_rhs_noalloc(const prandtl_mesh_desc *m, const 
         return fail(PRANDTL_EINVAL, "mesh arrays missing");
     if (cfg->precision != 0) return fail(PRANDTL_EUNSUPPORTED, "only precision 0 (FP64) is built");
     if (cfg->axisymmetric) return fail(PRANDTL_EUNSUPPORTED, "the axisymmetric form needs prandtl_create");
+    if (m->node_adj || m->node_detj || m->face_node_nor)
+        return fail(PRANDTL_EUNSUPPORTED, "non-affine elements need prandtl_create");
     if (!(cfg->gamma > 1.0) || !(cfg->Pr > 0.0)) return fail(PRANDTL_EINVAL, "bad gamma/Pr");
 
     const int dim = m->dim, E = m->num_elements, F = m->num_faces, NFACE = 2 * dim;

@@ -332,7 +332,8 @@ def set_multilinear(mesh: Mesh, corners: np.ndarray) -> None:
 
 def read_mesh(path: str, order: int, refine: int = 0, hilbert: bool = False, boundary_conditions=None) -> Mesh:
     """Read an MFEM v1.0 or Gmsh 2.2 ASCII mesh through the native reader
-    (``prandtl_mesh_read``: quadrilaterals / hexahedra, affine, aligned frames).
+    (``prandtl_mesh_read``: quadrilaterals / hexahedra with aligned frames;
+    non-affine elements come back multilinear, with per-node geometry).
 
     ``refine`` uniform refinements and ``hilbert`` element ordering follow the
     reference's ``ser_ref_levels`` and ``"mesh_ordering": "Hilbert"``.
@@ -379,9 +380,18 @@ def read_mesh(path: str, order: int, refine: int = 0, hilbert: bool = False, bou
         L.prandtl_mesh_node_coords(h, coords.ctypes.data_as(C.POINTER(C.c_double)))
         eattr = np.empty(E, dtype=np.int32)
         L.prandtl_mesh_element_attributes(h, eattr.ctypes.data_as(C.POINTER(C.c_int)))
+        node = None
+        if d.node_adj:   # multilinear elements: the per-node arrays
+            nd, nfn = Np ** dim, Np ** (dim - 1)
+            node = (np.ctypeslib.as_array(d.node_adj, shape=(E * nd * dim * dim,)).reshape(E, nd, dim, dim).copy(),
+                    np.ctypeslib.as_array(d.node_detj, shape=(E * nd,)).reshape(E, nd).copy(),
+                    np.ctypeslib.as_array(d.face_node_nor, shape=(F * nfn * dim,)).reshape(F, nfn, dim).copy())
     finally:
         L.prandtl_mesh_destroy(h)
     x, w = gauss_lobatto(order)
-    return Mesh(dim=dim, order=order, n=(E,), elem_adj=adj, elem_detj=detj, face_elems=faces.astype(np.int32),
+    mesh = Mesh(dim=dim, order=order, n=(E,), elem_adj=adj, elem_detj=detj, face_elems=faces.astype(np.int32),
                 face_nor=nor, coords=coords, hmin=float(hmin.value), nodes_1d=x, weights_1d=w,
                 face_attr=fattr, elem_attr=eattr)
+    if node is not None:
+        mesh.node_adj, mesh.node_detj, mesh.face_node_nor = node
+    return mesh

@@ -46,10 +46,14 @@ class MeshArrays:
         self.faces = np.ascontiguousarray(mesh.face_elems, dtype=np.int32)
         self.nor = np.ascontiguousarray(mesh.face_nor, dtype=np.float64)
         dp = C.POINTER(C.c_double)
+        # non-affine elements: per-node transformation and per-face-node normals
+        self.node = None if mesh.affine else tuple(
+            np.ascontiguousarray(a, dtype=np.float64) for a in (mesh.node_adj, mesh.node_detj, mesh.face_node_nor))
+        ng = [a.ctypes.data_as(dp) for a in self.node] if self.node else [None, None, None]
         self.desc = _lib.MeshDesc(mesh.dim, mesh.order, mesh.num_elements, mesh.num_faces,
                                   self.adj.ctypes.data_as(dp), self.detj.ctypes.data_as(dp),
                                   self.faces.ctypes.data_as(C.POINTER(C.c_int)),
-                                  self.nor.ctypes.data_as(dp))
+                                  self.nor.ctypes.data_as(dp), *ng)
 
 
 def make_bcs(bcs):

@@ -200,3 +200,36 @@ def test_axisymmetric_configuration_checked_before_the_device(lib):
     u = np.zeros(m.num_fields * m.ndof)
     assert lib.prandtl_rhs_noalloc(C.byref(d), C.byref(cfg), u.ctypes.data, u.ctypes.data, None) == \
         _lib.PRANDTL_EUNSUPPORTED
+
+
+def test_non_affine_descriptor_checked_before_the_device(lib):
+    """Per-node geometry: all three arrays or none, positive det J, FP64 only,
+    and in fixed Navier-Stokes the face-node normals must be the adjugate rows."""
+    import sys
+    from prandtl_b200 import _lib
+    from prandtl_b200.mesh import periodic_box
+    from prandtl_b200.operator import MeshArrays, make_config
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_golden
+    def mesh():   # MeshArrays shares the mesh's arrays: a fresh mesh per altered copy
+        return periodic_box(2, 3, 2, warp=make_golden.warp_field(2, 0.06))
+    arr = MeshArrays(mesh())
+    h = C.c_void_p()
+    st = lib.prandtl_create(C.byref(arr.desc), C.byref(make_config(precision="fp32")), C.byref(h))
+    assert st == _lib.PRANDTL_EUNSUPPORTED
+    assert b"FP64" in lib.prandtl_last_error(None)
+    part = MeshArrays(mesh())
+    part.desc.face_node_nor = None
+    assert lib.prandtl_create(C.byref(part.desc), C.byref(make_config()), C.byref(h)) == _lib.PRANDTL_EINVAL
+    bad = MeshArrays(mesh())
+    bad.node[1][3, 2] = -1.0
+    assert lib.prandtl_create(C.byref(bad.desc), C.byref(make_config()), C.byref(h)) == _lib.PRANDTL_EINVAL
+    skew = MeshArrays(mesh())
+    skew.node[2][4, 1, 0] += 1e-3
+    cfg = make_config(parabolic=True, quirks="fixed")
+    assert lib.prandtl_create(C.byref(skew.desc), C.byref(cfg), C.byref(h)) == _lib.PRANDTL_EUNSUPPORTED
+    # a valid descriptor gets as far as the device
+    st = lib.prandtl_create(C.byref(arr.desc), C.byref(make_config(parabolic=True, quirks="fixed")), C.byref(h))
+    assert st in (_lib.PRANDTL_ECUDA, _lib.PRANDTL_OK)
+    if st == _lib.PRANDTL_OK:
+        lib.prandtl_destroy(h)

@@ -153,10 +153,6 @@ def test_rejected_meshes(tmp_path):
     tri = _write(tmp_path, "tri.msh", GMSH_HEAD + "$Nodes\n3\n1 0 0 0\n2 1 0 0\n3 0 1 0\n$EndNodes\n"
                  "$Elements\n1\n1 2 2 1 1 1 2 3\n$EndElements\n")
     assert code(tri)[0] == _lib.PRANDTL_EUNSUPPORTED
-    trap = _write(tmp_path, "trap.msh", GMSH_HEAD + "$Nodes\n4\n1 0 0 0\n2 2 0 0\n3 1.5 1 0\n4 0 1 0\n$EndNodes\n"
-                  "$Elements\n1\n1 3 2 1 1 1 2 3 4\n$EndElements\n")
-    st, msg = code(trap)
-    assert st == _lib.PRANDTL_EUNSUPPORTED and "affine" in msg
     # three quads around a vertex: no aligned frames exist
     star = _write(tmp_path, "star.msh", GMSH_HEAD + "$Nodes\n7\n1 0 0 0\n2 1 0 0\n3 0.5 0.866 0\n"
                   "4 -0.5 0.866 0\n5 -0.5 -0.866 0\n6 0.5 -0.866 0\n7 -1 0 0\n$EndNodes\n"
@@ -175,7 +171,7 @@ REF_MESHES = {   # file -> (elements, boundary faces) as read at refine 0, or th
     "Euler/2D/ForwardFacingStep/ForwardFacingStep.msh": (3400, 260),
     "Euler/2D/DoubleMachReflection/DoubleMachReflection.msh": (36864, 960),
     "Euler/2D/BackwardFacingStep/BackwardFacingStep.msh": (35000, 800),
-    "Euler/2D/Ramp/Ramp15deg_v2.msh": "not affine",
+    "Euler/2D/Ramp/Ramp15deg_v2.msh": (4802, 294),
     "Euler/2D/Nagashima_Ramjet/TR0/Nagashima_TR0_10kQuad_v2.msh": "structured topology",
 }
 
@@ -194,6 +190,8 @@ def test_reference_test_case_meshes(rel):
     m = read_mesh(path, 3)
     assert (m.num_elements, int((m.face_elems[:, 2] < 0).sum())) == want
     assert (m.elem_detj > 0).all()
+    if rel.endswith("Ramp15deg_v2.msh"):   # quadrilaterals over the ramp are not parallelograms
+        assert not m.affine and (m.node_detj > 0).all()
     if rel.endswith("IsentropicVortex.mesh"):   # the 3x3 periodic [-1, 1]^2 box
         b = periodic_box(2, 3, 3, -1.0, 1.0)
         np.testing.assert_allclose(m.coords, b.coords, rtol=0, atol=1e-8)
@@ -201,3 +199,36 @@ def test_reference_test_case_meshes(rel):
         m2 = read_mesh(path, 3, boundary_conditions={"lid": 0, "left": 1, "right": 1, "bottom": 1})
         lid = m2.face_elems[(m2.face_elems[:, 2] < 0) & (m2.face_elems[:, 3] == 0)]
         assert len(lid) == 16
+
+
+def test_gmsh_trapezoid_is_multilinear(tmp_path):
+    """A quadrilateral that is not a parallelogram: the reader returns the
+    multilinear map's geometry at every node (the same as the Python
+    multilinear_geometry of its corners), per-face-node normals and the centre
+    Jacobian's values per element."""
+    from prandtl_b200.mesh import multilinear_geometry
+    trap = _write(tmp_path, "trap.msh", GMSH_HEAD + "$Nodes\n4\n1 0 0 0\n2 2 0 0\n3 1.5 1 0\n4 0 1 0\n$EndNodes\n"
+                  "$Elements\n1\n1 3 2 1 1 1 2 3 4\n$EndElements\n")
+    m = read_mesh(trap, 3)
+    assert not m.affine
+    corners = np.array([[[0.0, 0.0], [2.0, 0.0], [0.0, 1.0], [1.5, 1.0]]])
+    xy, adj, detj = multilinear_geometry(corners, m.nodes_1d)
+    np.testing.assert_allclose(m.coords, xy, rtol=0, atol=1e-15)
+    np.testing.assert_allclose(m.node_adj, adj, rtol=0, atol=1e-15)
+    np.testing.assert_allclose(m.node_detj, detj, rtol=0, atol=1e-15)
+    assert m.face_node_nor.shape == (4, 4, 2)
+    # boundary face normals: outward, |n| = edge length; left edge x = 0 points to -x
+    left = [f for f in range(4) if m.face_elems[f, 1] == 0][0]
+    np.testing.assert_allclose(m.face_node_nor[left], np.tile([-1.0, 0.0], (4, 1)), atol=1e-15)
+    assert m.hmin > 0
+
+
+def test_multilinear_refinement_keeps_the_geometry(tmp_path):
+    """Refining a multilinear element splits it in reference coordinates: the
+    children's node coordinates lie on the parent's map."""
+    trap = _write(tmp_path, "trap.msh", GMSH_HEAD + "$Nodes\n4\n1 0 0 0\n2 2 0 0\n3 1.5 1 0\n4 0 1 0\n$EndNodes\n"
+                  "$Elements\n1\n1 3 2 1 1 1 2 3 4\n$EndElements\n")
+    m = read_mesh(trap, 2, refine=1)
+    assert m.num_elements == 4 and not m.affine
+    area = (m.node_weights()).sum()
+    assert area == pytest.approx(1.75, rel=1e-14)   # (2 + 1.5) / 2 * 1
