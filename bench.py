@@ -604,6 +604,59 @@ def run_kh256(torch, t_final=3.0, precisions=("fp64", "fp32")):
     return out
 
 
+def run_ramp(torch, t_final=3.0, dt=1e-4):
+    """The reference's axisymmetric 15-degree ramp case (TestCases/Euler/2D/Ramp:
+    Mach-2 free stream, order 1, subcell FV blending, SSP-RK3 with the fixed dt
+    1e-4 of its config, to t = 3) on a 98 x 49 structured ramp mesh whose cells
+    over the cone are trapezoids: the FP64 kernels with per-node geometry.
+    Every stage checks every node for non-finite values; the density and
+    pressure range and the blending field are taken from the state at t = 3
+    (at N = 1 the modal indicator has no resolved modes to compare, so every
+    element takes alpha_max, as in the reference)."""
+    import numpy as np
+    from prandtl_b200 import cases
+    from prandtl_b200.operator import DGSEMOperator
+    mesh = cases.ramp_mesh(1)
+    u0 = cases.ramp_ic(mesh)
+    op = DGSEMOperator(mesh, quirks="reference", blending=True, bcs=cases.RAMP_BCS, axisymmetric=True)
+    stream = torch.cuda.current_stream()
+    op.set_stream(stream.cuda_stream)
+    u = torch.from_numpy(u0).cuda()
+    steps = int(round(t_final / dt))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    status, done = "ok", 0
+    a.record(stream)
+    try:
+        while done < steps:
+            k = min(2000, steps - done)
+            op.Step(u, dt, scheme="RK3SSP", nsteps=k)   # raises on a failed state check
+            done += k
+    except Exception as exc:
+        status = str(exc)
+    b.record(stream)
+    op.synchronize()
+    el = a.elapsed_time(b) / 1e3
+    dof = mesh.ndof * mesh.num_fields
+    rec = {"workload": "ramp15_axisymmetric_euler_98x49_N1_blended_ssprk3_dt1e-4_to_t3",
+           "mesh": "98 x 49 quadrilaterals, multilinear over the cone (per-node geometry)",
+           "dof": dof, "status": status, "steps": done, "t": done * dt, "device_s": el,
+           "dof_updates_per_s": dof * done / el, "ms_per_step": 1e3 * el / max(done, 1),
+           "state_check": "every node of every stage: finite" + (" - passed" if status == "ok" else " - FAILED")}
+    if status == "ok":
+        rU = u.cpu().numpy()
+        U = op.recover_state(rU).reshape(4, -1)
+        p = 0.4 * (U[3] - 0.5 * (U[1] ** 2 + U[2] ** 2) / U[0])
+        rec["min_rho"], rec["min_p"] = float(U[0].min()), float(p.min())
+        rec["max_rho"], rec["max_p"] = float(U[0].max()), float(p.max())   # the shock off the cone
+        d = np.empty_like(rU)
+        op.Mult(rU, d)
+        al = op.alpha()
+        rec["alpha_at_t"] = {"elements_blended": int((al > 0).sum()), "fraction": float((al > 0).mean()),
+                             "max": float(al.max())}
+    op.close()
+    return rec
+
+
 def run_serving(torch, n_req, check_every=15):
     """Calibrate the server's capacity with a closed burst, then replay a
     Poisson stream at 80 % of it.  Requests are FP32-bulk solves.  A submitter
@@ -800,6 +853,7 @@ def main():
                                "elements (ncu summary lift_batch_kernel_N5_fp32_ncu under profiles/)") if ltr else None}
         ivortex32 = run_ivortex32(torch) if not args.no_configs else None
         kh256 = run_kh256(torch) if not args.no_configs else None
+        ramp = run_ramp(torch) if not args.no_configs else None
         tgv32 = None
         if not args.no_tgv32:
             tgv32 = run_tgv32(torch, 50)
@@ -849,6 +903,7 @@ def main():
             "tgv32": tgv32,
             "ivortex32": ivortex32,
             "kh256": kh256,
+            "ramp": ramp,
             "serving": serving,
             "clocks": binfo["clocks"],
         }

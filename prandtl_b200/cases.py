@@ -94,3 +94,42 @@ def make_case(name: str, n=None, order=3):
         m = periodic_box(2, n or 256, order, -1.0, 1.0)
         return m, kelvin_helmholtz(m), dict(parabolic=0, blending=1, alpha_max=0.5)
     raise ValueError(name)
+
+
+# ---- axisymmetric 15-degree ramp (the reference's TestCases/Euler/2D/Ramp:
+# Ramp.hpp RampIC / RampInletBCVector, config.json: AXISYMMETRIC, blending,
+# order 1, RK3SSP, dt 1e-4).  In (z, r): [0, 2] x [0, 2], the axis r = 0 for
+# z < 1, a 15-degree cone surface from z = 1 to z = 2 (r = 0.26795 there).
+RAMP_TAN = 0.26795   # the ramp mesh's end height over its unit length (tan 15 deg)
+RAMP_INLET = [1.0, 2.0, 0.0, (1.0 / 1.4) / 0.4 + 0.5 * 1.0 * 2.0 * 2.0]   # rho, rho u, rho v, E (Ma 2)
+# boundary-condition table: inlet and top (supersonic inflow of the inlet
+# state), outlet (supersonic outflow), axis, ramp (slip wall)
+RAMP_BCS = [("state", RAMP_INLET), ("outflow",), ("axis",), ("slip_wall",)]
+
+
+def ramp_mesh(order=1, nx=98, ny=49) -> Mesh:
+    """Structured quadrilaterals of the ramp geometry, uniform in each
+    column (the reference's Ramp15deg_v2 mesh has the same 98 x 49 layout,
+    graded towards the floor): each column of cells runs from the bottom
+    boundary (axis, then ramp) to r = 2, so the cells over the ramp are
+    trapezoids, i.e. multilinear elements.  Boundary faces carry the RAMP_BCS
+    indices: z = 0 inlet 0, z = 2 outlet 1, bottom axis 2 (z < 1) or ramp 3,
+    top 0."""
+    def lift(X):   # the box [0,2]^2 mapped onto the ramp domain, r stretched over the floor
+        z, r = X[0], X[1]
+        floor = np.where(z > 1.0, (z - 1.0) * RAMP_TAN, 0.0)
+        return np.stack([np.zeros_like(z), floor * (1.0 - r / 2.0)])
+    m = periodic_box(2, (nx, ny), order, (0.0, 0.0), (2.0, 2.0), bcs=[0, 1, 2, 0], warp=lift)
+    fe = m.face_elems
+    bottom = (fe[:, 2] < 0) & (fe[:, 1] == 2)
+    zc = m.coords[0].reshape(m.num_elements, -1).mean(axis=1)
+    fe[bottom & (zc[fe[:, 0]] > 1.0), 3] = 3
+    return m
+
+
+def ramp_ic(mesh: Mesh) -> np.ndarray:
+    """RampIC (Ramp.hpp): Ma 2 free stream, rho 1, u 2, v 0, p 1/1.4, as the
+    axisymmetric RK state r U."""
+    nn = mesh.ndof
+    U = np.stack([np.full(nn, v) for v in RAMP_INLET])
+    return np.ascontiguousarray((U * mesh.coords[1][None, :]).reshape(-1))

@@ -188,3 +188,40 @@ def test_curved_rejected_where_not_built():
         assert ei.value.status == _lib.PRANDTL_EUNSUPPORTED
     finally:
         b.close()
+
+
+# ---------------------------------------------------------------- the axisymmetric ramp
+@pytest.mark.parametrize("order,nx,ny", [(1, 20, 10), (2, 12, 6)])
+@pytest.mark.parametrize("quirks", ["reference", "fixed"])
+def test_ramp_rhs_matches_oracle(oracle_mod, order, nx, ny, quirks):
+    """The reference's Ramp case (axisymmetric, blended, trapezoidal cells over
+    the cone; inflow, outflow, axis and slip-wall boundaries) on a coarse mesh,
+    from a perturbed Mach-2 state so the indicator fires."""
+    mesh = cases.ramp_mesh(order, nx, ny)
+    assert not mesh.affine
+    U = cases.perturbed(mesh, cases.free_stream(mesh, rho=1.0, vel=[2.0, 0.0], p=1 / 1.4),
+                        amp=0.3, seed=order).reshape(4, -1)
+    u = (U * mesh.coords[1][None, :]).reshape(-1)
+    q = 0 if quirks == "reference" else 1
+    ref = oracle_mod.Oracle(mesh, quirks=q, blending=1, bcs=cases.RAMP_BCS, axisymmetric=1).rhs(u, want_alpha=True)
+    assert (ref["alpha"] > 0).any()
+    op = _op(mesh, quirks=quirks, blending=True, bcs=cases.RAMP_BCS, axisymmetric=True)
+    d = np.empty_like(u)
+    op.Mult(u, d)
+    assert normalized_error(d, ref["dudt"], 4) <= RHS_TOL
+    np.testing.assert_allclose(op.alpha(), ref["alpha"], rtol=0, atol=1e-12)
+
+
+def test_ramp_trajectory_matches_oracle(oracle_mod):
+    """100 SSP-RK3 steps of the ramp flow from the reference's initial state:
+    the shock forms off the cone and the blending follows it."""
+    mesh = cases.ramp_mesh(1, 24, 12)
+    u0 = cases.ramp_ic(mesh)
+    orc = oracle_mod.Oracle(mesh, quirks=0, blending=1, bcs=cases.RAMP_BCS, axisymmetric=1)
+    dt = 0.3 * mesh.hmin / (3.0 * 4)
+    ref = orc.step(u0, dt, scheme=0, nsteps=100)
+    op = _op(mesh, quirks="reference", blending=True, bcs=cases.RAMP_BCS, axisymmetric=True)
+    u = u0.copy()
+    op.Step(u, dt, scheme="RK3SSP", nsteps=100)
+    assert normalized_error(u, ref, 4) <= TRAJ_TOL
+    assert (orc.rhs(ref, want_alpha=True)["alpha"] > 0).any()
