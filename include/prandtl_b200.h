@@ -186,7 +186,10 @@ prandtl_status prandtl_rhs(prandtl_handle *h, const double *u, double *dudt, dou
  * PRANDTL_ENONFINITE (state still copied back, reason in prandtl_last_error)
  * when any stage of these steps failed the check; with device pointers it
  * returns without waiting and the next prandtl_synchronize reports the flag.
- * Reporting clears the flag. */
+ * Reporting clears the flag.  Runs of 8 or more steps replay a CUDA graph of
+ * 4 steps (captured on the handle's own stream the first time for a given
+ * state pointer, dt and scheme; launched on the handle's stream), with the
+ * same results as step-by-step launches. */
 prandtl_status prandtl_step(prandtl_handle *h, double *u, double t, double dt, int scheme,
                             int nsteps, int ptr_flags);
 

@@ -20,6 +20,7 @@
 // class.
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 
 #include "dgsem_kernels.cuh"
@@ -301,7 +302,15 @@ struct RhsLayout {
     // work buffer (BODY, padded to 16 bytes), then (FP64) the element's
     // neighbour-table entries (2 DIM int4), and the whole a multiple of 4 words
     // so every element's area stays 16-byte aligned
-    static constexpr int BODY = (K * ND + cmax(BUF, NS ? DIM * NF * ND : 0) + 3) / 4 * 4;
+    // Navier-Stokes viscous-flux buffer [DIM][VROWS][ND]: the line tasks keep
+    // all NF rows (row 0 carries the direction's inviscid total), the pair form
+    // only rows 1..NF-1 (the viscous mass flux is zero); the smaller footprint
+    // leaves more of the SM's L1 to the face phase's loads (C2 FP64 RHS
+    // 0.362 -> 0.335 ms)
+    static constexpr bool LINE_FORM = NS && sizeof(Real) == 4 && (NP <= PRANDTL_LINE_MAX_NP || TASK128);
+    static constexpr int VROWS = LINE_FORM ? NF : NF - 1;
+    static constexpr int VOFF = NF - VROWS;             // buffer row of field f: f - VOFF
+    static constexpr int BODY = (K * ND + cmax(BUF, NS ? DIM * VROWS * ND : 0) + 3) / 4 * 4;
     static constexpr int NBR_REALS = sizeof(Real) == 8 ? 2 * DIM * 16 / (int)sizeof(Real) : 0;
     static constexpr int PER_ELEM = (BODY + NBR_REALS + 3) / 4 * 4;
     static constexpr bool F64 = sizeof(Real) == 8;
@@ -343,6 +352,7 @@ struct RhsLayout {
     // the 128-lane groups at Np = 6 (17 %); slower in FP64 and at Np = 5 (75
     // tasks over 64 or 128 lanes).
     static constexpr bool LINE = NS && !F64 && (NP <= PRANDTL_LINE_MAX_NP || TASK128);
+    static_assert(LINE == LINE_FORM, "viscous-buffer rows follow the volume form");
 };
 
 // Synchronise the GS lanes of lane group `gid` (its index within the CTA).
@@ -651,27 +661,6 @@ __device__ __forceinline__ void boundary_flux(const BcDev &bc, const double *s_i
                          P.quirks == 0, P.dissipation != 0, flux);
 }
 
-// State check of one node's new RK state: bit 0 a non-finite value, bit 1
-// rho <= 0, bit 2 p <= 0 (the last two only where `positivity`: the
-// axisymmetric RK state r U vanishes on the axis).
-template <int DIM>
-__device__ __forceinline__ unsigned state_health(const double *s, bool positivity) {
-    constexpr int NF = DIM + 2;
-    bool finite = true;
-#pragma unroll
-    for (int f = 0; f < NF; ++f) finite = finite && isfinite(s[f]);
-    unsigned bad = finite ? 0u : 1u;
-    if (positivity && finite) {
-        double mm = 0.0;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) mm += s[1 + d] * s[1 + d];
-        // p = (gamma - 1)(E - |m|^2 / (2 rho)) > 0  <=>  2 rho E - |m|^2 > 0 for rho > 0
-        if (!(s[0] > 0.0)) bad |= 2u;
-        else if (!(2.0 * s[0] * s[NF - 1] - mm > 0.0)) bad |= 4u;
-    }
-    return bad;
-}
-
 // ------------------------------------------------------------------- RHS
 // Real is the working precision of the O(Np^{d+1}) work (two-point fluxes,
 // flux differencing, surface fluxes, gradients): double for the plain FP64
@@ -886,7 +875,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 #pragma unroll
                 for (int r = 0; r < DIM; ++r)
 #pragma unroll
-                    for (int f = 1; f < NF; ++f) sV[(r * NF + f) * ND + n] = vrow[k][r][f - 1];
+                    for (int f = 1; f < NF; ++f) sV[(r * LY::VROWS + f - LY::VOFF) * ND + n] = vrow[k][r][f - 1];
             }
         }
     } else if constexpr (NS) {
@@ -921,7 +910,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 #pragma unroll
                 for (int r = 0; r < DIM; ++r)
 #pragma unroll
-                    for (int f = 0; f < NF; ++f) sV[(r * NF + f) * ND + n] = Vc[r][f];
+                    for (int f = LY::VOFF; f < NF; ++f) sV[(r * LY::VROWS + f - LY::VOFF) * ND + n] = Vc[r][f];
             }
         }
     }
@@ -997,6 +986,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                     }
                 }
             }
+            static_assert(LY::VROWS == NF, "line tasks use every row of the viscous buffer");
             Real vv[NP][NF - 1];
 #pragma unroll
             for (int l = 0; l < NP; ++l)
@@ -1049,7 +1039,8 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                         for (int l = 0; l < NP; ++l) {
                             const Real dh = sDh[pos * NP + l];
 #pragma unroll
-                            for (int f = 1; f < NF; ++f) dUv[k][f] += sV[(dir * NF + f) * ND + base + l * stride] * dh;
+                            for (int f = 1; f < NF; ++f)
+                                dUv[k][f] += sV[(dir * LY::VROWS + f - LY::VOFF) * ND + base + l * stride] * dh;
                         }
                     }
                 }
@@ -1447,31 +1438,67 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
                 for (int f = 0; f < NF; ++f) a.dudt[f * Ndof + gnode] = double(acc[k][f]);
                 continue;
             }
-            double nv[NF];   // the node's new RK state
+            // the node's new RK state, per scheme and stage, with the state check
+            // (Simulation.cpp:1024-1035 checks rho for NaN) tracked field by field
+            // as the values are stored: non-finite values anywhere, and (planar
+            // form) rho <= 0 or p <= 0, where p = (gamma-1)(E - |m|^2 / (2 rho)) > 0
+            // <=> 2 rho E - |m|^2 > 0 for rho > 0; one atomic per violating node,
+            // none on healthy states.  (One loop per mode: a mode test inside one
+            // loop over the fields raised the N=4 FP32 kernels' spills.)
+            bool finite = true;
+            double rho_n = 0.0, mm = 0.0, e_n = 0.0;
+            auto track = [&](int f, double v) {
+                finite = finite && isfinite(v);
+                if (f == 0) rho_n = v;
+                else if (f < NF - 1) mm += v * v;
+                else e_n = v;
+            };
+            switch (mode) {
+            case EPI_LSRK:
 #pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const long long g = f * Ndof + gnode;
-                const double L = double(acc[k][f]);
-                if (mode == EPI_LSRK) {
+                for (int f = 0; f < NF; ++f) {
+                    const long long g = f * Ndof + gnode;
+                    const double L = double(acc[k][f]);
                     const double dv = (a.rkA == 0.0) ? a.dt * L : a.rkA * ub[kk][f] + a.dt * L;
                     a.du[g] = dv;
-                    nv[f] = ua[kk][f] + a.rkB * dv;
-                } else if (mode == EPI_SSP1) {
-                    nv[f] = ua[kk][f] + a.dt * L;
-                } else if (mode == EPI_SSP2) {
-                    const double y = ua[kk][f] + a.dt * L;
-                    nv[f] = 3. / 4 * ub[kk][f] + 1. / 4 * y;
-                } else {
-                    const double y = ua[kk][f] + a.dt * L;
-                    nv[f] = 1. / 3 * ub[kk][f] + 2. / 3 * y;
+                    const double v = ua[kk][f] + a.rkB * dv;
+                    a.u_out[g] = v;
+                    track(f, v);
                 }
-                a.u_out[g] = nv[f];
+                break;
+            case EPI_SSP1:
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    const double v = ua[kk][f] + a.dt * double(acc[k][f]);
+                    a.u_out[f * Ndof + gnode] = v;
+                    track(f, v);
+                }
+                break;
+            case EPI_SSP2:
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    const double y = ua[kk][f] + a.dt * double(acc[k][f]);
+                    const double v = 3. / 4 * ub[kk][f] + 1. / 4 * y;
+                    a.u_out[f * Ndof + gnode] = v;
+                    track(f, v);
+                }
+                break;
+            default:
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    const double y = ua[kk][f] + a.dt * double(acc[k][f]);
+                    const double v = 1. / 3 * ub[kk][f] + 2. / 3 * y;
+                    a.u_out[f * Ndof + gnode] = v;
+                    track(f, v);
+                }
+                break;
             }
-            // state check (Simulation.cpp:1024-1035 checks rho for NaN): non-finite
-            // values anywhere, and (planar form) rho <= 0 or p <= 0; one atomic
-            // per violating node, none on healthy states
             if (a.health) {
-                const unsigned bad = state_health<DIM>(nv, rad == nullptr);
+                unsigned bad = finite ? 0u : 1u;
+                if (rad == nullptr && finite) {   // the axisymmetric r U vanishes on the axis
+                    if (!(rho_n > 0.0)) bad |= 2u;
+                    else if (!(2.0 * rho_n * e_n - mm > 0.0)) bad |= 4u;
+                }
                 if (bad) atomicOr(a.health, bad);
             }
         }
@@ -1940,14 +1967,29 @@ size_t lift_batch_smem() {
            sizeof(Out) * (size_t)LiftBatchShape<DIM, NP>::EPB * LiftLayout<DIM, NP>::PER_ELEM;
 }
 
+// The dynamic shared-memory limit of a kernel, raised once per device (the
+// attribute is a property of the function in the device's context): a launch
+// then costs only the launch.  `done` is the calling instantiation's bitmask
+// of devices already set.
+inline cudaError_t smem_attribute_once(const void *kernel, int bytes, std::atomic<unsigned> &done) {
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    const unsigned bit = dev < 32 ? 1u << dev : 0u;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (err == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
+    return err;
+}
+
 template <int DIM, int NP, bool NS, bool VC, typename Real, bool CURV>
 cudaError_t rhs_launch_np(const MeshDev &m, const RhsArgs &a, const PhysParams &P, const OpTables &T,
                           cudaStream_t s) {
     using LY = RhsLayout<DIM, NP, NS, Real, 0, VC>;
     const int grid = (m.E + LY::EPB - 1) / LY::EPB;
     const size_t sm = rhs_smem<DIM, NP, NS, VC, Real>();
-    cudaError_t err = cudaFuncSetAttribute(rhs_kernel<DIM, NP, NS, VC, Real, CURV>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    static std::atomic<unsigned> smem_set{0u};
+    cudaError_t err = smem_attribute_once((const void *)rhs_kernel<DIM, NP, NS, VC, Real, CURV>, (int)sm, smem_set);
     if (err != cudaSuccess) return err;
     rhs_kernel<DIM, NP, NS, VC, Real, CURV><<<grid, LY::THREADS, sm, s>>>(m, a, P, T);
     return cudaGetLastError();
@@ -1968,8 +2010,8 @@ cudaError_t lift_launch_np(const MeshDev &m, const LiftArgs &a, const PhysParams
     using S = Shape<DIM, NP>;
     const int grid = (m.E + S::EPB - 1) / S::EPB;
     const size_t sm = lift_smem<DIM, NP, Out, CURV>();
-    cudaError_t err = cudaFuncSetAttribute(lift_kernel<DIM, NP, Out, VC, CURV>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    static std::atomic<unsigned> smem_set{0u};
+    cudaError_t err = smem_attribute_once((const void *)lift_kernel<DIM, NP, Out, VC, CURV>, (int)sm, smem_set);
     if (err != cudaSuccess) return err;
     lift_kernel<DIM, NP, Out, VC, CURV><<<grid, S::THREADS, sm, s>>>(m, a, P, T);
     return cudaGetLastError();

@@ -53,6 +53,14 @@ struct prandtl_handle {
     // non-affine elements: per-node geometry [dim*dim + 1][Ndof], per-face-node
     // normals [F][Np^(dim-1)][dim], subcell interface normals (blending)
     double *d_ngeo = nullptr, *d_fnn = nullptr, *d_snor = nullptr;
+    // prandtl_step's launch graph: kGraphSteps steps of one scheme on one state
+    // buffer with one dt, captured on cap_stream and replayed on `stream`
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t step_graph = nullptr;
+    double *graph_x = nullptr;
+    double graph_dt = 0.0;
+    int graph_scheme = -1;
+    long long graph_launches = 0;        // kernels per replay
     size_t bytes = 0;
     long long launches = 0;
     // optional per-kernel CUDA-event timing (prandtl_profile)
@@ -205,12 +213,103 @@ void free_all(prandtl_handle *h) {
     cudaFree(h->d_ngeo);
     cudaFree(h->d_fnn);
     cudaFree(h->d_snor);
+    if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
+    if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     if (h->done) cudaEventDestroy(h->done);
     for (auto &r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (auto ev : h->ev_pool) cudaEventDestroy(ev);
     h->recs.clear();
     h->ev_pool.clear();
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+}
+
+// The stage launches of `nsteps` steps on the device state x: SSP-RK3 (Shu-Osher,
+// x -> y1 -> y2 -> x) or LSRK4(5) (2N storage, ping-pong with the state back in
+// x at the end).  Every stage ORs its state check into the handle's flag.
+prandtl_status enqueue_steps(prandtl_handle *h, double *x, double dt, int scheme, int nsteps) {
+    prandtl_status st = PRANDTL_OK;
+    if (scheme == PRANDTL_RK3SSP) {
+        double *y1 = h->d_rk1, *y2 = h->d_rk2;
+        for (int s = 0; s < nsteps && st == PRANDTL_OK; ++s) {
+            RhsArgs a{};
+            a.dt = dt;
+            a.x0 = x;
+            a.health = h->d_health;
+            a.mode = EPI_SSP1; a.u_out = y1;
+            if ((st = run_rhs(h, x, a)) != PRANDTL_OK) break;
+            a.mode = EPI_SSP2; a.u_out = y2;
+            if ((st = run_rhs(h, y1, a)) != PRANDTL_OK) break;
+            a.mode = EPI_SSP3; a.u_out = x;
+            st = run_rhs(h, y2, a);
+        }
+        return st;
+    }
+    static const double A[5] = {0.0, -567301805773.0 / 1357537059087.0,
+                                -2404267990393.0 / 2016746695238.0,
+                                -3550918686646.0 / 2091501179385.0,
+                                -1275806237668.0 / 842570457699.0};
+    static const double B[5] = {1432997174477.0 / 9575080441755.0,
+                                5161836677717.0 / 13612068292357.0,
+                                1720146321549.0 / 2090206949498.0,
+                                3134564353537.0 / 4481467310338.0,
+                                2277821191437.0 / 14882151754819.0};
+    double *cur = x, *other = (x == h->d_in) ? h->d_out : h->d_rk2;
+    double *du = h->d_rk1;
+    for (int s = 0; s < nsteps && st == PRANDTL_OK; ++s)
+        for (int k = 0; k < 5; ++k) {
+            RhsArgs a{};
+            a.mode = EPI_LSRK;
+            a.health = h->d_health;
+            a.dt = dt;
+            a.rkA = A[k];
+            a.rkB = B[k];
+            a.du = du;
+            a.u_out = other;
+            if ((st = run_rhs(h, cur, a)) != PRANDTL_OK) break;
+            std::swap(cur, other);
+        }
+    if (st == PRANDTL_OK && cur != x)
+        CK(h, cudaMemcpyAsync(x, cur, (size_t)h->nf * h->Ndof * sizeof(double), cudaMemcpyDeviceToDevice,
+                              h->stream), "copy result");
+    return st;
+}
+
+// Steps per captured graph: even, so that LSRK's ping-pong ends in x.
+constexpr int kGraphSteps = 4;
+
+// The handle's step graph for (x, dt, scheme), captured on its capture stream
+// the first time (and whenever one of them changes).
+prandtl_status step_graph_for(prandtl_handle *h, double *x, double dt, int scheme) {
+    if (h->step_graph && h->graph_x == x && h->graph_dt == dt && h->graph_scheme == scheme) return PRANDTL_OK;
+    if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
+    h->step_graph = nullptr;
+    const cudaStream_t run = h->stream;
+    const long long before = h->launches;
+    h->stream = h->cap_stream;
+    // relaxed: the first launch of a kernel on this device may set its
+    // shared-memory attribute (a host-side call) while the stream captures
+    cudaError_t e = cudaStreamBeginCapture(h->cap_stream, cudaStreamCaptureModeRelaxed);
+    prandtl_status st = e == cudaSuccess ? enqueue_steps(h, x, dt, scheme, kGraphSteps) : PRANDTL_OK;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e2 = e == cudaSuccess ? cudaStreamEndCapture(h->cap_stream, &g) : e;
+    h->stream = run;
+    h->graph_launches = h->launches - before;
+    h->launches = before;
+    if (st != PRANDTL_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e2 != cudaSuccess) return cuda_fail(h, e2, "capture step graph");
+    e = cudaGraphInstantiate(&h->step_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        h->step_graph = nullptr;
+        return cuda_fail(h, e, "instantiate step graph");
+    }
+    h->graph_x = x;
+    h->graph_dt = dt;
+    h->graph_scheme = scheme;
+    return PRANDTL_OK;
 }
 
 template <typename T>
@@ -304,6 +403,8 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
     h->own_stream = true;
     if ((ce = cudaEventCreateWithFlags(&h->done, cudaEventDisableTiming)) != cudaSuccess)
         return bail(cuda_fail(h, ce, "cudaEventCreate"));
+    if ((ce = cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(cuda_fail(h, ce, "cudaStreamCreate (capture)"));
     const size_t S = (size_t)h->nf * h->Ndof;
     const int GEO = dim * dim + 1;
     if ((st = dalloc(h, &h->d_geo, (size_t)E * GEO, "geometry")) != PRANDTL_OK) return bail(st);
@@ -453,48 +554,18 @@ prandtl_status prandtl_step(prandtl_handle *h, double *u, double t, double dt, i
         x = h->d_in;
     }
     prandtl_status st = PRANDTL_OK;
-    if (scheme == PRANDTL_RK3SSP) {
-        double *y1 = h->d_rk1, *y2 = h->d_rk2;
-        for (int s = 0; s < nsteps && st == PRANDTL_OK; ++s) {
-            RhsArgs a{};
-            a.dt = dt;
-            a.x0 = x;
-            a.health = h->d_health;
-            a.mode = EPI_SSP1; a.u_out = y1;
-            if ((st = run_rhs(h, x, a)) != PRANDTL_OK) break;
-            a.mode = EPI_SSP2; a.u_out = y2;
-            if ((st = run_rhs(h, y1, a)) != PRANDTL_OK) break;
-            a.mode = EPI_SSP3; a.u_out = x;
-            st = run_rhs(h, y2, a);
+    int left = nsteps;
+    // long runs replay a captured graph of kGraphSteps steps (one launch per
+    // replay instead of one per kernel); the remainder runs launch by launch
+    if (!h->profiling && nsteps >= 2 * kGraphSteps) {
+        st = step_graph_for(h, x, dt, scheme);
+        for (; st == PRANDTL_OK && left >= kGraphSteps; left -= kGraphSteps) {
+            cudaError_t e = cudaGraphLaunch(h->step_graph, h->stream);
+            if (e != cudaSuccess) st = cuda_fail(h, e, "step graph launch");
+            else h->launches += h->graph_launches;
         }
-    } else {
-        static const double A[5] = {0.0, -567301805773.0 / 1357537059087.0,
-                                    -2404267990393.0 / 2016746695238.0,
-                                    -3550918686646.0 / 2091501179385.0,
-                                    -1275806237668.0 / 842570457699.0};
-        static const double B[5] = {1432997174477.0 / 9575080441755.0,
-                                    5161836677717.0 / 13612068292357.0,
-                                    1720146321549.0 / 2090206949498.0,
-                                    3134564353537.0 / 4481467310338.0,
-                                    2277821191437.0 / 14882151754819.0};
-        double *cur = x, *other = (x == h->d_in) ? h->d_out : h->d_rk2;
-        double *du = h->d_rk1;
-        for (int s = 0; s < nsteps && st == PRANDTL_OK; ++s)
-            for (int k = 0; k < 5; ++k) {
-                RhsArgs a{};
-                a.mode = EPI_LSRK;
-                a.health = h->d_health;
-                a.dt = dt;
-                a.rkA = A[k];
-                a.rkB = B[k];
-                a.du = du;
-                a.u_out = other;
-                if ((st = run_rhs(h, cur, a)) != PRANDTL_OK) break;
-                std::swap(cur, other);
-            }
-        if (st == PRANDTL_OK && cur != x)
-            CK(h, cudaMemcpyAsync(x, cur, bytes, cudaMemcpyDeviceToDevice, h->stream), "copy result");
     }
+    if (st == PRANDTL_OK) st = enqueue_steps(h, x, dt, scheme, left);
     if (st != PRANDTL_OK) return st;
     if (!dev) {
         CK(h, cudaMemcpyAsync(u, x, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H u");

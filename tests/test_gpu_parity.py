@@ -222,3 +222,36 @@ def test_blending_in_alternate_elements_of_a_warp(oracle_mod, dim, n, order):
             assert normalized_error(d, ref["dudt"], mesh.num_fields) <= RHS_TOL
             np.testing.assert_allclose(op.alpha(), alpha, rtol=0, atol=1e-12)
     op.close()
+
+
+@pytest.mark.parametrize("scheme", ["RK3SSP", "LSRK45"])
+@pytest.mark.parametrize("device", [False, True])
+def test_step_graph_replay_bit_identical(scheme, device):
+    """prandtl_step replays a captured graph for runs of >= 8 steps: the same
+    states as one launch sequence per step, and the same launch count."""
+    mesh = periodic_box(2, 6, 3, 0.0, 1.0, affine=_affine(2))
+    u0 = _state(mesh, seed=3, amp=0.2)
+    op_a = _op(mesh, blending=True, quirks="fixed")
+    op_b = _op(mesh, blending=True, quirks="fixed")
+    dt = 1e-4
+    if device:
+        torch = pytest.importorskip("torch")
+        ua, ub = torch.from_numpy(u0).cuda(), torch.from_numpy(u0).cuda()
+    else:
+        ua, ub = u0.copy(), u0.copy()
+    op_a.Step(ua, dt, scheme=scheme, nsteps=13)   # 3 graph replays + 1 step launched directly
+    for _ in range(13):
+        op_b.Step(ub, dt, scheme=scheme, nsteps=1)
+    op_a.synchronize()
+    op_b.synchronize()
+    a = ua.cpu().numpy() if device else ua
+    b = ub.cpu().numpy() if device else ub
+    assert np.array_equal(a, b)
+    assert op_a.kernel_launches == op_b.kernel_launches
+    op_a.Step(ua, dt, scheme=scheme, nsteps=8)    # the cached graph again
+    op_b.Step(ub, dt, scheme=scheme, nsteps=8)
+    op_a.synchronize()
+    op_b.synchronize()
+    a = ua.cpu().numpy() if device else ua
+    b = ub.cpu().numpy() if device else ub
+    assert np.array_equal(a, b)
