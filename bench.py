@@ -741,6 +741,10 @@ def run_serving(torch, n_req, check_every=15):
     # per-request work, to relate latency to size
     work = np.array([(m.n ** (3 if m.kind == "tgv" else 2)) * (m.order + 1) ** (3 if m.kind == "tgv" else 2)
                      * (5 if m.kind == "tgv" else 4) * m.nsteps for m in reqs], dtype=np.float64)
+    # slowdown: time to solution over the request's own share of the device at the
+    # stream's busy throughput (its DOF-updates / busy rate); 1 = served as if alone
+    busy_rate = st["dof_updates"] / max(st["busy_s"], 1e-9)
+    slow = np.array([lat[k] / (work[k] / busy_rate) for k in range(len(reqs)) if lat[k] is not None])
     return {"requests": len(reqs), "completed": int(len(ok)), "failed": len(errors), "precision": "fp32-bulk",
             "arrivals": f"Poisson at {rate:.2f}/s = 0.8 x capacity {capacity:.2f}/s (closed burst of 48)",
             "p50_ms": float(np.percentile(ok, 50)), "p99_ms": float(np.percentile(ok, 99)),
@@ -751,6 +755,7 @@ def run_serving(torch, n_req, check_every=15):
             "batch_steps": st["steps"], "checked_vs_fp64_plain": checked,
             "max_rel_l2_vs_fp64_plain": worst,
             "work_dof_updates_p50_p99": [float(np.percentile(work, 50)), float(np.percentile(work, 99))],
+            "slowdown_p50_p99": [float(np.percentile(slow, 50)), float(np.percentile(slow, 99))],
             "admission": "arrival order; later requests that fit may pass a waiting one, at most 64 times each",
             "mix": "50% 2D Euler isentropic vortex (16^2..128^2, N 3|4), 50% 3D NS TGV (8^3..24^3, N 2|3), "
                    "50..500 steps"}
