@@ -27,7 +27,8 @@ Keys of the JSON line:
               time-to-solution and throughput.
   e2e         the headline metric through the C ABI with pinned host buffers:
               admission (H2D), tuning, W+K steps and reading every result
-              (D2H), by wall clock.
+              (D2H), by wall clock (the clock sampler's own start and stop,
+              0.4 s of sleeps, are left out of that window).
   roofline    the dominant launch (the N=5 class RHS): FP32 CUDA-core FLOP/s
               against the FP32 SGEMM rate measured live in this run, with the
               launch's HBM bytes alongside.
@@ -137,10 +138,12 @@ class ClockSampler:
         import tempfile
         self.index = index
         self.proc = None
+        self.overhead_s = 0.0   # time spent starting and stopping the sampler
         folder = os.environ.get("PRANDTL_BENCH_CLOCKS_DIR") or tempfile.mkdtemp(prefix="prandtl_clocks_")
         self.path = os.path.join(folder, f"clocks_{tag}_rank{index}.csv")
 
     def __enter__(self):
+        t0 = time.perf_counter()
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
@@ -154,9 +157,11 @@ class ClockSampler:
             time.sleep(0.3)
         except Exception:
             self.proc = None
+        self.overhead_s += time.perf_counter() - t0
         return self
 
     def __exit__(self, *a):
+        t0 = time.perf_counter()
         if self.proc:
             time.sleep(0.1)
             self.proc.terminate()
@@ -165,6 +170,7 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
             self.f.close()
+        self.overhead_s += time.perf_counter() - t0
 
     def summary(self):
         if not self.proc:
@@ -374,7 +380,8 @@ def run_batch(torch, items, K, W, barrier, local):
     launches = b.kernel_launches - launches0
     for k, sid in enumerate(ids):
         b.read(sid, outs[k])
-    wall = time.perf_counter() - t0
+    # the e2e window without the clock sampler's own start and stop (instrumentation)
+    wall = time.perf_counter() - t0 - clk.overhead_s
     classes = {}
     for order in sorted({m.order for m, _, _, _ in items}):
         v, ms, lift = b.class_info(3, order, True)
