@@ -293,3 +293,20 @@ def test_oracle_curved_free_stream(oracle_mod, dim, order):
     for par in (0, 1):
         d = oracle_mod.Oracle(mesh, quirks=1, parabolic=par).rhs(u)["dudt"]
         assert np.abs(d).max() < 1e-12
+
+
+@pytest.mark.parametrize("order,nx,ny", [(1, 12, 6), (2, 8, 4)])
+def test_oracle_ramp_matches_reference_sources(oracle_mod, order, nx, ny):
+    """The reference's axisymmetric Ramp case geometry (trapezoidal cells over
+    the cone, inflow / outflow / axis / slip-wall boundaries, blending) through
+    the reference's own integrators."""
+    _ref(oracle_mod)
+    mesh = cases.ramp_mesh(order, nx, ny)
+    U = cases.perturbed(mesh, cases.free_stream(mesh, rho=1.0, vel=[2.0, 0.0], p=1 / 1.4),
+                        amp=0.3, seed=order).reshape(4, -1)
+    rU = (U * mesh.coords[1][None, :]).reshape(-1)
+    kw = dict(quirks=0, bcs=cases.RAMP_BCS, axisymmetric=1, blending=1)
+    o = oracle_mod.Oracle(mesh, **kw).rhs(rU, want_alpha=True)
+    r = oracle_mod.RefOperator(mesh, **kw).rhs(rU, want_alpha=True)
+    assert normalized_error(o["dudt"], r["dudt"], 4) <= 1e-13
+    np.testing.assert_allclose(o["alpha"], r["alpha"], rtol=0, atol=1e-14)
