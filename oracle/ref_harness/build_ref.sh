@@ -41,10 +41,13 @@ build() {
   local name="$1"; shift
   $CXX $FLAGS "$@" $INC $FILES -o "$OUT/libref_$name.so"
 }
-build euler
-build euler_blend -DSUBCELL_FV_BLENDING
-build ns -DPARABOLIC
-build ns_blend -DPARABOLIC -DSUBCELL_FV_BLENDING
-build euler_axi -DAXISYMMETRIC
-build euler_blend_axi -DSUBCELL_FV_BLENDING -DAXISYMMETRIC
+# the six variants compile in parallel; any failure fails the script
+pids=()
+build euler & pids+=($!)
+build euler_blend -DSUBCELL_FV_BLENDING & pids+=($!)
+build ns -DPARABOLIC & pids+=($!)
+build ns_blend -DPARABOLIC -DSUBCELL_FV_BLENDING & pids+=($!)
+build euler_axi -DAXISYMMETRIC & pids+=($!)
+build euler_blend_axi -DSUBCELL_FV_BLENDING -DAXISYMMETRIC & pids+=($!)
+for p in "${pids[@]}"; do wait "$p"; done
 echo "built $(ls "$OUT"/libref_*.so | wc -l) reference libraries in $OUT"
