@@ -62,13 +62,17 @@ def _old_corner(frame, dim, b):
     return sum(((((b >> r) & 1) ^ ((f >> r) & 1)) << p[r]) for r in range(dim))
 
 
-def write_gmsh_box(path, dim, n, lo, hi, shear=None, names=None, seed=0):
+def write_gmsh_box(path, dim, n, lo, hi, shear=None, names=None, seed=0, warp=None):
     """Box of quads / hexes with one physical group per side (names[2*d+s]) and
-    elements listed from a random proper rotation of their corners."""
+    elements listed from a random proper rotation of their corners.  `warp`
+    (a function of the grid points [..., dim], returning moved points) makes
+    the elements non-affine."""
     rng = np.random.default_rng(seed)
     n = tuple(n)
     shear = np.eye(dim) if shear is None else np.asarray(shear)
     X = _grid(dim, n, lo, hi, shear)
+    if warp is not None:
+        X = warp(X)
     shape = tuple(v + 1 for v in n)
     nid = lambda idx: int(np.ravel_multi_index(idx, shape, order="F")) + 1
     names = names or [f"side{k}" for k in range(2 * dim)]
@@ -127,6 +131,22 @@ def main():
                    ["left", "right", "bottom", "lid"], seed=1)
     write_gmsh_box(os.path.join(OUT, "channel_4x3x2.msh"), 3, (4, 3, 2), (0.0, 0.0, 0.0), (2.0, 1.0, 1.0), SHEAR3,
                    ["inlet", "outlet", "south", "north", "bottom", "top"], seed=2)
+    # non-affine elements: a channel over a bump (trapezoids over the bump) and a
+    # smoothly warped box of hexahedra
+    def bump(X):
+        x, y = X[..., 0], X[..., 1]
+        floor = 0.12 * np.sin(np.pi * np.clip(x - 0.5, 0.0, 1.0)) ** 2
+        return np.stack([x, floor + (1.0 - floor) * y], axis=-1)
+
+    def wobble(X):
+        x, y, z = X[..., 0], X[..., 1], X[..., 2]
+        return np.stack([x + 0.04 * np.sin(np.pi * y) * np.sin(np.pi * z),
+                         y + 0.05 * np.sin(np.pi * x / 2) * np.sin(np.pi * z),
+                         z + 0.03 * np.sin(np.pi * x / 2) * np.sin(np.pi * y)], axis=-1)
+    write_gmsh_box(os.path.join(OUT, "bump_8x4.msh"), 2, (8, 4), (0.0, 0.0), (2.0, 1.0), None,
+                   ["inlet", "outlet", "floor", "top"], seed=3, warp=bump)
+    write_gmsh_box(os.path.join(OUT, "warped_3x3x2.msh"), 3, (3, 3, 2), (0.0, 0.0, 0.0), (2.0, 1.0, 1.0), None,
+                   ["inlet", "outlet", "south", "north", "bottom", "top"], seed=4, warp=wobble)
     print("wrote", sorted(os.listdir(OUT)))
 
 

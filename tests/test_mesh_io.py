@@ -232,3 +232,32 @@ def test_multilinear_refinement_keeps_the_geometry(tmp_path):
     assert m.num_elements == 4 and not m.affine
     area = (m.node_weights()).sum()
     assert area == pytest.approx(1.75, rel=1e-14)   # (2 + 1.5) / 2 * 1
+
+
+@pytest.mark.parametrize("name,order,measure", [("bump_8x4.msh", 3, None), ("warped_3x3x2.msh", 2, 2.0)])
+@pytest.mark.parametrize("refine,hilbert", [(0, False), (1, True), (2, False)])
+def test_multilinear_fixture_meshes(name, order, measure, refine, hilbert):
+    """Gmsh meshes of non-affine elements listed from random corner rotations:
+    read with multilinear geometry, positive det J at every node, the domain
+    measure kept by refinement, and face-node normals that are the elements'
+    adjugate rows on both sides of every interior face."""
+    m = read_mesh(os.path.join(MESHES, name), order, refine=refine, hilbert=hilbert)
+    assert not m.affine and (m.node_detj > 0).all()
+    area = m.node_weights().sum()
+    if measure is None:   # the bump channel: 2 minus the area under the piecewise-linear floor
+        xs = np.linspace(0.0, 2.0, 9)
+        floor = 0.12 * np.sin(np.pi * np.clip(xs - 0.5, 0.0, 1.0)) ** 2
+        measure = 2.0 - np.trapezoid(floor, xs)
+    assert area == pytest.approx(measure, rel=1e-13)
+    from prandtl_b200.mesh import face_node
+    dim, Np = m.dim, m.order + 1
+    for fc in range(m.num_faces):
+        e1, l1, e2, l2 = (int(v) for v in m.face_elems[fc])
+        if e2 < 0:
+            continue
+        for a in range(Np ** (dim - 1)):
+            n1, n2 = face_node(dim, Np, l1, a), face_node(dim, Np, l2, a)
+            s1 = 1.0 if l1 & 1 else -1.0
+            s2 = 1.0 if l2 & 1 else -1.0
+            np.testing.assert_allclose(m.face_node_nor[fc, a], s1 * m.node_adj[e1, n1, l1 >> 1], rtol=0, atol=1e-14)
+            np.testing.assert_allclose(m.face_node_nor[fc, a], -s2 * m.node_adj[e2, n2, l2 >> 1], rtol=0, atol=1e-13)
