@@ -361,7 +361,10 @@ def run_batch(torch, items, K, W, barrier, local):
     t0 = time.perf_counter()
     b = Batch("fp32", "LSRK45")
     ids = [b.add(mesh, pinned[k], dt=dt, nsteps=W + K, **m.physics()) for k, (m, mesh, _, dt) in enumerate(items)]
+    b.sync()
+    t_admit = time.perf_counter() - t0
     b.tune(reps=2)
+    t_tune = time.perf_counter() - t0 - t_admit
     b.advance(W)
     b.sync()
     stream = torch.cuda.ExternalStream(b.stream)
@@ -378,8 +381,10 @@ def run_batch(torch, items, K, W, barrier, local):
         barrier()
     device_s = ev0.elapsed_time(ev1) / 1e3
     launches = b.kernel_launches - launches0
+    t_r = time.perf_counter()
     for k, sid in enumerate(ids):
         b.read(sid, outs[k])
+    t_read = time.perf_counter() - t_r
     # the e2e window without the clock sampler's own start and stop (instrumentation)
     wall = time.perf_counter() - t0 - clk.overhead_s
     classes = {}
@@ -387,6 +392,7 @@ def run_batch(torch, items, K, W, barrier, local):
         v, ms, lift = b.class_info(3, order, True)
         classes[order] = {"variant": v, "rhs_ms_per_variant": ms, "lift_ms": lift}
     info = {"device_s": device_s, "wall_s": wall, "launches": launches, "device_bytes": b.device_bytes,
+            "window_s": {"admit": t_admit, "tune": t_tune, "read": t_read, "total": wall},
             "classes": classes, "clocks": clk.summary()}
     b.close()
     return [o.numpy() for o in outs], info
@@ -908,7 +914,8 @@ def main():
             "e2e": {"value": dof * (W + K) * world / wall_s, "unit": "DOF-updates/s",
                     "h2d_bytes_per_step": u_bytes / (W + K), "d2h_bytes_per_step": u_bytes / (W + K),
                     "window": "admission from pinned host memory + tuning + W+K steps + every state read back; "
-                              "the states cross once per solve, bytes shown per step"},
+                              "the states cross once per solve, bytes shown per step",
+                    "window_s": binfo["window_s"]},
             "gpu_launches": binfo["launches"],
             "roofline": roofline,
             "cpu_baseline": cpu,
