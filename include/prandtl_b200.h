@@ -80,9 +80,10 @@ typedef struct prandtl_mesh_desc {
      * node (ElementTransformation::SetIntPoint + AdjugateJacobian / Weight,
      * DGSEMIntegrator.cpp:254-267, LiftingBR1.cpp:184-186) and CalcOrtho at
      * every face point (DGSEMIntegrator.cpp:151-222); these arrays hold those
-     * values.  Only FP64 handles (prandtl_create, precision 0) take them:
-     * FP32-bulk handles, batches and prandtl_rhs_noalloc return
-     * PRANDTL_EUNSUPPORTED.  elem_adj / elem_detj / face_nor are still read
+     * values.  prandtl_create takes them in the FP64 form and, for Euler, in
+     * the FP32-bulk form; FP32-bulk Navier-Stokes, batches and
+     * prandtl_rhs_noalloc return PRANDTL_EUNSUPPORTED.  elem_adj / elem_detj /
+     * face_nor are still read
      * (validation, the element size) and may hold the element-centre values. */
     const double *node_adj;    /* [E][Np^dim][dim][dim] adj(J) at each node, row-major */
     const double *node_detj;   /* [E][Np^dim] det J at each node (> 0) */

@@ -670,7 +670,7 @@ template <int DIM, int NP, bool NS, bool VC, typename Real, typename LY, bool CU
 __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P, int e, bool active,
                                             const Real *sT, const uint32_t *sPair, Real *sH, int li, int lane,
                                             int gid) {
-    static_assert(!CURV || sizeof(Real) == 8, "non-affine elements: FP64 kernels only");
+    static_assert(!CURV || sizeof(Real) == 8 || !NS, "non-affine elements: FP64, or FP32-bulk Euler");
     using S = Shape<DIM, NP>;
     constexpr int ND = S::ND, NF = S::NF, PPL = S::PPL;
     constexpr int NFN = S::NFN, NFI = S::NFI, GS = LY::GS, NPL = LY::NPL;
@@ -1506,7 +1506,7 @@ __device__ __forceinline__ void rhs_element(const ElemIO &a, const PhysParams &P
 }
 
 // One-shot kernel: grid = ceil(E / EPB), one element per lane group.  CURV:
-// non-affine elements (per-node geometry, FP64).
+// non-affine elements (per-node geometry; FP64, or FP32-bulk Euler).
 template <int DIM, int NP, bool NS, bool VC, typename Real, bool CURV>
 __global__ void __launch_bounds__(RhsLayout<DIM, NP, NS, Real, 0, VC>::THREADS, (RhsLayout<DIM, NP, NS, Real, 0, VC>::MIN_BLOCKS))
 rhs_kernel(const MeshDev m, const RhsArgs a, const PhysParams P, const __grid_constant__ OpTables T) {
@@ -1998,8 +1998,8 @@ cudaError_t rhs_launch_np(const MeshDev &m, const RhsArgs &a, const PhysParams &
 template <int DIM, int NP, bool NS, bool VC, typename Real>
 cudaError_t rhs_launch_any(const MeshDev &m, const RhsArgs &a, const PhysParams &P, const OpTables &T,
                            cudaStream_t s) {
-    if (m.ngeo) {
-        if constexpr (sizeof(Real) == 8) return rhs_launch_np<DIM, NP, NS, VC, Real, true>(m, a, P, T, s);
+    if (m.ngeo) {   // FP64, or the FP32-bulk Euler form (pair phase; no lifting)
+        if constexpr (sizeof(Real) == 8 || !NS) return rhs_launch_np<DIM, NP, NS, VC, Real, true>(m, a, P, T, s);
         else return cudaErrorNotSupported;
     }
     return rhs_launch_np<DIM, NP, NS, VC, Real, false>(m, a, P, T, s);

@@ -359,8 +359,8 @@ prandtl_status prandtl_create(const prandtl_mesh_desc *md, const prandtl_config 
         if (vst == PRANDTL_OK) vst = validate_mesh(md, nbr, msg, cfg->num_bcs);
         if (vst == PRANDTL_OK) vst = check_viscous_bcs(md, cfg, msg);
         if (vst == PRANDTL_OK) vst = check_curved(md, msg);
-        if (vst == PRANDTL_OK && mesh_curved(md) && cfg->precision != 0) {
-            msg = "non-affine elements run in the FP64 form only (precision 0)";
+        if (vst == PRANDTL_OK && mesh_curved(md) && cfg->precision != 0 && cfg->parabolic) {
+            msg = "non-affine Navier-Stokes runs in the FP64 form only (precision 0); FP32 bulk takes Euler";
             vst = PRANDTL_EUNSUPPORTED;
         }
         if (vst == PRANDTL_OK && cfg->parabolic && cfg->quirks != 0)

@@ -203,8 +203,9 @@ def test_axisymmetric_configuration_checked_before_the_device(lib):
 
 
 def test_non_affine_descriptor_checked_before_the_device(lib):
-    """Per-node geometry: all three arrays or none, positive det J, FP64 only,
-    and in fixed Navier-Stokes the face-node normals must be the adjugate rows."""
+    """Per-node geometry: all three arrays or none, positive det J, FP64 or
+    FP32-bulk Euler, and in fixed Navier-Stokes the face-node normals must be
+    the adjugate rows."""
     import sys
     from prandtl_b200 import _lib
     from prandtl_b200.mesh import periodic_box
@@ -215,7 +216,7 @@ def test_non_affine_descriptor_checked_before_the_device(lib):
         return periodic_box(2, 3, 2, warp=make_golden.warp_field(2, 0.06))
     arr = MeshArrays(mesh())
     h = C.c_void_p()
-    st = lib.prandtl_create(C.byref(arr.desc), C.byref(make_config(precision="fp32")), C.byref(h))
+    st = lib.prandtl_create(C.byref(arr.desc), C.byref(make_config(precision="fp32", parabolic=True)), C.byref(h))
     assert st == _lib.PRANDTL_EUNSUPPORTED
     assert b"FP64" in lib.prandtl_last_error(None)
     part = MeshArrays(mesh())

@@ -174,11 +174,11 @@ def test_curved_conservation_budget():
 
 
 def test_curved_rejected_where_not_built():
-    """FP32-bulk handles and batches take affine meshes only."""
+    """FP32-bulk Navier-Stokes handles and batches take affine meshes only."""
     from prandtl_b200 import _lib
     mesh = _mesh(2, 3, 2)
     with pytest.raises(_lib.PrandtlError) as ei:
-        _op(mesh, precision="fp32")
+        _op(mesh, precision="fp32", parabolic=True)
     assert ei.value.status == _lib.PRANDTL_EUNSUPPORTED
     from prandtl_b200.batch import Batch
     b = Batch(precision="fp64", arena_bytes=64 << 20)
@@ -225,3 +225,34 @@ def test_ramp_trajectory_matches_oracle(oracle_mod):
     op.Step(u, dt, scheme="RK3SSP", nsteps=100)
     assert normalized_error(u, ref, 4) <= TRAJ_TOL
     assert (orc.rhs(ref, want_alpha=True)["alpha"] > 0).any()
+
+
+@pytest.mark.parametrize("dim,order", [(2, 1), (2, 3), (3, 2)])
+def test_curved_fp32_euler_tracks_fp64(dim, order):
+    """The FP32-bulk Euler form on multilinear elements: the same state after
+    20 LSRK steps as the FP64 form within 1e-5 relative L2 per field (the
+    FP32-bulk tolerance), with blending."""
+    mesh = _mesh(dim, 3, order)
+    u0 = _state(mesh, seed=11, amp=0.2)
+    dt = 0.2 * mesh.hmin / (2.0 * (order + 1) ** 2)
+    u64, u32 = u0.copy(), u0.copy()
+    _op(mesh, blending=True, quirks="fixed").Step(u64, dt, scheme="LSRK45", nsteps=20)
+    _op(mesh, blending=True, quirks="fixed", precision="fp32").Step(u32, dt, scheme="LSRK45", nsteps=20)
+    a, b = u32.reshape(mesh.num_fields, -1), u64.reshape(mesh.num_fields, -1)
+    for f in range(mesh.num_fields):
+        assert np.linalg.norm(a[f] - b[f]) <= 1e-5 * np.linalg.norm(b[f])
+    assert not np.array_equal(a, b)   # the FP32 kernels did run
+
+
+def test_ramp_fp32_tracks_fp64():
+    """The Ramp case in the FP32-bulk form (axisymmetric, blended, multilinear)
+    against the FP64 form after 200 SSP-RK3 steps at the reference's dt."""
+    mesh = cases.ramp_mesh(1, 24, 12)
+    u0 = cases.ramp_ic(mesh)
+    kw = dict(quirks="reference", blending=True, bcs=cases.RAMP_BCS, axisymmetric=True)
+    u64, u32 = u0.copy(), u0.copy()
+    _op(mesh, **kw).Step(u64, 1e-3, scheme="RK3SSP", nsteps=200)
+    _op(mesh, precision="fp32", **kw).Step(u32, 1e-3, scheme="RK3SSP", nsteps=200)
+    a, b = u32.reshape(4, -1), u64.reshape(4, -1)
+    for f in range(4):
+        assert np.linalg.norm(a[f] - b[f]) <= 1e-5 * np.linalg.norm(b[f])
