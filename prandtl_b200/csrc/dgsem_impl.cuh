@@ -1981,6 +1981,16 @@ inline cudaError_t smem_attribute_once(const void *kernel, int bytes, std::atomi
     if (err == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
     return err;
 }
+// A launch refused for its shared memory (cudaErrorInvalidValue) after the
+// attribute was recorded as set means the device's context was reset since:
+// forget the device's bit so the next smem_attribute_once sets it again.
+inline bool smem_attribute_lost(cudaError_t err, size_t bytes, std::atomic<unsigned> &done) {
+    if (err != cudaErrorInvalidValue || bytes <= 48 * 1024) return false;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev >= 32) return false;
+    done.fetch_and(~(1u << dev), std::memory_order_acq_rel);
+    return true;
+}
 
 template <int DIM, int NP, bool NS, bool VC, typename Real, bool CURV>
 cudaError_t rhs_launch_np(const MeshDev &m, const RhsArgs &a, const PhysParams &P, const OpTables &T,
@@ -1989,12 +1999,16 @@ cudaError_t rhs_launch_np(const MeshDev &m, const RhsArgs &a, const PhysParams &
     const int grid = (m.E + LY::EPB - 1) / LY::EPB;
     const size_t sm = rhs_smem<DIM, NP, NS, VC, Real>();
     static std::atomic<unsigned> smem_set{0u};
-    cudaError_t err = smem_attribute_once((const void *)rhs_kernel<DIM, NP, NS, VC, Real, CURV>, (int)sm, smem_set);
-    if (err != cudaSuccess) return err;
-    rhs_kernel<DIM, NP, NS, VC, Real, CURV><<<grid, LY::THREADS, sm, s>>>(m, a, P, T);
-    return cudaGetLastError();
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        cudaError_t err = smem_attribute_once((const void *)rhs_kernel<DIM, NP, NS, VC, Real, CURV>, (int)sm, smem_set);
+        if (err != cudaSuccess) return err;
+        rhs_kernel<DIM, NP, NS, VC, Real, CURV><<<grid, LY::THREADS, sm, s>>>(m, a, P, T);
+        err = cudaGetLastError();
+        if (!smem_attribute_lost(err, sm, smem_set)) return err;
+    }
+    return cudaErrorInvalidValue;
 }
-// non-affine meshes (m.ngeo set) run the per-node-geometry kernels, FP64 only
+// non-affine meshes (m.ngeo set) run the per-node-geometry kernels (FP64, or FP32-bulk Euler)
 template <int DIM, int NP, bool NS, bool VC, typename Real>
 cudaError_t rhs_launch_any(const MeshDev &m, const RhsArgs &a, const PhysParams &P, const OpTables &T,
                            cudaStream_t s) {
@@ -2011,10 +2025,14 @@ cudaError_t lift_launch_np(const MeshDev &m, const LiftArgs &a, const PhysParams
     const int grid = (m.E + S::EPB - 1) / S::EPB;
     const size_t sm = lift_smem<DIM, NP, Out, CURV>();
     static std::atomic<unsigned> smem_set{0u};
-    cudaError_t err = smem_attribute_once((const void *)lift_kernel<DIM, NP, Out, VC, CURV>, (int)sm, smem_set);
-    if (err != cudaSuccess) return err;
-    lift_kernel<DIM, NP, Out, VC, CURV><<<grid, S::THREADS, sm, s>>>(m, a, P, T);
-    return cudaGetLastError();
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        cudaError_t err = smem_attribute_once((const void *)lift_kernel<DIM, NP, Out, VC, CURV>, (int)sm, smem_set);
+        if (err != cudaSuccess) return err;
+        lift_kernel<DIM, NP, Out, VC, CURV><<<grid, S::THREADS, sm, s>>>(m, a, P, T);
+        err = cudaGetLastError();
+        if (!smem_attribute_lost(err, sm, smem_set)) return err;
+    }
+    return cudaErrorInvalidValue;
 }
 template <int DIM, int NP, typename Out, bool VC>
 cudaError_t lift_launch_any(const MeshDev &m, const LiftArgs &a, const PhysParams &P, const OpTables &T,
