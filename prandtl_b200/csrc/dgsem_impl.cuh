@@ -1647,6 +1647,51 @@ __device__ __forceinline__ void boundary_lift_trace(const ElemIO &a, const PhysP
     }
 }
 
+// Per-node field rows of the lifting in shared memory, as 16-byte vectors:
+// row group q holds fields q*VW .. q*VW+VW-1 of every node as one VW-wide
+// vector per node ([NV][NITEM] vectors, VW = 4 floats or 2 doubles); the NF % VW
+// remaining fields follow as scalar rows ([NR][NITEM]).  One node's NF values
+// then take NV 16-byte accesses and NR scalar ones (FP32, 3D: 2 instead of 5).
+// Consecutive items are 16 bytes apart, so a warp's accesses to distinct
+// items are free of bank conflicts.  The base must be 16-byte aligned.
+template <typename W, int NF, int NITEM>
+struct FieldRows {
+    static constexpr int VW = 16 / (int)sizeof(W);
+    static constexpr int NV = NF / VW, NR = NF - NV * VW;
+    static constexpr int SIZE = (NF * NITEM + VW - 1) / VW * VW;   // in W, a multiple of 16 bytes
+    __device__ static __forceinline__ void store(W *s, int i, const W *v) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            if constexpr (VW == 4) {
+                reinterpret_cast<float4 *>(s)[q * NITEM + i] =
+                    make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            } else {
+                reinterpret_cast<double2 *>(s)[q * NITEM + i] = make_double2(v[2 * q], v[2 * q + 1]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < NR; ++r) s[NV * VW * NITEM + r * NITEM + i] = v[NV * VW + r];
+    }
+    __device__ static __forceinline__ void load(const W *s, int i, W *v) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            if constexpr (VW == 4) {
+                const float4 t = reinterpret_cast<const float4 *>(s)[q * NITEM + i];
+                v[4 * q] = t.x;
+                v[4 * q + 1] = t.y;
+                v[4 * q + 2] = t.z;
+                v[4 * q + 3] = t.w;
+            } else {
+                const double2 t = reinterpret_cast<const double2 *>(s)[q * NITEM + i];
+                v[2 * q] = t.x;
+                v[2 * q + 1] = t.y;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < NR; ++r) v[NV * VW + r] = s[NV * VW * NITEM + r * NITEM + i];
+    }
+};
+
 template <int DIM, int NP, typename W, bool VC, bool CURV = false>
 __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &P, int e, bool active,
                                              const W *sT, W *sElem, int n) {
@@ -1654,11 +1699,13 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
     constexpr int ND = S::ND, NF = S::NF, NFN = S::NFN, NFI = S::NFI;
     constexpr bool F64 = sizeof(W) == 8;
     static_assert(!CURV || F64, "non-affine elements: FP64 kernels only");
+    using VE = FieldRows<W, NF, ND>;
+    using SJ = FieldRows<W, NF, NFI>;
     const W *sD = sT, *sW = sT + 4 * NP * NP;
     W *gout = reinterpret_cast<W *>(a.grad);
-    W *sVe = sElem;                 // entropy variables [NF][ND]
-    W *sS = sVe + NF * ND;          // face jumps [NF][NFI]
-    W *sN = sS + NF * NFI;          // face normals [2 DIM][DIM] (one per local face);
+    W *sVe = sElem;                 // entropy variables, FieldRows over the nodes
+    W *sS = sVe + VE::SIZE;         // face jumps, FieldRows over the face items
+    W *sN = sS + SJ::SIZE;          // face normals [2 DIM][DIM] (one per local face);
                                     // non-affine: [NFI][DIM] (one per face node)
     const long long Ndof = a.Ndof;
     const long long gnode = (long long)e * ND + n;
@@ -1700,8 +1747,7 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
         R = entropy_ref<DIM>(s0, P);
         conserv2entropy_rel<DIM>(st, P, R, reinterpret_cast<float *>(v));
     }
-#pragma unroll
-    for (int f = 0; f < NF; ++f) sVe[f * ND + n] = v[f];
+    VE::store(sVe, n, v);
     // the transformation: per element, or (non-affine) at this thread's node
     // (LiftingBR1.cpp:184-186: Tr.SetIntPoint, Weight, AdjugateJacobian)
     const double *geo = a.geo + (long long)e * (DIM * DIM + 1);
@@ -1756,11 +1802,11 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
     for (int k = 0; k < MAXIT; ++k) {
         const int it = n + k * ND;
         if (it < NFI) {
+            W vo[NF], jf[NF];
+            VE::load(sVe, no[k], vo);
 #pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const W vo = sVe[f * ND + no[k]];
-                sS[f * NFI + it] = own1[k] ? W(0.5) * (vn[k][f] - vo) : W(0.5) * (vo - vn[k][f]);
-            }
+            for (int f = 0; f < NF; ++f) jf[f] = own1[k] ? W(0.5) * (vn[k][f] - vo[f]) : W(0.5) * (vo[f] - vn[k][f]);
+            SJ::store(sS, it, jf);
             if (CURV || it % NFN == 0) {
 #pragma unroll
                 for (int q = 0; q < DIM; ++q) sN[(CURV ? it : it / NFN) * DIM + q] = nor[k][q];
@@ -1781,8 +1827,10 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
 #pragma unroll
         for (int l = 0; l < NP; ++l) {
             const W dl = sD[c[r] * NP + l];
+            W vl[NF];
+            VE::load(sVe, base + l * stride, vl);
 #pragma unroll
-            for (int f = 0; f < NF; ++f) g1[f][r] += sVe[f * ND + base + l * stride] * dl;
+            for (int f = 0; f < NF; ++f) g1[f][r] += vl[f] * dl;
         }
     }
     // grad_mat2 = grad_mat1 * adj, times 1/J (LiftingBR1.cpp:205-206)
@@ -1806,8 +1854,7 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
         if (lf >= 0) {
             const int it = lf * NFN + face_tangential<DIM, NP>(d, c);
             W jf[NF], nq[DIM];
-#pragma unroll
-            for (int f = 0; f < NF; ++f) jf[f] = sS[f * NFI + it];
+            SJ::load(sS, it, jf);
 #pragma unroll
             for (int q = 0; q < DIM; ++q) nq[q] = sN[(CURV ? it : lf) * DIM + q];
 #pragma unroll
@@ -1850,10 +1897,16 @@ __device__ __forceinline__ void lift_element(const ElemIO &a, const PhysParams &
     }
 }
 
-template <int DIM, int NP, bool CURV = false>
+// Shared memory of the lifting: the tables (rounded to 16 bytes), then per
+// element the entropy variables, the face jumps and the normals, each element's
+// part a multiple of 16 bytes (FieldRows wants 16-byte aligned rows).
+template <int DIM, int NP, typename W, bool CURV = false>
 struct LiftLayout {
     using S = Shape<DIM, NP>;
-    static constexpr int PER_ELEM = S::NF * S::ND + S::NF * S::NFI + (CURV ? S::NFI * DIM : 2 * DIM * DIM);
+    static constexpr int VW = 16 / (int)sizeof(W);
+    static constexpr int TABW = (S::TAB + VW - 1) / VW * VW;
+    static constexpr int PER_ELEM = (FieldRows<W, S::NF, S::ND>::SIZE + FieldRows<W, S::NF, S::NFI>::SIZE +
+                                     (CURV ? S::NFI * DIM : 2 * DIM * DIM) + VW - 1) / VW * VW;
 };
 constexpr int prev_pow2(int v) { return v <= 1 ? 1 : 2 * prev_pow2(v / 2); }
 // Batch lift CTA: a power-of-two number of elements, so an item (one CTA's
@@ -1902,8 +1955,9 @@ lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_
     io.ngeo = m.ngeo;
     io.fnn = m.fnn;
     io.snor = nullptr;
+    using LL = LiftLayout<DIM, NP, Out, CURV>;
     lift_element<DIM, NP, Out, VC, CURV>(io, P, active ? e_raw : m.E - 1, active, smem,
-                                         smem + S::TAB + el * LiftLayout<DIM, NP, CURV>::PER_ELEM, n);
+                                         smem + LL::TABW + el * LL::PER_ELEM, n);
 }
 
 // Persistent batch lift: CTA-level items of EPB elements of one solve.
@@ -1941,7 +1995,7 @@ lift_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_const
         const int e_raw = e0 + el;
         const bool active = e_raw < E;
         lift_element<DIM, NP, Out, VC>(ctx->io, ctx->P, active ? e_raw : E - 1, active, sT,
-                                   sE + el * LiftLayout<DIM, NP>::PER_ELEM, nn);
+                                   sE + el * LiftLayout<DIM, NP, Out>::PER_ELEM, nn);
     }
 }
 
@@ -1958,13 +2012,14 @@ size_t rhs_batch_smem() {
 template <int DIM, int NP, typename Out, bool CURV>
 size_t lift_smem() {
     using S = Shape<DIM, NP>;
-    return sizeof(Out) * (S::TAB + (size_t)S::EPB * LiftLayout<DIM, NP, CURV>::PER_ELEM);
+    using LL = LiftLayout<DIM, NP, Out, CURV>;
+    return sizeof(Out) * (LL::TABW + (size_t)S::EPB * LL::PER_ELEM);
 }
 template <int DIM, int NP, typename Out>
 size_t lift_batch_smem() {
     using S = Shape<DIM, NP>;
     return (S::TAB * sizeof(Out) + 15) / 16 * 16 + CTX_RESERVE +
-           sizeof(Out) * (size_t)LiftBatchShape<DIM, NP>::EPB * LiftLayout<DIM, NP>::PER_ELEM;
+           sizeof(Out) * (size_t)LiftBatchShape<DIM, NP>::EPB * LiftLayout<DIM, NP, Out>::PER_ELEM;
 }
 
 // The dynamic shared-memory limit of a kernel, raised once per device (the
