@@ -253,7 +253,7 @@ constexpr int next_pow2(int v) { return v <= 1 ? 1 : 2 * next_pow2((v + 1) / 2);
 #define PRANDTL_NS32_MINB 4
 #endif
 #ifndef PRANDTL_LINE_MAX_NP
-#define PRANDTL_LINE_MAX_NP 4
+#define PRANDTL_LINE_MAX_NP 5
 #endif
 #ifndef PRANDTL_EULER32_MINB
 #define PRANDTL_EULER32_MINB 6
@@ -348,9 +348,10 @@ struct RhsLayout {
     static constexpr int MIN_BLOCKS = MINB_REQ < SMEM_BLOCKS ? MINB_REQ : SMEM_BLOCKS;
     // volume terms by line tasks (Navier-Stokes: the viscous-flux buffer holds
     // the per-direction results) or by pairs and node-wise sums.  Line tasks
-    // were measured faster in the FP32-bulk form up to Np = 4 (3-4 %) and with
-    // the 128-lane groups at Np = 6 (17 %); slower in FP64 and at Np = 5 (75
-    // tasks over 64 or 128 lanes).
+    // were measured faster in the FP32-bulk form up to Np = 4 (3-4 %), at
+    // Np = 5 on 64-lane groups (12 %, once the two-point fluxes of two partners
+    // share paired FP32 instructions; 128 lanes: no gain) and with the 128-lane
+    // groups at Np = 6 (17 %); slower in FP64.
     static constexpr bool LINE = NS && !F64 && (NP <= PRANDTL_LINE_MAX_NP || TASK128);
     static_assert(LINE == LINE_FORM, "viscous-buffer rows follow the volume form");
 };
@@ -1924,10 +1925,12 @@ struct LiftBatchShape {
 };
 
 // Resident CTAs the one-shot lift's register budget is sized for (measured at
-// 3D N=3: 5 beats 4 by 3.5 % in FP64, 6 beats 4 by 11 % in FP32; larger
-// elements keep 4).
+// 3D N=3: 5 beats 4 by 3.5 % in FP64 and 6 by -8 %, 6 beats 4 by 11 % in FP32;
+// FP32 at N=4: 6 beats 4 by 7 %; FP32 at N=5 and FP64 at N >= 4 keep 4).
 template <int NP, typename Out>
-constexpr int lift_min_blocks() { return NP <= 4 ? (sizeof(Out) == 8 ? PRANDTL_LIFT64_MINB : 6) : 4; }
+constexpr int lift_min_blocks() {
+    return NP <= 4 ? (sizeof(Out) == 8 ? PRANDTL_LIFT64_MINB : 6) : ((NP == 5 && sizeof(Out) == 4) ? 6 : 4);
+}
 
 template <int DIM, int NP, typename Out, bool VC, bool CURV>
 __global__ void __launch_bounds__(Shape<DIM, NP>::THREADS, lift_min_blocks<NP, Out>())

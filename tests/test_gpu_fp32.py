@@ -43,10 +43,12 @@ def test_fp32_rhs_tgv(order):
     assert max(errs) <= 2e-3, errs
 
 
-@pytest.mark.parametrize("dim", [2, 3])
-def test_fp32_rhs_reference_mode_navier_stokes(dim):
-    """Reference-mode NS (gradient form, the reference's defects kept) in FP32."""
-    mesh = periodic_box(dim, 3, 3, 0.0, 1.0, affine=np.eye(dim) + 0.1 * np.eye(dim, k=1))
+@pytest.mark.parametrize("dim,order", [(2, 3), (3, 3), (2, 4), (3, 4), (3, 5)])
+def test_fp32_rhs_reference_mode_navier_stokes(dim, order):
+    """Reference-mode NS (gradient form, the reference's defects kept) in FP32:
+    line tasks up to N = 4 (3D: 32- and 64-lane groups, where the eta flux
+    replaces a zeta line's lower partners) and the pair form at N = 5."""
+    mesh = periodic_box(dim, 3, order, 0.0, 1.0, affine=np.eye(dim) + 0.1 * np.eye(dim, k=1))
     base = cases.free_stream(mesh, rho=1.2, vel=[0.4, -0.3, 0.2][:dim], p=1.5)
     u = cases.perturbed(mesh, base, amp=0.1, seed=4)
     kw = dict(parabolic=True, mu=0.01, Pr=0.71, quirks="reference")
