@@ -415,6 +415,15 @@ prandtl_status prandtl_batch_remove(prandtl_batch *b, int id);
  * launch shape on the next step's first stage (which the step recomputes) and
  * keep the fastest. */
 prandtl_status prandtl_batch_tune(prandtl_batch *b, int reps);
+/* Autotuner inside the steps: the next n_variants steps that advances run
+ * (n_variants as prandtl_batch_class_info reports it) time one RHS launch
+ * shape each, step v running shape v in every class that has solves, with
+ * events around every lifting and RHS launch; the host waits for each of
+ * those steps (up to timeout_s).  After the last one each class keeps its
+ * fastest shape and the step graphs are rebuilt.  The shapes give
+ * bit-identical results, so the tuning does real steps instead of repeated
+ * launches.  prandtl_batch_tune cancels a pending tuning in the steps. */
+prandtl_status prandtl_batch_tune_in_steps(prandtl_batch *b);
 /* Launch shape chosen for a class and the tuned times (ms per launch, -1 when
  * not timed) of each of the *n_variants RHS shapes and of the lifting launch;
  * ms and lift_ms may be NULL. */

@@ -30,7 +30,7 @@ EXPORTS = ["prandtl_config_default", "prandtl_create", "prandtl_destroy", "prand
            "prandtl_batch_config_default", "prandtl_batch_create", "prandtl_batch_destroy",
            "prandtl_batch_footprint", "prandtl_batch_add", "prandtl_batch_advance",
            "prandtl_batch_sync", "prandtl_batch_finished", "prandtl_batch_query",
-           "prandtl_batch_read", "prandtl_batch_remove", "prandtl_batch_tune",
+           "prandtl_batch_read", "prandtl_batch_remove", "prandtl_batch_tune", "prandtl_batch_tune_in_steps",
            "prandtl_batch_class_info", "prandtl_batch_stream", "prandtl_batch_device_bytes",
            "prandtl_batch_arena_bytes", "prandtl_batch_time",
            "prandtl_batch_kernel_launches", "prandtl_batch_last_error",
@@ -164,6 +164,7 @@ def load():
         "prandtl_batch_budgets": (ip, [vp, ip, vp]),
         "prandtl_batch_remove": (ip, [vp, ip]),
         "prandtl_batch_tune": (ip, [vp, ip]),
+        "prandtl_batch_tune_in_steps": (ip, [vp]),
         "prandtl_batch_class_info": (ip, [vp, ip, ip, ip, ipp, ipp, dp, dp]),
         "prandtl_batch_stream": (vp, [vp]),
         "prandtl_batch_device_bytes": (C.c_size_t, [vp]),

@@ -135,6 +135,12 @@ class Batch:
     def tune(self, reps: int = 3):
         self._check(self._L.prandtl_batch_tune(self._h, int(reps)))
 
+    def tune_in_steps(self):
+        """Tune inside the next advances: their first n_variants steps run every
+        class with one RHS launch shape each, timed by CUDA events, and the
+        fastest shape is kept (the host waits for each of those steps)."""
+        self._check(self._L.prandtl_batch_tune_in_steps(self._h))
+
     def class_info(self, dim: int, order: int, parabolic: bool):
         """(chosen RHS launch shape, tuned ms per RHS launch of each shape, tuned ms per lifting launch)."""
         v, n = C.c_int(), C.c_int()

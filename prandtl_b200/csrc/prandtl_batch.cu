@@ -140,6 +140,12 @@ struct Class {
     BatchKernelInfo linfo{};
     double ms[MAX_VARIANTS];
     double lift_ms = -1.0;
+    // tuning inside the steps: summed ms per RHS launch of each timed shape,
+    // the shapes timed so far (bitmask), summed lifting ms and launches
+    double tune_ms[MAX_VARIANTS];
+    unsigned tune_seen = 0;
+    double tune_lift_ms = 0.0;
+    int tune_lift_n = 0;
 };
 
 }   // namespace
@@ -163,6 +169,8 @@ struct prandtl_batch {
     std::map<int, Class> classes;
     cudaGraphExec_t g_many = nullptr, g_one = nullptr;
     bool graph_dirty = true;
+    int tune_left = 0;                 // steps of tuning inside the next advances
+    std::vector<cudaEvent_t> tev;      // their per-launch events
     long long launches = 0;
     size_t bytes = 0;
     std::string err;
@@ -300,6 +308,86 @@ prandtl_status enqueue_step(prandtl_batch *b, cudaStream_t s) {
     return PRANDTL_OK;
 }
 
+// One step of tuning inside the advance: every class with resident solves
+// runs RHS launch shape v (where it fits; else its current shape), and each
+// lifting and RHS launch is bracketed by events.  The host waits for the step
+// (bounded by the batch's timeout) and records the class's mean ms per RHS
+// launch of the step for shape v.  The shapes give bit-identical results, so
+// which shape a step ran does not change the solves.
+prandtl_status tune_step(prandtl_batch *b, int v) {
+    const bool fp32 = b->cfg.precision == 1;
+    const int scheme = b->cfg.scheme, K = stages_of(scheme);
+    const size_t need = (size_t)4 * K * b->classes.size();
+    while (b->tev.size() < need) {
+        cudaEvent_t e = nullptr;
+        BCK(b, cudaEventCreate(&e), "tuning event");
+        b->tev.push_back(e);
+    }
+    size_t q = 0;
+    for (int k = 0; k < K; ++k) {
+        const BatchStage st = stage_of(scheme, k);
+        for (auto &kv : b->classes) {
+            Class &c = kv.second;
+            if (c.ns) {
+                const int grid = c.linfo.blocks_per_sm * b->num_sms;
+                BCK(b, cudaEventRecord(b->tev[q], b->stream), "event");
+                BCK(b, batch_launch_lift(c.dim, c.order, c.vc, fp32, grid, c.dev, st, c.T, b->stream),
+                    "batch lift launch");
+                BCK(b, cudaEventRecord(b->tev[q + 1], b->stream), "event");
+            }
+            const int cv = c.rinfo[v].blocks_per_sm > 0 ? v : c.variant;
+            const int grid = c.rinfo[cv].blocks_per_sm * b->num_sms;
+            BCK(b, cudaEventRecord(b->tev[q + 2], b->stream), "event");
+            BCK(b, batch_launch_rhs(c.dim, c.order, c.ns, c.vc, fp32, cv, grid, c.dev, st, c.T, b->stream),
+                "batch rhs launch");
+            BCK(b, cudaEventRecord(b->tev[q + 3], b->stream), "event");
+            q += 4;
+        }
+    }
+    BCK(b, batch_launch_step_end(b->d_tab, b->d_live, b->d_live + b->cap,
+                                 scheme == PRANDTL_LSRK45 ? 1 : 0, b->d_left, b->stream),
+        "batch step-end launch");
+    prandtl_status st = bwait(b);
+    if (st != PRANDTL_OK) return st;
+    q = 0;
+    for (int k = 0; k < K; ++k) {
+        for (auto &kv : b->classes) {
+            Class &c = kv.second;
+            float ms = 0.f;
+            if (c.ns && !c.ids.empty()) {
+                BCK(b, cudaEventElapsedTime(&ms, b->tev[q], b->tev[q + 1]), "event time");
+                c.tune_lift_ms += ms;
+                ++c.tune_lift_n;
+            }
+            if (c.rinfo[v].blocks_per_sm > 0 && !c.ids.empty()) {
+                BCK(b, cudaEventElapsedTime(&ms, b->tev[q + 2], b->tev[q + 3]), "event time");
+                if (k == 0) c.tune_ms[v] = 0.0;
+                c.tune_ms[v] += ms / K;
+                if (k == K - 1) c.tune_seen |= 1u << v;
+            }
+            q += 4;
+        }
+    }
+    return PRANDTL_OK;
+}
+
+// End of tuning inside the advances: each class keeps its fastest timed shape
+// (its current one when none was timed) and the step graphs are rebuilt.
+void tune_finish(prandtl_batch *b) {
+    for (auto &kv : b->classes) {
+        Class &c = kv.second;
+        int best = c.variant;
+        double best_ms = 1e300;
+        for (int v = 0; v < b->nvar; ++v) {
+            c.ms[v] = (c.tune_seen >> v) & 1u ? c.tune_ms[v] : -1.0;
+            if (c.ms[v] >= 0.0 && c.ms[v] < best_ms) { best_ms = c.ms[v]; best = v; }
+        }
+        if (c.tune_lift_n > 0) c.lift_ms = c.tune_lift_ms / c.tune_lift_n;
+        if (best != c.variant) b->graph_dirty = true;
+        c.variant = best;
+    }
+}
+
 long long launches_per_step(const prandtl_batch *b) {
     long long n = 0;
     for (const auto &kv : b->classes) n += kv.second.ns ? 2 : 1;
@@ -341,6 +429,8 @@ prandtl_status rebuild_graphs(prandtl_batch *b) {
 
 void free_batch(prandtl_batch *b) {
     drop_graphs(b);
+    for (cudaEvent_t e : b->tev) cudaEventDestroy(e);
+    b->tev.clear();
     for (auto &kv : b->classes) cudaFree(kv.second.d_buf);
     b->classes.clear();
     cudaFree(b->arena);
@@ -595,6 +685,14 @@ prandtl_status prandtl_batch_advance(prandtl_batch *b, int nsteps) {
     if (nsteps == 0 || b->classes.empty()) return PRANDTL_OK;
     BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
     const long long per_step = launches_per_step(b);
+    while (nsteps > 0 && b->tune_left > 0) {   // tuning inside the first steps
+        prandtl_status st = tune_step(b, b->nvar - b->tune_left);
+        if (st != PRANDTL_OK) return st;
+        b->launches += per_step;
+        --nsteps;
+        if (--b->tune_left == 0) tune_finish(b);
+    }
+    if (nsteps == 0) return PRANDTL_OK;
     if (!b->cfg.use_graph) {
         for (int s = 0; s < nsteps; ++s) {
             prandtl_status st = enqueue_step(b, b->stream);
@@ -765,11 +863,26 @@ prandtl_status prandtl_batch_remove(prandtl_batch *b, int id) {
     return st;
 }
 
+prandtl_status prandtl_batch_tune_in_steps(prandtl_batch *b) {
+    if (!b) return PRANDTL_EINVAL;
+    std::lock_guard<std::mutex> lk(b->mu);
+    b->err.clear();
+    for (auto &kv : b->classes) {
+        Class &c = kv.second;
+        c.tune_seen = 0;
+        c.tune_lift_ms = 0.0;
+        c.tune_lift_n = 0;
+    }
+    b->tune_left = b->nvar;
+    return PRANDTL_OK;
+}
+
 prandtl_status prandtl_batch_tune(prandtl_batch *b, int reps) {
     if (!b) return PRANDTL_EINVAL;
     if (reps <= 0) return bfail(b, PRANDTL_EINVAL, "reps must be positive");
     std::lock_guard<std::mutex> lk(b->mu);
     b->err.clear();
+    b->tune_left = 0;   // replaces tuning inside the steps
     BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
     prandtl_status st = bwait(b);
     if (st != PRANDTL_OK) return st;

@@ -147,6 +147,31 @@ def test_autotuner_picks_a_timed_shape_and_keeps_results():
     b.close()
 
 
+def test_tuning_inside_steps_keeps_results():
+    """The tuner inside the steps: the first n_variants steps of the advance
+    time one launch shape each; the chosen shape is the fastest timed one and
+    every solve's state equals the untuned batch's, bit for bit."""
+    items = _setup(MIX)
+    states = []
+    for tuned in (False, True):
+        b = Batch("fp32", arena_bytes=1 << 30)
+        ids = [b.add(mesh, u0, dt=dt, nsteps=5, **m.physics()) for m, mesh, u0, dt in items]
+        if tuned:
+            b.tune_in_steps()
+        b.advance(2)   # tuning continues across advance calls
+        b.advance(3)
+        if tuned:
+            for m, mesh, _, _ in items:
+                v, ms, lift_ms = b.class_info(mesh.dim, mesh.order, m.kind == "tgv")
+                timed = [t for t in ms if t > 0]
+                assert timed and ms[v] == min(timed)
+                assert (lift_ms > 0) == (m.kind == "tgv")
+        states.append([b.read(sid) for sid in ids])
+        b.close()
+    for a, c in zip(*states):
+        assert np.array_equal(a, c)
+
+
 def test_cfl_time_step_follows_lambda():
     m = Member("tgv", 3, 2, 0.2, 400.0)
     mesh = m.mesh()
