@@ -5,8 +5,12 @@
 // stream.  All waits are bounded by the configured timeout.
 #include <cuda_runtime.h>
 
+#include <unistd.h>
+
+#include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -20,6 +24,15 @@
 
 using namespace prandtl;
 using namespace prandtl::host;
+
+namespace {
+// Host-pointer transfers above kStageMin bytes go through a pinned ring of
+// kStageSlots chunks: host threads copy a chunk between the caller's pageable
+// buffer and a pinned slot while the DMA engine moves the previous one.
+constexpr size_t kStageChunk = size_t(8) << 20;
+constexpr int kStageSlots = 4;
+constexpr size_t kStageMin = size_t(4) << 20;
+}   // namespace
 
 struct prandtl_handle {
     int dim = 0, order = 0, Np = 0, nd = 0, nf = 0, E = 0, F = 0;
@@ -70,11 +83,95 @@ struct prandtl_handle {
     std::vector<Rec> recs;
     double prof_ms[PRANDTL_NUM_KERNELS] = {0};
     long long prof_n[PRANDTL_NUM_KERNELS] = {0};
+    // pinned staging ring for host-pointer transfers (allocated at the first
+    // transfer above kStageMin bytes; null when pinned memory was refused)
+    char *h_stage = nullptr;
+    bool stage_tried = false;
+    cudaEvent_t stage_ev[kStageSlots] = {};
+    bool stage_pending[kStageSlots] = {};
     std::string err;
     std::mutex mu;
 };
 
 namespace {
+
+// memcpy split over a small persistent pool of host threads (one call at a
+// time; a process forked after the pool started copies on its calling thread,
+// since the workers do not exist there).
+class CopyPool {
+  public:
+    static CopyPool &get() {
+        static CopyPool pool;
+        return pool;
+    }
+    void copy(void *dst, const void *src, size_t n) {
+        if (n < (size_t(1) << 20) || workers_.empty() || getpid() != pid_) {
+            std::memcpy(dst, src, n);
+            return;
+        }
+        std::lock_guard<std::mutex> call(call_mu_);
+        const int parts = (int)workers_.size() + 1;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            dst_ = static_cast<char *>(dst);
+            src_ = static_cast<const char *>(src);
+            n_ = n;
+            parts_ = parts;
+            pending_ = parts - 1;
+            ++gen_;
+        }
+        cv_.notify_all();
+        part(0);
+        std::unique_lock<std::mutex> lk(mu_);
+        done_cv_.wait(lk, [&] { return pending_ == 0; });
+    }
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : workers_)
+            if (t.joinable()) t.join();
+    }
+
+  private:
+    CopyPool() : pid_(getpid()) {
+        const unsigned hw = std::thread::hardware_concurrency();
+        const int n = (int)std::min(8u, hw > 1 ? hw / 2 : 1u) - 1;
+        for (int i = 1; i <= n; ++i) workers_.emplace_back([this, i] { loop(i); });
+    }
+    void part(int i) {
+        // 64-byte aligned split points
+        const size_t per = (n_ / parts_ + 63) / 64 * 64;
+        const size_t b = std::min(n_, per * i), e = std::min(n_, per * (i + 1));
+        if (e > b) std::memcpy(dst_ + b, src_ + b, e - b);
+    }
+    void loop(int i) {
+        unsigned seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+            }
+            part(i);
+            std::lock_guard<std::mutex> lk(mu_);
+            if (--pending_ == 0) done_cv_.notify_one();
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex call_mu_, mu_;
+    std::condition_variable cv_, done_cv_;
+    unsigned gen_ = 0;
+    int pending_ = 0, parts_ = 1;
+    bool stop_ = false;
+    char *dst_ = nullptr;
+    const char *src_ = nullptr;
+    size_t n_ = 0;
+    pid_t pid_;
+};
 
 thread_local char g_unbound_error[512];
 
@@ -108,6 +205,112 @@ prandtl_status wait_stream(prandtl_handle *h) {
         if (el > limit) return fail(h, PRANDTL_ETIMEDOUT, "wait for the handle's stream timed out");
         std::this_thread::sleep_for(std::chrono::microseconds(50));
     }
+}
+
+// Waits (bounded by the handle's timeout) for one event.
+prandtl_status wait_event(prandtl_handle *h, cudaEvent_t ev) {
+    const double limit = h->cfg.timeout_s > 0 ? h->cfg.timeout_s : 120.0;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess) return PRANDTL_OK;
+        if (e != cudaErrorNotReady) return cuda_fail(h, e, "device work failed");
+        const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > limit) return fail(h, PRANDTL_ETIMEDOUT, "wait for a staged copy timed out");
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+}
+
+// The pinned staging ring, allocated once per handle; false when pinned host
+// memory is refused (the transfers then go straight from pageable memory).
+bool stage_ready(prandtl_handle *h) {
+    if (h->h_stage) return true;
+    if (h->stage_tried) return false;
+    h->stage_tried = true;
+    void *p = nullptr;
+    if (cudaHostAlloc(&p, kStageChunk * kStageSlots, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    for (int k = 0; k < kStageSlots; ++k) {
+        if (cudaEventCreateWithFlags(&h->stage_ev[k], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            for (int j = 0; j < k; ++j) cudaEventDestroy(h->stage_ev[j]);
+            cudaFreeHost(p);
+            return false;
+        }
+    }
+    h->h_stage = static_cast<char *>(p);
+    return true;
+}
+
+// Pinned slot k before the host writes into it: its last DMA has finished.
+prandtl_status stage_slot_free(prandtl_handle *h, int k) {
+    if (!h->stage_pending[k]) return PRANDTL_OK;
+    prandtl_status st = wait_event(h, h->stage_ev[k]);
+    if (st == PRANDTL_OK) h->stage_pending[k] = false;
+    return st;
+}
+
+// Host (pageable) -> device on the handle's stream.  Large transfers are
+// chunked through the pinned ring: the host threads fill slot k while the DMA
+// of slot k-1 runs.  Returns with the DMAs enqueued (not finished).
+prandtl_status copy_h2d(prandtl_handle *h, void *dst, const void *src, size_t bytes) {
+    if (bytes < kStageMin || !stage_ready(h)) {
+        CK(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream), "H2D");
+        return PRANDTL_OK;
+    }
+    const char *s = static_cast<const char *>(src);
+    char *d = static_cast<char *>(dst);
+    for (size_t off = 0, c = 0; off < bytes; off += kStageChunk, ++c) {
+        const int k = (int)(c % kStageSlots);
+        const size_t n = std::min(kStageChunk, bytes - off);
+        prandtl_status st = stage_slot_free(h, k);
+        if (st != PRANDTL_OK) return st;
+        char *slot = h->h_stage + (size_t)k * kStageChunk;
+        CopyPool::get().copy(slot, s + off, n);
+        CK(h, cudaMemcpyAsync(d + off, slot, n, cudaMemcpyHostToDevice, h->stream), "H2D chunk");
+        CK(h, cudaEventRecord(h->stage_ev[k], h->stream), "cudaEventRecord");
+        h->stage_pending[k] = true;
+    }
+    return PRANDTL_OK;
+}
+
+// Device -> host (pageable) after the work already on the handle's stream;
+// returns once the caller's buffer holds the data.  Chunks cross the pinned
+// ring; the host threads empty slot k while later DMAs run.
+prandtl_status copy_d2h(prandtl_handle *h, void *dst, const void *src, size_t bytes) {
+    if (bytes < kStageMin || !stage_ready(h)) {
+        CK(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H");
+        return wait_stream(h);
+    }
+    const char *s = static_cast<const char *>(src);
+    char *d = static_cast<char *>(dst);
+    const size_t nchunks = (bytes + kStageChunk - 1) / kStageChunk;
+    auto issue = [&](size_t c) -> prandtl_status {
+        const int k = (int)(c % kStageSlots);
+        const size_t off = c * kStageChunk, n = std::min(kStageChunk, bytes - off);
+        prandtl_status st = stage_slot_free(h, k);
+        if (st != PRANDTL_OK) return st;
+        CK(h, cudaMemcpyAsync(h->h_stage + (size_t)k * kStageChunk, s + off, n, cudaMemcpyDeviceToHost, h->stream),
+           "D2H chunk");
+        CK(h, cudaEventRecord(h->stage_ev[k], h->stream), "cudaEventRecord");
+        h->stage_pending[k] = true;
+        return PRANDTL_OK;
+    };
+    for (size_t c = 0; c < nchunks && c < (size_t)kStageSlots; ++c) {
+        prandtl_status st = issue(c);
+        if (st != PRANDTL_OK) return st;
+    }
+    for (size_t c = 0; c < nchunks; ++c) {
+        const int k = (int)(c % kStageSlots);
+        const size_t off = c * kStageChunk, n = std::min(kStageChunk, bytes - off);
+        prandtl_status st = stage_slot_free(h, k);
+        if (st != PRANDTL_OK) return st;
+        CopyPool::get().copy(d + off, h->h_stage + (size_t)k * kStageChunk, n);
+        if (c + kStageSlots < nchunks && (st = issue(c + kStageSlots)) != PRANDTL_OK) return st;
+    }
+    return PRANDTL_OK;
 }
 
 // Copies the sticky state-check flag to the pinned host word, waits (bounded),
@@ -213,6 +416,11 @@ void free_all(prandtl_handle *h) {
     cudaFree(h->d_ngeo);
     cudaFree(h->d_fnn);
     cudaFree(h->d_snor);
+    if (h->h_stage) {
+        for (int k = 0; k < kStageSlots; ++k) cudaEventDestroy(h->stage_ev[k]);
+        cudaFreeHost(h->h_stage);
+        h->h_stage = nullptr;
+    }
     if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     if (h->done) cudaEventDestroy(h->done);
@@ -510,7 +718,8 @@ prandtl_status prandtl_rhs(prandtl_handle *h, const double *u, double *dudt, dou
     const double *u_d = u;
     double *dudt_d = dudt;
     if (!dev) {
-        CK(h, cudaMemcpyAsync(h->d_in, u, bytes, cudaMemcpyHostToDevice, h->stream), "H2D u");
+        prandtl_status st = copy_h2d(h, h->d_in, u, bytes);
+        if (st != PRANDTL_OK) return st;
         u_d = h->d_in;
         dudt_d = h->d_out;
     }
@@ -522,7 +731,7 @@ prandtl_status prandtl_rhs(prandtl_handle *h, const double *u, double *dudt, dou
     prandtl_status st = run_rhs(h, u_d, a);
     if (st != PRANDTL_OK) return st;
     unsigned long long lam_bits = 0;
-    if (!dev) CK(h, cudaMemcpyAsync(dudt, h->d_out, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H dudt");
+    if (!dev && (st = copy_d2h(h, dudt, h->d_out, bytes)) != PRANDTL_OK) return st;
     if (lambda_max)
         CK(h, cudaMemcpyAsync(&lam_bits, h->d_lambda, sizeof(lam_bits), cudaMemcpyDeviceToHost, h->stream), "D2H lambda");
     if (!dev || lambda_max) {
@@ -549,11 +758,11 @@ prandtl_status prandtl_step(prandtl_handle *h, double *u, double t, double dt, i
     const size_t bytes = (size_t)h->nf * h->Ndof * sizeof(double);
     const bool dev = (ptr_flags & PRANDTL_PTR_DEVICE) != 0;
     double *x = u;
+    prandtl_status st = PRANDTL_OK;
     if (!dev) {
-        CK(h, cudaMemcpyAsync(h->d_in, u, bytes, cudaMemcpyHostToDevice, h->stream), "H2D u");
+        if ((st = copy_h2d(h, h->d_in, u, bytes)) != PRANDTL_OK) return st;
         x = h->d_in;
     }
-    prandtl_status st = PRANDTL_OK;
     int left = nsteps;
     // long runs replay a captured graph of kGraphSteps steps (one launch per
     // replay instead of one per kernel); the remainder runs launch by launch
@@ -568,7 +777,7 @@ prandtl_status prandtl_step(prandtl_handle *h, double *u, double t, double dt, i
     if (st == PRANDTL_OK) st = enqueue_steps(h, x, dt, scheme, left);
     if (st != PRANDTL_OK) return st;
     if (!dev) {
-        CK(h, cudaMemcpyAsync(u, x, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H u");
+        if ((st = copy_d2h(h, u, x, bytes)) != PRANDTL_OK) return st;
         st = wait_and_report_health(h);
     }
     return st;
