@@ -276,13 +276,14 @@ prandtl_status copy_h2d(prandtl_handle *h, void *dst, const void *src, size_t by
     return PRANDTL_OK;
 }
 
-// Device -> host (pageable) after the work already on the handle's stream;
-// returns once the caller's buffer holds the data.  Chunks cross the pinned
-// ring; the host threads empty slot k while later DMAs run.
+// Device -> host (pageable) after the work already on the handle's stream.
+// Small transfers are only enqueued (the caller's next stream wait completes
+// them); large ones cross the pinned ring, the host threads emptying slot k
+// while later DMAs run, and are in the caller's buffer on return.
 prandtl_status copy_d2h(prandtl_handle *h, void *dst, const void *src, size_t bytes) {
     if (bytes < kStageMin || !stage_ready(h)) {
         CK(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H");
-        return wait_stream(h);
+        return PRANDTL_OK;
     }
     const char *s = static_cast<const char *>(src);
     char *d = static_cast<char *>(dst);
