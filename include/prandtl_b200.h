@@ -387,6 +387,15 @@ prandtl_status prandtl_batch_footprint(prandtl_batch *b, const prandtl_mesh_desc
  * cfg->precision is ignored (the batch's applies). */
 prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *mesh, const prandtl_config *cfg,
                                  const double *u0, int ptr_flags, const prandtl_solve_desc *solve, int *id);
+/* prandtl_batch_add of n solves (mesh[k], cfg[k], u0[k], sd[k] -> ids[k]):
+ * the mesh checks, neighbour tables and geometry rows are prepared on
+ * several host threads, then the solves are admitted in order.  Stops at the
+ * first solve that fails (its status is returned, the message names the
+ * solve); ids of that solve and of those after it are -1, those before it
+ * stay admitted. */
+prandtl_status prandtl_batch_add_many(prandtl_batch *b, int n, const prandtl_mesh_desc *const *mesh,
+                                      const prandtl_config *const *cfg, const double *const *u0, int ptr_flags,
+                                      const prandtl_solve_desc *sd, int *ids);
 /* Enqueue nsteps steps; each solve stops at its own step count.  Asynchronous. */
 prandtl_status prandtl_batch_advance(prandtl_batch *b, int nsteps);
 /* Wait (bounded) for the enqueued work. */
@@ -405,6 +414,10 @@ prandtl_status prandtl_batch_time(prandtl_batch *b, int id, double *t);
 /* Waits, then copies the solve's current state (byNODES) out; PRANDTL_ENONFINITE
  * (state still copied) for a solve stopped by the state check. */
 prandtl_status prandtl_batch_read(prandtl_batch *b, int id, double *u, int ptr_flags);
+/* prandtl_batch_read of n solves with two waits in all: solve ids[k] into
+ * u[k].  Every state is copied; a solve stopped by the state check then
+ * makes it return PRANDTL_ENONFINITE (the first such id in the message). */
+prandtl_status prandtl_batch_read_many(prandtl_batch *b, int n, const int *ids, double *const *u, int ptr_flags);
 /* Waits, then the FP64 budgets of the solve's current state, reduced on the device where it
  * resides: out[0 .. nf-1] the integrals of the conserved fields, out[nf] the integral of the
  * entropy function (host memory, nf + 1 doubles; as prandtl_budgets without the rates). */

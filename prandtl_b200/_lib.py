@@ -28,9 +28,9 @@ EXPORTS = ["prandtl_config_default", "prandtl_create", "prandtl_destroy", "prand
            "prandtl_last_error", "prandtl_version", "prandtl_rhs_noalloc", "prandtl_recover_state",
            "prandtl_budgets", "prandtl_batch_budgets",
            "prandtl_batch_config_default", "prandtl_batch_create", "prandtl_batch_destroy",
-           "prandtl_batch_footprint", "prandtl_batch_add", "prandtl_batch_advance",
+           "prandtl_batch_footprint", "prandtl_batch_add", "prandtl_batch_add_many", "prandtl_batch_advance",
            "prandtl_batch_sync", "prandtl_batch_finished", "prandtl_batch_query",
-           "prandtl_batch_read", "prandtl_batch_remove", "prandtl_batch_tune", "prandtl_batch_tune_in_steps",
+           "prandtl_batch_read", "prandtl_batch_read_many", "prandtl_batch_remove", "prandtl_batch_tune", "prandtl_batch_tune_in_steps",
            "prandtl_batch_class_info", "prandtl_batch_stream", "prandtl_batch_device_bytes",
            "prandtl_batch_arena_bytes", "prandtl_batch_time",
            "prandtl_batch_kernel_launches", "prandtl_batch_last_error",
@@ -155,11 +155,13 @@ def load():
         "prandtl_batch_destroy": (ip, [vp]),
         "prandtl_batch_footprint": (ip, [vp, mdp, cfp, C.POINTER(C.c_size_t)]),
         "prandtl_batch_add": (ip, [vp, mdp, cfp, vp, ip, sdp, ipp]),
+        "prandtl_batch_add_many": (ip, [vp, ip, vp, vp, vp, ip, vp, vp]),
         "prandtl_batch_advance": (ip, [vp, ip]),
         "prandtl_batch_sync": (ip, [vp]),
         "prandtl_batch_finished": (ip, [vp, ipp, ip, ipp]),
         "prandtl_batch_query": (ip, [vp, ip, ipp, ipp, dp, dp]),
         "prandtl_batch_read": (ip, [vp, ip, vp, ip]),
+        "prandtl_batch_read_many": (ip, [vp, ip, vp, vp, ip]),
         "prandtl_batch_time": (ip, [vp, ip, dp]),
         "prandtl_batch_budgets": (ip, [vp, ip, vp]),
         "prandtl_batch_remove": (ip, [vp, ip]),

@@ -113,12 +113,63 @@ class Batch:
         self._check(self._L.prandtl_batch_time(self._h, int(sid), C.byref(t)))
         return t.value
 
+    def add_many(self, solves) -> list:
+        """Admit several solves at once (prandtl_batch_add_many): `solves` holds
+        (mesh, u0, dict(dt=..., nsteps=..., [cfl, hmin, t_final,] **phys)) items;
+        their mesh checks and tables are prepared on several host threads.  All
+        u0 are host arrays or all device tensors.  Raises PrandtlError for the
+        first solve that fails; the ones before it stay admitted."""
+        n = len(solves)
+        keep, descs, cfgs, ptrs, flags = [], [], [], [], set()
+        sds = (_lib.SolveDesc * max(n, 1))()
+        for k, (mesh, u0, kw) in enumerate(solves):
+            kw = dict(kw)
+            dt, nsteps = kw.pop("dt"), kw.pop("nsteps")
+            cfl, hmin, t_final = kw.pop("cfl", 0.0), kw.pop("hmin", None), kw.pop("t_final", 0.0)
+            arr = MeshArrays(mesh)
+            cfg = make_config(**kw)
+            p, flag = _ptr(u0)
+            keep += [arr, cfg, u0]
+            descs.append(C.addressof(arr.desc))
+            cfgs.append(C.addressof(cfg))
+            ptrs.append(p)
+            flags.add(flag)
+            sds[k] = _solve_desc(mesh, dt, nsteps, cfl, hmin, t_final)
+        if len(flags) > 1:
+            raise ValueError("add_many takes host or device initial states, not both")
+        ids = (C.c_int * max(n, 1))()
+        st = self._L.prandtl_batch_add_many(self._h, n, (C.c_void_p * max(n, 1))(*descs),
+                                            (C.c_void_p * max(n, 1))(*cfgs), (C.c_void_p * max(n, 1))(*ptrs),
+                                            flags.pop() if flags else 0, sds, ids)
+        out = [int(ids[k]) for k in range(n)]
+        for k, (mesh, _, _) in enumerate(solves):
+            if out[k] >= 0:
+                self._shape[out[k]] = (mesh.num_fields * mesh.ndof,)
+                self._nf[out[k]] = mesh.num_fields
+        self._check(st)
+        return out
+
     def read(self, sid: int, out=None):
         if out is None:
             out = np.empty(self._shape[sid], dtype=np.float64)
         p, flag = _ptr(out)
         self._check(self._L.prandtl_batch_read(self._h, int(sid), p, flag))
         return out
+
+    def read_many(self, sids, outs=None):
+        """States of several solves with two waits in all (prandtl_batch_read_many);
+        outs: arrays or tensors of one kind (host or device), one per id."""
+        sids = [int(x) for x in sids]
+        if outs is None:
+            outs = [np.empty(self._shape[x], dtype=np.float64) for x in sids]
+        ptrs = [_ptr(o) for o in outs]
+        flags = {f for _, f in ptrs}
+        if len(flags) > 1:
+            raise ValueError("read_many takes host or device outputs, not both")
+        ids = (C.c_int * len(sids))(*sids)
+        arr = (C.c_void_p * len(sids))(*[p for p, _ in ptrs])
+        self._check(self._L.prandtl_batch_read_many(self._h, len(sids), ids, arr, flags.pop() if flags else 0))
+        return outs
 
     def budgets(self, sid: int) -> dict:
         """FP64 integrals of the solve's resident state, reduced on the device:

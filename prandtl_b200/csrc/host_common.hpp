@@ -5,9 +5,11 @@
 
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -120,6 +122,14 @@ const char *unbound_error();
 bool batch_has_room(prandtl_batch *b, size_t bytes);
 
 // Text for the state-check bits the RK epilogue sets (PRANDTL_HEALTH_*).
+// Pause between polls of a device event (the host waits are all polls bounded
+// by a timeout): yield for the first 200 us, so short waits end within a few
+// microseconds of the event, then sleep 50 us at a time.
+inline void poll_pause(double waited_s) {
+    if (waited_s < 2e-4) std::this_thread::yield();
+    else std::this_thread::sleep_for(std::chrono::microseconds(50));
+}
+
 inline std::string health_text(unsigned bits) {
     std::string t = "the state left the admissible set:";
     if (bits & PRANDTL_HEALTH_NONFINITE) t += " non-finite values;";
@@ -477,13 +487,18 @@ inline prandtl_status check_face_node_normals(const prandtl_mesh_desc *md, std::
 }
 
 // Geometry rows [E][dim*dim + 1]: adj(J) row-major, then det J.
-inline std::vector<double> geometry_rows(const prandtl_mesh_desc *md) {
+// (into an existing vector, whose capacity is reused across admissions)
+inline void geometry_rows_into(const prandtl_mesh_desc *md, std::vector<double> &geo) {
     const int dim = md->dim, GEO = dim * dim + 1, E = md->num_elements;
-    std::vector<double> geo((size_t)E * GEO);
+    geo.resize((size_t)E * GEO);
     for (int e = 0; e < E; ++e) {
         for (int q = 0; q < dim * dim; ++q) geo[(size_t)e * GEO + q] = md->elem_adj[(size_t)e * dim * dim + q];
         geo[(size_t)e * GEO + dim * dim] = md->elem_detj[e];
     }
+}
+inline std::vector<double> geometry_rows(const prandtl_mesh_desc *md) {
+    std::vector<double> geo;
+    geometry_rows_into(md, geo);
     return geo;
 }
 

@@ -203,7 +203,7 @@ prandtl_status wait_stream(prandtl_handle *h) {
         if (e != cudaErrorNotReady) return cuda_fail(h, e, "device work failed");
         const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (el > limit) return fail(h, PRANDTL_ETIMEDOUT, "wait for the handle's stream timed out");
-        std::this_thread::sleep_for(std::chrono::microseconds(50));
+        poll_pause(el);
     }
 }
 
@@ -217,7 +217,7 @@ prandtl_status wait_event(prandtl_handle *h, cudaEvent_t ev) {
         if (e != cudaErrorNotReady) return cuda_fail(h, e, "device work failed");
         const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (el > limit) return fail(h, PRANDTL_ETIMEDOUT, "wait for a staged copy timed out");
-        std::this_thread::sleep_for(std::chrono::microseconds(20));
+        poll_pause(el);
     }
 }
 

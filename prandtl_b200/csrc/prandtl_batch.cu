@@ -12,10 +12,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <deque>
 #include <iterator>
 #include <map>
 #include <mutex>
@@ -146,6 +148,17 @@ struct Class {
     unsigned tune_seen = 0;
     double tune_lift_ms = 0.0;
     int tune_lift_n = 0;
+    bool tables_dirty = true;    // ids / prefix / header differ from the device copy
+};
+
+// Pinned ring for the small per-solve uploads of an admission (geometry rows,
+// neighbour table, normals, boundary conditions, solve record): the host
+// copies a blob into the ring and the DMA runs behind the next admission's
+// host work instead of stalling the stream as a pageable copy does.
+constexpr size_t kUpRing = size_t(32) << 20;
+struct UpSegment {
+    size_t begin, end;
+    cudaEvent_t ev;
 };
 
 }   // namespace
@@ -171,6 +184,13 @@ struct prandtl_batch {
     bool graph_dirty = true;
     int tune_left = 0;                 // steps of tuning inside the next advances
     std::vector<cudaEvent_t> tev;      // their per-launch events
+    bool live_dirty = true;            // live list differs from the device copy
+    char *up_ring = nullptr;           // pinned upload ring (kUpRing bytes), null if refused
+    bool up_tried = false;
+    size_t up_head = 0;
+    std::deque<UpSegment> up_pending;  // ring ranges whose DMA may still run
+    std::vector<cudaEvent_t> up_free;  // spare events
+    BatchInst *h_tab = nullptr;        // pinned copy of the solve records (read_many)
     long long launches = 0;
     size_t bytes = 0;
     std::string err;
@@ -207,7 +227,7 @@ prandtl_status bwait(prandtl_batch *b) {
         if (e != cudaErrorNotReady) return bcuda(b, e, "device work failed");
         const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (el > limit) return bfail(b, PRANDTL_ETIMEDOUT, "wait for the batch's stream timed out");
-        std::this_thread::sleep_for(std::chrono::microseconds(50));
+        poll_pause(el);
     }
 }
 
@@ -247,6 +267,90 @@ prandtl_status upload_live(prandtl_batch *b) {
     return PRANDTL_OK;
 }
 
+// The class tables and the live list the launches read, uploaded once before
+// the next launches instead of at every admission or removal.
+prandtl_status flush_tables(prandtl_batch *b) {
+    for (auto &kv : b->classes) {
+        if (!kv.second.tables_dirty) continue;
+        prandtl_status st = upload_class(b, kv.second);
+        if (st != PRANDTL_OK) return st;
+        kv.second.tables_dirty = false;
+    }
+    if (b->live_dirty) {
+        prandtl_status st = upload_live(b);
+        if (st != PRANDTL_OK) return st;
+        b->live_dirty = false;
+    }
+    return PRANDTL_OK;
+}
+
+// Waits (bounded by the batch's timeout) for one event.
+prandtl_status bwait_event(prandtl_batch *b, cudaEvent_t ev) {
+    const double limit = b->cfg.timeout_s > 0 ? b->cfg.timeout_s : 120.0;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess) return PRANDTL_OK;
+        if (e != cudaErrorNotReady) return bcuda(b, e, "device work failed");
+        const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > limit) return bfail(b, PRANDTL_ETIMEDOUT, "wait for an upload timed out");
+        poll_pause(el);
+    }
+}
+
+// Host -> device upload of n bytes for an admission, on the batch stream.
+// Blobs up to a quarter of the ring go through it (ranges still being read
+// by their DMA are waited for first); larger ones, or all of them when pinned
+// memory was refused, are copied directly.
+prandtl_status up_copy(prandtl_batch *b, void *dst, const void *src, size_t n) {
+    if (n == 0) return PRANDTL_OK;
+    if (!b->up_ring && !b->up_tried) {
+        b->up_tried = true;
+        void *p = nullptr;
+        if (cudaHostAlloc(&p, kUpRing, cudaHostAllocDefault) == cudaSuccess) b->up_ring = static_cast<char *>(p);
+        else cudaGetLastError();
+    }
+    if (!b->up_ring || n > kUpRing / 4) {
+        BCK(b, cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, b->stream), "upload");
+        return PRANDTL_OK;
+    }
+    const size_t need = (n + 255) / 256 * 256;
+    if (b->up_head + need > kUpRing) b->up_head = 0;
+    const size_t lo = b->up_head, hi = lo + need;
+    for (auto it = b->up_pending.begin(); it != b->up_pending.end();) {
+        const bool overlap = it->begin < hi && lo < it->end;
+        const cudaError_t q = overlap ? cudaErrorNotReady : cudaEventQuery(it->ev);
+        if (!overlap && q != cudaSuccess) {
+            if (q != cudaErrorNotReady) return bcuda(b, q, "device work failed");
+            ++it;
+            continue;
+        }
+        if (overlap) {
+            prandtl_status st = bwait_event(b, it->ev);
+            if (st != PRANDTL_OK) return st;
+        }
+        b->up_free.push_back(it->ev);
+        it = b->up_pending.erase(it);
+    }
+    std::memcpy(b->up_ring + lo, src, n);
+    BCK(b, cudaMemcpyAsync(dst, b->up_ring + lo, n, cudaMemcpyHostToDevice, b->stream), "upload");
+    cudaEvent_t ev = nullptr;
+    if (!b->up_free.empty()) {
+        ev = b->up_free.back();
+        b->up_free.pop_back();
+    } else {
+        BCK(b, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "upload event");
+    }
+    const cudaError_t e = cudaEventRecord(ev, b->stream);
+    if (e != cudaSuccess) {
+        b->up_free.push_back(ev);
+        return bcuda(b, e, "cudaEventRecord");
+    }
+    b->up_pending.push_back({lo, hi, ev});
+    b->up_head = hi;
+    return PRANDTL_OK;
+}
+
 prandtl_status get_class(prandtl_batch *b, int dim, int order, bool ns, bool vc, Class **out) {
     const int key = class_key(dim, order, ns, vc);
     auto it = b->classes.find(key);
@@ -278,8 +382,7 @@ prandtl_status get_class(prandtl_batch *b, int dim, int order, bool ns, bool vc,
     c.dev.prefix = c.d_buf + b->cap;
     c.dev.hdr = c.d_buf + 2 * b->cap + 1;
     Class &ref = b->classes.emplace(key, c).first->second;
-    prandtl_status st = upload_class(b, ref);
-    if (st != PRANDTL_OK) return st;
+    ref.tables_dirty = true;
     b->graph_dirty = true;
     *out = &ref;
     return PRANDTL_OK;
@@ -433,6 +536,14 @@ void free_batch(prandtl_batch *b) {
     b->tev.clear();
     for (auto &kv : b->classes) cudaFree(kv.second.d_buf);
     b->classes.clear();
+    for (auto &g : b->up_pending) cudaEventDestroy(g.ev);
+    b->up_pending.clear();
+    for (cudaEvent_t e : b->up_free) cudaEventDestroy(e);
+    b->up_free.clear();
+    if (b->up_ring) cudaFreeHost(b->up_ring);
+    b->up_ring = nullptr;
+    if (b->h_tab) cudaFreeHost(b->h_tab);
+    b->h_tab = nullptr;
     cudaFree(b->arena);
     cudaFree(b->d_tab);
     cudaFree(b->d_live);
@@ -564,36 +675,72 @@ prandtl_status prandtl_batch_footprint(prandtl_batch *b, const prandtl_mesh_desc
     return PRANDTL_OK;
 }
 
-prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, const prandtl_config *cfg,
-                                 const double *u0, int ptr_flags, const prandtl_solve_desc *sd, int *id) {
-    if (!b) return PRANDTL_EINVAL;
-    if (!md || !cfg || !u0 || !sd || !id) return bfail(b, PRANDTL_EINVAL, "null argument");
+}   // extern "C"
+
+namespace {
+
+// Host-side preparation of one admission, touching no batch state: the
+// argument and mesh checks, the neighbour table and the geometry rows.  The
+// preparations of different solves are independent, so
+// prandtl_batch_add_many runs them on several host threads.  A Prep is
+// reused across admissions: its tables keep their capacity, so admissions do
+// not fault in fresh host pages for them (page faults, serialised in the
+// kernel, were most of a large admission's host time).
+struct Prep {
+    prandtl_status st = PRANDTL_OK;
+    std::string msg;
+    std::vector<int4> nbr;
+    std::vector<double> geo;
+    // tables of a very large mesh are not kept for the next admission
+    void trim() {
+        if (nbr.capacity() * sizeof(int4) + geo.capacity() * sizeof(double) > (size_t(64) << 20)) {
+            std::vector<int4>().swap(nbr);
+            std::vector<double>().swap(geo);
+        }
+    }
+};
+
+void prep_solve(const prandtl_mesh_desc *md, const prandtl_config *cfg, const prandtl_solve_desc *sd, Prep &p) {
+    p.st = PRANDTL_OK;
+    p.msg.clear();
     if (sd->nsteps < 0 || !std::isfinite(sd->dt) || (sd->nsteps > 0 && !(sd->dt > 0.0)) ||
         !std::isfinite(sd->cfl) || (sd->cfl > 0.0 && !(sd->hmin > 0.0)) || !std::isfinite(sd->t_final) ||
-        sd->t_final < 0.0)
-        return bfail(b, PRANDTL_EINVAL, "bad solve description (dt, cfl, hmin, nsteps, t_final)");
-    if (!(cfg->gamma > 1.0) || !(cfg->Pr > 0.0)) return bfail(b, PRANDTL_EINVAL, "bad gamma/Pr");
-    std::lock_guard<std::mutex> lk(b->mu);
-    b->err.clear();
-    std::vector<int4> nbr;
-    std::string msg;
-    prandtl_status st = check_bcs(cfg, md->dim, msg);
-    if (st == PRANDTL_OK) st = validate_mesh(md, nbr, msg, cfg->num_bcs);
-    if (st == PRANDTL_OK) st = check_viscous_bcs(md, cfg, msg);
+        sd->t_final < 0.0) {
+        p.st = PRANDTL_EINVAL;
+        p.msg = "bad solve description (dt, cfl, hmin, nsteps, t_final)";
+        return;
+    }
+    if (!(cfg->gamma > 1.0) || !(cfg->Pr > 0.0)) {
+        p.st = PRANDTL_EINVAL;
+        p.msg = "bad gamma/Pr";
+        return;
+    }
+    prandtl_status st = check_bcs(cfg, md->dim, p.msg);
+    if (st == PRANDTL_OK) st = validate_mesh(md, p.nbr, p.msg, cfg->num_bcs);
+    if (st == PRANDTL_OK) st = check_viscous_bcs(md, cfg, p.msg);
     if (st == PRANDTL_OK && cfg->axisymmetric) {
         st = PRANDTL_EUNSUPPORTED;
-        msg = "the axisymmetric form runs on a prandtl_create operator, not in a batch";
+        p.msg = "the axisymmetric form runs on a prandtl_create operator, not in a batch";
     }
     if (st == PRANDTL_OK && (md->node_adj || md->node_detj || md->face_node_nor)) {
         st = PRANDTL_EUNSUPPORTED;
-        msg = "non-affine elements run on a prandtl_create FP64 operator, not in a batch";
+        p.msg = "non-affine elements run on a prandtl_create FP64 operator, not in a batch";
     }
-    if (st != PRANDTL_OK) return bfail(b, st, msg);
+    if (st == PRANDTL_OK && cfg->parabolic && cfg->quirks != 0) st = check_face_normals(md, p.msg);
+    if (st == PRANDTL_OK) geometry_rows_into(md, p.geo);
+    p.st = st;
+}
+
+// Admission of a prepared solve (the batch's mutex held).
+prandtl_status admit_prepared(prandtl_batch *b, const prandtl_mesh_desc *md, const prandtl_config *cfg,
+                              const double *u0, int ptr_flags, const prandtl_solve_desc *sd, Prep &p, int *id) {
+    if (p.st != PRANDTL_OK) return bfail(b, p.st, p.msg);
+    prandtl_status st = PRANDTL_OK;
+    const std::vector<int4> &nbr = p.nbr;
     BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
     const int dim = md->dim, order = md->order, E = md->num_elements, F = md->num_faces;
     const bool ns = cfg->parabolic != 0, fp32 = b->cfg.precision == 1, blend = cfg->blending != 0;
     const bool vc = ns && cfg->quirks != 0;
-    if (vc && (st = check_face_normals(md, msg)) != PRANDTL_OK) return bfail(b, st, msg);
     const Layout L = solve_layout(dim, order, E, F, ns, blend, fp32, cfg->num_bcs);
     if (b->free_ids.empty()) return bfail(b, PRANDTL_ENOMEM, "solve table full");
     Class *c = nullptr;
@@ -621,24 +768,21 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, 
         b->alloc.release(off, L.total);
         return r;
     };
-    const std::vector<double> geo = geometry_rows(md);
+    const std::vector<double> &geo = p.geo;
     const size_t S = (size_t)s.nf * s.Ndof * sizeof(double);
     cudaError_t e;
-    if ((e = cudaMemcpyAsync(base + L.geo, geo.data(), geo.size() * sizeof(double), cudaMemcpyHostToDevice,
-                             b->stream)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(base + L.nbr, nbr.data(), nbr.size() * sizeof(int4), cudaMemcpyHostToDevice,
-                             b->stream)) != cudaSuccess ||
-        (F > 0 && (e = cudaMemcpyAsync(base + L.fnor, md->face_nor, (size_t)F * dim * sizeof(double),
-                                       cudaMemcpyHostToDevice, b->stream)) != cudaSuccess) ||
-        (e = cudaMemcpyAsync(base + L.u[0], u0, S,
+    if ((st = up_copy(b, base + L.geo, geo.data(), geo.size() * sizeof(double))) != PRANDTL_OK ||
+        (st = up_copy(b, base + L.nbr, nbr.data(), nbr.size() * sizeof(int4))) != PRANDTL_OK ||
+        (F > 0 && (st = up_copy(b, base + L.fnor, md->face_nor, (size_t)F * dim * sizeof(double))) != PRANDTL_OK))
+        return undo(st);
+    if ((e = cudaMemcpyAsync(base + L.u[0], u0, S,
                              (ptr_flags & PRANDTL_PTR_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                              b->stream)) != cudaSuccess ||
         (blend && (e = cudaMemsetAsync(base + L.alpha, 0, (size_t)E * sizeof(double), b->stream)) != cudaSuccess))
         return undo(bcuda(b, e, "upload solve"));
     const std::vector<BcDev> bcs = device_bcs(cfg, md->dim);
-    if (!bcs.empty() && (e = cudaMemcpyAsync(base + L.bcs, bcs.data(), bcs.size() * sizeof(BcDev),
-                                             cudaMemcpyHostToDevice, b->stream)) != cudaSuccess)
-        return undo(bcuda(b, e, "upload boundary conditions"));
+    if (!bcs.empty() && (st = up_copy(b, base + L.bcs, bcs.data(), bcs.size() * sizeof(BcDev))) != PRANDTL_OK)
+        return undo(st);
     BatchInst I;
     std::memset(&I, 0, sizeof(I));
     build_phys(*cfg, order, I.P);
@@ -659,21 +803,78 @@ prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, 
     I.hmin = sd->hmin;
     I.steps_left = sd->nsteps;
     const int left = sd->nsteps;
-    if ((e = cudaMemcpyAsync(b->d_tab + sid, &I, sizeof(I), cudaMemcpyHostToDevice, b->stream)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(b->d_left + sid, &left, sizeof(int), cudaMemcpyHostToDevice, b->stream)) != cudaSuccess)
-        return undo(bcuda(b, e, "upload solve record"));
-    // the work prefix is built from the solve records: record this one first
+    if ((st = up_copy(b, b->d_tab + sid, &I, sizeof(I))) != PRANDTL_OK ||
+        (st = up_copy(b, b->d_left + sid, &left, sizeof(int))) != PRANDTL_OK)
+        return undo(st);
+    // the work prefix is built from the solve records: record this one first;
+    // the class tables and the live list go up before the next launches
     b->solves[sid] = s;
     c->ids.push_back(sid);
     b->live.push_back(sid);
-    if ((st = upload_class(b, *c)) != PRANDTL_OK || (st = upload_live(b)) != PRANDTL_OK) {
-        c->ids.pop_back();
-        b->live.pop_back();
-        b->solves[sid] = Solve();
-        return undo(st);
-    }
+    c->tables_dirty = true;
+    b->live_dirty = true;
     b->free_ids.pop_back();
     *id = sid;
+    return PRANDTL_OK;
+}
+
+}   // namespace
+
+extern "C" {
+
+prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *md, const prandtl_config *cfg,
+                                 const double *u0, int ptr_flags, const prandtl_solve_desc *sd, int *id) {
+    if (!b) return PRANDTL_EINVAL;
+    if (!md || !cfg || !u0 || !sd || !id) return bfail(b, PRANDTL_EINVAL, "null argument");
+    thread_local Prep p;
+    prep_solve(md, cfg, sd, p);
+    std::lock_guard<std::mutex> lk(b->mu);
+    b->err.clear();
+    const prandtl_status st = admit_prepared(b, md, cfg, u0, ptr_flags, sd, p, id);
+    p.trim();
+    return st;
+}
+
+prandtl_status prandtl_batch_add_many(prandtl_batch *b, int n, const prandtl_mesh_desc *const *mds,
+                                      const prandtl_config *const *cfgs, const double *const *u0s, int ptr_flags,
+                                      const prandtl_solve_desc *sds, int *ids) {
+    if (!b) return PRANDTL_EINVAL;
+    if (n < 0 || (n > 0 && (!mds || !cfgs || !u0s || !sds || !ids))) return bfail(b, PRANDTL_EINVAL, "null argument");
+    for (int k = 0; k < n; ++k) {
+        ids[k] = -1;
+        if (!mds[k] || !cfgs[k] || !u0s[k]) return bfail(b, PRANDTL_EINVAL, "null argument");
+    }
+    // windows of solves: prepared on host threads, then admitted in order
+    constexpr int kWindow = 64;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int threads = (int)std::max(1u, std::min(16u, hw / 2));
+    // the calling thread's buffers; the worker threads reach them through this
+    // reference (inside a worker, the thread_local name is that worker's own)
+    thread_local std::vector<Prep> tl_preps;
+    std::vector<Prep> &preps = tl_preps;
+    if (preps.size() < (size_t)kWindow) preps.resize(kWindow);
+    for (int k0 = 0; k0 < n; k0 += kWindow) {
+        const int k1 = std::min(n, k0 + kWindow);
+        std::atomic<int> next{k0};
+        auto work = [&] {
+            for (int k = next.fetch_add(1); k < k1; k = next.fetch_add(1)) prep_solve(mds[k], cfgs[k], &sds[k], preps[k - k0]);
+        };
+        std::vector<std::thread> pool;
+        for (int t = 1; t < std::min(threads, k1 - k0); ++t) pool.emplace_back(work);
+        work();
+        for (auto &t : pool) t.join();
+        std::lock_guard<std::mutex> lk(b->mu);
+        b->err.clear();
+        for (int k = k0; k < k1; ++k) {
+            prandtl_status st = admit_prepared(b, mds[k], cfgs[k], u0s[k], ptr_flags, &sds[k], preps[k - k0], &ids[k]);
+            if (st != PRANDTL_OK) {
+                b->err = "solve " + std::to_string(k) + ": " + b->err;
+                for (auto &q : preps) q.trim();
+                return st;
+            }
+        }
+        for (int k = k0; k < k1; ++k) preps[k - k0].trim();
+    }
     return PRANDTL_OK;
 }
 
@@ -684,6 +885,7 @@ prandtl_status prandtl_batch_advance(prandtl_batch *b, int nsteps) {
     b->err.clear();
     if (nsteps == 0 || b->classes.empty()) return PRANDTL_OK;
     BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
+    if (prandtl_status fs = flush_tables(b); fs != PRANDTL_OK) return fs;
     const long long per_step = launches_per_step(b);
     while (nsteps > 0 && b->tune_left > 0) {   // tuning inside the first steps
         prandtl_status st = tune_step(b, b->nvar - b->tune_left);
@@ -809,6 +1011,40 @@ prandtl_status prandtl_batch_read(prandtl_batch *b, int id, double *u, int ptr_f
     return st;
 }
 
+prandtl_status prandtl_batch_read_many(prandtl_batch *b, int n, const int *ids, double *const *u, int ptr_flags) {
+    if (!b) return PRANDTL_EINVAL;
+    if (n < 0 || (n > 0 && (!ids || !u))) return bfail(b, PRANDTL_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(b->mu);
+    for (int k = 0; k < n; ++k) {
+        if (ids[k] < 0 || ids[k] >= b->cap || !b->solves[ids[k]].used)
+            return bfail(b, PRANDTL_EINVAL, "unknown solve id " + std::to_string(ids[k]));
+        if (!u[k]) return bfail(b, PRANDTL_EINVAL, "null argument");
+    }
+    if (n == 0) return PRANDTL_OK;
+    BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
+    // every record's LSRK parity and state-check bits in one copy
+    if (!b->h_tab) BCK(b, cudaMallocHost(&b->h_tab, (size_t)b->cap * sizeof(BatchInst)), "pinned solve records");
+    BCK(b, cudaMemcpyAsync(b->h_tab, b->d_tab, (size_t)b->cap * sizeof(BatchInst), cudaMemcpyDeviceToHost, b->stream),
+        "D2H solve records");
+    prandtl_status st = bwait(b);
+    if (st != PRANDTL_OK) return st;
+    for (int k = 0; k < n; ++k) {
+        const Solve &s = b->solves[ids[k]];
+        const int cur = b->cfg.scheme == PRANDTL_LSRK45 ? b->h_tab[ids[k]].cur : 0;
+        const size_t S = (size_t)s.nf * s.Ndof * sizeof(double);
+        BCK(b, cudaMemcpyAsync(u[k], b->arena + s.off + s.L.u[cur & 1], S,
+                               (ptr_flags & PRANDTL_PTR_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                               b->stream),
+            "copy state");
+    }
+    if ((st = bwait(b)) != PRANDTL_OK) return st;
+    for (int k = 0; k < n; ++k)
+        if (b->h_tab[ids[k]].health != 0)
+            return bfail(b, PRANDTL_ENONFINITE,
+                         "solve " + std::to_string(ids[k]) + ": " + health_text((unsigned)b->h_tab[ids[k]].health));
+    return PRANDTL_OK;
+}
+
 prandtl_status prandtl_batch_budgets(prandtl_batch *b, int id, double *out) {
     if (!b) return PRANDTL_EINVAL;
     if (!out) return bfail(b, PRANDTL_EINVAL, "null argument");
@@ -851,11 +1087,10 @@ prandtl_status prandtl_batch_remove(prandtl_batch *b, int id) {
     Class &c = b->classes.at(s.key);
     c.ids.erase(std::find(c.ids.begin(), c.ids.end(), id));
     b->live.erase(std::find(b->live.begin(), b->live.end(), id));
-    prandtl_status st = upload_class(b, c);
-    if (st == PRANDTL_OK) st = upload_live(b);
+    c.tables_dirty = true;   // uploaded before the next launches
+    b->live_dirty = true;
     const int zero = 0;
-    if (st == PRANDTL_OK)
-        BCK(b, cudaMemcpyAsync(b->d_left + id, &zero, sizeof(int), cudaMemcpyHostToDevice, b->stream), "reset steps");
+    prandtl_status st = up_copy(b, b->d_left + id, &zero, sizeof(int));
     // later uploads into this range are ordered after the work already enqueued
     b->alloc.release(s.off, s.L.total);
     s = Solve();
@@ -884,7 +1119,9 @@ prandtl_status prandtl_batch_tune(prandtl_batch *b, int reps) {
     b->err.clear();
     b->tune_left = 0;   // replaces tuning inside the steps
     BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
-    prandtl_status st = bwait(b);
+    prandtl_status st = flush_tables(b);
+    if (st != PRANDTL_OK) return st;
+    st = bwait(b);
     if (st != PRANDTL_OK) return st;
     const bool fp32 = b->cfg.precision == 1;
     // The first stage reads the step-start state and writes only the other RK

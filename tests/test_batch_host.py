@@ -42,6 +42,8 @@ def test_null_batch_and_server_calls_fail_cleanly():
     assert L.prandtl_batch_remove(None, 0) == _lib.PRANDTL_EINVAL
     assert L.prandtl_batch_tune(None, 1) == _lib.PRANDTL_EINVAL
     assert L.prandtl_batch_tune_in_steps(None) == _lib.PRANDTL_EINVAL
+    assert L.prandtl_batch_read_many(None, 0, None, None, 0) == _lib.PRANDTL_EINVAL
+    assert L.prandtl_batch_add_many(None, 0, None, None, None, 0, None, None) == _lib.PRANDTL_EINVAL
     assert L.prandtl_batch_kernel_launches(None) == 0
     assert L.prandtl_serve_destroy(None) == _lib.PRANDTL_EINVAL
     assert L.prandtl_serve_create(None, 1, None) == _lib.PRANDTL_EINVAL

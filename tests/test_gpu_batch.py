@@ -172,6 +172,55 @@ def test_tuning_inside_steps_keeps_results():
         assert np.array_equal(a, c)
 
 
+def test_many_admissions_through_the_upload_ring_and_read_many():
+    """Enough admissions that their geometry, neighbour tables and normals wrap
+    the 32 MB pinned upload ring; the class tables go up once,
+    before the first launches.  A sample of solves matches the FP64 plain path
+    and read_many returns exactly what read returns."""
+    ens = tgv_ensemble(160, n_range=(10, 12), orders=(2, 3), seed=7)   # ~53 MB of uploads
+    items = _setup(ens, cfl=0.2)
+    b = Batch("fp64", arena_bytes=4 << 30)
+    ids = [b.add(mesh, u0, dt=dt, nsteps=2, **m.physics()) for m, mesh, u0, dt in items]
+    b.advance(2)
+    many = b.read_many(ids)
+    for k in list(range(0, len(items), 23)) + [len(items) - 1]:
+        m, mesh, u0, dt = items[k]
+        assert np.array_equal(many[k], b.read(ids[k]))
+        assert norm_err(many[k], plain(m, u0, dt, 2), mesh.num_fields) <= 1e-12
+    b.close()
+
+
+def test_add_many_matches_add_and_stops_at_a_bad_solve():
+    """add_many prepares the solves on host threads and admits them in order:
+    the states match one-by-one admission bit for bit; a solve whose mesh
+    fails the checks stops the call there, the solves before it stay
+    admitted and the ids from it on are -1."""
+    from prandtl_b200._lib import PrandtlError
+    items = _setup(MIX)
+    spec = [(mesh, u0, dict(dt=dt, nsteps=3, **m.physics())) for m, mesh, u0, dt in items]
+    b1 = Batch("fp32", arena_bytes=1 << 30)
+    ids1 = [b1.add(mesh, u0, **kw) for mesh, u0, kw in spec]
+    b2 = Batch("fp32", arena_bytes=1 << 30)
+    ids2 = b2.add_many(spec)
+    assert sorted(ids2) == sorted(set(ids2)) and min(ids2) >= 0
+    b1.advance(3)
+    b2.advance(3)
+    for i1, i2 in zip(ids1, ids2):
+        assert np.array_equal(b1.read(i1), b2.read(i2))
+    b1.close()
+    b2.close()
+    # a mesh with a non-positive det J in the middle of the list
+    bad_mesh, bad_u0, bad_kw = spec[1]
+    import copy
+    bad = copy.deepcopy(bad_mesh)
+    bad.elem_detj[0] = -1.0
+    b3 = Batch("fp32", arena_bytes=1 << 30)
+    with pytest.raises(PrandtlError) as ei:
+        b3.add_many([spec[0], (bad, bad_u0, bad_kw), spec[2]])
+    assert "solve 1" in str(ei.value)
+    b3.close()
+
+
 def test_cfl_time_step_follows_lambda():
     m = Member("tgv", 3, 2, 0.2, 400.0)
     mesh = m.mesh()
