@@ -21,6 +21,7 @@
 #include <iterator>
 #include <map>
 #include <mutex>
+#include <new>
 #include <string>
 #include <thread>
 #include <vector>
@@ -857,7 +858,14 @@ prandtl_status prandtl_batch_add_many(prandtl_batch *b, int n, const prandtl_mes
         const int k1 = std::min(n, k0 + kWindow);
         std::atomic<int> next{k0};
         auto work = [&] {
-            for (int k = next.fetch_add(1); k < k1; k = next.fetch_add(1)) prep_solve(mds[k], cfgs[k], &sds[k], preps[k - k0]);
+            for (int k = next.fetch_add(1); k < k1; k = next.fetch_add(1)) {
+                try {
+                    prep_solve(mds[k], cfgs[k], &sds[k], preps[k - k0]);
+                } catch (const std::bad_alloc &) {   // host memory for the tables
+                    preps[k - k0].st = PRANDTL_ENOMEM;
+                    preps[k - k0].msg = "host memory for the mesh tables";
+                }
+            }
         };
         std::vector<std::thread> pool;
         for (int t = 1; t < std::min(threads, k1 - k0); ++t) pool.emplace_back(work);
