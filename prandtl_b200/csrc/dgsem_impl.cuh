@@ -1912,15 +1912,19 @@ struct LiftLayout {
 constexpr int prev_pow2(int v) { return v <= 1 ? 1 : 2 * prev_pow2(v / 2); }
 // Batch lift CTA: a power-of-two number of elements, so an item (one CTA's
 // elements) never straddles two solves' BATCH_CHUNK-padded ranges.
-template <int DIM, int NP>
+template <int DIM, int NP, typename Out>
 struct LiftBatchShape {
     static constexpr int ND = Shape<DIM, NP>::ND;
-    static constexpr int EPB = prev_pow2(cmax(1, 128 / ND));
+    // FP32 27-node elements (3D, N = 2): 8 per CTA (216 threads) fill 96 % of
+    // the lanes against 84 % with 4 (measured on the one-shot FP32 lift: -14 %
+    // at 4 resident CTAs)
+    static constexpr bool WIDE27 = sizeof(Out) == 4 && ND == 27;
+    static constexpr int EPB = WIDE27 ? 8 : prev_pow2(cmax(1, 128 / ND));
     static constexpr int THREADS = EPB * ND;
     // resident CTAs the FP32 lift's register budget is sized for (measured on the
     // 3D Navier-Stokes classes: 5 beats 4 by up to 13 %; 6 is better still at
-    // Np = 5, N = 4); the FP64 lift keeps 4
-    static constexpr int MIN_BLOCKS32 = (DIM == 3 && NP == 5) ? 6 : 5;
+    // Np = 5, N = 4; 4 for the 216-thread CTAs of N = 2); the FP64 lift keeps 4
+    static constexpr int MIN_BLOCKS32 = WIDE27 ? 4 : ((DIM == 3 && NP == 5) ? 6 : 5);
     static_assert(BATCH_CHUNK % EPB == 0, "lift item must divide the padding chunk");
 };
 
@@ -1965,11 +1969,11 @@ lift_kernel(const MeshDev m, const LiftArgs a, const PhysParams P, const __grid_
 
 // Persistent batch lift: CTA-level items of EPB elements of one solve.
 template <int DIM, int NP, typename Out, bool VC>
-__global__ void __launch_bounds__(LiftBatchShape<DIM, NP>::THREADS,
-                                  sizeof(Out) == 8 ? 4 : LiftBatchShape<DIM, NP>::MIN_BLOCKS32)
+__global__ void __launch_bounds__(LiftBatchShape<DIM, NP, Out>::THREADS,
+                                  sizeof(Out) == 8 ? 4 : LiftBatchShape<DIM, NP, Out>::MIN_BLOCKS32)
 lift_batch_kernel(const BatchClassDev c, const BatchStage st, const __grid_constant__ OpTables T) {
     using S = Shape<DIM, NP>;
-    using LB = LiftBatchShape<DIM, NP>;
+    using LB = LiftBatchShape<DIM, NP, Out>;
     constexpr int TABB = (S::TAB * (int)sizeof(Out) + 15) / 16 * 16;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Out *sT = reinterpret_cast<Out *>(smem_raw);
@@ -2022,7 +2026,7 @@ template <int DIM, int NP, typename Out>
 size_t lift_batch_smem() {
     using S = Shape<DIM, NP>;
     return (S::TAB * sizeof(Out) + 15) / 16 * 16 + CTX_RESERVE +
-           sizeof(Out) * (size_t)LiftBatchShape<DIM, NP>::EPB * LiftLayout<DIM, NP, Out>::PER_ELEM;
+           sizeof(Out) * (size_t)LiftBatchShape<DIM, NP, Out>::EPB * LiftLayout<DIM, NP, Out>::PER_ELEM;
 }
 
 // The dynamic shared-memory limit of a kernel, raised once per device (the
@@ -2132,7 +2136,7 @@ cudaError_t rhs_batch_launch_np(int grid, const BatchClassDev &c, const BatchSta
 }
 template <int DIM, int NP, typename Out, bool VC>
 cudaError_t lift_batch_prepare_np(BatchKernelInfo *info) {
-    using S = LiftBatchShape<DIM, NP>;
+    using S = LiftBatchShape<DIM, NP, Out>;
     const size_t sm = lift_batch_smem<DIM, NP, Out>();
     cudaError_t err = cudaFuncSetAttribute(lift_batch_kernel<DIM, NP, Out, VC>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -2152,7 +2156,7 @@ cudaError_t lift_batch_prepare_np(BatchKernelInfo *info) {
 template <int DIM, int NP, typename Out, bool VC>
 cudaError_t lift_batch_launch_np(int grid, const BatchClassDev &c, const BatchStage &st, const OpTables &T,
                                  cudaStream_t s) {
-    using S = LiftBatchShape<DIM, NP>;
+    using S = LiftBatchShape<DIM, NP, Out>;
     lift_batch_kernel<DIM, NP, Out, VC><<<grid, S::THREADS, lift_batch_smem<DIM, NP, Out>(), s>>>(c, st, T);
     return cudaGetLastError();
 }
