@@ -900,7 +900,14 @@ prandtl_status prandtl_batch_advance(prandtl_batch *b, int nsteps) {
         if (st != PRANDTL_OK) return st;
         b->launches += per_step;
         --nsteps;
-        if (--b->tune_left == 0) tune_finish(b);
+        if (--b->tune_left == 0) {
+            tune_finish(b);
+            // capture the tuned shapes' graphs now rather than in the next call
+            if (b->cfg.use_graph && b->graph_dirty) {
+                prandtl_status gs = rebuild_graphs(b);
+                if (gs != PRANDTL_OK) return gs;
+            }
+        }
     }
     if (nsteps == 0) return PRANDTL_OK;
     if (!b->cfg.use_graph) {
