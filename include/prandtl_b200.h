@@ -166,7 +166,11 @@ void prandtl_config_default(prandtl_config *cfg);
 
 /* Build an operator for one mesh (DGSEMOperator ctor, DGSEMOperator.cpp:5-50,
  * plus DGSEMIntegrator ctor tables, DGSEMIntegrator.cpp:8-149).  Selects the
- * current CUDA device.  Allocates all device memory it will ever use. */
+ * current CUDA device.  Allocates all device memory it will ever use.  The
+ * first host-pointer call (prandtl_rhs / prandtl_step with PRANDTL_PTR_HOST)
+ * on a state above 4 MB also allocates a 32 MB pinned host staging ring,
+ * kept until prandtl_destroy, through which such calls copy the state in
+ * 8 MB chunks filled and emptied by host threads. */
 prandtl_status prandtl_create(const prandtl_mesh_desc *mesh, const prandtl_config *cfg,
                               prandtl_handle **out);
 
