@@ -388,7 +388,9 @@ prandtl_status prandtl_batch_destroy(prandtl_batch *b);
 prandtl_status prandtl_batch_footprint(prandtl_batch *b, const prandtl_mesh_desc *mesh,
                                        const prandtl_config *cfg, size_t *bytes);
 /* Admit a solve with initial state u0 (byNODES; host or device per ptr_flags).
- * cfg->precision is ignored (the batch's applies). */
+ * cfg->precision is ignored (the batch's applies).  The mesh tables go up
+ * through a 32 MB pinned host ring the first admission allocates (kept until
+ * prandtl_batch_destroy); the class tables go up before the next launches. */
 prandtl_status prandtl_batch_add(prandtl_batch *b, const prandtl_mesh_desc *mesh, const prandtl_config *cfg,
                                  const double *u0, int ptr_flags, const prandtl_solve_desc *solve, int *id);
 /* prandtl_batch_add of n solves (mesh[k], cfg[k], u0[k], sd[k] -> ids[k]):
