@@ -101,21 +101,23 @@ namespace {
 
 // memcpy split over a small persistent pool of host threads (one call at a
 // time; a process forked after the pool started copies on its calling thread,
-// since the workers do not exist there).
+// since the workers do not exist there).  The pool is never destroyed: its
+// workers sleep on a condition variable until the process ends, and a forked
+// child never joins threads it does not have.
 class CopyPool {
   public:
     static CopyPool &get() {
-        static CopyPool pool;
-        return pool;
+        static CopyPool *pool = new CopyPool();
+        return *pool;
     }
     // max_parts: how many threads (the caller included) share the copy
     void copy(void *dst, const void *src, size_t n, int max_parts) {
-        if (n < (size_t(1) << 20) || workers_.empty() || getpid() != pid_ || max_parts < 2) {
+        if (n < (size_t(1) << 20) || workers_ == 0 || getpid() != pid_ || max_parts < 2) {
             std::memcpy(dst, src, n);
             return;
         }
         std::lock_guard<std::mutex> call(call_mu_);
-        const int parts = std::min((int)workers_.size() + 1, max_parts);
+        const int parts = std::min(workers_ + 1, max_parts);
         {
             std::lock_guard<std::mutex> lk(mu_);
             dst_ = static_cast<char *>(dst);
@@ -130,21 +132,15 @@ class CopyPool {
         std::unique_lock<std::mutex> lk(mu_);
         done_cv_.wait(lk, [&] { return pending_ == 0; });
     }
-    ~CopyPool() {
-        {
-            std::lock_guard<std::mutex> lk(mu_);
-            stop_ = true;
-        }
-        cv_.notify_all();
-        for (auto &t : workers_)
-            if (t.joinable()) t.join();
-    }
-
   private:
     CopyPool() : pid_(getpid()) {
         const unsigned hw = std::thread::hardware_concurrency();
         const int n = (int)std::min(12u, hw > 1 ? hw * 3 / 4 : 1u) - 1;
-        for (int i = 1; i <= n; ++i) workers_.emplace_back([this, i] { loop(i); });
+        for (int i = 1; i <= n; ++i) {
+            std::thread t([this, i] { loop(i); });
+            t.detach();
+            ++workers_;
+        }
     }
     void part(int i) {
         // 64-byte aligned split points
@@ -157,8 +153,7 @@ class CopyPool {
         for (;;) {
             {
                 std::unique_lock<std::mutex> lk(mu_);
-                cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
-                if (stop_) return;
+                cv_.wait(lk, [&] { return gen_ != seen; });
                 seen = gen_;
                 if (i >= parts_) continue;   // not one of this copy's parts
             }
@@ -167,12 +162,11 @@ class CopyPool {
             if (--pending_ == 0) done_cv_.notify_one();
         }
     }
-    std::vector<std::thread> workers_;
+    int workers_ = 0;
     std::mutex call_mu_, mu_;
     std::condition_variable cv_, done_cv_;
     unsigned gen_ = 0;
     int pending_ = 0, parts_ = 1;
-    bool stop_ = false;
     char *dst_ = nullptr;
     const char *src_ = nullptr;
     size_t n_ = 0;
